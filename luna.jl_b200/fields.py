@@ -1,0 +1,83 @@
+"""Input pulses and energy functions (host setup of the initial state y0).
+
+Restates Luna.jl ``src/Fields.jl``: ``PulseField`` with Gaussian / sech^2 shapes
+(Fields.jl:40-145), the instantaneous power ``It`` (Fields.jl:503-504) and
+``energyfuncs`` (Fields.jl:510-533). Simpson integration follows
+NumericalIntegration.jl's ``SimpsonEven`` rule (composite 3/8-style end correction).
+"""
+import math
+
+import numpy as np
+
+from . import physdata as pd
+from .maths import gauss
+
+
+def simpson_even(x, y):
+    """NumericalIntegration.jl ``integrate(x, y, SimpsonEven())`` for uniform x."""
+    y = np.asarray(y)
+    n = len(y)
+    h = x[1] - x[0]
+    retval = (17 * (y[0] + y[-1]) + 59 * (y[1] + y[-2]) + 43 * (y[2] + y[-3])
+              + 49 * (y[3] + y[-4])) / 48
+    retval = retval + np.sum(y[4:n - 4])
+    return h * retval
+
+
+def analytic(x):
+    """Analytic signal (Maths.jl:560-569)."""
+    xf = np.fft.fft(x)
+    n = len(x)
+    n1 = n // 2
+    xf[1:n1] *= 2
+    xf[n1:] = 0
+    return np.fft.ifft(xf)
+
+
+def It(Et, grid):
+    if grid.kind == "real":
+        return np.abs(analytic(Et)) ** 2
+    return np.abs(Et) ** 2
+
+
+def energy_t(grid, Et):
+    return simpson_even(grid.t, It(Et, grid))
+
+
+def to_freq_coarse(grid, Et):
+    """Forward transform on the coarse grid: rfft (real) / fft (envelope), unnormalised."""
+    return np.fft.rfft(Et) if grid.kind == "real" else np.fft.fft(Et)
+
+
+class PulseField:
+    def __init__(self, λ0, Itshape, energy=None, power=None):
+        if (energy is None) == (power is None):
+            raise ValueError("exactly one of energy or power must be given")
+        self.λ0, self.Itshape, self.energy, self.power = λ0, Itshape, energy, power
+
+    def __call__(self, grid):
+        t = grid.t
+        ω0 = pd.wlfreq(self.λ0)
+        if grid.kind == "real":
+            Et = np.sqrt(self.Itshape(t)) * np.cos(ω0 * t)
+        else:
+            Δω = ω0 - grid.ω0
+            Et = np.sqrt(self.Itshape(t)) * np.exp(1j * (Δω * t))
+        if self.energy is not None:
+            Et = Et * (math.sqrt(self.energy) / math.sqrt(energy_t(grid, Et)))
+        else:
+            Et = Et * (math.sqrt(self.power) / math.sqrt(np.max(It(Et, grid))))
+        return to_freq_coarse(grid, Et)
+
+
+def GaussField(λ0, τfwhm, energy=None, power=None, m=1):
+    return PulseField(λ0, lambda t: gauss(t, τfwhm, power=2 * m), energy, power)
+
+
+def SechField(λ0, τfwhm=None, τw=None, energy=None, power=None):
+    if τw is None:
+        τw = τfwhm / (2 * math.log(1 + math.sqrt(2)))
+    def shape(t):
+        with np.errstate(over="ignore"):
+            return 1 / np.cosh(t / τw) ** 2
+    return PulseField(λ0, shape, energy, power)

@@ -1,0 +1,106 @@
+"""Waveguide modes that feed the linear operator and normalisation (host setup).
+
+* ``SimpleMode``: Taylor-expanded propagation constant for the GNLSE
+  (SimpleFibre.jl:9-53).
+* ``MarcatiliMode``: hollow-capillary HE/TE/TM modes with the complex effective index of
+  Marcatili & Schmeltzer (Capillary.jl:29-186), effective area (Capillary.jl:284-300)
+  and the group delay beta1 by a central finite difference (the reference uses
+  FiniteDifferences.jl, Maths.jl:18-32).
+"""
+import math
+
+import numpy as np
+from scipy import integrate, special
+
+from . import physdata as pd
+
+
+class SimpleMode:
+    def __init__(self, ωref, βs, Aeff=1.0, loss=0.0):
+        self.ωref = ωref
+        self.coef = [b / math.factorial(i) for i, b in enumerate(βs)]
+        self._Aeff = Aeff
+        self._α = math.log(10) / 10 * loss
+
+    def β(self, ω):
+        x = np.asarray(ω, dtype=np.float64) - self.ωref
+        out = np.zeros_like(x)
+        for cf in reversed(self.coef):  # Horner, as Polynomials.jl evaluates
+            out = out * x + cf
+        return out
+
+    def α(self, ω):
+        return np.full_like(np.asarray(ω, dtype=np.float64), self._α)
+
+    def dispersion(self, order, ω):
+        coef = list(self.coef)
+        for _ in range(order):
+            coef = [coef[i] * i for i in range(1, len(coef))]
+        x = ω - self.ωref
+        out = 0.0
+        for cf in reversed(coef):
+            out = out * x + cf
+        return out
+
+    def Aeff(self, z=0.0):
+        return self._Aeff
+
+
+def _unm(n, m, kind):
+    if kind in ("TE", "TM"):
+        return special.jn_zeros(1, m)[-1]
+    return special.jn_zeros(n - 1, m)[-1]
+
+
+class MarcatiliMode:
+    """Hollow capillary mode filled with ``gas`` at pressure ``P`` (Capillary.jl:95-109)."""
+
+    def __init__(self, a, gas, P, n=1, m=1, kind="HE", T=pd.roomtemp, model="full", loss=True):
+        self.a, self.n, self.m, self.kind = a, n, m, kind
+        self.model, self.loss = model, loss
+        self.unm = _unm(n, m, kind)
+        self.coren = pd.ref_index_fun(gas, P, T) if gas is not None else (lambda lam: 1.0 + 0j)
+        den, _ = integrate.quad(lambda r: r * special.jv(n - 1, self.unm * r) ** 4, 0, 1,
+                                epsabs=0, epsrel=1e-12, limit=200)
+        np1 = n if kind == "HE" else 2
+        num = 0.25 * special.jv(np1, self.unm) ** 4
+        self.aeff_intg = 2 * math.pi * num / den
+
+    def _vn(self, εcl):
+        εcl = np.asarray(εcl, dtype=complex)
+        if self.kind == "HE":
+            return (εcl + 1) / (2 * np.sqrt(εcl - 1))
+        if self.kind == "TE":
+            return 1 / np.sqrt(εcl - 1)
+        return εcl / np.sqrt(εcl - 1)
+
+    def neff(self, ω):
+        ω = np.asarray(ω, dtype=np.float64)
+        lam = pd.wlfreq(ω)
+        εcl = pd.sio2_index(lam) ** 2
+        εco = self.coren(lam) ** 2
+        vn = self._vn(εcl)
+        k = ω / pd.c
+        nn = np.sqrt(εco - (self.unm / (k * self.a)) ** 2 * (1 - 1j * vn / (k * self.a)) ** 2)
+        if not self.loss:
+            nn = np.real(nn) + 0j
+        re = np.where(np.real(nn) < 1e-3, 1e-3, np.real(nn))
+        im = np.where(np.real(nn) < 1e-3, np.clip(np.imag(nn), 0, None), np.imag(nn))
+        return re + 1j * im
+
+    def β(self, ω):
+        return np.asarray(ω) / pd.c * np.real(self.neff(ω))
+
+    def α(self, ω):
+        return 2 * np.asarray(ω) / pd.c * np.imag(self.neff(ω))
+
+    def dispersion(self, order, ω):
+        if order != 1:
+            raise NotImplementedError
+        h = ω * 1e-4
+        # 4th-order central difference for d(beta)/d(omega)
+        f = lambda x: float(self.β(np.array([x]))[0])
+        return (-f(ω + 2 * h) + 8 * f(ω + h) - 8 * f(ω - h) + f(ω - 2 * h)) / (12 * h)
+
+    def Aeff(self, z=0.0):
+        return self.a ** 2 * self.aeff_intg

@@ -1,0 +1,143 @@
+"""Raman response models (host setup of the device response tables).
+
+Restates Luna.jl ``src/Raman.jl``: the normalised single damped oscillator
+(Raman.jl:53-65), the molecular vibrational model (Raman.jl:142-157), the non-rigid rotor
+sum over J (Raman.jl:196-240) and ``CombinedRamanResponse`` (Raman.jl:242-262).
+
+A response is reduced to what the device needs to rebuild h(t; rho) on the Raman
+grid: for each component its undamped response ``hpre_i(t)`` sampled on
+``tt = (0..N-1)*dt``, its density-dependent dephasing time ``tau2_i(rho)`` and the
+Planck-taper window ``w`` (Raman.jl:249-262). The device forms
+``h = w * sum_i hpre_i * exp(-tt/tau2_i)`` and transforms it.
+"""
+import math
+
+import numpy as np
+
+from . import physdata as pd
+from .maths import planck_taper
+
+
+class SDO:
+    """Single damped oscillator K*sin(Omega t), t>0, with dephasing tau2(rho)."""
+
+    def __init__(self, K, Omega, tau2fun):
+        self.K, self.Omega, self.tau2fun = K, Omega, tau2fun
+
+    def hrpre(self, t):
+        t = np.asarray(t, dtype=np.float64)
+        return np.where(t > 0.0, self.K * np.sin(self.Omega * t), 0.0)
+
+    def hrdamp(self, rho):
+        return self.tau2fun(rho)
+
+    def __call__(self, t, rho):
+        return self.hrpre(t) * np.exp(-np.asarray(t) / self.hrdamp(rho))
+
+
+def RamanRespNormedSingleDampedOscillator(K, Omega, tau2):
+    """SDO normalised to unit integral then scaled by K (Raman.jl:53-59)."""
+    K = K * (Omega ** 2 + 1 / tau2 ** 2) / Omega
+    return SDO(K, Omega, lambda rho: tau2)
+
+
+def RamanRespVibrational(Omega_v, dadQ, mu, tau2=None, Brho=None, Arho=None, C=0.0):
+    """Molecular vibrational Raman oscillator (Raman.jl:142-157)."""
+    K = (4 * math.pi * pd.eps_0) ** 2 * dadQ ** 2 / (4 * mu * Omega_v)
+    if Brho is None:
+        if tau2 is None:
+            raise ValueError("one of tau2 or Brho must be specified")
+        f = lambda rho: tau2
+    else:
+        f = lambda rho: 1 / (math.pi * (C + Arho / (rho / pd.amg) + Brho * rho / pd.amg))
+    return SDO(K, Omega_v, f)
+
+
+class RotationalNonRigid:
+    """Sum of SDOs over rotational J -> J+2 transitions (Raman.jl:196-240)."""
+
+    def __init__(self, B, dalpha, qJodd, qJeven, D=0.0, minJ=0, maxJ=50, temp=pd.roomtemp,
+                 tau2=None, Brho=None, Arho=None):
+        J = np.arange(minJ, maxJ + 1)
+        EJ = 2 * math.pi * pd.hbar * pd.c * (B * J * (J + 1) - D * (J * (J + 1)) ** 2)
+        dE = np.diff(EJ)
+        neg = np.nonzero(dE < 0)[0]
+        if len(neg):
+            mJ = neg[0] + 1  # 1-based index of the last monotonic level
+            J = J[:mJ]
+            EJ = EJ[:mJ]
+        DJ = np.where(J % 2 == 1, qJodd, qJeven)
+        rhoJ = DJ * (2 * J + 1) * np.exp(-EJ / (pd.k_B * temp))
+        rhoJ = rhoJ / np.sum(rhoJ)
+        Js = J[:-2]
+        Om = (EJ[2:] - EJ[:-2]) / pd.hbar
+        K = -(4 * math.pi * pd.eps_0) ** 2 * 2 / 15 * dalpha ** 2 / pd.hbar
+        if Brho is None:
+            if tau2 is None:
+                raise ValueError("one of tau2 or Brho must be specified")
+            self.tau2fun = lambda rho: tau2
+        else:
+            self.tau2fun = lambda rho: (1 / (math.pi * (Arho / (rho / pd.amg) + Brho * rho / pd.amg))
+                                        if rho > 0 else math.inf)
+        self.Rs = [SDO(K * (Js[i] + 1) * (Js[i] + 2) / (2 * Js[i] + 3)
+                       * (rhoJ[i + 2] / (2 * Js[i] + 5) - rhoJ[i] / (2 * Js[i] + 1)),
+                       Om[i], self.tau2fun) for i in range(len(Js))]
+
+    def hrpre(self, t):
+        return sum(R.hrpre(t) for R in self.Rs)
+
+    def hrdamp(self, rho):
+        return self.tau2fun(rho)
+
+    def __call__(self, t, rho):
+        return self.hrpre(t) * np.exp(-np.asarray(t) / self.hrdamp(rho))
+
+
+class CombinedRamanResponse:
+    """Raman response on the grid ``t`` as the sum of several damped components."""
+
+    def __init__(self, t, Rs):
+        t = np.asarray(t, dtype=np.float64)
+        self.Rs = list(Rs)
+        self.dt = t[1] - t[0]
+        self.tt = np.arange(len(t), dtype=np.float64) * self.dt
+        self.hpres = [R.hrpre(self.tt) for R in self.Rs]
+        te = self.tt[-1]
+        self.w = planck_taper(self.tt, -te, -te * 0.7, te * 0.7, te)
+
+    def tau2s(self, rho):
+        return [R.hrdamp(rho) for R in self.Rs]
+
+    def h(self, rho):
+        """h(t; rho) on tt (Raman.jl:256-262): sum of damped components times window."""
+        ht = np.zeros_like(self.tt)
+        for hp, R in zip(self.hpres, self.Rs):
+            ht += hp * np.exp(-self.tt / R.hrdamp(rho))
+        return ht * self.w
+
+
+def molecular_raman_response(t, rp, rotation=True, vibration=True, minJ=0, maxJ=50,
+                             temp=pd.roomtemp):
+    """Rotational + vibrational response for a molecular gas (Raman.jl:279-307)."""
+    Rs = []
+    if rotation and rp.get("rotation") == "nonrigid":
+        if "Brho_r" in rp:
+            Rs.append(RotationalNonRigid(rp["B"], rp["dalpha"], rp["qJodd"], rp["qJeven"],
+                                         D=rp["D"], minJ=minJ, maxJ=maxJ, temp=temp,
+                                         Brho=rp["Brho_r"], Arho=rp["Arho_r"]))
+        else:
+            Rs.append(RotationalNonRigid(rp["B"], rp["dalpha"], rp["qJodd"], rp["qJeven"],
+                                         D=rp["D"], minJ=minJ, maxJ=maxJ, temp=temp,
+                                         tau2=rp["tau2_r"]))
+    if vibration and rp.get("vibration") == "sdo":
+        if "Brho_v" in rp:
+            Rs.append(RamanRespVibrational(rp["Omega_v"], rp["dadQ"], rp["mu"],
+                                           Brho=rp["Brho_v"], Arho=rp["Arho_v"],
+                                           C=rp.get("Cv", 0.0)))
+        else:
+            Rs.append(RamanRespVibrational(rp["Omega_v"], rp["dadQ"], rp["mu"], tau2=rp["tau2_v"]))
+    return CombinedRamanResponse(t, Rs)
+
+
+def raman_response(t, gas, **kw):
+    return molecular_raman_response(t, pd.raman_parameters(gas), **kw)

@@ -1,0 +1,411 @@
+"""FP64 numpy restatement of the UPPE hot path (test infrastructure only).
+
+Every function cites the reference file:line it follows (Luna.jl v0.6.2). The
+transform object it consumes is the same ``TransModeAvg`` description that the device
+plan is built from, so both sides see identical inputs.
+"""
+import math
+
+import numpy as np
+
+# ------------------------------------------------------------------- Maths.cumtrapz!
+
+def cumtrapz(y, dx):
+    """Running trapezoid integral (Maths.jl:323-328).
+
+    ``out[i] = out[i-1] + 1/2*(y[i-1]+y[i])*dx`` evaluated left to right; numpy's
+    cumsum is a sequential left-to-right sum, so the rounding matches the reference.
+    """
+    inc = np.empty_like(y)
+    inc[0] = 0.0
+    inc[1:] = (0.5 * (y[:-1] + y[1:])) * dx
+    return np.cumsum(inc)
+
+
+# ------------------------------------------------------------------- rate functions
+
+def ppt_rate(spl, E):
+    """PPT log-rate spline closure (Ionisation.jl:257-270, Maths.jl:764-848).
+
+    Raises ``ValueError`` for fields above the table maximum, as the reference errors.
+    """
+    aE = np.abs(E)
+    out = np.zeros_like(aE)
+    if np.any(aE > spl.Emax):
+        raise ValueError(f"Field strength {aE.max()} V/m exceeds maximum for PPT "
+                         f"ionisation rate ({spl.Emax} V/m).")
+    m = aE >= spl.Emin
+    x0 = aE[m]
+    x, y, D = spl.x, spl.y, spl.D
+    n = len(x)
+    xmin, xmax = x[0], x[-1]
+    # uniform-axis index function (Maths.jl:772-774), 1-based
+    i1 = np.where(x0 <= xmin, 2,
+                  np.where(x0 >= xmax, n,
+                           np.ceil((x0 - xmin) / (xmax - xmin) * (n - 1)).astype(np.int64) + 1))
+    i = i1 - 1  # 0-based index of the knot above x0
+    xi, xim = x[i], x[i - 1]
+    yi, yim = y[i], y[i - 1]
+    Di, Dim = D[i], D[i - 1]
+    t = (x0 - xim) / (xi - xim)
+    val = (yim + Dim * t + (3 * (yi - yim) - 2 * Dim - Di) * t ** 2
+           + (2 * (yim - yi) + Dim + Di) * t ** 3)
+    val = np.where(x0 == xi, yi, np.where(x0 == xim, yim, val))
+    out[m] = np.exp(val)
+    return out
+
+
+def adk_rate(r, E):
+    """ADK closure (Ionisation.jl:43-59)."""
+    aE = np.abs(E)
+    out = np.zeros_like(aE)
+    m = aE >= r.thr
+    x = aE[m]
+    out[m] = (r.w_p * r.cn_sq * (4 * r.w_p / (r.w_t_prefac * x)) ** (2 * r.nstar - 1)
+              * np.exp(-4 / 3 * r.w_p / (r.w_t_prefac * x)))
+    return out
+
+
+def rate(ratefunc, E):
+    if ratefunc.kind == "adk":
+        return adk_rate(ratefunc, E)
+    return ppt_rate(ratefunc, E)
+
+
+# ------------------------------------------------------------------- responses
+
+EPS0 = 8.854187817620389e-12
+E_RATIO = 1.6021766208e-19 ** 2 / 9.10938356e-31
+
+
+def kerr_field(out, E, rho, g3):
+    """Nonlinear.jl:8-10, 24-34."""
+    out += (rho * EPS0 * g3) * E ** 3
+
+
+def kerr_env(out, E, rho, g3):
+    """Nonlinear.jl:47-49, 63-73."""
+    out += 3 / 4 * (rho * EPS0 * g3) * np.abs(E) ** 2 * E
+
+
+def plasma(out, E, rho, p):
+    """PlasmaCumtrapz scalar response (Nonlinear.jl:121-133, 164-177)."""
+    r = rate(p.ratefunc, E)
+    frac = cumtrapz(r, p.δt)
+    frac = p.preionfrac + 1 - np.exp(-frac)
+    phase = frac * E_RATIO * E
+    J = cumtrapz(phase, p.δt)
+    nz = np.abs(E) > 0
+    J[nz] += p.ionpot * r[nz] * (1 - frac[nz]) / E[nz]
+    P = cumtrapz(J, p.δt)
+    out += rho * P
+
+
+def raman_h(resp, rho):
+    """CombinedRamanResponse(ht, rho) (Raman.jl:256-262)."""
+    return resp.r.h(rho)
+
+
+def raman_field(out, E, rho, resp):
+    """RamanPolarField with thg=true (Nonlinear.jl:282-333) on a 2x zero-padded grid."""
+    n = len(E)
+    h = np.zeros(2 * n)
+    h[:n] = raman_h(resp, rho)
+    hw = np.fft.rfft(h)
+    E2 = np.zeros(2 * n)
+    E2[:n] = E ** 2
+    Pw = hw * np.fft.rfft(E2) * resp.dt
+    P = np.fft.irfft(Pw, 2 * n)
+    out += rho * E * P[:n]
+
+
+def raman_env(out, E, rho, resp):
+    """RamanPolarEnv (Nonlinear.jl:276-279, 282-333) with complex FFTs of length 2n."""
+    n = len(E)
+    h = np.zeros(2 * n, dtype=np.complex128)
+    h[:n] = raman_h(resp, rho)
+    hw = np.fft.fft(h)
+    E2 = np.zeros(2 * n, dtype=np.complex128)
+    E2[:n] = 0.5 * np.abs(E) ** 2
+    Pw = hw * np.fft.fft(E2) * resp.dt
+    P = np.fft.ifft(Pw)
+    out += rho * E * P[:n]
+
+
+def et_to_pt(Et, resp, rho):
+    """Et_to_Pt! (NonlinearRHS.jl:121-126): zero, then accumulate each response in order."""
+    Pt = np.zeros_like(Et)
+    for r in resp:
+        if r.kind == "kerr_field":
+            kerr_field(Pt, Et, rho, r.γ3)
+        elif r.kind == "kerr_env":
+            kerr_env(Pt, Et, rho, r.γ3)
+        elif r.kind == "plasma":
+            plasma(Pt, Et, rho, r)
+        elif r.kind == "raman_field":
+            raman_field(Pt, Et, rho, r)
+        elif r.kind == "raman_env":
+            raman_env(Pt, Et, rho, r)
+        else:
+            raise ValueError(r.kind)
+    return Pt
+
+
+# ------------------------------------------------------------------- transform
+
+def to_time(grid, Ew):
+    """to_time! (NonlinearRHS.jl:16-32): zero-pad, rescale and inverse-transform."""
+    Nw = len(Ew)
+    if grid.kind == "real":
+        Nwo = len(grid.ωo)
+        scale = (Nwo - 1) / (Nw - 1)
+        Ewo = np.zeros(Nwo, dtype=np.complex128)
+        Ewo[:Nw] = scale * Ew
+        return np.fft.irfft(Ewo, grid.No)
+    No = grid.No
+    scale = No / Nw
+    h = Nw // 2
+    Ewo = np.zeros(No, dtype=np.complex128)
+    Ewo[:h] = scale * Ew[:h]
+    Ewo[No - h:] = scale * Ew[Nw - h:]
+    return np.fft.ifft(Ewo)
+
+
+def to_freq(grid, Pt, Nw):
+    """to_freq! (NonlinearRHS.jl:39-53): forward transform, crop and rescale."""
+    if grid.kind == "real":
+        Pwo = np.fft.rfft(Pt)
+        scale = (Nw - 1) / (len(Pwo) - 1)
+        return scale * Pwo[:Nw]
+    No = len(Pt)
+    Pwo = np.fft.fft(Pt)
+    scale = Nw / No
+    h = Nw // 2
+    out = np.empty(Nw, dtype=np.complex128)
+    out[:h] = scale * Pwo[:h]
+    out[Nw - h:] = scale * Pwo[No - h:]
+    return out
+
+
+NLSCALE = math.sqrt(EPS0 * 299792458.0 / 2)
+
+
+def trans_mode_avg(t, Ew, z):
+    """(t::TransModeAvg)(nl, Eω, z) (NonlinearRHS.jl:362-373)."""
+    g = t.grid
+    Et = to_time(g, Ew)
+    Et = Et / (NLSCALE * math.sqrt(t.aeff))
+    Pt = et_to_pt(Et, t.resp, t.density)
+    Pt = Pt * g.towin
+    nl = to_freq(g, Pt, len(Ew))
+    s = g.sidx
+    nl[s] = nl[s] * (t.norm.pre[s] * math.sqrt(t.aeff))
+    nl[s] = nl[s] * g.ωwin[s]
+    return nl
+
+
+# ------------------------------------------------------------------- RK45 (dopri)
+
+# Butcher tableau, nodes, weights and dense-output coefficients (dopri.jl:2-28)
+B = [[1 / 5],
+     [3 / 40, 9 / 40],
+     [44 / 45, -56 / 15, 32 / 9],
+     [19372 / 6561, -25360 / 2187, 64448 / 6561, -212 / 729],
+     [9017 / 3168, -355 / 33, 46732 / 5247, 49 / 176, -5103 / 18656],
+     [35 / 384, 0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84]]
+NODES = [1 / 5, 3 / 10, 4 / 5, 8 / 9, 1, 1]
+B5 = [5179 / 57600, 0, 7571 / 16695, 393 / 640, -92097 / 339200, 187 / 2100, 1 / 40]
+B4 = [35 / 384, 0, 500 / 1113, 125 / 192, -2187 / 6784, 11 / 84, 0]
+ERREST = [a - b for a, b in zip(B5, B4)]
+INTERPC = np.array([
+    [1, 0, 0, 0, 0, 0, 0],
+    [-183 / 64, 0, 1500 / 371, -125 / 32, 9477 / 3392, -11 / 7, 3 / 2],
+    [37 / 12, 0, -1000 / 159, 125 / 12, -729 / 106, 11 / 3, -4],
+    [-145 / 128, 0, 1000 / 371, -375 / 64, 25515 / 6784, -55 / 28, 5 / 2]])
+
+
+def weaknorm(yerr, y, yn, rtol, atol):
+    """RK45.jl:343-354."""
+    sy = np.sum(np.abs(y) ** 2)
+    syn = np.sum(np.abs(yn) ** 2)
+    syerr = np.sum(np.abs(yerr) ** 2)
+    errwt = max(max(math.sqrt(sy), math.sqrt(syn)), atol)
+    return math.sqrt(syerr) / rtol / errwt
+
+
+class PreconStepper:
+    """Interaction-picture embedded RK (RK45.jl:128-226, 249-297, 374-406)."""
+
+    def __init__(self, f, linop, y0, t, dt, rtol=1e-6, atol=1e-10, safety=0.9,
+                 max_dt=math.inf, min_dt=0.0, locextrap=True):
+        self.f = f
+        self.linop = linop
+        y0 = np.array(y0, dtype=np.complex128)
+        self.y = y0.copy()
+        self.yn = y0.copy()
+        self.ks = [None] * 7
+        self.t = float(t)
+        self.tn = float(t)
+        self.dt = float(dt)
+        self.dtn = float(dt)
+        self.rtol, self.atol, self.safety = rtol, atol, safety
+        self.max_dt, self.min_dt = max_dt, min_dt
+        self.locextrap = locextrap
+        self.ok = False
+        self.err = 0.0
+        self.errlast = 0.0
+        self.nrhs = 0
+        self.ks[0] = self.fbar(y0, self.t, self.t)
+
+    def prop(self, y, t1, t2, bwd=False):
+        """make_prop! for a constant linop (RK45.jl:271-281)."""
+        d = (t1 - t2) if bwd else (t2 - t1)
+        return y * np.exp(self.linop * d)
+
+    def fbar(self, ybar, t1, t2):
+        """make_fbar! (RK45.jl:299-310)."""
+        y = self.prop(ybar, t1, t2)
+        out = self.f(y, t2)
+        self.nrhs += 1
+        return self.prop(out, t1, t2, True)
+
+    def evaluate(self):
+        """evaluate!(::PreconStepper) (RK45.jl:209-223)."""
+        self.y = self.yn.copy()
+        self.ks[0] = self.prop(self.ks[0], self.t, self.tn)
+        self.dt = self.dtn
+        self.t = self.tn
+        for ii in range(6):
+            yn = self.y.copy()
+            for jj in range(ii + 1):
+                if B[ii][jj] != 0:
+                    yn = yn + (self.dt * B[ii][jj]) * self.ks[jj]
+            self.ks[ii + 1] = self.fbar(yn, self.t, self.t + NODES[ii] * self.dt)
+
+    def step(self):
+        """step! (RK45.jl:167-192)."""
+        self.evaluate()
+        if self.locextrap:
+            yn = self.y.copy()
+            for jj in range(7):
+                if B5[jj] != 0:
+                    yn = yn + (self.dt * B5[jj]) * self.ks[jj]
+            self.yn = yn
+        yerr = np.zeros_like(self.y)
+        for ii in range(7):
+            if ERREST[ii] != 0:
+                yerr = yerr + self.dt * self.ks[ii] * ERREST[ii]
+        self.err = weaknorm(yerr, self.y, self.yn, self.rtol, self.atol)
+        self.ok = self.err <= 1
+        self.stepcontrol()
+        if self.ok:
+            self.tn = self.t + self.dt
+            self.ks[0] = self.ks[6].copy()
+        else:
+            self.yn = self.y.copy()
+        self.yn = self.prop(self.yn, self.t, self.tn)
+        return self.ok
+
+    def stepcontrol(self):
+        """stepcontrolPI! + steplims! (RK45.jl:374-406)."""
+        b1 = 3 / 5 / 5
+        b2 = -1 / 5 / 5
+        eps = 0.8
+        if self.ok:
+            if self.errlast == 0:
+                self.errlast = self.err
+            if self.err == 0:
+                fac = 1.5
+            else:
+                fac = self.safety * (eps / self.err) ** b1 * (eps / self.errlast) ** b2
+            self.dtn = fac * self.dt
+            self.errlast = self.err
+        else:
+            if not math.isfinite(self.err):
+                self.dtn = self.dt / 2
+            else:
+                self.dtn = self.dt * max(0.1, self.safety * self.err ** (-1 / 5))
+        if self.dtn > self.max_dt:
+            self.dtn = self.max_dt
+        elif self.dtn < self.min_dt:
+            self.dtn = self.min_dt
+            self.ok = True
+
+    def interpolate(self, ti):
+        """Dense output (RK45.jl:249-268); ks[0] already holds k7 after an accepted step."""
+        if ti > self.tn:
+            raise ValueError("Attempting to extrapolate!")
+        if ti == self.t:
+            return self.y.copy()
+        if ti == self.tn:
+            return self.yn.copy()
+        s = (ti - self.t) / self.dt
+        sp = np.array([s, s * s, s * s * s, (s * s) * (s * s)])
+        b = np.sum(sp[:, None] * INTERPC, axis=0)
+        yi = np.zeros_like(self.y)
+        for ii in range(7):
+            yi = yi + self.ks[ii] * b[ii]
+        out = self.y + self.dt * yi
+        return self.prop(out, self.t, ti)
+
+
+class RunResult:
+    def __init__(self):
+        self.z = []
+        self.Eω = []
+        self.steps = 0
+        self.accepted = []  # (t, dt, err) of every accepted step
+        self.rejected = 0
+        self.nrhs = 0
+
+
+def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rtol=1e-6,
+        atol=1e-10, safety=0.9, saveN=201, repeat_limit=10, max_steps=None):
+    """Luna.run (Luna.jl:358-391) with a MemoryOutput on a GridCondition (Output.jl:65-82,
+    490-502) and RK45.solve's loop (RK45.jl:27-89)."""
+    max_dz = grid.zmax / 2 if max_dz is None else max_dz
+    zgrid = np.linspace(z0, grid.zmax, saveN)
+    res = RunResult()
+    f = lambda y, z: trans_mode_avg(t, y, z)
+    s = PreconStepper(f, linop, Eω0, z0, init_dz, rtol=rtol, atol=atol, safety=safety,
+                      max_dt=max_dz, min_dt=min_dz)
+    saved = 0
+    repeated = 0
+    kind = grid.kind
+
+    def stepfun(yn, z, dz):
+        # Luna.jl:366-372: window in frequency, back to time, window in time, forward
+        nonlocal saved
+        y = yn * grid.ωwin
+        if kind == "real":
+            Et = np.fft.irfft(y, grid.N) * grid.twin
+            y = np.fft.rfft(Et)
+        else:
+            Et = np.fft.ifft(y) * grid.twin
+            y = np.fft.fft(Et)
+        s.yn = y
+        while saved < saveN and zgrid[saved] <= z:
+            res.z.append(zgrid[saved])
+            res.Eω.append(s.interpolate(zgrid[saved]))
+            saved += 1
+
+    # the output is initialised with the first save point at z0 when it is reached by
+    # the first accepted step's condition check (z0 <= tn)
+    while s.tn <= grid.zmax:
+        ok = s.step()
+        res.steps += 1
+        if ok:
+            res.accepted.append((s.t, s.dt, s.err))
+            stepfun(s.yn, s.tn, s.dtn)
+            repeated = 0
+        else:
+            res.rejected += 1
+            repeated += 1
+            if repeated > repeat_limit:
+                raise RuntimeError(f"Reached limit for step repetition ({repeat_limit})")
+        if max_steps is not None and res.steps >= max_steps:
+            break
+    res.nrhs = s.nrhs
+    res.Eω = np.array(res.Eω)
+    res.z = np.array(res.z)
+    return res

@@ -1,0 +1,151 @@
+/*
+ * libluna_b200 — C ABI of the B200 (sm_100a) UPPE right-hand side and RK45 integrator.
+ *
+ * This library replaces, for one GPU, the hot path of Luna.jl v0.6.2:
+ *   - the mode-averaged transform  (t::TransModeAvg)(nl, Eω, z)   NonlinearRHS.jl:362-373
+ *     with its responses  Kerr_field / Kerr_env                   Nonlinear.jl:8-73
+ *                         PlasmaCumtrapz (PPT spline / ADK rate)  Nonlinear.jl:88-177,
+ *                                                                 Ionisation.jl:22-63, 247-271
+ *                         RamanPolarField / RamanPolarEnv         Nonlinear.jl:183-333,
+ *                                                                 Raman.jl:242-262
+ *   - the integrator RK45.solve_precon(...) and Luna.run's loop    RK45.jl:19-89, 128-406,
+ *     (window filter stepfun, GridCondition saves)                Luna.jl:358-391,
+ *                                                                 Output.jl:65-82, 490-502
+ *
+ * Conventions
+ *   - Complex arrays are interleaved (re, im) doubles, i.e. the memory layout of Julia's
+ *     Vector{ComplexF64}; `Nw` complex values = 2*Nw doubles.
+ *   - Every entry point returns a status code (LUNA_OK = 0 on success); the message of the
+ *     last failure on the calling thread is available from luna_b200_last_error().
+ *   - A plan owns its device copies of the grid, normalisation and response tables. Calls
+ *     on one plan must be serialised; different plans may be used from different threads.
+ *   - There is no CPU fallback: without a usable CUDA device every call fails with
+ *     LUNA_ERR_CUDA.
+ */
+#ifndef LUNA_B200_H
+#define LUNA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define LUNA_OK 0
+#define LUNA_FIELD_ABOVE_EMAX 1 /* PPT field above the table maximum (Ionisation.jl:262-265) */
+#define LUNA_REPEAT_LIMIT 2     /* more than repeat_limit rejected steps (RK45.jl:72-76) */
+#define LUNA_NONFINITE 3
+#define LUNA_STEP_BUDGET 4      /* max_steps reached before zmax */
+#define LUNA_ERR_BAD_ARG 16
+#define LUNA_ERR_UNSUPPORTED 17
+#define LUNA_ERR_CUDA 18
+
+/* response kinds */
+#define LUNA_RESP_KERR_FIELD 1  /* Nonlinear.Kerr_field(γ3)                 Nonlinear.jl:24-34 */
+#define LUNA_RESP_KERR_ENV 2    /* Nonlinear.Kerr_env(γ3)                   Nonlinear.jl:63-73 */
+#define LUNA_RESP_PLASMA_PPT 3  /* PlasmaCumtrapz with ionrate_fun!_PPTcached  Nonlinear.jl:107 */
+#define LUNA_RESP_PLASMA_ADK 4  /* PlasmaCumtrapz with ionrate_fun!_ADK         Nonlinear.jl:107 */
+#define LUNA_RESP_RAMAN 5       /* RamanPolarField(thg=true) / RamanPolarEnv Nonlinear.jl:223-264 */
+
+/* precision modes */
+#define LUNA_PREC_FP64 0  /* plain: every operation in FP64 */
+#define LUNA_PREC_MIXED 1 /* FP32 transforms/responses/stage derivatives; FP64 state, phase,
+                             controller, norms and plasma prefix sums */
+
+/* Grid and normalisation of one TransModeAvg (Grid.jl:12-194, NonlinearRHS.jl:375-399). */
+typedef struct {
+    int kind;              /* 0: RealGrid (field-resolved), 1: EnvGrid (envelope)        */
+    int N;                 /* coarse time samples length(grid.t)                         */
+    int Nw;                /* coarse frequency bins length(grid.ω)                       */
+    int No;                /* oversampled time samples length(grid.to)                   */
+    const double* outfac;  /* [2*Nw] crop scale x (norm*sqrt(Aeff)*ωwin on sidx, 1 else) */
+    const double* wwin;    /* [Nw] grid.ωwin                                             */
+    const double* towin;   /* [No] grid.towin                                            */
+    const double* twin;    /* [N]  grid.twin                                             */
+    double in_scale;       /* pad scale / No / (nlscale*sqrt(Aeff))                      */
+} luna_grid_desc;
+
+/* One nonlinear response, applied in the order given (Et_to_Pt!, NonlinearRHS.jl:121-126). */
+typedef struct {
+    int kind;               /* LUNA_RESP_*                                               */
+    double coef;            /* Kerr: ρ*ε0*γ3; plasma and Raman: ρ                         */
+    /* PlasmaCumtrapz */
+    double ionpot;          /* ionisation potential [J]                                  */
+    double dt;              /* t[2]-t[1] of the oversampled grid                         */
+    double preionfrac;      /* in [0, 1]                                                 */
+    double eratio;          /* e^2/m_e                                                   */
+    const double* spl_x;    /* [spl_n] uniform field axis of the PPT log-rate spline     */
+    const double* spl_y;    /* [spl_n] log(rate)                                         */
+    const double* spl_D;    /* [spl_n] Hermite slopes (Maths.jl:812-828)                 */
+    int spl_n;
+    double adk_pre, adk_a, adk_b, adk_pw, adk_thr; /* rate = pre*(a/|E|)^pw*exp(-b/|E|)   */
+    /* Raman (CombinedRamanResponse evaluated at the plan's density) */
+    int ncomp;
+    const double* hpre;     /* [ncomp*No] undamped component responses on htt             */
+    const double* tau2;     /* [ncomp] dephasing time of each component at this density  */
+    const double* hwin;     /* [No] Planck-taper window of the response                  */
+    const double* htt;      /* [No] response time axis (0..No-1)*dt                      */
+    double hdt;             /* response grid spacing (scales the convolution)            */
+} luna_resp_desc;
+
+typedef struct {
+    double rtol, atol, safety, max_dt, min_dt; /* RK45.solve_precon keywords (RK45.jl:19-21) */
+    int repeat_limit;                          /* RK45.solve keyword (RK45.jl:27-28)        */
+    long long max_steps;                       /* 0: unlimited                              */
+    int saveN;                                 /* number of GridCondition save points       */
+    const double* zsave;                       /* [saveN] save points (Output.jl:495-497)   */
+    long long steplog_cap;                     /* rows of (z, dz, err, ok) to record; 0: off */
+    const double* replay;                      /* optional [2*nreplay] (dz, accepted) per step:
+                                                  follow this step sequence instead of the
+                                                  controller's choice (verification aid)      */
+    long long nreplay;
+} luna_solve_opts;
+
+typedef struct {
+    int status;
+    int nsaved;
+    long long steps, accepted, rejected, nrhs;
+    double z, dz; /* final z (first tn > zmax) and next step size */
+} luna_solve_stats;
+
+typedef struct luna_plan luna_plan;
+typedef struct luna_batch luna_batch;
+
+/* Replaces the TransModeAvg constructor (NonlinearRHS.jl:344-358) as built by Luna.setup
+ * (Luna.jl:115-151): copies grid, normalisation and response tables to the device. */
+int luna_b200_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
+                          int precision, luna_plan** out);
+void luna_b200_plan_destroy(luna_plan* plan);
+
+/* (t::TransModeAvg)(nl, Eω, z)  — NonlinearRHS.jl:362-373. Host arrays of Nw complex. */
+int luna_b200_rhs(luna_plan* plan, double* nl, const double* Ew, double z);
+/* Same with device pointers, enqueued on `stream` (a cudaStream_t, may be NULL). */
+int luna_b200_rhs_device(luna_plan* plan, double* nl_dev, const double* Ew_dev, double z, void* stream);
+
+/* RK45.solve_precon(transform, linop, Eω, z0, dz0, zmax; ...) driven by Luna.run
+ * (Luna.jl:358-391): integrates y_inout in place to the first step beyond zmax, saving the
+ * GridCondition points into `saves` ([saveN*2*Nw] doubles) and optionally the step log
+ * ([4*steplog_cap] doubles). All pointers are host memory. */
+int luna_b200_solve(luna_plan* plan, const double* linop, double* y_inout, double z0, double dz0,
+                    double zmax, const luna_solve_opts* opts, double* saves, double* steplog,
+                    luna_solve_stats* stats);
+
+/* Batched scan of independent instances in one persistent launch (replaces a sequential
+ * Scans.runscan loop over prop_capillary calls, Scans.jl:275-494). All plans must share
+ * one precision. Device buffers live in the batch; upload/run/download split the work so
+ * the device-only part can be timed. */
+int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts* opts, luna_batch** out);
+int luna_b200_batch_upload(luna_batch* b, const double* const* linops, const double* const* y0,
+                           const double* z0, const double* dz0, const double* zmax);
+int luna_b200_batch_run(luna_batch* b, float* device_ms);
+int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
+                             luna_solve_stats* stats);
+int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
+void luna_b200_batch_destroy(luna_batch* b);
+
+const char* luna_b200_last_error(void);
+int luna_b200_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

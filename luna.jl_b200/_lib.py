@@ -1,0 +1,121 @@
+"""ctypes bindings of ``libluna_b200.so`` (declarations in ``include/luna_b200.h``).
+
+The library is built in-tree by ``build.py``. Loading fails loudly when it is missing:
+there is no host implementation of the right-hand side or the integrator to fall back on.
+"""
+import ctypes
+import os
+from ctypes import POINTER, c_double, c_float, c_int, c_longlong, c_void_p
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libluna_b200.so")
+
+LUNA_OK = 0
+LUNA_FIELD_ABOVE_EMAX = 1
+LUNA_REPEAT_LIMIT = 2
+LUNA_NONFINITE = 3
+LUNA_STEP_BUDGET = 4
+LUNA_ERR_BAD_ARG = 16
+LUNA_ERR_UNSUPPORTED = 17
+LUNA_ERR_CUDA = 18
+
+RESP_KERR_FIELD = 1
+RESP_KERR_ENV = 2
+RESP_PLASMA_PPT = 3
+RESP_PLASMA_ADK = 4
+RESP_RAMAN = 5
+
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+PD = POINTER(c_double)
+
+
+class GridDesc(ctypes.Structure):
+    _fields_ = [("kind", c_int), ("N", c_int), ("Nw", c_int), ("No", c_int),
+                ("outfac", PD), ("wwin", PD), ("towin", PD), ("twin", PD),
+                ("in_scale", c_double)]
+
+
+class RespDesc(ctypes.Structure):
+    _fields_ = [("kind", c_int), ("coef", c_double),
+                ("ionpot", c_double), ("dt", c_double), ("preionfrac", c_double),
+                ("eratio", c_double),
+                ("spl_x", PD), ("spl_y", PD), ("spl_D", PD), ("spl_n", c_int),
+                ("adk_pre", c_double), ("adk_a", c_double), ("adk_b", c_double),
+                ("adk_pw", c_double), ("adk_thr", c_double),
+                ("ncomp", c_int), ("hpre", PD), ("tau2", PD), ("hwin", PD), ("htt", PD),
+                ("hdt", c_double)]
+
+
+class SolveOpts(ctypes.Structure):
+    _fields_ = [("rtol", c_double), ("atol", c_double), ("safety", c_double),
+                ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
+                ("max_steps", c_longlong), ("saveN", c_int), ("zsave", PD),
+                ("steplog_cap", c_longlong), ("replay", PD), ("nreplay", c_longlong)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("status", c_int), ("nsaved", c_int), ("steps", c_longlong),
+                ("accepted", c_longlong), ("rejected", c_longlong), ("nrhs", c_longlong),
+                ("z", c_double), ("dz", c_double)]
+
+
+EXPORTS = [
+    "luna_b200_plan_create", "luna_b200_plan_destroy", "luna_b200_rhs", "luna_b200_rhs_device",
+    "luna_b200_solve", "luna_b200_batch_create", "luna_b200_batch_upload", "luna_b200_batch_run",
+    "luna_b200_batch_download", "luna_b200_batch_steplog", "luna_b200_batch_destroy",
+    "luna_b200_last_error", "luna_b200_version",
+]
+
+_lib = None
+
+
+class LunaError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libluna_b200 error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with luna.jl_b200/build.py "
+                          "(there is no CPU implementation of the UPPE hot path)")
+    lib = ctypes.CDLL(LIB_PATH)
+    lib.luna_b200_plan_create.argtypes = [POINTER(GridDesc), POINTER(RespDesc), c_int, c_int,
+                                          POINTER(c_void_p)]
+    lib.luna_b200_plan_destroy.argtypes = [c_void_p]
+    lib.luna_b200_plan_destroy.restype = None
+    lib.luna_b200_rhs.argtypes = [c_void_p, PD, PD, c_double]
+    lib.luna_b200_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
+    lib.luna_b200_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
+                                    POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
+    lib.luna_b200_batch_create.argtypes = [POINTER(c_void_p), c_int, POINTER(SolveOpts),
+                                           POINTER(c_void_p)]
+    lib.luna_b200_batch_upload.argtypes = [c_void_p, POINTER(PD), POINTER(PD), PD, PD, PD]
+    lib.luna_b200_batch_run.argtypes = [c_void_p, POINTER(c_float)]
+    lib.luna_b200_batch_download.argtypes = [c_void_p, POINTER(PD), POINTER(PD), POINTER(SolveStats)]
+    lib.luna_b200_batch_steplog.argtypes = [c_void_p, c_int, PD]
+    lib.luna_b200_batch_destroy.argtypes = [c_void_p]
+    lib.luna_b200_batch_destroy.restype = None
+    lib.luna_b200_last_error.restype = ctypes.c_char_p
+    lib.luna_b200_version.restype = c_int
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != LUNA_OK:
+        msg = load().luna_b200_last_error().decode(errors="replace")
+        raise LunaError(rc, msg)
+    return rc
+
+
+def dptr(a):
+    """double* pointing at a C-contiguous float64/complex128 numpy array (or NULL)."""
+    if a is None:
+        return ctypes.cast(None, PD)
+    return a.ctypes.data_as(PD)

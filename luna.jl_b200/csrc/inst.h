@@ -1,0 +1,80 @@
+// Device-visible description of one propagation instance (plan + solver state).
+// Filled by the host side of the C ABI; read by the persistent solver kernel.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define LUNA_MAX_RESP 4
+
+// response kinds (same values as the public header)
+#ifndef LUNA_RESP_KERR_FIELD
+#define LUNA_RESP_KERR_FIELD 1
+#define LUNA_RESP_KERR_ENV 2
+#define LUNA_RESP_PLASMA_PPT 3
+#define LUNA_RESP_PLASMA_ADK 4
+#define LUNA_RESP_RAMAN 5
+#endif
+
+typedef struct {
+    int kind;
+    double coef;      // Kerr: rho*eps0*gamma3; Raman: rho; plasma: rho
+    // plasma (PlasmaCumtrapz)
+    double ionpot, dt, preion, eratio;
+    // PPT log-rate spline on a uniform field axis
+    const double* sx;
+    const double* sy;
+    const double* sD;
+    const float* sxf;
+    const float* syf;
+    const float* sDf;
+    int sn;
+    double Emin, Emax;
+    // ADK: rate = pre * (a/|E|)^pw * exp(-b/|E|) for |E| >= thr
+    double adk_pre, adk_a, adk_b, adk_pw, adk_thr;
+    // Raman: spectrum H[k], k = 0..No, of the normalised response on the 2*No grid
+    // (complex of the compute precision); coef carries rho * max|h| * dt / (2*No)
+    const void* H;
+    // Raman response build inputs (used once at plan creation)
+    const double* hpre;    // [ncomp * No] undamped responses
+    const double* tau2;    // [ncomp] dephasing times at this density
+    const double* hwin;    // [No] window
+    const double* htt;     // [No] response time axis
+    double hdt;            // response grid spacing
+    int ncomp;
+} LunaResp;
+
+typedef struct {
+    // ---- grid / transform (NonlinearRHS.TransModeAvg) ----
+    int kind;            // 0: field-resolved (RealGrid), 1: envelope (EnvGrid)
+    int N, Nw, No;       // coarse time samples, coarse frequency bins, oversampled samples
+    const double2* linop;   // [Nw]
+    const double2* outfac;  // [Nw] crop scale x (norm * sqrt(Aeff) * omega window on sidx, 1 elsewhere)
+    const double* wwin;     // [Nw] omega window (stepfun)
+    const double* towin;    // [No]
+    const double* twin;     // [N] (stepfun)
+    double in_scale;        // pad scale / No / (nlscale * sqrt(Aeff))
+    int nresp;
+    LunaResp resp[LUNA_MAX_RESP];
+    // ---- integrator (RK45.solve_precon) ----
+    const double2* y0;   // [Nw] initial field (kept, so a batch can be re-run)
+    double2* y;
+    double2* yn;
+    void* k[7];          // stage derivatives, double2 (plain) or float2 (mixed)
+    double2* e1;         // exp(L*dz) of the last stage-5 node
+    void* gscr;          // global scratch for buffers that do not fit in shared memory
+    double2* saves;      // [saveN * Nw]
+    const double* zsave; // [saveN]
+    int saveN;
+    double z0, dz0, zmax, rtol, atol, safety, max_dt, min_dt;
+    int repeat_limit;
+    long long max_steps;
+    double* steplog;     // optional [4 * steplog_cap]: t, dt, err, ok per step
+    long long steplog_cap;
+    const double* replay; // optional [2 * nreplay]: (dt, ok) of each step to follow
+    long long nreplay;
+    // ---- results ----
+    int status;
+    int nsaved;
+    long long steps, accepted, rejected, nrhs;
+    double z, dz;
+} LunaInst;

@@ -1,0 +1,673 @@
+// Kernels and the C ABI of libluna_b200 (see include/luna_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/luna_b200.h"
+#include "uppe.cuh"
+
+using namespace luna;
+
+// ===================================================================== kernels
+
+// Persistent solver: each CTA pulls instances from `counter` until the list is empty and
+// integrates each one to completion (RK45.solve loop, RK45.jl:43-78).
+template <typename Rl, typename Kt>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes) {
+    extern __shared__ __align__(256) char smem[];
+    __shared__ Ctl ctl;
+    __shared__ int sidx;
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) sidx = atomicAdd(counter, 1);
+        __syncthreads();
+        const int i = sidx;
+        if (i >= n) break;
+        LunaInst& I = insts[i];
+        Ws<Rl> w;
+        plan_ws<Rl>(I, smem, smem_bytes, w, tw);
+        solve_instance<Rl, Kt>(I, w, ctl);
+    }
+}
+
+// One right-hand-side evaluation nl = T(Eω) on one CTA (TransModeAvg call).
+template <typename Rl>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int smem_bytes, int* status) {
+    extern __shared__ __align__(256) char smem[];
+    LunaInst& I = *inst;
+    Ws<Rl> w;
+    plan_ws<Rl>(I, smem, smem_bytes, w, tw);
+    if (threadIdx.x == 0) *w.flag = 0;
+    __syncthreads();
+    const cpx<double>* E = reinterpret_cast<const cpx<double>*>(Ew);
+    cpx<double>* o = reinterpret_cast<cpx<double>*>(nl);
+    rhs<Rl>(I, w, [&](int k) { return E[k]; }, [&](int k, cpx<double> v) { o[k] = v; });
+    __syncthreads();
+    if (threadIdx.x == 0) *status = (*w.flag & (1 << ST_FIELD_ABOVE_EMAX)) ? ST_FIELD_ABOVE_EMAX : ST_OK;
+}
+
+// Raman response spectrum at plan creation (Raman.jl:256-262, Nonlinear.jl:306-307):
+// h(t) = w(t) * sum_c hpre_c(t) exp(-t/tau2_c) on the first half of a 2*No grid,
+// H[k] = rfft(hscale * h)[k], k = 0..No, computed in FP64. The response is normalised by
+// hscale = 1/max|hpre| so that its spectrum is representable in FP32 (molecular responses
+// are ~1e-48 in SI units); the plan folds max|hpre| * hdt / (2*No) into the FP64 coefficient.
+template <typename Rl>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<double>* alt, cpx<Rl>* H,
+               TwTab<double> tw) {
+    const int tid = threadIdx.x;
+    for (int m = tid; m < No; m += LUNA_BLOCK) {
+        double a = 0, b = 0;
+        if (m < No / 2) {
+            for (int j = 0; j < 2; ++j) {
+                const int n = 2 * m + j;
+                double h = 0;
+                for (int c = 0; c < r.ncomp; ++c) h += r.hpre[(size_t)c * No + n] * exp(-r.htt[n] / r.tau2[c]);
+                h *= r.hwin[n] * hscale;
+                if (j == 0) a = h;
+                else b = h;
+            }
+        }
+        buf[Swz<double>::f(m)] = mk<double>(a, b);
+    }
+    __syncthreads();
+    cpx<double>* Z = block_fft<double, false>(buf, alt, No, tw);
+    const int M = No;
+    for (int k = tid; k <= M; k += LUNA_BLOCK) {
+        const int kk = k & (M - 1);
+        const int km = (M - k) & (M - 1);
+        cpx<double> Zk = Z[Swz<double>::f(kk)];
+        cpx<double> Zm = Z[Swz<double>::f(km)];
+        cpx<double> X;
+        if (k == 0) X = mk<double>(Zk.x + Zk.y, 0.0);
+        else if (k == M) X = mk<double>(Zk.x - Zk.y, 0.0);
+        else {
+            cpx<double> Wk = half_twiddle<double, false>(tw, k, M);
+            X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
+        }
+        H[k] = cvt<Rl>(X);
+    }
+}
+
+// ===================================================================== host side
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define CK(call)                                                                       \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return fail(LUNA_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+struct TwDev {
+    TwTab<double> d;
+    TwTab<float> f;
+};
+
+std::mutex g_tw_mu;
+std::map<int, TwDev> g_tw;
+
+int get_tw(TwDev& out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    auto it = g_tw.find(dev);
+    if (it != g_tw.end()) {
+        out = it->second;
+        return LUNA_OK;
+    }
+    std::vector<cpx<double>> lo(TW_NLO), hi(TW_NHI);
+    std::vector<cpx<float>> lof(TW_NLO), hif(TW_NHI);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int j = 0; j < TW_NLO; ++j) {
+        double a = -two_pi * (double)j / (double)TW_MMAX;
+        lo[j] = mk<double>(std::cos(a), std::sin(a));
+        lof[j] = mk<float>((float)lo[j].x, (float)lo[j].y);
+    }
+    for (int j = 0; j < TW_NHI; ++j) {
+        double a = -two_pi * (double)(j * TW_NLO) / (double)TW_MMAX;
+        hi[j] = mk<double>(std::cos(a), std::sin(a));
+        hif[j] = mk<float>((float)hi[j].x, (float)hi[j].y);
+    }
+    TwDev t;
+    void* p;
+    CK(cudaMalloc(&p, sizeof(cpx<double>) * (TW_NLO + TW_NHI)));
+    CK(cudaMemcpy(p, lo.data(), sizeof(cpx<double>) * TW_NLO, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((char*)p + sizeof(cpx<double>) * TW_NLO, hi.data(), sizeof(cpx<double>) * TW_NHI,
+                  cudaMemcpyHostToDevice));
+    t.d.lo = (const cpx<double>*)p;
+    t.d.hi = (const cpx<double>*)((char*)p + sizeof(cpx<double>) * TW_NLO);
+    CK(cudaMalloc(&p, sizeof(cpx<float>) * (TW_NLO + TW_NHI)));
+    CK(cudaMemcpy(p, lof.data(), sizeof(cpx<float>) * TW_NLO, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy((char*)p + sizeof(cpx<float>) * TW_NLO, hif.data(), sizeof(cpx<float>) * TW_NHI,
+                  cudaMemcpyHostToDevice));
+    t.f.lo = (const cpx<float>*)p;
+    t.f.hi = (const cpx<float>*)((char*)p + sizeof(cpx<float>) * TW_NLO);
+    g_tw[dev] = t;
+    out = t;
+    return LUNA_OK;
+}
+
+bool is_pow2(int x) { return x > 0 && (x & (x - 1)) == 0; }
+
+int max_smem_optin() {
+    int dev = 0, v = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    return v - 1024;  // leave room for the kernels' static shared memory
+}
+
+template <typename Rl>
+size_t smem_wanted(const LunaInst& I) {
+    const size_t c = sizeof(cpx<Rl>);
+    const int emax = (sizeof(Rl) == 8) ? 16 : 32;
+    size_t s = LUNA_SMALL_BYTES;
+    const int Mm = main_len(I);
+    if (Mm / LUNA_BLOCK <= emax) s += align_up((size_t)Mm * c, 256);
+    s += align_up((size_t)I.Nw * c, 256);
+    if (has_raman(I) && I.No / LUNA_BLOCK <= emax) s += align_up((size_t)I.No * c, 256);
+    return s;
+}
+
+}  // namespace
+
+struct luna_plan {
+    int precision = 0;
+    LunaInst proto{};
+    std::vector<void*> allocs;
+    // single-call RHS resources
+    LunaInst* d_inst = nullptr;
+    void* d_gscr = nullptr;
+    double2* d_Ew = nullptr;
+    double2* d_nl = nullptr;
+    int* d_status = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+struct luna_batch {
+    int n = 0;
+    int precision = 0;
+    std::vector<luna_plan*> plans;
+    luna_solve_opts opts{};
+    std::vector<LunaInst> h;
+    LunaInst* d_insts = nullptr;
+    int* d_counter = nullptr;
+    std::vector<void*> allocs;
+    std::vector<double2*> y0buf;  // per instance y (holds y0 before the run)
+    std::vector<double2*> ybuf, ynbuf;
+    std::vector<double*> steplogs;
+    double* d_zsave = nullptr;
+    int smem = 0;
+    int grid = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(std::vector<void*>& allocs, T** p, size_t bytes) {
+    void* q = nullptr;
+    CK(cudaMalloc(&q, bytes > 0 ? bytes : 16));
+    allocs.push_back(q);
+    *p = reinterpret_cast<T*>(q);
+    return LUNA_OK;
+}
+
+template <typename T>
+int upload(std::vector<void*>& allocs, const T* src, size_t n, const T** dst) {
+    T* p = nullptr;
+    int rc = dalloc(allocs, &p, n * sizeof(T));
+    if (rc) return rc;
+    CK(cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+    *dst = p;
+    return LUNA_OK;
+}
+
+void free_all(std::vector<void*>& allocs) {
+    for (void* p : allocs) cudaFree(p);
+    allocs.clear();
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* luna_b200_last_error(void) { return g_err.c_str(); }
+
+int luna_b200_version(void) { return 1; }
+
+int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, int nresp, int precision,
+                          luna_plan** out) {
+    if (!g || !out || nresp < 0 || nresp > LUNA_MAX_RESP || (nresp > 0 && !resps))
+        return fail(LUNA_ERR_BAD_ARG, "plan_create: null argument or too many responses");
+    if (precision != LUNA_PREC_FP64 && precision != LUNA_PREC_MIXED)
+        return fail(LUNA_ERR_BAD_ARG, "plan_create: unknown precision");
+    if (g->kind != 0 && g->kind != 1) return fail(LUNA_ERR_BAD_ARG, "plan_create: grid kind must be 0 or 1");
+    if (!is_pow2(g->N) || !is_pow2(g->No) || g->No < g->N || g->N < 16)
+        return fail(LUNA_ERR_BAD_ARG, "plan_create: N and No must be powers of two with 16 <= N <= No");
+    if (g->kind == 0 && g->Nw != g->N / 2 + 1)
+        return fail(LUNA_ERR_BAD_ARG, "plan_create: RealGrid needs Nw == N/2 + 1");
+    if (g->kind == 1 && g->Nw != g->N) return fail(LUNA_ERR_BAD_ARG, "plan_create: EnvGrid needs Nw == N");
+    if (2 * g->No > TW_MMAX) return fail(LUNA_ERR_UNSUPPORTED, "plan_create: No too large");
+    if (!g->outfac || !g->wwin || !g->towin || !g->twin) return fail(LUNA_ERR_BAD_ARG, "plan_create: null grid array");
+    int dev_count = 0;
+    if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
+        return fail(LUNA_ERR_CUDA, "plan_create: no CUDA device available");
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+
+    luna_plan* p = new luna_plan();
+    p->precision = precision;
+    LunaInst& I = p->proto;
+    memset(&I, 0, sizeof(I));
+    I.kind = g->kind;
+    I.N = g->N;
+    I.Nw = g->Nw;
+    I.No = g->No;
+    I.in_scale = g->in_scale;
+#define UP(src, n, dst)                                          \
+    do {                                                         \
+        int rc_ = upload(p->allocs, (src), (size_t)(n), (dst));  \
+        if (rc_) {                                               \
+            free_all(p->allocs);                                 \
+            delete p;                                            \
+            return rc_;                                          \
+        }                                                        \
+    } while (0)
+    const double* tmp;
+    UP(g->outfac, 2 * (size_t)g->Nw, &tmp);
+    I.outfac = (const double2*)tmp;
+    UP(g->wwin, g->Nw, &I.wwin);
+    UP(g->towin, g->No, &I.towin);
+    UP(g->twin, g->N, &I.twin);
+    I.nresp = nresp;
+    int nplasma = 0, nraman = 0;
+    for (int i = 0; i < nresp; ++i) {
+        const luna_resp_desc& d = resps[i];
+        LunaResp& r = I.resp[i];
+        memset(&r, 0, sizeof(r));
+        r.kind = d.kind;
+        r.coef = d.coef;
+        switch (d.kind) {
+            case LUNA_RESP_KERR_FIELD:
+                if (g->kind != 0) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Kerr_field needs a RealGrid"); }
+                break;
+            case LUNA_RESP_KERR_ENV:
+                if (g->kind != 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Kerr_env needs an EnvGrid"); }
+                break;
+            case LUNA_RESP_PLASMA_PPT:
+            case LUNA_RESP_PLASMA_ADK: {
+                if (g->kind != 0) { free_all(p->allocs); delete p; return fail(LUNA_ERR_UNSUPPORTED, "plasma response for envelope fields is not implemented (as in the reference)"); }
+                if (!(d.preionfrac >= 0.0 && d.preionfrac <= 1.0)) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "preionfrac must be between 0 and 1"); }
+                if (++nplasma > 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_UNSUPPORTED, "at most one plasma response"); }
+                r.ionpot = d.ionpot;
+                r.dt = d.dt;
+                r.preion = d.preionfrac;
+                r.eratio = d.eratio;
+                if (d.kind == LUNA_RESP_PLASMA_PPT) {
+                    if (d.spl_n < 4 || !d.spl_x || !d.spl_y || !d.spl_D) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "PPT spline table missing"); }
+                    UP(d.spl_x, d.spl_n, &r.sx);
+                    UP(d.spl_y, d.spl_n, &r.sy);
+                    UP(d.spl_D, d.spl_n, &r.sD);
+                    std::vector<float> fx(d.spl_n), fy(d.spl_n), fD(d.spl_n);
+                    for (int j = 0; j < d.spl_n; ++j) {
+                        fx[j] = (float)d.spl_x[j];
+                        fy[j] = (float)d.spl_y[j];
+                        fD[j] = (float)d.spl_D[j];
+                    }
+                    UP(fx.data(), d.spl_n, &r.sxf);
+                    UP(fy.data(), d.spl_n, &r.syf);
+                    UP(fD.data(), d.spl_n, &r.sDf);
+                    r.sn = d.spl_n;
+                    r.Emin = d.spl_x[0];
+                    r.Emax = d.spl_x[d.spl_n - 1];
+                } else {
+                    r.adk_pre = d.adk_pre;
+                    r.adk_a = d.adk_a;
+                    r.adk_b = d.adk_b;
+                    r.adk_pw = d.adk_pw;
+                    r.adk_thr = d.adk_thr;
+                }
+                break;
+            }
+            case LUNA_RESP_RAMAN: {
+                if (++nraman > 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_UNSUPPORTED, "at most one Raman response"); }
+                if (d.ncomp < 1 || !d.hpre || !d.tau2 || !d.hwin || !d.htt) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Raman response tables missing"); }
+                r.ncomp = d.ncomp;
+                r.hdt = d.hdt;
+                double hmax = 0;
+                for (size_t j = 0; j < (size_t)d.ncomp * g->No; ++j) hmax = std::max(hmax, std::fabs(d.hpre[j]));
+                if (!(hmax > 0)) hmax = 1;
+                r.coef = d.coef * hmax * d.hdt / (2.0 * (double)g->No);
+                UP(d.hpre, (size_t)d.ncomp * g->No, &r.hpre);
+                UP(d.tau2, d.ncomp, &r.tau2);
+                UP(d.hwin, g->No, &r.hwin);
+                UP(d.htt, g->No, &r.htt);
+                // spectrum of the response, computed once on the device in FP64
+                cpx<double>* b1 = nullptr;
+                cpx<double>* b2 = nullptr;
+                if (dalloc(p->allocs, &b1, sizeof(cpx<double>) * g->No) || dalloc(p->allocs, &b2, sizeof(cpx<double>) * g->No)) {
+                    free_all(p->allocs); delete p; return LUNA_ERR_CUDA;
+                }
+                if (precision == LUNA_PREC_FP64) {
+                    cpx<double>* H = nullptr;
+                    if (dalloc(p->allocs, &H, sizeof(cpx<double>) * (g->No + 1))) { free_all(p->allocs); delete p; return LUNA_ERR_CUDA; }
+                    raman_h_kernel<double><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, b2, H, tw.d);
+                    r.H = H;
+                } else {
+                    cpx<float>* H = nullptr;
+                    if (dalloc(p->allocs, &H, sizeof(cpx<float>) * (g->No + 1))) { free_all(p->allocs); delete p; return LUNA_ERR_CUDA; }
+                    raman_h_kernel<float><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, b2, H, tw.d);
+                    r.H = H;
+                }
+                cudaError_t e = cudaDeviceSynchronize();
+                if (e == cudaSuccess) e = cudaGetLastError();
+                if (e != cudaSuccess) { free_all(p->allocs); delete p; return fail(LUNA_ERR_CUDA, std::string("raman_h_kernel: ") + cudaGetErrorString(e)); }
+                break;
+            }
+            default:
+                free_all(p->allocs);
+                delete p;
+                return fail(LUNA_ERR_UNSUPPORTED, "unknown response kind");
+        }
+    }
+#undef UP
+    *out = p;
+    return LUNA_OK;
+}
+
+void luna_b200_plan_destroy(luna_plan* p) {
+    if (!p) return;
+    if (p->stream) cudaStreamDestroy(p->stream);
+    free_all(p->allocs);
+    delete p;
+}
+
+static int launch_rhs(luna_plan* p, const double2* Ew, double2* nl, cudaStream_t st) {
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+    if (!p->d_inst) {
+        LunaInst I = p->proto;
+        size_t gb = (p->precision == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
+        if (dalloc(p->allocs, &p->d_gscr, gb)) return LUNA_ERR_CUDA;
+        I.gscr = p->d_gscr;
+        if (dalloc(p->allocs, &p->d_inst, sizeof(LunaInst))) return LUNA_ERR_CUDA;
+        CK(cudaMemcpy(p->d_inst, &I, sizeof(LunaInst), cudaMemcpyHostToDevice));
+        if (dalloc(p->allocs, &p->d_status, sizeof(int))) return LUNA_ERR_CUDA;
+    }
+    const int maxs = max_smem_optin();
+    if (p->precision == LUNA_PREC_FP64) {
+        int sm = (int)std::min<size_t>(smem_wanted<double>(p->proto), (size_t)maxs);
+        CK(cudaFuncSetAttribute(rhs_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        rhs_kernel<double><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.d, sm, p->d_status);
+    } else {
+        int sm = (int)std::min<size_t>(smem_wanted<float>(p->proto), (size_t)maxs);
+        CK(cudaFuncSetAttribute(rhs_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        rhs_kernel<float><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.f, sm, p->d_status);
+    }
+    CK(cudaGetLastError());
+    return LUNA_OK;
+}
+
+int luna_b200_rhs_device(luna_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
+    (void)z;  // constant density and effective area: the transform does not depend on z
+    if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "rhs_device: null argument");
+    return launch_rhs(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+}
+
+int luna_b200_rhs(luna_plan* p, double* nl, const double* Ew, double z) {
+    (void)z;
+    if (!p || !nl || !Ew) return fail(LUNA_ERR_BAD_ARG, "rhs: null argument");
+    const size_t bytes = sizeof(double2) * p->proto.Nw;
+    if (!p->d_Ew) {
+        if (dalloc(p->allocs, &p->d_Ew, bytes) || dalloc(p->allocs, &p->d_nl, bytes)) return LUNA_ERR_CUDA;
+        CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    }
+    CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
+    int rc = launch_rhs(p, p->d_Ew, p->d_nl, p->stream);
+    if (rc) return rc;
+    int st = 0;
+    CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(&st, p->d_status, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    if (st == ST_FIELD_ABOVE_EMAX) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
+    return LUNA_OK;
+}
+
+// ---------------------------------------------------------------- batches
+int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts* opts, luna_batch** out) {
+    if (!plans || n <= 0 || !opts || !out) return fail(LUNA_ERR_BAD_ARG, "batch_create: bad argument");
+    if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "batch_create: save points missing");
+    const int prec = plans[0]->precision;
+    for (int i = 0; i < n; ++i)
+        if (!plans[i] || plans[i]->precision != prec) return fail(LUNA_ERR_BAD_ARG, "batch_create: plans must share one precision");
+    luna_batch* b = new luna_batch();
+    b->n = n;
+    b->precision = prec;
+    b->plans.assign(plans, plans + n);
+    b->opts = *opts;
+    b->h.resize(n);
+    b->ybuf.resize(n);
+    b->ynbuf.resize(n);
+    b->steplogs.assign(n, nullptr);
+    const size_t kel = (prec == LUNA_PREC_FP64) ? sizeof(double2) : sizeof(float2);
+    auto bail = [&](int rc) {
+        free_all(b->allocs);
+        delete b;
+        return rc;
+    };
+    if (opts->saveN > 0) {
+        const double* zs = nullptr;
+        if (upload(b->allocs, opts->zsave, (size_t)opts->saveN, &zs)) return bail(LUNA_ERR_CUDA);
+        b->d_zsave = const_cast<double*>(zs);
+    }
+    // one slab per instance
+    size_t maxsm = 0;
+    for (int i = 0; i < n; ++i) {
+        LunaInst I = plans[i]->proto;
+        const size_t Nw = I.Nw;
+        const size_t gsb = (prec == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
+        size_t off = 0;
+        auto carve = [&](size_t bytes) { size_t o = off; off += align_up(bytes, 256); return o; };
+        const size_t oy0 = carve(Nw * sizeof(double2));
+        const size_t oy = carve(Nw * sizeof(double2)), oyn = carve(Nw * sizeof(double2));
+        size_t ok[7];
+        for (int j = 0; j < 7; ++j) ok[j] = carve(Nw * kel);
+        const size_t oe1 = carve(Nw * sizeof(double2));
+        const size_t og = carve(gsb);
+        const size_t osv = carve((size_t)opts->saveN * Nw * sizeof(double2));
+        const size_t olog = carve((size_t)(opts->steplog_cap > 0 ? opts->steplog_cap : 0) * 4 * sizeof(double));
+        char* slab = nullptr;
+        if (dalloc(b->allocs, &slab, off)) return bail(LUNA_ERR_CUDA);
+        I.y0 = (const double2*)(slab + oy0);
+        I.y = (double2*)(slab + oy);
+        I.yn = (double2*)(slab + oyn);
+        for (int j = 0; j < 7; ++j) I.k[j] = slab + ok[j];
+        I.e1 = (double2*)(slab + oe1);
+        I.gscr = slab + og;
+        I.saves = (double2*)(slab + osv);
+        I.zsave = b->d_zsave;
+        I.saveN = opts->saveN;
+        I.rtol = opts->rtol;
+        I.atol = opts->atol;
+        I.safety = opts->safety;
+        I.max_dt = opts->max_dt;
+        I.min_dt = opts->min_dt;
+        I.repeat_limit = opts->repeat_limit;
+        I.max_steps = opts->max_steps;
+        I.steplog = opts->steplog_cap > 0 ? (double*)(slab + olog) : nullptr;
+        I.steplog_cap = opts->steplog_cap;
+        I.replay = nullptr;
+        I.nreplay = 0;
+        if (opts->replay && opts->nreplay > 0) {
+            const double* rp = nullptr;
+            if (upload(b->allocs, opts->replay, 2 * (size_t)opts->nreplay, &rp)) return bail(LUNA_ERR_CUDA);
+            I.replay = rp;
+            I.nreplay = opts->nreplay;
+        }
+        b->steplogs[i] = I.steplog;
+        b->ybuf[i] = I.y;
+        b->ynbuf[i] = I.yn;
+        b->h[i] = I;
+        maxsm = std::max(maxsm, (prec == LUNA_PREC_FP64) ? smem_wanted<double>(I) : smem_wanted<float>(I));
+    }
+    if (dalloc(b->allocs, &b->d_insts, sizeof(LunaInst) * n)) return bail(LUNA_ERR_CUDA);
+    if (dalloc(b->allocs, &b->d_counter, sizeof(int))) return bail(LUNA_ERR_CUDA);
+    b->smem = (int)std::min<size_t>(maxsm, (size_t)max_smem_optin());
+    int dev = 0, nsm = 0, occ = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (prec == LUNA_PREC_FP64) {
+        if (cudaFuncSetAttribute(solve_kernel<double, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->smem) != cudaSuccess)
+            return bail(fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size"));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel<double, double>, LUNA_BLOCK, b->smem);
+    } else {
+        if (cudaFuncSetAttribute(solve_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->smem) != cudaSuccess)
+            return bail(fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size"));
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, solve_kernel<float, float>, LUNA_BLOCK, b->smem);
+    }
+    if (occ < 1) return bail(fail(LUNA_ERR_CUDA, "batch_create: solver kernel does not fit on an SM"));
+    b->grid = std::min(n, nsm * occ);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        return bail(fail(LUNA_ERR_CUDA, "batch_create: stream/event creation failed"));
+    *out = b;
+    return LUNA_OK;
+}
+
+int luna_b200_batch_upload(luna_batch* b, const double* const* linops, const double* const* y0, const double* z0,
+                           const double* dz0, const double* zmax) {
+    if (!b || !linops || !y0 || !z0 || !dz0 || !zmax) return fail(LUNA_ERR_BAD_ARG, "batch_upload: null argument");
+    for (int i = 0; i < b->n; ++i) {
+        LunaInst& I = b->h[i];
+        const size_t bytes = sizeof(double2) * I.Nw;
+        if (!I.linop) {
+            double2* L = nullptr;
+            if (dalloc(b->allocs, &L, bytes)) return LUNA_ERR_CUDA;
+            I.linop = L;
+        }
+        CK(cudaMemcpyAsync((void*)I.linop, linops[i], bytes, cudaMemcpyHostToDevice, b->stream));
+        I.y = b->ybuf[i];
+        I.yn = b->ynbuf[i];
+        CK(cudaMemcpyAsync((void*)I.y0, y0[i], bytes, cudaMemcpyHostToDevice, b->stream));
+        I.z0 = z0[i];
+        I.dz0 = dz0[i];
+        I.zmax = zmax[i];
+        I.status = 0;
+        I.nsaved = 0;
+        I.steps = I.accepted = I.rejected = I.nrhs = 0;
+    }
+    CK(cudaMemcpyAsync(b->d_insts, b->h.data(), sizeof(LunaInst) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return LUNA_OK;
+}
+
+int luna_b200_batch_run(luna_batch* b, float* device_ms) {
+    if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_run: null batch");
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+    // instances restart from y0: restore the per-instance pointers and counters
+    CK(cudaMemcpyAsync(b->d_insts, b->h.data(), sizeof(LunaInst) * b->n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+    CK(cudaEventRecord(b->ev0, b->stream));
+    if (b->precision == LUNA_PREC_FP64)
+        solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem);
+    else
+        solve_kernel<float, float><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.f, b->smem);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(b->ev1, b->stream));
+    CK(cudaEventSynchronize(b->ev1));
+    if (device_ms) CK(cudaEventElapsedTime(device_ms, b->ev0, b->ev1));
+    return LUNA_OK;
+}
+
+int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out, luna_solve_stats* stats) {
+    if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_download: null batch");
+    std::vector<LunaInst> res(b->n);
+    CK(cudaMemcpyAsync(res.data(), b->d_insts, sizeof(LunaInst) * b->n, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < b->n; ++i) {
+        const LunaInst& I = res[i];
+        const size_t Nw = I.Nw;
+        if (saves && saves[i] && b->opts.saveN > 0)
+            CK(cudaMemcpyAsync(saves[i], I.saves, sizeof(double2) * Nw * b->opts.saveN, cudaMemcpyDeviceToHost, b->stream));
+        if (y_out && y_out[i]) {
+            // the integrator state after the last step: yn when that step was accepted
+            CK(cudaMemcpyAsync(y_out[i], I.yn, sizeof(double2) * Nw, cudaMemcpyDeviceToHost, b->stream));
+        }
+        if (stats) {
+            luna_solve_stats& s = stats[i];
+            s.status = I.status;
+            s.nsaved = I.nsaved;
+            s.steps = I.steps;
+            s.accepted = I.accepted;
+            s.rejected = I.rejected;
+            s.nrhs = I.nrhs;
+            s.z = I.z;
+            s.dz = I.dz;
+        }
+    }
+    CK(cudaStreamSynchronize(b->stream));
+    return LUNA_OK;
+}
+
+int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog) {
+    if (!b || i < 0 || i >= b->n || !steplog || !b->steplogs[i]) return fail(LUNA_ERR_BAD_ARG, "batch_steplog: bad argument");
+    CK(cudaMemcpy(steplog, b->steplogs[i], sizeof(double) * 4 * b->opts.steplog_cap, cudaMemcpyDeviceToHost));
+    return LUNA_OK;
+}
+
+void luna_b200_batch_destroy(luna_batch* b) {
+    if (!b) return;
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    free_all(b->allocs);
+    delete b;
+}
+
+int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z0, double dz0, double zmax,
+                    const luna_solve_opts* opts, double* saves, double* steplog, luna_solve_stats* stats) {
+    if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "solve: null argument");
+    luna_batch* b = nullptr;
+    int rc = luna_b200_batch_create(&p, 1, opts, &b);
+    if (rc) return rc;
+    const double* L[1] = {linop};
+    const double* Y[1] = {y_inout};
+    rc = luna_b200_batch_upload(b, L, Y, &z0, &dz0, &zmax);
+    if (!rc) rc = luna_b200_batch_run(b, nullptr);
+    double* S[1] = {saves};
+    double* YO[1] = {y_inout};
+    luna_solve_stats st{};
+    if (!rc) rc = luna_b200_batch_download(b, S, YO, &st);
+    if (!rc && steplog && opts->steplog_cap > 0) rc = luna_b200_batch_steplog(b, 0, steplog);
+    luna_b200_batch_destroy(b);
+    if (rc) return rc;
+    if (stats) *stats = st;
+    if (st.status == ST_FIELD_ABOVE_EMAX) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
+    if (st.status == ST_REPEAT_LIMIT) return fail(LUNA_REPEAT_LIMIT, "Reached limit for step repetition");
+    if (st.status == ST_STEP_BUDGET) return fail(LUNA_STEP_BUDGET, "Step budget exhausted before zmax");
+    return LUNA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,899 @@
+// Fused mode-averaged UPPE right-hand side and the interaction-picture RK45 loop,
+// one instance per CTA.
+//
+// Right-hand side (NonlinearRHS.jl:362-373, TransModeAvg):
+//   load E(omega) (fused with the RK stage combine and exp(L*dz))
+//   -> zero-pad + inverse transform to the oversampled time grid (real: half-length
+//      complex FFT with the split pre-twiddle; envelope: complex FFT)
+//   -> responses accumulated in tuple order: Kerr, PlasmaCumtrapz (three block scans
+//      for the cumulative integrals), Raman convolution on the 2x grid
+//   -> time window -> forward transform -> crop, normalisation, frequency window
+//   -> store (fused with exp(-L*dz) into the stage derivative).
+//
+// Integrator (RK45.jl:128-226, 249-297, 343-406 with dopri.jl) and Luna.run's per-step
+// window filter and GridCondition saves (Luna.jl:366-372, Output.jl:65-82, 490-502).
+#pragma once
+#include "common.cuh"
+#include "fft.cuh"
+#include "inst.h"
+
+namespace luna {
+
+// ------------------------------------------------------------------ workspace layout
+template <typename Rl>
+struct Ws {
+    cpx<Rl>* main;      // transform buffer
+    cpx<Rl>* main_alt;  // second buffer when the transform is out of place (global)
+    cpx<Rl>* efac;      // exp(L*dz) of the current stage, Nw entries
+    cpx<Rl>* ram;       // Raman convolution buffer (No complex)
+    cpx<Rl>* ram_alt;
+    double* red;        // 3 * LUNA_WARPS reduction scratch
+    double* tot;        // 3 * LUNA_WARPS scan totals
+    double* edge;       // 4 edge values carried between scan chunks
+    int* flag;          // status flags raised inside the RHS
+    TwTab<Rl> tw;
+};
+
+struct Ctl {  // controller state shared by the CTA (shared memory)
+    double t, tn, dt, dtn, err, errlast;
+    int ok;
+    int done;
+    int status;
+    int repeated;
+    long long steps;
+    int inst;
+};
+
+__host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// main transform length (complex elements) for an instance
+__host__ __device__ inline int main_len(const LunaInst& I) {
+    int M = (I.kind == 0) ? I.No / 2 : I.No;
+    int Mc = (I.kind == 0) ? I.N / 2 : I.N;
+    return M > Mc ? M : Mc;
+}
+
+__host__ __device__ inline bool has_raman(const LunaInst& I) {
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].kind == LUNA_RESP_RAMAN) return true;
+    return false;
+}
+
+// Bytes of global scratch an instance needs when nothing lives in shared memory.
+template <typename Rl>
+__host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
+    size_t c = sizeof(cpx<Rl>);
+    size_t b = 0;
+    b += align_up(2 * (size_t)main_len(I) * c, 256);
+    b += align_up((size_t)I.Nw * c, 256);
+    if (has_raman(I)) b += align_up(2 * (size_t)I.No * c, 256);
+    return b;
+}
+
+#define LUNA_SMALL_BYTES 2048
+
+template <typename Rl>
+__device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w, const TwTab<Rl>& tw) {
+    w.red = reinterpret_cast<double*>(smem);
+    w.tot = w.red + 3 * LUNA_WARPS;
+    w.edge = w.tot + 3 * LUNA_WARPS;
+    w.flag = reinterpret_cast<int*>(w.edge + 4);
+    w.tw = tw;
+    size_t off = LUNA_SMALL_BYTES;
+    const size_t c = sizeof(cpx<Rl>);
+    char* g = reinterpret_cast<char*>(I.gscr);
+    size_t goff = 0;
+    const int Mm = main_len(I);
+    size_t mb = align_up((size_t)Mm * c, 256);
+    if (fft_is_inplace<Rl>(Mm) && off + mb <= (size_t)smem_bytes) {
+        w.main = reinterpret_cast<cpx<Rl>*>(smem + off);
+        w.main_alt = nullptr;
+        off += mb;
+    } else {
+        w.main = reinterpret_cast<cpx<Rl>*>(g + goff);
+        w.main_alt = reinterpret_cast<cpx<Rl>*>(g + goff + mb);
+    }
+    goff += 2 * mb;
+    size_t eb = align_up((size_t)I.Nw * c, 256);
+    if (off + eb <= (size_t)smem_bytes) {
+        w.efac = reinterpret_cast<cpx<Rl>*>(smem + off);
+        off += eb;
+    } else {
+        w.efac = reinterpret_cast<cpx<Rl>*>(g + goff);
+    }
+    goff += eb;
+    w.ram = w.ram_alt = nullptr;
+    if (has_raman(I)) {
+        size_t rb = align_up((size_t)I.No * c, 256);
+        if (fft_is_inplace<Rl>(I.No) && off + rb <= (size_t)smem_bytes) {
+            w.ram = reinterpret_cast<cpx<Rl>*>(smem + off);
+            off += rb;
+        } else {
+            w.ram = reinterpret_cast<cpx<Rl>*>(g + goff);
+            w.ram_alt = reinterpret_cast<cpx<Rl>*>(g + goff + rb);
+        }
+        goff += 2 * rb;
+    }
+}
+
+// ------------------------------------------------------------------ block reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum of three values; result valid in every thread.
+__device__ __forceinline__ void block_sum3(double& a, double& b, double& c, double* red) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    a = warp_sum(a);
+    b = warp_sum(b);
+    c = warp_sum(c);
+    __syncthreads();
+    if (lane == 0) {
+        red[wid] = a;
+        red[LUNA_WARPS + wid] = b;
+        red[2 * LUNA_WARPS + wid] = c;
+    }
+    __syncthreads();
+    double sa = 0, sb = 0, sc = 0;
+#pragma unroll
+    for (int i = 0; i < LUNA_WARPS; ++i) {
+        sa += red[i];
+        sb += red[LUNA_WARPS + i];
+        sc += red[2 * LUNA_WARPS + i];
+    }
+    a = sa;
+    b = sb;
+    c = sc;
+}
+
+// Block exclusive scan of one double per thread (one barrier). `tot` must not be
+// reused by another scan before the next barrier that follows every thread's return.
+__device__ __forceinline__ double block_exscan(double v, double* tot, double& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) tot[wid] = x;
+    __syncthreads();
+    double off = 0, all = 0;
+#pragma unroll
+    for (int i = 0; i < LUNA_WARPS; ++i) {
+        double tv = tot[i];
+        off += (i < wid) ? tv : 0.0;
+        all += tv;
+    }
+    total = all;
+    return off + x - v;
+}
+
+// ------------------------------------------------------------------ rate functions
+template <typename Rl>
+__device__ __forceinline__ Rl ppt_rate(const LunaResp& r, Rl aE, int* flag);
+
+template <>
+__device__ __forceinline__ double ppt_rate<double>(const LunaResp& r, double aE, int* flag) {
+    // Ionisation.jl:257-270 with CSpline evaluation (Maths.jl:835-848) and the uniform
+    // index function (Maths.jl:772-774)
+    if (aE < r.Emin) return 0.0;
+    if (aE > r.Emax) {
+        atomicOr(flag, 1 << ST_FIELD_ABOVE_EMAX);
+        return 0.0;
+    }
+    const int n = r.sn;
+    const double xmin = r.Emin, xmax = r.Emax;
+    int i1;
+    if (aE <= xmin) i1 = 2;
+    else if (aE >= xmax) i1 = n;
+    else i1 = (int)ceil((aE - xmin) / (xmax - xmin) * (double)(n - 1)) + 1;
+    const int i = i1 - 1;
+    const double xi = __ldg(r.sx + i), xm = __ldg(r.sx + i - 1);
+    const double yi = __ldg(r.sy + i), ym = __ldg(r.sy + i - 1);
+    double v;
+    if (aE == xi) v = yi;
+    else if (aE == xm) v = ym;
+    else {
+        const double Di = __ldg(r.sD + i), Dm = __ldg(r.sD + i - 1);
+        const double t = (aE - xm) / (xi - xm);
+        v = ym + Dm * t + (3.0 * (yi - ym) - 2.0 * Dm - Di) * (t * t)
+            + (2.0 * (ym - yi) + Dm + Di) * (t * t * t);
+    }
+    return exp(v);
+}
+
+template <>
+__device__ __forceinline__ float ppt_rate<float>(const LunaResp& r, float aE, int* flag) {
+    if (aE < (float)r.Emin) return 0.0f;
+    if (aE > (float)r.Emax) {
+        atomicOr(flag, 1 << ST_FIELD_ABOVE_EMAX);
+        return 0.0f;
+    }
+    const int n = r.sn;
+    const float xmin = (float)r.Emin, xmax = (float)r.Emax;
+    int i1 = (int)ceilf((aE - xmin) / (xmax - xmin) * (float)(n - 1)) + 1;
+    i1 = max(2, min(n, i1));
+    const int i = i1 - 1;
+    const float xi = __ldg(r.sxf + i), xm = __ldg(r.sxf + i - 1);
+    const float yi = __ldg(r.syf + i), ym = __ldg(r.syf + i - 1);
+    const float Di = __ldg(r.sDf + i), Dm = __ldg(r.sDf + i - 1);
+    const float t = (aE - xm) / (xi - xm);
+    const float v = ym + Dm * t + (3.0f * (yi - ym) - 2.0f * Dm - Di) * (t * t)
+                    + (2.0f * (ym - yi) + Dm + Di) * (t * t * t);
+    return expf(v);
+}
+
+template <typename Rl>
+__device__ __forceinline__ Rl adk_rate(const LunaResp& r, Rl aE) {
+    // Ionisation.jl:43-59: pre * (a/|E|)^(2n*-1) * exp(-b/|E|) above the threshold
+    if (aE < (Rl)r.adk_thr || aE == (Rl)0) return (Rl)0;
+    if (sizeof(Rl) == 8) {
+        double x = (double)aE;
+        return (Rl)(r.adk_pre * pow(r.adk_a / x, r.adk_pw) * exp(-r.adk_b / x));
+    } else {
+        float x = (float)aE;
+        float lg = (float)r.adk_pw * logf((float)r.adk_a / x) - (float)r.adk_b / x + logf((float)r.adk_pre);
+        return (Rl)expf(lg);
+    }
+}
+
+template <typename Rl>
+__device__ __forceinline__ Rl eval_rate(const LunaResp& r, Rl aE, int* flag) {
+    return r.kind == LUNA_RESP_PLASMA_PPT ? ppt_rate<Rl>(r, aE, flag) : adk_rate<Rl>(r, aE);
+}
+
+// ------------------------------------------------------------------ real-FFT helpers
+// exp(+-2*pi*i*k/(2M)) as a table twiddle
+template <typename Rl, bool INV>
+__device__ __forceinline__ cpx<double> half_twiddle(const TwTab<Rl>& tw, int k, int M) {
+    const int shift = TW_LOG_MMAX - (ilog2i((unsigned)M) + 1);
+    cpx<Rl> w = twiddle<Rl, INV>(tw, (unsigned)k << shift);
+    return cvt<double>(w);
+}
+
+// Raman convolution on the 2*No grid (Nonlinear.jl:282-333): the input samples s[n]
+// (n < No) are in `ram` as complex pairs (s[2m], s[2m+1]) for m < No/2 and zero above;
+// the result P[n], n < No, is returned in the same pair layout.
+template <typename Rl>
+__device__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
+    __syncthreads();
+    cpx<Rl>* Z = block_fft<Rl, false>(w.ram, w.ram_alt, No, w.tw);
+    const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(r.H);
+    const int M = No;  // complex length of the 2*No real transform
+    for (int k = threadIdx.x; k <= M / 2; k += LUNA_BLOCK) {
+        const int km = (M - k) & (M - 1);
+        cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k)]);
+        cpx<double> Zm = cvt<double>(Z[Swz<Rl>::f(km)]);
+        // forward split: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k])
+        cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
+        cpx<double> a = Zk + conj(Zm), b = Zk - conj(Zm);
+        cpx<double> Xk = scale(0.5, a) + scale(0.5, mul_mi<double, false>(Wk * b));
+        cpx<double> Xm;  // X[M-k]
+        if (k == 0) {
+            Xk = mk<double>(Zk.x + Zk.y, 0.0);
+            Xm = mk<double>(Zk.x - Zk.y, 0.0);  // X[M]
+        } else {
+            // W^(M-k) = -conj(W^k)
+            cpx<double> Wm = scale(-1.0, conj(Wk));
+            cpx<double> a2 = Zm + conj(Zk), b2 = Zm - conj(Zk);
+            Xm = scale(0.5, a2) + scale(0.5, mul_mi<double, false>(Wm * b2));
+        }
+        cpx<double> Yk = Xk * cvt<double>(ldg(H + k));
+        cpx<double> Ym = Xm * cvt<double>(ldg(H + (M - k)));
+        // inverse split: Z'[k] = (Y[k] + conj Y[M-k]) + i W^-k (Y[k] - conj Y[M-k])
+        cpx<double> Wi = conj(Wk);
+        cpx<double> Zk2 = (Yk + conj(Ym)) + mul_mi<double, true>(Wi * (Yk - conj(Ym)));
+        Z[Swz<Rl>::f(k)] = cvt<Rl>(Zk2);
+        if (k != 0 && km != k) {
+            cpx<double> Wmi = scale(-1.0, Wk);  // W^-(M-k) = -W^k
+            cpx<double> Zm2 = (Ym + conj(Yk)) + mul_mi<double, true>(Wmi * (Ym - conj(Yk)));
+            Z[Swz<Rl>::f(km)] = cvt<Rl>(Zm2);
+        }
+    }
+    cpx<Rl>* other = (Z == w.ram) ? w.ram_alt : w.ram;
+    __syncthreads();
+    return block_fft<Rl, true>(Z, other, No, w.tw);
+}
+
+
+// ------------------------------------------------------------------ plasma chunk
+// PlasmaScalar! (Nonlinear.jl:121-133) for the pair of samples (2m, 2m+1) held by this
+// thread. Each running trapezoid is written as dt*(prefix_sum(y)[n] - (y[0]+y[n])/2), so
+// the three cumulative integrals are plain block prefix sums (FP64) carried across
+// chunks; y[0] of each integrand is broadcast from the first chunk through `edge`.
+struct PlasmaCarry {
+    double c1, c2, c3;
+};
+
+template <typename Rl>
+__device__ __forceinline__ void plasma_pair(const LunaResp& r, bool act, int m, double E0, double E1,
+                                            PlasmaCarry& cr, Ws<Rl>& w, double& P0, double& P1) {
+    const double dt = r.dt;
+    const double r0 = act ? (double)eval_rate<Rl>(r, (Rl)fabs(E0), w.flag) : 0.0;
+    const double r1 = act ? (double)eval_rate<Rl>(r, (Rl)fabs(E1), w.flag) : 0.0;
+    const bool first = (m == 0);
+    if (first) w.edge[0] = r0;
+    double tot;
+    double x = block_exscan(r0 + r1, w.tot, tot);
+    const double y0r = w.edge[0];
+    const double S0 = cr.c1 + x + r0, S1 = S0 + r1;
+    cr.c1 += tot;
+    // fraction = preionfrac + 1 - exp(-int rate)
+    const double f0 = dt * (S0 - 0.5 * (y0r + r0)), f1 = dt * (S1 - 0.5 * (y0r + r1));
+    const double fr0 = r.preion + 1.0 - ((f0 == 0.0) ? 1.0 : exp(-f0));
+    const double fr1 = r.preion + 1.0 - ((f1 == 0.0) ? 1.0 : exp(-f1));
+    const double er = r.eratio;  // e^2/m_e
+    const double ph0 = act ? fr0 * er * E0 : 0.0, ph1 = act ? fr1 * er * E1 : 0.0;
+    if (first) w.edge[1] = ph0;
+    x = block_exscan(ph0 + ph1, w.tot + LUNA_WARPS, tot);
+    const double y0p = w.edge[1];
+    const double T0 = cr.c2 + x + ph0, T1 = T0 + ph1;
+    cr.c2 += tot;
+    double J0 = dt * (T0 - 0.5 * (y0p + ph0)), J1 = dt * (T1 - 0.5 * (y0p + ph1));
+    // ionisation loss term where |E| > 0
+    if (act && fabs(E0) > 0) J0 += r.ionpot * r0 * (1.0 - fr0) / E0;
+    if (act && fabs(E1) > 0) J1 += r.ionpot * r1 * (1.0 - fr1) / E1;
+    if (!act) { J0 = 0; J1 = 0; }
+    if (first) w.edge[2] = J0;
+    x = block_exscan(J0 + J1, w.tot + 2 * LUNA_WARPS, tot);
+    const double y0J = w.edge[2];
+    const double U0 = cr.c3 + x + J0, U1 = U0 + J1;
+    cr.c3 += tot;
+    P0 += r.coef * (dt * (U0 - 0.5 * (y0J + J0)));
+    P1 += r.coef * (dt * (U1 - 0.5 * (y0J + J1)));
+}
+
+// ------------------------------------------------------------------ the right-hand sides
+// load(k) -> cpx<double> input bin k (k < Nw); store(k, v) consumes output bin k (k < Nw).
+
+// field-resolved grid (RealGrid): to_time! / to_freq! with rfft semantics
+template <typename Rl, typename LoadF, typename StoreF>
+__device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+    const int M = I.No / 2;
+    const int Nw = I.Nw;
+    const int T = LUNA_BLOCK;
+    const int tid = threadIdx.x;
+    cpx<Rl>* buf = w.main;
+    // C2R pre-twiddle: Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
+    for (int k = tid; k <= M / 2; k += T) {
+        const int km = M - k;
+        cpx<double> Xk = (k < Nw) ? load(k) : mk<double>(0, 0);
+        // each bin is loaded once (the loader may update stage state in place)
+        cpx<double> Xm = (km == k) ? Xk : ((km < Nw) ? load(km) : mk<double>(0, 0));
+        if (k == 0) {  // imaginary parts of DC and Nyquist do not enter a real transform
+            Xk.y = 0;
+            Xm.y = 0;
+        }
+        cpx<double> Wi = half_twiddle<Rl, true>(w.tw, k, M);
+        cpx<double> Zk = (Xk + conj(Xm)) + mul_mi<double, true>(Wi * (Xk - conj(Xm)));
+        buf[Swz<Rl>::f(k)] = cvt<Rl>(Zk);
+        if (k != 0 && km != k) {
+            cpx<double> Wmi = scale(-1.0, conj(Wi));
+            cpx<double> Zm = (Xm + conj(Xk)) + mul_mi<double, true>(Wmi * (Xm - conj(Xk)));
+            buf[Swz<Rl>::f(km)] = cvt<Rl>(Zm);
+        }
+    }
+    __syncthreads();
+    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+    const double sc = I.in_scale;
+    int ip = -1, ir = -1;
+    for (int i = 0; i < I.nresp; ++i) {
+        if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
+        if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
+    }
+    cpx<Rl>* Pr = nullptr;
+    if (ir >= 0) {
+        // E^2 on the first half of the 2*No grid (thg=true form of sqr!)
+        for (int m = tid; m < I.No; m += T) {
+            cpx<Rl> v = mk<Rl>(0, 0);
+            if (m < M) {
+                cpx<Rl> e = x[Swz<Rl>::f(m)];
+                Rl e0 = e.x * (Rl)sc, e1 = e.y * (Rl)sc;
+                v = mk<Rl>(e0 * e0, e1 * e1);
+            }
+            w.ram[Swz<Rl>::f(m)] = v;
+        }
+        Pr = raman_conv<Rl>(I.resp[ir], I.No, w);
+    }
+    PlasmaCarry cr = {0, 0, 0};
+    for (int c0 = 0; c0 < M; c0 += T) {
+        const int m = c0 + tid;
+        const bool act = m < M;
+        cpx<Rl> e = act ? x[Swz<Rl>::f(m)] : mk<Rl>(0, 0);
+        const double E0 = (double)e.x * sc, E1 = (double)e.y * sc;
+        double P0 = 0, P1 = 0;
+        for (int i = 0; i < I.nresp; ++i) {
+            const LunaResp& r = I.resp[i];
+            if (r.kind == LUNA_RESP_KERR_FIELD) {
+                P0 += r.coef * (E0 * E0 * E0);
+                P1 += r.coef * (E1 * E1 * E1);
+            } else if (i == ir) {
+                cpx<Rl> p = act ? Pr[Swz<Rl>::f(m)] : mk<Rl>(0, 0);
+                P0 += r.coef * E0 * (double)p.x;
+                P1 += r.coef * E1 * (double)p.y;
+            } else if (i == ip) {
+                plasma_pair<Rl>(r, act, m, E0, E1, cr, w, P0, P1);
+            }
+        }
+        if (act) {
+            const double tw0 = __ldg(I.towin + 2 * m), tw1 = __ldg(I.towin + 2 * m + 1);
+            x[Swz<Rl>::f(m)] = mk<Rl>((Rl)(P0 * tw0), (Rl)(P1 * tw1));
+        }
+    }
+    __syncthreads();
+    cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, M, w.tw);
+    // R2C split: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw
+    for (int k = tid; k < Nw; k += T) {
+        const int km = (M - k) & (M - 1);
+        cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
+        cpx<double> Zm = cvt<double>(Z[Swz<Rl>::f(km)]);
+        cpx<double> X;
+        if (k == 0) X = mk<double>(Zk.x + Zk.y, 0.0);
+        else if (k == M) X = mk<double>(Zk.x - Zk.y, 0.0);
+        else {
+            cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
+            X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
+        }
+        store(k, X * ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k));
+    }
+    __syncthreads();
+}
+
+// envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
+template <typename Rl, typename LoadF, typename StoreF>
+__device__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+    const int No = I.No, N = I.N, h = I.N / 2;
+    const int T = LUNA_BLOCK;
+    const int tid = threadIdx.x;
+    cpx<Rl>* buf = w.main;
+    for (int j = tid; j < No; j += T) {
+        cpx<double> X = mk<double>(0, 0);
+        if (j < h) X = load(j);
+        else if (j >= No - h) X = load(j - No + N);
+        buf[Swz<Rl>::f(j)] = cvt<Rl>(X);
+    }
+    __syncthreads();
+    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, No, w.tw);
+    const double sc = I.in_scale;
+    int ir = -1;
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
+    cpx<Rl>* Pr = nullptr;
+    if (ir >= 0) {
+        // 1/2 |E|^2 on the first half of the 2*No grid (sqr! for RamanPolarEnv)
+        for (int m = tid; m < No; m += T) {
+            cpx<Rl> v = mk<Rl>(0, 0);
+            if (m < No / 2) {
+                cpx<double> a = scale(sc, cvt<double>(x[Swz<Rl>::f(2 * m)]));
+                cpx<double> b = scale(sc, cvt<double>(x[Swz<Rl>::f(2 * m + 1)]));
+                v = mk<Rl>((Rl)(0.5 * abs2(a)), (Rl)(0.5 * abs2(b)));
+            }
+            w.ram[Swz<Rl>::f(m)] = v;
+        }
+        Pr = raman_conv<Rl>(I.resp[ir], No, w);
+    }
+    for (int n = tid; n < No; n += T) {
+        cpx<double> E = scale(sc, cvt<double>(x[Swz<Rl>::f(n)]));
+        cpx<double> P = mk<double>(0, 0);
+        for (int i = 0; i < I.nresp; ++i) {
+            const LunaResp& r = I.resp[i];
+            if (r.kind == LUNA_RESP_KERR_ENV) {
+                P = P + scale(0.75 * r.coef * abs2(E), E);
+            } else if (i == ir) {
+                cpx<Rl> p = Pr[Swz<Rl>::f(n >> 1)];
+                double pv = (n & 1) ? (double)p.y : (double)p.x;
+                P = P + scale(r.coef * pv, E);
+            }
+        }
+        x[Swz<Rl>::f(n)] = cvt<Rl>(scale(__ldg(I.towin + n), P));
+    }
+    __syncthreads();
+    cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, No, w.tw);
+    for (int k = tid; k < N; k += T) {
+        const int src = (k < h) ? k : (No - N + k);
+        cpx<double> X = cvt<double>(Z[Swz<Rl>::f(src)]);
+        store(k, X * ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k));
+    }
+    __syncthreads();
+}
+
+template <typename Rl, typename LoadF, typename StoreF>
+__device__ __forceinline__ void rhs(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+    if (I.kind == 0) rhs_real<Rl>(I, w, load, store);
+    else rhs_env<Rl>(I, w, load, store);
+}
+
+// ------------------------------------------------------------------ stepfun filter
+// Luna.jl:366-372: Eω .*= ωwin; Et = FT \ Eω; Et .*= twin; Eω = FT * Et (coarse grid),
+// applied to yn after multiplying by exp(L*dz) (prop!_maybe, RK45.jl:225).
+template <typename Rl>
+__device__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double2* yn, const double2* e1) {
+    const int tid = threadIdx.x, T = LUNA_BLOCK;
+    const int Nw = I.Nw, N = I.N;
+    cpx<Rl>* buf = w.main;
+    const cpx<double>* Y = reinterpret_cast<const cpx<double>*>(yn);
+    const cpx<double>* P = reinterpret_cast<const cpx<double>*>(e1);
+    auto ld = [&](int k) -> cpx<double> { return scale(__ldg(I.wwin + k), Y[k] * P[k]); };
+    cpx<double>* Yo = reinterpret_cast<cpx<double>*>(yn);
+    if (I.kind == 0) {
+        const int M = N / 2;
+        for (int k = tid; k <= M / 2; k += T) {
+            const int km = M - k;
+            cpx<double> Xk = (k < Nw) ? ld(k) : mk<double>(0, 0);
+            cpx<double> Xm = (km == k) ? Xk : ((km < Nw) ? ld(km) : mk<double>(0, 0));
+            if (k == 0) {
+                Xk.y = 0;
+                Xm.y = 0;
+            }
+            cpx<double> Wi = half_twiddle<Rl, true>(w.tw, k, M);
+            cpx<double> Zk = (Xk + conj(Xm)) + mul_mi<double, true>(Wi * (Xk - conj(Xm)));
+            buf[Swz<Rl>::f(k)] = cvt<Rl>(Zk);
+            if (k != 0 && km != k) {
+                cpx<double> Wmi = scale(-1.0, conj(Wi));
+                cpx<double> Zm = (Xm + conj(Xk)) + mul_mi<double, true>(Wmi * (Xm - conj(Xk)));
+                buf[Swz<Rl>::f(km)] = cvt<Rl>(Zm);
+            }
+        }
+        __syncthreads();
+        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+        const double inv = 1.0 / (double)N;
+        for (int m = tid; m < M; m += T) {
+            cpx<Rl> e = x[Swz<Rl>::f(m)];
+            double a = (double)e.x * inv * __ldg(I.twin + 2 * m);
+            double b = (double)e.y * inv * __ldg(I.twin + 2 * m + 1);
+            x[Swz<Rl>::f(m)] = mk<Rl>((Rl)a, (Rl)b);
+        }
+        __syncthreads();
+        cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, M, w.tw);
+        for (int k = tid; k < Nw; k += T) {
+            const int km = (M - k) & (M - 1);
+            cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
+            cpx<double> Zm = cvt<double>(Z[Swz<Rl>::f(km)]);
+            cpx<double> X;
+            if (k == 0) X = mk<double>(Zk.x + Zk.y, 0.0);
+            else if (k == M) X = mk<double>(Zk.x - Zk.y, 0.0);
+            else {
+                cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
+                X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
+            }
+            Yo[k] = X;
+        }
+    } else {
+        for (int j = tid; j < N; j += T) buf[Swz<Rl>::f(j)] = cvt<Rl>(ld(j));
+        __syncthreads();
+        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, N, w.tw);
+        const double inv = 1.0 / (double)N;
+        for (int n = tid; n < N; n += T)
+            x[Swz<Rl>::f(n)] = cvt<Rl>(scale(inv * __ldg(I.twin + n), cvt<double>(x[Swz<Rl>::f(n)])));
+        __syncthreads();
+        cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, N, w.tw);
+        for (int k = tid; k < N; k += T) Yo[k] = cvt<double>(Z[Swz<Rl>::f(k)]);
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ integrator
+// Dormand-Prince tableau as shipped with the reference (dopri.jl:2-28): the step uses
+// the 4th-order weights b5, error weights b5-b4 and the 4x7 dense-output matrix.
+__device__ __constant__ double c_B[6][6] = {
+    {1.0 / 5, 0, 0, 0, 0, 0},
+    {3.0 / 40, 9.0 / 40, 0, 0, 0, 0},
+    {44.0 / 45, -56.0 / 15, 32.0 / 9, 0, 0, 0},
+    {19372.0 / 6561, -25360.0 / 2187, 64448.0 / 6561, -212.0 / 729, 0, 0},
+    {9017.0 / 3168, -355.0 / 33, 46732.0 / 5247, 49.0 / 176, -5103.0 / 18656, 0},
+    {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84}};
+__device__ __constant__ double c_nodes[6] = {1.0 / 5, 3.0 / 10, 4.0 / 5, 8.0 / 9, 1.0, 1.0};
+__device__ __constant__ double c_b5[7] = {5179.0 / 57600, 0, 7571.0 / 16695, 393.0 / 640,
+                                          -92097.0 / 339200, 187.0 / 2100, 1.0 / 40};
+__device__ __constant__ double c_b4[7] = {35.0 / 384, 0, 500.0 / 1113, 125.0 / 192, -2187.0 / 6784, 11.0 / 84, 0};
+__device__ __constant__ double c_interp[4][7] = {
+    {1, 0, 0, 0, 0, 0, 0},
+    {-183.0 / 64, 0, 1500.0 / 371, -125.0 / 32, 9477.0 / 3392, -11.0 / 7, 3.0 / 2},
+    {37.0 / 12, 0, -1000.0 / 159, 125.0 / 12, -729.0 / 106, 11.0 / 3, -4},
+    {-145.0 / 128, 0, 1000.0 / 371, -375.0 / 64, 25515.0 / 6784, -55.0 / 28, 5.0 / 2}};
+
+template <typename Kt> struct KT;
+template <> struct KT<double> {
+    static __device__ __forceinline__ cpx<double> ld(const void* p, int k) {
+        return reinterpret_cast<const cpx<double>*>(p)[k];
+    }
+    static __device__ __forceinline__ void st(void* p, int k, cpx<double> v) {
+        reinterpret_cast<cpx<double>*>(p)[k] = v;
+    }
+};
+template <> struct KT<float> {
+    static __device__ __forceinline__ cpx<double> ld(const void* p, int k) {
+        return cvt<double>(reinterpret_cast<const cpx<float>*>(p)[k]);
+    }
+    static __device__ __forceinline__ void st(void* p, int k, cpx<double> v) {
+        reinterpret_cast<cpx<float>*>(p)[k] = cvt<float>(v);
+    }
+};
+
+// exp(L*d): FP64 throughout for the plain path; for the mixed path the phase is formed
+// and reduced modulo 2*pi in FP64 and the trigonometry runs in FP32.
+template <typename Rl>
+__device__ __forceinline__ cpx<Rl> expLd(cpx<double> L, double d);
+template <>
+__device__ __forceinline__ cpx<double> expLd<double>(cpx<double> L, double d) {
+    const double a = exp(L.x * d);
+    double s, c;
+    sincos(L.y * d, &s, &c);
+    return mk<double>(a * c, a * s);
+}
+template <>
+__device__ __forceinline__ cpx<float> expLd<float>(cpx<double> L, double d) {
+    const double th = L.y * d;
+    const double r = th - 6.283185307179586 * rint(th * 0.15915494309189535);
+    float s, c;
+    sincosf((float)r, &s, &c);
+    const float a = expf((float)(L.x * d));
+    return mk<float>(a * c, a * s);
+}
+
+template <typename Rl>
+__device__ __forceinline__ cpx<double> inv_fac(cpx<Rl> f) {
+    cpx<double> d = cvt<double>(f);
+    const double inv = 1.0 / abs2(d);
+    return scale(inv, conj(d));
+}
+
+// Dense output (RK45.jl:249-268) into row `out`; after an accepted step ks[1] holds k7,
+// so the k1 and k7 coefficients both apply to that buffer.
+template <typename Rl, typename Kt>
+__device__ void interpolate_row(const LunaInst& I, const Ctl& c, double ti, void* const* k,
+                                const double2* py, const double2* pyn, double2* out) {
+    const int Nw = I.Nw;
+    const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
+    const cpx<double>* yn = reinterpret_cast<const cpx<double>*>(pyn);
+    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
+    cpx<double>* o = reinterpret_cast<cpx<double>*>(out);
+    if (ti == c.t) {
+        for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) o[i] = y[i];
+        return;
+    }
+    if (ti == c.tn) {
+        for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) o[i] = yn[i];
+        return;
+    }
+    const double s = (ti - c.t) / c.dt;
+    const double sp[4] = {s, s * s, s * s * s, (s * s) * (s * s)};
+    double b[7];
+#pragma unroll
+    for (int j = 0; j < 7; ++j) {
+        double acc = 0;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) acc += sp[p] * c_interp[p][j];
+        b[j] = acc;
+    }
+    const double d = ti - c.t;
+    for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) {
+        cpx<double> yi = mk<double>(0, 0);
+        cpx<double> k1 = KT<Kt>::ld(k[0], i);
+        yi = yi + scale(b[0], k1);
+#pragma unroll
+        for (int j = 1; j < 6; ++j) yi = yi + scale(b[j], KT<Kt>::ld(k[j], i));
+        yi = yi + scale(b[6], k1);
+        cpx<double> v = y[i] + scale(c.dt, yi);
+        o[i] = v * cvt<double>(expLd<double>(L[i], d));
+    }
+}
+
+template <typename Rl, typename Kt>
+__device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
+    const int tid = threadIdx.x, T = LUNA_BLOCK;
+    const int Nw = I.Nw;
+    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
+    void* k[7];
+    for (int j = 0; j < 7; ++j) k[j] = I.k[j];
+    cpx<double>* e1 = reinterpret_cast<cpx<double>*>(I.e1);
+    double2* py = I.y;
+    double2* pyn = I.yn;
+    long long nrhs = 0;
+    if (tid == 0) {
+        c.t = c.tn = I.z0;
+        c.dt = c.dtn = I.dz0;
+        c.err = c.errlast = 0;
+        c.ok = 0;
+        c.done = 0;
+        c.status = 0;
+        c.repeated = 0;
+        c.steps = 0;
+        *w.flag = 0;
+    }
+    // y = yn = y0
+    {
+        const cpx<double>* y0 = reinterpret_cast<const cpx<double>*>(I.y0);
+        cpx<double>* y = reinterpret_cast<cpx<double>*>(py);
+        cpx<double>* yn = reinterpret_cast<cpx<double>*>(pyn);
+        for (int i = tid; i < Nw; i += T) {
+            y[i] = y0[i];
+            yn[i] = y0[i];
+        }
+    }
+    __syncthreads();
+    // k1 = fbar(y0, t, t): propagation by exp(L*0) == 1
+    {
+        const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
+        void* k0 = k[0];
+        rhs<Rl>(I, w, [&](int i) { return y[i]; }, [&](int i, cpx<double> v) { KT<Kt>::st(k0, i, v); });
+        ++nrhs;
+    }
+    int saved = 0;
+    bool swap_y = false;  // y <- yn at the next step start (after an accepted step)
+    while (true) {
+        __syncthreads();
+        if (!(c.tn <= I.zmax) || c.done) break;
+        // ---------------- evaluate! (RK45.jl:209-223)
+        if (swap_y) {
+            double2* tmp = py;
+            py = pyn;
+            pyn = tmp;
+        }
+        const double dprop = c.tn - c.t;  // k1 <- exp(L*(tn-t)) k1
+        __syncthreads();
+        if (tid == 0) {
+            c.dt = c.dtn;
+            c.t = c.tn;
+        }
+        __syncthreads();
+        const double t0 = c.t, dt = c.dt;
+        const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
+        for (int s = 0; s < 6; ++s) {
+            const double d = (t0 + c_nodes[s] * dt) - t0;
+            const bool reuse = (s == 5);  // nodes 5 and 6 coincide
+            if (!reuse) {
+                for (int i = tid; i < Nw; i += T) {
+                    cpx<Rl> f = expLd<Rl>(L[i], d);
+                    w.efac[i] = f;
+                    if (s == 4) e1[i] = cvt<double>(f);
+                }
+            }
+            __syncthreads();
+            double coef[6];
+#pragma unroll
+            for (int j = 0; j < 6; ++j) coef[j] = dt * c_B[s][j];
+            void* kout = k[s + 1];
+            const bool propk1 = (s == 0) && (dprop != 0.0);
+            auto load = [&](int i) -> cpx<double> {
+                cpx<double> k1 = KT<Kt>::ld(k[0], i);
+                if (propk1) {
+                    k1 = k1 * e1[i];
+                    KT<Kt>::st(k[0], i, k1);
+                }
+                cpx<double> acc = y[i];
+                acc = acc + scale(coef[0], k1);
+                for (int j = 1; j <= s; ++j)
+                    if (c_B[s][j] != 0) acc = acc + scale(coef[j], KT<Kt>::ld(k[j], i));
+                return cvt<double>(w.efac[i]) * acc;
+            };
+            auto store = [&](int i, cpx<double> v) { KT<Kt>::st(kout, i, v * inv_fac<Rl>(w.efac[i])); };
+            rhs<Rl>(I, w, load, store);
+            ++nrhs;
+        }
+        // ---------------- step! (RK45.jl:167-192): combine, weak norm, PI control
+        double sy = 0, syn = 0, se = 0;
+        {
+            cpx<double>* yn = reinterpret_cast<cpx<double>*>(pyn);
+            double cb5[7], cer[7];
+#pragma unroll
+            for (int j = 0; j < 7; ++j) {
+                cb5[j] = dt * c_b5[j];
+                cer[j] = c_b5[j] - c_b4[j];
+            }
+            for (int i = tid; i < Nw; i += T) {
+                cpx<double> yi = y[i];
+                cpx<double> acc = yi;
+                cpx<double> er = mk<double>(0, 0);
+#pragma unroll
+                for (int j = 0; j < 7; ++j) {
+                    cpx<double> kj = KT<Kt>::ld(k[j], i);
+                    if (c_b5[j] != 0) acc = acc + scale(cb5[j], kj);
+                    if (cer[j] != 0) er = er + scale(cer[j], scale(dt, kj));
+                }
+                yn[i] = acc;
+                sy += abs2(yi);
+                syn += abs2(acc);
+                se += abs2(er);
+            }
+        }
+        block_sum3(sy, syn, se, w.red);
+        if (tid == 0) {
+            const double errwt = fmax(fmax(sqrt(sy), sqrt(syn)), I.atol);
+            const double err = sqrt(se) / I.rtol / errwt;
+            c.err = err;
+            int ok = err <= 1.0;
+            // stepcontrolPI! (RK45.jl:374-396)
+            const double b1 = 3.0 / 5 / 5, b2 = -1.0 / 5 / 5, eps = 0.8;
+            if (ok) {
+                if (c.errlast == 0) c.errlast = err;
+                double fac = (err == 0) ? 1.5 : I.safety * pow(eps / err, b1) * pow(eps / c.errlast, b2);
+                c.dtn = fac * c.dt;
+                c.errlast = err;
+            } else {
+                if (!isfinite(err)) c.dtn = c.dt / 2;
+                else c.dtn = c.dt * fmax(0.1, I.safety * pow(err, -1.0 / 5));
+            }
+            // steplims! (RK45.jl:399-406)
+            if (c.dtn > I.max_dt) c.dtn = I.max_dt;
+            else if (c.dtn < I.min_dt) {
+                c.dtn = I.min_dt;
+                ok = 1;
+            }
+            // replay mode: follow a given step sequence (dt of the next step, accept flag)
+            if (I.replay && c.steps < I.nreplay) {
+                ok = I.replay[2 * c.steps + 1] != 0.0;
+                if (c.steps + 1 < I.nreplay) c.dtn = I.replay[2 * (c.steps + 1)];
+            }
+            c.ok = ok;
+            if (ok) c.tn = c.t + c.dt;
+            c.steps += 1;
+            const long long si = c.steps - 1;
+            if (I.steplog && si < I.steplog_cap) {
+                I.steplog[4 * si + 0] = c.t;
+                I.steplog[4 * si + 1] = c.dt;
+                I.steplog[4 * si + 2] = err;
+                I.steplog[4 * si + 3] = (double)ok;
+            }
+            if (ok) {
+                c.repeated = 0;
+                I.accepted += 1;
+            } else {
+                c.repeated += 1;
+                I.rejected += 1;
+                if (c.repeated > I.repeat_limit) {
+                    c.status = ST_REPEAT_LIMIT;
+                    c.done = 1;
+                }
+            }
+            if (*w.flag & (1 << ST_FIELD_ABOVE_EMAX)) {
+                c.status = ST_FIELD_ABOVE_EMAX;
+                c.done = 1;
+            }
+            if (I.max_steps > 0 && c.steps >= I.max_steps && !c.done) {
+                c.status = ST_STEP_BUDGET;
+                c.done = 1;
+            }
+        }
+        __syncthreads();
+        if (c.done && c.status != 0) break;
+        if (c.ok) {
+            // FSAL: ks[1] <- ks[7]
+            void* tmp = k[0];
+            k[0] = k[6];
+            k[6] = tmp;
+            // prop!_maybe + stepfun window filter on yn
+            stepfun_filter<Rl>(I, w, pyn, I.e1);
+            // GridCondition saves (Output.jl:65-82, 490-502)
+            while (saved < I.saveN && I.zsave[saved] <= c.tn) {
+                interpolate_row<Rl, Kt>(I, c, I.zsave[saved], k, py, pyn, I.saves + (size_t)saved * Nw);
+                ++saved;
+            }
+            swap_y = true;
+        } else {
+            // yn = y; prop!_maybe with tn == t multiplies by exp(0) == 1
+            cpx<double>* yn = reinterpret_cast<cpx<double>*>(pyn);
+            for (int i = tid; i < Nw; i += T) yn[i] = y[i];
+            swap_y = false;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        // final state: the last accepted yn (already filtered)
+        I.status = c.status;
+        I.steps = c.steps;
+        I.nrhs = nrhs;
+        I.nsaved = saved;
+        I.z = c.tn;
+        I.dz = c.dtn;
+        I.y = py;
+        I.yn = pyn;
+        for (int j = 0; j < 7; ++j) I.k[j] = k[j];
+    }
+    __syncthreads();
+}
+
+}  // namespace luna

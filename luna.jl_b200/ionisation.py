@@ -172,6 +172,8 @@ class PPTSpline:
     ``x`` (fields), ``y`` (log rate) and ``D`` (Hermite slopes) are the device table.
     """
 
+    kind = "ppt"
+
     def __init__(self, E, rate):
         keep = rate > 0
         self.x = np.ascontiguousarray(E[keep], dtype=np.float64)

@@ -355,6 +355,7 @@ class RunResult:
         self.Eω = []
         self.steps = 0
         self.accepted = []  # (t, dt, err) of every accepted step
+        self.steps_all = []  # (dt, ok) of every step, accepted or not
         self.rejected = 0
         self.nrhs = 0
 
@@ -394,6 +395,7 @@ def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rto
     while s.tn <= grid.zmax:
         ok = s.step()
         res.steps += 1
+        res.steps_all.append((s.dt, 1.0 if ok else 0.0))
         if ok:
             res.accepted.append((s.t, s.dt, s.err))
             stepfun(s.yn, s.tn, s.dtn)

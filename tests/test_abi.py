@@ -1,0 +1,93 @@
+"""The C-ABI library loads, exports every entry point declared in include/luna_b200.h, and
+its descriptor structs have the layout the ctypes bindings assume. No compute calls."""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import ctypes
+import os
+import pathlib
+import re
+import subprocess
+
+import pytest
+
+from luna_b200 import _lib
+
+ROOT = pathlib.Path(__file__).resolve().parent.parent
+HEADER = ROOT / "include" / "luna_b200.h"
+
+
+def declared_functions():
+    txt = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(luna_b200_\w+)\s*\(", txt)))
+
+
+def test_library_present_and_loads():
+    assert os.path.exists(_lib.LIB_PATH), "build with luna.jl_b200/build.py"
+    lib = _lib.load()
+    assert lib.luna_b200_version() >= 1
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 12
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    missing = [n for n in names if n not in exported]
+    assert not missing, missing
+    assert set(names) == set(_lib.EXPORTS)
+
+
+def test_plan_create_without_device_fails_loudly():
+    # On a machine without a GPU the library must refuse, not compute on the host.
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    lib = _lib.load()
+    gd = _lib.GridDesc()
+    h = _lib.c_void_p()
+    rc = lib.luna_b200_plan_create(ctypes.byref(gd), None, 0, 0, ctypes.byref(h))
+    assert rc != _lib.LUNA_OK
+    assert lib.luna_b200_last_error()
+
+
+C_PROBE = r"""
+#include <stdio.h>
+#include <stddef.h>
+#include "luna_b200.h"
+#define P(T, f) printf(#T "." #f " %zu\n", offsetof(T, f))
+int main(void) {
+    printf("luna_grid_desc %zu\nluna_resp_desc %zu\nluna_solve_opts %zu\nluna_solve_stats %zu\n",
+           sizeof(luna_grid_desc), sizeof(luna_resp_desc), sizeof(luna_solve_opts), sizeof(luna_solve_stats));
+    P(luna_grid_desc, in_scale); P(luna_resp_desc, spl_n); P(luna_resp_desc, adk_thr);
+    P(luna_resp_desc, hdt); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
+    P(luna_solve_stats, z); P(luna_solve_stats, dz);
+    return 0;
+}
+"""
+
+
+def test_struct_layout_matches_ctypes(tmp_path):
+    src = tmp_path / "probe.c"
+    src.write_text(C_PROBE)
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c99", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                        check=True).stdout.splitlines())
+    assert int(out["luna_grid_desc"]) == ctypes.sizeof(_lib.GridDesc)
+    assert int(out["luna_resp_desc"]) == ctypes.sizeof(_lib.RespDesc)
+    assert int(out["luna_solve_opts"]) == ctypes.sizeof(_lib.SolveOpts)
+    assert int(out["luna_solve_stats"]) == ctypes.sizeof(_lib.SolveStats)
+    assert int(out["luna_grid_desc.in_scale"]) == _lib.GridDesc.in_scale.offset
+    assert int(out["luna_resp_desc.spl_n"]) == _lib.RespDesc.spl_n.offset
+    assert int(out["luna_resp_desc.adk_thr"]) == _lib.RespDesc.adk_thr.offset
+    assert int(out["luna_resp_desc.hdt"]) == _lib.RespDesc.hdt.offset
+    assert int(out["luna_solve_opts.zsave"]) == _lib.SolveOpts.zsave.offset
+    assert int(out["luna_solve_opts.steplog_cap"]) == _lib.SolveOpts.steplog_cap.offset
+    assert int(out["luna_solve_stats.z"]) == _lib.SolveStats.z.offset
+    assert int(out["luna_solve_stats.dz"]) == _lib.SolveStats.dz.offset

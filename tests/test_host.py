@@ -1,0 +1,111 @@
+"""Host-side logic: grid sizes of the benchmark configurations, plan descriptors, the
+scan generator, and the multi-rank split of a scan (gloo, world size 2, CPU only)."""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from luna_b200 import scan
+from luna_b200.grid import EnvGrid, RealGrid
+from luna_b200.interface import prop_capillary_args, prop_gnlse_args
+
+
+def test_capillary_readme_grid_sizes():
+    # prop_capillary(125e-6, 3, :He, 1; λ0=800e-9, λlims=(150e-9, 4e-6), trange=1e-12)
+    g = RealGrid(3.0, 800e-9, (150e-9, 4e-6), 1e-12)
+    assert (g.N, len(g.ω), g.No, len(g.ωo)) == (8192, 4097, 16384, 8193)
+    assert abs(g.to[1] - g.to[0] - 8.339e-17) < 1e-19
+
+
+def test_gnlse_grid_sizes():
+    g = EnvGrid(0.15, 835e-9, (500e-9, 2400e-9), 12.5e-12)
+    assert g.N == g.No == 8192
+    g = EnvGrid(1.0, 835e-9, (450e-9, 8000e-9), 13e-12)
+    assert g.N == 16384
+
+
+def test_linop_zero_outside_sidx_and_loss_clamped():
+    p = prop_capillary_args(125e-6, 3.0, "He", 1.0, λ0=800e-9, τfwhm=10e-15, energy=120e-6,
+                            λlims=(150e-9, 4e-6), trange=1e-12)
+    g = p.grid
+    assert np.all(p.linop[~g.sidx] == 0)
+    assert np.all(-2 * p.linop.real <= 3000 + 1e-9)
+    # the output factor is 1 outside sidx (raw transform output, NonlinearRHS.jl:368-372)
+    f = p.transform.output_factor()
+    assert np.all(f[~g.sidx] == 1)
+
+
+def test_gnlse_input_peak_power():
+    p = prop_gnlse_args(0.11, 0.15, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9, τfwhm=50e-15,
+                        power=10e3, pulseshape="sech", λlims=(500e-9, 2400e-9), trange=12.5e-12)
+    Et = np.fft.ifft(p.Eω)
+    assert abs(np.max(np.abs(Et) ** 2) / 10e3 - 1) < 1e-12
+
+
+def test_scan_draw_is_seeded_and_in_range():
+    a = scan.draw_instances(256)
+    b = scan.draw_instances(256)
+    assert a == b
+    for p in a:
+        assert 50e-6 <= p["energy"] <= 400e-6 and 0.5 <= p["pressure"] <= 5
+        assert p["gas"] in scan.GASES and p["radius"] in scan.RADII
+        assert 8e-15 <= p["τfwhm"] <= 30e-15 and 1 <= p["flength"] <= 3
+        assert 0.5e-12 <= p["trange"] <= 2e-12
+
+
+def test_partition_covers_every_instance_once():
+    costs = np.random.default_rng(3).uniform(1, 10, 257)
+    for n in (1, 2, 3, 8):
+        parts = scan.partition(costs, n)
+        allidx = sorted(i for p in parts for i in p)
+        assert allidx == list(range(len(costs)))
+        loads = [costs[p].sum() for p in parts]
+        assert max(loads) - min(loads) <= costs.max() + 1e-9
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _rank_main(rank, world, port, costs, q):
+    import torch
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mine = scan.shard(costs, rank, world)
+    t = torch.zeros(len(costs), dtype=torch.int64)
+    t[mine] = 1
+    gathered = [torch.zeros_like(t) for _ in range(world)]
+    dist.all_gather(gathered, t)
+    if rank == 0:
+        q.put([g.tolist() for g in gathered])
+    dist.destroy_process_group()
+
+
+def test_multi_rank_scan_split_gloo():
+    torch = pytest.importorskip("torch")
+    import torch.multiprocessing as mp
+    costs = np.random.default_rng(5).uniform(1, 10, 64).tolist()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, costs, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    masks = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    m = np.array(masks)
+    assert np.all(m.sum(axis=0) == 1)  # every instance on exactly one rank
+    assert m[0].sum() > 0 and m[1].sum() > 0

@@ -1,0 +1,219 @@
+"""Pin the CPU oracle (and the host set-up it consumes) to the reference's own known answers.
+
+Each test cites the reference test it restates. These run without a GPU.
+"""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import math
+
+import numpy as np
+import pytest
+
+from luna_b200 import ionisation as I
+from luna_b200 import maths, physdata as pd, raman
+from luna_b200.grid import EnvGrid, RealGrid
+from luna_b200.interface import prop_gnlse_args
+from oracle import uppe
+
+SQRT_EPS = math.sqrt(np.finfo(float).eps)
+
+
+def isapprox(a, b, rtol):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.linalg.norm(a - b) <= rtol * max(np.linalg.norm(a), np.linalg.norm(b))
+
+
+# ---------------------------------------------------------------- test_ionisation.jl:6-47
+@pytest.mark.parametrize("gas,E,ref", [
+    ("He", 1e10, 1.2416371415312408e-18),
+    ("He", 2e10, 1.0772390893742478),
+    ("Ar", 7e9, 2.4422306306649472e-08),
+    ("Ar", 8e9, 4.494711488416766e-05),
+])
+def test_adk_known_answers(gas, E, ref):
+    r = I.ionrate_ADK(gas, np.array([E]))[0]
+    assert isapprox(r, ref, SQRT_EPS)
+
+
+def test_adk_even_in_field():
+    E = np.linspace(1e9, 1e11, 32)
+    assert np.array_equal(I.ionrate_ADK("He", E), I.ionrate_ADK("He", -E))
+
+
+@pytest.mark.parametrize("E,ref", [(1e10, 2 * 1.40432138471583e-5), (1.3e10, 2 * 0.04517809797503506)])
+def test_ppt_known_answers(E, ref):
+    r = I.ionrate_PPT_gas("He", 800e-9, np.array([E]), dipole_corr=False)[0]
+    assert isapprox(r, ref, 1e-3)
+
+
+def test_cspline_uniform_index_matches_search():
+    # test_ionisation.jl:18-34: an arithmetic index function and the brute-force
+    # first-larger search give the same indices and the same spline values
+    Emin, Emax, N = 1e9, 1e11, 2 ** 9
+    E = np.linspace(Emin, Emax, N)
+    rate = I.ionrate_PPT_gas("He", 800e-9, E)
+    D = maths.cspline_slopes(rate)
+
+    def ifun(x0):
+        return 2 if x0 <= Emin else (N if x0 >= Emax else int(math.ceil((x0 - Emin) / (Emax - Emin) * N)) + 1)
+
+    def ifun2(x0):
+        return 2 if x0 <= E[0] else (len(E) if x0 >= E[-1] else int(np.argmax(E > x0)) + 1)
+
+    def ev(i1, x0):
+        i = i1 - 1
+        if x0 == E[i]:
+            return rate[i]
+        if x0 == E[i - 1]:
+            return rate[i - 1]
+        t = (x0 - E[i - 1]) / (E[i] - E[i - 1])
+        return (rate[i - 1] + D[i - 1] * t + (3 * (rate[i] - rate[i - 1]) - 2 * D[i - 1] - D[i]) * t ** 2
+                + (2 * (rate[i - 1] - rate[i]) + D[i - 1] + D[i]) * t ** 3)
+
+    for x0 in E:
+        assert ifun(x0) == ifun2(x0)
+        assert ev(ifun(x0), x0) == ev(ifun2(x0), x0)
+        # the library's own index function (Maths.jl:772-774) evaluates to the same value
+        assert maths.cspline_eval(E, rate, D, x0) == ev(ifun2(x0), x0)
+    mid = 0.5 * (E[:-1] + E[1:])
+    for x0 in mid:
+        assert maths.cspline_eval(E, rate, D, x0) == ev(ifun2(x0), x0)
+
+
+def test_ppt_spline_table_vs_direct():
+    E = np.linspace(1e9, 1e11, 2 ** 9)
+    direct = I.ionrate_PPT_gas("He", 800e-9, E)
+    spl = I.ionrate_PPTaccel("He", 800e-9)
+    acc = uppe.ppt_rate(spl, E)
+    assert np.all(np.isclose(acc, direct, rtol=1e-2, atol=0))
+    assert np.array_equal(acc, uppe.ppt_rate(spl, -E))
+
+
+def test_ppt_above_table_raises():
+    spl = I.ionrate_PPTaccel("He", 800e-9)
+    with pytest.raises(ValueError):
+        uppe.ppt_rate(spl, np.array([spl.Emax * 1.01]))
+
+
+# ---------------------------------------------------------------- test_kerr.jl:5-30
+def test_kerr_field_vs_envelope_low_frequencies():
+    n = 2 ** 16
+    t = (np.arange(n) - n / 2) * 3.430944979182369e-16 / 4
+    E = np.exp(-0.5 * (t / 10e-15) ** 2) * np.cos(2 * np.pi * pd.c / 800e-9 * t)
+    outf = np.zeros_like(E)
+    uppe.kerr_field(outf, E, 1.0, 1.0 / pd.eps_0)
+    xf = np.fft.fft(E)
+    xf[1:n // 2] *= 2
+    xf[n // 2:] = 0
+    Eenv = np.fft.ifft(xf)
+    oute = np.zeros_like(Eenv)
+    uppe.kerr_env(oute, Eenv, 1.0, 1.0 / pd.eps_0)
+    a = np.abs(np.fft.rfft(outf))[1799:2400]
+    b = np.abs(np.fft.rfft(oute.real))[1799:2400]
+    assert isapprox(b, a, 1e-15)
+
+
+# ---------------------------------------------------------------- test_raman.jl:9-70
+def _raman_peak(grid, resp, rho, env):
+    h = np.zeros(2 * len(grid.to))
+    h[:len(grid.to)] = resp.h(rho)
+    hw = np.fft.fft(h) if env else np.fft.rfft(h)
+    n = len(grid.to)
+    wR = 2 * np.pi * np.arange(n) / ((grid.to[1] - grid.to[0]) * n * 2)
+    return wR[np.argmin(hw.imag[:n])]
+
+
+def test_raman_response_causal_and_normalised():
+    grid = RealGrid(1.0, 800e-9, (200e-9, 2000e-9), 40e-12)
+    rho = pd.density("N2", 5.0)
+    h = raman.raman_response(grid.to, "N2")
+    T = np.linspace(-5e-12, 20e-12, 2 ** 16)
+    for R in h.Rs:
+        assert R(0.0, rho) == 0.0
+        assert np.all(R(T[T <= 0], rho) == 0.0)
+    hsdo = raman.RamanRespNormedSingleDampedOscillator(1.0, 2 * np.pi * 100e12, 100e-15)
+    x = np.linspace(-1e-12, 2e-12, 2 ** 21 + 1)
+    from scipy.integrate import simpson
+    assert abs(simpson(hsdo(x, 1.0), x=x) - 1.0) < 1e-8
+
+
+@pytest.mark.parametrize("env", [False, True])
+def test_raman_n2_vibrational_peak(env):
+    G = EnvGrid if env else RealGrid
+    grid = G(1.0, 800e-9, (200e-9, 2000e-9), 40e-12)
+    rho = pd.density("N2", 5.0)
+    hv = raman.raman_response(grid.to, "N2", rotation=False)
+    wpk = _raman_peak(grid, hv, rho, env)
+    assert abs(wpk / pd.raman_parameters("N2")["Omega_v"] - 1) < 1e-4
+
+
+def test_raman_h2_vibrational_and_rotational_peaks():
+    grid = EnvGrid(1.0, 800e-9, (200e-9, 2000e-9), 40e-12)
+    rho = pd.density("H2", 5.0)
+    hv = raman.raman_response(grid.to, "H2", rotation=False)
+    assert abs(_raman_peak(grid, hv, rho, True) / pd.raman_parameters("H2")["Omega_v"] - 1) < 1e-4
+    hr = raman.raman_response(grid.to, "H2", vibration=False)
+    assert abs(_raman_peak(grid, hr, rho, True) / (2 * np.pi * 17.45e12) - 1) < 1e-4
+
+
+# ---------------------------------------------------------------- Maths.cumtrapz!
+def test_cumtrapz_is_the_sequential_recurrence():
+    rng = np.random.default_rng(0)
+    y = rng.standard_normal(1000)
+    out = np.zeros_like(y)
+    for i in range(1, len(y)):
+        out[i] = out[i - 1] + 0.5 * (y[i - 1] + y[i]) * 0.3
+    assert np.array_equal(uppe.cumtrapz(y, 0.3), out)
+
+
+# ---------------------------------------------------------------- test_rk45.jl:5-135
+def _nlse_init():
+    trange, wrange = 32, 160
+    samples = 2 ** int(math.ceil(math.log2(trange * wrange / (2 * np.pi))))
+    dt = trange / samples
+    dw = 2 * np.pi / trange
+    n = np.arange(samples)
+    t = (n - samples / 2) * dt
+    w = (n - samples / 2) * dw
+    At = 5 / np.cosh(t)
+    Aw = np.fft.fftshift(np.fft.fft(At))
+    Lin = -1j / 2 * w ** 2
+
+    def fnl(Aw, z):
+        a = np.fft.ifft(Aw)
+        return 1j * np.fft.fft(np.abs(a) ** 2 * a)
+
+    return Aw, Lin, fnl
+
+
+def test_rk45_precon_nlse_soliton_recovers():
+    Aw, Lin, fnl = _nlse_init()
+    zmax = np.pi / 2 * 2
+    s = uppe.PreconStepper(fnl, Lin, Aw, 0.0, 1e-3, rtol=1e-8)
+    while s.tn <= zmax:
+        s.step()
+    # the reference compares the dense output at zmax
+    out = s.interpolate(zmax)
+    assert isapprox(np.abs(Aw) ** 2, np.abs(out) ** 2, 1e-3)
+
+
+# ---------------------------------------------------------------- test_gnlse.jl:33-56
+@pytest.mark.slow
+def test_soliton_shift_golden_values():
+    """Soliton self-frequency shift: peak frequency and time checked against two
+    independent GNLSE codes by the reference (rtol 1e-14)."""
+    γ, β2, fr, τ0 = 0.1, -1e-26, 0.18, 10e-15
+    P0 = abs(β2) / ((1 - fr) * γ * τ0 ** 2)
+    flength = np.pi / 2 * τ0 ** 2 / abs(β2) * 90
+    p = prop_gnlse_args(γ, flength, [0.0, 0.0, β2], λ0=835e-9, τfwhm=1.763 * τ0, power=P0,
+                        pulseshape="sech", λlims=[450e-9, 8000e-9], trange=13e-12, raman=True,
+                        shock=False, fr=fr)
+    res = uppe.run(p.transform, p.grid, p.linop, p.Eω)
+    Ew = res.Eω[-1]
+    wpk = p.grid.ω[np.argmax(np.abs(Ew) ** 2)]
+    assert abs(wpk / 1.3975031072069625e15 - 1) <= 1e-14
+    Et = np.fft.ifft(Ew) * np.exp(1j * p.grid.ω0 * p.grid.t)
+    tpk = p.grid.t[np.argmax(np.abs(Et) ** 2)]
+    assert abs(tpk / 6.079566076444579e-12 - 1) <= 1e-14

@@ -135,7 +135,11 @@ int luna_b200_solve(luna_plan* plan, const double* linop, double* y_inout, doubl
  * the device-only part can be timed. */
 int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts* opts, luna_batch** out);
 int luna_b200_batch_upload(luna_batch* b, const double* const* linops, const double* const* y0,
-                           const double* z0, const double* dz0, const double* zmax);
+                           const double* z0, const double* dz0, const double* zmax,
+                           const double* const* zsave, const double* max_dt);
+/* zsave (optional, NULL): per-instance [saveN] GridCondition points, e.g. range(0, zmax_i,
+ * saveN) as Luna.run uses for each instance; max_dt (optional, NULL): per-instance step
+ * limits (Luna.run's max_dz = zmax/2). NULL falls back to the batch-wide options. */
 int luna_b200_batch_run(luna_batch* b, float* device_ms);
 int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
                              luna_solve_stats* stats);

@@ -95,7 +95,8 @@ def load():
                                     POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
     lib.luna_b200_batch_create.argtypes = [POINTER(c_void_p), c_int, POINTER(SolveOpts),
                                            POINTER(c_void_p)]
-    lib.luna_b200_batch_upload.argtypes = [c_void_p, POINTER(PD), POINTER(PD), PD, PD, PD]
+    lib.luna_b200_batch_upload.argtypes = [c_void_p, POINTER(PD), POINTER(PD), PD, PD, PD,
+                                           POINTER(PD), PD]
     lib.luna_b200_batch_run.argtypes = [c_void_p, POINTER(c_float)]
     lib.luna_b200_batch_download.argtypes = [c_void_p, POINTER(PD), POINTER(PD), POINTER(SolveStats)]
     lib.luna_b200_batch_steplog.argtypes = [c_void_p, c_int, PD]

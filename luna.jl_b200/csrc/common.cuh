@@ -4,8 +4,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#ifndef LUNA_BLOCK
 #define LUNA_BLOCK 512
+#endif
+#ifndef LUNA_WARPS
 #define LUNA_WARPS (LUNA_BLOCK / 32)
+#endif
 
 namespace luna {
 

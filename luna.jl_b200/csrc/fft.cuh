@@ -1,16 +1,20 @@
-// Block-wide Stockham FFT for one CTA of LUNA_BLOCK threads.
+// Block-wide FFT for one CTA of LUNA_BLOCK threads, in place in shared or global memory.
 //
-// Two forms:
-//  * in-place: every active thread holds E = M/nact elements in registers, so each
-//    radix-R pass reads all of its inputs, synchronises, and writes its outputs back
-//    to the same (swizzled) buffer. Used whenever E <= EMAX (16 for FP64, 32 for FP32);
-//    this is the shared-memory path.
-//  * out-of-place: ping-pongs between two swizzled buffers (used for transforms too
-//    large to hold in registers, which then live in L2-resident global scratch).
+// A length-M transform is split as M = P * Mb with Mb <= EMAX * LUNA_BLOCK (EMAX = 8
+// complex values per thread for FP64, 16 for FP32, the most a thread can hold in
+// registers across a barrier without spilling). The P sub-transforms of length Mb are
+// Stockham passes done in place: every thread loads its E = Mb/LUNA_BLOCK inputs,
+// synchronises, computes its radix-R butterflies and writes the outputs back.
+// One radix-P pass joins the sub-transforms:
+//   * inverse transforms run decimation-in-frequency: natural-order input, radix-P pass,
+//     sub-transforms; the result is in the "split" order  X[P*k + p] at p*Mb + k;
+//   * forward transforms run decimation-in-time: split-order input (element n at
+//     (n mod P)*Mb + n/P), sub-transforms, radix-P pass; the result is in natural order.
+// An inverse transform followed by pointwise work in place and a forward transform thus
+// never needs a reordering pass. For P == 1 both orders are the natural order.
 //
-// Pass p with radix R and span L (product of the earlier radices) maps butterfly j,
-// k = j mod L, inputs x[j + r*M/R] -> twiddle exp(-+2*pi*i*r*k/(L*R)) -> R-point DFT ->
-// outputs y[(j-k)*R + k + r*L]; after the last pass the data is in natural order.
+// Stockham pass with radix R and span L: butterfly j, k = j mod L, inputs x[j + r*Mb/R],
+// twiddle exp(-+2*pi*i*r*k/(L*R)), R-point DFT, outputs y[(j-k)*R + k + r*L].
 #pragma once
 #include "common.cuh"
 
@@ -36,13 +40,14 @@ template <typename R, bool INV, int Q>
 __device__ __forceinline__ cpx<R> rot32(cpx<R> b) {
     if (Q == 0) return b;
     if (Q == 8) return mul_mi<R, INV>(b);
-    // cos/sin of 2*pi*Q/32 = pi*Q/16
     const R c = (R)(Q <= 8 ? cos16(Q) : -cos16(16 - Q));
     const R s = (R)(Q <= 8 ? cos16(8 - Q) : cos16(Q - 8));
     // forward: b * (c - i s); inverse: b * (c + i s)
     return INV ? mk<R>(b.x * c - b.y * s, b.x * s + b.y * c)
                : mk<R>(b.x * c + b.y * s, b.y * c - b.x * s);
 }
+
+template <int N> __host__ __device__ constexpr int ilog2c() { return N <= 1 ? 0 : 1 + ilog2c<N / 2>(); }
 
 template <int RAD>
 __host__ __device__ constexpr int bitrev(int i) {
@@ -81,37 +86,61 @@ __device__ __forceinline__ void bfly_stages(cpx<R>* v) {
     }
 }
 
-// in-register RAD-point DFT, natural order in and out (radix-2 DIT network)
+// In-register RAD-point DFT (radix-2 decimation-in-time network): the inputs must sit in
+// bit-reversed order (v[i] = x[bitrev(i)]); the outputs come out in natural order.
 template <typename R, bool INV, int RAD>
-__device__ __forceinline__ void dft(cpx<R>* u) {
-    cpx<R> v[RAD];
-#pragma unroll
-    for (int i = 0; i < RAD; ++i) v[i] = u[bitrev<RAD>(i)];
+__device__ __forceinline__ void dft_br(cpx<R>* v) {
     bfly_stages<R, INV, RAD, 1>(v);
-#pragma unroll
-    for (int i = 0; i < RAD; ++i) u[i] = v[i];
 }
 
 template <typename R>
-struct FftEmax { static constexpr int v = (sizeof(R) == 8) ? 16 : 32; };
+struct FftEmax { static constexpr int v = (sizeof(R) == 8) ? 8 : 16; };
 
-template <int N> __host__ __device__ constexpr int ilog2c() { return N <= 1 ? 0 : 1 + ilog2c<N / 2>(); }
+// largest transform held by one CTA: P <= 8 sub-transforms of EMAX*LUNA_BLOCK
+template <typename R>
+struct FftMmax { static constexpr int v = 8 * FftEmax<R>::v * LUNA_BLOCK; };
 
 __device__ __forceinline__ int ilog2i(unsigned x) { return 31 - __clz(x); }
 
-// One in-place pass: nact active threads, each with E/RAD butterflies.
+// Multiply v[i] (bit-reversed slot i holds input r = bitrev(i)) by w^r for r = 1..RAD-1.
+// w comes from one table lookup; w^r is a product of the binary powers w, w^2, w^4, ...
+template <typename R, int RAD>
+__device__ __forceinline__ void apply_twiddles(cpx<R>* v, cpx<R> w) {
+    constexpr int NB = ilog2c<RAD>();
+    cpx<R> wb[NB > 0 ? NB : 1];
+    wb[0] = w;
+#pragma unroll
+    for (int b = 1; b < NB; ++b) wb[b] = wb[b - 1] * wb[b - 1];
+#pragma unroll
+    for (int i = 1; i < RAD; ++i) {
+        const int r = bitrev<RAD>(i);
+        cpx<R> f;
+        bool have = false;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            if (r & (1 << b)) {
+                f = have ? f * wb[b] : wb[b];
+                have = true;
+            }
+        }
+        v[i] = v[i] * f;
+    }
+}
+
+// One in-place Stockham pass over a sub-transform of length Mb at `buf`; nact threads
+// are active, each with E/RAD butterflies.
 template <typename R, bool INV, int E, int RAD>
-__device__ __forceinline__ void pass_inplace(cpx<R>* buf, int M, int L, int nact, const TwTab<R>& tw) {
+__device__ __forceinline__ void pass_inplace(cpx<R>* buf, int Mb, int L, int nact, const TwTab<R>& tw) {
     const int t = threadIdx.x;
     constexpr int NB = E / RAD;
     cpx<R> v[E];
-    const int stride = M / RAD;
+    const int stride = Mb / RAD;
     if (t < nact) {
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             const int j = t + b * nact;
 #pragma unroll
-            for (int r = 0; r < RAD; ++r) v[b * RAD + r] = buf[Swz<R>::f(j + r * stride)];
+            for (int i = 0; i < RAD; ++i) v[b * RAD + i] = buf[Swz<R>::f(j + bitrev<RAD>(i) * stride)];
         }
     }
     __syncthreads();
@@ -121,12 +150,8 @@ __device__ __forceinline__ void pass_inplace(cpx<R>* buf, int M, int L, int nact
         for (int b = 0; b < NB; ++b) {
             const int j = t + b * nact;
             const int k = j & (L - 1);
-            if (L > 1) {
-#pragma unroll
-                for (int r = 1; r < RAD; ++r)
-                    v[b * RAD + r] = v[b * RAD + r] * twiddle<R, INV>(tw, (unsigned)(r * k) << shift);
-            }
-            dft<R, INV, RAD>(&v[b * RAD]);
+            if (L > 1) apply_twiddles<R, RAD>(&v[b * RAD], twiddle<R, INV>(tw, (unsigned)k << shift));
+            dft_br<R, INV, RAD>(&v[b * RAD]);
             const int base = (j - k) * RAD + k;
 #pragma unroll
             for (int r = 0; r < RAD; ++r) buf[Swz<R>::f(base + r * L)] = v[b * RAD + r];
@@ -135,84 +160,105 @@ __device__ __forceinline__ void pass_inplace(cpx<R>* buf, int M, int L, int nact
     __syncthreads();
 }
 
+// In-place Stockham transform of one sub-block of length Mb = E * nact: a twiddle-free
+// first pass of the remainder radix, then passes of radix E.
 template <typename R, bool INV, int E>
-__device__ void fft_inplace(cpx<R>* buf, int M, const TwTab<R>& tw) {
-    const int nact = M / E;
+__device__ __forceinline__ void sub_fft(cpx<R>* buf, int Mb, const TwTab<R>& tw) {
+    constexpr int LR = ilog2c<E>();
+    const int nact = Mb / E;
+    const int rem = ilog2i((unsigned)Mb) % LR;
     int L = 1;
-    while (L < M) {
-        const int rad = min(E, M / L);
-        if constexpr (E >= 2) if (rad == 2) pass_inplace<R, INV, E, 2>(buf, M, L, nact, tw);
-        if constexpr (E >= 4) if (rad == 4) pass_inplace<R, INV, E, 4>(buf, M, L, nact, tw);
-        if constexpr (E >= 8) if (rad == 8) pass_inplace<R, INV, E, 8>(buf, M, L, nact, tw);
-        if constexpr (E >= 16) if (rad == 16) pass_inplace<R, INV, E, 16>(buf, M, L, nact, tw);
-        if constexpr (E >= 32) if (rad == 32) pass_inplace<R, INV, E, 32>(buf, M, L, nact, tw);
-        L *= rad;
+    if (rem != 0) {
+        const int r0 = 1 << rem;
+        if constexpr (E > 2) { if (r0 == 2) pass_inplace<R, INV, E, 2>(buf, Mb, 1, nact, tw); }
+        if constexpr (E > 4) { if (r0 == 4) pass_inplace<R, INV, E, 4>(buf, Mb, 1, nact, tw); }
+        if constexpr (E > 8) { if (r0 == 8) pass_inplace<R, INV, E, 8>(buf, Mb, 1, nact, tw); }
+        L = r0;
+    }
+    while (L < Mb) {
+        pass_inplace<R, INV, E, E>(buf, Mb, L, nact, tw);
+        L *= E;
     }
 }
 
-template <typename R, bool INV, int RAD>
-__device__ __forceinline__ void pass_oop(const cpx<R>* src, cpx<R>* dst, int M, int L, const TwTab<R>& tw) {
-    const int stride = M / RAD;
-    const int shift = TW_LOG_MMAX - ilog2i((unsigned)(L * RAD));
-    for (int j = threadIdx.x; j < stride; j += LUNA_BLOCK) {
-        cpx<R> v[RAD];
+// Radix-P pass joining the sub-transforms, in place (each thread owns the P elements
+// k + q*Mb). DIT (forward): X[k + q*Mb] = sum_p W_P^{pq} * (W_M^{pk} * A_p[k]).
+// DIF (inverse):           b_p[k] = W_M^{-pk} * sum_q W_P^{-pq} * x[k + q*Mb].
+template <typename R, bool INV, int P>
+__device__ __forceinline__ void join_pass(cpx<R>* buf, int M, const TwTab<R>& tw) {
+    const int Mb = M / P;
+    const int shift = TW_LOG_MMAX - ilog2i((unsigned)M);
+    __syncthreads();
+    for (int k = threadIdx.x; k < Mb; k += LUNA_BLOCK) {
+        cpx<R> v[P];
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) v[r] = src[Swz<R>::f(j + r * stride)];
-        const int k = j & (L - 1);
-        if (L > 1) {
+        for (int i = 0; i < P; ++i) v[i] = buf[Swz<R>::f(k + bitrev<P>(i) * Mb)];
+        if (!INV) {
+            apply_twiddles<R, P>(v, twiddle<R, INV>(tw, (unsigned)k << shift));
+            dft_br<R, INV, P>(v);
+        } else {
+            dft_br<R, INV, P>(v);
+            // v[p] = sum_q W_P^{-pq} x_q; apply W_M^{-pk}
+            const cpx<R> w = twiddle<R, INV>(tw, (unsigned)k << shift);
+            cpx<R> f = w;
 #pragma unroll
-            for (int r = 1; r < RAD; ++r) v[r] = v[r] * twiddle<R, INV>(tw, (unsigned)(r * k) << shift);
+            for (int p = 1; p < P; ++p) {
+                v[p] = v[p] * f;
+                f = f * w;
+            }
         }
-        dft<R, INV, RAD>(v);
-        const int base = (j - k) * RAD + k;
 #pragma unroll
-        for (int r = 0; r < RAD; ++r) dst[Swz<R>::f(base + r * L)] = v[r];
+        for (int q = 0; q < P; ++q) buf[Swz<R>::f(k + q * Mb)] = v[q];
     }
     __syncthreads();
 }
 
-// returns the buffer holding the result (a or b)
 template <typename R, bool INV>
-__device__ cpx<R>* fft_oop(cpx<R>* a, cpx<R>* b, int M, const TwTab<R>& tw) {
-    int L = 1;
-    cpx<R>* src = a;
-    cpx<R>* dst = b;
-    while (L < M) {
-        const int rad = min(16, M / L);
-        if (rad == 2) pass_oop<R, INV, 2>(src, dst, M, L, tw);
-        else if (rad == 4) pass_oop<R, INV, 4>(src, dst, M, L, tw);
-        else if (rad == 8) pass_oop<R, INV, 8>(src, dst, M, L, tw);
-        else pass_oop<R, INV, 16>(src, dst, M, L, tw);
-        cpx<R>* tmp = src;
-        src = dst;
-        dst = tmp;
-        L *= rad;
-    }
-    return src;
-}
-
-// Whether a length-M transform runs in place (registers) for this block size.
-template <typename R>
-__device__ __forceinline__ bool fft_is_inplace(int M) {
-    int E = M / LUNA_BLOCK;
-    return E <= FftEmax<R>::v;
-}
-
-// Unnormalised DFT (forward, exp(-...)) or inverse (exp(+...)) of length M (power of two,
-// 2 <= M <= TW_MMAX). Returns the buffer that holds the result: `buf` for in-place
-// transforms, otherwise `buf` or `alt`.
-template <typename R, bool INV>
-__device__ cpx<R>* block_fft(cpx<R>* buf, cpx<R>* alt, int M, const TwTab<R>& tw) {
-    int E = M / LUNA_BLOCK;
+__device__ __forceinline__ void sub_ffts(cpx<R>* buf, int M, int P, const TwTab<R>& tw) {
+    const int Mb = M / P;
+    int E = Mb / LUNA_BLOCK;
     if (E < 2) E = 2;
-    if (E == 2) { fft_inplace<R, INV, 2>(buf, M, tw); return buf; }
-    if (E == 4) { fft_inplace<R, INV, 4>(buf, M, tw); return buf; }
-    if (E == 8) { fft_inplace<R, INV, 8>(buf, M, tw); return buf; }
-    if (E == 16) { fft_inplace<R, INV, 16>(buf, M, tw); return buf; }
-    if constexpr (FftEmax<R>::v >= 32) {
-        if (E == 32) { fft_inplace<R, INV, 32>(buf, M, tw); return buf; }
+    for (int p = 0; p < P; ++p) {
+        cpx<R>* b = buf + (size_t)p * Mb;
+        if (E == 2) sub_fft<R, INV, 2>(b, Mb, tw);
+        else if (E == 4) sub_fft<R, INV, 4>(b, Mb, tw);
+        else if (E == 8) sub_fft<R, INV, 8>(b, Mb, tw);
+        else if constexpr (FftEmax<R>::v >= 16) sub_fft<R, INV, 16>(b, Mb, tw);
     }
-    return fft_oop<R, INV>(buf, alt, M, tw);
+}
+
+// number of sub-transforms for a length-M transform
+template <typename R>
+__host__ __device__ __forceinline__ int fft_nsplit(int M) {
+    int P = 1;
+    while (M / P > FftEmax<R>::v * LUNA_BLOCK) P *= 2;
+    return P;
+}
+
+// Position of element n of a split-order array of length M with P sub-transforms.
+__device__ __forceinline__ int split_pos(int n, int M, int P) {
+    return (n & (P - 1)) * (M / P) + n / P;
+}
+
+// Unnormalised DFT of length M (power of two, 2 <= M <= FftMmax), in place.
+//   forward (INV=false): split-order input -> natural-order output
+//   inverse (INV=true):  natural-order input -> split-order output
+// The caller synchronises before the call (the input is written by other threads); the
+// call ends with a barrier.
+template <typename R, bool INV>
+__device__ __noinline__ void block_fft(cpx<R>* buf, int M, const TwTab<R>& tw) {
+    const int P = fft_nsplit<R>(M);
+    if (INV) {
+        if (P == 2) join_pass<R, INV, 2>(buf, M, tw);
+        else if (P == 4) join_pass<R, INV, 4>(buf, M, tw);
+        else if (P == 8) join_pass<R, INV, 8>(buf, M, tw);
+        sub_ffts<R, INV>(buf, M, P, tw);
+    } else {
+        sub_ffts<R, INV>(buf, M, P, tw);
+        if (P == 2) join_pass<R, INV, 2>(buf, M, tw);
+        else if (P == 4) join_pass<R, INV, 4>(buf, M, tw);
+        else if (P == 8) join_pass<R, INV, 8>(buf, M, tw);
+    }
 }
 
 }  // namespace luna

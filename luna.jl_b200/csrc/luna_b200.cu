@@ -62,9 +62,9 @@ rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int sme
 // are ~1e-48 in SI units); the plan folds max|hpre| * hdt / (2*No) into the FP64 coefficient.
 template <typename Rl>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
-raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<double>* alt, cpx<Rl>* H,
-               TwTab<double> tw) {
+raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<Rl>* H, TwTab<double> tw) {
     const int tid = threadIdx.x;
+    const int P = fft_nsplit<double>(No);
     for (int m = tid; m < No; m += LUNA_BLOCK) {
         double a = 0, b = 0;
         if (m < No / 2) {
@@ -77,10 +77,11 @@ raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<double>*
                 else b = h;
             }
         }
-        buf[Swz<double>::f(m)] = mk<double>(a, b);
+        buf[Swz<double>::f(split_pos(m, No, P))] = mk<double>(a, b);
     }
     __syncthreads();
-    cpx<double>* Z = block_fft<double, false>(buf, alt, No, tw);
+    block_fft<double, false>(buf, No, tw);
+    cpx<double>* Z = buf;
     const int M = No;
     for (int k = tid; k <= M; k += LUNA_BLOCK) {
         const int kk = k & (M - 1);
@@ -176,12 +177,10 @@ int max_smem_optin() {
 template <typename Rl>
 size_t smem_wanted(const LunaInst& I) {
     const size_t c = sizeof(cpx<Rl>);
-    const int emax = (sizeof(Rl) == 8) ? 16 : 32;
     size_t s = LUNA_SMALL_BYTES;
-    const int Mm = main_len(I);
-    if (Mm / LUNA_BLOCK <= emax) s += align_up((size_t)Mm * c, 256);
+    s += align_up((size_t)main_len(I) * c, 256);
     s += align_up((size_t)I.Nw * c, 256);
-    if (has_raman(I) && I.No / LUNA_BLOCK <= emax) s += align_up((size_t)I.No * c, 256);
+    if (has_raman(I)) s += align_up((size_t)I.No * c, 256);
     return s;
 }
 
@@ -212,6 +211,7 @@ struct luna_batch {
     std::vector<double2*> y0buf;  // per instance y (holds y0 before the run)
     std::vector<double2*> ybuf, ynbuf;
     std::vector<double*> steplogs;
+    std::vector<double*> zsave_own;  // per-instance save points (optional)
     double* d_zsave = nullptr;
     int smem = 0;
     int grid = 0;
@@ -266,6 +266,17 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
         return fail(LUNA_ERR_BAD_ARG, "plan_create: RealGrid needs Nw == N/2 + 1");
     if (g->kind == 1 && g->Nw != g->N) return fail(LUNA_ERR_BAD_ARG, "plan_create: EnvGrid needs Nw == N");
     if (2 * g->No > TW_MMAX) return fail(LUNA_ERR_UNSUPPORTED, "plan_create: No too large");
+    {
+        // every transform must fit one CTA's split transform (8 sub-transforms)
+        const int Mmain = (g->kind == 0) ? g->No / 2 : g->No;
+        const int lim = (precision == LUNA_PREC_FP64) ? FftMmax<double>::v : FftMmax<float>::v;
+        bool raman = false;
+        for (int i = 0; i < nresp; ++i) raman = raman || resps[i].kind == LUNA_RESP_RAMAN;
+        if (Mmain > lim || (raman && g->No > lim) || g->No > FftMmax<double>::v * 2)
+            return fail(LUNA_ERR_UNSUPPORTED, "plan_create: grid too large for one CTA");
+        if (g->No < 2 * LUNA_BLOCK)
+            return fail(LUNA_ERR_UNSUPPORTED, "plan_create: oversampled grid below 1024 samples");
+    }
     if (!g->outfac || !g->wwin || !g->towin || !g->twin) return fail(LUNA_ERR_BAD_ARG, "plan_create: null grid array");
     int dev_count = 0;
     if (cudaGetDeviceCount(&dev_count) != cudaSuccess || dev_count == 0)
@@ -363,19 +374,18 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
                 UP(d.htt, g->No, &r.htt);
                 // spectrum of the response, computed once on the device in FP64
                 cpx<double>* b1 = nullptr;
-                cpx<double>* b2 = nullptr;
-                if (dalloc(p->allocs, &b1, sizeof(cpx<double>) * g->No) || dalloc(p->allocs, &b2, sizeof(cpx<double>) * g->No)) {
+                if (dalloc(p->allocs, &b1, sizeof(cpx<double>) * g->No)) {
                     free_all(p->allocs); delete p; return LUNA_ERR_CUDA;
                 }
                 if (precision == LUNA_PREC_FP64) {
                     cpx<double>* H = nullptr;
                     if (dalloc(p->allocs, &H, sizeof(cpx<double>) * (g->No + 1))) { free_all(p->allocs); delete p; return LUNA_ERR_CUDA; }
-                    raman_h_kernel<double><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, b2, H, tw.d);
+                    raman_h_kernel<double><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, H, tw.d);
                     r.H = H;
                 } else {
                     cpx<float>* H = nullptr;
                     if (dalloc(p->allocs, &H, sizeof(cpx<float>) * (g->No + 1))) { free_all(p->allocs); delete p; return LUNA_ERR_CUDA; }
-                    raman_h_kernel<float><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, b2, H, tw.d);
+                    raman_h_kernel<float><<<1, LUNA_BLOCK>>>(r, g->No, 1.0 / hmax, b1, H, tw.d);
                     r.H = H;
                 }
                 cudaError_t e = cudaDeviceSynchronize();
@@ -469,6 +479,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
     b->ybuf.resize(n);
     b->ynbuf.resize(n);
     b->steplogs.assign(n, nullptr);
+    b->zsave_own.assign(n, nullptr);
     const size_t kel = (prec == LUNA_PREC_FP64) ? sizeof(double2) : sizeof(float2);
     auto bail = [&](int rc) {
         free_all(b->allocs);
@@ -555,11 +566,21 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
 }
 
 int luna_b200_batch_upload(luna_batch* b, const double* const* linops, const double* const* y0, const double* z0,
-                           const double* dz0, const double* zmax) {
+                           const double* dz0, const double* zmax, const double* const* zsave, const double* max_dt) {
     if (!b || !linops || !y0 || !z0 || !dz0 || !zmax) return fail(LUNA_ERR_BAD_ARG, "batch_upload: null argument");
     for (int i = 0; i < b->n; ++i) {
         LunaInst& I = b->h[i];
         const size_t bytes = sizeof(double2) * I.Nw;
+        if (zsave && zsave[i] && b->opts.saveN > 0) {
+            if (!b->zsave_own[i]) {
+                double* zp = nullptr;
+                if (dalloc(b->allocs, &zp, sizeof(double) * b->opts.saveN)) return LUNA_ERR_CUDA;
+                b->zsave_own[i] = zp;
+            }
+            CK(cudaMemcpyAsync(b->zsave_own[i], zsave[i], sizeof(double) * b->opts.saveN, cudaMemcpyHostToDevice, b->stream));
+            I.zsave = b->zsave_own[i];
+        }
+        if (max_dt) I.max_dt = max_dt[i];
         if (!I.linop) {
             double2* L = nullptr;
             if (dalloc(b->allocs, &L, bytes)) return LUNA_ERR_CUDA;
@@ -654,7 +675,7 @@ int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z
     if (rc) return rc;
     const double* L[1] = {linop};
     const double* Y[1] = {y_inout};
-    rc = luna_b200_batch_upload(b, L, Y, &z0, &dz0, &zmax);
+    rc = luna_b200_batch_upload(b, L, Y, &z0, &dz0, &zmax, nullptr, nullptr);
     if (!rc) rc = luna_b200_batch_run(b, nullptr);
     double* S[1] = {saves};
     double* YO[1] = {y_inout};

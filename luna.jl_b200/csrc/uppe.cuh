@@ -23,10 +23,8 @@ namespace luna {
 template <typename Rl>
 struct Ws {
     cpx<Rl>* main;      // transform buffer
-    cpx<Rl>* main_alt;  // second buffer when the transform is out of place (global)
     cpx<Rl>* efac;      // exp(L*dz) of the current stage, Nw entries
     cpx<Rl>* ram;       // Raman convolution buffer (No complex)
-    cpx<Rl>* ram_alt;
     double* red;        // 3 * LUNA_WARPS reduction scratch
     double* tot;        // 3 * LUNA_WARPS scan totals
     double* edge;       // 4 edge values carried between scan chunks
@@ -35,6 +33,7 @@ struct Ws {
 };
 
 struct Ctl {  // controller state shared by the CTA (shared memory)
+    void* k[7];  // stage derivative buffers (FSAL rotates k1 and k7)
     double t, tn, dt, dtn, err, errlast;
     int ok;
     int done;
@@ -59,14 +58,20 @@ __host__ __device__ inline bool has_raman(const LunaInst& I) {
     return false;
 }
 
+__host__ __device__ inline bool has_plasma(const LunaInst& I) {
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) return true;
+    return false;
+}
+
 // Bytes of global scratch an instance needs when nothing lives in shared memory.
 template <typename Rl>
 __host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
     size_t c = sizeof(cpx<Rl>);
     size_t b = 0;
-    b += align_up(2 * (size_t)main_len(I) * c, 256);
+    b += align_up((size_t)main_len(I) * c, 256);
     b += align_up((size_t)I.Nw * c, 256);
-    if (has_raman(I)) b += align_up(2 * (size_t)I.No * c, 256);
+    if (has_raman(I)) b += align_up((size_t)I.No * c, 256);
     return b;
 }
 
@@ -85,15 +90,13 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
     size_t goff = 0;
     const int Mm = main_len(I);
     size_t mb = align_up((size_t)Mm * c, 256);
-    if (fft_is_inplace<Rl>(Mm) && off + mb <= (size_t)smem_bytes) {
+    if (off + mb <= (size_t)smem_bytes) {
         w.main = reinterpret_cast<cpx<Rl>*>(smem + off);
-        w.main_alt = nullptr;
         off += mb;
     } else {
         w.main = reinterpret_cast<cpx<Rl>*>(g + goff);
-        w.main_alt = reinterpret_cast<cpx<Rl>*>(g + goff + mb);
     }
-    goff += 2 * mb;
+    goff += mb;
     size_t eb = align_up((size_t)I.Nw * c, 256);
     if (off + eb <= (size_t)smem_bytes) {
         w.efac = reinterpret_cast<cpx<Rl>*>(smem + off);
@@ -102,17 +105,16 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
         w.efac = reinterpret_cast<cpx<Rl>*>(g + goff);
     }
     goff += eb;
-    w.ram = w.ram_alt = nullptr;
+    w.ram = nullptr;
     if (has_raman(I)) {
         size_t rb = align_up((size_t)I.No * c, 256);
-        if (fft_is_inplace<Rl>(I.No) && off + rb <= (size_t)smem_bytes) {
+        if (off + rb <= (size_t)smem_bytes) {
             w.ram = reinterpret_cast<cpx<Rl>*>(smem + off);
             off += rb;
         } else {
             w.ram = reinterpret_cast<cpx<Rl>*>(g + goff);
-            w.ram_alt = reinterpret_cast<cpx<Rl>*>(g + goff + rb);
         }
-        goff += 2 * rb;
+        goff += rb;
     }
 }
 
@@ -255,12 +257,13 @@ __device__ __forceinline__ cpx<double> half_twiddle(const TwTab<Rl>& tw, int k, 
 }
 
 // Raman convolution on the 2*No grid (Nonlinear.jl:282-333): the input samples s[n]
-// (n < No) are in `ram` as complex pairs (s[2m], s[2m+1]) for m < No/2 and zero above;
-// the result P[n], n < No, is returned in the same pair layout.
+// (n < No) are in `ram` as complex pairs (s[2m], s[2m+1]) for m < No/2 (zero above), in
+// split order; on return `ram` holds P[n], n < No, as pairs in split order.
 template <typename Rl>
-__device__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
+__device__ __forceinline__ void raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
     __syncthreads();
-    cpx<Rl>* Z = block_fft<Rl, false>(w.ram, w.ram_alt, No, w.tw);
+    cpx<Rl>* Z = w.ram;
+    block_fft<Rl, false>(Z, No, w.tw);
     const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(r.H);
     const int M = No;  // complex length of the 2*No real transform
     for (int k = threadIdx.x; k <= M / 2; k += LUNA_BLOCK) {
@@ -293,11 +296,9 @@ __device__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
             Z[Swz<Rl>::f(km)] = cvt<Rl>(Zm2);
         }
     }
-    cpx<Rl>* other = (Z == w.ram) ? w.ram_alt : w.ram;
     __syncthreads();
-    return block_fft<Rl, true>(Z, other, No, w.tw);
+    block_fft<Rl, true>(Z, No, w.tw);
 }
-
 
 // ------------------------------------------------------------------ plasma chunk
 // PlasmaScalar! (Nonlinear.jl:121-133) for the pair of samples (2m, 2m+1) held by this
@@ -351,7 +352,7 @@ __device__ __forceinline__ void plasma_pair(const LunaResp& r, bool act, int m, 
 
 // field-resolved grid (RealGrid): to_time! / to_freq! with rfft semantics
 template <typename Rl, typename LoadF, typename StoreF>
-__device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+__device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
     const int M = I.No / 2;
     const int Nw = I.Nw;
     const int T = LUNA_BLOCK;
@@ -377,32 +378,35 @@ __device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& st
         }
     }
     __syncthreads();
-    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+    block_fft<Rl, true>(buf, M, w.tw);
+    cpx<Rl>* x = buf;  // time samples (2m, 2m+1) in slot m, split order
+    const int P = fft_nsplit<Rl>(M);
     const double sc = I.in_scale;
     int ip = -1, ir = -1;
     for (int i = 0; i < I.nresp; ++i) {
         if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
     }
-    cpx<Rl>* Pr = nullptr;
+    const int Pr_split = (ir >= 0) ? fft_nsplit<Rl>(I.No) : 1;
     if (ir >= 0) {
-        // E^2 on the first half of the 2*No grid (thg=true form of sqr!)
+        // E^2 on the first half of the 2*No grid (thg=true form of sqr!), split order
         for (int m = tid; m < I.No; m += T) {
             cpx<Rl> v = mk<Rl>(0, 0);
             if (m < M) {
-                cpx<Rl> e = x[Swz<Rl>::f(m)];
+                cpx<Rl> e = x[Swz<Rl>::f(split_pos(m, M, P))];
                 Rl e0 = e.x * (Rl)sc, e1 = e.y * (Rl)sc;
                 v = mk<Rl>(e0 * e0, e1 * e1);
             }
-            w.ram[Swz<Rl>::f(m)] = v;
+            w.ram[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] = v;
         }
-        Pr = raman_conv<Rl>(I.resp[ir], I.No, w);
+        raman_conv<Rl>(I.resp[ir], I.No, w);
     }
     PlasmaCarry cr = {0, 0, 0};
     for (int c0 = 0; c0 < M; c0 += T) {
         const int m = c0 + tid;
         const bool act = m < M;
-        cpx<Rl> e = act ? x[Swz<Rl>::f(m)] : mk<Rl>(0, 0);
+        const int pos = Swz<Rl>::f(split_pos(m, M, P));
+        cpx<Rl> e = act ? x[pos] : mk<Rl>(0, 0);
         const double E0 = (double)e.x * sc, E1 = (double)e.y * sc;
         double P0 = 0, P1 = 0;
         for (int i = 0; i < I.nresp; ++i) {
@@ -411,7 +415,7 @@ __device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& st
                 P0 += r.coef * (E0 * E0 * E0);
                 P1 += r.coef * (E1 * E1 * E1);
             } else if (i == ir) {
-                cpx<Rl> p = act ? Pr[Swz<Rl>::f(m)] : mk<Rl>(0, 0);
+                cpx<Rl> p = act ? w.ram[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
                 P0 += r.coef * E0 * (double)p.x;
                 P1 += r.coef * E1 * (double)p.y;
             } else if (i == ip) {
@@ -420,11 +424,12 @@ __device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& st
         }
         if (act) {
             const double tw0 = __ldg(I.towin + 2 * m), tw1 = __ldg(I.towin + 2 * m + 1);
-            x[Swz<Rl>::f(m)] = mk<Rl>((Rl)(P0 * tw0), (Rl)(P1 * tw1));
+            x[pos] = mk<Rl>((Rl)(P0 * tw0), (Rl)(P1 * tw1));
         }
     }
     __syncthreads();
-    cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, M, w.tw);
+    block_fft<Rl, false>(x, M, w.tw);
+    cpx<Rl>* Z = x;
     // R2C split: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw
     for (int k = tid; k < Nw; k += T) {
         const int km = (M - k) & (M - 1);
@@ -444,7 +449,7 @@ __device__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& st
 
 // envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
 template <typename Rl, typename LoadF, typename StoreF>
-__device__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+__device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
     const int No = I.No, N = I.N, h = I.N / 2;
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
@@ -456,42 +461,46 @@ __device__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& sto
         buf[Swz<Rl>::f(j)] = cvt<Rl>(X);
     }
     __syncthreads();
-    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, No, w.tw);
+    block_fft<Rl, true>(buf, No, w.tw);
+    cpx<Rl>* x = buf;  // E(t) in split order
+    const int P = fft_nsplit<Rl>(No);
     const double sc = I.in_scale;
     int ir = -1;
     for (int i = 0; i < I.nresp; ++i)
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
-    cpx<Rl>* Pr = nullptr;
+    const int Pr_split = (ir >= 0) ? fft_nsplit<Rl>(No) : 1;
     if (ir >= 0) {
-        // 1/2 |E|^2 on the first half of the 2*No grid (sqr! for RamanPolarEnv)
+        // 1/2 |E|^2 on the first half of the 2*No grid (sqr! for RamanPolarEnv), split order
         for (int m = tid; m < No; m += T) {
             cpx<Rl> v = mk<Rl>(0, 0);
             if (m < No / 2) {
-                cpx<double> a = scale(sc, cvt<double>(x[Swz<Rl>::f(2 * m)]));
-                cpx<double> b = scale(sc, cvt<double>(x[Swz<Rl>::f(2 * m + 1)]));
+                cpx<double> a = scale(sc, cvt<double>(x[Swz<Rl>::f(split_pos(2 * m, No, P))]));
+                cpx<double> b = scale(sc, cvt<double>(x[Swz<Rl>::f(split_pos(2 * m + 1, No, P))]));
                 v = mk<Rl>((Rl)(0.5 * abs2(a)), (Rl)(0.5 * abs2(b)));
             }
-            w.ram[Swz<Rl>::f(m)] = v;
+            w.ram[Swz<Rl>::f(split_pos(m, No, Pr_split))] = v;
         }
-        Pr = raman_conv<Rl>(I.resp[ir], No, w);
+        raman_conv<Rl>(I.resp[ir], No, w);
     }
     for (int n = tid; n < No; n += T) {
-        cpx<double> E = scale(sc, cvt<double>(x[Swz<Rl>::f(n)]));
-        cpx<double> P = mk<double>(0, 0);
+        const int pos = Swz<Rl>::f(split_pos(n, No, P));
+        cpx<double> E = scale(sc, cvt<double>(x[pos]));
+        cpx<double> Pt = mk<double>(0, 0);
         for (int i = 0; i < I.nresp; ++i) {
             const LunaResp& r = I.resp[i];
             if (r.kind == LUNA_RESP_KERR_ENV) {
-                P = P + scale(0.75 * r.coef * abs2(E), E);
+                Pt = Pt + scale(0.75 * r.coef * abs2(E), E);
             } else if (i == ir) {
-                cpx<Rl> p = Pr[Swz<Rl>::f(n >> 1)];
+                cpx<Rl> p = w.ram[Swz<Rl>::f(split_pos(n >> 1, No, Pr_split))];
                 double pv = (n & 1) ? (double)p.y : (double)p.x;
-                P = P + scale(r.coef * pv, E);
+                Pt = Pt + scale(r.coef * pv, E);
             }
         }
-        x[Swz<Rl>::f(n)] = cvt<Rl>(scale(__ldg(I.towin + n), P));
+        x[pos] = cvt<Rl>(scale(__ldg(I.towin + n), Pt));
     }
     __syncthreads();
-    cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, No, w.tw);
+    block_fft<Rl, false>(x, No, w.tw);
+    cpx<Rl>* Z = x;
     for (int k = tid; k < N; k += T) {
         const int src = (k < h) ? k : (No - N + k);
         cpx<double> X = cvt<double>(Z[Swz<Rl>::f(src)]);
@@ -510,7 +519,7 @@ __device__ __forceinline__ void rhs(const LunaInst& I, Ws<Rl>& w, LoadF&& load, 
 // Luna.jl:366-372: Eω .*= ωwin; Et = FT \ Eω; Et .*= twin; Eω = FT * Et (coarse grid),
 // applied to yn after multiplying by exp(L*dz) (prop!_maybe, RK45.jl:225).
 template <typename Rl>
-__device__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double2* yn, const double2* e1) {
+__device__ __noinline__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double2* yn, const double2* e1) {
     const int tid = threadIdx.x, T = LUNA_BLOCK;
     const int Nw = I.Nw, N = I.N;
     cpx<Rl>* buf = w.main;
@@ -538,16 +547,20 @@ __device__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double2* yn, const 
             }
         }
         __syncthreads();
-        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+        block_fft<Rl, true>(buf, M, w.tw);
+        cpx<Rl>* x = buf;
+        const int P = fft_nsplit<Rl>(M);
         const double inv = 1.0 / (double)N;
         for (int m = tid; m < M; m += T) {
-            cpx<Rl> e = x[Swz<Rl>::f(m)];
+            const int pos = Swz<Rl>::f(split_pos(m, M, P));
+            cpx<Rl> e = x[pos];
             double a = (double)e.x * inv * __ldg(I.twin + 2 * m);
             double b = (double)e.y * inv * __ldg(I.twin + 2 * m + 1);
-            x[Swz<Rl>::f(m)] = mk<Rl>((Rl)a, (Rl)b);
+            x[pos] = mk<Rl>((Rl)a, (Rl)b);
         }
         __syncthreads();
-        cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, M, w.tw);
+        block_fft<Rl, false>(x, M, w.tw);
+        cpx<Rl>* Z = x;
         for (int k = tid; k < Nw; k += T) {
             const int km = (M - k) & (M - 1);
             cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
@@ -564,12 +577,17 @@ __device__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double2* yn, const 
     } else {
         for (int j = tid; j < N; j += T) buf[Swz<Rl>::f(j)] = cvt<Rl>(ld(j));
         __syncthreads();
-        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, N, w.tw);
+        block_fft<Rl, true>(buf, N, w.tw);
+        cpx<Rl>* x = buf;
+        const int P = fft_nsplit<Rl>(N);
         const double inv = 1.0 / (double)N;
-        for (int n = tid; n < N; n += T)
-            x[Swz<Rl>::f(n)] = cvt<Rl>(scale(inv * __ldg(I.twin + n), cvt<double>(x[Swz<Rl>::f(n)])));
+        for (int n = tid; n < N; n += T) {
+            const int pos = Swz<Rl>::f(split_pos(n, N, P));
+            x[pos] = cvt<Rl>(scale(inv * __ldg(I.twin + n), cvt<double>(x[pos])));
+        }
         __syncthreads();
-        cpx<Rl>* Z = block_fft<Rl, false>(x, (x == buf) ? w.main_alt : buf, N, w.tw);
+        block_fft<Rl, false>(x, N, w.tw);
+        cpx<Rl>* Z = x;
         for (int k = tid; k < N; k += T) Yo[k] = cvt<double>(Z[Swz<Rl>::f(k)]);
     }
     __syncthreads();
@@ -687,8 +705,9 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
     const int tid = threadIdx.x, T = LUNA_BLOCK;
     const int Nw = I.Nw;
     const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
-    void* k[7];
-    for (int j = 0; j < 7; ++j) k[j] = I.k[j];
+    void** k = c.k;
+    if (tid == 0)
+        for (int j = 0; j < 7; ++j) k[j] = I.k[j];
     cpx<double>* e1 = reinterpret_cast<cpx<double>*>(I.e1);
     double2* py = I.y;
     double2* pyn = I.yn;
@@ -753,21 +772,22 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
                 }
             }
             __syncthreads();
-            double coef[6];
-#pragma unroll
-            for (int j = 0; j < 6; ++j) coef[j] = dt * c_B[s][j];
             void* kout = k[s + 1];
+            void* k1p = k[0];
+            const double c0 = dt * c_B[s][0];
             const bool propk1 = (s == 0) && (dprop != 0.0);
             auto load = [&](int i) -> cpx<double> {
-                cpx<double> k1 = KT<Kt>::ld(k[0], i);
+                cpx<double> k1 = KT<Kt>::ld(k1p, i);
                 if (propk1) {
                     k1 = k1 * e1[i];
-                    KT<Kt>::st(k[0], i, k1);
+                    KT<Kt>::st(k1p, i, k1);
                 }
                 cpx<double> acc = y[i];
-                acc = acc + scale(coef[0], k1);
-                for (int j = 1; j <= s; ++j)
-                    if (c_B[s][j] != 0) acc = acc + scale(coef[j], KT<Kt>::ld(k[j], i));
+                acc = acc + scale(c0, k1);
+                for (int j = 1; j <= s; ++j) {
+                    const double bj = c_B[s][j];
+                    if (bj != 0) acc = acc + scale(dt * bj, KT<Kt>::ld(k[j], i));
+                }
                 return cvt<double>(w.efac[i]) * acc;
             };
             auto store = [&](int i, cpx<double> v) { KT<Kt>::st(kout, i, v * inv_fac<Rl>(w.efac[i])); };
@@ -862,9 +882,13 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
         if (c.done && c.status != 0) break;
         if (c.ok) {
             // FSAL: ks[1] <- ks[7]
-            void* tmp = k[0];
-            k[0] = k[6];
-            k[6] = tmp;
+            __syncthreads();
+            if (tid == 0) {
+                void* tmp = k[0];
+                k[0] = k[6];
+                k[6] = tmp;
+            }
+            __syncthreads();
             // prop!_maybe + stepfun window filter on yn
             stepfun_filter<Rl>(I, w, pyn, I.e1);
             // GridCondition saves (Output.jl:65-82, 490-502)

@@ -187,7 +187,9 @@ class Batch:
                 pass
             self._h = None
 
-    def upload(self, linops, y0s, z0s, dz0s, zmaxs):
+    def upload(self, linops, y0s, z0s, dz0s, zmaxs, zsaves=None, max_dts=None):
+        """Copy the inputs of every instance to the device. ``zsaves`` (per-instance save
+        points) and ``max_dts`` (per-instance step limits) are optional."""
         n = len(self.plans)
         self._L = [_c128(L) for L in linops]
         self._Y = [_c128(y) for y in y0s]
@@ -196,8 +198,17 @@ class Batch:
         z0 = _f64(z0s)
         dz0 = _f64(dz0s)
         zm = _f64(zmaxs)
+        Zp = None
+        if zsaves is not None:
+            self._Z = [_f64(z) for z in zsaves]
+            Zp = (_lib.PD * n)(*[_lib.dptr(z) for z in self._Z])
+        md = None
+        if max_dts is not None:
+            self._MD = _f64(max_dts)
+            md = _lib.dptr(self._MD)
         _lib.check(_lib.load().luna_b200_batch_upload(self._h, Lp, Yp, _lib.dptr(z0),
-                                                     _lib.dptr(dz0), _lib.dptr(zm)))
+                                                     _lib.dptr(dz0), _lib.dptr(zm), Zp,
+                                                     md if md is not None else _lib.dptr(None)))
 
     def run(self):
         ms = _lib.c_float(0)

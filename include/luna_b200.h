@@ -146,6 +146,23 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
 void luna_b200_batch_destroy(luna_batch* b);
 
+/* Allocation-free variant of luna_b200_rhs_device. It has no counterpart in the reference:
+ * it serves host programs that must not allocate device memory while they run (for
+ * example a solver inside an allocator-managed runtime, or a process whose device memory
+ * is owned by another framework's caching pool, where a cudaMalloc could fail or
+ * fragment the pool). It allocates nothing: its scratch is a fixed buffer of
+ * LUNA_NOALLOC_SCRATCH_BYTES in the library's static device memory, held by every device
+ * that loads the library until the process exits. The plan (created beforehand) and the
+ * caller's device buffers nl_dev/Ew_dev ([2*Nw] doubles) and status_dev (one int, may be
+ * NULL; receives LUNA_OK or LUNA_FIELD_ABOVE_EMAX) are the only other memory it touches.
+ * The first call on a device resolves the buffer's device address; make that first call
+ * before any stream capture. Plans whose transforms need more scratch than the buffer are
+ * rejected with LUNA_ERR_UNSUPPORTED. All calls share the one buffer: calls that overlap on
+ * the GPU (different streams, or different host threads) race and must be serialised. */
+#define LUNA_NOALLOC_SCRATCH_BYTES (1u << 20)
+int luna_b200_rhs_device_noalloc(luna_plan* plan, double* nl_dev, const double* Ew_dev, double z,
+                                 void* stream, int* status_dev);
+
 const char* luna_b200_last_error(void);
 int luna_b200_version(void);
 

@@ -18,6 +18,7 @@ LUNA_STEP_BUDGET = 4
 LUNA_ERR_BAD_ARG = 16
 LUNA_ERR_UNSUPPORTED = 17
 LUNA_ERR_CUDA = 18
+NOALLOC_SCRATCH_BYTES = 1 << 20
 
 RESP_KERR_FIELD = 1
 RESP_KERR_ENV = 2
@@ -65,7 +66,7 @@ EXPORTS = [
     "luna_b200_plan_create", "luna_b200_plan_destroy", "luna_b200_rhs", "luna_b200_rhs_device",
     "luna_b200_solve", "luna_b200_batch_create", "luna_b200_batch_upload", "luna_b200_batch_run",
     "luna_b200_batch_download", "luna_b200_batch_steplog", "luna_b200_batch_destroy",
-    "luna_b200_last_error", "luna_b200_version",
+    "luna_b200_last_error", "luna_b200_version", "luna_b200_rhs_device_noalloc",
 ]
 
 _lib = None
@@ -102,6 +103,8 @@ def load():
     lib.luna_b200_batch_steplog.argtypes = [c_void_p, c_int, PD]
     lib.luna_b200_batch_destroy.argtypes = [c_void_p]
     lib.luna_b200_batch_destroy.restype = None
+    lib.luna_b200_rhs_device_noalloc.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p,
+                                                 c_void_p]
     lib.luna_b200_last_error.restype = ctypes.c_char_p
     lib.luna_b200_version.restype = c_int
     _lib = lib

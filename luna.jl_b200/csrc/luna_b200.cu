@@ -691,4 +691,92 @@ int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z
     return LUNA_OK;
 }
 
+// ---------------------------------------------------------------- allocation-free RHS
+// The scratch lives in static device memory. Host code must not pass the symbol itself to
+// a kernel (on the host it names a host-side shadow); its device address is resolved with
+// cudaGetSymbolAddress once per device and cached.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[LUNA_NOALLOC_SCRATCH_BYTES];
+
 }  // extern "C"
+
+namespace {
+std::mutex g_na_mu;
+std::map<int, void*> g_na_ptr;
+
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    auto it = g_na_ptr.find(dev);
+    if (it != g_na_ptr.end()) {
+        *out = it->second;
+        return LUNA_OK;
+    }
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(LUNA_ERR_CUDA, std::string("noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+    g_na_ptr[dev] = p;
+    *out = p;
+    return LUNA_OK;
+}
+
+// twiddle tables of the current device without creating them (plan creation did)
+int find_tw(TwDev& out) {
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_tw_mu);
+    auto it = g_tw.find(dev);
+    if (it == g_tw.end()) return fail(LUNA_ERR_BAD_ARG, "noalloc: no plan was created on this device");
+    out = it->second;
+    return LUNA_OK;
+}
+}  // namespace
+
+// The instance description travels as a kernel parameter, so the call needs no device copy.
+template <typename Rl>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+rhs_kernel_noalloc(const LunaInst I, const double2* Ew, double2* nl, TwTab<Rl> tw, int smem_bytes, int* status) {
+    extern __shared__ __align__(256) char smem[];
+    Ws<Rl> w;
+    plan_ws<Rl>(I, smem, smem_bytes, w, tw);
+    if (threadIdx.x == 0) *w.flag = 0;
+    __syncthreads();
+    const cpx<double>* E = reinterpret_cast<const cpx<double>*>(Ew);
+    cpx<double>* o = reinterpret_cast<cpx<double>*>(nl);
+    rhs<Rl>(I, w, [&](int k) { return E[k]; }, [&](int k, cpx<double> v) { o[k] = v; });
+    __syncthreads();
+    if (threadIdx.x == 0 && status) *status = (*w.flag & (1 << ST_FIELD_ABOVE_EMAX)) ? ST_FIELD_ABOVE_EMAX : ST_OK;
+}
+
+extern "C" int luna_b200_rhs_device_noalloc(luna_plan* p, double* nl_dev, const double* Ew_dev, double z,
+                                            void* stream, int* status_dev) {
+    (void)z;  // constant density and effective area: the transform does not depend on z
+    if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "rhs_device_noalloc: null argument");
+    LunaInst I = p->proto;
+    const size_t need = (p->precision == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
+    if (need > (size_t)LUNA_NOALLOC_SCRATCH_BYTES)
+        return fail(LUNA_ERR_UNSUPPORTED, "rhs_device_noalloc: the plan needs " + std::to_string(need) +
+                                              " bytes of scratch, more than LUNA_NOALLOC_SCRATCH_BYTES (" +
+                                              std::to_string((size_t)LUNA_NOALLOC_SCRATCH_BYTES) + ")");
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    TwDev tw;
+    rc = find_tw(tw);
+    if (rc) return rc;
+    I.gscr = scratch;
+    const int maxs = max_smem_optin();
+    cudaStream_t st = (cudaStream_t)stream;
+    if (p->precision == LUNA_PREC_FP64) {
+        int sm = (int)std::min<size_t>(smem_wanted<double>(I), (size_t)maxs);
+        CK(cudaFuncSetAttribute(rhs_kernel_noalloc<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        rhs_kernel_noalloc<double><<<1, LUNA_BLOCK, sm, st>>>(I, (const double2*)Ew_dev, (double2*)nl_dev, tw.d, sm, status_dev);
+    } else {
+        int sm = (int)std::min<size_t>(smem_wanted<float>(I), (size_t)maxs);
+        CK(cudaFuncSetAttribute(rhs_kernel_noalloc<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+        rhs_kernel_noalloc<float><<<1, LUNA_BLOCK, sm, st>>>(I, (const double2*)Ew_dev, (double2*)nl_dev, tw.f, sm, status_dev);
+    }
+    CK(cudaGetLastError());
+    return LUNA_OK;
+}

@@ -227,6 +227,53 @@ __device__ __forceinline__ void sub_ffts(cpx<R>* buf, int M, int P, const TwTab<
     }
 }
 
+// Out-of-place Stockham pass (natural order in and out) between two global-memory buffers;
+// used when a transform does not fit in shared memory and a second buffer is available.
+// Each butterfly's twiddles come from independent table lookups (no dependent chain), which
+// keeps more L2 requests in flight than the binary-power form used in shared memory.
+template <typename R, bool INV, int RAD>
+__device__ __forceinline__ void pass_oop(const cpx<R>* src, cpx<R>* dst, int M, int L, const TwTab<R>& tw) {
+    const int stride = M / RAD;
+    const int shift = TW_LOG_MMAX - ilog2i((unsigned)(L * RAD));
+    for (int j = threadIdx.x; j < stride; j += LUNA_BLOCK) {
+        cpx<R> v[RAD];
+#pragma unroll
+        for (int i = 0; i < RAD; ++i) v[i] = src[Swz<R>::f(j + bitrev<RAD>(i) * stride)];
+        const int k = j & (L - 1);
+        if (L > 1) {
+#pragma unroll
+            for (int i = 1; i < RAD; ++i)
+                v[i] = v[i] * twiddle<R, INV>(tw, (unsigned)(bitrev<RAD>(i) * k) << shift);
+        }
+        dft_br<R, INV, RAD>(v);
+        const int base = (j - k) * RAD + k;
+#pragma unroll
+        for (int r = 0; r < RAD; ++r) dst[Swz<R>::f(base + r * L)] = v[r];
+    }
+    __syncthreads();
+}
+
+// Natural-order out-of-place transform with radix-16 passes (the last one takes the
+// remainder radix); returns the buffer holding the result (a or b).
+template <typename R, bool INV>
+__device__ __forceinline__ cpx<R>* fft_oop(cpx<R>* a, cpx<R>* b, int M, const TwTab<R>& tw) {
+    int L = 1;
+    cpx<R>* src = a;
+    cpx<R>* dst = b;
+    while (L < M) {
+        const int rad = min(16, M / L);
+        if (rad == 2) pass_oop<R, INV, 2>(src, dst, M, L, tw);
+        else if (rad == 4) pass_oop<R, INV, 4>(src, dst, M, L, tw);
+        else if (rad == 8) pass_oop<R, INV, 8>(src, dst, M, L, tw);
+        else pass_oop<R, INV, 16>(src, dst, M, L, tw);
+        cpx<R>* t = src;
+        src = dst;
+        dst = t;
+        L *= rad;
+    }
+    return src;
+}
+
 // number of sub-transforms for a length-M transform
 template <typename R>
 __host__ __device__ __forceinline__ int fft_nsplit(int M) {
@@ -240,13 +287,31 @@ __device__ __forceinline__ int split_pos(int n, int M, int P) {
     return (n & (P - 1)) * (M / P) + n / P;
 }
 
-// Unnormalised DFT of length M (power of two, 2 <= M <= FftMmax), in place.
+// Unnormalised DFT of length M (power of two, 2 <= M <= FftMmax).
+// With alt == nullptr (shared-memory buffers) it runs in place:
 //   forward (INV=false): split-order input -> natural-order output
 //   inverse (INV=true):  natural-order input -> split-order output
-// The caller synchronises before the call (the input is written by other threads); the
-// call ends with a barrier.
+// With a second buffer alt (global-memory buffers) it runs out of place in natural order
+// both ways. Returns the buffer holding the result. The caller synchronises before the
+// call (the input is written by other threads); the call ends with a barrier.
 template <typename R, bool INV>
-__device__ __noinline__ void block_fft(cpx<R>* buf, int M, const TwTab<R>& tw) {
+__device__ __forceinline__ void block_fft_split(cpx<R>* buf, int M, const TwTab<R>& tw);
+
+template <typename R, bool INV>
+__device__ __noinline__ cpx<R>* block_fft(cpx<R>* buf, cpx<R>* alt, int M, const TwTab<R>& tw) {
+    if (alt) return fft_oop<R, INV>(buf, alt, M, tw);
+    block_fft_split<R, INV>(buf, M, tw);
+    return buf;
+}
+
+// split factor of a length-M transform on a buffer (1: natural order, out of place)
+template <typename R>
+__device__ __forceinline__ int buf_split(const cpx<R>* alt, int M) {
+    return alt ? 1 : fft_nsplit<R>(M);
+}
+
+template <typename R, bool INV>
+__device__ __forceinline__ void block_fft_split(cpx<R>* buf, int M, const TwTab<R>& tw) {
     const int P = fft_nsplit<R>(M);
     if (INV) {
         if (P == 2) join_pass<R, INV, 2>(buf, M, tw);

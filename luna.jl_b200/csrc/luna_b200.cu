@@ -80,8 +80,7 @@ raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<Rl>* H, 
         buf[Swz<double>::f(split_pos(m, No, P))] = mk<double>(a, b);
     }
     __syncthreads();
-    block_fft<double, false>(buf, No, tw);
-    cpx<double>* Z = buf;
+    cpx<double>* Z = block_fft<double, false>(buf, nullptr, No, tw);
     const int M = No;
     for (int k = tid; k <= M; k += LUNA_BLOCK) {
         const int kk = k & (M - 1);

@@ -23,8 +23,10 @@ namespace luna {
 template <typename Rl>
 struct Ws {
     cpx<Rl>* main;      // transform buffer
+    cpx<Rl>* main_alt;  // second buffer (global memory only): out-of-place transforms
     cpx<Rl>* efac;      // exp(L*dz) of the current stage, Nw entries
     cpx<Rl>* ram;       // Raman convolution buffer (No complex)
+    cpx<Rl>* ram_alt;
     double* red;        // 3 * LUNA_WARPS reduction scratch
     double* tot;        // 3 * LUNA_WARPS scan totals
     double* edge;       // 4 edge values carried between scan chunks
@@ -69,9 +71,9 @@ template <typename Rl>
 __host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
     size_t c = sizeof(cpx<Rl>);
     size_t b = 0;
-    b += align_up((size_t)main_len(I) * c, 256);
+    b += 2 * align_up((size_t)main_len(I) * c, 256);
     b += align_up((size_t)I.Nw * c, 256);
-    if (has_raman(I)) b += align_up((size_t)I.No * c, 256);
+    if (has_raman(I)) b += 2 * align_up((size_t)I.No * c, 256);
     return b;
 }
 
@@ -92,11 +94,13 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
     size_t mb = align_up((size_t)Mm * c, 256);
     if (off + mb <= (size_t)smem_bytes) {
         w.main = reinterpret_cast<cpx<Rl>*>(smem + off);
+        w.main_alt = nullptr;
         off += mb;
     } else {
         w.main = reinterpret_cast<cpx<Rl>*>(g + goff);
+        w.main_alt = reinterpret_cast<cpx<Rl>*>(g + goff + mb);
     }
-    goff += mb;
+    goff += 2 * mb;
     size_t eb = align_up((size_t)I.Nw * c, 256);
     if (off + eb <= (size_t)smem_bytes) {
         w.efac = reinterpret_cast<cpx<Rl>*>(smem + off);
@@ -105,7 +109,7 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
         w.efac = reinterpret_cast<cpx<Rl>*>(g + goff);
     }
     goff += eb;
-    w.ram = nullptr;
+    w.ram = w.ram_alt = nullptr;
     if (has_raman(I)) {
         size_t rb = align_up((size_t)I.No * c, 256);
         if (off + rb <= (size_t)smem_bytes) {
@@ -113,8 +117,9 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
             off += rb;
         } else {
             w.ram = reinterpret_cast<cpx<Rl>*>(g + goff);
+            w.ram_alt = reinterpret_cast<cpx<Rl>*>(g + goff + rb);
         }
-        goff += rb;
+        goff += 2 * rb;
     }
 }
 
@@ -259,11 +264,11 @@ __device__ __forceinline__ cpx<double> half_twiddle(const TwTab<Rl>& tw, int k, 
 // Raman convolution on the 2*No grid (Nonlinear.jl:282-333): the input samples s[n]
 // (n < No) are in `ram` as complex pairs (s[2m], s[2m+1]) for m < No/2 (zero above), in
 // split order; on return `ram` holds P[n], n < No, as pairs in split order.
+// Returns the buffer that holds P (w.ram or, out of place, w.ram_alt).
 template <typename Rl>
-__device__ __forceinline__ void raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
+__device__ __forceinline__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>& w) {
     __syncthreads();
-    cpx<Rl>* Z = w.ram;
-    block_fft<Rl, false>(Z, No, w.tw);
+    cpx<Rl>* Z = block_fft<Rl, false>(w.ram, w.ram_alt, No, w.tw);
     const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(r.H);
     const int M = No;  // complex length of the 2*No real transform
     for (int k = threadIdx.x; k <= M / 2; k += LUNA_BLOCK) {
@@ -297,7 +302,8 @@ __device__ __forceinline__ void raman_conv(const LunaResp& r, int No, Ws<Rl>& w)
         }
     }
     __syncthreads();
-    block_fft<Rl, true>(Z, No, w.tw);
+    cpx<Rl>* other = w.ram_alt ? ((Z == w.ram) ? w.ram_alt : w.ram) : nullptr;
+    return block_fft<Rl, true>(Z, other, No, w.tw);
 }
 
 // ------------------------------------------------------------------ plasma chunk
@@ -378,16 +384,16 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
         }
     }
     __syncthreads();
-    block_fft<Rl, true>(buf, M, w.tw);
-    cpx<Rl>* x = buf;  // time samples (2m, 2m+1) in slot m, split order
-    const int P = fft_nsplit<Rl>(M);
+    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);  // slot m: samples 2m, 2m+1
+    const int P = buf_split<Rl>(w.main_alt, M);
     const double sc = I.in_scale;
     int ip = -1, ir = -1;
     for (int i = 0; i < I.nresp; ++i) {
         if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
     }
-    const int Pr_split = (ir >= 0) ? fft_nsplit<Rl>(I.No) : 1;
+    const int Pr_split = (ir >= 0) ? buf_split<Rl>(w.ram_alt, I.No) : 1;
+    cpx<Rl>* Pr = nullptr;
     if (ir >= 0) {
         // E^2 on the first half of the 2*No grid (thg=true form of sqr!), split order
         for (int m = tid; m < I.No; m += T) {
@@ -399,7 +405,7 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
             }
             w.ram[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] = v;
         }
-        raman_conv<Rl>(I.resp[ir], I.No, w);
+        Pr = raman_conv<Rl>(I.resp[ir], I.No, w);
     }
     PlasmaCarry cr = {0, 0, 0};
     for (int c0 = 0; c0 < M; c0 += T) {
@@ -415,7 +421,7 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
                 P0 += r.coef * (E0 * E0 * E0);
                 P1 += r.coef * (E1 * E1 * E1);
             } else if (i == ir) {
-                cpx<Rl> p = act ? w.ram[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
+                cpx<Rl> p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
                 P0 += r.coef * E0 * (double)p.x;
                 P1 += r.coef * E1 * (double)p.y;
             } else if (i == ip) {
@@ -428,8 +434,7 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
         }
     }
     __syncthreads();
-    block_fft<Rl, false>(x, M, w.tw);
-    cpx<Rl>* Z = x;
+    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, M, w.tw);
     // R2C split: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw
     for (int k = tid; k < Nw; k += T) {
         const int km = (M - k) & (M - 1);
@@ -461,14 +466,14 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
         buf[Swz<Rl>::f(j)] = cvt<Rl>(X);
     }
     __syncthreads();
-    block_fft<Rl, true>(buf, No, w.tw);
-    cpx<Rl>* x = buf;  // E(t) in split order
-    const int P = fft_nsplit<Rl>(No);
+    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, No, w.tw);  // E(t), split order
+    const int P = buf_split<Rl>(w.main_alt, No);
     const double sc = I.in_scale;
     int ir = -1;
     for (int i = 0; i < I.nresp; ++i)
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
-    const int Pr_split = (ir >= 0) ? fft_nsplit<Rl>(No) : 1;
+    const int Pr_split = (ir >= 0) ? buf_split<Rl>(w.ram_alt, No) : 1;
+    cpx<Rl>* Pr = nullptr;
     if (ir >= 0) {
         // 1/2 |E|^2 on the first half of the 2*No grid (sqr! for RamanPolarEnv), split order
         for (int m = tid; m < No; m += T) {
@@ -480,7 +485,7 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
             }
             w.ram[Swz<Rl>::f(split_pos(m, No, Pr_split))] = v;
         }
-        raman_conv<Rl>(I.resp[ir], No, w);
+        Pr = raman_conv<Rl>(I.resp[ir], No, w);
     }
     for (int n = tid; n < No; n += T) {
         const int pos = Swz<Rl>::f(split_pos(n, No, P));
@@ -491,7 +496,7 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
             if (r.kind == LUNA_RESP_KERR_ENV) {
                 Pt = Pt + scale(0.75 * r.coef * abs2(E), E);
             } else if (i == ir) {
-                cpx<Rl> p = w.ram[Swz<Rl>::f(split_pos(n >> 1, No, Pr_split))];
+                cpx<Rl> p = Pr[Swz<Rl>::f(split_pos(n >> 1, No, Pr_split))];
                 double pv = (n & 1) ? (double)p.y : (double)p.x;
                 Pt = Pt + scale(r.coef * pv, E);
             }
@@ -499,8 +504,7 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
         x[pos] = cvt<Rl>(scale(__ldg(I.towin + n), Pt));
     }
     __syncthreads();
-    block_fft<Rl, false>(x, No, w.tw);
-    cpx<Rl>* Z = x;
+    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, No, w.tw);
     for (int k = tid; k < N; k += T) {
         const int src = (k < h) ? k : (No - N + k);
         cpx<double> X = cvt<double>(Z[Swz<Rl>::f(src)]);
@@ -547,9 +551,8 @@ __device__ __noinline__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double
             }
         }
         __syncthreads();
-        block_fft<Rl, true>(buf, M, w.tw);
-        cpx<Rl>* x = buf;
-        const int P = fft_nsplit<Rl>(M);
+        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+        const int P = buf_split<Rl>(w.main_alt, M);
         const double inv = 1.0 / (double)N;
         for (int m = tid; m < M; m += T) {
             const int pos = Swz<Rl>::f(split_pos(m, M, P));
@@ -559,8 +562,7 @@ __device__ __noinline__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double
             x[pos] = mk<Rl>((Rl)a, (Rl)b);
         }
         __syncthreads();
-        block_fft<Rl, false>(x, M, w.tw);
-        cpx<Rl>* Z = x;
+        cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, M, w.tw);
         for (int k = tid; k < Nw; k += T) {
             const int km = (M - k) & (M - 1);
             cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
@@ -577,17 +579,15 @@ __device__ __noinline__ void stepfun_filter(const LunaInst& I, Ws<Rl>& w, double
     } else {
         for (int j = tid; j < N; j += T) buf[Swz<Rl>::f(j)] = cvt<Rl>(ld(j));
         __syncthreads();
-        block_fft<Rl, true>(buf, N, w.tw);
-        cpx<Rl>* x = buf;
-        const int P = fft_nsplit<Rl>(N);
+        cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, N, w.tw);
+        const int P = buf_split<Rl>(w.main_alt, N);
         const double inv = 1.0 / (double)N;
         for (int n = tid; n < N; n += T) {
             const int pos = Swz<Rl>::f(split_pos(n, N, P));
             x[pos] = cvt<Rl>(scale(inv * __ldg(I.twin + n), cvt<double>(x[pos])));
         }
         __syncthreads();
-        block_fft<Rl, false>(x, N, w.tw);
-        cpx<Rl>* Z = x;
+        cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, N, w.tw);
         for (int k = tid; k < N; k += T) Yo[k] = cvt<double>(Z[Swz<Rl>::f(k)]);
     }
     __syncthreads();

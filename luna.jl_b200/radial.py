@@ -1,0 +1,145 @@
+"""Radially symmetric free-space propagation (host setup), mirroring Luna.jl.
+
+* ``make_const_linop_radial`` — LinearOps.make_const_linop(grid::RealGrid, q::QDHT, nfun)
+  (LinearOps.jl:130-144, 185-197): L(ω, k) = -i(sqrt(k(ω)^2 - k_r^2) - β1 ω), evanescent
+  components damped by min(sqrt|.|, 200).
+* ``const_norm_radial`` — NonlinearRHS.const_norm_radial / norm_radial
+  (NonlinearRHS.jl:482-524): sqrt(k^2 - k_r^2)/(μ0 ω), 1 where that is not real or ω = 0.
+* ``TransRadial`` — the transform description (NonlinearRHS.jl:406-474) that the device
+  plan is built from.
+* ``GaussGaussField`` — Fields.SpatioTemporalField with a Gaussian profile in time and
+  radius, energy normalisation by ``energyfuncs(grid, q)`` and free-space propagation by
+  ``propz`` (Fields.jl:343-411, 536-549); ``focal_length`` adds a thin-lens phase.
+"""
+import math
+
+import numpy as np
+
+from . import physdata as pd
+from .fields import analytic, simpson_even
+from .grid import RealGrid
+from .hankel import QDHT
+from .maths import gauss
+from .nonlinear import Kerr_field, PlasmaCumtrapz, ionrate_fun_ADK
+from . import ionisation
+
+
+def _n_on_sidx(grid, nfun):
+    n = np.zeros(len(grid.ω))
+    s = grid.sidx
+    n[s] = np.real(nfun(2 * math.pi * pd.c / grid.ω[s]))
+    return n
+
+
+def _beta1(nfun, λ0):
+    """d/dω [ω/c Re n(ω)] at the reference wavelength (central difference)."""
+    w0 = pd.wlfreq(λ0)
+    f = lambda w: w / pd.c * float(np.real(nfun(np.array([pd.wlfreq(w)]))[0]))
+    h = w0 * 1e-4
+    return (-f(w0 + 2 * h) + 8 * f(w0 + h) - 8 * f(w0 - h) + f(w0 - 2 * h)) / (12 * h)
+
+
+def make_const_linop_radial(grid, q, nfun):
+    n = _n_on_sidx(grid, nfun)
+    β1 = _beta1(nfun, grid.referenceλ)
+    k2 = (n * grid.ω / pd.c) ** 2
+    kr2 = q.k ** 2
+    βsq = k2[:, None] - kr2[None, :]
+    w = grid.ω[:, None]
+    L = np.where(βsq < 0,
+                 -1j * (-β1 * w) - np.minimum(np.sqrt(np.abs(βsq)), 200.0),
+                 -1j * (np.sqrt(np.maximum(βsq, 0.0)) - β1 * w))
+    return np.ascontiguousarray(L.astype(np.complex128)), β1
+
+
+def const_norm_radial(grid, q, nfun):
+    n = _n_on_sidx(grid, nfun)
+    k2 = np.zeros(len(grid.ω))
+    s = grid.sidx
+    k2[s] = (n[s] * grid.ω[s] / pd.c) ** 2
+    βsq = k2[:, None] - (q.k ** 2)[None, :]
+    w = grid.ω[:, None] * np.ones((1, q.N))
+    out = np.ones((len(grid.ω), q.N))
+    ok = (w != 0) & (βsq > 0)
+    out[ok] = np.sqrt(βsq[ok]) / (pd.mu_0 * w[ok])
+    return out
+
+
+class TransRadial:
+    """Radial transform E(ω, k) -> P_nl(ω, k) with constant density."""
+
+    kind = "radial"
+
+    def __init__(self, grid, q, resp, density, normfun):
+        self.grid, self.q = grid, q
+        self.resp = tuple(resp)
+        self.density = float(density)
+        self.normfun = np.asarray(normfun, dtype=np.float64)
+        self._plan = None
+
+    def output_factor(self):
+        """ωwin (-iω) / (2 normfun) over (ω, k) (NonlinearRHS.jl:473)."""
+        g = self.grid
+        return (g.ωwin * (-1j * g.ω))[:, None] / (2 * self.normfun)
+
+    def plan(self):
+        if self._plan is None:
+            from .radial_plan import RadialPlan
+            self._plan = RadialPlan.from_transform(self)
+        return self._plan
+
+    def __call__(self, nl, Eω, z):
+        self.plan().rhs(nl, Eω, z)
+
+
+def energy_t_radial(grid, q, Etr):
+    """energyfuncs(grid::RealGrid, q)[1] (Fields.jl:536-541): Etr is (Nt, Nr)."""
+    Eta = np.apply_along_axis(analytic, 0, Etr)
+    tint = np.array([simpson_even(grid.t, np.abs(Eta[:, i]) ** 2) for i in range(Etr.shape[1])])
+    return 2 * math.pi * pd.c * pd.eps_0 / 2 * q.integrateR(tint)
+
+
+def GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=0.0, focal_length=None, ϕ=0.0):
+    t = grid.t
+    ω0 = pd.wlfreq(λ0)
+    shape = gauss(t, τfwhm)[:, None] * np.exp(-0.5 * (q.r / (w0 / 2)) ** 2)[None, :]
+    Etr = np.sqrt(shape) * np.cos(ω0 * t + ϕ)[:, None]
+    Etr = Etr * math.sqrt(energy) / math.sqrt(energy_t_radial(grid, q, Etr))
+    Eωr = np.fft.rfft(Etr, axis=0)
+    if focal_length is not None:
+        # thin lens: exp(-i ω r^2 / (2 c f)) applied in (ω, r)
+        Eωr = Eωr * np.exp(-1j * grid.ω[:, None] * (q.r ** 2)[None, :] / (2 * pd.c * focal_length))
+    Eωk = q.forward(Eωr, axis=1)
+    if propz != 0.0:
+        kzsq = (grid.ω / pd.c)[:, None] ** 2 - (q.k ** 2)[None, :]
+        kz = np.sqrt(np.maximum(kzsq, 0.0))
+        Eωk = Eωk * np.exp(-1j * propz * (kz - (grid.ω / pd.c)[:, None]))
+    return np.ascontiguousarray(Eωk)
+
+
+class RadialProblem:
+    def __init__(self, Eω, grid, linop, transform, q, saveN=201):
+        self.Eω, self.grid, self.linop, self.transform, self.q = Eω, grid, linop, transform, q
+        self.saveN = saveN
+
+
+def prop_radial_args(gas, pressure, *, R, N, flength, λ0, λlims, trange, τfwhm, energy, w0,
+                     propz=0.0, focal_length=None, plasma="PPT", kerr=True, saveN=201,
+                     ppt_N=2 ** 16):
+    """Low-level radial set-up as in test/test_radial.jl and the freespace/radial example."""
+    grid = RealGrid(flength, λ0, λlims, trange)
+    q = QDHT(R, N)
+    nfun = pd.ref_index_fun(gas, pressure)
+    dens0 = pd.density(gas, pressure)
+    resp = []
+    if kerr:
+        resp.append(Kerr_field(pd.gamma3_gas(gas)))
+    if plasma:
+        ionpot = pd.ionisation_potential(gas)
+        rate = ionrate_fun_ADK(gas) if plasma == "ADK" else ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
+        resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, ionpot))
+    linop, _ = make_const_linop_radial(grid, q, nfun)
+    norm = const_norm_radial(grid, q, nfun)
+    transform = TransRadial(grid, q, resp, dens0, norm)
+    Eω = GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=propz, focal_length=focal_length)
+    return RadialProblem(Eω, grid, linop, transform, q, saveN)

@@ -204,6 +204,30 @@ def trans_mode_avg(t, Ew, z):
     return nl
 
 
+def trans_radial(t, Ew, z):
+    """(t::TransRadial)(nl, Eω, z) (NonlinearRHS.jl:466-474) for a field-resolved grid:
+    Ew is (Nω, Nr) in (ω, k) space."""
+    g, q = t.grid, t.q
+    Nw = Ew.shape[0]
+    Nwo = len(g.ωo)
+    Ewo = np.zeros((Nwo, Ew.shape[1]), dtype=np.complex128)
+    Ewo[:Nw] = ((Nwo - 1) / (Nw - 1)) * Ew
+    Et = np.fft.irfft(Ewo, g.No, axis=0)          # to_time! along dim 1
+    Er = q.inverse(Et, axis=1)                     # ldiv!(Eto, QDHT, Eto): k -> r
+    Pr = np.zeros_like(Er)
+    for i in range(Er.shape[1]):                   # Et_to_Pt! per radial column
+        Pr[:, i] = et_to_pt(Er[:, i], t.resp, t.density)
+    Pr = Pr * g.towin[:, None]
+    Pk = q.forward(Pr, axis=1)                     # mul!(Pto, QDHT, Pto): r -> k
+    Pwo = np.fft.rfft(Pk, axis=0)
+    nl = ((Nw - 1) / (Nwo - 1)) * Pwo[:Nw]          # to_freq!
+    return nl * t.output_factor()
+
+
+def rhs(t, Ew, z):
+    return trans_radial(t, Ew, z) if getattr(t, "kind", "") == "radial" else trans_mode_avg(t, Ew, z)
+
+
 # ------------------------------------------------------------------- RK45 (dopri)
 
 # Butcher tableau, nodes, weights and dense-output coefficients (dopri.jl:2-28)
@@ -367,7 +391,7 @@ def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rto
     max_dz = grid.zmax / 2 if max_dz is None else max_dz
     zgrid = np.linspace(z0, grid.zmax, saveN)
     res = RunResult()
-    f = lambda y, z: trans_mode_avg(t, y, z)
+    f = lambda y, z: rhs(t, y, z)
     s = PreconStepper(f, linop, Eω0, z0, init_dz, rtol=rtol, atol=atol, safety=safety,
                       max_dt=max_dz, min_dt=min_dz)
     saved = 0
@@ -377,13 +401,15 @@ def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rto
     def stepfun(yn, z, dz):
         # Luna.jl:366-372: window in frequency, back to time, window in time, forward
         nonlocal saved
-        y = yn * grid.ωwin
+        ww = grid.ωwin if yn.ndim == 1 else grid.ωwin[:, None]
+        tw = grid.twin if yn.ndim == 1 else grid.twin[:, None]
+        y = yn * ww
         if kind == "real":
-            Et = np.fft.irfft(y, grid.N) * grid.twin
-            y = np.fft.rfft(Et)
+            Et = np.fft.irfft(y, grid.N, axis=0) * tw
+            y = np.fft.rfft(Et, axis=0)
         else:
-            Et = np.fft.ifft(y) * grid.twin
-            y = np.fft.fft(Et)
+            Et = np.fft.ifft(y, axis=0) * tw
+            y = np.fft.fft(Et, axis=0)
         s.yn = y
         while saved < saveN and zgrid[saved] <= z:
             res.z.append(zgrid[saved])

@@ -217,3 +217,35 @@ def test_soliton_shift_golden_values():
     Et = np.fft.ifft(Ew) * np.exp(1j * p.grid.ω0 * p.grid.t)
     tpk = p.grid.t[np.argmax(np.abs(Et) ** 2)]
     assert abs(tpk / 6.079566076444579e-12 - 1) <= 1e-14
+
+
+# ---------------------------------------------------------------- test_radial.jl:3-65
+def test_radial_focus_matches_paraxial_gaussian_beam():
+    """Radially symmetric propagation through a focus (TransRadial + QDHT + Kerr + PPT
+    plasma at negligible energy): the fluence profile at ω0 after 0.6 m matches the
+    paraxial Gaussian-beam width to 1.5e-4 (test_radial.jl:64)."""
+    from luna_b200.radial import prop_radial_args
+    w0, L = 40e-6, 0.6
+    p = prop_radial_args("Ar", 1.2, R=4e-3, N=128, flength=L, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=1e-12, w0=w0, propz=-0.3)
+    res = uppe.run(p.transform, p.grid, p.linop, p.Eω)
+    g, q = p.grid, p.q
+    Er = q.inverse(res.Eω[-1], axis=1)
+    i0 = np.argmin(np.abs(g.ω - 2 * np.pi * pd.c / 800e-9))
+    lam0 = 2 * np.pi * pd.c / g.ω[i0]
+    w1 = w0 * np.sqrt(1 + (L / 2 * lam0 / (np.pi * w0 ** 2)) ** 2)
+    Ia = np.exp(-0.5 * (q.r / (w1 / 2)) ** 2) * (w0 / w1) ** 2
+    Ir = np.abs(Er[i0]) ** 2
+    Ir, Ia = Ir / Ir.max(), Ia / Ia.max()
+    assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < 1.5e-4
+
+
+def test_qdht_roundtrip_and_gaussian_pair():
+    from luna_b200.hankel import QDHT
+    q = QDHT(4e-3, 128)
+    assert np.abs(q.Mi @ q.Mf - np.eye(128)).max() < 1e-9
+    w = 0.5e-3
+    F = q.Mf @ np.exp(-q.r ** 2 / w ** 2)
+    Fa = w ** 2 / 2 * np.exp(-q.k ** 2 * w ** 2 / 4)
+    assert np.abs(F - Fa).max() / Fa.max() < 1e-12

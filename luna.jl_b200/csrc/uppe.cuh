@@ -356,15 +356,18 @@ __device__ __forceinline__ void plasma_pair(const LunaResp& r, bool act, int m, 
 // ------------------------------------------------------------------ the right-hand sides
 // load(k) -> cpx<double> input bin k (k < Nw); store(k, v) consumes output bin k (k < Nw).
 
-// field-resolved grid (RealGrid): to_time! / to_freq! with rfft semantics
-template <typename Rl, typename LoadF, typename StoreF>
-__device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
-    const int M = I.No / 2;
-    const int Nw = I.Nw;
+// field-resolved grid (RealGrid): to_time! / to_freq! with rfft semantics, in three
+// phases that the radial transform reuses per column.
+
+// to_time! (NonlinearRHS.jl:16-23): C2R pre-twiddle of the zero-padded spectrum and the
+// inverse transform. Returns the buffer holding slot m = samples (2m, 2m+1) in split
+// order with factor *P (unscaled: multiply by the pad scale / No).
+template <typename Rl, typename LoadF>
+__device__ __forceinline__ cpx<Rl>* c2r_to_time(Ws<Rl>& w, int M, int Nw, LoadF&& load, int* P) {
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
     cpx<Rl>* buf = w.main;
-    // C2R pre-twiddle: Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
+    // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
     for (int k = tid; k <= M / 2; k += T) {
         const int km = M - k;
         cpx<double> Xk = (k < Nw) ? load(k) : mk<double>(0, 0);
@@ -384,9 +387,17 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
         }
     }
     __syncthreads();
-    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);  // slot m: samples 2m, 2m+1
-    const int P = buf_split<Rl>(w.main_alt, M);
-    const double sc = I.in_scale;
+    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
+    *P = buf_split<Rl>(w.main_alt, M);
+    return x;
+}
+
+// Et_to_Pt! (NonlinearRHS.jl:121-126) and the time window, in place on the samples held
+// by x (split factor P); sc converts the stored samples to the field in V/m.
+template <typename Rl>
+__device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int M, int P, double sc) {
+    const int T = LUNA_BLOCK;
+    const int tid = threadIdx.x;
     int ip = -1, ir = -1;
     for (int i = 0; i < I.nresp; ++i) {
         if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
@@ -434,8 +445,17 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
         }
     }
     __syncthreads();
-    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, M, w.tw);
-    // R2C split: X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw
+}
+
+// to_freq! (NonlinearRHS.jl:39-45): forward transform of x (split factor of the buffer),
+// R2C split X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw,
+// multiply by outfac[k] and hand bin k to store.
+template <typename Rl, typename StoreF>
+__device__ __forceinline__ void r2c_to_freq(Ws<Rl>& w, cpx<Rl>* x, int M, int Nw, const cpx<double>* outfac,
+                                            StoreF&& store) {
+    const int T = LUNA_BLOCK;
+    const int tid = threadIdx.x;
+    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == w.main) ? w.main_alt : w.main) : nullptr, M, w.tw);
     for (int k = tid; k < Nw; k += T) {
         const int km = (M - k) & (M - 1);
         cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
@@ -447,9 +467,18 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
             cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
             X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
         }
-        store(k, X * ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k));
+        store(k, X * ldg(outfac + k));
     }
     __syncthreads();
+}
+
+template <typename Rl, typename LoadF, typename StoreF>
+__device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+    const int M = I.No / 2;
+    int P;
+    cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P);
+    pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
+    r2c_to_freq<Rl>(w, x, M, I.Nw, reinterpret_cast<const cpx<double>*>(I.outfac), store);
 }
 
 // envelope grid (EnvGrid): complex transforms with copy_scale_both! padding

@@ -146,6 +146,37 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
 void luna_b200_batch_destroy(luna_batch* b);
 
+/* ---------------------------------------------------------------- radial transform
+ * TransRadial (NonlinearRHS.jl:406-474) on a field-resolved grid with an order-0 QDHT of
+ * Nr points (Hankel.jl QDHT(R, N, dim=2), as built by Luna.setup for radial symmetry,
+ * Luna.jl:239-279). Fields are column-major Nw x Nr complex arrays (Julia's
+ * Matrix{ComplexF64}): element (ω, k) at k*Nw + ω. */
+typedef struct {
+    int Nr;                /* radial points QDHT.N                                        */
+    const double* Mi;      /* [Nr*Nr] row-major: E(r_n) = sum_m Mi[n*Nr+m] E(k_m)  (QDHT \ E) */
+    const double* Mf;      /* [Nr*Nr] row-major: P(k_m) = sum_n Mf[m*Nr+n] P(r_n)  (QDHT * P) */
+    const double* outfac;  /* [2*Nw*Nr] crop scale x ωwin (-iω) / (2 normfun(ω, k))        */
+} luna_radial_desc;
+
+typedef struct luna_radial_plan luna_radial_plan;
+
+/* Replaces the TransRadial constructor (NonlinearRHS.jl:430-458). The grid descriptor is
+ * that of one radial column (kind 0; its outfac is ignored, in_scale = pad scale / No);
+ * responses as for luna_b200_plan_create (Raman is not available here). */
+int luna_b200_radial_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
+                                 const luna_radial_desc* radial, int precision, luna_radial_plan** out);
+void luna_b200_radial_plan_destroy(luna_radial_plan* plan);
+/* (t::TransRadial)(nl, Eω, z) — NonlinearRHS.jl:466-474. Host arrays of Nw*Nr complex. */
+int luna_b200_radial_rhs(luna_radial_plan* plan, double* nl, const double* Ew, double z);
+int luna_b200_radial_rhs_device(luna_radial_plan* plan, double* nl_dev, const double* Ew_dev, double z,
+                                void* stream);
+/* RK45.solve_precon driven by Luna.run (Luna.jl:358-391) for a radial problem: linop and
+ * y_inout are Nw*Nr complex (LinearOps.make_const_linop(grid, q, nfun), LinearOps.jl:130-144),
+ * saves [saveN*2*Nw*Nr] doubles, steplog as for luna_b200_solve. Host memory. */
+int luna_b200_radial_solve(luna_radial_plan* plan, const double* linop, double* y_inout, double z0,
+                           double dz0, double zmax, const luna_solve_opts* opts, double* saves,
+                           double* steplog, luna_solve_stats* stats);
+
 /* Allocation-free variant of luna_b200_rhs_device. It has no counterpart in the reference:
  * it serves host programs that must not allocate device memory while they run (for
  * example a solver inside an allocator-managed runtime, or a process whose device memory

@@ -49,6 +49,10 @@ class RespDesc(ctypes.Structure):
                 ("hdt", c_double)]
 
 
+class RadialDesc(ctypes.Structure):
+    _fields_ = [("Nr", c_int), ("Mi", PD), ("Mf", PD), ("outfac", PD)]
+
+
 class SolveOpts(ctypes.Structure):
     _fields_ = [("rtol", c_double), ("atol", c_double), ("safety", c_double),
                 ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
@@ -67,6 +71,8 @@ EXPORTS = [
     "luna_b200_solve", "luna_b200_batch_create", "luna_b200_batch_upload", "luna_b200_batch_run",
     "luna_b200_batch_download", "luna_b200_batch_steplog", "luna_b200_batch_destroy",
     "luna_b200_last_error", "luna_b200_version", "luna_b200_rhs_device_noalloc",
+    "luna_b200_radial_plan_create", "luna_b200_radial_plan_destroy", "luna_b200_radial_rhs",
+    "luna_b200_radial_rhs_device", "luna_b200_radial_solve",
 ]
 
 _lib = None
@@ -105,6 +111,14 @@ def load():
     lib.luna_b200_batch_destroy.restype = None
     lib.luna_b200_rhs_device_noalloc.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p,
                                                  c_void_p]
+    lib.luna_b200_radial_plan_create.argtypes = [POINTER(GridDesc), POINTER(RespDesc), c_int,
+                                                 POINTER(RadialDesc), c_int, POINTER(c_void_p)]
+    lib.luna_b200_radial_plan_destroy.argtypes = [c_void_p]
+    lib.luna_b200_radial_plan_destroy.restype = None
+    lib.luna_b200_radial_rhs.argtypes = [c_void_p, PD, PD, c_double]
+    lib.luna_b200_radial_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
+    lib.luna_b200_radial_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
+                                           POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
     lib.luna_b200_last_error.restype = ctypes.c_char_p
     lib.luna_b200_version.restype = c_int
     _lib = lib

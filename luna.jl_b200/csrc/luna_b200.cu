@@ -4,14 +4,16 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstddef>
 #include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/luna_b200.h"
-#include "uppe.cuh"
+#include "radial.cuh"
 
 using namespace luna;
 
@@ -688,6 +690,314 @@ int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z
     if (st.status == ST_REPEAT_LIMIT) return fail(LUNA_REPEAT_LIMIT, "Reached limit for step repetition");
     if (st.status == ST_STEP_BUDGET) return fail(LUNA_STEP_BUDGET, "Step budget exhausted before zmax");
     return LUNA_OK;
+}
+
+// ===================================================================== radial transform
+}  // extern "C"
+
+struct luna_radial_plan {
+    int precision = 0;
+    int Nw = 0, Nr = 0;
+    luna_plan* col = nullptr;   // grid and responses of one radial column
+    LunaInst* d_col = nullptr;  // device copy of the column descriptor
+    std::vector<void*> allocs;
+    const double* Mi = nullptr;      // [Nr*Nr] row-major QDHT k -> r
+    const double* Mf = nullptr;      // [Nr*Nr] row-major QDHT r -> k
+    const double2* outfac = nullptr; // [Nw*Nr]
+    char* gscr = nullptr;            // per-column scratch when a column does not fit in shared memory
+    size_t gstride = 0;
+    int smem = 0;                    // dynamic shared memory of the column kernels
+    void* A = nullptr;               // [Nw*Nr] stage input, then column output
+    void* B = nullptr;               // [Nw*Nr] QDHT output
+    int* d_flags = nullptr;
+    double2* d_Ew = nullptr;
+    double2* d_nl = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+template <typename Rl>
+int rad_column_setup(luna_radial_plan* p) {
+    const LunaInst& I = p->col->proto;
+    const int maxs = max_smem_optin();
+    const size_t want = smem_wanted<Rl>(I);
+    p->smem = (int)std::min<size_t>(want, (size_t)maxs);
+    if (want > (size_t)maxs) {
+        p->gstride = align_up(gscr_bytes<Rl>(I), 256);
+        if (dalloc(p->allocs, &p->gscr, p->gstride * p->Nr)) return LUNA_ERR_CUDA;
+    }
+    CK(cudaFuncSetAttribute(rad_column_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
+    return LUNA_OK;
+}
+
+int rad_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
+
+// Pk or Er = X * M^T along the radial index of the 2Nw x Nr real view.
+int rad_qdht(luna_radial_plan* p, const void* X, const double* M, void* Y, const RadState* st, cudaStream_t s) {
+    const int rows = 2 * p->Nw;
+    dim3 g((rows + RG_BM - 1) / RG_BM, (p->Nr + RG_BN - 1) / RG_BN);
+    rad_gemm_f64<<<g, 256, 0, s>>>((const double*)X, rows, rows, M, (double*)Y, p->Nr, st);
+    return LUNA_OK;
+}
+
+// One transform evaluation: stage input already in A; column output back in A; the
+// QDHT r -> k result in B.
+template <typename Rl>
+int rad_transform(luna_radial_plan* p, const TwTab<Rl>& tw, RadState* st, int* flags, cudaStream_t s) {
+    rad_qdht(p, p->A, p->Mi, p->B, st, s);
+    rad_column_kernel<Rl><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(p->d_col, (const cpx<Rl>*)p->B, (cpx<Rl>*)p->A, tw,
+                                                            p->smem, p->gscr, p->gstride, st, flags);
+    rad_qdht(p, p->A, p->Mf, p->B, st, s);
+    return LUNA_OK;
+}
+
+template <typename Rl>
+int rad_rhs(luna_radial_plan* p, const double2* Ew, double2* nl, cudaStream_t s) {
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+    const TwTab<Rl>& t = *reinterpret_cast<const TwTab<Rl>*>(std::is_same<Rl, double>::value ? (const void*)&tw.d : (const void*)&tw.f);
+    RadArgs a{p->Nw, p->Nr, nullptr, p->outfac, nullptr, nullptr};
+    const size_t n = (size_t)p->Nw * p->Nr;
+    CK(cudaMemsetAsync(p->d_flags, 0, sizeof(int), s));
+    rad_stage_kernel<Rl, double><<<rad_grid(n), 256, 0, s>>>(a, -1, Ew, (cpx<Rl>*)p->A);
+    rad_transform<Rl>(p, t, nullptr, p->d_flags, s);
+    rad_store_kernel<Rl, double><<<rad_grid(n), 256, 0, s>>>(a, -1, (const cpx<Rl>*)p->B, nl);
+    CK(cudaGetLastError());
+    return LUNA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, int nresp,
+                                 const luna_radial_desc* rd, int precision, luna_radial_plan** out) {
+    if (!g || !rd || !out || !rd->Mi || !rd->Mf || !rd->outfac)
+        return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: null argument");
+    if (g->kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: only field-resolved (RealGrid) radial transforms");
+    if (rd->Nr < 1 || rd->Nr > 4096) return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: Nr must be in 1..4096");
+    if (precision != LUNA_PREC_FP64) return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: precision not available for the radial transform");
+    for (int i = 0; i < nresp; ++i)
+        if (resps[i].kind == LUNA_RESP_RAMAN)
+            return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Raman response not available for the radial transform");
+    // the column plan: grid and responses; its output factor is unused (the radial one
+    // is applied after the QDHT)
+    std::vector<double> ones(2 * (size_t)g->Nw, 0.0);
+    for (int k = 0; k < g->Nw; ++k) ones[2 * k] = 1.0;
+    luna_grid_desc gc = *g;
+    gc.outfac = ones.data();
+    luna_plan* col = nullptr;
+    int rc = luna_b200_plan_create(&gc, resps, nresp, precision, &col);
+    if (rc) return rc;
+    luna_radial_plan* p = new luna_radial_plan();
+    p->precision = precision;
+    p->Nw = g->Nw;
+    p->Nr = rd->Nr;
+    p->col = col;
+    auto bail = [&](int code) {
+        free_all(p->allocs);
+        luna_b200_plan_destroy(p->col);
+        delete p;
+        return code;
+    };
+    const size_t n = (size_t)p->Nw * p->Nr, nn = (size_t)p->Nr * p->Nr;
+    const double* tmp = nullptr;
+    if (upload(p->allocs, rd->Mi, nn, &p->Mi) || upload(p->allocs, rd->Mf, nn, &p->Mf) ||
+        upload(p->allocs, rd->outfac, 2 * n, &tmp))
+        return bail(LUNA_ERR_CUDA);
+    p->outfac = (const double2*)tmp;
+    const size_t cb = sizeof(double2);
+    if (dalloc(p->allocs, &p->A, cb * n) || dalloc(p->allocs, &p->B, cb * n) || dalloc(p->allocs, &p->d_flags, sizeof(int)) ||
+        dalloc(p->allocs, &p->d_col, sizeof(LunaInst)))
+        return bail(LUNA_ERR_CUDA);
+    if (cudaMemcpy(p->d_col, &col->proto, sizeof(LunaInst), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(LUNA_ERR_CUDA, "radial_plan_create: copy of the column descriptor failed"));
+    rc = rad_column_setup<double>(p);
+    if (rc) return bail(rc);
+    *out = p;
+    return LUNA_OK;
+}
+
+void luna_b200_radial_plan_destroy(luna_radial_plan* p) {
+    if (!p) return;
+    if (p->stream) cudaStreamDestroy(p->stream);
+    free_all(p->allocs);
+    luna_b200_plan_destroy(p->col);
+    delete p;
+}
+
+int luna_b200_radial_rhs_device(luna_radial_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
+    (void)z;  // constant density and normalisation
+    if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "radial_rhs_device: null argument");
+    return rad_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+}
+
+int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, double z) {
+    (void)z;
+    if (!p || !nl || !Ew) return fail(LUNA_ERR_BAD_ARG, "radial_rhs: null argument");
+    const size_t bytes = sizeof(double2) * p->Nw * p->Nr;
+    if (!p->d_Ew) {
+        if (dalloc(p->allocs, &p->d_Ew, bytes) || dalloc(p->allocs, &p->d_nl, bytes)) return LUNA_ERR_CUDA;
+        CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    }
+    CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
+    int rc = rad_rhs<double>(p, p->d_Ew, p->d_nl, p->stream);
+    if (rc) return rc;
+    int fl = 0;
+    CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(&fl, p->d_flags, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    if (fl & (1 << ST_FIELD_ABOVE_EMAX)) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
+    return LUNA_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Device buffers of one radial solve.
+struct RadSolve {
+    std::vector<void*> allocs;
+    double2 *L = nullptr, *y = nullptr, *yn = nullptr, *e1 = nullptr, *saves = nullptr;
+    void* k[7] = {};
+    void** d_k = nullptr;
+    double *zsave = nullptr, *steplog = nullptr, *replay = nullptr, *partial = nullptr;
+    RadState* st = nullptr;
+    LunaInst* opt = nullptr;
+    int* h_fin = nullptr;  // pinned
+    ~RadSolve() {
+        free_all(allocs);
+        if (h_fin) cudaFreeHost(h_fin);
+    }
+};
+
+template <typename Rl, typename Kt>
+int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double z0, double dz0, double zmax,
+              const luna_solve_opts* o, double* saves, double* steplog, luna_solve_stats* stats) {
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+    const TwTab<Rl>& t = *reinterpret_cast<const TwTab<Rl>*>(std::is_same<Rl, double>::value ? (const void*)&tw.d : (const void*)&tw.f);
+    const size_t n = (size_t)p->Nw * p->Nr;
+    const size_t cb = sizeof(double2);
+    RadSolve S;
+    if (dalloc(S.allocs, &S.L, cb * n) || dalloc(S.allocs, &S.y, cb * n) || dalloc(S.allocs, &S.yn, cb * n) ||
+        dalloc(S.allocs, &S.e1, cb * n) || dalloc(S.allocs, &S.st, sizeof(RadState)) ||
+        dalloc(S.allocs, &S.opt, sizeof(LunaInst)) || dalloc(S.allocs, &S.d_k, sizeof(void*) * 7))
+        return LUNA_ERR_CUDA;
+    for (int j = 0; j < 7; ++j)
+        if (dalloc(S.allocs, &S.k[j], sizeof(cpx<Kt>) * n)) return LUNA_ERR_CUDA;
+    const int nblk = rad_grid(n);
+    if (dalloc(S.allocs, &S.partial, sizeof(double) * 3 * nblk)) return LUNA_ERR_CUDA;
+    if (o->saveN > 0) {
+        if (dalloc(S.allocs, &S.saves, cb * n * o->saveN) || dalloc(S.allocs, &S.zsave, sizeof(double) * o->saveN))
+            return LUNA_ERR_CUDA;
+        CK(cudaMemcpy(S.zsave, o->zsave, sizeof(double) * o->saveN, cudaMemcpyHostToDevice));
+    }
+    if (o->steplog_cap > 0 && dalloc(S.allocs, &S.steplog, sizeof(double) * 4 * o->steplog_cap)) return LUNA_ERR_CUDA;
+    if (o->replay && o->nreplay > 0) {
+        if (dalloc(S.allocs, &S.replay, sizeof(double) * 2 * o->nreplay)) return LUNA_ERR_CUDA;
+        CK(cudaMemcpy(S.replay, o->replay, sizeof(double) * 2 * o->nreplay, cudaMemcpyHostToDevice));
+    }
+    CK(cudaMallocHost(&S.h_fin, sizeof(int)));
+    LunaInst I{};
+    memset(&I, 0, sizeof(I));
+    I.z0 = z0;
+    I.dz0 = dz0;
+    I.zmax = zmax;
+    I.rtol = o->rtol;
+    I.atol = o->atol;
+    I.safety = o->safety;
+    I.max_dt = o->max_dt;
+    I.min_dt = o->min_dt;
+    I.repeat_limit = o->repeat_limit;
+    I.max_steps = o->max_steps;
+    I.saveN = o->saveN;
+    I.zsave = S.zsave;
+    I.saves = S.saves;
+    I.steplog = S.steplog;
+    I.steplog_cap = S.steplog ? o->steplog_cap : 0;
+    I.replay = S.replay;
+    I.nreplay = S.replay ? o->nreplay : 0;
+    CK(cudaMemcpy(S.opt, &I, sizeof(LunaInst), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.L, linop, cb * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.y, y_inout, cb * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.yn, y_inout, cb * n, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(S.d_k, S.k, sizeof(void*) * 7, cudaMemcpyHostToDevice));
+    if (!p->stream) CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    cudaStream_t s = p->stream;
+    RadArgs a{p->Nw, p->Nr, S.L, p->outfac, S.e1, S.st};
+    const int eg = rad_grid(n);
+    int* flags_dev = (int*)((char*)S.st + offsetof(RadState, flags));
+    const int* fin_dev = (const int*)((char*)S.st + offsetof(RadState, finished));
+    rad_init_kernel<<<1, 32, 0, s>>>(S.st, S.opt, S.y, S.yn, S.d_k);
+    // k1 = f(y0)
+    rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, nullptr, (cpx<Rl>*)p->A);
+    rad_transform<Rl>(p, t, S.st, flags_dev, s);
+    rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, (const cpx<Rl>*)p->B, nullptr);
+    CK(cudaGetLastError());
+    // steps are enqueued in chunks; the loop state on the device says when to stop
+    int chunk = 4;
+    long long enq = 0;
+    const long long cap = (o->max_steps > 0) ? o->max_steps : (long long)1 << 40;
+    while (true) {
+        for (int q = 0; q < chunk; ++q) {
+            rad_begin_kernel<<<1, 32, 0, s>>>(S.st, S.opt);
+            for (int sg = 0; sg < 6; ++sg) {
+                rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, nullptr, (cpx<Rl>*)p->A);
+                rad_transform<Rl>(p, t, S.st, flags_dev, s);
+                rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, (const cpx<Rl>*)p->B, nullptr);
+            }
+            rad_combine_kernel<Kt><<<nblk, 256, 0, s>>>(a, S.partial);
+            rad_control_kernel<<<1, 32, 0, s>>>(S.st, S.opt, S.partial, nblk);
+            rad_post_kernel<Rl, Kt><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(a, p->d_col, S.opt, t, p->smem, p->gscr, p->gstride);
+        }
+        CK(cudaGetLastError());
+        enq += chunk;
+        CK(cudaMemcpyAsync(S.h_fin, fin_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (*S.h_fin) break;
+        if (enq > cap + 1) return fail(LUNA_ERR_CUDA, "radial_solve: loop did not end after max_steps");
+        chunk = std::min(chunk * 2, 64);
+    }
+    // results
+    RadState hs;
+    LunaInst ho;
+    CK(cudaMemcpy(&hs, S.st, sizeof(RadState), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&ho, S.opt, sizeof(LunaInst), cudaMemcpyDeviceToHost));
+    if (saves && o->saveN > 0 && hs.nsaved > 0) CK(cudaMemcpy(saves, S.saves, cb * n * hs.nsaved, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(y_inout, hs.yn, cb * n, cudaMemcpyDeviceToHost));
+    if (steplog && S.steplog) CK(cudaMemcpy(steplog, S.steplog, sizeof(double) * 4 * o->steplog_cap, cudaMemcpyDeviceToHost));
+    luna_solve_stats r{};
+    r.status = hs.c.status;
+    r.nsaved = hs.nsaved;
+    r.steps = hs.c.steps;
+    r.accepted = ho.accepted;
+    r.rejected = ho.rejected;
+    r.nrhs = 1 + 6 * hs.c.steps;
+    r.z = hs.c.tn;
+    r.dz = hs.c.dtn;
+    if (stats) *stats = r;
+    if (r.status == ST_FIELD_ABOVE_EMAX) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
+    if (r.status == ST_REPEAT_LIMIT) return fail(LUNA_REPEAT_LIMIT, "Reached limit for step repetition");
+    if (r.status == ST_STEP_BUDGET) return fail(LUNA_STEP_BUDGET, "Step budget exhausted before zmax");
+    return LUNA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int luna_b200_radial_solve(luna_radial_plan* p, const double* linop, double* y_inout, double z0, double dz0,
+                           double zmax, const luna_solve_opts* opts, double* saves, double* steplog,
+                           luna_solve_stats* stats) {
+    if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "radial_solve: null argument");
+    if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "radial_solve: save points missing");
+    return rad_solve<double, double>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
 }
 
 // ---------------------------------------------------------------- allocation-free RHS

@@ -80,7 +80,8 @@ __host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
 #define LUNA_SMALL_BYTES 2048
 
 template <typename Rl>
-__device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w, const TwTab<Rl>& tw) {
+__device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w, const TwTab<Rl>& tw,
+                        void* gscr = nullptr) {
     w.red = reinterpret_cast<double*>(smem);
     w.tot = w.red + 3 * LUNA_WARPS;
     w.edge = w.tot + 3 * LUNA_WARPS;
@@ -88,7 +89,7 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
     w.tw = tw;
     size_t off = LUNA_SMALL_BYTES;
     const size_t c = sizeof(cpx<Rl>);
-    char* g = reinterpret_cast<char*>(I.gscr);
+    char* g = reinterpret_cast<char*>(gscr ? gscr : I.gscr);
     size_t goff = 0;
     const int Mm = main_len(I);
     size_t mb = align_up((size_t)Mm * c, 256);
@@ -449,10 +450,9 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
 
 // to_freq! (NonlinearRHS.jl:39-45): forward transform of x (split factor of the buffer),
 // R2C split X[k] = 1/2 (Z[k] + conj Z[M-k]) - i/2 W^k (Z[k] - conj Z[M-k]), crop to Nw,
-// multiply by outfac[k] and hand bin k to store.
+// and hand bin k to store.
 template <typename Rl, typename StoreF>
-__device__ __forceinline__ void r2c_to_freq(Ws<Rl>& w, cpx<Rl>* x, int M, int Nw, const cpx<double>* outfac,
-                                            StoreF&& store) {
+__device__ __forceinline__ void r2c_to_freq(Ws<Rl>& w, cpx<Rl>* x, int M, int Nw, StoreF&& store) {
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
     cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == w.main) ? w.main_alt : w.main) : nullptr, M, w.tw);
@@ -467,7 +467,7 @@ __device__ __forceinline__ void r2c_to_freq(Ws<Rl>& w, cpx<Rl>* x, int M, int Nw
             cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
             X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
         }
-        store(k, X * ldg(outfac + k));
+        store(k, X);
     }
     __syncthreads();
 }
@@ -478,7 +478,8 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
     int P;
     cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P);
     pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
-    r2c_to_freq<Rl>(w, x, M, I.Nw, reinterpret_cast<const cpx<double>*>(I.outfac), store);
+    const cpx<double>* of = reinterpret_cast<const cpx<double>*>(I.outfac);
+    r2c_to_freq<Rl>(w, x, M, I.Nw, [&](int k, cpx<double> X) { store(k, X * ldg(of + k)); });
 }
 
 // envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
@@ -691,12 +692,11 @@ __device__ __forceinline__ cpx<double> inv_fac(cpx<Rl> f) {
 // Dense output (RK45.jl:249-268) into row `out`; after an accepted step ks[1] holds k7,
 // so the k1 and k7 coefficients both apply to that buffer.
 template <typename Rl, typename Kt>
-__device__ void interpolate_row(const LunaInst& I, const Ctl& c, double ti, void* const* k,
+__device__ void interpolate_row(int Nw, const double2* linop, const Ctl& c, double ti, void* const* k,
                                 const double2* py, const double2* pyn, double2* out) {
-    const int Nw = I.Nw;
     const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
     const cpx<double>* yn = reinterpret_cast<const cpx<double>*>(pyn);
-    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
+    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(linop);
     cpx<double>* o = reinterpret_cast<cpx<double>*>(out);
     if (ti == c.t) {
         for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) o[i] = y[i];
@@ -726,6 +726,67 @@ __device__ void interpolate_row(const LunaInst& I, const Ctl& c, double ti, void
         yi = yi + scale(b[6], k1);
         cpx<double> v = y[i] + scale(c.dt, yi);
         o[i] = v * cvt<double>(expLd<double>(L[i], d));
+    }
+}
+
+// Weak error norm, PI step control, step limits and step bookkeeping after the stage
+// evaluations (RK45.jl:167-192, 343-354, 374-406); one thread. sy, syn and se are the
+// sums of |y|^2, |yn|^2 and |yerr|^2; flags are the status bits raised by the RHS.
+__device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, double syn, double se, int flags) {
+    const double errwt = fmax(fmax(sqrt(sy), sqrt(syn)), I.atol);
+    const double err = sqrt(se) / I.rtol / errwt;
+    c.err = err;
+    int ok = err <= 1.0;
+    // stepcontrolPI! (RK45.jl:374-396)
+    const double b1 = 3.0 / 5 / 5, b2 = -1.0 / 5 / 5, eps = 0.8;
+    if (ok) {
+        if (c.errlast == 0) c.errlast = err;
+        double fac = (err == 0) ? 1.5 : I.safety * pow(eps / err, b1) * pow(eps / c.errlast, b2);
+        c.dtn = fac * c.dt;
+        c.errlast = err;
+    } else {
+        if (!isfinite(err)) c.dtn = c.dt / 2;
+        else c.dtn = c.dt * fmax(0.1, I.safety * pow(err, -1.0 / 5));
+    }
+    // steplims! (RK45.jl:399-406)
+    if (c.dtn > I.max_dt) c.dtn = I.max_dt;
+    else if (c.dtn < I.min_dt) {
+        c.dtn = I.min_dt;
+        ok = 1;
+    }
+    // replay mode: follow a given step sequence (dt of the next step, accept flag)
+    if (I.replay && c.steps < I.nreplay) {
+        ok = I.replay[2 * c.steps + 1] != 0.0;
+        if (c.steps + 1 < I.nreplay) c.dtn = I.replay[2 * (c.steps + 1)];
+    }
+    c.ok = ok;
+    if (ok) c.tn = c.t + c.dt;
+    c.steps += 1;
+    const long long si = c.steps - 1;
+    if (I.steplog && si < I.steplog_cap) {
+        I.steplog[4 * si + 0] = c.t;
+        I.steplog[4 * si + 1] = c.dt;
+        I.steplog[4 * si + 2] = err;
+        I.steplog[4 * si + 3] = (double)ok;
+    }
+    if (ok) {
+        c.repeated = 0;
+        I.accepted += 1;
+    } else {
+        c.repeated += 1;
+        I.rejected += 1;
+        if (c.repeated > I.repeat_limit) {
+            c.status = ST_REPEAT_LIMIT;
+            c.done = 1;
+        }
+    }
+    if (flags & (1 << ST_FIELD_ABOVE_EMAX)) {
+        c.status = ST_FIELD_ABOVE_EMAX;
+        c.done = 1;
+    }
+    if (I.max_steps > 0 && c.steps >= I.max_steps && !c.done) {
+        c.status = ST_STEP_BUDGET;
+        c.done = 1;
     }
 }
 
@@ -850,63 +911,7 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
             }
         }
         block_sum3(sy, syn, se, w.red);
-        if (tid == 0) {
-            const double errwt = fmax(fmax(sqrt(sy), sqrt(syn)), I.atol);
-            const double err = sqrt(se) / I.rtol / errwt;
-            c.err = err;
-            int ok = err <= 1.0;
-            // stepcontrolPI! (RK45.jl:374-396)
-            const double b1 = 3.0 / 5 / 5, b2 = -1.0 / 5 / 5, eps = 0.8;
-            if (ok) {
-                if (c.errlast == 0) c.errlast = err;
-                double fac = (err == 0) ? 1.5 : I.safety * pow(eps / err, b1) * pow(eps / c.errlast, b2);
-                c.dtn = fac * c.dt;
-                c.errlast = err;
-            } else {
-                if (!isfinite(err)) c.dtn = c.dt / 2;
-                else c.dtn = c.dt * fmax(0.1, I.safety * pow(err, -1.0 / 5));
-            }
-            // steplims! (RK45.jl:399-406)
-            if (c.dtn > I.max_dt) c.dtn = I.max_dt;
-            else if (c.dtn < I.min_dt) {
-                c.dtn = I.min_dt;
-                ok = 1;
-            }
-            // replay mode: follow a given step sequence (dt of the next step, accept flag)
-            if (I.replay && c.steps < I.nreplay) {
-                ok = I.replay[2 * c.steps + 1] != 0.0;
-                if (c.steps + 1 < I.nreplay) c.dtn = I.replay[2 * (c.steps + 1)];
-            }
-            c.ok = ok;
-            if (ok) c.tn = c.t + c.dt;
-            c.steps += 1;
-            const long long si = c.steps - 1;
-            if (I.steplog && si < I.steplog_cap) {
-                I.steplog[4 * si + 0] = c.t;
-                I.steplog[4 * si + 1] = c.dt;
-                I.steplog[4 * si + 2] = err;
-                I.steplog[4 * si + 3] = (double)ok;
-            }
-            if (ok) {
-                c.repeated = 0;
-                I.accepted += 1;
-            } else {
-                c.repeated += 1;
-                I.rejected += 1;
-                if (c.repeated > I.repeat_limit) {
-                    c.status = ST_REPEAT_LIMIT;
-                    c.done = 1;
-                }
-            }
-            if (*w.flag & (1 << ST_FIELD_ABOVE_EMAX)) {
-                c.status = ST_FIELD_ABOVE_EMAX;
-                c.done = 1;
-            }
-            if (I.max_steps > 0 && c.steps >= I.max_steps && !c.done) {
-                c.status = ST_STEP_BUDGET;
-                c.done = 1;
-            }
-        }
+        if (tid == 0) control_step(I, c, sy, syn, se, *w.flag);
         __syncthreads();
         if (c.done && c.status != 0) break;
         if (c.ok) {
@@ -922,7 +927,7 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
             stepfun_filter<Rl>(I, w, pyn, I.e1);
             // GridCondition saves (Output.jl:65-82, 490-502)
             while (saved < I.saveN && I.zsave[saved] <= c.tn) {
-                interpolate_row<Rl, Kt>(I, c, I.zsave[saved], k, py, pyn, I.saves + (size_t)saved * Nw);
+                interpolate_row<Rl, Kt>(Nw, I.linop, c, I.zsave[saved], k, py, pyn, I.saves + (size_t)saved * Nw);
                 ++saved;
             }
             swap_y = true;

@@ -21,6 +21,56 @@ def _c128(a):
     return np.ascontiguousarray(a, dtype=np.complex128)
 
 
+def resp_descs(resp, rho, keep):
+    """C-ABI descriptors of the responses (Et_to_Pt! order) at density ``rho``; arrays the
+    descriptors point to are appended to ``keep``."""
+    rds = []
+    for r in resp:
+        d = _lib.RespDesc()
+        if r.kind == "kerr_field":
+            d.kind = _lib.RESP_KERR_FIELD
+            d.coef = rho * pd.eps_0 * r.γ3
+        elif r.kind == "kerr_env":
+            d.kind = _lib.RESP_KERR_ENV
+            d.coef = rho * pd.eps_0 * r.γ3
+        elif r.kind == "plasma":
+            d.coef = rho
+            d.ionpot = r.ionpot
+            d.dt = r.δt
+            d.preionfrac = r.preionfrac
+            d.eratio = pd.e_ratio
+            rf = r.ratefunc
+            if rf.kind == "adk":
+                d.kind = _lib.RESP_PLASMA_ADK
+                d.adk_pre = rf.w_p * rf.cn_sq
+                d.adk_a = 4 * rf.w_p / rf.w_t_prefac
+                d.adk_b = 4 / 3 * rf.w_p / rf.w_t_prefac
+                d.adk_pw = 2 * rf.nstar - 1
+                d.adk_thr = rf.thr
+            else:
+                d.kind = _lib.RESP_PLASMA_PPT
+                x, y, D = _f64(rf.x), _f64(rf.y), _f64(rf.D)
+                keep += [x, y, D]
+                d.spl_x, d.spl_y, d.spl_D = _lib.dptr(x), _lib.dptr(y), _lib.dptr(D)
+                d.spl_n = len(x)
+        elif r.kind in ("raman_field", "raman_env"):
+            d.kind = _lib.RESP_RAMAN
+            d.coef = rho
+            resp = r.r
+            hpre = _f64(np.stack(resp.hpres))
+            tau2 = _f64(resp.tau2s(rho))
+            hwin, htt = _f64(resp.w), _f64(resp.tt)
+            keep += [hpre, tau2, hwin, htt]
+            d.ncomp = len(resp.hpres)
+            d.hpre, d.tau2 = _lib.dptr(hpre), _lib.dptr(tau2)
+            d.hwin, d.htt = _lib.dptr(hwin), _lib.dptr(htt)
+            d.hdt = r.dt
+        else:
+            raise ValueError(f"unsupported response {r.kind}")
+        rds.append(d)
+    return rds
+
+
 class Plan:
     """Owns one ``luna_plan`` (device copy of the grid, normalisation and responses)."""
 
@@ -71,51 +121,7 @@ class Plan:
         gd.outfac = _lib.dptr(outfac.view(np.float64))
         gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
         gd.in_scale = pad / No / (nlscale * math.sqrt(t.aeff))
-        rds = []
-        rho = t.density
-        for r in t.resp:
-            d = _lib.RespDesc()
-            if r.kind == "kerr_field":
-                d.kind = _lib.RESP_KERR_FIELD
-                d.coef = rho * pd.eps_0 * r.γ3
-            elif r.kind == "kerr_env":
-                d.kind = _lib.RESP_KERR_ENV
-                d.coef = rho * pd.eps_0 * r.γ3
-            elif r.kind == "plasma":
-                d.coef = rho
-                d.ionpot = r.ionpot
-                d.dt = r.δt
-                d.preionfrac = r.preionfrac
-                d.eratio = pd.e_ratio
-                rf = r.ratefunc
-                if rf.kind == "adk":
-                    d.kind = _lib.RESP_PLASMA_ADK
-                    d.adk_pre = rf.w_p * rf.cn_sq
-                    d.adk_a = 4 * rf.w_p / rf.w_t_prefac
-                    d.adk_b = 4 / 3 * rf.w_p / rf.w_t_prefac
-                    d.adk_pw = 2 * rf.nstar - 1
-                    d.adk_thr = rf.thr
-                else:
-                    d.kind = _lib.RESP_PLASMA_PPT
-                    x, y, D = _f64(rf.x), _f64(rf.y), _f64(rf.D)
-                    keep += [x, y, D]
-                    d.spl_x, d.spl_y, d.spl_D = _lib.dptr(x), _lib.dptr(y), _lib.dptr(D)
-                    d.spl_n = len(x)
-            elif r.kind in ("raman_field", "raman_env"):
-                d.kind = _lib.RESP_RAMAN
-                d.coef = rho
-                resp = r.r
-                hpre = _f64(np.stack(resp.hpres))
-                tau2 = _f64(resp.tau2s(rho))
-                hwin, htt = _f64(resp.w), _f64(resp.tt)
-                keep += [hpre, tau2, hwin, htt]
-                d.ncomp = len(resp.hpres)
-                d.hpre, d.tau2 = _lib.dptr(hpre), _lib.dptr(tau2)
-                d.hwin, d.htt = _lib.dptr(hwin), _lib.dptr(htt)
-                d.hdt = r.dt
-            else:
-                raise ValueError(f"unsupported response {r.kind}")
-            rds.append(d)
+        rds = resp_descs(t.resp, t.density, keep)
         return cls(gd, rds, keep, precision, Nw)
 
     def rhs(self, nl, Eω, z=0.0):

@@ -1,0 +1,125 @@
+"""Radial transform (TransRadial + QDHT) on the GPU against the FP64 oracle.
+
+Cases follow test/test_radial.jl: argon, a focused Gaussian beam, Kerr plus PPT or ADK
+plasma, at energies where the plasma term is a visible part of the response (20 µJ: ~0.3%
+with PPT; 50 µJ: ~6% with ADK, ~97% with PPT).
+"""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import numpy as np
+import pytest
+
+from luna_b200 import _lib
+from luna_b200 import physdata as pd
+from luna_b200 import radial_plan
+from luna_b200.radial import prop_radial_args
+from oracle import uppe
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _problem(energy, plasma, flength=0.01, N=64, saveN=5):
+    return prop_radial_args("Ar", 1.2, R=1e-3, N=N, flength=flength, λ0=800e-9,
+                            λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                            energy=energy, w0=40e-6, propz=0.0, plasma=plasma, saveN=saveN)
+
+
+@pytest.mark.parametrize("energy,plasma", [(20e-6, "PPT"), (50e-6, "PPT"), (50e-6, "ADK"),
+                                           (20e-6, False)])
+def test_radial_rhs_fp64_matches_oracle(energy, plasma):
+    """(t::TransRadial)(nl, Eω, z) through the C ABI vs the oracle (NonlinearRHS.jl:466-474).
+    The device applies both QDHT products on the frequency side (they commute with the time
+    transforms); the difference is rounding only."""
+    p = _problem(energy, plasma)
+    rng = np.random.default_rng(3)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    nl = np.zeros_like(Ew)
+    p.transform(nl, Ew, 0.0)
+    ref = uppe.trans_radial(p.transform, Ew, 0.0)
+    tol = 1e-11 if plasma else 1e-12
+    assert _rel(nl, ref) < tol, _rel(nl, ref)
+    # the device-pointer entry point gives the same numbers
+    torch = pytest.importorskip("torch")
+    lib = _lib.load()
+    plan = p.transform.plan()
+    Ec = np.ascontiguousarray(Ew.T)
+    dE = torch.from_numpy(Ec.view(np.float64).copy()).cuda()
+    out = torch.zeros_like(dE)
+    s = torch.cuda.current_stream()
+    _lib.check(lib.luna_b200_radial_rhs_device(plan.handle, _lib.ctypes.c_void_p(out.data_ptr()),
+                                               _lib.ctypes.c_void_p(dE.data_ptr()), 0.0,
+                                               _lib.ctypes.c_void_p(s.cuda_stream)))
+    torch.cuda.synchronize()
+    dev = out.cpu().numpy().view(np.complex128).reshape(Ec.shape).T
+    assert np.array_equal(dev, nl)
+
+
+@pytest.mark.parametrize("energy,plasma,flength", [(20e-6, "PPT", 0.03), (50e-6, "ADK", 0.01)])
+def test_radial_solve_fp64_same_steps_as_oracle(energy, plasma, flength):
+    """RK45.solve_precon + Luna.run on the radial problem: the same accepted-step sequence
+    as the oracle and every saved field within 1e-10."""
+    p = _problem(energy, plasma, flength=flength)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    r = radial_plan.run(p, steplog_cap=1000)
+    assert r.status == 0 and r.nsaved == 5
+    assert r.steps == ores.steps
+    acc = r.steplog[r.steplog[:, 3] == 1]
+    oacc = np.array(ores.accepted)
+    assert len(acc) == len(oacc)
+    # the error estimate is a difference of nearly equal sums, so rounding moves the
+    # controller's step sizes at the 1e-7 level (as for the capillary cases with plasma)
+    np.testing.assert_allclose(acc[:, 1], oacc[:, 1], rtol=1e-6)
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+
+
+def test_radial_solve_replay_matches_oracle():
+    """Following the oracle's step sequence exactly (replay), the saved fields agree to
+    1e-10 at every save point."""
+    p = _problem(50e-6, "PPT", flength=0.01)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    r = radial_plan.run(p, replay=replay)
+    assert r.nsaved == 5
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+
+
+def test_radial_focus_matches_paraxial_gaussian_beam_on_gpu():
+    """test_radial.jl:3-65 on the device: after 0.6 m through a focus the fluence profile at
+    ω0 matches the paraxial Gaussian-beam width to 1.5e-4."""
+    w0, L = 40e-6, 0.6
+    p = prop_radial_args("Ar", 1.2, R=4e-3, N=128, flength=L, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=1e-12, w0=w0, propz=-0.3)
+    r = radial_plan.run(p)
+    assert r.status == 0
+    g, q = p.grid, p.q
+    Er = q.inverse(r.Eω[-1], axis=1)
+    i0 = np.argmin(np.abs(g.ω - 2 * np.pi * pd.c / 800e-9))
+    lam0 = 2 * np.pi * pd.c / g.ω[i0]
+    w1 = w0 * np.sqrt(1 + (L / 2 * lam0 / (np.pi * w0 ** 2)) ** 2)
+    Ia = np.exp(-0.5 * (q.r / (w1 / 2)) ** 2) * (w0 / w1) ** 2
+    Ir = np.abs(Er[i0]) ** 2
+    Ir, Ia = Ir / Ir.max(), Ia / Ia.max()
+    assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < 1.5e-4
+
+
+def test_radial_plan_rejects_raman_and_envelope():
+    from luna_b200 import raman
+    from luna_b200.nonlinear import RamanPolarField
+    from luna_b200.radial import TransRadial
+    p = _problem(20e-6, "PPT")
+    t = p.transform
+    rr = raman.raman_response(t.grid.to, "N2")
+    bad = TransRadial(t.grid, t.q, list(t.resp) + [RamanPolarField(t.grid.to, rr)],
+                      t.density, t.normfun)
+    with pytest.raises(_lib.LunaError) as e:
+        radial_plan.RadialPlan.from_transform(bad)
+    assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED

@@ -35,6 +35,7 @@ extern "C" {
 #define LUNA_REPEAT_LIMIT 2     /* more than repeat_limit rejected steps (RK45.jl:72-76) */
 #define LUNA_NONFINITE 3
 #define LUNA_STEP_BUDGET 4      /* max_steps reached before zmax */
+#define LUNA_WAIT_TIMEOUT 5     /* a bounded device-side wait gave up (the result is invalid) */
 #define LUNA_ERR_BAD_ARG 16
 #define LUNA_ERR_UNSUPPORTED 17
 #define LUNA_ERR_CUDA 18

@@ -15,6 +15,7 @@ LUNA_FIELD_ABOVE_EMAX = 1
 LUNA_REPEAT_LIMIT = 2
 LUNA_NONFINITE = 3
 LUNA_STEP_BUDGET = 4
+LUNA_WAIT_TIMEOUT = 5
 LUNA_ERR_BAD_ARG = 16
 LUNA_ERR_UNSUPPORTED = 17
 LUNA_ERR_CUDA = 18

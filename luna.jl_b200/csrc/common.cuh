@@ -81,6 +81,7 @@ enum {
     ST_REPEAT_LIMIT = 2,
     ST_NONFINITE = 3,
     ST_STEP_BUDGET = 4,
+    ST_WAIT_TIMEOUT = 5,  // a bounded device-side wait (tensor-core completion) ran out
 };
 
 }  // namespace luna

@@ -14,6 +14,7 @@
 
 #include "../../include/luna_b200.h"
 #include "radial.cuh"
+#include "tc_gemm.cuh"
 
 using namespace luna;
 
@@ -703,6 +704,8 @@ struct luna_radial_plan {
     std::vector<void*> allocs;
     const double* Mi = nullptr;      // [Nr*Nr] row-major QDHT k -> r
     const double* Mf = nullptr;      // [Nr*Nr] row-major QDHT r -> k
+    // mixed precision: BF16 hi/lo splits of the QDHT matrices for the tensor-core products
+    const __nv_bfloat16 *Mi_hi = nullptr, *Mi_lo = nullptr, *Mf_hi = nullptr, *Mf_lo = nullptr;
     const double2* outfac = nullptr; // [Nw*Nr]
     char* gscr = nullptr;            // per-column scratch when a column does not fit in shared memory
     size_t gstride = 0;
@@ -735,11 +738,36 @@ int rad_column_setup(luna_radial_plan* p) {
 
 int rad_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
-// Pk or Er = X * M^T along the radial index of the 2Nw x Nr real view.
-int rad_qdht(luna_radial_plan* p, const void* X, const double* M, void* Y, const RadState* st, cudaStream_t s) {
+#define RAD_TC_BN 64
+
+uint16_t bf16_rne(float f) {
+    uint32_t b;
+    memcpy(&b, &f, 4);
+    b += 0x7FFFu + ((b >> 16) & 1u);
+    return (uint16_t)(b >> 16);
+}
+
+float bf16_val(uint16_t h) {
+    uint32_t b = (uint32_t)h << 16;
+    float f;
+    memcpy(&f, &b, 4);
+    return f;
+}
+
+// Er = A Mi^T or Pk = Pw Mf^T along the radial index of the 2Nw x Nr real view: FP64
+// CUDA-core tiles for the plain path, 3xBF16 tensor-core products for the mixed path.
+int rad_qdht(luna_radial_plan* p, const void* X, bool fwd, void* Y, const RadState* st, int* flags, cudaStream_t s) {
     const int rows = 2 * p->Nw;
-    dim3 g((rows + RG_BM - 1) / RG_BM, (p->Nr + RG_BN - 1) / RG_BN);
-    rad_gemm_f64<<<g, 256, 0, s>>>((const double*)X, rows, rows, M, (double*)Y, p->Nr, st);
+    if (p->precision == LUNA_PREC_FP64) {
+        dim3 g((rows + RG_BM - 1) / RG_BM, (p->Nr + RG_BN - 1) / RG_BN);
+        rad_gemm_f64<<<g, 256, 0, s>>>((const double*)X, rows, rows, fwd ? p->Mf : p->Mi, (double*)Y, p->Nr, st);
+    } else {
+        dim3 g((rows + TC_BM - 1) / TC_BM, p->Nr / RAD_TC_BN);
+        const int* fin = st ? (const int*)((const char*)st + offsetof(RadState, finished)) : nullptr;
+        tc_gemm_3xbf16<RAD_TC_BN><<<g, TC_THREADS, tc_smem_bytes<RAD_TC_BN>(), s>>>(
+            (const float*)X, rows, rows, fwd ? p->Mf_hi : p->Mi_hi, fwd ? p->Mf_lo : p->Mi_lo, (float*)Y, p->Nr,
+            fin, flags);
+    }
     return LUNA_OK;
 }
 
@@ -747,10 +775,10 @@ int rad_qdht(luna_radial_plan* p, const void* X, const double* M, void* Y, const
 // QDHT r -> k result in B.
 template <typename Rl>
 int rad_transform(luna_radial_plan* p, const TwTab<Rl>& tw, RadState* st, int* flags, cudaStream_t s) {
-    rad_qdht(p, p->A, p->Mi, p->B, st, s);
+    rad_qdht(p, p->A, false, p->B, st, flags, s);
     rad_column_kernel<Rl><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(p->d_col, (const cpx<Rl>*)p->B, (cpx<Rl>*)p->A, tw,
                                                             p->smem, p->gscr, p->gstride, st, flags);
-    rad_qdht(p, p->A, p->Mf, p->B, st, s);
+    rad_qdht(p, p->A, true, p->B, st, flags, s);
     return LUNA_OK;
 }
 
@@ -780,7 +808,10 @@ int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* 
         return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: null argument");
     if (g->kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: only field-resolved (RealGrid) radial transforms");
     if (rd->Nr < 1 || rd->Nr > 4096) return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: Nr must be in 1..4096");
-    if (precision != LUNA_PREC_FP64) return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: precision not available for the radial transform");
+    if (precision != LUNA_PREC_FP64 && precision != LUNA_PREC_MIXED)
+        return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: unknown precision");
+    if (precision == LUNA_PREC_MIXED && rd->Nr % 64 != 0)
+        return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: the mixed-precision QDHT needs Nr to be a multiple of 64");
     for (int i = 0; i < nresp; ++i)
         if (resps[i].kind == LUNA_RESP_RAMAN)
             return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Raman response not available for the radial transform");
@@ -810,13 +841,32 @@ int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* 
         upload(p->allocs, rd->outfac, 2 * n, &tmp))
         return bail(LUNA_ERR_CUDA);
     p->outfac = (const double2*)tmp;
+    if (precision == LUNA_PREC_MIXED) {
+        std::vector<uint16_t> h(nn), l(nn);
+        const double* src[2] = {rd->Mi, rd->Mf};
+        const __nv_bfloat16** dh[2] = {&p->Mi_hi, &p->Mf_hi};
+        const __nv_bfloat16** dl[2] = {&p->Mi_lo, &p->Mf_lo};
+        for (int w = 0; w < 2; ++w) {
+            for (size_t j = 0; j < nn; ++j) {
+                h[j] = bf16_rne((float)src[w][j]);
+                l[j] = bf16_rne((float)(src[w][j] - (double)bf16_val(h[j])));
+            }
+            const uint16_t *th = nullptr, *tl = nullptr;
+            if (upload(p->allocs, h.data(), nn, &th) || upload(p->allocs, l.data(), nn, &tl)) return bail(LUNA_ERR_CUDA);
+            *dh[w] = (const __nv_bfloat16*)th;
+            *dl[w] = (const __nv_bfloat16*)tl;
+        }
+        if (cudaFuncSetAttribute(tc_gemm_3xbf16<RAD_TC_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 tc_smem_bytes<RAD_TC_BN>()) != cudaSuccess)
+            return bail(fail(LUNA_ERR_CUDA, "radial_plan_create: cannot configure the tensor-core kernel"));
+    }
     const size_t cb = sizeof(double2);
     if (dalloc(p->allocs, &p->A, cb * n) || dalloc(p->allocs, &p->B, cb * n) || dalloc(p->allocs, &p->d_flags, sizeof(int)) ||
         dalloc(p->allocs, &p->d_col, sizeof(LunaInst)))
         return bail(LUNA_ERR_CUDA);
     if (cudaMemcpy(p->d_col, &col->proto, sizeof(LunaInst), cudaMemcpyHostToDevice) != cudaSuccess)
         return bail(fail(LUNA_ERR_CUDA, "radial_plan_create: copy of the column descriptor failed"));
-    rc = rad_column_setup<double>(p);
+    rc = (precision == LUNA_PREC_FP64) ? rad_column_setup<double>(p) : rad_column_setup<float>(p);
     if (rc) return bail(rc);
     *out = p;
     return LUNA_OK;
@@ -833,7 +883,8 @@ void luna_b200_radial_plan_destroy(luna_radial_plan* p) {
 int luna_b200_radial_rhs_device(luna_radial_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
     (void)z;  // constant density and normalisation
     if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "radial_rhs_device: null argument");
-    return rad_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+    if (p->precision == LUNA_PREC_FP64) return rad_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+    return rad_rhs<float>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
 }
 
 int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, double z) {
@@ -845,12 +896,14 @@ int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, doub
         CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     }
     CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
-    int rc = rad_rhs<double>(p, p->d_Ew, p->d_nl, p->stream);
+    int rc = (p->precision == LUNA_PREC_FP64) ? rad_rhs<double>(p, p->d_Ew, p->d_nl, p->stream)
+                                              : rad_rhs<float>(p, p->d_Ew, p->d_nl, p->stream);
     if (rc) return rc;
     int fl = 0;
     CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
     CK(cudaMemcpyAsync(&fl, p->d_flags, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
     CK(cudaStreamSynchronize(p->stream));
+    if (fl & (1 << ST_WAIT_TIMEOUT)) return fail(LUNA_WAIT_TIMEOUT, "radial_rhs: a tensor-core wait timed out");
     if (fl & (1 << ST_FIELD_ABOVE_EMAX)) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
     return LUNA_OK;
 }
@@ -985,6 +1038,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
     if (r.status == ST_FIELD_ABOVE_EMAX) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
     if (r.status == ST_REPEAT_LIMIT) return fail(LUNA_REPEAT_LIMIT, "Reached limit for step repetition");
     if (r.status == ST_STEP_BUDGET) return fail(LUNA_STEP_BUDGET, "Step budget exhausted before zmax");
+    if (r.status == ST_WAIT_TIMEOUT) return fail(LUNA_WAIT_TIMEOUT, "radial_solve: a tensor-core wait timed out");
     return LUNA_OK;
 }
 
@@ -997,7 +1051,9 @@ int luna_b200_radial_solve(luna_radial_plan* p, const double* linop, double* y_i
                            luna_solve_stats* stats) {
     if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "radial_solve: null argument");
     if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "radial_solve: save points missing");
-    return rad_solve<double, double>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+    if (p->precision == LUNA_PREC_FP64)
+        return rad_solve<double, double>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+    return rad_solve<float, float>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
 }
 
 // ---------------------------------------------------------------- allocation-free RHS

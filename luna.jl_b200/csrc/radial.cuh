@@ -315,6 +315,10 @@ __global__ void rad_control_kernel(RadState* st, LunaInst* opt, const double* pa
     }
     Ctl& c = st->c;
     control_step(*opt, c, sy, syn, se, st->flags);
+    if (st->flags & (1 << ST_WAIT_TIMEOUT)) {
+        c.status = ST_WAIT_TIMEOUT;
+        c.done = 1;
+    }
     if (c.done && c.status != 0) {
         st->finished = 1;
         return;

@@ -123,3 +123,39 @@ def test_radial_plan_rejects_raman_and_envelope():
     with pytest.raises(_lib.LunaError) as e:
         radial_plan.RadialPlan.from_transform(bad)
     assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED
+
+
+# ------------------------------------------------------------------ mixed precision
+# FP32 transforms and responses, QDHT as 3xBF16 tensor-core products (tcgen05) with FP32
+# accumulation; FP64 state, phase, controller and plasma prefix sums.
+
+@pytest.mark.parametrize("energy,plasma", [(20e-6, "PPT"), (50e-6, "ADK"), (20e-6, False)])
+def test_radial_rhs_mixed_close_to_oracle(energy, plasma):
+    p = _problem(energy, plasma)
+    rng = np.random.default_rng(5)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    plan = radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    nl = np.zeros_like(Ew)
+    plan.rhs(nl, Ew, 0.0)
+    ref = uppe.trans_radial(p.transform, Ew, 0.0)
+    assert _rel(nl, ref) < 2e-4, _rel(nl, ref)
+
+
+def test_radial_solve_mixed_spectral_error():
+    """The mixed-precision radial solve stays within 1e-3 relative spectral L2 error of the
+    FP64 oracle at every save point."""
+    p = _problem(20e-6, "PPT", flength=0.03)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    r = radial_plan.run(p, precision=_lib.PREC_MIXED)
+    assert r.status == 0 and r.nsaved == 5
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-3, _rel(a, b)
+
+
+def test_radial_mixed_rejects_nr_not_multiple_of_64():
+    p = prop_radial_args("Ar", 1.2, R=1e-3, N=48, flength=0.01, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=1e-6, w0=40e-6, plasma=False)
+    with pytest.raises(_lib.LunaError) as e:
+        radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED

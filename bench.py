@@ -73,6 +73,14 @@ class Clocks:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.p = None
+        # start timing only once the sampler runs (its start-up must not overlap the
+        # timed region)
+        t0 = time.time()
+        while self.p is not None and time.time() - t0 < 15.0:
+            self.f.flush()
+            if os.path.getsize(self.f.name) > 0 or self.p.poll() is not None:
+                break
+            time.sleep(0.05)
 
     def stop(self):
         if self.p is None:
@@ -215,6 +223,130 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- radial
+RADIAL_METRIC = "radial UPPE RHS evaluations/s (TransRadial, mixed precision, QDHT on tensor cores)"
+RADIAL_WORKLOAD = ("radial: TransRadial Nr=256 (R=3 mm) x Nt=2048/No=4096 over 0.5 ps, Ar 1 bar, "
+                   "w0=1 mm, 800 nm, 30 fs, 0.5 mJ, f=1 m focusing, 2 m, Kerr + PPT plasma")
+
+
+def radial_problem():
+    from luna_b200.radial import prop_radial_args
+    return prop_radial_args("Ar", 1.0, R=3e-3, N=256, flength=2.0, λ0=800e-9,
+                            λlims=(400e-9, 2000e-9), trange=0.5e-12, τfwhm=30e-15, energy=0.5e-3,
+                            w0=1e-3, focal_length=1.0, plasma="PPT")
+
+
+def radial_cpu_rate(p, seconds=10.0):
+    """Oracle RHS evaluations per second on one core (bounded sample)."""
+    from oracle import uppe
+    n, t0 = 0, time.perf_counter()
+    while n < 2 or time.perf_counter() - t0 < seconds:
+        uppe.trans_radial(p.transform, p.Eω, 0.0)
+        n += 1
+    return n / (time.perf_counter() - t0), n
+
+
+def run_radial(args, world, rank, local):
+    """Per-RHS throughput of the radial transform (one bench step = one evaluation of
+    (t::TransRadial)(nl, Eω, z) on the Nw x Nr field), replicas only across GPUs."""
+    if args.impl == "reference":
+        if rank == 0:
+            p = radial_problem()
+            rate, n = radial_cpu_rate(p)
+            print(json.dumps({"impl": "reference", "metric": RADIAL_METRIC, "value": rate, "unit": "RHS/s",
+                              "n_gpus": world, "steps": n, "warmup": 0, "ms_per_step": 1e3 / rate,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f64", "data": "synthetic", "config": {"workload": RADIAL_WORKLOAD},
+                              "cpu_baseline": {"value": rate, "unit": "RHS/s", "cores": 1, "kind": "port",
+                                               "sample": f"{n} oracle evaluations (numpy FP64)"},
+                              "e2e": {"value": rate, "unit": "RHS/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from luna_b200 import radial_plan as RP
+    p = radial_problem()
+    lib = _lib.load()
+    plan = RP.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    Nw, Nr = p.Eω.shape
+    Ec = np.ascontiguousarray(p.Eω.T)
+    dE = torch.from_numpy(Ec.view(np.float64).copy()).cuda()
+    dN = torch.zeros_like(dE)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    s = torch.cuda.current_stream()
+    vp = lambda t: _lib.ctypes.c_void_p(t.data_ptr())
+    sp = _lib.ctypes.c_void_p(s.cuda_stream)
+
+    def timed(fn, k, w):
+        for _ in range(w):
+            fn()
+        ts = []
+        for _ in range(k):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return ts
+
+    rhs = lambda: _lib.check(lib.luna_b200_radial_rhs_device(plan.handle, vp(dN), vp(dE), 0.0, sp))
+    clk = Clocks(local)
+    torch.cuda.synchronize()
+    t_rhs = timed(rhs, args.steps, args.warmup)
+    # the QDHT product alone (FP32 complex in and out, 3xBF16 tensor-core MMAs)
+    X = torch.randn(2 * Nw * Nr, dtype=torch.float32, device="cuda")
+    Y = torch.empty_like(X)
+    qd = lambda: _lib.check(lib.luna_b200_qdht_device(plan.handle, vp(Y), vp(X), 1, sp))
+    t_q = timed(qd, args.steps, args.warmup)
+    clocks = clk.stop()
+    # end to end through the host-buffer entry point (pinned host memory)
+    Eh = torch.empty(Ec.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    Nh = torch.empty(Ec.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    Eh[:] = Ec
+    for _ in range(args.warmup):
+        lib.luna_b200_radial_rhs(plan.handle, _lib.dptr(Nh.view(np.float64)), _lib.dptr(Eh.view(np.float64)), 0.0)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        _lib.check(lib.luna_b200_radial_rhs(plan.handle, _lib.dptr(Nh.view(np.float64)),
+                                            _lib.dptr(Eh.view(np.float64)), 0.0))
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    # one full propagation (22-28 RK steps, 201 saves of the Nw x Nr field)
+    t0 = time.perf_counter()
+    r = RP.run(p, precision=_lib.PREC_MIXED)
+    solve_s = time.perf_counter() - t0
+    ms = statistics.mean(t_rhs)
+    q_ms = statistics.mean(t_q)
+    flops = 3 * 2.0 * (2 * Nw) * Nr * Nr
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            tpk, pk_kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        tpk, pk_kind = 1590.0, "fallback"
+    ach = flops / (q_ms / 1e3) / 1e12
+    line = {"metric": RADIAL_METRIC, "value": 1e3 / ms, "unit": "RHS/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3", "data": "synthetic",
+            "config": {"workload": RADIAL_WORKLOAD, "Nw": Nw, "Nr": Nr, "No": p.grid.No,
+                       "l2": "256 MB buffer written between timed evaluations"},
+            "e2e": {"value": 1.0 / e2e_s, "unit": "RHS/s", "h2d_bytes_per_step": Eh.nbytes,
+                    "d2h_bytes_per_step": Nh.nbytes},
+            "gpu_launches": 5 * args.steps,
+            "roofline": {"bound": "tensor", "kernel": "tc_gemm_3xbf16 (QDHT r->k)", "achieved": ach,
+                         "peak": tpk, "unit": "TFLOP/s", "frac": ach / tpk, "traffic": None,
+                         "peak_kind": pk_kind, "qdht_ms": q_ms,
+                         "note": "3 BF16 products x 2*(2Nw)*Nr^2 flops per launch; latency-bound at this size"},
+            "solve": {"sims_per_hour_e2e": 3600.0 / solve_s, "rk_steps": int(r.steps), "status": int(r.status)},
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        rate, n = radial_cpu_rate(p)
+        line["cpu_baseline"] = {"value": rate, "unit": "RHS/s", "cores": 1, "kind": "port",
+                                "sample": f"{n} oracle evaluations of the same field (numpy FP64, one core)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -226,8 +358,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-rk-steps", type=int, default=200000,
                     help="per-instance step budget (profiling aid; the scan needs < 30000)")
+    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial"],
+                    help="scan256: the batched capillary scan (headline); radial: TransRadial RHS")
     args = ap.parse_args()
     world, rank, local = dist_info()
+    if args.workload == "radial":
+        return run_radial(args, world, rank, local)
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist

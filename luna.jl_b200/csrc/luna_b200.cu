@@ -887,6 +887,13 @@ int luna_b200_radial_rhs_device(luna_radial_plan* p, double* nl_dev, const doubl
     return rad_rhs<float>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
 }
 
+int luna_b200_qdht_device(luna_radial_plan* p, void* Y_dev, const void* X_dev, int forward, void* stream) {
+    if (!p || !Y_dev || !X_dev || X_dev == Y_dev) return fail(LUNA_ERR_BAD_ARG, "qdht_device: null or aliased argument");
+    rad_qdht(p, X_dev, forward != 0, Y_dev, nullptr, p->d_flags, (cudaStream_t)stream);
+    CK(cudaGetLastError());
+    return LUNA_OK;
+}
+
 int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, double z) {
     (void)z;
     if (!p || !nl || !Ew) return fail(LUNA_ERR_BAD_ARG, "radial_rhs: null argument");
@@ -1006,7 +1013,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
                 rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, (const cpx<Rl>*)p->B, nullptr);
             }
             rad_combine_kernel<Kt><<<nblk, 256, 0, s>>>(a, S.partial);
-            rad_control_kernel<<<1, 32, 0, s>>>(S.st, S.opt, S.partial, nblk);
+            rad_control_kernel<<<1, 256, 0, s>>>(S.st, S.opt, S.partial, nblk);
             rad_post_kernel<Rl, Kt><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(a, p->d_col, S.opt, t, p->smem, p->gscr, p->gstride);
         }
         CK(cudaGetLastError());

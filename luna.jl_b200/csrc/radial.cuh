@@ -304,15 +304,31 @@ __global__ void __launch_bounds__(256) rad_combine_kernel(RadArgs a, double* par
 }
 
 // Weak norm, PI controller and bookkeeping (the same code as the fused solver), FSAL
-// rotation and the save points the accepted step covers.
-__global__ void rad_control_kernel(RadState* st, LunaInst* opt, const double* partial, int nblocks) {
-    if (threadIdx.x != 0 || blockIdx.x != 0 || st->finished) return;
+// rotation and the save points the accepted step covers. One CTA of 256 threads: thread t
+// sums the partials t, t+256, ... in order, then a fixed-order tree (deterministic).
+__global__ void __launch_bounds__(256) rad_control_kernel(RadState* st, LunaInst* opt, const double* partial,
+                                                          int nblocks) {
+    if (st->finished) return;
+    __shared__ double red[3][256];
     double sy = 0, syn = 0, se = 0;
-    for (int b = 0; b < nblocks; ++b) {
+    for (int b = threadIdx.x; b < nblocks; b += 256) {
         sy += partial[3 * b];
         syn += partial[3 * b + 1];
         se += partial[3 * b + 2];
     }
+    red[0][threadIdx.x] = sy;
+    red[1][threadIdx.x] = syn;
+    red[2][threadIdx.x] = se;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if (threadIdx.x < h)
+            for (int q = 0; q < 3; ++q) red[q][threadIdx.x] += red[q][threadIdx.x + h];
+        __syncthreads();
+    }
+    if (threadIdx.x != 0) return;
+    sy = red[0][0];
+    syn = red[1][0];
+    se = red[2][0];
     Ctl& c = st->c;
     control_step(*opt, c, sy, syn, se, st->flags);
     if (st->flags & (1 << ST_WAIT_TIMEOUT)) {

@@ -159,3 +159,30 @@ def test_radial_mixed_rejects_nr_not_multiple_of_64():
     with pytest.raises(_lib.LunaError) as e:
         radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
     assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-13), (_lib.PREC_MIXED, 3e-5)])
+@pytest.mark.parametrize("forward", [True, False])
+def test_qdht_device_matches_matrix_product(prec, tol, forward):
+    """luna_b200_qdht_device: the plan's Hankel transform along the radial index (mul!/ldiv!
+    of Hankel.jl's QDHT), FP64 CUDA-core tiles or 3xBF16 tensor-core products."""
+    torch = pytest.importorskip("torch")
+    p = prop_radial_args("Ar", 1.2, R=1e-3, N=128, flength=0.01, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=1e-6, w0=40e-6, plasma=False)
+    plan = radial_plan.RadialPlan.from_transform(p.transform, prec)
+    rng = np.random.default_rng(11)
+    X = rng.standard_normal(p.Eω.shape) + 1j * rng.standard_normal(p.Eω.shape)
+    ref = p.q.forward(X, axis=1) if forward else p.q.inverse(X, axis=1)
+    ct = np.complex128 if prec == _lib.PREC_FP64 else np.complex64
+    Xc = np.ascontiguousarray(X.T).astype(ct)
+    rt = np.float64 if prec == _lib.PREC_FP64 else np.float32
+    dX = torch.from_numpy(Xc.view(rt).copy()).cuda()
+    dY = torch.full_like(dX, float("nan"))
+    s = torch.cuda.current_stream()
+    _lib.check(_lib.load().luna_b200_qdht_device(plan.handle, _lib.ctypes.c_void_p(dY.data_ptr()),
+                                                 _lib.ctypes.c_void_p(dX.data_ptr()), int(forward),
+                                                 _lib.ctypes.c_void_p(s.cuda_stream)))
+    torch.cuda.synchronize()
+    Y = dY.cpu().numpy().view(ct).reshape(Xc.shape).T.astype(np.complex128)
+    assert _rel(Y, ref) < tol, _rel(Y, ref)

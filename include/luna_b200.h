@@ -145,6 +145,10 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms);
 int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
                              luna_solve_stats* stats);
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
+/* Scheduling record of the last run (no counterpart in the reference): per instance the
+ * start and end of its integration in seconds from the earliest start ([2*n] doubles) and
+ * the SM that integrated it ([n] ints, may be NULL). */
+int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm);
 void luna_b200_batch_destroy(luna_batch* b);
 
 /* ---------------------------------------------------------------- radial transform

@@ -77,4 +77,6 @@ typedef struct {
     int nsaved;
     long long steps, accepted, rejected, nrhs;
     double z, dz;
+    unsigned long long t_begin, t_end;  // device global timer (ns) around the integration
+    int sm;                             // SM that integrated the instance
 } LunaInst;

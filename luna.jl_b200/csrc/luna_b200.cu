@@ -35,9 +35,22 @@ solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes)
         const int i = sidx;
         if (i >= n) break;
         LunaInst& I = insts[i];
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            unsigned int sm;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+            I.t_begin = t;
+            I.sm = (int)sm;
+        }
         Ws<Rl> w;
         plan_ws<Rl>(I, smem, smem_bytes, w, tw);
         solve_instance<Rl, Kt>(I, w, ctl);
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            I.t_end = t;
+        }
     }
 }
 
@@ -651,6 +664,20 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
         }
     }
     CK(cudaStreamSynchronize(b->stream));
+    return LUNA_OK;
+}
+
+int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm) {
+    if (!b || !begin_end_s) return fail(LUNA_ERR_BAD_ARG, "batch_timeline: null argument");
+    std::vector<LunaInst> res(b->n);
+    CK(cudaMemcpy(res.data(), b->d_insts, sizeof(LunaInst) * b->n, cudaMemcpyDeviceToHost));
+    unsigned long long t0 = ~0ull;
+    for (const LunaInst& I : res) t0 = std::min(t0, I.t_begin);
+    for (int i = 0; i < b->n; ++i) {
+        begin_end_s[2 * i] = (double)(res[i].t_begin - t0) * 1e-9;
+        begin_end_s[2 * i + 1] = (double)(res[i].t_end - t0) * 1e-9;
+        if (sm) sm[i] = res[i].sm;
+    }
     return LUNA_OK;
 }
 

@@ -233,6 +233,15 @@ class Batch:
         _lib.check(_lib.load().luna_b200_batch_download(self._h, Sp, Yp, stats))
         return saves, ys, list(stats)
 
+    def timeline(self):
+        """(begin, end) seconds of every instance's integration in the last run, and the SM
+        that ran it."""
+        n = len(self.plans)
+        be = np.zeros((n, 2))
+        sm = (_lib.c_int * n)()
+        _lib.check(_lib.load().luna_b200_batch_timeline(self._h, _lib.dptr(be), sm))
+        return be, np.array(list(sm))
+
     def steplog(self, i):
         out = np.zeros((self.steplog_cap, 4))
         _lib.check(_lib.load().luna_b200_batch_steplog(self._h, i, _lib.dptr(out)))

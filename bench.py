@@ -135,7 +135,7 @@ def build(world, rank, n_per_rank):
 # ----------------------------------------------------------------------------- CPU side
 def _oracle_sample(args):
     """Time `nsteps` oracle RK steps of one scan instance (FP64 numpy, one core)."""
-    idx, nsteps = args
+    idx, budget = args
     import luna_b200_loader as L
     L.load()
     from luna_b200 import scan as S
@@ -147,7 +147,7 @@ def _oracle_sample(args):
     t0 = time.perf_counter()
     done = 0
     try:
-        for _ in range(nsteps):
+        while done < 3 or time.perf_counter() - t0 < budget:
             st.step()
             done += 1
     except ValueError:
@@ -172,9 +172,9 @@ def cpu_estimate(sample_seconds=20.0, workers=1):
     classes = sorted(set(cls))
     # one completed (status 0) instance represents each grid class
     reps = [next(i for i in range(len(cls)) if cls[i] == c and status[i] == 0) for c in classes]
-    # about sample_seconds of CPU work in total: a few RK steps per class
-    nsteps = 3
-    jobs = [(i, nsteps) for i in reps]
+    # about sample_seconds of CPU work in total: RK steps per class until the class's
+    # share of the time is used (at least 3)
+    jobs = [(i, sample_seconds / len(reps)) for i in reps]
     t0 = time.perf_counter()
     if workers > 1:
         import multiprocessing as mp
@@ -189,10 +189,43 @@ def cpu_estimate(sample_seconds=20.0, workers=1):
     total = sum(per_rhs[cls[i]] * nrhs[i] for i in range(len(nrhs)))
     ok = int(np.sum(status == 0))
     sims_per_hour_core = 3600.0 * ok / total
-    return sims_per_hour_core, {"classes": len(classes), "rk_steps_each": nsteps,
+    return sims_per_hour_core, {"classes": len(classes), "rk_steps_each": [r[3] for r in res],
                                 "sample_wall_s": round(wall, 1),
                                 "per_rhs_ms": {f"No={k[0]}{'+Raman' if k[1] else ''}": round(v * 1e3, 2)
                                                for k, v in per_rhs.items()}}
+
+
+def plain_fp64_estimate(inst):
+    """Plain FP64 drop-in on this GPU: one instance per solve (one CTA, as the Julia shim
+    calls luna_b200_solve for each prop_capillary). Device time per RK step is measured on
+    one instance of each grid class (difference of a 250-step and a 50-step run) and scaled
+    by every instance's FP64 step count (oracle/scan256_nrhs.json)."""
+    with open(STEPS_FILE) as f:
+        ref = json.load(f)
+    steps = np.array(ref["steps"], dtype=np.float64)
+    status = np.array(ref["status"])
+    from luna_b200.grid import RealGrid
+    cls = []
+    for p in inst:
+        g = RealGrid(p["flength"], 800e-9, (p["λmin"], p["λmax"]), p["trange"])
+        cls.append((g.No, p["gas"] == "H2"))
+    per_step = {}
+    for c in sorted(set(cls)):
+        i = next(j for j in range(len(cls)) if cls[j] == c and status[j] == 0)
+        pr = scan.build_problem(inst[i], saveN=SAVEN)
+        plan = P.Plan.from_transform(pr.transform, _lib.PREC_FP64)
+        t = []
+        for cap in (50, 250):
+            b = P.Batch([plan], SAVEN, np.linspace(0.0, pr.grid.zmax, SAVEN), max_steps=cap,
+                        max_dt=pr.grid.zmax / 2)
+            b.upload([pr.linop], [pr.Eω], [0.0], [1e-4], [pr.grid.zmax])
+            b.run()
+            t.append(b.run())
+        per_step[c] = (t[1] - t[0]) / 200.0 / 1e3
+    total = sum(per_step[cls[i]] * steps[i] for i in range(len(steps)))
+    ok = int(np.sum(status == 0))
+    return 3600.0 * ok / total, {f"No={k[0]}{'+Raman' if k[1] else ''}": round(v * 1e3, 3)
+                                 for k, v in per_step.items()}
 
 
 def run_reference(args, world, rank):
@@ -473,6 +506,21 @@ def main():
                              "peak_kind": peak_kind,
                              "note": "algorithmic bytes = RK stage vectors per step (y/yn FP64, k FP32) x steps; kernel is latency/SMEM bound"},
                 "clocks": clocks, "setup_s": round(setup_s, 1)}
+        try:
+            be, _ = batch.timeline()
+            line["timeline"] = {"long_pole_s": float(np.max(be[:, 1] - be[:, 0])),
+                                "p90_end_s": float(np.percentile(be[:, 1], 90)),
+                                "busy_cta_s": float(np.sum(be[:, 1] - be[:, 0]))}
+        except Exception as e:
+            line["timeline"] = {"error": str(e)[:200]}
+        if world == 1 and args.instances == 256:
+            try:
+                v0, per = plain_fp64_estimate(inst)
+                line["plain_fp64"] = {"value": v0, "unit": "sims/hour", "ms_per_rk_step": per,
+                                      "method": "FP64 single-instance solves (luna_b200_solve path), device time per RK step per grid class x FP64 step counts",
+                                      "speedup_of_value": value / v0}
+            except Exception as e:
+                line["plain_fp64"] = {"value": None, "error": str(e)[:200]}
         if not args.no_cpu_baseline and world == 1:
             try:
                 v1, info = cpu_estimate(workers=1)

@@ -99,7 +99,12 @@ typedef struct {
                                                   follow this step sequence instead of the
                                                   controller's choice (verification aid)      */
     long long nreplay;
+    int flags;                                 /* LUNA_SOLVE_* bits, 0 for the defaults     */
 } luna_solve_opts;
+
+/* luna_solve_opts.flags */
+#define LUNA_SOLVE_NO_CLUSTERS 1 /* batches: integrate every instance on one CTA (no Raman
+                                    clusters); a verification and timing aid            */
 
 typedef struct {
     int status;

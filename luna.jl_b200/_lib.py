@@ -20,6 +20,7 @@ LUNA_ERR_BAD_ARG = 16
 LUNA_ERR_UNSUPPORTED = 17
 LUNA_ERR_CUDA = 18
 NOALLOC_SCRATCH_BYTES = 1 << 20
+SOLVE_NO_CLUSTERS = 1
 
 RESP_KERR_FIELD = 1
 RESP_KERR_ENV = 2
@@ -58,7 +59,8 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("rtol", c_double), ("atol", c_double), ("safety", c_double),
                 ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
                 ("max_steps", c_longlong), ("saveN", c_int), ("zsave", PD),
-                ("steplog_cap", c_longlong), ("replay", PD), ("nreplay", c_longlong)]
+                ("steplog_cap", c_longlong), ("replay", PD), ("nreplay", c_longlong),
+                ("flags", c_int)]
 
 
 class SolveStats(ctypes.Structure):

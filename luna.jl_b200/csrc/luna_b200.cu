@@ -1,4 +1,5 @@
 // Kernels and the C ABI of libluna_b200 (see include/luna_b200.h).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -35,6 +36,205 @@ solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes)
         const int i = sidx;
         if (i >= n) break;
         LunaInst& I = insts[i];
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            unsigned int sm;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+            I.t_begin = t;
+            I.sm = (int)sm;
+        }
+        Ws<Rl> w;
+        plan_ws<Rl>(I, smem, smem_bytes, w, tw);
+        solve_instance<Rl, Kt>(I, w, ctl);
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            I.t_end = t;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- Raman clusters
+// Helper CTA (rank 1 or 2) of a Raman cluster. The Raman convolution of an instance with
+// No time samples is a 2*No-point real convolution, i.e. an Mr = No point complex
+// transform of the packed input z[m] = (E[2m]^2, E[2m+1]^2), m < No/2 (zero above), and
+// only P[m < No/2] is used. With HM = Mr/2 the even and odd frequencies separate:
+//   Z[2j]   = FFT_HM(z)[j],               Z[2j+1] = FFT_HM(z[m] e^{-2 pi i m/Mr})[j],
+//   P[m]    = IFFT_HM(Z'_even)[m] + e^{+2 pi i m/Mr} IFFT_HM(Z'_odd)[m],
+// and the real-transform split / response product / split of the convolution pairs k
+// with Mr-k, which has the parity of k. Each helper therefore holds one half (HM points)
+// in its own shared memory; rank 0 adds the two halves (distributed shared memory).
+template <typename Rl>
+__device__ void raman_helper(const LunaInst* insts, char* smem, const TwTab<Rl>& tw, unsigned rank, ClBox* box,
+                             int* err) {
+    namespace cg = cooperative_groups;
+    const int tid = threadIdx.x, T = LUNA_BLOCK;
+    cpx<Rl>* buf = reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES);
+    __shared__ int s_ok;
+    int seen = 0;
+    const int par = (int)rank - 1;
+    while (true) {
+        if (tid == 0) {
+            const long long t0 = clock64();
+            int ok = 1;
+            while ((int)cl_ld_acquire(&box->seq) == seen) {
+                if (clock64() - t0 > CL_WAIT_CYCLES) {
+                    ok = 0;
+                    break;
+                }
+            }
+            s_ok = ok;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) atomicOr(err, 1);
+            return;
+        }
+        seen = box->seq;
+        if (box->cmd != CL_RAMAN) return;  // CL_EXIT
+        const LunaInst& I = insts[box->inst];
+        const LunaResp* rr = nullptr;
+        for (int i = 0; i < I.nresp; ++i)
+            if (I.resp[i].kind == LUNA_RESP_RAMAN) rr = &I.resp[i];
+        const int Mr = I.No, HM = Mr / 2;
+        const int M = box->M, P = box->P;
+        const Rl sc = (Rl)box->sc;
+        const int Ph = fft_nsplit<Rl>(HM);
+        const unsigned tsh = TW_LOG_MMAX - ilog2i((unsigned)Mr);
+        const cpx<Rl>* xr = cg::this_cluster().map_shared_rank(
+            reinterpret_cast<cpx<Rl>*>(__cvta_shared_to_generic(box->xaddr)), 0);
+        // packed squares of the field (odd half: times e^{-2 pi i m/Mr}), split order
+        for (int m = tid; m < HM; m += T) {
+            const cpx<Rl> e = xr[Swz<Rl>::f(split_pos(m, M, P))];
+            const Rl e0 = e.x * sc, e1 = e.y * sc;
+            cpx<Rl> v = mk<Rl>(e0 * e0, e1 * e1);
+            if (par) v = v * twiddle<Rl, false>(tw, (unsigned)m << tsh);
+            buf[Swz<Rl>::f(split_pos(m, HM, Ph))] = v;
+        }
+        __syncthreads();
+        cpx<Rl>* Z = block_fft<Rl, false>(buf, nullptr, HM, tw);
+        const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(rr->H);
+        // real-transform split, response product, inverse split (as in raman_conv) for the
+        // frequencies k = 2t + par <= Mr/2 and their partners Mr - k
+        for (int t = tid;; t += T) {
+            const int k = 2 * t + par;
+            if (k > Mr / 2) break;
+            const int km = (Mr - k) & (Mr - 1);
+            const int jk = k >> 1, jm = km >> 1;
+            cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(jk)]);
+            cpx<double> Zm = cvt<double>(Z[Swz<Rl>::f(jm)]);
+            cpx<double> Wk = half_twiddle<Rl, false>(tw, k, Mr);
+            cpx<double> a = Zk + conj(Zm), b = Zk - conj(Zm);
+            cpx<double> Xk = scale(0.5, a) + scale(0.5, mul_mi<double, false>(Wk * b));
+            cpx<double> Xm;
+            if (k == 0) {
+                Xk = mk<double>(Zk.x + Zk.y, 0.0);
+                Xm = mk<double>(Zk.x - Zk.y, 0.0);
+            } else {
+                cpx<double> Wm = scale(-1.0, conj(Wk));
+                cpx<double> a2 = Zm + conj(Zk), b2 = Zm - conj(Zk);
+                Xm = scale(0.5, a2) + scale(0.5, mul_mi<double, false>(Wm * b2));
+            }
+            cpx<double> Yk = Xk * cvt<double>(ldg(H + k));
+            cpx<double> Ym = Xm * cvt<double>(ldg(H + (Mr - k)));
+            cpx<double> Wi = conj(Wk);
+            cpx<double> Zk2 = (Yk + conj(Ym)) + mul_mi<double, true>(Wi * (Yk - conj(Ym)));
+            Z[Swz<Rl>::f(jk)] = cvt<Rl>(Zk2);
+            if (k != 0 && km != k) {
+                cpx<double> Wmi = scale(-1.0, Wk);
+                cpx<double> Zm2 = (Ym + conj(Yk)) + mul_mi<double, true>(Wmi * (Ym - conj(Yk)));
+                Z[Swz<Rl>::f(jm)] = cvt<Rl>(Zm2);
+            }
+        }
+        __syncthreads();
+        cpx<Rl>* Y = block_fft<Rl, true>(Z, nullptr, HM, tw);
+        if (par) {
+            for (int m = tid; m < HM; m += T) {
+                const int pos = Swz<Rl>::f(split_pos(m, HM, Ph));
+                Y[pos] = Y[pos] * twiddle<Rl, true>(tw, (unsigned)m << tsh);
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            cl_fence();
+            cl_st_release(cl_map(&box->done[par], 0), (unsigned)seen);
+        }
+    }
+}
+
+// Persistent solver with Raman clusters (launched with clusters of 3 CTAs). Phase 1: each
+// cluster integrates the instances of `big` (FP32 Raman buffers too large for one CTA's
+// shared memory), rank 0 running the solver and ranks 1-2 the Raman halves. Phase 2: once
+// `big` is empty, every CTA integrates instances of `reg` on its own (no cluster traffic).
+template <typename Rl, typename Kt>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, const int* reg, int nreg,
+                int* reg_counter, TwTab<Rl> tw, int smem_bytes, int* err) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(256) char smem[];
+    __shared__ Ctl ctl;
+    __shared__ ClBox box;
+    __shared__ int sidx;
+    cg::cluster_group cl = cg::this_cluster();
+    const unsigned rank = cl.block_rank();
+    if (threadIdx.x == 0) {
+        box.seq = 0;
+        box.cmd = 0;
+        box.done[0] = box.done[1] = 0;
+        box.inst = -1;
+    }
+    cl.sync();  // every mailbox is initialised before any remote write
+    if (rank == 0) {
+        while (true) {
+            __syncthreads();
+            if (threadIdx.x == 0) sidx = (box.cmd == -1) ? nbig : atomicAdd(big_counter, 1);
+            __syncthreads();
+            const int q = sidx;
+            if (q >= nbig) break;
+            const int i = big[q];
+            LunaInst& I = insts[i];
+            if (threadIdx.x == 0) {
+                unsigned long long t;
+                unsigned int sm;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+                I.t_begin = t;
+                I.sm = (int)sm;
+                box.inst = i;
+            }
+            __syncthreads();
+            Ws<Rl> w;
+            plan_ws<Rl>(I, smem, smem_bytes, w, tw, nullptr, true);
+            w.cl = &box;
+            w.rem_e = cl.map_shared_rank(reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES), 1);
+            w.rem_o = cl.map_shared_rank(reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES), 2);
+            solve_instance<Rl, Kt>(I, w, ctl);
+            if (threadIdx.x == 0) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                I.t_end = t;
+            }
+        }
+        // release the helpers (not after a timeout: they may have left already)
+        if (threadIdx.x == 0 && box.cmd != -1) {
+            const int seq = ++box.seq;
+            for (unsigned h = 1; h <= 2; ++h) cl_st(cl_map(&box.cmd, h), CL_EXIT);
+            cl_fence();
+            for (unsigned h = 1; h <= 2; ++h) cl_st_release(cl_map(&box.seq, h), (unsigned)seq);
+        }
+        __syncthreads();
+    } else if (rank <= 2) {
+        raman_helper<Rl>(insts, smem, tw, rank, &box, err);
+    }
+    __syncthreads();
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) sidx = atomicAdd(reg_counter, 1);
+        __syncthreads();
+        const int q = sidx;
+        if (q >= nreg) break;
+        LunaInst& I = insts[reg[q]];
         if (threadIdx.x == 0) {
             unsigned long long t;
             unsigned int sm;
@@ -222,6 +422,12 @@ struct luna_batch {
     std::vector<LunaInst> h;
     LunaInst* d_insts = nullptr;
     int* d_counter = nullptr;
+    // Raman clusters (mixed precision): instances whose FP32 Raman buffer does not fit in
+    // one CTA's shared memory run on clusters of 3 CTAs; the rest in cost order
+    int nbig = 0, nreg = 0, cl_grid = 0;
+    int* d_big = nullptr;
+    int* d_reg = nullptr;
+    int* d_cl_counters = nullptr;  // [0] big, [1] regular, [2] error flag
     std::vector<void*> allocs;
     std::vector<double2*> y0buf;  // per instance y (holds y0 before the run)
     std::vector<double2*> ybuf, ynbuf;
@@ -573,6 +779,55 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
     }
     if (occ < 1) return bail(fail(LUNA_ERR_CUDA, "batch_create: solver kernel does not fit on an SM"));
     b->grid = std::min(n, nsm * occ);
+    if (prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
+        // Raman clusters for the instances whose Raman buffer alone overflows one CTA
+        const int maxs = max_smem_optin();
+        std::vector<int> big, reg;
+        std::vector<double> cost(n);
+        for (int i = 0; i < n; ++i) {
+            const LunaInst& I = b->h[i];
+            const size_t half = align_up((size_t)(I.No / 2) * sizeof(float2), 256);
+            const size_t efac = align_up((size_t)I.Nw * sizeof(float2), 256);
+            const bool fits1 = smem_wanted<float>(I) <= (size_t)maxs;
+            const bool ok_cl = I.kind == 0 && has_raman(I) && !fits1 &&
+                               LUNA_SMALL_BYTES + half + efac <= (size_t)std::min<int>(maxs, b->smem);
+            if (ok_cl) big.push_back(i);
+            else reg.push_back(i);
+            cost[i] = (double)I.No * std::log2((double)I.No) * (has_raman(I) ? 2.0 : 1.0);
+        }
+        std::stable_sort(reg.begin(), reg.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+        if (!big.empty()) {
+            if (cudaFuncSetAttribute(solve_kernel_cl<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b->smem) != cudaSuccess)
+                return bail(fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size (clusters)"));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = 3;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(3 * 64, 1, 1);
+            cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+            cfg.dynamicSmemBytes = b->smem;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, solve_kernel_cl<float, float>, &cfg) != cudaSuccess || ncl < 1) {
+                cudaGetLastError();
+                ncl = 0;
+            }
+            if (ncl >= 1) {
+                b->nbig = (int)big.size();
+                b->nreg = (int)reg.size();
+                b->cl_grid = 3 * ncl;
+                std::vector<int> regp(reg);
+                if (regp.empty()) regp.push_back(0);  // never read (nreg == 0)
+                if (upload(b->allocs, big.data(), big.size(), (const int**)&b->d_big) ||
+                    upload(b->allocs, regp.data(), regp.size(), (const int**)&b->d_reg) ||
+                    dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
+                    return bail(LUNA_ERR_CUDA);
+            }
+        }
+    }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
         return bail(fail(LUNA_ERR_CUDA, "batch_create: stream/event creation failed"));
@@ -625,11 +880,29 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
     // instances restart from y0: restore the per-instance pointers and counters
     CK(cudaMemcpyAsync(b->d_insts, b->h.data(), sizeof(LunaInst) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
+    if (b->cl_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
-    if (b->precision == LUNA_PREC_FP64)
+    if (b->precision == LUNA_PREC_FP64) {
         solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem);
-    else
+    } else if (b->cl_grid > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = 3;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(b->cl_grid, 1, 1);
+        cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+        cfg.dynamicSmemBytes = b->smem;
+        cfg.stream = b->stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int* c = b->d_cl_counters;
+        CK(cudaLaunchKernelEx(&cfg, solve_kernel_cl<float, float>, b->d_insts, (const int*)b->d_big, b->nbig, c,
+                              (const int*)b->d_reg, b->nreg, c + 1, tw.f, b->smem, c + 2));
+    } else {
         solve_kernel<float, float><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.f, b->smem);
+    }
     CK(cudaGetLastError());
     CK(cudaEventRecord(b->ev1, b->stream));
     CK(cudaEventSynchronize(b->ev1));

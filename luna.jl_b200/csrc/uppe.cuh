@@ -32,7 +32,29 @@ struct Ws {
     double* edge;       // 4 edge values carried between scan chunks
     int* flag;          // status flags raised inside the RHS
     TwTab<Rl> tw;
+    // Raman convolution on two helper CTAs of a thread-block cluster (rank 1: even,
+    // rank 2: odd frequency half); null when the convolution runs in this CTA
+    struct ClBox* cl;
+    const cpx<Rl>* rem_e;  // helper buffers in distributed shared memory
+    const cpx<Rl>* rem_o;
 };
+
+// Mailbox of one CTA of a Raman cluster (static shared memory). Rank 0 writes the
+// command fields of the helpers' boxes and then their `seq` (release); helper h writes
+// `done[h-1]` of rank 0's box (release) when its half of the convolution is ready.
+struct ClBox {
+    int seq;
+    int cmd;
+    unsigned xaddr;  // shared-window offset of rank 0's field buffer
+    int P;           // split factor of that buffer
+    int M;           // pairs in that buffer (No/2)
+    int inst;        // instance index
+    float sc;        // field scale of the stored samples
+    int done[2];
+};
+
+#define CL_RAMAN 1
+#define CL_EXIT 2
 
 struct Ctl {  // controller state shared by the CTA (shared memory)
     void* k[7];  // stage derivative buffers (FSAL rotates k1 and k7)
@@ -81,7 +103,9 @@ __host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
 
 template <typename Rl>
 __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w, const TwTab<Rl>& tw,
-                        void* gscr = nullptr) {
+                        void* gscr = nullptr, bool raman_remote = false) {
+    w.cl = nullptr;
+    w.rem_e = w.rem_o = nullptr;
     w.red = reinterpret_cast<double*>(smem);
     w.tot = w.red + 3 * LUNA_WARPS;
     w.edge = w.tot + 3 * LUNA_WARPS;
@@ -111,7 +135,7 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
     }
     goff += eb;
     w.ram = w.ram_alt = nullptr;
-    if (has_raman(I)) {
+    if (has_raman(I) && !raman_remote) {
         size_t rb = align_up((size_t)I.No * c, 256);
         if (off + rb <= (size_t)smem_bytes) {
             w.ram = reinterpret_cast<cpx<Rl>*>(smem + off);
@@ -307,6 +331,69 @@ __device__ __forceinline__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>
     return block_fft<Rl, true>(Z, other, No, w.tw);
 }
 
+// ------------------------------------------------------------------ Raman clusters
+#define CL_WAIT_CYCLES (4000000000LL)  // ~2 s at the B200 boost clock
+
+__device__ __forceinline__ unsigned cl_map(const void* p, unsigned rank) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    unsigned r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cl_st(unsigned caddr, unsigned v) {
+    asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(caddr), "r"(v) : "memory");
+}
+__device__ __forceinline__ void cl_st_release(unsigned caddr, unsigned v) {
+    asm volatile("st.release.cluster.shared::cluster.u32 [%0], %1;" ::"r"(caddr), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned cl_ld_acquire(const void* p) {
+    const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+    unsigned v;
+    asm volatile("ld.acquire.cluster.shared::cta.u32 %0, [%1];" : "=r"(v) : "r"(a) : "memory");
+    return v;
+}
+__device__ __forceinline__ void cl_fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
+
+// Rank 0 of a Raman cluster: post the field buffer x (shared memory, split factor P) to
+// both helpers and wait, bounded, until each holds its half of the convolution. False
+// after a timeout (or once the cluster is marked broken): the caller then drops the
+// Raman term and raises ST_WAIT_TIMEOUT, and no further command is posted.
+template <typename Rl>
+__device__ bool raman_remote(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, double sc, int inst) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ClBox* box = w.cl;
+        int ok = box->cmd != -1;  // -1 marks a broken cluster
+        if (ok) {
+            const int seq = ++box->seq;
+            const unsigned xa = (unsigned)__cvta_generic_to_shared(x);
+            for (unsigned h = 1; h <= 2; ++h) {
+                cl_st(cl_map(&box->cmd, h), CL_RAMAN);
+                cl_st(cl_map(&box->xaddr, h), xa);
+                cl_st(cl_map(&box->P, h), (unsigned)P);
+                cl_st(cl_map(&box->M, h), (unsigned)M);
+                cl_st(cl_map(&box->inst, h), (unsigned)inst);
+                cl_st(cl_map(&box->sc, h), __float_as_uint((float)sc));
+            }
+            cl_fence();
+            for (unsigned h = 1; h <= 2; ++h) cl_st_release(cl_map(&box->seq, h), (unsigned)seq);
+            const long long t0 = clock64();
+            while (!((int)cl_ld_acquire(&box->done[0]) == seq && (int)cl_ld_acquire(&box->done[1]) == seq)) {
+                if (clock64() - t0 > CL_WAIT_CYCLES) {
+                    ok = 0;
+                    box->cmd = -1;
+                    break;
+                }
+            }
+        }
+        if (!ok) atomicOr(w.flag, 1 << ST_WAIT_TIMEOUT);
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // ------------------------------------------------------------------ plasma chunk
 // PlasmaScalar! (Nonlinear.jl:121-133) for the pair of samples (2m, 2m+1) held by this
 // thread. Each running trapezoid is written as dt*(prefix_sum(y)[n] - (y[0]+y[n])/2), so
@@ -352,6 +439,55 @@ __device__ __forceinline__ void plasma_pair(const LunaResp& r, bool act, int m, 
     cr.c3 += tot;
     P0 += r.coef * (dt * (U0 - 0.5 * (y0J + J0)));
     P1 += r.coef * (dt * (U1 - 0.5 * (y0J + J1)));
+}
+
+// PlasmaScalar! for the two consecutive pairs (samples 4t..4t+3 of a chunk) held by this
+// thread: as plasma_pair, with the thread's four samples summed in order before each
+// block scan (half the chunks, and two independent rate evaluations per thread).
+template <typename Rl>
+__device__ __forceinline__ void plasma_quad(const LunaResp& r, const bool act[2], int m0, const double E[4],
+                                            PlasmaCarry& cr, Ws<Rl>& w, double Pq[4]) {
+    const double dt = r.dt, er = r.eratio;
+    double rr[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) rr[s] = act[s >> 1] ? (double)eval_rate<Rl>(r, (Rl)fabs(E[s]), w.flag) : 0.0;
+    if (m0 == 0) w.edge[0] = rr[0];
+    double tot;
+    double x = block_exscan(((rr[0] + rr[1]) + rr[2]) + rr[3], w.tot, tot);
+    const double y0r = w.edge[0];
+    double S = cr.c1 + x;
+    cr.c1 += tot;
+    double fr[4], ph[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        S += rr[s];
+        const double f = dt * (S - 0.5 * (y0r + rr[s]));
+        fr[s] = r.preion + 1.0 - ((f == 0.0) ? 1.0 : exp(-f));
+        ph[s] = act[s >> 1] ? fr[s] * er * E[s] : 0.0;
+    }
+    if (m0 == 0) w.edge[1] = ph[0];
+    x = block_exscan(((ph[0] + ph[1]) + ph[2]) + ph[3], w.tot + LUNA_WARPS, tot);
+    const double y0p = w.edge[1];
+    double T = cr.c2 + x;
+    cr.c2 += tot;
+    double J[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        T += ph[s];
+        J[s] = dt * (T - 0.5 * (y0p + ph[s]));
+        if (act[s >> 1] && fabs(E[s]) > 0) J[s] += r.ionpot * rr[s] * (1.0 - fr[s]) / E[s];
+        if (!act[s >> 1]) J[s] = 0;
+    }
+    if (m0 == 0) w.edge[2] = J[0];
+    x = block_exscan(((J[0] + J[1]) + J[2]) + J[3], w.tot + 2 * LUNA_WARPS, tot);
+    const double y0J = w.edge[2];
+    double U = cr.c3 + x;
+    cr.c3 += tot;
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+        U += J[s];
+        Pq[s] += r.coef * (dt * (U - 0.5 * (y0J + J[s])));
+    }
 }
 
 // ------------------------------------------------------------------ the right-hand sides
@@ -406,7 +542,14 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
     }
     const int Pr_split = (ir >= 0) ? buf_split<Rl>(w.ram_alt, I.No) : 1;
     cpx<Rl>* Pr = nullptr;
-    if (ir >= 0) {
+    // Raman halves on the helper CTAs: P_raman[m] = even[m] + odd[m] in split order of
+    // the helpers' No/2-point transforms
+    const bool remote = (ir >= 0) && (w.cl != nullptr);
+    const int Ph = remote ? fft_nsplit<Rl>(M) : 1;
+    bool rem_ok = true;
+    if (remote) {
+        rem_ok = raman_remote<Rl>(w, x, M, P, sc, w.cl->inst);
+    } else if (ir >= 0) {
         // E^2 on the first half of the 2*No grid (thg=true form of sqr!), split order
         for (int m = tid; m < I.No; m += T) {
             cpx<Rl> v = mk<Rl>(0, 0);
@@ -420,6 +563,55 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
         Pr = raman_conv<Rl>(I.resp[ir], I.No, w);
     }
     PlasmaCarry cr = {0, 0, 0};
+    if (ip >= 0) {
+        // chunks of 2*T pairs, two consecutive pairs per thread
+        for (int c0 = 0; c0 < M; c0 += 2 * T) {
+            const int m0 = c0 + 2 * tid;
+            const bool act[2] = {m0 < M, m0 + 1 < M};
+            int pos[2];
+            double E[4];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                pos[q] = Swz<Rl>::f(split_pos(act[q] ? m0 + q : 0, M, P));
+                const cpx<Rl> e = act[q] ? x[pos[q]] : mk<Rl>(0, 0);
+                E[2 * q] = (double)e.x * sc;
+                E[2 * q + 1] = (double)e.y * sc;
+            }
+            double Pq[4] = {0, 0, 0, 0};
+            for (int i = 0; i < I.nresp; ++i) {
+                const LunaResp& r = I.resp[i];
+                if (r.kind == LUNA_RESP_KERR_FIELD) {
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) Pq[s] += r.coef * (E[s] * E[s] * E[s]);
+                } else if (i == ir) {
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int m = m0 + q;
+                        cpx<Rl> pr;
+                        if (remote) {
+                            const int ph = Swz<Rl>::f(split_pos(act[q] ? m : 0, M, Ph));
+                            pr = (act[q] && rem_ok) ? w.rem_e[ph] + w.rem_o[ph] : mk<Rl>(0, 0);
+                        } else {
+                            pr = act[q] ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
+                        }
+                        Pq[2 * q] += r.coef * E[2 * q] * (double)pr.x;
+                        Pq[2 * q + 1] += r.coef * E[2 * q + 1] * (double)pr.y;
+                    }
+                } else if (i == ip) {
+                    plasma_quad<Rl>(r, act, m0, E, cr, w, Pq);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                if (!act[q]) continue;
+                const int m = m0 + q;
+                const double tw0 = __ldg(I.towin + 2 * m), tw1 = __ldg(I.towin + 2 * m + 1);
+                x[pos[q]] = mk<Rl>((Rl)(Pq[2 * q] * tw0), (Rl)(Pq[2 * q + 1] * tw1));
+            }
+        }
+        __syncthreads();
+        return;
+    }
     for (int c0 = 0; c0 < M; c0 += T) {
         const int m = c0 + tid;
         const bool act = m < M;
@@ -433,7 +625,13 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
                 P0 += r.coef * (E0 * E0 * E0);
                 P1 += r.coef * (E1 * E1 * E1);
             } else if (i == ir) {
-                cpx<Rl> p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
+                cpx<Rl> p;
+                if (remote) {
+                    const int ph = Swz<Rl>::f(split_pos(m, M, Ph));
+                    p = (act && rem_ok) ? w.rem_e[ph] + w.rem_o[ph] : mk<Rl>(0, 0);
+                } else {
+                    p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
+                }
                 P0 += r.coef * E0 * (double)p.x;
                 P1 += r.coef * E1 * (double)p.y;
             } else if (i == ip) {
@@ -782,6 +980,10 @@ __device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, dou
     }
     if (flags & (1 << ST_FIELD_ABOVE_EMAX)) {
         c.status = ST_FIELD_ABOVE_EMAX;
+        c.done = 1;
+    }
+    if (flags & (1 << ST_WAIT_TIMEOUT)) {
+        c.status = ST_WAIT_TIMEOUT;
         c.done = 1;
     }
     if (I.max_steps > 0 && c.steps >= I.max_steps && !c.done) {

@@ -64,8 +64,11 @@ C_PROBE = r"""
 int main(void) {
     printf("luna_grid_desc %zu\nluna_resp_desc %zu\nluna_solve_opts %zu\nluna_solve_stats %zu\n",
            sizeof(luna_grid_desc), sizeof(luna_resp_desc), sizeof(luna_solve_opts), sizeof(luna_solve_stats));
+    printf("luna_radial_desc %zu\n", sizeof(luna_radial_desc));
     P(luna_grid_desc, in_scale); P(luna_resp_desc, spl_n); P(luna_resp_desc, adk_thr);
     P(luna_resp_desc, hdt); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
+    P(luna_solve_opts, replay); P(luna_solve_opts, nreplay); P(luna_solve_opts, flags);
+    P(luna_radial_desc, Mf); P(luna_radial_desc, outfac);
     P(luna_solve_stats, z); P(luna_solve_stats, dz);
     return 0;
 }
@@ -89,5 +92,10 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_resp_desc.hdt"]) == _lib.RespDesc.hdt.offset
     assert int(out["luna_solve_opts.zsave"]) == _lib.SolveOpts.zsave.offset
     assert int(out["luna_solve_opts.steplog_cap"]) == _lib.SolveOpts.steplog_cap.offset
+    assert int(out["luna_radial_desc"]) == ctypes.sizeof(_lib.RadialDesc)
+    for f in ("replay", "nreplay", "flags"):
+        assert int(out[f"luna_solve_opts.{f}"]) == getattr(_lib.SolveOpts, f).offset
+    for f in ("Mf", "outfac"):
+        assert int(out[f"luna_radial_desc.{f}"]) == getattr(_lib.RadialDesc, f).offset
     assert int(out["luna_solve_stats.z"]) == _lib.SolveStats.z.offset
     assert int(out["luna_solve_stats.dz"]) == _lib.SolveStats.dz.offset

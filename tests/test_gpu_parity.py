@@ -240,3 +240,33 @@ def test_batch_is_deterministic_and_matches_single_solves():
         s = single.results()[0]
         assert np.array_equal(s.Eω, r1[i].Eω) and np.array_equal(s.y, r1[i].y)
     del zs
+
+
+def test_raman_cluster_path_matches_single_cta_and_fp64():
+    """Mixed-precision instances whose FP32 Raman buffer exceeds one CTA's shared memory
+    (H2, No = 32768) run on a 3-CTA cluster: the two helper CTAs hold the even and odd
+    frequency halves of the Raman convolution. Following the FP64 path's step sequence,
+    the cluster result agrees with the single-CTA mixed path to FP32 rounding and with the
+    FP64 path to the mixed-precision level."""
+    from luna_b200 import scan
+    p = scan.build_problem(scan.draw_instances(256)[93], saveN=201)
+    assert p.grid.No == 32768 and any(r.kind == "raman_field" for r in p.transform.resp)
+    zs = np.linspace(0.0, p.grid.zmax, 201)
+
+    def run(prec, flags=0, replay=None, log=0):
+        plan = P.Plan.from_transform(p.transform, prec)
+        b = P.Batch([plan], 201, zs, max_dt=p.grid.zmax / 2, max_steps=30, steplog_cap=log,
+                    replay=replay, flags=flags)
+        b.upload([p.linop], [p.Eω], [0.0], [1e-4], [p.grid.zmax])
+        b.run()
+        return b.results()[0]
+
+    r64 = run(_lib.PREC_FP64, log=40)
+    replay = np.stack([r64.steplog[:, 1], r64.steplog[:, 3]], axis=1).ravel()
+    rc = run(_lib.PREC_MIXED, replay=replay)
+    rs = run(_lib.PREC_MIXED, flags=_lib.SOLVE_NO_CLUSTERS, replay=replay)
+    assert r64.status == rc.status == rs.status == _lib.LUNA_STEP_BUDGET
+    e_c, e_s, e_cs = rel(rc.y, r64.y), rel(rs.y, r64.y), rel(rc.y, rs.y)
+    assert e_c < 1e-4 and e_s < 1e-4, (e_c, e_s)
+    assert e_cs < 1e-5, e_cs
+    assert not np.array_equal(rc.y, rs.y)  # the cluster path did run

@@ -452,6 +452,7 @@ def main():
         return float(t.item())
 
     batch.upload(Lh, Yh, z0, dz0, zmax, zsaves, max_dts)
+    batch.set_priority([scan.schedule_priority(p, q) for p, q in zip(inst, probs)])
     for _ in range(args.warmup):
         batch.run()
     dev_ms, e2e_s, stats = [], [], None

@@ -150,6 +150,9 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms);
 int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
                              luna_solve_stats* stats);
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
+/* Processing order of a batch (no counterpart in the reference): instances with a larger
+ * priority[i] are started first ([n] doubles, e.g. an estimate of the instance's work). */
+int luna_b200_batch_set_priority(luna_batch* b, const double* priority);
 /* Scheduling record of the last run (no counterpart in the reference): per instance the
  * start and end of its integration in seconds from the earliest start ([2*n] doubles) and
  * the SM that integrated it ([n] ints, may be NULL). */

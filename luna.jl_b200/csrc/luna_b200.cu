@@ -23,9 +23,10 @@ using namespace luna;
 
 // Persistent solver: each CTA pulls instances from `counter` until the list is empty and
 // integrates each one to completion (RK45.solve loop, RK45.jl:43-78).
+// With `list`, the q-th instance pulled is insts[list[q]] (q < n), else insts[q].
 template <typename Rl, typename Kt>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
-solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes) {
+solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes, const int* list) {
     extern __shared__ __align__(256) char smem[];
     __shared__ Ctl ctl;
     __shared__ int sidx;
@@ -33,9 +34,9 @@ solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes)
         __syncthreads();
         if (threadIdx.x == 0) sidx = atomicAdd(counter, 1);
         __syncthreads();
-        const int i = sidx;
-        if (i >= n) break;
-        LunaInst& I = insts[i];
+        const int q = sidx;
+        if (q >= n) break;
+        LunaInst& I = insts[list ? list[q] : q];
         if (threadIdx.x == 0) {
             unsigned long long t;
             unsigned int sm;
@@ -66,8 +67,8 @@ solve_kernel(LunaInst* insts, int n, int* counter, TwTab<Rl> tw, int smem_bytes)
 // with Mr-k, which has the parity of k. Each helper therefore holds one half (HM points)
 // in its own shared memory; rank 0 adds the two halves (distributed shared memory).
 template <typename Rl>
-__device__ void raman_helper(const LunaInst* insts, char* smem, const TwTab<Rl>& tw, unsigned rank, ClBox* box,
-                             int* err) {
+__device__ void cluster_helper(LunaInst* insts, char* smem, int smem_bytes, const TwTab<Rl>& tw, unsigned rank,
+                               ClBox* box, int* err) {
     namespace cg = cooperative_groups;
     const int tid = threadIdx.x, T = LUNA_BLOCK;
     cpx<Rl>* buf = reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES);
@@ -94,6 +95,28 @@ __device__ void raman_helper(const LunaInst* insts, char* smem, const TwTab<Rl>&
         seen = box->seq;
         if (box->cmd != CL_RAMAN) return;  // CL_EXIT
         const LunaInst& I = insts[box->inst];
+        if (rank == 3) {
+            // plasma helper: rho * P_plasma of every sample into this CTA's buffer
+            int ip = -1;
+            for (int i = 0; i < I.nresp; ++i)
+                if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
+            Ws<Rl> w;
+            plan_ws<Rl>(I, smem, smem_bytes, w, tw, nullptr, true);
+            if (tid == 0) *w.flag = 0;
+            __syncthreads();
+            if (ip >= 0) {
+                const cpx<Rl>* xr = cooperative_groups::this_cluster().map_shared_rank(
+                    reinterpret_cast<cpx<Rl>*>(__cvta_shared_to_generic(box->xaddr)), 0);
+                plasma_only<Rl>(I, w, xr, w.main, box->M, box->P, (double)box->sc, ip);
+            }
+            __syncthreads();
+            if (tid == 0) {
+                cl_st(cl_map(&box->pflag, 0), (unsigned)*w.flag);
+                cl_fence();
+                cl_st_release(cl_map(&box->done[2], 0), (unsigned)seen);
+            }
+            continue;
+        }
         const LunaResp* rr = nullptr;
         for (int i = 0; i < I.nresp; ++i)
             if (I.resp[i].kind == LUNA_RESP_RAMAN) rr = &I.resp[i];
@@ -181,7 +204,8 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
     if (threadIdx.x == 0) {
         box.seq = 0;
         box.cmd = 0;
-        box.done[0] = box.done[1] = 0;
+        for (int h = 0; h < CL_HELPERS; ++h) box.done[h] = 0;
+        box.pflag = 0;
         box.inst = -1;
     }
     cl.sync();  // every mailbox is initialised before any remote write
@@ -209,6 +233,7 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
             w.cl = &box;
             w.rem_e = cl.map_shared_rank(reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES), 1);
             w.rem_o = cl.map_shared_rank(reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES), 2);
+            w.rem_p = cl.map_shared_rank(reinterpret_cast<cpx<Rl>*>(smem + LUNA_SMALL_BYTES), 3);
             solve_instance<Rl, Kt>(I, w, ctl);
             if (threadIdx.x == 0) {
                 unsigned long long t;
@@ -219,13 +244,13 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
         // release the helpers (not after a timeout: they may have left already)
         if (threadIdx.x == 0 && box.cmd != -1) {
             const int seq = ++box.seq;
-            for (unsigned h = 1; h <= 2; ++h) cl_st(cl_map(&box.cmd, h), CL_EXIT);
+            for (unsigned h = 1; h <= CL_HELPERS; ++h) cl_st(cl_map(&box.cmd, h), CL_EXIT);
             cl_fence();
-            for (unsigned h = 1; h <= 2; ++h) cl_st_release(cl_map(&box.seq, h), (unsigned)seq);
+            for (unsigned h = 1; h <= CL_HELPERS; ++h) cl_st_release(cl_map(&box.seq, h), (unsigned)seq);
         }
         __syncthreads();
-    } else if (rank <= 2) {
-        raman_helper<Rl>(insts, smem, tw, rank, &box, err);
+    } else if (rank <= CL_HELPERS) {
+        cluster_helper<Rl>(insts, smem, smem_bytes, tw, rank, &box, err);
     }
     __syncthreads();
     while (true) {
@@ -428,6 +453,7 @@ struct luna_batch {
     int* d_big = nullptr;
     int* d_reg = nullptr;
     int* d_cl_counters = nullptr;  // [0] big, [1] regular, [2] error flag
+    std::vector<int> big, reg;     // host copies of the two lists
     std::vector<void*> allocs;
     std::vector<double2*> y0buf;  // per instance y (holds y0 before the run)
     std::vector<double2*> ybuf, ynbuf;
@@ -437,7 +463,9 @@ struct luna_batch {
     int smem = 0;
     int grid = 0;
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaStream_t stream2 = nullptr;  // single-CTA solver beside the cluster solver
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf = nullptr, evj = nullptr;
+    int reg_grid = 0;
 };
 
 namespace {
@@ -802,10 +830,10 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
             cudaLaunchConfig_t cfg = {};
             cudaLaunchAttribute at[1];
             at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = 3;
+            at[0].val.clusterDim.x = CL_HELPERS + 1;
             at[0].val.clusterDim.y = 1;
             at[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3(3 * 64, 1, 1);
+            cfg.gridDim = dim3((CL_HELPERS + 1) * 32, 1, 1);
             cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
             cfg.dynamicSmemBytes = b->smem;
             cfg.attrs = at;
@@ -816,9 +844,15 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
                 ncl = 0;
             }
             if (ncl >= 1) {
+                b->big = big;
+                b->reg = reg;
                 b->nbig = (int)big.size();
                 b->nreg = (int)reg.size();
-                b->cl_grid = 3 * ncl;
+                // clusters for the big instances (no more than there are), single CTAs
+                // on the remaining SMs; both pull the regular instances
+                ncl = std::min(ncl, (int)big.size());
+                b->cl_grid = (CL_HELPERS + 1) * ncl;
+                b->reg_grid = std::max(0, std::min((int)reg.size(), nsm - b->cl_grid));
                 std::vector<int> regp(reg);
                 if (regp.empty()) regp.push_back(0);  // never read (nreg == 0)
                 if (upload(b->allocs, big.data(), big.size(), (const int**)&b->d_big) ||
@@ -829,7 +863,10 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         }
     }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess)
+        cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->evf, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->evj, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(LUNA_ERR_CUDA, "batch_create: stream/event creation failed"));
     *out = b;
     return LUNA_OK;
@@ -883,12 +920,12 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
     if (b->cl_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
     if (b->precision == LUNA_PREC_FP64) {
-        solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem);
+        solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem, nullptr);
     } else if (b->cl_grid > 0) {
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
         at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = 3;
+        at[0].val.clusterDim.x = CL_HELPERS + 1;
         at[0].val.clusterDim.y = 1;
         at[0].val.clusterDim.z = 1;
         cfg.gridDim = dim3(b->cl_grid, 1, 1);
@@ -898,10 +935,21 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
         cfg.attrs = at;
         cfg.numAttrs = 1;
         int* c = b->d_cl_counters;
+        if (b->reg_grid > 0) {
+            CK(cudaEventRecord(b->evf, b->stream));
+            CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
+        }
         CK(cudaLaunchKernelEx(&cfg, solve_kernel_cl<float, float>, b->d_insts, (const int*)b->d_big, b->nbig, c,
                               (const int*)b->d_reg, b->nreg, c + 1, tw.f, b->smem, c + 2));
+        if (b->reg_grid > 0) {
+            // the single-CTA solver on the other SMs, submitted after the clusters
+            solve_kernel<float, float><<<b->reg_grid, LUNA_BLOCK, b->smem, b->stream2>>>(
+                b->d_insts, b->nreg, c + 1, tw.f, b->smem, (const int*)b->d_reg);
+            CK(cudaEventRecord(b->evj, b->stream2));
+            CK(cudaStreamWaitEvent(b->stream, b->evj, 0));
+        }
     } else {
-        solve_kernel<float, float><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.f, b->smem);
+        solve_kernel<float, float><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.f, b->smem, nullptr);
     }
     CK(cudaGetLastError());
     CK(cudaEventRecord(b->ev1, b->stream));
@@ -940,6 +988,17 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
     return LUNA_OK;
 }
 
+int luna_b200_batch_set_priority(luna_batch* b, const double* priority) {
+    if (!b || !priority) return fail(LUNA_ERR_BAD_ARG, "batch_set_priority: null argument");
+    if (b->cl_grid == 0) return LUNA_OK;  // single list in index order
+    auto by = [&](int a, int c) { return priority[a] > priority[c]; };
+    std::stable_sort(b->big.begin(), b->big.end(), by);
+    std::stable_sort(b->reg.begin(), b->reg.end(), by);
+    CK(cudaMemcpy(b->d_big, b->big.data(), sizeof(int) * b->big.size(), cudaMemcpyHostToDevice));
+    if (!b->reg.empty()) CK(cudaMemcpy(b->d_reg, b->reg.data(), sizeof(int) * b->reg.size(), cudaMemcpyHostToDevice));
+    return LUNA_OK;
+}
+
 int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm) {
     if (!b || !begin_end_s) return fail(LUNA_ERR_BAD_ARG, "batch_timeline: null argument");
     std::vector<LunaInst> res(b->n);
@@ -964,7 +1023,10 @@ void luna_b200_batch_destroy(luna_batch* b) {
     if (!b) return;
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->evf) cudaEventDestroy(b->evf);
+    if (b->evj) cudaEventDestroy(b->evj);
     if (b->stream) cudaStreamDestroy(b->stream);
+    if (b->stream2) cudaStreamDestroy(b->stream2);
     free_all(b->allocs);
     delete b;
 }

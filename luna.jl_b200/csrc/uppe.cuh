@@ -37,11 +37,13 @@ struct Ws {
     struct ClBox* cl;
     const cpx<Rl>* rem_e;  // helper buffers in distributed shared memory
     const cpx<Rl>* rem_o;
+    const cpx<Rl>* rem_p;  // plasma polarisation from the plasma helper (rank 3)
 };
 
-// Mailbox of one CTA of a Raman cluster (static shared memory). Rank 0 writes the
+// Mailbox of one CTA of a response cluster (static shared memory). Rank 0 writes the
 // command fields of the helpers' boxes and then their `seq` (release); helper h writes
-// `done[h-1]` of rank 0's box (release) when its half of the convolution is ready.
+// `done[h-1]` of rank 0's box (release) when its part of the responses is ready.
+#define CL_HELPERS 3
 struct ClBox {
     int seq;
     int cmd;
@@ -50,7 +52,8 @@ struct ClBox {
     int M;           // pairs in that buffer (No/2)
     int inst;        // instance index
     float sc;        // field scale of the stored samples
-    int done[2];
+    int done[CL_HELPERS];
+    int pflag;       // status bits raised by the plasma helper's rate evaluations
 };
 
 #define CL_RAMAN 1
@@ -105,7 +108,7 @@ template <typename Rl>
 __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w, const TwTab<Rl>& tw,
                         void* gscr = nullptr, bool raman_remote = false) {
     w.cl = nullptr;
-    w.rem_e = w.rem_o = nullptr;
+    w.rem_e = w.rem_o = w.rem_p = nullptr;
     w.red = reinterpret_cast<double*>(smem);
     w.tot = w.red + 3 * LUNA_WARPS;
     w.edge = w.tot + 3 * LUNA_WARPS;
@@ -354,12 +357,13 @@ __device__ __forceinline__ unsigned cl_ld_acquire(const void* p) {
 }
 __device__ __forceinline__ void cl_fence() { asm volatile("fence.acq_rel.cluster;" ::: "memory"); }
 
-// Rank 0 of a Raman cluster: post the field buffer x (shared memory, split factor P) to
-// both helpers and wait, bounded, until each holds its half of the convolution. False
-// after a timeout (or once the cluster is marked broken): the caller then drops the
-// Raman term and raises ST_WAIT_TIMEOUT, and no further command is posted.
+// Rank 0 of a response cluster: post the field buffer x (shared memory, split factor P)
+// to the helpers and wait, bounded, until the two Raman halves and the plasma
+// polarisation are in their shared memory. False after a timeout (or once the cluster is
+// marked broken): the caller then drops those terms and raises ST_WAIT_TIMEOUT, and no
+// further command is posted.
 template <typename Rl>
-__device__ bool raman_remote(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, double sc, int inst) {
+__device__ bool cluster_post_wait(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, double sc, int inst) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -368,7 +372,7 @@ __device__ bool raman_remote(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, double s
         if (ok) {
             const int seq = ++box->seq;
             const unsigned xa = (unsigned)__cvta_generic_to_shared(x);
-            for (unsigned h = 1; h <= 2; ++h) {
+            for (unsigned h = 1; h <= CL_HELPERS; ++h) {
                 cl_st(cl_map(&box->cmd, h), CL_RAMAN);
                 cl_st(cl_map(&box->xaddr, h), xa);
                 cl_st(cl_map(&box->P, h), (unsigned)P);
@@ -377,15 +381,19 @@ __device__ bool raman_remote(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, double s
                 cl_st(cl_map(&box->sc, h), __float_as_uint((float)sc));
             }
             cl_fence();
-            for (unsigned h = 1; h <= 2; ++h) cl_st_release(cl_map(&box->seq, h), (unsigned)seq);
+            for (unsigned h = 1; h <= CL_HELPERS; ++h) cl_st_release(cl_map(&box->seq, h), (unsigned)seq);
             const long long t0 = clock64();
-            while (!((int)cl_ld_acquire(&box->done[0]) == seq && (int)cl_ld_acquire(&box->done[1]) == seq)) {
+            while (true) {
+                bool all = true;
+                for (int h = 0; h < CL_HELPERS; ++h) all = all && ((int)cl_ld_acquire(&box->done[h]) == seq);
+                if (all) break;
                 if (clock64() - t0 > CL_WAIT_CYCLES) {
                     ok = 0;
                     box->cmd = -1;
                     break;
                 }
             }
+            if (ok && box->pflag) atomicOr(w.flag, box->pflag);
         }
         if (!ok) atomicOr(w.flag, 1 << ST_WAIT_TIMEOUT);
         s_ok = ok;
@@ -490,6 +498,35 @@ __device__ __forceinline__ void plasma_quad(const LunaResp& r, const bool act[2]
     }
 }
 
+// Plasma polarisation alone, for the plasma helper of a response cluster: the field is
+// read from xr (rank 0's buffer, split factor P) and rho * P_plasma is written to out at
+// the same positions.
+template <typename Rl>
+__device__ void plasma_only(const LunaInst& I, Ws<Rl>& w, const cpx<Rl>* xr, cpx<Rl>* out, int M, int P, double sc,
+                            int ip) {
+    const int T = LUNA_BLOCK, tid = threadIdx.x;
+    PlasmaCarry cr = {0, 0, 0};
+    for (int c0 = 0; c0 < M; c0 += 2 * T) {
+        const int m0 = c0 + 2 * tid;
+        const bool act[2] = {m0 < M, m0 + 1 < M};
+        int pos[2];
+        double E[4];
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            pos[q] = Swz<Rl>::f(split_pos(act[q] ? m0 + q : 0, M, P));
+            const cpx<Rl> e = act[q] ? xr[pos[q]] : mk<Rl>(0, 0);
+            E[2 * q] = (double)e.x * sc;
+            E[2 * q + 1] = (double)e.y * sc;
+        }
+        double Pq[4] = {0, 0, 0, 0};
+        plasma_quad<Rl>(I.resp[ip], act, m0, E, cr, w, Pq);
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (act[q]) out[pos[q]] = mk<Rl>((Rl)Pq[2 * q], (Rl)Pq[2 * q + 1]);
+    }
+    __syncthreads();
+}
+
 // ------------------------------------------------------------------ the right-hand sides
 // load(k) -> cpx<double> input bin k (k < Nw); store(k, v) consumes output bin k (k < Nw).
 
@@ -542,14 +579,40 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
     }
     const int Pr_split = (ir >= 0) ? buf_split<Rl>(w.ram_alt, I.No) : 1;
     cpx<Rl>* Pr = nullptr;
-    // Raman halves on the helper CTAs: P_raman[m] = even[m] + odd[m] in split order of
-    // the helpers' No/2-point transforms
-    const bool remote = (ir >= 0) && (w.cl != nullptr);
-    const int Ph = remote ? fft_nsplit<Rl>(M) : 1;
-    bool rem_ok = true;
-    if (remote) {
-        rem_ok = raman_remote<Rl>(w, x, M, P, sc, w.cl->inst);
-    } else if (ir >= 0) {
+    if (w.cl) {
+        // response cluster: Raman halves on ranks 1-2 (P_raman[m] = even[m] + odd[m] in
+        // the split order of their No/2-point transforms), plasma polarisation on rank 3
+        // (same positions as x); the responses are added here in tuple order
+        const bool ok = cluster_post_wait<Rl>(w, x, M, P, sc, w.cl->inst);
+        const int Ph = fft_nsplit<Rl>(M);
+        for (int m = tid; m < M; m += T) {
+            const int pos = Swz<Rl>::f(split_pos(m, M, P));
+            const cpx<Rl> e = x[pos];
+            const double E0 = (double)e.x * sc, E1 = (double)e.y * sc;
+            double P0 = 0, P1 = 0;
+            for (int i = 0; i < I.nresp; ++i) {
+                const LunaResp& r = I.resp[i];
+                if (r.kind == LUNA_RESP_KERR_FIELD) {
+                    P0 += r.coef * (E0 * E0 * E0);
+                    P1 += r.coef * (E1 * E1 * E1);
+                } else if (i == ir && ok) {
+                    const int ph = Swz<Rl>::f(split_pos(m, M, Ph));
+                    const cpx<Rl> pr = w.rem_e[ph] + w.rem_o[ph];
+                    P0 += r.coef * E0 * (double)pr.x;
+                    P1 += r.coef * E1 * (double)pr.y;
+                } else if (i == ip && ok) {
+                    const cpx<Rl> pl = w.rem_p[pos];
+                    P0 += (double)pl.x;
+                    P1 += (double)pl.y;
+                }
+            }
+            const double tw0 = __ldg(I.towin + 2 * m), tw1 = __ldg(I.towin + 2 * m + 1);
+            x[pos] = mk<Rl>((Rl)(P0 * tw0), (Rl)(P1 * tw1));
+        }
+        __syncthreads();
+        return;
+    }
+    if (ir >= 0) {
         // E^2 on the first half of the 2*No grid (thg=true form of sqr!), split order
         for (int m = tid; m < I.No; m += T) {
             cpx<Rl> v = mk<Rl>(0, 0);
@@ -587,13 +650,7 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
                         const int m = m0 + q;
-                        cpx<Rl> pr;
-                        if (remote) {
-                            const int ph = Swz<Rl>::f(split_pos(act[q] ? m : 0, M, Ph));
-                            pr = (act[q] && rem_ok) ? w.rem_e[ph] + w.rem_o[ph] : mk<Rl>(0, 0);
-                        } else {
-                            pr = act[q] ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
-                        }
+                        const cpx<Rl> pr = act[q] ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
                         Pq[2 * q] += r.coef * E[2 * q] * (double)pr.x;
                         Pq[2 * q + 1] += r.coef * E[2 * q + 1] * (double)pr.y;
                     }
@@ -625,13 +682,7 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
                 P0 += r.coef * (E0 * E0 * E0);
                 P1 += r.coef * (E1 * E1 * E1);
             } else if (i == ir) {
-                cpx<Rl> p;
-                if (remote) {
-                    const int ph = Swz<Rl>::f(split_pos(m, M, Ph));
-                    p = (act && rem_ok) ? w.rem_e[ph] + w.rem_o[ph] : mk<Rl>(0, 0);
-                } else {
-                    p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
-                }
+                cpx<Rl> p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
                 P0 += r.coef * E0 * (double)p.x;
                 P1 += r.coef * E1 * (double)p.y;
             } else if (i == ip) {

@@ -234,6 +234,11 @@ class Batch:
         _lib.check(_lib.load().luna_b200_batch_download(self._h, Sp, Yp, stats))
         return saves, ys, list(stats)
 
+    def set_priority(self, priority):
+        """Start instances with a larger priority first (an estimate of their work)."""
+        self._prio = _f64(priority)
+        _lib.check(_lib.load().luna_b200_batch_set_priority(self._h, _lib.dptr(self._prio)))
+
     def timeline(self):
         """(begin, end) seconds of every instance's integration in the last run, and the SM
         that ran it."""

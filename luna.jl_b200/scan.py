@@ -45,6 +45,22 @@ def cost_estimate(prob):
     return No * math.log2(No) * prob.grid.zmax
 
 
+def nonlinear_phase(p):
+    """Scale of the nonlinear phase of an instance, gamma3 * pressure * (energy/duration) *
+    length / radius^2 (arbitrary units): the step count of the adaptive integrator grows
+    with it, so it orders a batch's instances longest first."""
+    from . import physdata as pd
+    return (pd.gamma3_gas(p["gas"]) * p["pressure"] * p["energy"] / p["τfwhm"] * p["flength"]
+            / p["radius"] ** 2)
+
+
+def schedule_priority(p, prob):
+    """Estimated work of an instance: per-step transform cost times nonlinear phase^0.6."""
+    No = prob.grid.No
+    raman = any(r.kind in ("raman_field", "raman_env") for r in prob.transform.resp)
+    return No * math.log2(No) * (2.0 if raman else 1.0) * nonlinear_phase(p) ** 0.6
+
+
 def partition(costs, nparts):
     """Longest-processing-time-first split of instance indices into ``nparts`` shards."""
     order = np.argsort(-np.asarray(costs, dtype=np.float64), kind="stable")

@@ -150,6 +150,10 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms);
 int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
                              luna_solve_stats* stats);
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
+/* How a batch is scheduled (no counterpart in the reference): kernel launches per
+ * luna_b200_batch_run, instances integrated on response clusters (mixed precision,
+ * Raman buffers larger than one CTA's shared memory) and the number of clusters. */
+int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_instances, int* clusters);
 /* Processing order of a batch (no counterpart in the reference): instances with a larger
  * priority[i] are started first ([n] doubles, e.g. an estimate of the instance's work). */
 int luna_b200_batch_set_priority(luna_batch* b, const double* priority);

@@ -77,6 +77,7 @@ EXPORTS = [
     "luna_b200_radial_plan_create", "luna_b200_radial_plan_destroy", "luna_b200_radial_rhs",
     "luna_b200_radial_rhs_device", "luna_b200_radial_solve", "luna_b200_qdht_device",
     "luna_b200_batch_timeline", "luna_b200_batch_set_priority",
+    "luna_b200_batch_info",
 ]
 
 _lib = None
@@ -123,6 +124,7 @@ def load():
     lib.luna_b200_radial_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
     lib.luna_b200_radial_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
                                            POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
+    lib.luna_b200_batch_info.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]
     lib.luna_b200_batch_set_priority.argtypes = [c_void_p, PD]
     lib.luna_b200_batch_timeline.argtypes = [c_void_p, PD, POINTER(c_int)]
     lib.luna_b200_qdht_device.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p]

@@ -988,6 +988,14 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
     return LUNA_OK;
 }
 
+int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_instances, int* clusters) {
+    if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_info: null batch");
+    if (kernels_per_run) *kernels_per_run = (b->cl_grid > 0) ? 1 + (b->reg_grid > 0) : 1;
+    if (cluster_instances) *cluster_instances = (b->cl_grid > 0) ? b->nbig : 0;
+    if (clusters) *clusters = b->cl_grid / (CL_HELPERS + 1);
+    return LUNA_OK;
+}
+
 int luna_b200_batch_set_priority(luna_batch* b, const double* priority) {
     if (!b || !priority) return fail(LUNA_ERR_BAD_ARG, "batch_set_priority: null argument");
     if (b->cl_grid == 0) return LUNA_OK;  // single list in index order

@@ -234,6 +234,13 @@ class Batch:
         _lib.check(_lib.load().luna_b200_batch_download(self._h, Sp, Yp, stats))
         return saves, ys, list(stats)
 
+    def info(self):
+        """(kernel launches per run, instances on response clusters, clusters)."""
+        k, ci, cl = _lib.c_int(), _lib.c_int(), _lib.c_int()
+        _lib.check(_lib.load().luna_b200_batch_info(self._h, _lib.ctypes.byref(k), _lib.ctypes.byref(ci),
+                                                    _lib.ctypes.byref(cl)))
+        return k.value, ci.value, cl.value
+
     def set_priority(self, priority):
         """Start instances with a larger priority first (an estimate of their work)."""
         self._prio = _f64(priority)

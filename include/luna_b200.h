@@ -63,6 +63,11 @@ typedef struct {
     const double* towin;   /* [No] grid.towin                                            */
     const double* twin;    /* [N]  grid.twin                                             */
     double in_scale;       /* pad scale / No / (nlscale*sqrt(Aeff))                      */
+    /* per-step statistics (Stats.default); may be NULL / 0 when they are not requested */
+    const double* omega;   /* [Nw] grid.ω                                                */
+    const double* t;       /* [N]  grid.t                                                */
+    double aeff;           /* effective area Aeff                                        */
+    double escale;         /* 1/sqrt(ε0 c Aeff/2): mode-averaged field to V/m            */
 } luna_grid_desc;
 
 /* One nonlinear response, applied in the order given (Et_to_Pt!, NonlinearRHS.jl:121-126). */
@@ -100,7 +105,14 @@ typedef struct {
                                                   controller's choice (verification aid)      */
     long long nreplay;
     int flags;                                 /* LUNA_SOLVE_* bits, 0 for the defaults     */
+    long long stats_cap;                       /* rows of per-step statistics; 0: off       */
 } luna_solve_opts;
+
+/* Per-step statistics (Stats.default, Stats.jl:495-532, for a mode-averaged field-resolved
+ * transform), one row of LUNA_NSTATS doubles per accepted step, in this order:
+ * z, dz, ω0, energy, peakpower, peakintensity, fwhm_t_min, fwhm_t_max, electrondensity,
+ * peak_ionisation_rate (the last two NaN without a plasma response). */
+#define LUNA_NSTATS 10
 
 /* luna_solve_opts.flags */
 #define LUNA_SOLVE_NO_CLUSTERS 1 /* batches: integrate every instance on one CTA (no Raman
@@ -111,6 +123,7 @@ typedef struct {
     int nsaved;
     long long steps, accepted, rejected, nrhs;
     double z, dz; /* final z (first tn > zmax) and next step size */
+    long long nstats; /* rows of per-step statistics recorded */
 } luna_solve_stats;
 
 typedef struct luna_plan luna_plan;
@@ -150,6 +163,9 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms);
 int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const* y_out,
                              luna_solve_stats* stats);
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog);
+/* Per-step statistics of instance i ([LUNA_NSTATS * stats_cap] doubles; stats.nstats rows
+ * are valid) — the `stats` group a MemoryOutput collects through Stats.default. */
+int luna_b200_batch_stats(luna_batch* b, int i, double* stats);
 /* How a batch is scheduled (no counterpart in the reference): kernel launches per
  * luna_b200_batch_run, instances integrated on response clusters (mixed precision,
  * Raman buffers larger than one CTA's shared memory) and the number of clusters. */

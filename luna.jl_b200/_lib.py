@@ -21,6 +21,9 @@ LUNA_ERR_UNSUPPORTED = 17
 LUNA_ERR_CUDA = 18
 NOALLOC_SCRATCH_BYTES = 1 << 20
 SOLVE_NO_CLUSTERS = 1
+NSTATS = 10
+STATS_KEYS = ("z", "dz", "ω0", "energy", "peakpower", "peakintensity", "fwhm_t_min",
+              "fwhm_t_max", "electrondensity", "peak_ionisation_rate")
 
 RESP_KERR_FIELD = 1
 RESP_KERR_ENV = 2
@@ -37,7 +40,8 @@ PD = POINTER(c_double)
 class GridDesc(ctypes.Structure):
     _fields_ = [("kind", c_int), ("N", c_int), ("Nw", c_int), ("No", c_int),
                 ("outfac", PD), ("wwin", PD), ("towin", PD), ("twin", PD),
-                ("in_scale", c_double)]
+                ("in_scale", c_double), ("omega", PD), ("t", PD), ("aeff", c_double),
+                ("escale", c_double)]
 
 
 class RespDesc(ctypes.Structure):
@@ -60,13 +64,13 @@ class SolveOpts(ctypes.Structure):
                 ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
                 ("max_steps", c_longlong), ("saveN", c_int), ("zsave", PD),
                 ("steplog_cap", c_longlong), ("replay", PD), ("nreplay", c_longlong),
-                ("flags", c_int)]
+                ("flags", c_int), ("stats_cap", c_longlong)]
 
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("status", c_int), ("nsaved", c_int), ("steps", c_longlong),
                 ("accepted", c_longlong), ("rejected", c_longlong), ("nrhs", c_longlong),
-                ("z", c_double), ("dz", c_double)]
+                ("z", c_double), ("dz", c_double), ("nstats", c_longlong)]
 
 
 EXPORTS = [
@@ -77,7 +81,7 @@ EXPORTS = [
     "luna_b200_radial_plan_create", "luna_b200_radial_plan_destroy", "luna_b200_radial_rhs",
     "luna_b200_radial_rhs_device", "luna_b200_radial_solve", "luna_b200_qdht_device",
     "luna_b200_batch_timeline", "luna_b200_batch_set_priority",
-    "luna_b200_batch_info",
+    "luna_b200_batch_info", "luna_b200_batch_stats",
 ]
 
 _lib = None
@@ -112,6 +116,7 @@ def load():
     lib.luna_b200_batch_run.argtypes = [c_void_p, POINTER(c_float)]
     lib.luna_b200_batch_download.argtypes = [c_void_p, POINTER(PD), POINTER(PD), POINTER(SolveStats)]
     lib.luna_b200_batch_steplog.argtypes = [c_void_p, c_int, PD]
+    lib.luna_b200_batch_stats.argtypes = [c_void_p, c_int, PD]
     lib.luna_b200_batch_destroy.argtypes = [c_void_p]
     lib.luna_b200_batch_destroy.restype = None
     lib.luna_b200_rhs_device_noalloc.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p,

@@ -5,6 +5,9 @@
 #include <stdint.h>
 
 #define LUNA_MAX_RESP 4
+#ifndef LUNA_NSTATS
+#define LUNA_NSTATS 10
+#endif
 
 // response kinds (same values as the public header)
 #ifndef LUNA_RESP_KERR_FIELD
@@ -53,6 +56,10 @@ typedef struct {
     const double* towin;    // [No]
     const double* twin;     // [N] (stepfun)
     double in_scale;        // pad scale / No / (nlscale * sqrt(Aeff))
+    const double* omega;    // [Nw] grid.ω (per-step statistics; may be null)
+    const double* tgrid;    // [N] grid.t (per-step statistics)
+    double aeff;            // effective area (per-step statistics)
+    double escale;          // 1/sqrt(eps0*c*Aeff/2): mode-averaged field -> V/m
     int nresp;
     LunaResp resp[LUNA_MAX_RESP];
     // ---- integrator (RK45.solve_precon) ----
@@ -72,6 +79,9 @@ typedef struct {
     long long steplog_cap;
     const double* replay; // optional [2 * nreplay]: (dt, ok) of each step to follow
     long long nreplay;
+    double* stats;        // optional [LUNA_NSTATS * stats_cap]: Stats.default row per accepted step
+    long long stats_cap;
+    long long nstats;
     // ---- results ----
     int status;
     int nsaved;

@@ -558,6 +558,12 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
     UP(g->wwin, g->Nw, &I.wwin);
     UP(g->towin, g->No, &I.towin);
     UP(g->twin, g->N, &I.twin);
+    if (g->omega && g->t) {
+        UP(g->omega, g->Nw, &I.omega);
+        UP(g->t, g->N, &I.tgrid);
+    }
+    I.aeff = g->aeff;
+    I.escale = g->escale;
     I.nresp = nresp;
     int nplasma = 0, nraman = 0;
     for (int i = 0; i < nresp; ++i) {
@@ -756,6 +762,10 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         const size_t og = carve(gsb);
         const size_t osv = carve((size_t)opts->saveN * Nw * sizeof(double2));
         const size_t olog = carve((size_t)(opts->steplog_cap > 0 ? opts->steplog_cap : 0) * 4 * sizeof(double));
+        const size_t ost = carve((size_t)(opts->stats_cap > 0 ? opts->stats_cap : 0) * LUNA_NSTATS * sizeof(double));
+        if (opts->stats_cap > 0 && (I.kind != 0 || !I.omega || !I.tgrid || main_len(I) < I.N || I.Nw < 8 || !(I.aeff > 0)))
+            return bail(fail(LUNA_ERR_UNSUPPORTED, "batch_create: per-step statistics need a field-resolved grid with "
+                                                   "oversampled length >= 2N and the grid's ω, t and Aeff"));
         char* slab = nullptr;
         if (dalloc(b->allocs, &slab, off)) return bail(LUNA_ERR_CUDA);
         I.y0 = (const double2*)(slab + oy0);
@@ -776,6 +786,9 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         I.max_steps = opts->max_steps;
         I.steplog = opts->steplog_cap > 0 ? (double*)(slab + olog) : nullptr;
         I.steplog_cap = opts->steplog_cap;
+        I.stats = opts->stats_cap > 0 ? (double*)(slab + ost) : nullptr;
+        I.stats_cap = opts->stats_cap > 0 ? opts->stats_cap : 0;
+        I.nstats = 0;
         I.replay = nullptr;
         I.nreplay = 0;
         if (opts->replay && opts->nreplay > 0) {
@@ -982,6 +995,7 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
             s.nrhs = I.nrhs;
             s.z = I.z;
             s.dz = I.dz;
+            s.nstats = I.nstats;
         }
     }
     CK(cudaStreamSynchronize(b->stream));
@@ -1018,6 +1032,13 @@ int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm) {
         begin_end_s[2 * i + 1] = (double)(res[i].t_end - t0) * 1e-9;
         if (sm) sm[i] = res[i].sm;
     }
+    return LUNA_OK;
+}
+
+int luna_b200_batch_stats(luna_batch* b, int i, double* stats) {
+    if (!b || !stats || i < 0 || i >= b->n) return fail(LUNA_ERR_BAD_ARG, "batch_stats: bad argument");
+    if (!b->h[i].stats) return fail(LUNA_ERR_BAD_ARG, "batch_stats: statistics were not requested (stats_cap = 0)");
+    CK(cudaMemcpy(stats, b->h[i].stats, sizeof(double) * LUNA_NSTATS * b->h[i].stats_cap, cudaMemcpyDeviceToHost));
     return LUNA_OK;
 }
 

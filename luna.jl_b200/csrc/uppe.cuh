@@ -978,6 +978,178 @@ __device__ void interpolate_row(int Nw, const double2* linop, const Ctl& c, doub
     }
 }
 
+// ------------------------------------------------------------------ per-step statistics
+// Block reductions returning the result in every thread (fixed order). `sh` holds at
+// least 4 * LUNA_WARPS doubles; the calls end with a barrier, so `sh` can be reused.
+__device__ __forceinline__ void block_argmax(double& v, int& i, double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        if (v2 > v || (v2 == v && i2 < i)) {
+            v = v2;
+            i = i2;
+        }
+    }
+    __syncthreads();
+    if (lane == 0) {
+        sh[wid] = v;
+        sh[LUNA_WARPS + wid] = (double)i;
+    }
+    __syncthreads();
+    v = sh[0];
+    i = (int)sh[LUNA_WARPS];
+    for (int q = 1; q < LUNA_WARPS; ++q) {
+        const double v2 = sh[q];
+        const int i2 = (int)sh[LUNA_WARPS + q];
+        if (v2 > v || (v2 == v && i2 < i)) {
+            v = v2;
+            i = i2;
+        }
+    }
+    __syncthreads();
+}
+
+// four index reductions at once: a, b by max; c, d by min
+__device__ __forceinline__ void block_idx4(int& a, int& b, int& c, int& d, double* sh) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a = max(a, __shfl_xor_sync(0xffffffffu, a, o));
+        b = max(b, __shfl_xor_sync(0xffffffffu, b, o));
+        c = min(c, __shfl_xor_sync(0xffffffffu, c, o));
+        d = min(d, __shfl_xor_sync(0xffffffffu, d, o));
+    }
+    __syncthreads();
+    if (lane == 0) {
+        sh[wid] = a;
+        sh[LUNA_WARPS + wid] = b;
+        sh[2 * LUNA_WARPS + wid] = c;
+        sh[3 * LUNA_WARPS + wid] = d;
+    }
+    __syncthreads();
+    for (int q = 0; q < LUNA_WARPS; ++q) {
+        a = max(a, (int)sh[q]);
+        b = max(b, (int)sh[LUNA_WARPS + q]);
+        c = min(c, (int)sh[2 * LUNA_WARPS + q]);
+        d = min(d, (int)sh[3 * LUNA_WARPS + q]);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ double linterpx(double x1, double x2, double y1, double y2, double val) {
+    const double slope = (y2 - y1) / (x2 - x1);
+    const double icpt = y1 - slope * x1;
+    return (val - icpt) / slope;
+}
+
+// Stats.default for a mode-averaged field-resolved transform (Stats.jl:495-532) on the
+// accepted, window-filtered state Y at z with the next step dz, into row[LUNA_NSTATS]:
+// z, dz, spectral centroid ω0 (Stats.jl:18-24), energy_ω (Fields.jl:510-520; SimpsonEven
+// weights 17/48, 59/48, 43/48, 49/48 at both ends), peak power and peak intensity of the
+// analytic field (plan_analytic, Stats.jl:434-462: 2*E[k] for k < Nw-1, inverse transform
+// of length N), FWHM min/max with linear crossings (Maths.jl:128-190) and, with a plasma
+// response, electron density and peak ionisation rate (Stats.jl:228-257).
+template <typename Rl>
+__device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const double2* yn, double z, double dz,
+                                        double* row) {
+    const int tid = threadIdx.x, T = LUNA_BLOCK;
+    const int Nw = I.Nw, N = I.N;
+    const cpx<double>* Y = reinterpret_cast<const cpx<double>*>(yn);
+    int ip = -1;
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
+    double sw = 0, s1 = 0, ss = 0;
+    for (int k = tid; k < Nw; k += T) {
+        const double a = abs2(Y[k]);
+        s1 += a;
+        sw += I.omega[k] * a;
+        const int kk = min(k, Nw - 1 - k);
+        const double wt = (kk == 0) ? 17.0 / 48 : (kk == 1) ? 59.0 / 48 : (kk == 2) ? 43.0 / 48 : (kk == 3) ? 49.0 / 48 : 1.0;
+        ss += wt * a;
+    }
+    block_sum3(sw, s1, ss, w.red);
+    __syncthreads();
+    // analytic field
+    cpx<Rl>* buf = w.main;
+    for (int k = tid; k < N; k += T) buf[Swz<Rl>::f(k)] = (k < Nw - 1) ? cvt<Rl>(scale(2.0, Y[k])) : mk<Rl>(0, 0);
+    __syncthreads();
+    const cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, N, w.tw);
+    const int P = buf_split<Rl>(w.main_alt, N);
+    const double invN = 1.0 / (double)N;
+    auto Pt = [&](int n) -> double { return abs2(scale(invN, cvt<double>(x[Swz<Rl>::f(split_pos(n, N, P))]))); };
+    double vmax = -1.0;
+    int imax = 0;
+    double rs = 0, rmax = 0, redge = 0;
+    for (int n = tid; n < N; n += T) {
+        const cpx<double> e = scale(invN, cvt<double>(x[Swz<Rl>::f(split_pos(n, N, P))]));
+        const double pt = abs2(e);
+        if (pt > vmax) {
+            vmax = pt;
+            imax = n;
+        }
+        if (ip >= 0) {
+            const double E = e.x * I.escale;
+            const double r = (double)eval_rate<Rl>(I.resp[ip], (Rl)fabs(E), w.flag);
+            rs += r;
+            rmax = fmax(rmax, r);
+            if (n == 0 || n == N - 1) redge += r;
+        }
+    }
+    block_argmax(vmax, imax, w.tot);
+    {
+        double c = 0;
+        block_sum3(rs, redge, c, w.red);  // sum of the rates and r[0] + r[N-1]
+        int dummy = 0;
+        block_argmax(rmax, dummy, w.tot);
+    }
+    const double val = 0.5 * vmax;
+    int minL = -1, maxR = -1, minR = N, maxL = N;
+    for (int n = tid; n < N; n += T) {
+        const double pt = Pt(n);
+        if (n < imax && pt < val) minL = max(minL, n);
+        if (n > imax && pt > val) maxR = max(maxR, n);
+        if (n > imax && pt < val) minR = min(minR, n);
+        if (n < imax && pt > val) maxL = min(maxL, n);
+    }
+    block_idx4(minL, maxR, minR, maxL, w.red);
+    if (tid == 0) {
+        const double* t = I.tgrid;
+        double fmn = NAN, fmx = NAN;
+        if (minL >= 0 && minR < N) {
+            const double left = linterpx(t[minL], t[minL + 1], Pt(minL), Pt(minL + 1), val);
+            const double right = linterpx(t[minR - 1], t[minR], Pt(minR - 1), Pt(minR), val);
+            fmn = fabs(right - left);
+        }
+        if (maxL < N && maxR >= 0 && maxL >= 1 && maxR + 1 <= N - 1) {
+            const double left = linterpx(t[maxL - 1], t[maxL], Pt(maxL - 1), Pt(maxL), val);
+            const double right = linterpx(t[maxR], t[maxR + 1], Pt(maxR), Pt(maxR + 1), val);
+            fmx = fabs(right - left);
+        }
+        const double h = I.omega[1] - I.omega[0];
+        const double wl = I.omega[Nw - 1];
+        row[0] = z;
+        row[1] = dz;
+        row[2] = sw / s1;
+        row[3] = 2.0 * 3.141592653589793 / (wl * wl) * (h * ss);
+        row[4] = vmax;
+        row[5] = vmax / I.aeff;
+        row[6] = fmn;
+        row[7] = fmx;
+        if (ip >= 0) {
+            const double dtg = t[1] - t[0];
+            const double Tr = dtg * (rs - 0.5 * redge);  // trapezoid integral of the rate
+            row[8] = (1.0 - exp(-Tr)) * I.resp[ip].coef;
+            row[9] = rmax;
+        } else {
+            row[8] = NAN;
+            row[9] = NAN;
+        }
+    }
+    __syncthreads();
+}
+
 // Weak error norm, PI step control, step limits and step bookkeeping after the stage
 // evaluations (RK45.jl:167-192, 343-354, 374-406); one thread. sy, syn and se are the
 // sums of |y|^2, |yn|^2 and |yerr|^2; flags are the status bits raised by the RHS.
@@ -1178,6 +1350,11 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
             __syncthreads();
             // prop!_maybe + stepfun window filter on yn
             stepfun_filter<Rl>(I, w, pyn, I.e1);
+            // Stats.default of the filtered state (MemoryOutput calls it before the saves)
+            if (I.stats && I.nstats < I.stats_cap) {
+                step_stats<Rl>(I, w, pyn, c.tn, c.dtn, I.stats + (size_t)LUNA_NSTATS * I.nstats);
+                if (tid == 0) I.nstats += 1;
+            }
             // GridCondition saves (Output.jl:65-82, 490-502)
             while (saved < I.saveN && I.zsave[saved] <= c.tn) {
                 interpolate_row<Rl, Kt>(Nw, I.linop, c, I.zsave[saved], k, py, pyn, I.saves + (size_t)saved * Nw);

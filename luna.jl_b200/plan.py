@@ -121,6 +121,12 @@ class Plan:
         gd.outfac = _lib.dptr(outfac.view(np.float64))
         gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
         gd.in_scale = pad / No / (nlscale * math.sqrt(t.aeff))
+        # per-step statistics (Stats.default): grid axes, Aeff and the field scale
+        om, tt = _f64(g.ω), _f64(g.t)
+        keep += [om, tt]
+        gd.omega, gd.t = _lib.dptr(om), _lib.dptr(tt)
+        gd.aeff = t.aeff
+        gd.escale = 1.0 / math.sqrt(pd.eps_0 * pd.c * t.aeff / 2)
         rds = resp_descs(t.resp, t.density, keep)
         return cls(gd, rds, keep, precision, Nw)
 
@@ -135,9 +141,10 @@ class Plan:
 
 
 def make_opts(saveN, zsave, rtol=1e-6, atol=1e-10, safety=0.9, max_dt=math.inf, min_dt=0.0,
-              repeat_limit=10, max_steps=200000, steplog_cap=0, replay=None, flags=0):
+              repeat_limit=10, max_steps=200000, steplog_cap=0, replay=None, flags=0, stats_cap=0):
     o = _lib.SolveOpts()
     o.flags = flags
+    o.stats_cap = stats_cap
     if replay is not None:
         o.replay = _lib.dptr(replay)
         o.nreplay = len(replay) // 2
@@ -152,7 +159,7 @@ def make_opts(saveN, zsave, rtol=1e-6, atol=1e-10, safety=0.9, max_dt=math.inf, 
 
 
 class SolveResult:
-    def __init__(self, z, Eω, y, stats, steplog=None):
+    def __init__(self, z, Eω, y, stats, steplog=None, step_stats=None):
         self.z = z
         self.Eω = Eω
         self.y = y
@@ -165,6 +172,8 @@ class SolveResult:
         self.dzfinal = stats.dz
         self.nsaved = stats.nsaved
         self.steplog = steplog
+        # Stats.default rows of the accepted steps (columns _lib.STATS_KEYS), or None
+        self.stats = step_stats
 
 
 class Batch:
@@ -175,6 +184,7 @@ class Batch:
         self.zsave = _f64(zsave)
         self.saveN = saveN
         self.steplog_cap = opt.get("steplog_cap", 0)
+        self.stats_cap = opt.get("stats_cap", 0)
         if opt.get("replay") is not None:
             opt["replay"] = _f64(opt["replay"])
             self._replay = opt["replay"]
@@ -255,6 +265,12 @@ class Batch:
         _lib.check(_lib.load().luna_b200_batch_timeline(self._h, _lib.dptr(be), sm))
         return be, np.array(list(sm))
 
+    def stats(self, i):
+        """Per-step statistics of instance i: (stats_cap, NSTATS) array."""
+        out = np.zeros((self.stats_cap, _lib.NSTATS))
+        _lib.check(_lib.load().luna_b200_batch_stats(self._h, i, _lib.dptr(out)))
+        return out
+
     def steplog(self, i):
         out = np.zeros((self.steplog_cap, 4))
         _lib.check(_lib.load().luna_b200_batch_steplog(self._h, i, _lib.dptr(out)))
@@ -267,7 +283,8 @@ class Batch:
             log = None
             if self.steplog_cap:
                 log = self.steplog(i)[: min(st.steps, self.steplog_cap)]
-            res.append(SolveResult(self.zsave[: st.nsaved], s[: st.nsaved], y, st, log))
+            sts = self.stats(i)[: st.nstats] if self.stats_cap else None
+            res.append(SolveResult(self.zsave[: st.nsaved], s[: st.nsaved], y, st, log, sts))
         return res
 
 
@@ -280,7 +297,8 @@ _STATUS_MSG = {
 
 def solve_precon(transform, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, atol=1e-10,
                  safety=0.9, max_dt=math.inf, min_dt=0.0, repeat_limit=10, max_steps=200000,
-                 steplog_cap=0, precision=_lib.PREC_FP64, raise_on_status=True, replay=None):
+                 steplog_cap=0, precision=_lib.PREC_FP64, raise_on_status=True, replay=None,
+                 stats_cap=0):
     """RK45.solve_precon (RK45.jl:19-25) with Luna.run's window filter and saves, on the GPU.
 
     ``replay`` (optional, flat (dz, accepted) pairs) makes the integrator follow a given
@@ -290,7 +308,7 @@ def solve_precon(transform, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, ato
     zs = np.linspace(z0, zmax, saveN)
     b = Batch([plan], saveN, zs, rtol=rtol, atol=atol, safety=safety, max_dt=max_dt,
               min_dt=min_dt, repeat_limit=repeat_limit, max_steps=max_steps,
-              steplog_cap=steplog_cap, replay=replay)
+              steplog_cap=steplog_cap, replay=replay, stats_cap=stats_cap)
     b.upload([linop], [Eω], [z0], [dz0], [zmax])
     b.run()
     r = b.results()[0]

@@ -373,10 +373,92 @@ class PreconStepper:
         return self.prop(out, self.t, ti)
 
 
+# ------------------------------------------------------------------- per-step statistics
+
+STATS_KEYS = ("z", "dz", "ω0", "energy", "peakpower", "peakintensity", "fwhm_t_min",
+              "fwhm_t_max", "electrondensity", "peak_ionisation_rate")
+
+
+def _linterpx(x1, x2, y1, y2, val):
+    """Maths.linterpx (Maths.jl:230-236)."""
+    slope = (y2 - y1) / (x2 - x1)
+    icpt = y1 - slope * x1
+    return (val - icpt) / slope
+
+
+def fwhm_linear(x, y, minmax):
+    """Maths.fwhm / level_xings with method=:linear, baseline=false, level=0.5
+    (Maths.jl:128-190); NaN where a crossing is missing."""
+    val = 0.5 * np.max(y)
+    maxidx = int(np.argmax(y))
+    xmax = x[maxidx]
+    n = len(y)
+    try:
+        if minmax == "min":
+            li = np.nonzero((x < xmax) & (y < val))[0]
+            ri = np.nonzero((x > xmax) & (y < val))[0]
+            lefti, righti = int(li[-1]), int(ri[0])
+            left = _linterpx(x[lefti], x[lefti + 1], y[lefti], y[lefti + 1], val)
+            right = _linterpx(x[righti - 1], x[righti], y[righti - 1], y[righti], val)
+        else:
+            li = np.nonzero((x < xmax) & (y > val))[0]
+            ri = np.nonzero((x > xmax) & (y > val))[0]
+            lefti, righti = int(li[0]), int(ri[-1])
+            if lefti - 1 < 0 or righti + 1 > n - 1:
+                raise IndexError
+            left = _linterpx(x[lefti - 1], x[lefti], y[lefti - 1], y[lefti], val)
+            right = _linterpx(x[righti], x[righti + 1], y[righti], y[righti + 1], val)
+        return abs(right - left)
+    except IndexError:
+        return math.nan
+
+
+def _simpson_even(x, y):
+    """NumericalIntegration.jl integrate(x, y, SimpsonEven()) for uniform x."""
+    h = x[1] - x[0]
+    r = (17 * (y[0] + y[-1]) + 59 * (y[1] + y[-2]) + 43 * (y[2] + y[-3]) + 49 * (y[3] + y[-4])) / 48
+    return h * (r + np.sum(y[4:len(y) - 4]))
+
+
+def stats_default(t, Ew, z, dz):
+    """Stats.default for a mode-averaged field-resolved transform (Stats.jl:495-532): the
+    spectral centroid ω0 (:18-24), energy from energyfuncs' energy_ω (Fields.jl:510-520),
+    peak power and peak intensity of the analytic field (:86-100, :150-154, plan_analytic
+    :434-462), FWHM min/max (:182-200) and, with a plasma response, the electron density and
+    peak ionisation rate (:228-257)."""
+    g = t.grid
+    a2 = np.abs(Ew) ** 2
+    w = g.ω
+    out = {"z": z, "dz": dz}
+    out["ω0"] = np.sum(w * a2) / np.sum(a2)
+    out["energy"] = 2 * math.pi / (w[-1] ** 2) * _simpson_even(w, a2)
+    N = g.N
+    Ewa = np.zeros(N, dtype=np.complex128)
+    n = len(Ew) - 1
+    Ewa[:n] = 2 * Ew[:n]
+    Eta = np.fft.ifft(Ewa)
+    Pt = np.abs(Eta) ** 2
+    out["peakpower"] = np.max(Pt)
+    out["peakintensity"] = np.max(Pt) / t.aeff
+    out["fwhm_t_min"] = fwhm_linear(g.t, Pt, "min")
+    out["fwhm_t_max"] = fwhm_linear(g.t, Pt, "max")
+    out["electrondensity"] = math.nan
+    out["peak_ionisation_rate"] = math.nan
+    for r in t.resp:
+        if getattr(r, "kind", "") == "plasma":
+            Eto = np.real(Eta) / math.sqrt(EPS0 * 299792458.0 * t.aeff / 2)
+            rr = rate(r.ratefunc, Eto)
+            frac = cumtrapz(rr, g.t[1] - g.t[0])
+            out["electrondensity"] = (1 - math.exp(-frac[-1])) * t.density
+            out["peak_ionisation_rate"] = np.max(rr)
+    return out
+
+
 class RunResult:
     def __init__(self):
         self.z = []
         self.Eω = []
+        self.stats = []  # Stats.default rows (STATS_KEYS) of every accepted step
         self.steps = 0
         self.accepted = []  # (t, dt, err) of every accepted step
         self.steps_all = []  # (dt, ok) of every step, accepted or not
@@ -385,7 +467,7 @@ class RunResult:
 
 
 def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rtol=1e-6,
-        atol=1e-10, safety=0.9, saveN=201, repeat_limit=10, max_steps=None):
+        atol=1e-10, safety=0.9, saveN=201, repeat_limit=10, max_steps=None, stats=False):
     """Luna.run (Luna.jl:358-391) with a MemoryOutput on a GridCondition (Output.jl:65-82,
     490-502) and RK45.solve's loop (RK45.jl:27-89)."""
     max_dz = grid.zmax / 2 if max_dz is None else max_dz
@@ -411,6 +493,9 @@ def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rto
             Et = np.fft.ifft(y, axis=0) * tw
             y = np.fft.fft(Et, axis=0)
         s.yn = y
+        if stats:  # MemoryOutput calls statsfun before the saves (Output.jl:65-82)
+            d = stats_default(t, y, z, dz)
+            res.stats.append([d[k] for k in STATS_KEYS])
         while saved < saveN and zgrid[saved] <= z:
             res.z.append(zgrid[saved])
             res.Eω.append(s.interpolate(zgrid[saved]))
@@ -434,6 +519,7 @@ def run(t, grid, linop, Eω0, z0=0.0, init_dz=1e-4, max_dz=None, min_dz=0.0, rto
         if max_steps is not None and res.steps >= max_steps:
             break
     res.nrhs = s.nrhs
+    res.stats = np.array(res.stats)
     res.Eω = np.array(res.Eω)
     res.z = np.array(res.z)
     return res

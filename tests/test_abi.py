@@ -69,6 +69,8 @@ int main(void) {
     P(luna_resp_desc, hdt); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
     P(luna_solve_opts, replay); P(luna_solve_opts, nreplay); P(luna_solve_opts, flags);
     P(luna_radial_desc, Mf); P(luna_radial_desc, outfac);
+    P(luna_grid_desc, omega); P(luna_grid_desc, escale); P(luna_solve_opts, stats_cap);
+    P(luna_solve_stats, nstats);
     P(luna_solve_stats, z); P(luna_solve_stats, dz);
     return 0;
 }
@@ -95,6 +97,10 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_radial_desc"]) == ctypes.sizeof(_lib.RadialDesc)
     for f in ("replay", "nreplay", "flags"):
         assert int(out[f"luna_solve_opts.{f}"]) == getattr(_lib.SolveOpts, f).offset
+    assert int(out["luna_grid_desc.omega"]) == _lib.GridDesc.omega.offset
+    assert int(out["luna_grid_desc.escale"]) == _lib.GridDesc.escale.offset
+    assert int(out["luna_solve_opts.stats_cap"]) == _lib.SolveOpts.stats_cap.offset
+    assert int(out["luna_solve_stats.nstats"]) == _lib.SolveStats.nstats.offset
     for f in ("Mf", "outfac"):
         assert int(out[f"luna_radial_desc.{f}"]) == getattr(_lib.RadialDesc, f).offset
     assert int(out["luna_solve_stats.z"]) == _lib.SolveStats.z.offset

@@ -270,3 +270,28 @@ def test_raman_cluster_path_matches_single_cta_and_fp64():
     assert e_c < 1e-4 and e_s < 1e-4, (e_c, e_s)
     assert e_cs < 1e-5, e_cs
     assert not np.array_equal(rc.y, rs.y)  # the cluster path did run
+
+
+@pytest.mark.parametrize("gas", ["Ar", "He"])
+def test_step_stats_match_oracle(gas):
+    """Stats.default per accepted step (Stats.jl:495-532) computed on the device after the
+    window filter, against the oracle's restatement on the same step sequence (replay)."""
+    prob = prop_capillary_args(125e-6, 0.05, gas, 1.0, λ0=800e-9, τfwhm=10e-15, energy=120e-6,
+                               λlims=(150e-9, 4e-6), trange=0.25e-12, saveN=5)
+    ores = uppe.run(prob.transform, prob.grid, prob.linop, prob.Eω, saveN=5, init_dz=1e-3,
+                    stats=True)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    r = P.solve_precon(prob.transform, prob.linop, prob.Eω, 0.0, 1e-3, prob.grid.zmax, saveN=5,
+                       max_dt=prob.grid.zmax / 2, replay=replay, stats_cap=4096)
+    assert r.stats is not None and r.stats.shape == ores.stats.shape
+    for j, key in enumerate(_lib.STATS_KEYS):
+        a, b = r.stats[:, j], ores.stats[:, j]
+        assert np.array_equal(np.isnan(a), np.isnan(b)), key
+        ok = ~np.isnan(b)
+        if key == "electrondensity":
+            # 1 - exp(-x) is resolved to ~1e-16 near zero (in the reference as here)
+            rho = prob.transform.density
+            assert np.all(np.abs(a[ok] - b[ok]) <= 1e-9 * np.abs(b[ok]) + 1e-15 * rho), key
+            continue
+        err = np.max(np.abs(a[ok] - b[ok]) / np.maximum(np.abs(b[ok]), 1e-300))
+        assert err < 1e-9, (key, err)

@@ -249,3 +249,26 @@ def test_qdht_roundtrip_and_gaussian_pair():
     F = q.Mf @ np.exp(-q.r ** 2 / w ** 2)
     Fa = w ** 2 / 2 * np.exp(-q.k ** 2 * w ** 2 / 4)
     assert np.abs(F - Fa).max() / Fa.max() < 1e-12
+
+
+# ---------------------------------------------------------------- test_maths.jl:121-137
+def test_fwhm_linear_matches_reference_cases():
+    x = np.linspace(-1, 1, 2048)
+    g = lambda x, fw, x0=0.0: np.exp(-4 * math.log(2) * ((x - x0) / fw) ** 2)
+    assert isapprox(uppe.fwhm_linear(x, g(x, 0.2), "min"), 0.2, 1e-4)
+    fw, sep = 0.1, 0.5
+    y = g(x, fw, -sep / 2) + g(x, fw, sep / 2)
+    assert isapprox(uppe.fwhm_linear(x, y, "min"), fw, 1e-4)
+    assert isapprox(uppe.fwhm_linear(x, y, "max"), fw + sep, 1e-4)
+
+
+def test_stats_energy_of_input_pulse():
+    """Stats.default's energy (energyfuncs' energy_ω, Fields.jl:510-520) of the input field
+    equals the requested pulse energy, and the FWHM of the analytic power is the pulse's."""
+    from luna_b200.interface import prop_capillary_args
+    p = prop_capillary_args(125e-6, 0.3, "He", 1.0, λ0=800e-9, τfwhm=10e-15, energy=120e-6,
+                            λlims=(150e-9, 4e-6), trange=0.25e-12)
+    d = uppe.stats_default(p.transform, p.Eω, 0.0, 1e-4)
+    assert isapprox(d["energy"], 120e-6, 1e-6)
+    assert abs(d["fwhm_t_min"] - 10e-15) < 0.5e-15
+    assert d["ω0"] > 0 and d["peakpower"] > 0 and d["electrondensity"] >= 0

@@ -1,8 +1,8 @@
 // Block-wide FFT for one CTA of LUNA_BLOCK threads, in place in shared or global memory.
 //
 // A length-M transform is split as M = P * Mb with Mb <= EMAX * LUNA_BLOCK (EMAX = 8
-// complex values per thread for FP64, 16 for FP32, the most a thread can hold in
-// registers across a barrier without spilling). The P sub-transforms of length Mb are
+// complex values per thread; with 16 for FP32 the butterflies spill registers and the
+// solver steps are ~20 % slower on B200). The P sub-transforms of length Mb are
 // Stockham passes done in place: every thread loads its E = Mb/LUNA_BLOCK inputs,
 // synchronises, computes its radix-R butterflies and writes the outputs back.
 // One radix-P pass joins the sub-transforms:
@@ -94,7 +94,7 @@ __device__ __forceinline__ void dft_br(cpx<R>* v) {
 }
 
 template <typename R>
-struct FftEmax { static constexpr int v = (sizeof(R) == 8) ? 8 : 16; };
+struct FftEmax { static constexpr int v = 8; };
 
 // largest transform held by one CTA: P <= 8 sub-transforms of EMAX*LUNA_BLOCK
 template <typename R>

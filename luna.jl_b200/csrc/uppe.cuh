@@ -403,55 +403,16 @@ __device__ bool cluster_post_wait(Ws<Rl>& w, const cpx<Rl>* x, int M, int P, dou
 }
 
 // ------------------------------------------------------------------ plasma chunk
-// PlasmaScalar! (Nonlinear.jl:121-133) for the pair of samples (2m, 2m+1) held by this
-// thread. Each running trapezoid is written as dt*(prefix_sum(y)[n] - (y[0]+y[n])/2), so
-// the three cumulative integrals are plain block prefix sums (FP64) carried across
-// chunks; y[0] of each integrand is broadcast from the first chunk through `edge`.
+// Running integrals carried from one chunk of samples to the next.
 struct PlasmaCarry {
     double c1, c2, c3;
 };
 
-template <typename Rl>
-__device__ __forceinline__ void plasma_pair(const LunaResp& r, bool act, int m, double E0, double E1,
-                                            PlasmaCarry& cr, Ws<Rl>& w, double& P0, double& P1) {
-    const double dt = r.dt;
-    const double r0 = act ? (double)eval_rate<Rl>(r, (Rl)fabs(E0), w.flag) : 0.0;
-    const double r1 = act ? (double)eval_rate<Rl>(r, (Rl)fabs(E1), w.flag) : 0.0;
-    const bool first = (m == 0);
-    if (first) w.edge[0] = r0;
-    double tot;
-    double x = block_exscan(r0 + r1, w.tot, tot);
-    const double y0r = w.edge[0];
-    const double S0 = cr.c1 + x + r0, S1 = S0 + r1;
-    cr.c1 += tot;
-    // fraction = preionfrac + 1 - exp(-int rate)
-    const double f0 = dt * (S0 - 0.5 * (y0r + r0)), f1 = dt * (S1 - 0.5 * (y0r + r1));
-    const double fr0 = r.preion + 1.0 - ((f0 == 0.0) ? 1.0 : exp(-f0));
-    const double fr1 = r.preion + 1.0 - ((f1 == 0.0) ? 1.0 : exp(-f1));
-    const double er = r.eratio;  // e^2/m_e
-    const double ph0 = act ? fr0 * er * E0 : 0.0, ph1 = act ? fr1 * er * E1 : 0.0;
-    if (first) w.edge[1] = ph0;
-    x = block_exscan(ph0 + ph1, w.tot + LUNA_WARPS, tot);
-    const double y0p = w.edge[1];
-    const double T0 = cr.c2 + x + ph0, T1 = T0 + ph1;
-    cr.c2 += tot;
-    double J0 = dt * (T0 - 0.5 * (y0p + ph0)), J1 = dt * (T1 - 0.5 * (y0p + ph1));
-    // ionisation loss term where |E| > 0
-    if (act && fabs(E0) > 0) J0 += r.ionpot * r0 * (1.0 - fr0) / E0;
-    if (act && fabs(E1) > 0) J1 += r.ionpot * r1 * (1.0 - fr1) / E1;
-    if (!act) { J0 = 0; J1 = 0; }
-    if (first) w.edge[2] = J0;
-    x = block_exscan(J0 + J1, w.tot + 2 * LUNA_WARPS, tot);
-    const double y0J = w.edge[2];
-    const double U0 = cr.c3 + x + J0, U1 = U0 + J1;
-    cr.c3 += tot;
-    P0 += r.coef * (dt * (U0 - 0.5 * (y0J + J0)));
-    P1 += r.coef * (dt * (U1 - 0.5 * (y0J + J1)));
-}
-
-// PlasmaScalar! for the two consecutive pairs (samples 4t..4t+3 of a chunk) held by this
-// thread: as plasma_pair, with the thread's four samples summed in order before each
-// block scan (half the chunks, and two independent rate evaluations per thread).
+// PlasmaScalar! (Nonlinear.jl:121-133) for the two consecutive pairs (samples 4t..4t+3 of
+// a chunk of 4*LUNA_BLOCK samples) held by this thread. Each running trapezoid is written
+// as dt*(prefix_sum(y)[n] - (y[0]+y[n])/2), so the three cumulative integrals are block
+// prefix sums (FP64) of the thread's four samples summed in order, carried across chunks;
+// y[0] of each integrand is broadcast from the first chunk through `edge`.
 template <typename Rl>
 __device__ __forceinline__ void plasma_quad(const LunaResp& r, const bool act[2], int m0, const double E[4],
                                             PlasmaCarry& cr, Ws<Rl>& w, double Pq[4]) {
@@ -685,8 +646,6 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
                 cpx<Rl> p = act ? Pr[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] : mk<Rl>(0, 0);
                 P0 += r.coef * E0 * (double)p.x;
                 P1 += r.coef * E1 * (double)p.y;
-            } else if (i == ip) {
-                plasma_pair<Rl>(r, act, m, E0, E1, cr, w, P0, P1);
             }
         }
         if (act) {

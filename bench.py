@@ -393,6 +393,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--max-rk-steps", type=int, default=200000,
                     help="per-instance step budget (profiling aid; the scan needs < 30000)")
+    ap.add_argument("--no-clusters", action="store_true",
+                    help="integrate every instance on one CTA (profiling aid)")
     ap.add_argument("--workload", default="scan256", choices=["scan256", "radial"],
                     help="scan256: the batched capillary scan (headline); radial: TransRadial RHS")
     args = ap.parse_args()
@@ -422,7 +424,8 @@ def main():
     n = len(probs)
     plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
     # each instance saves on its own GridCondition range(0, zmax, 201) with max_dz = zmax/2
-    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps)
+    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps,
+                    flags=_lib.SOLVE_NO_CLUSTERS if args.no_clusters else 0)
     zsaves = [np.linspace(0.0, p.grid.zmax, SAVEN) for p in probs]
     max_dts = [p.grid.zmax / 2 for p in probs]
     # pinned host buffers for the end-to-end path

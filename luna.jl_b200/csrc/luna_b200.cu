@@ -128,12 +128,23 @@ __device__ void cluster_helper(LunaInst* insts, char* smem, int smem_bytes, cons
         const cpx<Rl>* xr = cg::this_cluster().map_shared_rank(
             reinterpret_cast<cpx<Rl>*>(__cvta_shared_to_generic(box->xaddr)), 0);
         // packed squares of the field (odd half: times e^{-2 pi i m/Mr}), split order
-        for (int m = tid; m < HM; m += T) {
-            const cpx<Rl> e = xr[Swz<Rl>::f(split_pos(m, M, P))];
-            const Rl e0 = e.x * sc, e1 = e.y * sc;
-            cpx<Rl> v = mk<Rl>(e0 * e0, e1 * e1);
-            if (par) v = v * twiddle<Rl, false>(tw, (unsigned)m << tsh);
-            buf[Swz<Rl>::f(split_pos(m, HM, Ph))] = v;
+        // (four remote loads in flight per thread)
+        for (int m0 = tid; m0 < HM; m0 += 4 * T) {
+            cpx<Rl> e[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int m = m0 + q * T;
+                e[q] = (m < HM) ? xr[Swz<Rl>::f(split_pos(m, M, P))] : mk<Rl>(0, 0);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int m = m0 + q * T;
+                if (m >= HM) continue;
+                const Rl e0 = e[q].x * sc, e1 = e[q].y * sc;
+                cpx<Rl> v = mk<Rl>(e0 * e0, e1 * e1);
+                if (par) v = v * twiddle<Rl, false>(tw, (unsigned)m << tsh);
+                buf[Swz<Rl>::f(split_pos(m, HM, Ph))] = v;
+            }
         }
         __syncthreads();
         cpx<Rl>* Z = block_fft<Rl, false>(buf, nullptr, HM, tw);

@@ -467,6 +467,13 @@ __device__ void plasma_only(const LunaInst& I, Ws<Rl>& w, const cpx<Rl>* xr, cpx
                             int ip) {
     const int T = LUNA_BLOCK, tid = threadIdx.x;
     PlasmaCarry cr = {0, 0, 0};
+    // the remote field of the next chunk is loaded while the current one is processed
+    cpx<Rl> nx[2];
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const int m = 2 * tid + q;
+        nx[q] = (m < M) ? xr[Swz<Rl>::f(split_pos(m, M, P))] : mk<Rl>(0, 0);
+    }
     for (int c0 = 0; c0 < M; c0 += 2 * T) {
         const int m0 = c0 + 2 * tid;
         const bool act[2] = {m0 < M, m0 + 1 < M};
@@ -475,9 +482,11 @@ __device__ void plasma_only(const LunaInst& I, Ws<Rl>& w, const cpx<Rl>* xr, cpx
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
             pos[q] = Swz<Rl>::f(split_pos(act[q] ? m0 + q : 0, M, P));
-            const cpx<Rl> e = act[q] ? xr[pos[q]] : mk<Rl>(0, 0);
+            const cpx<Rl> e = act[q] ? nx[q] : mk<Rl>(0, 0);
             E[2 * q] = (double)e.x * sc;
             E[2 * q + 1] = (double)e.y * sc;
+            const int mn = m0 + 2 * T + q;
+            nx[q] = (mn < M) ? xr[Swz<Rl>::f(split_pos(mn, M, P))] : mk<Rl>(0, 0);
         }
         double Pq[4] = {0, 0, 0, 0};
         plasma_quad<Rl>(I.resp[ip], act, m0, E, cr, w, Pq);
@@ -546,29 +555,45 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
         // (same positions as x); the responses are added here in tuple order
         const bool ok = cluster_post_wait<Rl>(w, x, M, P, sc, w.cl->inst);
         const int Ph = fft_nsplit<Rl>(M);
-        for (int m = tid; m < M; m += T) {
-            const int pos = Swz<Rl>::f(split_pos(m, M, P));
-            const cpx<Rl> e = x[pos];
-            const double E0 = (double)e.x * sc, E1 = (double)e.y * sc;
-            double P0 = 0, P1 = 0;
-            for (int i = 0; i < I.nresp; ++i) {
-                const LunaResp& r = I.resp[i];
-                if (r.kind == LUNA_RESP_KERR_FIELD) {
-                    P0 += r.coef * (E0 * E0 * E0);
-                    P1 += r.coef * (E1 * E1 * E1);
-                } else if (i == ir && ok) {
-                    const int ph = Swz<Rl>::f(split_pos(m, M, Ph));
-                    const cpx<Rl> pr = w.rem_e[ph] + w.rem_o[ph];
-                    P0 += r.coef * E0 * (double)pr.x;
-                    P1 += r.coef * E1 * (double)pr.y;
-                } else if (i == ip && ok) {
-                    const cpx<Rl> pl = w.rem_p[pos];
-                    P0 += (double)pl.x;
-                    P1 += (double)pl.y;
-                }
+        const bool use_r = ok && ir >= 0, use_p = ok && ip >= 0;
+        // four samples pairs per thread and round: every load of a round (own buffer,
+        // helpers' shared memory, time window) is issued before the arithmetic
+        constexpr int U = 4;
+        for (int m0 = tid; m0 < M; m0 += U * T) {
+            int pos[U];
+            cpx<Rl> e[U], pr[U], pl[U];
+            double2 tw[U];
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                const int m = m0 + q * T;
+                const bool a = m < M;
+                pos[q] = Swz<Rl>::f(split_pos(a ? m : 0, M, P));
+                const int ph = Swz<Rl>::f(split_pos(a ? m : 0, M, Ph));
+                e[q] = x[pos[q]];
+                pr[q] = use_r ? w.rem_e[ph] + w.rem_o[ph] : mk<Rl>(0, 0);
+                pl[q] = use_p ? w.rem_p[pos[q]] : mk<Rl>(0, 0);
+                tw[q] = __ldg(reinterpret_cast<const double2*>(I.towin) + (a ? m : 0));
             }
-            const double tw0 = __ldg(I.towin + 2 * m), tw1 = __ldg(I.towin + 2 * m + 1);
-            x[pos] = mk<Rl>((Rl)(P0 * tw0), (Rl)(P1 * tw1));
+#pragma unroll
+            for (int q = 0; q < U; ++q) {
+                if (m0 + q * T >= M) continue;
+                const double E0 = (double)e[q].x * sc, E1 = (double)e[q].y * sc;
+                double P0 = 0, P1 = 0;
+                for (int i = 0; i < I.nresp; ++i) {
+                    const LunaResp& r = I.resp[i];
+                    if (r.kind == LUNA_RESP_KERR_FIELD) {
+                        P0 += r.coef * (E0 * E0 * E0);
+                        P1 += r.coef * (E1 * E1 * E1);
+                    } else if (i == ir && use_r) {
+                        P0 += r.coef * E0 * (double)pr[q].x;
+                        P1 += r.coef * E1 * (double)pr[q].y;
+                    } else if (i == ip && use_p) {
+                        P0 += (double)pl[q].x;
+                        P1 += (double)pl[q].y;
+                    }
+                }
+                x[pos[q]] = mk<Rl>((Rl)(P0 * tw[q].x), (Rl)(P1 * tw[q].y));
+            }
         }
         __syncthreads();
         return;

@@ -66,7 +66,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         energy=None, power=None, pulseshape="gauss", shotnoise=False,
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16):
-    """Mode-averaged HE11 capillary set-up with constant pressure (Interface.jl:360-401)."""
+    """Mode-averaged HE11 capillary set-up (Interface.jl:360-401); ``pressure`` is a number
+    or a (p0, p1) gradient over the fibre (Capillary.gradient, Capillary.jl:306-315)."""
     if shotnoise:
         raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
     if envelope:
@@ -74,8 +75,19 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     plasma = (not envelope) if plasma is None else plasma
     thg = (not envelope) if thg is None else thg
     grid = RealGrid(flength, λ0, λlims, trange, δt)
-    mode = modes.MarcatiliMode(radius, gas, pressure, model=model, loss=loss)
-    density = pd.density(gas, pressure)
+    grad = None
+    if isinstance(pressure, (tuple, list)):
+        # simple gradient (p0, p1) over the fibre (Interface.jl:495-499, 524-526)
+        from .gradient import Gradient, MarcatiliGradientMode
+        if len(pressure) == 2 and all(np.ndim(x) == 0 for x in pressure):
+            grad = Gradient(gas, flength, *pressure)      # (p0, p1)
+        else:
+            grad = Gradient(gas, *pressure)               # (Z, P)
+        mode = MarcatiliGradientMode(radius, grad, model=model, loss=loss)
+        density = grad.density(0.0)
+    else:
+        mode = modes.MarcatiliMode(radius, gas, pressure, model=model, loss=loss)
+        density = pd.density(gas, pressure)
     resp = []
     if kerr:
         if not thg:
@@ -93,10 +105,19 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     if raman:
         rr = _raman.raman_response(grid.to, gas)
         resp.append(RamanPolarField(grid.to, rr))
-    linop, βconst, β1 = make_const_linop(grid, mode, λ0)
     aeff = mode.Aeff()
-    norm = norm_mode_average(grid, βconst)
-    transform = TransModeAvg(grid, resp, density, norm, aeff)
+    if grad is not None:
+        # z-dependent linear operator and normalisation (LinearOps.make_linop,
+        # LinearOps.jl:337-360; norm_mode_average with βfun!(β, z))
+        from .gradient import TransModeAvgZ, make_linop
+        if raman:
+            raise NotImplementedError("Raman responses with a pressure gradient are not supported")
+        linop, _ = make_linop(grid, mode, λ0)
+        transform = TransModeAvgZ(grid, resp, grad, mode, aeff, λ0)
+    else:
+        linop, βconst, β1 = make_const_linop(grid, mode, λ0)
+        norm = norm_mode_average(grid, βconst)
+        transform = TransModeAvg(grid, resp, density, norm, aeff)
     if pulseshape == "gauss":
         fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
     else:

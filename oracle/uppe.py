@@ -191,14 +191,19 @@ NLSCALE = math.sqrt(EPS0 * 299792458.0 / 2)
 
 
 def trans_mode_avg(t, Ew, z):
-    """(t::TransModeAvg)(nl, Eω, z) (NonlinearRHS.jl:362-373)."""
+    """(t::TransModeAvg)(nl, Eω, z) (NonlinearRHS.jl:362-373); with a pressure gradient the
+    density is densityfun(z) and the normalisation uses βfun!(β, z) (:375-387)."""
     g = t.grid
     Et = to_time(g, Ew)
     Et = Et / (NLSCALE * math.sqrt(t.aeff))
-    Pt = et_to_pt(Et, t.resp, t.density)
+    zdep = getattr(t, "kind", "") == "modeavg_z"
+    Pt = et_to_pt(Et, t.resp, t.densityfun(z) if zdep else t.density)
     Pt = Pt * g.towin
     nl = to_freq(g, Pt, len(Ew))
     s = g.sidx
+    if zdep:
+        nl[s] = nl[s] * t.norm_factor(z)[s]
+        return nl
     nl[s] = nl[s] * (t.norm.pre[s] * math.sqrt(t.aeff))
     nl[s] = nl[s] * g.ωwin[s]
     return nl
@@ -282,8 +287,14 @@ class PreconStepper:
         self.ks[0] = self.fbar(y0, self.t, self.t)
 
     def prop(self, y, t1, t2, bwd=False):
-        """make_prop! for a constant linop (RK45.jl:271-281)."""
+        """make_prop! (RK45.jl:271-297): a constant linop, or linop(z) evaluated at the later
+        point t2 (re-evaluated only when t2 changes)."""
         d = (t1 - t2) if bwd else (t2 - t1)
+        if callable(self.linop):
+            if getattr(self, "_lastt2", None) != t2:
+                self._lin = self.linop(t2)
+                self._lastt2 = t2
+            return y * np.exp(self._lin * d)
         return y * np.exp(self.linop * d)
 
     def fbar(self, ybar, t1, t2):

@@ -59,6 +59,18 @@ class RadialDesc(ctypes.Structure):
     _fields_ = [("Nr", c_int), ("Mi", PD), ("Mf", PD), ("outfac", PD)]
 
 
+GRAD_MAXPTS = 16
+
+
+class GradientDesc(ctypes.Structure):
+    _fields_ = [("npts", c_int), ("two_point", c_int),
+                ("Z", c_double * GRAD_MAXPTS), ("P", c_double * GRAD_MAXPTS),
+                ("P2", c_double * GRAD_MAXPTS), ("dens_a", c_double), ("dens_b", c_double),
+                ("loss", c_int), ("gam", PD), ("nwg", PD), ("wc", PD), ("om", PD),
+                ("imcap", PD), ("ofs", PD), ("fd_xc", c_double * 4), ("fd_gam", c_double * 4),
+                ("fd_nwg", c_double * 8), ("fd_h12", c_double)]
+
+
 class SolveOpts(ctypes.Structure):
     _fields_ = [("rtol", c_double), ("atol", c_double), ("safety", c_double),
                 ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
@@ -81,7 +93,8 @@ EXPORTS = [
     "luna_b200_radial_plan_create", "luna_b200_radial_plan_destroy", "luna_b200_radial_rhs",
     "luna_b200_radial_rhs_device", "luna_b200_radial_solve", "luna_b200_qdht_device",
     "luna_b200_batch_timeline", "luna_b200_batch_set_priority",
-    "luna_b200_batch_info", "luna_b200_batch_stats",
+    "luna_b200_batch_info", "luna_b200_batch_stats", "luna_b200_plan_set_gradient",
+    "luna_b200_plan_linop",
 ]
 
 _lib = None
@@ -103,6 +116,8 @@ def load():
     lib = ctypes.CDLL(LIB_PATH)
     lib.luna_b200_plan_create.argtypes = [POINTER(GridDesc), POINTER(RespDesc), c_int, c_int,
                                           POINTER(c_void_p)]
+    lib.luna_b200_plan_set_gradient.argtypes = [c_void_p, POINTER(GradientDesc)]
+    lib.luna_b200_plan_linop.argtypes = [c_void_p, c_double, PD, PD]
     lib.luna_b200_plan_destroy.argtypes = [c_void_p]
     lib.luna_b200_plan_destroy.restype = None
     lib.luna_b200_rhs.argtypes = [c_void_p, PD, PD, c_double]

@@ -293,18 +293,26 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
 // One right-hand-side evaluation nl = T(Eω) on one CTA (TransModeAvg call).
 template <typename Rl>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
-rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int smem_bytes, int* status) {
+rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int smem_bytes, int* status, double z) {
     extern __shared__ __align__(256) char smem[];
     LunaInst& I = *inst;
     Ws<Rl> w;
     plan_ws<Rl>(I, smem, smem_bytes, w, tw);
     if (threadIdx.x == 0) *w.flag = 0;
     __syncthreads();
+    if (I.grad) grad_fill<Rl>(I, w, z, false);  // ρ(z) and the normalisation at z
     const cpx<double>* E = reinterpret_cast<const cpx<double>*>(Ew);
     cpx<double>* o = reinterpret_cast<cpx<double>*>(nl);
     rhs<Rl>(I, w, [&](int k) { return E[k]; }, [&](int k, cpx<double> v) { o[k] = v; });
     __syncthreads();
     if (threadIdx.x == 0) *status = (*w.flag & (1 << ST_FIELD_ABOVE_EMAX)) ? ST_FIELD_ABOVE_EMAX : ST_OK;
+}
+
+// linop!(out, z) of a pressure-gradient plan and the output factor at z, on one CTA.
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+grad_linop_kernel(LunaInst I, double z, double2* L, double2* of) {
+    __shared__ double bc[2];
+    grad_fill_to(I, bc, z, true, L, of);
 }
 
 // Raman response spectrum at plan creation (Raman.jl:256-262, Nonlinear.jl:306-307):
@@ -441,7 +449,11 @@ struct luna_plan {
     int precision = 0;
     LunaInst proto{};
     std::vector<void*> allocs;
+    bool has_raman = false;
+    LunaGrad* d_grad = nullptr;  // pressure gradient (device copy), or null
     // single-call RHS resources
+    bool inst_stale = false;     // d_inst predates a change of proto
+    double2* d_outz = nullptr;   // output factor at z (pressure gradient)
     LunaInst* d_inst = nullptr;
     void* d_gscr = nullptr;
     double2* d_Ew = nullptr;
@@ -626,6 +638,7 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
                 break;
             }
             case LUNA_RESP_RAMAN: {
+                p->has_raman = true;
                 if (++nraman > 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_UNSUPPORTED, "at most one Raman response"); }
                 if (d.ncomp < 1 || !d.hpre || !d.tau2 || !d.hwin || !d.htt) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Raman response tables missing"); }
                 r.ncomp = d.ncomp;
@@ -677,41 +690,117 @@ void luna_b200_plan_destroy(luna_plan* p) {
     delete p;
 }
 
-static int launch_rhs(luna_plan* p, const double2* Ew, double2* nl, cudaStream_t st) {
+static int launch_rhs(luna_plan* p, const double2* Ew, double2* nl, cudaStream_t st, double z) {
     TwDev tw;
     int rc = get_tw(tw);
     if (rc) return rc;
-    if (!p->d_inst) {
+    if (!p->d_inst || p->inst_stale) {
         LunaInst I = p->proto;
-        size_t gb = (p->precision == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
-        if (dalloc(p->allocs, &p->d_gscr, gb)) return LUNA_ERR_CUDA;
+        if (!p->d_gscr) {
+            size_t gb = (p->precision == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
+            if (dalloc(p->allocs, &p->d_gscr, gb)) return LUNA_ERR_CUDA;
+        }
         I.gscr = p->d_gscr;
-        if (dalloc(p->allocs, &p->d_inst, sizeof(LunaInst))) return LUNA_ERR_CUDA;
+        if (I.grad) {
+            if (!p->d_outz && dalloc(p->allocs, &p->d_outz, sizeof(double2) * I.Nw)) return LUNA_ERR_CUDA;
+            I.outz = p->d_outz;
+        }
+        if (!p->d_inst && dalloc(p->allocs, &p->d_inst, sizeof(LunaInst))) return LUNA_ERR_CUDA;
         CK(cudaMemcpy(p->d_inst, &I, sizeof(LunaInst), cudaMemcpyHostToDevice));
-        if (dalloc(p->allocs, &p->d_status, sizeof(int))) return LUNA_ERR_CUDA;
+        if (!p->d_status && dalloc(p->allocs, &p->d_status, sizeof(int))) return LUNA_ERR_CUDA;
+        p->inst_stale = false;
     }
     const int maxs = max_smem_optin();
     if (p->precision == LUNA_PREC_FP64) {
         int sm = (int)std::min<size_t>(smem_wanted<double>(p->proto), (size_t)maxs);
         CK(cudaFuncSetAttribute(rhs_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        rhs_kernel<double><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.d, sm, p->d_status);
+        rhs_kernel<double><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.d, sm, p->d_status, z);
     } else {
         int sm = (int)std::min<size_t>(smem_wanted<float>(p->proto), (size_t)maxs);
         CK(cudaFuncSetAttribute(rhs_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
-        rhs_kernel<float><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.f, sm, p->d_status);
+        rhs_kernel<float><<<1, LUNA_BLOCK, sm, st>>>(p->d_inst, Ew, nl, tw.f, sm, p->d_status, z);
     }
     CK(cudaGetLastError());
     return LUNA_OK;
 }
 
+int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
+    if (!p) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: null plan");
+    if (!g) {
+        p->proto.grad = nullptr;
+        p->inst_stale = true;
+        return LUNA_OK;
+    }
+    if (p->proto.kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "plan_set_gradient: field-resolved grids only");
+    if (p->has_raman)
+        return fail(LUNA_ERR_UNSUPPORTED, "plan_set_gradient: Raman responses depend on the density through "
+                                          "their dephasing times; not available with a pressure gradient");
+    if (g->npts < 2 || g->npts > LUNA_GRAD_MAXPTS) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: npts out of range");
+    if (g->two_point && g->npts != 2) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: a two-point fill has npts == 2");
+    for (int i = 0; i + 1 < g->npts; ++i)
+        if (!(g->Z[i + 1] > g->Z[i])) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: Z must increase");
+    if (g->two_point && g->Z[0] != 0.0) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: a two-point fill starts at z = 0");
+    for (int i = 0; i < g->npts; ++i)
+        if (!(g->P[i] >= 0) || g->P2[i] != g->P[i] * g->P[i])
+            return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: pressures must be >= 0 with P2 = P*P");
+    if (!g->gam || !g->nwg || !g->wc || !g->om || !g->imcap || !g->ofs || !(g->fd_h12 > 0))
+        return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: null table");
+    const size_t Nw = (size_t)p->proto.Nw;
+    LunaGrad h;
+    memset(&h, 0, sizeof(h));
+    h.npts = g->npts;
+    h.two_point = g->two_point;
+    h.loss = g->loss;
+    for (int i = 0; i < g->npts; ++i) {
+        h.Z[i] = g->Z[i];
+        h.P[i] = g->P[i];
+        h.P2[i] = g->P2[i];
+    }
+    h.dens_a = g->dens_a;
+    h.dens_b = g->dens_b;
+    for (int j = 0; j < 4; ++j) {
+        h.fd_xc[j] = g->fd_xc[j];
+        h.fd_gam[j] = g->fd_gam[j];
+        h.fd_nwg[j] = make_double2(g->fd_nwg[2 * j], g->fd_nwg[2 * j + 1]);
+    }
+    h.fd_h12 = g->fd_h12;
+    const double* t;
+    if (upload(p->allocs, g->gam, Nw, &h.gam) || upload(p->allocs, g->nwg, 2 * Nw, &t)) return LUNA_ERR_CUDA;
+    h.nwg = (const double2*)t;
+    if (upload(p->allocs, g->wc, Nw, &h.wc) || upload(p->allocs, g->om, Nw, &h.om) ||
+        upload(p->allocs, g->imcap, Nw, &h.imcap) || upload(p->allocs, g->ofs, 2 * Nw, &t))
+        return LUNA_ERR_CUDA;
+    h.ofs = (const double2*)t;
+    const LunaGrad* d = nullptr;
+    if (upload(p->allocs, &h, 1, &d)) return LUNA_ERR_CUDA;
+    p->d_grad = const_cast<LunaGrad*>(d);
+    p->proto.grad = p->d_grad;
+    p->inst_stale = true;
+    return LUNA_OK;
+}
+
+int luna_b200_plan_linop(luna_plan* p, double z, double* linop, double* outfac) {
+    if (!p || !linop) return fail(LUNA_ERR_BAD_ARG, "plan_linop: null argument");
+    if (!p->proto.grad) return fail(LUNA_ERR_BAD_ARG, "plan_linop: the plan has no pressure gradient");
+    const size_t bytes = sizeof(double2) * p->proto.Nw;
+    double2 *dL = nullptr, *dO = nullptr;
+    CK(cudaMalloc(&dL, 2 * bytes));
+    dO = dL + p->proto.Nw;
+    grad_linop_kernel<<<1, LUNA_BLOCK>>>(p->proto, z, dL, dO);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(linop, dL, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && outfac) e = cudaMemcpy(outfac, dO, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dL);
+    if (e != cudaSuccess) return fail(LUNA_ERR_CUDA, std::string("plan_linop: ") + cudaGetErrorString(e));
+    return LUNA_OK;
+}
+
 int luna_b200_rhs_device(luna_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
-    (void)z;  // constant density and effective area: the transform does not depend on z
     if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "rhs_device: null argument");
-    return launch_rhs(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+    return launch_rhs(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream, z);
 }
 
 int luna_b200_rhs(luna_plan* p, double* nl, const double* Ew, double z) {
-    (void)z;
     if (!p || !nl || !Ew) return fail(LUNA_ERR_BAD_ARG, "rhs: null argument");
     const size_t bytes = sizeof(double2) * p->proto.Nw;
     if (!p->d_Ew) {
@@ -719,7 +808,7 @@ int luna_b200_rhs(luna_plan* p, double* nl, const double* Ew, double z) {
         CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     }
     CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
-    int rc = launch_rhs(p, p->d_Ew, p->d_nl, p->stream);
+    int rc = launch_rhs(p, p->d_Ew, p->d_nl, p->stream, z);
     if (rc) return rc;
     int st = 0;
     CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
@@ -770,6 +859,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         size_t ok[7];
         for (int j = 0; j < 7; ++j) ok[j] = carve(Nw * kel);
         const size_t oe1 = carve(Nw * sizeof(double2));
+        const size_t olz = carve(I.grad ? Nw * sizeof(double2) : 0), ooz = carve(I.grad ? Nw * sizeof(double2) : 0);
         const size_t og = carve(gsb);
         const size_t osv = carve((size_t)opts->saveN * Nw * sizeof(double2));
         const size_t olog = carve((size_t)(opts->steplog_cap > 0 ? opts->steplog_cap : 0) * 4 * sizeof(double));
@@ -784,6 +874,10 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         I.yn = (double2*)(slab + oyn);
         for (int j = 0; j < 7; ++j) I.k[j] = slab + ok[j];
         I.e1 = (double2*)(slab + oe1);
+        if (I.grad) {
+            I.linz = (double2*)(slab + olz);
+            I.outz = (double2*)(slab + ooz);
+        }
         I.gscr = slab + og;
         I.saves = (double2*)(slab + osv);
         I.zsave = b->d_zsave;
@@ -912,12 +1006,16 @@ int luna_b200_batch_upload(luna_batch* b, const double* const* linops, const dou
             I.zsave = b->zsave_own[i];
         }
         if (max_dt) I.max_dt = max_dt[i];
-        if (!I.linop) {
-            double2* L = nullptr;
-            if (dalloc(b->allocs, &L, bytes)) return LUNA_ERR_CUDA;
-            I.linop = L;
+        // with a pressure gradient L(z) is evaluated on the device and linops[i] is ignored
+        if (!I.grad) {
+            if (!linops[i]) return fail(LUNA_ERR_BAD_ARG, "batch_upload: null linop for a plan without a pressure gradient");
+            if (!I.linop) {
+                double2* L = nullptr;
+                if (dalloc(b->allocs, &L, bytes)) return LUNA_ERR_CUDA;
+                I.linop = L;
+            }
+            CK(cudaMemcpyAsync((void*)I.linop, linops[i], bytes, cudaMemcpyHostToDevice, b->stream));
         }
-        CK(cudaMemcpyAsync((void*)I.linop, linops[i], bytes, cudaMemcpyHostToDevice, b->stream));
         I.y = b->ybuf[i];
         I.yn = b->ynbuf[i];
         CK(cudaMemcpyAsync((void*)I.y0, y0[i], bytes, cudaMemcpyHostToDevice, b->stream));
@@ -1073,7 +1171,7 @@ void luna_b200_batch_destroy(luna_batch* b) {
 
 int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z0, double dz0, double zmax,
                     const luna_solve_opts* opts, double* saves, double* steplog, luna_solve_stats* stats) {
-    if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "solve: null argument");
+    if (!p || (!linop && !p->proto.grad) || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "solve: null argument");
     luna_batch* b = nullptr;
     int rc = luna_b200_batch_create(&p, 1, opts, &b);
     if (rc) return rc;
@@ -1527,6 +1625,9 @@ extern "C" int luna_b200_rhs_device_noalloc(luna_plan* p, double* nl_dev, const 
                                             void* stream, int* status_dev) {
     (void)z;  // constant density and effective area: the transform does not depend on z
     if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "rhs_device_noalloc: null argument");
+    if (p->proto.grad)
+        return fail(LUNA_ERR_UNSUPPORTED, "rhs_device_noalloc: plans with a pressure gradient need a per-plan "
+                                          "buffer for the z-dependent normalisation; use luna_b200_rhs_device");
     LunaInst I = p->proto;
     const size_t need = (p->precision == LUNA_PREC_FP64) ? gscr_bytes<double>(I) : gscr_bytes<float>(I);
     if (need > (size_t)LUNA_NOALLOC_SCRATCH_BYTES)

@@ -712,7 +712,11 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
     cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P);
     pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
     const cpx<double>* of = reinterpret_cast<const cpx<double>*>(I.outfac);
-    r2c_to_freq<Rl>(w, x, M, I.Nw, [&](int k, cpx<double> X) { store(k, X * ldg(of + k)); });
+    // with a pressure gradient the factor of the current z is in outz, written by this
+    // kernel (plain loads, not the read-only path)
+    const cpx<double>* oz = reinterpret_cast<const cpx<double>*>(I.outz);
+    const bool zdep = I.grad != nullptr;
+    r2c_to_freq<Rl>(w, x, M, I.Nw, [&](int k, cpx<double> X) { store(k, X * (zdep ? oz[k] : ldg(of + k))); });
 }
 
 // envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
@@ -1028,6 +1032,107 @@ __device__ __forceinline__ double linterpx(double x1, double x2, double y1, doub
     return (val - icpt) / slope;
 }
 
+// ------------------------------------------------------------------ pressure gradients
+// Capillary.gradient (Capillary.jl:306-337) and LinearOps.make_linop (LinearOps.jl:337-360)
+// evaluated at z. Every operation is an explicitly rounded IEEE operation (no contraction
+// into fused multiply-adds) in the order of the host restatement: the group delay β1(z) is a
+// finite difference with h = 1e-4 ω0, which turns one ulp of an effective index into ~1e-12
+// of β1 and a visible time shift of the pulse, so host and device evaluate identical
+// sequences.
+__device__ __forceinline__ double grad_pressure(const LunaGrad* g, double z) {
+    if (g->two_point) {
+        if (z > g->Z[1]) return g->P[1];
+        if (z <= 0) return g->P[0];
+        return __dsqrt_rn(__dadd_rn(g->P2[0], __dmul_rn(__ddiv_rn(z, g->Z[1]), __dsub_rn(g->P2[1], g->P2[0]))));
+    }
+    const int n = g->npts;
+    if (z <= g->Z[0]) return g->P[0];
+    if (z >= g->Z[n - 1]) return g->P[n - 1];
+    int i = 0;
+    while (i + 1 < n - 1 && g->Z[i + 1] < z) ++i;  // last i with Z[i] < z
+    const double f = __ddiv_rn(__dsub_rn(z, g->Z[i]), __dsub_rn(g->Z[i + 1], g->Z[i]));
+    return __dsqrt_rn(__dadd_rn(g->P2[i], __dmul_rn(f, __dsub_rn(g->P2[i + 1], g->P2[i]))));
+}
+
+__device__ __forceinline__ double grad_density(const LunaGrad* g, double z) {
+    const double p = grad_pressure(g, z);
+    return __ddiv_rn(__dmul_rn(g->dens_a, p), __dadd_rn(1.0, __dmul_rn(g->dens_b, p)));
+}
+
+// sqrt(coren^2 - nwg), coren = sqrt(1 + γ ρ): principal root from r = |w|,
+// t = sqrt((r + |a|)/2); a >= 0: t + i b/(2t), else |b|/(2t) + i copysign(t, b)
+__device__ __forceinline__ double2 grad_neff(double gam, double2 nwg, double rho, int loss) {
+    const double cr = __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(gam, rho)));
+    const double a = __dsub_rn(__dmul_rn(cr, cr), nwg.x);
+    const double b = -nwg.y;
+    const double r = __dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+    double re, im;
+    if (a >= 0) {
+        const double t = __dsqrt_rn(__dmul_rn(__dadd_rn(r, a), 0.5));
+        re = t;
+        im = (t != 0) ? __ddiv_rn(b, __dmul_rn(2.0, t)) : 0.0;
+    } else {
+        const double t = __dsqrt_rn(__dmul_rn(__dsub_rn(r, a), 0.5));
+        re = fabs(__ddiv_rn(b, __dmul_rn(2.0, t)));
+        im = copysign(t, b);
+    }
+    return make_double2(re, loss ? im : 0.0);
+}
+
+// β1(z): 4-point central difference of x/c Re neff(x) (low-index rule) at ω0
+__device__ __forceinline__ double grad_beta1(const LunaGrad* g, double rho) {
+    double f[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const double re = grad_neff(g->fd_gam[j], g->fd_nwg[j], rho, g->loss).x;
+        f[j] = __dmul_rn(g->fd_xc[j], (re < 1e-3) ? 1e-3 : re);
+    }
+    const double num = __dadd_rn(__dsub_rn(__dadd_rn(-f[0], __dmul_rn(8.0, f[1])), __dmul_rn(8.0, f[2])), f[3]);
+    return __ddiv_rn(num, g->fd_h12);
+}
+
+// The gradient at z for the whole CTA: L(ω; z) into Lout (when wantL) and the output
+// factor ρ(z) ofs/β(z) (ρ(z) ofs off sidx) into oout. One thread evaluates ρ and β1 and
+// passes them through bc (2 doubles of shared memory).
+__device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double z, bool wantL, double2* Lout,
+                                          double2* oout) {
+    const LunaGrad* g = I.grad;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double rho = grad_density(g, z);
+        bc[0] = rho;
+        bc[1] = wantL ? grad_beta1(g, rho) : 0.0;
+    }
+    __syncthreads();
+    const double rho = bc[0], b1 = bc[1];
+    cpx<double>* Lz = reinterpret_cast<cpx<double>*>(Lout);
+    cpx<double>* oz = reinterpret_cast<cpx<double>*>(oout);
+    for (int i = threadIdx.x; i < I.Nw; i += LUNA_BLOCK) {
+        const double wc = __ldg(g->wc + i);
+        const double2 o = __ldg(g->ofs + i);
+        if (wc == 0) {
+            if (wantL) Lz[i] = mk<double>(0, 0);
+            oz[i] = mk<double>(rho * o.x, rho * o.y);
+            continue;
+        }
+        const double2 n = grad_neff(__ldg(g->gam + i), __ldg(g->nwg + i), rho, g->loss);
+        if (wantL) {
+            const double re = fmax(n.x, 1e-3);                       // conj_clamp
+            const double im = fmin(fmax(n.y, 0.0), __ldg(g->imcap + i));
+            const double X = __dsub_rn(__dmul_rn(wc, re), __dmul_rn(__ldg(g->om + i), b1));
+            Lz[i] = mk<double>(-__dmul_rn(wc, im), -X);
+        }
+        const double f = rho / __dmul_rn(wc, n.x);  // ρ / β(z)
+        oz[i] = mk<double>(f * o.x, f * o.y);
+    }
+    __syncthreads();
+}
+
+template <typename Rl>
+__device__ __forceinline__ void grad_fill(const LunaInst& I, Ws<Rl>& w, double z, bool wantL) {
+    grad_fill_to(I, w.red, z, wantL, I.linz, I.outz);
+}
+
 // Stats.default for a mode-averaged field-resolved transform (Stats.jl:495-532) on the
 // accepted, window-filtered state Y at z with the next step dz, into row[LUNA_NSTATS]:
 // z, dz, spectral centroid ω0 (Stats.jl:18-24), energy_ω (Fields.jl:510-520; SimpsonEven
@@ -1124,7 +1229,8 @@ __device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const doub
         if (ip >= 0) {
             const double dtg = t[1] - t[0];
             const double Tr = dtg * (rs - 0.5 * redge);  // trapezoid integral of the rate
-            row[8] = (1.0 - exp(-Tr)) * I.resp[ip].coef;
+            const double rho = I.grad ? grad_density(I.grad, z) : 1.0;  // coef is 1 then
+            row[8] = (1.0 - exp(-Tr)) * I.resp[ip].coef * rho;
             row[9] = rmax;
         } else {
             row[8] = NAN;
@@ -1203,7 +1309,8 @@ template <typename Rl, typename Kt>
 __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
     const int tid = threadIdx.x, T = LUNA_BLOCK;
     const int Nw = I.Nw;
-    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
+    // constant linop, or L(z) of the current stage node (pressure gradient)
+    const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.grad ? I.linz : I.linop);
     void** k = c.k;
     if (tid == 0)
         for (int j = 0; j < 7; ++j) k[j] = I.k[j];
@@ -1234,6 +1341,7 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
     }
     __syncthreads();
     // k1 = fbar(y0, t, t): propagation by exp(L*0) == 1
+    if (I.grad) grad_fill<Rl>(I, w, I.z0, false);
     {
         const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
         void* k0 = k[0];
@@ -1261,9 +1369,12 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
         const double t0 = c.t, dt = c.dt;
         const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
         for (int s = 0; s < 6; ++s) {
-            const double d = (t0 + c_nodes[s] * dt) - t0;
+            // stage node t + c_s dt and the propagation distance to it, rounded as written
+            const double zs = __dadd_rn(t0, __dmul_rn(c_nodes[s], dt));
+            const double d = __dsub_rn(zs, t0);
             const bool reuse = (s == 5);  // nodes 5 and 6 coincide
             if (!reuse) {
+                if (I.grad) grad_fill<Rl>(I, w, zs, true);
                 for (int i = tid; i < Nw; i += T) {
                     cpx<Rl> f = expLd<Rl>(L[i], d);
                     w.efac[i] = f;
@@ -1341,7 +1452,10 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
             }
             // GridCondition saves (Output.jl:65-82, 490-502)
             while (saved < I.saveN && I.zsave[saved] <= c.tn) {
-                interpolate_row<Rl, Kt>(Nw, I.linop, c, I.zsave[saved], k, py, pyn, I.saves + (size_t)saved * Nw);
+                // make_prop! evaluates a z-dependent linop at the save point itself
+                if (I.grad) grad_fill<Rl>(I, w, I.zsave[saved], true);
+                interpolate_row<Rl, Kt>(Nw, I.grad ? I.linz : I.linop, c, I.zsave[saved], k, py, pyn,
+                                        I.saves + (size_t)saved * Nw);
                 ++saved;
             }
             swap_y = true;

@@ -39,6 +39,7 @@ class Gradient:
             self.P = np.asarray(p0_or_P, dtype=np.float64).copy()
             if len(self.Z) != len(self.P) or len(self.Z) < 2 or np.any(np.diff(self.Z) <= 0):
                 raise ValueError("Z must be increasing and match P in length")
+        self.P2 = self.P * self.P
         self.L = float(self.Z[-1])
         self.p0, self.p1 = float(self.P[0]), float(self.P[-1])
         self.gam = pd.sellmeier_gas(gas)
@@ -47,19 +48,19 @@ class Gradient:
         self.dens_b = pd._B2.get(gas, 0.0) * pd.bar / (pd._R_GAS * T)
 
     def p(self, z):
-        Z, P = self.Z, self.P
+        Z, P, P2 = self.Z, self.P, self.P2
         if self.two_point:
             if z > Z[1]:
-                return P[1]
+                return float(P[1])
             if z <= 0:
-                return P[0]
-            return math.sqrt(P[0] ** 2 + z / Z[1] * (P[1] ** 2 - P[0] ** 2))
+                return float(P[0])
+            return math.sqrt(P2[0] + z / Z[1] * (P2[1] - P2[0]))
         if z <= Z[0]:
-            return P[0]
+            return float(P[0])
         if z >= Z[-1]:
-            return P[-1]
+            return float(P[-1])
         i = int(np.searchsorted(Z, z, side="left")) - 1  # last i with Z[i] < z
-        return math.sqrt(P[i] ** 2 + (z - Z[i]) / (Z[i + 1] - Z[i]) * (P[i + 1] ** 2 - P[i] ** 2))
+        return math.sqrt(P2[i] + (z - Z[i]) / (Z[i + 1] - Z[i]) * (P2[i + 1] - P2[i]))
 
     def density(self, z):
         p = self.p(z)
@@ -70,7 +71,7 @@ class Gradient:
         return np.asarray(self.gam(pd.wlfreq(np.asarray(ω, dtype=np.float64)) * 1e6), dtype=np.float64)
 
     def coren(self, ω, z):
-        return np.sqrt(1 + (self.gamma(ω) * self.density(z)).astype(complex))
+        return np.sqrt(1 + self.gamma(ω) * self.density(z))
 
 
 class MarcatiliGradientMode(modes.MarcatiliMode):
@@ -88,11 +89,19 @@ class MarcatiliGradientMode(modes.MarcatiliMode):
         k = ω / pd.c
         return (self.unm / (k * self.a)) ** 2 * (1 - 1j * vn / (k * self.a)) ** 2
 
+    def neff_parts(self, gam, nwg, rho):
+        """(Re, Im) of sqrt(coren^2 - nwg) with coren = sqrt(1 + gam rho), in the operation
+        order the device uses (Capillary.jl:216-224)."""
+        cr = np.sqrt(1 + gam * rho)
+        re, im = modes.csqrt_rn(cr * cr - np.real(nwg), -np.imag(nwg))
+        if not self.loss:
+            im = np.zeros_like(im)
+        return re, im
+
     def neff_grid(self, ω, z):
         """neff(mode, coren^2, nwg) (Capillary.jl:216-224): no clamp."""
-        εco = self.grad.coren(ω, z) ** 2
-        n = np.sqrt(εco - self.nwg(ω))
-        return n if self.loss else np.real(n) + 0j
+        re, im = self.neff_parts(self.grad.gamma(ω), self.nwg(ω), self.grad.density(z))
+        return re + 1j * im
 
     def neff_z(self, ω, z):
         """neff(m, ω; z) of the full model with its low-index rule (Capillary.jl:162-173)."""
@@ -101,11 +110,21 @@ class MarcatiliGradientMode(modes.MarcatiliMode):
         im = np.where(np.real(n) < 1e-3, np.clip(np.imag(n), 0, None), np.imag(n))
         return re + 1j * im
 
-    def dispersion_z(self, ω0, z):
-        """β1(z) = dβ/dω at ω0: the 4-point central difference of MarcatiliMode.dispersion."""
+    def fd_tables(self, ω0):
+        """The z-independent inputs of the group-delay finite difference at ω0 + 2h, ω0 + h,
+        ω0 - h, ω0 - 2h (h = 1e-4 ω0): x/c, gam(x), nwg(x), and 12h."""
         h = ω0 * 1e-4
-        f = lambda x: float(x / pd.c * np.real(self.neff_z(np.array([x]), z))[0])
-        return (-f(ω0 + 2 * h) + 8 * f(ω0 + h) - 8 * f(ω0 - h) + f(ω0 - 2 * h)) / (12 * h)
+        x = np.array([ω0 + 2 * h, ω0 + h, ω0 - h, ω0 - 2 * h])
+        return x / pd.c, self.grad.gamma(x), self.nwg(x), 12 * h
+
+    def dispersion_z(self, ω0, z):
+        """β1(z) = dβ/dω at ω0: the 4-point central difference of MarcatiliMode.dispersion,
+        with β = x/c Re(neff) and the low-index rule."""
+        xc, gam, nwg, h12 = self.fd_tables(ω0)
+        re, _ = self.neff_parts(gam, nwg, self.grad.density(z))
+        re = np.where(re < 1e-3, 1e-3, re)
+        f = xc * re
+        return float((-f[0] + 8 * f[1] - 8 * f[2] + f[3]) / h12)
 
 
 def conj_clamp(n, ω):
@@ -114,21 +133,31 @@ def conj_clamp(n, ω):
 
 
 def make_linop(grid, mode, λ0):
-    """(linop(z), βfun(z)) for a field-resolved grid (LinearOps.jl:337-360)."""
+    """(linop(z), βfun(z)) for a field-resolved grid (LinearOps.jl:337-360):
+    L = -i(ω/c conj_clamp(neff) - ω β1(z)) on sidx, written out in real arithmetic
+    (Re L = -ω/c Im nc, Im L = -(ω/c Re nc - ω β1)), as the device evaluates it."""
     ω0 = pd.wlfreq(λ0)
     s = grid.sidx
-    ω = grid.ω
+    ω = grid.ω[s]
+    wc = ω / pd.c
+    cap = 3000 * pd.c / ω
+    gam = mode.grad.gamma(ω)
+    nwg = mode.nwg(ω)
 
     def linop(z):
-        out = np.zeros(len(ω), dtype=np.complex128)
+        out = np.zeros(len(grid.ω), dtype=np.complex128)
         β1 = mode.dispersion_z(ω0, z)
-        nc = conj_clamp(mode.neff_grid(ω[s], z), ω[s])
-        out[s] = -1j * (ω[s] / pd.c * nc - ω[s] * β1)
+        re, im = mode.neff_parts(gam, nwg, mode.grad.density(z))
+        re = np.maximum(re, 1e-3)                   # conj_clamp (LinearOps.jl:254)
+        im = np.minimum(np.maximum(im, 0.0), cap)
+        out.real[s] = -(wc * im)
+        out.imag[s] = -(wc * re - ω * β1)
         return out
 
     def βfun(z):
-        out = np.ones(len(ω))
-        out[s] = ω[s] / pd.c * np.real(mode.neff_grid(ω[s], z))
+        out = np.ones(len(grid.ω))
+        re, _ = mode.neff_parts(gam, nwg, mode.grad.density(z))
+        out[s] = wc * re
         return out
 
     return linop, βfun
@@ -161,3 +190,41 @@ class TransModeAvgZ(TransModeAvg):
 
     def output_factor(self):
         raise TypeError("the normalisation of a pressure gradient depends on z")
+
+
+def gradient_desc(t, crop, keep):
+    """luna_gradient_desc of a TransModeAvgZ for the C ABI (luna_b200_plan_set_gradient);
+    ``crop`` is the plan's crop scale, ``keep`` collects the host arrays it points to."""
+    from . import _lib
+    g, grid, mode, grad = t, t.grid, t.mode, t.grad
+    n = len(grad.Z)
+    if n > _lib.GRAD_MAXPTS:
+        raise ValueError(f"at most {_lib.GRAD_MAXPTS} pressure nodes")
+    s = np.zeros(len(grid.ω), dtype=bool)
+    s[grid.sidx] = True
+    ω = grid.ω
+    gam = np.zeros(len(ω))
+    nwg = np.zeros(len(ω), dtype=np.complex128)
+    wc = np.zeros(len(ω))
+    cap = np.zeros(len(ω))
+    gam[s] = grad.gamma(ω[s])
+    nwg[s] = mode.nwg(ω[s])
+    wc[s] = ω[s] / pd.c
+    cap[s] = 3000 * pd.c / ω[s]
+    ofs = np.full(len(ω), crop, dtype=np.complex128)
+    ofs[s] = crop * (t.pre[s] * math.sqrt(t.aeff) * grid.ωwin[s])
+    om = np.ascontiguousarray(ω, dtype=np.float64)
+    arrs = [np.ascontiguousarray(a) for a in (gam, nwg, wc, om, cap, ofs)]
+    keep += arrs
+    d = _lib.GradientDesc()
+    d.npts, d.two_point, d.loss = n, int(grad.two_point), int(bool(mode.loss))
+    for i in range(n):
+        d.Z[i], d.P[i], d.P2[i] = grad.Z[i], grad.P[i], grad.P2[i]
+    d.dens_a, d.dens_b = grad.dens_a, grad.dens_b
+    d.gam, d.nwg, d.wc, d.om, d.imcap, d.ofs = [_lib.dptr(a.view(np.float64)) for a in arrs]
+    xc, fg, fn, h12 = mode.fd_tables(pd.wlfreq(g.λ0))
+    for j in range(4):
+        d.fd_xc[j], d.fd_gam[j] = xc[j], fg[j]
+        d.fd_nwg[2 * j], d.fd_nwg[2 * j + 1] = fn[j].real, fn[j].imag
+    d.fd_h12 = h12
+    return d

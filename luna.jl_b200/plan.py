@@ -113,7 +113,9 @@ class Plan:
             pad = No / Nw
             crop = Nw / No
             kind = 1
-        outfac = _c128(crop * t.output_factor())
+        zdep = getattr(t, "kind", "") == "modeavg_z"
+        # a pressure gradient scales the output by ρ(z) pre/β(z) on the device
+        outfac = _c128(np.full(Nw, crop, dtype=np.complex128) if zdep else crop * t.output_factor())
         wwin, towin, twin = _f64(g.ωwin), _f64(g.towin), _f64(g.twin)
         keep += [outfac, wwin, towin, twin]
         gd = _lib.GridDesc()
@@ -127,8 +129,14 @@ class Plan:
         gd.omega, gd.t = _lib.dptr(om), _lib.dptr(tt)
         gd.aeff = t.aeff
         gd.escale = 1.0 / math.sqrt(pd.eps_0 * pd.c * t.aeff / 2)
-        rds = resp_descs(t.resp, t.density, keep)
-        return cls(gd, rds, keep, precision, Nw)
+        rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep)
+        plan = cls(gd, rds, keep, precision, Nw)
+        if zdep:
+            from .gradient import gradient_desc
+            gdesc = gradient_desc(t, crop, plan._keep)
+            plan._gdesc = gdesc
+            _lib.check(_lib.load().luna_b200_plan_set_gradient(plan.handle, _lib.ctypes.byref(gdesc)))
+        return plan
 
     def rhs(self, nl, Eω, z=0.0):
         """nl[:] = T(Eω) on the GPU (host arrays of complex128)."""
@@ -208,9 +216,10 @@ class Batch:
         """Copy the inputs of every instance to the device. ``zsaves`` (per-instance save
         points) and ``max_dts`` (per-instance step limits) are optional."""
         n = len(self.plans)
-        self._L = [_c128(L) for L in linops]
+        # a z-dependent linop (pressure gradient) is evaluated on the device: pass NULL
+        self._L = [None if (L is None or callable(L)) else _c128(L) for L in linops]
         self._Y = [_c128(y) for y in y0s]
-        Lp = (_lib.PD * n)(*[_lib.dptr(L.view(np.float64)) for L in self._L])
+        Lp = (_lib.PD * n)(*[_lib.dptr(None if L is None else L.view(np.float64)) for L in self._L])
         Yp = (_lib.PD * n)(*[_lib.dptr(y.view(np.float64)) for y in self._Y])
         z0 = _f64(z0s)
         dz0 = _f64(dz0s)

@@ -460,7 +460,8 @@ def stats_default(t, Ew, z, dz):
             Eto = np.real(Eta) / math.sqrt(EPS0 * 299792458.0 * t.aeff / 2)
             rr = rate(r.ratefunc, Eto)
             frac = cumtrapz(rr, g.t[1] - g.t[0])
-            out["electrondensity"] = (1 - math.exp(-frac[-1])) * t.density
+            rho = t.densityfun(z) if getattr(t, "kind", "") == "modeavg_z" else t.density
+            out["electrondensity"] = (1 - math.exp(-frac[-1])) * rho
             out["peak_ionisation_rate"] = np.max(rr)
     return out
 

@@ -72,6 +72,10 @@ int main(void) {
     P(luna_grid_desc, omega); P(luna_grid_desc, escale); P(luna_solve_opts, stats_cap);
     P(luna_solve_stats, nstats);
     P(luna_solve_stats, z); P(luna_solve_stats, dz);
+    printf("luna_gradient_desc %zu\n", sizeof(luna_gradient_desc));
+    P(luna_gradient_desc, Z); P(luna_gradient_desc, P2); P(luna_gradient_desc, dens_b);
+    P(luna_gradient_desc, loss); P(luna_gradient_desc, gam); P(luna_gradient_desc, ofs);
+    P(luna_gradient_desc, fd_xc); P(luna_gradient_desc, fd_nwg); P(luna_gradient_desc, fd_h12);
     return 0;
 }
 """
@@ -105,3 +109,6 @@ def test_struct_layout_matches_ctypes(tmp_path):
         assert int(out[f"luna_radial_desc.{f}"]) == getattr(_lib.RadialDesc, f).offset
     assert int(out["luna_solve_stats.z"]) == _lib.SolveStats.z.offset
     assert int(out["luna_solve_stats.dz"]) == _lib.SolveStats.dz.offset
+    assert int(out["luna_gradient_desc"]) == ctypes.sizeof(_lib.GradientDesc)
+    for f in ("Z", "P2", "dens_b", "loss", "gam", "ofs", "fd_xc", "fd_nwg", "fd_h12"):
+        assert int(out[f"luna_gradient_desc.{f}"]) == getattr(_lib.GradientDesc, f).offset

@@ -113,3 +113,161 @@ def test_gradient_rejects_raman():
     with pytest.raises(NotImplementedError):
         prop_capillary_args(125e-6, 1.0, "H2", (2.0, 0.2), λ0=800e-9, τfwhm=10e-15,
                             energy=50e-6, λlims=(400e-9, 2000e-9), trange=0.5e-12)
+
+
+# ------------------------------------------------------------------ GPU
+_CASES = {
+    "Ar-falling": dict(radius=125e-6, flength=0.3, gas="Ar", pressure=(2.0, 0.2), λ0=800e-9,
+                       τfwhm=10e-15, energy=150e-6, λlims=(150e-9, 4e-6), trange=0.25e-12),
+    "He-rising": dict(radius=75e-6, flength=0.2, gas="He", pressure=(0.2, 3.0), λ0=800e-9,
+                      τfwhm=10e-15, energy=120e-6, λlims=(120e-9, 4e-6), trange=0.25e-12),
+    "Ne-multipoint": dict(radius=100e-6, flength=0.3, gas="Ne",
+                          pressure=([0, 0.1, 0.2, 0.3], [0.5, 3.0, 3.0, 0.5]), λ0=800e-9,
+                          τfwhm=10e-15, energy=150e-6, λlims=(150e-9, 4e-6), trange=0.25e-12),
+}
+
+
+def _case(name, saveN=11, **kw):
+    c = dict(_CASES[name])
+    c.update(kw)
+    return prop_capillary_args(c.pop("radius"), c.pop("flength"), c.pop("gas"), c.pop("pressure"),
+                               saveN=saveN, **c)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(_CASES))
+def test_device_linop_is_bit_identical_to_host(name):
+    """linop!(out, z) on the device (luna_b200_plan_linop) equals the host restatement bit for
+    bit at every z, including both ends and outside the fibre; the output factor agrees with
+    ρ(z) x crop x norm_factor(z) to rounding."""
+    from luna_b200 import _lib
+    p = _case(name)
+    t = p.transform
+    plan = t.plan()
+    g = p.grid
+    crop = (len(g.ω) - 1) / (len(g.ωo) - 1)
+    L = np.zeros(len(g.ω), dtype=np.complex128)
+    of = np.zeros_like(L)
+    for z in [-0.01, 0.0, 1e-9, 0.05, 0.1, 0.1 + 1e-12, 0.1234567, 0.2, 0.29999, g.zmax, g.zmax + 0.1]:
+        _lib.check(_lib.load().luna_b200_plan_linop(plan.handle, z, _lib.dptr(L.view(np.float64)),
+                                                   _lib.dptr(of.view(np.float64))))
+        ref = p.linop(z)
+        assert np.array_equal(L, ref), (z, _rel(L, ref))
+        oref = crop * t.densityfun(z) * t.norm_factor(z)
+        assert _rel(of, oref) < 1e-14, (z, _rel(of, oref))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint"])
+def test_gradient_rhs_matches_oracle(name):
+    """(t::TransModeAvg)(nl, Eω, z) with densityfun(z) and βfun!(β, z) through the C ABI."""
+    p = _case(name)
+    rng = np.random.default_rng(7)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    for z in (0.0, 0.07, 0.15, 0.3):
+        nl = np.zeros_like(Ew)
+        p.transform(nl, Ew, z)
+        ref = uppe.trans_mode_avg(p.transform, Ew, z)
+        assert _rel(nl, ref) < 1e-12, (z, _rel(nl, ref))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(_CASES))
+def test_gradient_solve_fp64_same_steps_as_oracle(name):
+    """Luna.run with a pressure gradient: the z-dependent linop is evaluated at every stage
+    node, step end and save point (make_prop!, RK45.jl:284-297); the device takes the
+    oracle's accepted steps and every saved field is within 1e-10."""
+    from luna_b200 import plan as P
+    p = _case(name)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
+    r = P.run(p, steplog_cap=5000)
+    assert r.status == 0 and r.nsaved == 11
+    assert r.steps == ores.steps
+    acc = r.steplog[r.steplog[:, 3] == 1]
+    oacc = np.array(ores.accepted)
+    np.testing.assert_allclose(acc[:, 1], oacc[:, 1], rtol=1e-6)
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+
+
+@pytest.mark.gpu
+def test_equal_pressure_gradient_on_device_matches_constant():
+    """test_gradient.jl "field" on the device: a gradient at equal pressures integrates like
+    the constant fill (same steps; fields equal to rounding)."""
+    from luna_b200 import plan as P
+    c = _field_case(5.0)
+    rc = P.run(c)
+    for pr in ((5.0, 5.0), ([0, 5e-2], [5.0, 5.0])):
+        p = _field_case(pr)
+        r = P.run(p)
+        assert r.steps == rc.steps
+        for a, b in zip(r.Eω, rc.Eω):
+            assert _rel(a, b) < 1e-12, _rel(a, b)
+
+
+@pytest.mark.gpu
+def test_gradient_solve_mixed_spectral_error():
+    from luna_b200 import _lib
+    from luna_b200 import plan as P
+    p = _case("Ar-falling")
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
+    r = P.run(p, precision=_lib.PREC_MIXED)
+    assert r.status == 0 and r.nsaved == 11
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-3, _rel(a, b)
+
+
+@pytest.mark.gpu
+def test_gradient_step_stats_use_local_density():
+    """Stats.default with a gradient on the oracle's step sequence (replay): electrondensity is
+    the ionisation fraction x densityfun(z) (Stats.jl:228-257); the other keys as for a
+    constant fill."""
+    from luna_b200 import _lib
+    from luna_b200 import plan as P
+    p = _case("Ar-falling", saveN=5)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5, stats=True)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    r = P.solve_precon(p.transform, p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=5,
+                       max_dt=p.grid.zmax / 2, replay=replay, stats_cap=4096)
+    assert r.stats is not None and r.stats.shape == ores.stats.shape
+    rho0 = p.transform.densityfun(0.0)
+    for j, key in enumerate(_lib.STATS_KEYS):
+        a, b = r.stats[:, j], ores.stats[:, j]
+        assert np.array_equal(np.isnan(a), np.isnan(b)), key
+        ok = ~np.isnan(b)
+        if key == "electrondensity":
+            assert np.all(np.abs(a[ok] - b[ok]) <= 1e-9 * np.abs(b[ok]) + 1e-15 * rho0), key
+            continue
+        err = np.max(np.abs(a[ok] - b[ok]) / np.maximum(np.abs(b[ok]), 1e-300))
+        assert err < 1e-9, (key, err)
+
+
+@pytest.mark.gpu
+def test_gradient_rejections():
+    """A Raman plan takes no gradient (its dephasing times depend on the density); the
+    allocation-free entry point rejects gradient plans; a plan without a gradient has no
+    device linop(z)."""
+    from luna_b200 import _lib
+    from luna_b200.gradient import gradient_desc
+    from luna_b200.plan import Plan
+    lib = _lib.load()
+    p = _case("Ar-falling")
+    t = p.transform
+    g = t.grid
+    crop = (len(g.ω) - 1) / (len(g.ωo) - 1)
+    keep = []
+    d = gradient_desc(t, crop, keep)
+    h2 = prop_capillary_args(125e-6, 0.3, "H2", 1.0, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
+                             λlims=(150e-9, 4e-6), trange=0.25e-12)
+    rplan = Plan.from_transform(h2.transform)
+    assert lib.luna_b200_plan_set_gradient(rplan.handle, _lib.ctypes.byref(d)) == _lib.LUNA_ERR_UNSUPPORTED
+    L = np.zeros(len(h2.grid.ω), dtype=np.complex128)
+    assert lib.luna_b200_plan_linop(rplan.handle, 0.0, _lib.dptr(L.view(np.float64)),
+                                    _lib.dptr(None)) == _lib.LUNA_ERR_BAD_ARG
+    torch = pytest.importorskip("torch")
+    gp = t.plan()
+    dE = torch.zeros(2 * len(g.ω), dtype=torch.float64, device="cuda")
+    out = torch.zeros_like(dE)
+    rc = lib.luna_b200_rhs_device_noalloc(gp.handle, _lib.ctypes.c_void_p(out.data_ptr()),
+                                          _lib.ctypes.c_void_p(dE.data_ptr()), 0.0, None, None)
+    assert rc == _lib.LUNA_ERR_UNSUPPORTED

@@ -140,21 +140,26 @@ int luna_b200_rhs(luna_plan* plan, double* nl, const double* Ew, double z);
 /* Same with device pointers, enqueued on `stream` (a cudaStream_t, may be NULL). */
 int luna_b200_rhs_device(luna_plan* plan, double* nl_dev, const double* Ew_dev, double z, void* stream);
 
-/* ---------------------------------------------------------------- pressure gradients
+/* ---------------------------------------------------------------- pressure gradients, tapers
  * A gas fill whose pressure varies along the fibre, Capillary.gradient(gas, L, p0, p1) or
- * Capillary.gradient(gas, Z, P) (Capillary.jl:306-337), in a MarcatiliMode(a, coren) of the
- * full model. Attached to a plan it makes the transform z-dependent, as TransModeAvg is with
- * a density function and βfun!(β, z) (NonlinearRHS.jl:362-387): the response coefficients
- * are given for ρ = 1 and the polarisation is scaled by ρ(z); the normalisation on sidx is
- * pre/β(z). The solvers then evaluate the linear operator of LinearOps.make_linop
- * (LinearOps.jl:337-360) at every stage node, save point and step end (make_prop! for a
- * z-dependent linop, RK45.jl:284-297):
+ * Capillary.gradient(gas, Z, P) (Capillary.jl:306-337), and/or a core radius a(z)
+ * (MarcatiliMode(afun, ...), Interface.jl:249-250), in a MarcatiliMode of the full model.
+ * Attached to a plan it makes the transform z-dependent, as TransModeAvg is with a density
+ * function, aeff(z) and βfun!(β, z) (NonlinearRHS.jl:362-387): the response coefficients
+ * are given for ρ = 1 and the polarisation is scaled by ρ(z); the field scale is
+ * in_base/sqrt(Aeff(z)) and the normalisation on sidx pre sqrt(Aeff(z))/β(z). The solvers
+ * evaluate the linear operator of LinearOps.make_linop (LinearOps.jl:330-360) at every
+ * stage node, save point and step end (make_prop! for a z-dependent linop, RK45.jl:284-297):
  *   p(z) = sqrt(P[i]^2 + (z - Z[i])/(Z[i+1] - Z[i]) (P[i+1]^2 - P[i]^2)) on segment i,
  *   ρ(z) = dens_a p / (1 + dens_b p),  coren = sqrt(1 + γ(ω) ρ),
- *   neff = sqrt(coren^2 - nwg(ω)) (principal root in IEEE-rounded real operations),
+ *   a(z) = A[i] + (z - ZA[i])/(ZA[i+1] - ZA[i]) (A[i+1] - A[i]) (A[0] / A[end] outside),
+ *   nwg = (unm/(k a))^2 (1 - i vn/(k a))^2,  neff = sqrt(coren^2 - nwg) (principal root),
  *   β1(z) = (-f(ω0+2h) + 8 f(ω0+h) - 8 f(ω0-h) + f(ω0-2h)) / (12 h), f(x) = x/c Re neff(x)
  *           with Re neff raised to 1e-3 where it is below (Capillary.jl:162-173),
- *   L(ω; z) = -i (ω/c conj_clamp(neff) - ω β1(z)) on sidx, 0 elsewhere (LinearOps.jl:254).
+ *   L(ω; z) = -i (ω/c conj_clamp(neff) - ω β1(z)) on sidx, 0 elsewhere (LinearOps.jl:254),
+ *   β(ω; z) = ω/c Re neff (with the 1e-3 rule when the radius has more than one node),
+ *   Aeff(z) = a(z)^2 aeff_intg (Capillary.jl:295),
+ * each in IEEE-rounded real operations in the order written (no fused multiply-adds).
  * The linop argument of the solve entry points is ignored for such a plan (may be NULL).
  * Field-resolved grids only; plans with a Raman response are rejected (its dephasing
  * times depend on the density). */
@@ -165,29 +170,36 @@ typedef struct {
                                     z > L; 0: (Z, P) form: P[0] for z <= Z[0], P[end] for
                                     z >= Z[end]                                              */
     double Z[LUNA_GRAD_MAXPTS];  /* node positions, increasing (two-point: 0, L)            */
-    double P[LUNA_GRAD_MAXPTS];  /* node pressures [bar]                                    */
+    double P[LUNA_GRAD_MAXPTS];  /* node pressures [bar]; equal values: constant pressure   */
     double P2[LUNA_GRAD_MAXPTS]; /* P[i]*P[i]                                               */
     double dens_a, dens_b;       /* ρ(p) = dens_a p / (1 + dens_b p) [m^-3], p in bar        */
     int loss;                    /* 0: real effective index (MarcatiliMode loss=false)      */
+    int nta;                     /* radius nodes, 1 (constant radius)..LUNA_GRAD_MAXPTS     */
+    double ZA[LUNA_GRAD_MAXPTS]; /* radius node positions, increasing                       */
+    double A[LUNA_GRAD_MAXPTS];  /* core radius at the nodes [m]                            */
+    double unm;                  /* mode's Bessel zero                                      */
+    double aeff_intg;            /* Aeff / a^2                                              */
+    double in_base;              /* pad scale / No / nlscale                                */
+    double eps0c2;               /* ε0 c / 2 (field scale of the statistics)                */
     const double* gam;           /* [Nw] γ(ω): Sellmeier susceptibility per unit density    */
-    const double* nwg;           /* [2*Nw] (unm/(k a))^2 (1 - i vn/(k a))^2 (Capillary.jl:188-200) */
+    const double* vn;            /* [2*Nw] cladding term get_vn(εcl(ω)) (Capillary.jl:88-93) */
     const double* wc;            /* [Nw] ω/c on sidx, 0 elsewhere                           */
     const double* om;            /* [Nw] ω                                                  */
     const double* imcap;         /* [Nw] 3000 c/ω: conj_clamp's bound on Im neff            */
-    const double* ofs;           /* [2*Nw] crop scale x pre*sqrt(Aeff)*ωwin on sidx (divided
-                                    by β(z) = ω/c Re neff on the device), crop scale else;
+    const double* ofs;           /* [2*Nw] crop scale x pre*ωwin on sidx (times
+                                    sqrt(Aeff(z))/β(z) on the device), crop scale else;
                                     pre = -i ω^2/(4 nlscale c)                              */
     double fd_xc[4];             /* x/c at x = ω0+2h, ω0+h, ω0-h, ω0-2h (h = 1e-4 ω0)        */
     double fd_gam[4];            /* γ(x)                                                    */
-    double fd_nwg[8];            /* nwg(x), complex                                         */
+    double fd_vn[8];             /* vn(x), complex                                          */
     double fd_h12;               /* 12 h                                                    */
 } luna_gradient_desc;
-/* Attach (or, with grad == NULL, remove) a pressure gradient. Replaces building the
- * transform with densityfun/βfun! and the linop with make_linop (Luna.jl:115-151). */
+/* Attach (or, with grad == NULL, remove) a pressure gradient and/or taper. Replaces building
+ * the transform with densityfun/aeff/βfun! and the linop with make_linop (Luna.jl:115-151). */
 int luna_b200_plan_set_gradient(luna_plan* plan, const luna_gradient_desc* grad);
-/* linop!(out, z) of make_linop (LinearOps.jl:337-360) for a plan with a pressure gradient,
- * evaluated on the device as the solvers do: linop [2*Nw] receives L(ω; z); outfac
- * (optional, [2*Nw]) the output factor ρ(z) x crop scale x pre*sqrt(Aeff)*ωwin/β(z)
+/* linop!(out, z) of make_linop (LinearOps.jl:330-360) for a plan with a pressure gradient
+ * or taper, evaluated on the device as the solvers do: linop [2*Nw] receives L(ω; z);
+ * outfac (optional, [2*Nw]) the output factor ρ(z) x crop scale x pre*sqrt(Aeff(z))*ωwin/β(z)
  * (ρ(z) x crop scale off sidx). Host arrays. */
 int luna_b200_plan_linop(luna_plan* plan, double z, double* linop, double* outfac);
 

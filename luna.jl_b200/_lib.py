@@ -66,9 +66,12 @@ class GradientDesc(ctypes.Structure):
     _fields_ = [("npts", c_int), ("two_point", c_int),
                 ("Z", c_double * GRAD_MAXPTS), ("P", c_double * GRAD_MAXPTS),
                 ("P2", c_double * GRAD_MAXPTS), ("dens_a", c_double), ("dens_b", c_double),
-                ("loss", c_int), ("gam", PD), ("nwg", PD), ("wc", PD), ("om", PD),
+                ("loss", c_int), ("nta", c_int), ("ZA", c_double * GRAD_MAXPTS),
+                ("A", c_double * GRAD_MAXPTS), ("unm", c_double), ("aeff_intg", c_double),
+                ("in_base", c_double), ("eps0c2", c_double),
+                ("gam", PD), ("vn", PD), ("wc", PD), ("om", PD),
                 ("imcap", PD), ("ofs", PD), ("fd_xc", c_double * 4), ("fd_gam", c_double * 4),
-                ("fd_nwg", c_double * 8), ("fd_h12", c_double)]
+                ("fd_vn", c_double * 8), ("fd_h12", c_double)]
 
 
 class SolveOpts(ctypes.Structure):

@@ -46,21 +46,22 @@ typedef struct {
     int ncomp;
 } LunaResp;
 
-// Pressure-gradient fill (z-dependent density, normalisation and linear operator); the
-// fields mirror luna_gradient_desc of the public header.
+// Pressure-gradient fill and/or taper (z-dependent density, radius, normalisation and
+// linear operator); the fields mirror luna_gradient_desc of the public header.
 #define LUNA_GRAD_NPTS 16
 typedef struct {
-    int npts, two_point, loss;
+    int npts, two_point, loss, nta;
     double Z[LUNA_GRAD_NPTS], P[LUNA_GRAD_NPTS], P2[LUNA_GRAD_NPTS];
-    double dens_a, dens_b;
+    double ZA[LUNA_GRAD_NPTS], A[LUNA_GRAD_NPTS];
+    double dens_a, dens_b, unm, aeff_intg, in_base, eps0c2;
     const double* gam;    // [Nw]
-    const double2* nwg;   // [Nw]
+    const double2* vn;    // [Nw]
     const double* wc;     // [Nw] ω/c on sidx, 0 elsewhere
     const double* om;     // [Nw]
     const double* imcap;  // [Nw]
     const double2* ofs;   // [Nw]
     double fd_xc[4], fd_gam[4];
-    double2 fd_nwg[4];
+    double2 fd_vn[4];
     double fd_h12;
 } LunaGrad;
 
@@ -80,11 +81,12 @@ typedef struct {
     double escale;          // 1/sqrt(eps0*c*Aeff/2): mode-averaged field -> V/m
     int nresp;
     LunaResp resp[LUNA_MAX_RESP];
-    // pressure gradient (null: constant density and linop); linz/outz hold L(z) and the
-    // output factor at the current stage node, written by the solver
+    // pressure gradient / taper (null: constant density, area and linop); linz/outz hold
+    // L(z) and the output factor at the current stage node, written by the solver;
+    // outz[Nw] = (field scale, Aeff) at that node
     const LunaGrad* grad;
     double2* linz;  // [Nw]
-    double2* outz;  // [Nw]
+    double2* outz;  // [Nw + 1]
     // ---- integrator (RK45.solve_precon) ----
     const double2* y0;   // [Nw] initial field (kept, so a batch can be re-run)
     double2* y;

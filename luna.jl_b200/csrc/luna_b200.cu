@@ -311,7 +311,7 @@ rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int sme
 // linop!(out, z) of a pressure-gradient plan and the output factor at z, on one CTA.
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
 grad_linop_kernel(LunaInst I, double z, double2* L, double2* of) {
-    __shared__ double bc[2];
+    __shared__ double bc[4];
     grad_fill_to(I, bc, z, true, L, of);
 }
 
@@ -702,7 +702,7 @@ static int launch_rhs(luna_plan* p, const double2* Ew, double2* nl, cudaStream_t
         }
         I.gscr = p->d_gscr;
         if (I.grad) {
-            if (!p->d_outz && dalloc(p->allocs, &p->d_outz, sizeof(double2) * I.Nw)) return LUNA_ERR_CUDA;
+            if (!p->d_outz && dalloc(p->allocs, &p->d_outz, sizeof(double2) * (I.Nw + 1))) return LUNA_ERR_CUDA;
             I.outz = p->d_outz;
         }
         if (!p->d_inst && dalloc(p->allocs, &p->d_inst, sizeof(LunaInst))) return LUNA_ERR_CUDA;
@@ -743,7 +743,13 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
     for (int i = 0; i < g->npts; ++i)
         if (!(g->P[i] >= 0) || g->P2[i] != g->P[i] * g->P[i])
             return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: pressures must be >= 0 with P2 = P*P");
-    if (!g->gam || !g->nwg || !g->wc || !g->om || !g->imcap || !g->ofs || !(g->fd_h12 > 0))
+    if (g->nta < 1 || g->nta > LUNA_GRAD_MAXPTS) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: nta out of range");
+    for (int i = 0; i < g->nta; ++i)
+        if (!(g->A[i] > 0) || (i + 1 < g->nta && !(g->ZA[i + 1] > g->ZA[i])))
+            return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: radii must be positive at increasing ZA");
+    if (!(g->unm > 0) || !(g->aeff_intg > 0) || !(g->in_base > 0) || !(g->eps0c2 > 0))
+        return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: mode constants must be positive");
+    if (!g->gam || !g->vn || !g->wc || !g->om || !g->imcap || !g->ofs || !(g->fd_h12 > 0))
         return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: null table");
     const size_t Nw = (size_t)p->proto.Nw;
     LunaGrad h;
@@ -758,15 +764,24 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
     }
     h.dens_a = g->dens_a;
     h.dens_b = g->dens_b;
+    h.nta = g->nta;
+    for (int i = 0; i < g->nta; ++i) {
+        h.ZA[i] = g->ZA[i];
+        h.A[i] = g->A[i];
+    }
+    h.unm = g->unm;
+    h.aeff_intg = g->aeff_intg;
+    h.in_base = g->in_base;
+    h.eps0c2 = g->eps0c2;
     for (int j = 0; j < 4; ++j) {
         h.fd_xc[j] = g->fd_xc[j];
         h.fd_gam[j] = g->fd_gam[j];
-        h.fd_nwg[j] = make_double2(g->fd_nwg[2 * j], g->fd_nwg[2 * j + 1]);
+        h.fd_vn[j] = make_double2(g->fd_vn[2 * j], g->fd_vn[2 * j + 1]);
     }
     h.fd_h12 = g->fd_h12;
     const double* t;
-    if (upload(p->allocs, g->gam, Nw, &h.gam) || upload(p->allocs, g->nwg, 2 * Nw, &t)) return LUNA_ERR_CUDA;
-    h.nwg = (const double2*)t;
+    if (upload(p->allocs, g->gam, Nw, &h.gam) || upload(p->allocs, g->vn, 2 * Nw, &t)) return LUNA_ERR_CUDA;
+    h.vn = (const double2*)t;
     if (upload(p->allocs, g->wc, Nw, &h.wc) || upload(p->allocs, g->om, Nw, &h.om) ||
         upload(p->allocs, g->imcap, Nw, &h.imcap) || upload(p->allocs, g->ofs, 2 * Nw, &t))
         return LUNA_ERR_CUDA;
@@ -784,7 +799,7 @@ int luna_b200_plan_linop(luna_plan* p, double z, double* linop, double* outfac) 
     if (!p->proto.grad) return fail(LUNA_ERR_BAD_ARG, "plan_linop: the plan has no pressure gradient");
     const size_t bytes = sizeof(double2) * p->proto.Nw;
     double2 *dL = nullptr, *dO = nullptr;
-    CK(cudaMalloc(&dL, 2 * bytes));
+    CK(cudaMalloc(&dL, 2 * bytes + sizeof(double2)));
     dO = dL + p->proto.Nw;
     grad_linop_kernel<<<1, LUNA_BLOCK>>>(p->proto, z, dL, dO);
     cudaError_t e = cudaGetLastError();
@@ -859,7 +874,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         size_t ok[7];
         for (int j = 0; j < 7; ++j) ok[j] = carve(Nw * kel);
         const size_t oe1 = carve(Nw * sizeof(double2));
-        const size_t olz = carve(I.grad ? Nw * sizeof(double2) : 0), ooz = carve(I.grad ? Nw * sizeof(double2) : 0);
+        const size_t olz = carve(I.grad ? Nw * sizeof(double2) : 0), ooz = carve(I.grad ? (Nw + 1) * sizeof(double2) : 0);
         const size_t og = carve(gsb);
         const size_t osv = carve((size_t)opts->saveN * Nw * sizeof(double2));
         const size_t olog = carve((size_t)(opts->steplog_cap > 0 ? opts->steplog_cap : 0) * 4 * sizeof(double));

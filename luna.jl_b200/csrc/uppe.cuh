@@ -710,7 +710,9 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
     const int M = I.No / 2;
     int P;
     cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P);
-    pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
+    // field scale 1/(nlscale sqrt(Aeff)) x pad/No; a taper's is in outz[Nw] at this node
+    const double sc = I.grad ? I.outz[I.Nw].x : I.in_scale;
+    pointwise_real<Rl>(I, w, x, M, P, sc);
     const cpx<double>* of = reinterpret_cast<const cpx<double>*>(I.outfac);
     // with a pressure gradient the factor of the current z is in outz, written by this
     // kernel (plain loads, not the read-only path)
@@ -1059,52 +1061,83 @@ __device__ __forceinline__ double grad_density(const LunaGrad* g, double z) {
     return __ddiv_rn(__dmul_rn(g->dens_a, p), __dadd_rn(1.0, __dmul_rn(g->dens_b, p)));
 }
 
-// sqrt(coren^2 - nwg), coren = sqrt(1 + γ ρ): principal root from r = |w|,
-// t = sqrt((r + |a|)/2); a >= 0: t + i b/(2t), else |b|/(2t) + i copysign(t, b)
-__device__ __forceinline__ double2 grad_neff(double gam, double2 nwg, double rho, int loss) {
+// core radius a(z): linear between nodes, the end values outside
+__device__ __forceinline__ double grad_radius(const LunaGrad* g, double z) {
+    const int n = g->nta;
+    if (n == 1 || z <= g->ZA[0]) return g->A[0];
+    if (z >= g->ZA[n - 1]) return g->A[n - 1];
+    int i = 0;
+    while (i + 1 < n - 1 && g->ZA[i + 1] < z) ++i;  // last i with ZA[i] < z
+    const double f = __ddiv_rn(__dsub_rn(z, g->ZA[i]), __dsub_rn(g->ZA[i + 1], g->ZA[i]));
+    return __dadd_rn(g->A[i], __dmul_rn(f, __dsub_rn(g->A[i + 1], g->A[i])));
+}
+
+__device__ __forceinline__ double grad_aeff(const LunaGrad* g, double a) {
+    return __dmul_rn(__dmul_rn(a, a), g->aeff_intg);
+}
+
+// sqrt(coren^2 - nwg), coren = sqrt(1 + γ ρ), nwg = (unm/(k a))^2 (1 - i vn/(k a))^2 written
+// as s^2 (p^2 - q^2, 2pq), p = 1 + Im vn/(k a), q = -Re vn/(k a); principal root from
+// r = |w|, t = sqrt((r + |x|)/2): x >= 0 gives t + i y/(2t), else |y|/(2t) + i copysign(t, y)
+__device__ __forceinline__ double2 grad_neff(double gam, double kc, double2 vn, double unm, double a, double rho,
+                                             int loss) {
+    const double ka = __dmul_rn(kc, a);
+    const double s = __ddiv_rn(unm, ka);
+    const double s2 = __dmul_rn(s, s);
+    const double p = __dadd_rn(1.0, __ddiv_rn(vn.y, ka));
+    const double q = -__ddiv_rn(vn.x, ka);
+    const double nr = __dmul_rn(s2, __dsub_rn(__dmul_rn(p, p), __dmul_rn(q, q)));
+    const double ni = __dmul_rn(s2, __dmul_rn(2.0, __dmul_rn(p, q)));
     const double cr = __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(gam, rho)));
-    const double a = __dsub_rn(__dmul_rn(cr, cr), nwg.x);
-    const double b = -nwg.y;
-    const double r = __dsqrt_rn(__dadd_rn(__dmul_rn(a, a), __dmul_rn(b, b)));
+    const double x = __dsub_rn(__dmul_rn(cr, cr), nr);
+    const double y = -ni;
+    const double r = __dsqrt_rn(__dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y)));
     double re, im;
-    if (a >= 0) {
-        const double t = __dsqrt_rn(__dmul_rn(__dadd_rn(r, a), 0.5));
+    if (x >= 0) {
+        const double t = __dsqrt_rn(__dmul_rn(__dadd_rn(r, x), 0.5));
         re = t;
-        im = (t != 0) ? __ddiv_rn(b, __dmul_rn(2.0, t)) : 0.0;
+        im = (t != 0) ? __ddiv_rn(y, __dmul_rn(2.0, t)) : 0.0;
     } else {
-        const double t = __dsqrt_rn(__dmul_rn(__dsub_rn(r, a), 0.5));
-        re = fabs(__ddiv_rn(b, __dmul_rn(2.0, t)));
-        im = copysign(t, b);
+        const double t = __dsqrt_rn(__dmul_rn(__dsub_rn(r, x), 0.5));
+        re = fabs(__ddiv_rn(y, __dmul_rn(2.0, t)));
+        im = copysign(t, y);
     }
     return make_double2(re, loss ? im : 0.0);
 }
 
 // β1(z): 4-point central difference of x/c Re neff(x) (low-index rule) at ω0
-__device__ __forceinline__ double grad_beta1(const LunaGrad* g, double rho) {
+__device__ __forceinline__ double grad_beta1(const LunaGrad* g, double rho, double a) {
     double f[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
-        const double re = grad_neff(g->fd_gam[j], g->fd_nwg[j], rho, g->loss).x;
+        const double re = grad_neff(g->fd_gam[j], g->fd_xc[j], g->fd_vn[j], g->unm, a, rho, g->loss).x;
         f[j] = __dmul_rn(g->fd_xc[j], (re < 1e-3) ? 1e-3 : re);
     }
     const double num = __dadd_rn(__dsub_rn(__dadd_rn(-f[0], __dmul_rn(8.0, f[1])), __dmul_rn(8.0, f[2])), f[3]);
     return __ddiv_rn(num, g->fd_h12);
 }
 
-// The gradient at z for the whole CTA: L(ω; z) into Lout (when wantL) and the output
-// factor ρ(z) ofs/β(z) (ρ(z) ofs off sidx) into oout. One thread evaluates ρ and β1 and
-// passes them through bc (2 doubles of shared memory).
+// The gradient/taper at z for the whole CTA: L(ω; z) into Lout (when wantL), the output
+// factor ρ(z) sqrt(Aeff(z)) ofs/β(z) (ρ(z) ofs off sidx) into oout[0..Nw-1] and
+// (field scale, Aeff) into oout[Nw]. One thread evaluates the scalars and passes them
+// through bc (4 doubles of shared memory).
 __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double z, bool wantL, double2* Lout,
                                           double2* oout) {
     const LunaGrad* g = I.grad;
     __syncthreads();
     if (threadIdx.x == 0) {
         const double rho = grad_density(g, z);
+        const double a = grad_radius(g, z);
+        const double ae = grad_aeff(g, a);
         bc[0] = rho;
-        bc[1] = wantL ? grad_beta1(g, rho) : 0.0;
+        bc[1] = a;
+        bc[2] = wantL ? grad_beta1(g, rho, a) : 0.0;
+        bc[3] = ae;
+        oout[I.Nw] = make_double2(g->in_base / sqrt(ae), ae);
     }
     __syncthreads();
-    const double rho = bc[0], b1 = bc[1];
+    const double rho = bc[0], a = bc[1], b1 = bc[2], sae = sqrt(bc[3]);
+    const bool tapered = g->nta > 1;
     cpx<double>* Lz = reinterpret_cast<cpx<double>*>(Lout);
     cpx<double>* oz = reinterpret_cast<cpx<double>*>(oout);
     for (int i = threadIdx.x; i < I.Nw; i += LUNA_BLOCK) {
@@ -1115,14 +1148,16 @@ __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double 
             oz[i] = mk<double>(rho * o.x, rho * o.y);
             continue;
         }
-        const double2 n = grad_neff(__ldg(g->gam + i), __ldg(g->nwg + i), rho, g->loss);
+        const double2 n = grad_neff(__ldg(g->gam + i), wc, __ldg(g->vn + i), g->unm, a, rho, g->loss);
         if (wantL) {
             const double re = fmax(n.x, 1e-3);                       // conj_clamp
             const double im = fmin(fmax(n.y, 0.0), __ldg(g->imcap + i));
             const double X = __dsub_rn(__dmul_rn(wc, re), __dmul_rn(__ldg(g->om + i), b1));
             Lz[i] = mk<double>(-__dmul_rn(wc, im), -X);
         }
-        const double f = rho / __dmul_rn(wc, n.x);  // ρ / β(z)
+        // β(z) = ω/c Re neff, with the low-index rule of neff(m, ω; z) for a taper
+        const double nb = (tapered && n.x < 1e-3) ? 1e-3 : n.x;
+        const double f = rho * sae / __dmul_rn(wc, nb);
         oz[i] = mk<double>(f * o.x, f * o.y);
     }
     __syncthreads();
@@ -1171,6 +1206,9 @@ __device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const doub
     double vmax = -1.0;
     int imax = 0;
     double rs = 0, rmax = 0, redge = 0;
+    // a taper's effective area and field scale at z
+    const double aeff = I.grad ? grad_aeff(I.grad, grad_radius(I.grad, z)) : I.aeff;
+    const double esc = I.grad ? 1.0 / sqrt(I.grad->eps0c2 * aeff) : I.escale;
     for (int n = tid; n < N; n += T) {
         const cpx<double> e = scale(invN, cvt<double>(x[Swz<Rl>::f(split_pos(n, N, P))]));
         const double pt = abs2(e);
@@ -1179,7 +1217,7 @@ __device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const doub
             imax = n;
         }
         if (ip >= 0) {
-            const double E = e.x * I.escale;
+            const double E = e.x * esc;
             const double r = (double)eval_rate<Rl>(I.resp[ip], (Rl)fabs(E), w.flag);
             rs += r;
             rmax = fmax(rmax, r);
@@ -1223,7 +1261,7 @@ __device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const doub
         row[2] = sw / s1;
         row[3] = 2.0 * 3.141592653589793 / (wl * wl) * (h * ss);
         row[4] = vmax;
-        row[5] = vmax / I.aeff;
+        row[5] = vmax / aeff;
         row[6] = fmn;
         row[7] = fmx;
         if (ip >= 0) {

@@ -1,4 +1,4 @@
-"""Pressure-gradient capillary fills, mirroring Luna.jl.
+"""Pressure-gradient fills and tapered capillaries, mirroring Luna.jl.
 
 * ``Gradient`` — Capillary.gradient(gas, L, p0, p1) (Capillary.jl:306-315):
   p(z) = sqrt(p0^2 + z/L (p1^2 - p0^2)) inside [0, L], p0 before and p1 after, and the
@@ -6,14 +6,23 @@
   index sqrt(1 + γ(λ) ρ(z)). The density is this package's closed form (ideal gas with a
   second virial coefficient, ``physdata.density``) where the reference interpolates a
   CoolProp spline.
-* ``MarcatiliGradientMode`` — MarcatiliMode(a, coren) with that z-dependent core index:
-  the waveguide term nwg(ω) (``neff_wg``, Capillary.jl:188-200) is fixed and
-  neff(ω; z) = sqrt(coren(ω; z)^2 - nwg(ω)) (Capillary.jl:216-224, neff_β_grid :345-360).
-* ``make_linop`` — LinearOps.make_linop for a field-resolved grid (LinearOps.jl:337-360):
+* ``Taper`` — a core radius a(z) (MarcatiliMode(afun, ...), Capillary.jl:95-109, 236-242),
+  given as piecewise-linear nodes: the reference takes any Julia function; a C ABI takes
+  tables.
+* ``MarcatiliGradientMode`` — MarcatiliMode(a, coren) with the z-dependent core index and,
+  with a taper, radius: neff(ω; z) = sqrt(coren(ω; z)^2 - nwg(ω; a(z)))
+  (Capillary.jl:153-224, neff_β_grid :345-360), Aeff(z) = a(z)^2 x the mode integral
+  (Capillary.jl:295).
+* ``make_linop`` — LinearOps.make_linop for a field-resolved grid (LinearOps.jl:330-360):
   L(ω; z) = -i(ω/c conj_clamp(neff(ω; z)) - ω β1(z)) on sidx (conj_clamp, :254), and
-  βfun(z) for the normalisation.
-* ``TransModeAvgZ`` — TransModeAvg with densityfun(z) and norm_mode_average's βfun!(β, z)
-  (NonlinearRHS.jl:362-387).
+  βfun(z) for the normalisation (with the low-index rule of neff(m, ω; z) for a taper, whose
+  make_linop goes through Modes.neff/Modes.β, LinearOps.jl:330-335).
+* ``TransModeAvgZ`` — TransModeAvg with densityfun(z), aeff(z) and norm_mode_average's
+  βfun!(β, z) (NonlinearRHS.jl:362-387).
+
+Every z-dependent quantity is written out in IEEE-rounded real operations in the order the
+device evaluates it: β1(z) is a finite difference with h = 1e-4 ω0 that turns an ulp of
+neff into ~1e-12 of β1, so host and device must not differ in a single rounding.
 """
 import math
 
@@ -21,6 +30,8 @@ import numpy as np
 
 from . import modes, physdata as pd
 from .nonlinearrhs import TransModeAvg, nlscale
+
+MAXPTS = 16
 
 
 class Gradient:
@@ -74,33 +85,70 @@ class Gradient:
         return np.sqrt(1 + self.gamma(ω) * self.density(z))
 
 
+class Taper:
+    """Core radius through nodes (Z, A): linear on each segment, A[0] for z <= Z[0] and A[-1]
+    for z >= Z[-1]. One node is a constant radius."""
+
+    def __init__(self, Z, A):
+        self.Z = np.atleast_1d(np.asarray(Z, dtype=np.float64)).copy()
+        self.A = np.atleast_1d(np.asarray(A, dtype=np.float64)).copy()
+        if len(self.Z) != len(self.A) or not 1 <= len(self.Z) <= MAXPTS:
+            raise ValueError(f"1 to {MAXPTS} radius nodes with one position each")
+        if np.any(np.diff(self.Z) <= 0) or np.any(self.A <= 0):
+            raise ValueError("taper nodes need increasing z and positive radii")
+
+    @property
+    def constant(self):
+        return len(self.A) == 1
+
+    def a(self, z):
+        Z, A = self.Z, self.A
+        if z <= Z[0]:
+            return float(A[0])
+        if z >= Z[-1]:
+            return float(A[-1])
+        i = int(np.searchsorted(Z, z, side="left")) - 1  # last i with Z[i] < z
+        return float(A[i] + (z - Z[i]) / (Z[i + 1] - Z[i]) * (A[i + 1] - A[i]))
+
+
 class MarcatiliGradientMode(modes.MarcatiliMode):
+    """Full Marcatili model with a z-dependent fill (``Gradient``) and core radius
+    (``Taper``; a number is a constant radius)."""
+
     def __init__(self, a, grad, n=1, m=1, kind="HE", model="full", loss=True):
         if model != "full":
             raise NotImplementedError("only the full Marcatili model")
-        super().__init__(a, None, 1.0, n=n, m=m, kind=kind, model=model, loss=loss)
+        self.taper = a if isinstance(a, Taper) else Taper([0.0], [a])
+        super().__init__(self.taper.a(0.0), None, 1.0, n=n, m=m, kind=kind, model=model, loss=loss)
         self.grad = grad
 
-    def nwg(self, ω):
-        """Waveguide part (unm/(k a))^2 (1 - i vn/(k a))^2 (Capillary.jl:188-200)."""
-        ω = np.asarray(ω, dtype=np.float64)
-        εcl = pd.sio2_index(pd.wlfreq(ω)) ** 2
-        vn = self._vn(εcl)
-        k = ω / pd.c
-        return (self.unm / (k * self.a)) ** 2 * (1 - 1j * vn / (k * self.a)) ** 2
+    @property
+    def tapered(self):
+        return not self.taper.constant
 
-    def neff_parts(self, gam, nwg, rho):
-        """(Re, Im) of sqrt(coren^2 - nwg) with coren = sqrt(1 + gam rho), in the operation
-        order the device uses (Capillary.jl:216-224)."""
+    def radius(self, z):
+        return self.taper.a(z)
+
+    def Aeff_z(self, z):
+        """Modes.Aeff(m; z) = radius(m, z)^2 x the mode integral (Capillary.jl:295)."""
+        r = self.radius(z)
+        return r * r * self.aeff_intg
+
+    def neff_parts(self, gam, kc, vn, rho, a):
+        """(Re, Im) of sqrt(coren^2 - nwg) with coren = sqrt(1 + gam rho) and nwg at radius a
+        (Capillary.jl:153-224), in the operation order the device uses."""
+        nr, ni = modes.nwg_rn(kc, a, self.unm, vn)
         cr = np.sqrt(1 + gam * rho)
-        re, im = modes.csqrt_rn(cr * cr - np.real(nwg), -np.imag(nwg))
+        re, im = modes.csqrt_rn(cr * cr - nr, -ni)
         if not self.loss:
             im = np.zeros_like(im)
         return re, im
 
     def neff_grid(self, ω, z):
-        """neff(mode, coren^2, nwg) (Capillary.jl:216-224): no clamp."""
-        re, im = self.neff_parts(self.grad.gamma(ω), self.nwg(ω), self.grad.density(z))
+        """sqrt(coren(ω; z)^2 - nwg(ω; a(z))) without the low-index rule."""
+        ω = np.asarray(ω, dtype=np.float64)
+        re, im = self.neff_parts(self.grad.gamma(ω), ω / pd.c, self.vn(ω), self.grad.density(z),
+                                 self.radius(z))
         return re + 1j * im
 
     def neff_z(self, ω, z):
@@ -112,16 +160,16 @@ class MarcatiliGradientMode(modes.MarcatiliMode):
 
     def fd_tables(self, ω0):
         """The z-independent inputs of the group-delay finite difference at ω0 + 2h, ω0 + h,
-        ω0 - h, ω0 - 2h (h = 1e-4 ω0): x/c, gam(x), nwg(x), and 12h."""
+        ω0 - h, ω0 - 2h (h = 1e-4 ω0): x/c, gam(x), vn(x), and 12h."""
         h = ω0 * 1e-4
         x = np.array([ω0 + 2 * h, ω0 + h, ω0 - h, ω0 - 2 * h])
-        return x / pd.c, self.grad.gamma(x), self.nwg(x), 12 * h
+        return x / pd.c, self.grad.gamma(x), self.vn(x), 12 * h
 
     def dispersion_z(self, ω0, z):
         """β1(z) = dβ/dω at ω0: the 4-point central difference of MarcatiliMode.dispersion,
         with β = x/c Re(neff) and the low-index rule."""
-        xc, gam, nwg, h12 = self.fd_tables(ω0)
-        re, _ = self.neff_parts(gam, nwg, self.grad.density(z))
+        xc, gam, vn, h12 = self.fd_tables(ω0)
+        re, _ = self.neff_parts(gam, xc, vn, self.grad.density(z), self.radius(z))
         re = np.where(re < 1e-3, 1e-3, re)
         f = xc * re
         return float((-f[0] + 8 * f[1] - 8 * f[2] + f[3]) / h12)
@@ -133,7 +181,7 @@ def conj_clamp(n, ω):
 
 
 def make_linop(grid, mode, λ0):
-    """(linop(z), βfun(z)) for a field-resolved grid (LinearOps.jl:337-360):
+    """(linop(z), βfun(z)) for a field-resolved grid (LinearOps.jl:330-360):
     L = -i(ω/c conj_clamp(neff) - ω β1(z)) on sidx, written out in real arithmetic
     (Re L = -ω/c Im nc, Im L = -(ω/c Re nc - ω β1)), as the device evaluates it."""
     ω0 = pd.wlfreq(λ0)
@@ -142,12 +190,15 @@ def make_linop(grid, mode, λ0):
     wc = ω / pd.c
     cap = 3000 * pd.c / ω
     gam = mode.grad.gamma(ω)
-    nwg = mode.nwg(ω)
+    vn = mode.vn(ω)
+
+    def parts(z):
+        return mode.neff_parts(gam, wc, vn, mode.grad.density(z), mode.radius(z))
 
     def linop(z):
         out = np.zeros(len(grid.ω), dtype=np.complex128)
         β1 = mode.dispersion_z(ω0, z)
-        re, im = mode.neff_parts(gam, nwg, mode.grad.density(z))
+        re, im = parts(z)
         re = np.maximum(re, 1e-3)                   # conj_clamp (LinearOps.jl:254)
         im = np.minimum(np.maximum(im, 0.0), cap)
         out.real[s] = -(wc * im)
@@ -156,7 +207,9 @@ def make_linop(grid, mode, λ0):
 
     def βfun(z):
         out = np.ones(len(grid.ω))
-        re, _ = mode.neff_parts(gam, nwg, mode.grad.density(z))
+        re, _ = parts(z)
+        if mode.tapered:
+            re = np.where(re < 1e-3, 1e-3, re)      # Modes.β through neff(m, ω; z)
         out[s] = wc * re
         return out
 
@@ -164,67 +217,78 @@ def make_linop(grid, mode, λ0):
 
 
 class TransModeAvgZ(TransModeAvg):
-    """TransModeAvg with a z-dependent density and normalisation (pressure gradient)."""
+    """TransModeAvg with a z-dependent density, effective area and normalisation
+    (pressure gradient and/or taper)."""
 
     kind = "modeavg_z"
 
-    def __init__(self, grid, resp, grad, mode, aeff, λ0, shock=True):
+    def __init__(self, grid, resp, grad, mode, λ0, shock=True):
         self.grad, self.mode, self.λ0 = grad, mode, λ0
         ω = grid.ω
         shockterm = ω ** 2 if shock else ω * pd.wlfreq(grid.referenceλ)
         self.pre = -1j * shockterm / 4 / nlscale / pd.c
         _, self.βfun = make_linop(grid, mode, λ0)
-        super().__init__(grid, resp, grad.density(0.0), None, aeff)
+        super().__init__(grid, resp, grad.density(0.0), None, mode.Aeff_z(0.0))
 
     def densityfun(self, z):
         return self.grad.density(z)
 
+    def aefffun(self, z):
+        return self.mode.Aeff_z(z)
+
     def norm_factor(self, z):
-        """pre/β(z) sqrt(Aeff) ωwin on sidx (NonlinearRHS.jl:375-387 and the ωwin loop)."""
+        """pre/β(z) sqrt(Aeff(z)) ωwin on sidx (NonlinearRHS.jl:375-387 and the ωwin loop)."""
         g = self.grid
         s = g.sidx
         f = np.ones(len(g.ω), dtype=np.complex128)
         β = self.βfun(z)
-        f[s] = self.pre[s] / β[s] * math.sqrt(self.aeff) * g.ωwin[s]
+        f[s] = self.pre[s] / β[s] * math.sqrt(self.aefffun(z)) * g.ωwin[s]
         return f
 
     def output_factor(self):
-        raise TypeError("the normalisation of a pressure gradient depends on z")
+        raise TypeError("the normalisation of a pressure gradient or taper depends on z")
 
 
-def gradient_desc(t, crop, keep):
+def gradient_desc(t, crop, pad_No, keep):
     """luna_gradient_desc of a TransModeAvgZ for the C ABI (luna_b200_plan_set_gradient);
-    ``crop`` is the plan's crop scale, ``keep`` collects the host arrays it points to."""
+    ``crop`` is the plan's crop scale, ``pad_No`` its pad scale / No, ``keep`` collects the
+    host arrays the descriptor points to."""
     from . import _lib
-    g, grid, mode, grad = t, t.grid, t.mode, t.grad
-    n = len(grad.Z)
-    if n > _lib.GRAD_MAXPTS:
-        raise ValueError(f"at most {_lib.GRAD_MAXPTS} pressure nodes")
+    grid, mode, grad = t.grid, t.mode, t.grad
+    n, nta = len(grad.Z), len(mode.taper.Z)
+    if n > _lib.GRAD_MAXPTS or nta > _lib.GRAD_MAXPTS:
+        raise ValueError(f"at most {_lib.GRAD_MAXPTS} pressure or radius nodes")
     s = np.zeros(len(grid.ω), dtype=bool)
     s[grid.sidx] = True
     ω = grid.ω
     gam = np.zeros(len(ω))
-    nwg = np.zeros(len(ω), dtype=np.complex128)
+    vn = np.zeros(len(ω), dtype=np.complex128)
     wc = np.zeros(len(ω))
     cap = np.zeros(len(ω))
     gam[s] = grad.gamma(ω[s])
-    nwg[s] = mode.nwg(ω[s])
+    vn[s] = mode.vn(ω[s])
     wc[s] = ω[s] / pd.c
     cap[s] = 3000 * pd.c / ω[s]
     ofs = np.full(len(ω), crop, dtype=np.complex128)
-    ofs[s] = crop * (t.pre[s] * math.sqrt(t.aeff) * grid.ωwin[s])
+    ofs[s] = crop * (t.pre[s] * grid.ωwin[s])
     om = np.ascontiguousarray(ω, dtype=np.float64)
-    arrs = [np.ascontiguousarray(a) for a in (gam, nwg, wc, om, cap, ofs)]
+    arrs = [np.ascontiguousarray(a) for a in (gam, vn, wc, om, cap, ofs)]
     keep += arrs
     d = _lib.GradientDesc()
     d.npts, d.two_point, d.loss = n, int(grad.two_point), int(bool(mode.loss))
     for i in range(n):
         d.Z[i], d.P[i], d.P2[i] = grad.Z[i], grad.P[i], grad.P2[i]
     d.dens_a, d.dens_b = grad.dens_a, grad.dens_b
-    d.gam, d.nwg, d.wc, d.om, d.imcap, d.ofs = [_lib.dptr(a.view(np.float64)) for a in arrs]
-    xc, fg, fn, h12 = mode.fd_tables(pd.wlfreq(g.λ0))
+    d.nta = nta
+    for i in range(nta):
+        d.ZA[i], d.A[i] = mode.taper.Z[i], mode.taper.A[i]
+    d.unm, d.aeff_intg = mode.unm, mode.aeff_intg
+    d.in_base = pad_No / nlscale
+    d.eps0c2 = pd.eps_0 * pd.c / 2
+    d.gam, d.vn, d.wc, d.om, d.imcap, d.ofs = [_lib.dptr(a.view(np.float64)) for a in arrs]
+    xc, fg, fv, h12 = mode.fd_tables(pd.wlfreq(t.λ0))
     for j in range(4):
         d.fd_xc[j], d.fd_gam[j] = xc[j], fg[j]
-        d.fd_nwg[2 * j], d.fd_nwg[2 * j + 1] = fn[j].real, fn[j].imag
+        d.fd_vn[2 * j], d.fd_vn[2 * j + 1] = fv[j].real, fv[j].imag
     d.fd_h12 = h12
     return d

@@ -66,8 +66,10 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         energy=None, power=None, pulseshape="gauss", shotnoise=False,
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16):
-    """Mode-averaged HE11 capillary set-up (Interface.jl:360-401); ``pressure`` is a number
-    or a (p0, p1) gradient over the fibre (Capillary.gradient, Capillary.jl:306-315)."""
+    """Mode-averaged HE11 capillary set-up (Interface.jl:360-401). ``pressure`` is a number,
+    a (p0, p1) gradient over the fibre or (Z, P) nodes (Capillary.gradient,
+    Capillary.jl:306-337); ``radius`` is a number or (Z, A) nodes of a piecewise-linear taper
+    (a z-dependent radius, Interface.jl:249-250)."""
     if shotnoise:
         raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
     if envelope:
@@ -76,13 +78,19 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     thg = (not envelope) if thg is None else thg
     grid = RealGrid(flength, λ0, λlims, trange, δt)
     grad = None
-    if isinstance(pressure, (tuple, list)):
-        # simple gradient (p0, p1) over the fibre (Interface.jl:495-499, 524-526)
-        from .gradient import Gradient, MarcatiliGradientMode
-        if len(pressure) == 2 and all(np.ndim(x) == 0 for x in pressure):
+    tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
+    if isinstance(pressure, (tuple, list)) or tapered:
+        # pressure gradient (p0, p1) or (Z, P) (Interface.jl:495-504, 524-531) and/or a
+        # z-dependent radius (Interface.jl:249-250), given here as nodes (Z, A)
+        from .gradient import Gradient, MarcatiliGradientMode, Taper
+        if not isinstance(pressure, (tuple, list)):
+            grad = Gradient(gas, flength, pressure, pressure)
+        elif len(pressure) == 2 and all(np.ndim(x) == 0 for x in pressure):
             grad = Gradient(gas, flength, *pressure)      # (p0, p1)
         else:
             grad = Gradient(gas, *pressure)               # (Z, P)
+        if isinstance(radius, (tuple, list)):
+            radius = Taper(*radius)
         mode = MarcatiliGradientMode(radius, grad, model=model, loss=loss)
         density = grad.density(0.0)
     else:
@@ -105,7 +113,6 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     if raman:
         rr = _raman.raman_response(grid.to, gas)
         resp.append(RamanPolarField(grid.to, rr))
-    aeff = mode.Aeff()
     if grad is not None:
         # z-dependent linear operator and normalisation (LinearOps.make_linop,
         # LinearOps.jl:337-360; norm_mode_average with βfun!(β, z))
@@ -113,8 +120,9 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         if raman:
             raise NotImplementedError("Raman responses with a pressure gradient are not supported")
         linop, _ = make_linop(grid, mode, λ0)
-        transform = TransModeAvgZ(grid, resp, grad, mode, aeff, λ0)
+        transform = TransModeAvgZ(grid, resp, grad, mode, λ0)
     else:
+        aeff = mode.Aeff()
         linop, βconst, β1 = make_const_linop(grid, mode, λ0)
         norm = norm_mode_average(grid, βconst)
         transform = TransModeAvg(grid, resp, density, norm, aeff)

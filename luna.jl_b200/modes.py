@@ -30,6 +30,20 @@ def csqrt_rn(a, b):
     return np.where(pos, t, np.abs(q)), np.where(pos, q, np.copysign(t, b))
 
 
+def nwg_rn(kc, a, unm, vn):
+    """(Re, Im) of the Marcatili waveguide term (unm/(k a))^2 (1 - i vn/(k a))^2
+    (Capillary.jl:188-200), in IEEE-rounded real operations: s = unm/(k a),
+    p + iq = 1 - i vn/(k a) = (1 + Im vn/(k a)) - i Re vn/(k a), term = s^2 (p^2 - q^2, 2pq).
+    The device evaluates the same sequence for a tapered core."""
+    vn = np.asarray(vn)
+    ka = kc * a
+    s = unm / ka
+    s2 = s * s
+    p = 1 + np.imag(vn) / ka
+    q = -(np.real(vn) / ka)
+    return s2 * (p * p - q * q), s2 * (2 * (p * q))
+
+
 class SimpleMode:
     def __init__(self, ωref, βs, Aeff=1.0, loss=0.0):
         self.ωref = ωref
@@ -89,15 +103,17 @@ class MarcatiliMode:
             return 1 / np.sqrt(εcl - 1)
         return εcl / np.sqrt(εcl - 1)
 
+    def vn(self, ω):
+        """get_vn(εcl, kind) (Capillary.jl:88-93) with the silica cladding index at ω."""
+        return np.ascontiguousarray(self._vn(pd.sio2_index(pd.wlfreq(np.asarray(ω, dtype=np.float64))) ** 2))
+
     def neff(self, ω):
         ω = np.asarray(ω, dtype=np.float64)
         lam = pd.wlfreq(ω)
-        εcl = pd.sio2_index(lam) ** 2
-        εco = self.coren(lam) ** 2
-        vn = self._vn(εcl)
+        εco = np.real(self.coren(lam) ** 2)
         k = ω / pd.c
-        d = εco - (self.unm / (k * self.a)) ** 2 * (1 - 1j * vn / (k * self.a)) ** 2
-        re, im = csqrt_rn(np.real(d), np.imag(d))
+        nr, ni = nwg_rn(k, self.a, self.unm, self.vn(ω))
+        re, im = csqrt_rn(εco - nr, -ni)
         nn = re + 1j * im
         if not self.loss:
             nn = np.real(nn) + 0j

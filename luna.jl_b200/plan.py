@@ -133,7 +133,7 @@ class Plan:
         plan = cls(gd, rds, keep, precision, Nw)
         if zdep:
             from .gradient import gradient_desc
-            gdesc = gradient_desc(t, crop, plan._keep)
+            gdesc = gradient_desc(t, crop, pad / No, plan._keep)
             plan._gdesc = gdesc
             _lib.check(_lib.load().luna_b200_plan_set_gradient(plan.handle, _lib.ctypes.byref(gdesc)))
         return plan

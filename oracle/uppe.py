@@ -197,6 +197,8 @@ def trans_mode_avg(t, Ew, z):
     Et = to_time(g, Ew)
     Et = Et / (NLSCALE * math.sqrt(t.aeff))
     zdep = getattr(t, "kind", "") == "modeavg_z"
+    if zdep:  # aeff(z) of a taper (Modes.Aeff(m; z))
+        Et = to_time(g, Ew) / (NLSCALE * math.sqrt(t.aefffun(z)))
     Pt = et_to_pt(Et, t.resp, t.densityfun(z) if zdep else t.density)
     Pt = Pt * g.towin
     nl = to_freq(g, Pt, len(Ew))
@@ -449,18 +451,20 @@ def stats_default(t, Ew, z, dz):
     Ewa[:n] = 2 * Ew[:n]
     Eta = np.fft.ifft(Ewa)
     Pt = np.abs(Eta) ** 2
+    zdep = getattr(t, "kind", "") == "modeavg_z"
+    aeff = t.aefffun(z) if zdep else t.aeff
     out["peakpower"] = np.max(Pt)
-    out["peakintensity"] = np.max(Pt) / t.aeff
+    out["peakintensity"] = np.max(Pt) / aeff
     out["fwhm_t_min"] = fwhm_linear(g.t, Pt, "min")
     out["fwhm_t_max"] = fwhm_linear(g.t, Pt, "max")
     out["electrondensity"] = math.nan
     out["peak_ionisation_rate"] = math.nan
     for r in t.resp:
         if getattr(r, "kind", "") == "plasma":
-            Eto = np.real(Eta) / math.sqrt(EPS0 * 299792458.0 * t.aeff / 2)
+            Eto = np.real(Eta) / math.sqrt(EPS0 * 299792458.0 * aeff / 2)
             rr = rate(r.ratefunc, Eto)
             frac = cumtrapz(rr, g.t[1] - g.t[0])
-            rho = t.densityfun(z) if getattr(t, "kind", "") == "modeavg_z" else t.density
+            rho = t.densityfun(z) if zdep else t.density
             out["electrondensity"] = (1 - math.exp(-frac[-1])) * rho
             out["peak_ionisation_rate"] = np.max(rr)
     return out

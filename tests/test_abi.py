@@ -75,7 +75,9 @@ int main(void) {
     printf("luna_gradient_desc %zu\n", sizeof(luna_gradient_desc));
     P(luna_gradient_desc, Z); P(luna_gradient_desc, P2); P(luna_gradient_desc, dens_b);
     P(luna_gradient_desc, loss); P(luna_gradient_desc, gam); P(luna_gradient_desc, ofs);
-    P(luna_gradient_desc, fd_xc); P(luna_gradient_desc, fd_nwg); P(luna_gradient_desc, fd_h12);
+    P(luna_gradient_desc, fd_xc); P(luna_gradient_desc, fd_vn); P(luna_gradient_desc, fd_h12);
+    P(luna_gradient_desc, nta); P(luna_gradient_desc, ZA); P(luna_gradient_desc, eps0c2);
+    P(luna_gradient_desc, vn);
     return 0;
 }
 """
@@ -110,5 +112,6 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_solve_stats.z"]) == _lib.SolveStats.z.offset
     assert int(out["luna_solve_stats.dz"]) == _lib.SolveStats.dz.offset
     assert int(out["luna_gradient_desc"]) == ctypes.sizeof(_lib.GradientDesc)
-    for f in ("Z", "P2", "dens_b", "loss", "gam", "ofs", "fd_xc", "fd_nwg", "fd_h12"):
+    for f in ("Z", "P2", "dens_b", "loss", "gam", "ofs", "fd_xc", "fd_vn", "fd_h12", "nta", "ZA",
+              "eps0c2", "vn"):
         assert int(out[f"luna_gradient_desc.{f}"]) == getattr(_lib.GradientDesc, f).offset

@@ -65,7 +65,7 @@ def test_equal_pressure_linop_matches_constant(loss):
     lin, βfun = make_linop(grid, m, 800e-9)
     linc, βc, _ = make_const_linop(grid, mc, 800e-9)
     normc = norm_mode_average(grid, βc)
-    t = TransModeAvgZ(grid, p.transform.resp, g, m, m.Aeff(), 800e-9)
+    t = TransModeAvgZ(grid, p.transform.resp, g, m, 800e-9)
     s = grid.sidx
     for z in np.linspace(0, 1.0, 10):
         assert _rel(lin(z), linc) < 1e-14
@@ -115,6 +115,44 @@ def test_gradient_rejects_raman():
                             energy=50e-6, λlims=(400e-9, 2000e-9), trange=0.5e-12)
 
 
+def _taper_case(radius, pressure=5.0, flength=5e-2):
+    return prop_capillary_args(radius, flength, "Ar", pressure, λ0=800e-9, τfwhm=30e-15,
+                               energy=1e-6, λlims=(160e-9, 3000e-9), trange=0.5e-12,
+                               plasma=False, loss=False, saveN=21)
+
+
+def test_constant_taper_matches_constant_radius():
+    """test_tapers.jl "const vs afun": a taper whose radius does not change reproduces the
+    constant-radius linop and propagation."""
+    a = 13e-6
+    c = _taper_case(a)
+    t = _taper_case(([0.0, 5e-2], [a, a]))
+    for z in (0.0, 0.02, 0.05):
+        assert np.array_equal(t.linop(z), c.linop)
+        assert t.transform.aefffun(z) == pytest.approx(c.transform.aeff, rel=1e-15)
+    rc = uppe.run(c.transform, c.grid, c.linop, c.Eω, saveN=21)
+    rt = uppe.run(t.transform, t.grid, t.linop, t.Eω, saveN=21)
+    assert rt.steps == rc.steps
+    for x, y in zip(rt.Eω, rc.Eω):
+        assert _rel(x, y) < 1e-12
+
+
+def test_taper_linop_and_area_track_local_radius():
+    """A linear taper a(z) = a0 + (aL - a0) z/L: at each z the linop is the constant-radius
+    linop at a(z) and Aeff(z) = a(z)^2 x the mode integral (Capillary.jl:295)."""
+    a0, aL, L = 13e-6, 0.75 * 13e-6, 0.1
+    t = _taper_case(([0.0, L], [a0, aL]), flength=L)
+    m = t.transform.mode
+    for z in (0.0, 0.03, 0.07, L):
+        az = a0 + (z / L) * (aL - a0)
+        assert m.radius(z) == pytest.approx(az, rel=1e-15)
+        c = _taper_case(m.radius(z), flength=L)
+        assert _rel(t.linop(z), c.linop) < 1e-12, z
+        assert t.transform.aefffun(z) == pytest.approx(m.radius(z) ** 2 * m.aeff_intg, rel=1e-15)
+    # a narrower core has more waveguide dispersion and loss-free here: |L| grows along z
+    assert np.linalg.norm(t.linop(L)) > np.linalg.norm(t.linop(0.0))
+
+
 # ------------------------------------------------------------------ GPU
 _CASES = {
     "Ar-falling": dict(radius=125e-6, flength=0.3, gas="Ar", pressure=(2.0, 0.2), λ0=800e-9,
@@ -124,6 +162,16 @@ _CASES = {
     "Ne-multipoint": dict(radius=100e-6, flength=0.3, gas="Ne",
                           pressure=([0, 0.1, 0.2, 0.3], [0.5, 3.0, 3.0, 0.5]), λ0=800e-9,
                           τfwhm=10e-15, energy=150e-6, λlims=(150e-9, 4e-6), trange=0.25e-12),
+    # test_tapers.jl's linear taper (13 µm to 3/4 of it over 10 cm, Ar 5 bar, Kerr, no loss)
+    "Ar-taper": dict(radius=([0, 0.1], [13e-6, 9.75e-6]), flength=0.1, gas="Ar", pressure=5.0,
+                     λ0=800e-9, τfwhm=30e-15, energy=600e-9, λlims=(160e-9, 3000e-9),
+                     trange=0.5e-12, plasma=False, loss=False),
+    "He-taper-gradient": dict(radius=([0, 0.2], [100e-6, 60e-6]), flength=0.2, gas="He",
+                              pressure=(0.5, 3.0), λ0=800e-9, τfwhm=10e-15, energy=150e-6,
+                              λlims=(120e-9, 4e-6), trange=0.25e-12),
+    "Ne-taper-3node": dict(radius=([0, 0.05, 0.15], [120e-6, 80e-6, 80e-6]), flength=0.15,
+                           gas="Ne", pressure=2.0, λ0=800e-9, τfwhm=10e-15, energy=200e-6,
+                           λlims=(150e-9, 4e-6), trange=0.25e-12),
 }
 
 
@@ -158,13 +206,13 @@ def test_device_linop_is_bit_identical_to_host(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint"])
+@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "He-taper-gradient"])
 def test_gradient_rhs_matches_oracle(name):
     """(t::TransModeAvg)(nl, Eω, z) with densityfun(z) and βfun!(β, z) through the C ABI."""
     p = _case(name)
     rng = np.random.default_rng(7)
     Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
-    for z in (0.0, 0.07, 0.15, 0.3):
+    for z in (0.0, 0.07, 0.15, 0.2, 0.3):
         nl = np.zeros_like(Ew)
         p.transform(nl, Ew, z)
         ref = uppe.trans_mode_avg(p.transform, Ew, z)
@@ -238,13 +286,15 @@ def test_gradient_solve_mixed_spectral_error():
 
 
 @pytest.mark.gpu
-def test_gradient_step_stats_use_local_density():
-    """Stats.default with a gradient on the oracle's step sequence (replay): electrondensity is
-    the ionisation fraction x densityfun(z) (Stats.jl:228-257); the other keys as for a
-    constant fill."""
+@pytest.mark.parametrize("name", ["Ar-falling", "He-taper-gradient"])
+def test_gradient_step_stats_use_local_density(name):
+    """Stats.default with a gradient or taper on the oracle's step sequence (replay):
+    electrondensity is the ionisation fraction x densityfun(z) (Stats.jl:228-257), peak
+    intensity and the ionisation field scale use aeff(z); the other keys as for a constant
+    fill."""
     from luna_b200 import _lib
     from luna_b200 import plan as P
-    p = _case("Ar-falling", saveN=5)
+    p = _case(name, saveN=5)
     ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5, stats=True)
     replay = np.array(ores.steps_all, dtype=np.float64).ravel()
     r = P.solve_precon(p.transform, p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=5,

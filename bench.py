@@ -390,9 +390,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--instances", type=int, default=256)
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the CPU and plain-FP64 baselines (timing experiments)")
     ap.add_argument("--max-rk-steps", type=int, default=200000,
                     help="per-instance step budget (profiling aid; the scan needs < 30000)")
+    ap.add_argument("--no-dist", action="store_true",
+                    help="integrate every instance on one CTA or a Raman cluster (no distributed instances)")
+    ap.add_argument("--dist-min-no", type=int, default=0,
+                    help="oversampled length from which an instance runs distributed (0: library default)")
     ap.add_argument("--no-clusters", action="store_true",
                     help="integrate every instance on one CTA (profiling aid)")
     ap.add_argument("--workload", default="scan256", choices=["scan256", "radial"],
@@ -425,7 +430,9 @@ def main():
     plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
     # each instance saves on its own GridCondition range(0, zmax, 201) with max_dz = zmax/2
     batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps,
-                    flags=_lib.SOLVE_NO_CLUSTERS if args.no_clusters else 0)
+                    flags=(_lib.SOLVE_NO_CLUSTERS if args.no_clusters else 0) |
+                    (_lib.SOLVE_NO_DIST if args.no_dist else 0),
+                    dist_min_no=args.dist_min_no)
     zsaves = [np.linspace(0.0, p.grid.zmax, SAVEN) for p in probs]
     max_dts = [p.grid.zmax / 2 for p in probs]
     # pinned host buffers for the end-to-end path
@@ -522,7 +529,7 @@ def main():
                                 "busy_cta_s": float(np.sum(be[:, 1] - be[:, 0]))}
         except Exception as e:
             line["timeline"] = {"error": str(e)[:200]}
-        if world == 1 and args.instances == 256:
+        if world == 1 and args.instances == 256 and not args.no_cpu_baseline:
             try:
                 v0, per = plain_fp64_estimate(inst)
                 line["plain_fp64"] = {"value": v0, "unit": "sims/hour", "ms_per_rk_step": per,

@@ -106,6 +106,9 @@ typedef struct {
     long long nreplay;
     int flags;                                 /* LUNA_SOLVE_* bits, 0 for the defaults     */
     long long stats_cap;                       /* rows of per-step statistics; 0: off       */
+    int dist_min_no;                           /* batches (mixed precision): instances with at
+                                                  least this many oversampled samples run on a
+                                                  cluster of CTAs each; 0: 16384            */
 } luna_solve_opts;
 
 /* Per-step statistics (Stats.default, Stats.jl:495-532, for a mode-averaged field-resolved
@@ -115,8 +118,11 @@ typedef struct {
 #define LUNA_NSTATS 10
 
 /* luna_solve_opts.flags */
+#define LUNA_SOLVE_NO_DIST 2     /* batches: no distributed (multi-CTA) integration of the
+                                    long instances; a verification and timing aid          */
 #define LUNA_SOLVE_NO_CLUSTERS 1 /* batches: integrate every instance on one CTA (no Raman
-                                    clusters); a verification and timing aid            */
+                                    clusters, no distributed instances); a verification
+                                    and timing aid                                      */
 
 typedef struct {
     int status;

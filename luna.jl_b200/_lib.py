@@ -21,6 +21,7 @@ LUNA_ERR_UNSUPPORTED = 17
 LUNA_ERR_CUDA = 18
 NOALLOC_SCRATCH_BYTES = 1 << 20
 SOLVE_NO_CLUSTERS = 1
+SOLVE_NO_DIST = 2
 NSTATS = 10
 STATS_KEYS = ("z", "dz", "ω0", "energy", "peakpower", "peakintensity", "fwhm_t_min",
               "fwhm_t_max", "electrondensity", "peak_ionisation_rate")
@@ -79,7 +80,7 @@ class SolveOpts(ctypes.Structure):
                 ("max_dt", c_double), ("min_dt", c_double), ("repeat_limit", c_int),
                 ("max_steps", c_longlong), ("saveN", c_int), ("zsave", PD),
                 ("steplog_cap", c_longlong), ("replay", PD), ("nreplay", c_longlong),
-                ("flags", c_int), ("stats_cap", c_longlong)]
+                ("flags", c_int), ("stats_cap", c_longlong), ("dist_min_no", c_int)]
 
 
 class SolveStats(ctypes.Structure):

@@ -14,6 +14,7 @@
 #include <vector>
 
 #include "../../include/luna_b200.h"
+#include "dist.cuh"
 #include "radial.cuh"
 #include "tc_gemm.cuh"
 
@@ -290,6 +291,70 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
     }
 }
 
+// Persistent solver on clusters of DIST_R CTAs. Phase 1: each cluster integrates the
+// instances of `dl` (the long ones, in priority order) together, every CTA holding one
+// residue class of the frequency bins and one block of the time samples. Phase 2: once
+// `dl` is empty, every CTA integrates instances of `reg` on its own.
+template <typename Rl, typename Kt>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+solve_kernel_dist(LunaInst* insts, const int* dl, int nd, int* d_counter, const int* reg, int nreg,
+                  int* reg_counter, TwTab<Rl> tw, int smem_bytes) {
+    namespace cg = cooperative_groups;
+    extern __shared__ __align__(256) char smem[];
+    __shared__ Ctl ctl;
+    __shared__ int sidx;
+    cg::cluster_group cl = cg::this_cluster();
+    const int rank = (int)cl.block_rank();
+    while (true) {
+        if (rank == 0 && threadIdx.x == 0) sidx = atomicAdd(d_counter, 1);
+        cl.sync();
+        const int q = *cl.map_shared_rank(&sidx, 0);
+        cl.sync();  // rank 0's index is read everywhere before the next pull overwrites it
+        if (q >= nd) break;
+        LunaInst& I = insts[dl[q]];
+        if (rank == 0 && threadIdx.x == 0) {
+            unsigned long long t;
+            unsigned int sm;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+            I.t_begin = t;
+            I.sm = (int)sm;
+        }
+        DWs<Rl> d;
+        plan_dws<Rl>(I, smem, d, tw, rank);
+        solve_instance_dist<Rl, Kt>(I, d, ctl);
+        if (rank == 0 && threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            I.t_end = t;
+        }
+    }
+    while (true) {
+        __syncthreads();
+        if (threadIdx.x == 0) sidx = atomicAdd(reg_counter, 1);
+        __syncthreads();
+        const int q = sidx;
+        if (q >= nreg) break;
+        LunaInst& I = insts[reg[q]];
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            unsigned int sm;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(sm));
+            I.t_begin = t;
+            I.sm = (int)sm;
+        }
+        Ws<Rl> w;
+        plan_ws<Rl>(I, smem, smem_bytes, w, tw);
+        solve_instance<Rl, Kt>(I, w, ctl);
+        if (threadIdx.x == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            I.t_end = t;
+        }
+    }
+}
+
 // One right-hand-side evaluation nl = T(Eω) on one CTA (TransModeAvg call).
 template <typename Rl>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
@@ -489,6 +554,10 @@ struct luna_batch {
     cudaStream_t stream2 = nullptr;  // single-CTA solver beside the cluster solver
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf = nullptr, evj = nullptr;
     int reg_grid = 0;
+    // distributed instances (clusters of DIST_R CTAs per instance)
+    int ndist = 0, dist_grid = 0;
+    int* d_dist = nullptr;
+    std::vector<int> dist;
 };
 
 namespace {
@@ -940,7 +1009,70 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
     }
     if (occ < 1) return bail(fail(LUNA_ERR_CUDA, "batch_create: solver kernel does not fit on an SM"));
     b->grid = std::min(n, nsm * occ);
-    if (prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
+    if (prec == LUNA_PREC_MIXED && !(opts->flags & (LUNA_SOLVE_NO_CLUSTERS | LUNA_SOLVE_NO_DIST))) {
+        // distributed instances: the long ones (No >= LUNA_DIST_MIN_NO) that the cluster
+        // solver supports, each on DIST_R CTAs
+        const int maxs = max_smem_optin();
+        std::vector<int> dl, reg;
+        std::vector<double> cost(n);
+        size_t dsm = 0;
+        for (int i = 0; i < n; ++i) {
+            const LunaInst& I = b->h[i];
+            const int M = I.No / 2, Mc = I.N / 2;
+            const bool ok = I.kind == 0 && !I.grad && opts->stats_cap <= 0 && I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
+                            M % DIST_R == 0 && M / DIST_R >= 2 * LUNA_BLOCK &&
+                            M / DIST_R <= FftEmax<float>::v * LUNA_BLOCK && Mc % DIST_R == 0 &&
+                            Mc / DIST_R >= 64 && Mc <= M && I.Nw <= Mc + 1 &&
+                            dist_smem_bytes(I.No, sizeof(float2)) <= (size_t)maxs;
+            if (ok) {
+                dl.push_back(i);
+                dsm = std::max(dsm, dist_smem_bytes(I.No, sizeof(float2)));
+            } else {
+                reg.push_back(i);
+            }
+            cost[i] = (double)I.No * std::log2((double)I.No) * (has_raman(I) ? 2.0 : 1.0);
+        }
+        if (!dl.empty()) {
+            const int sm = (int)std::max<size_t>((size_t)b->smem, dsm);
+            if (cudaFuncSetAttribute(solve_kernel_dist<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
+                cudaFuncSetAttribute(solve_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
+                return bail(fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size (distributed solver)"));
+            cudaLaunchConfig_t cfg = {};
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeClusterDimension;
+            at[0].val.clusterDim.x = DIST_R;
+            at[0].val.clusterDim.y = 1;
+            at[0].val.clusterDim.z = 1;
+            cfg.gridDim = dim3(DIST_R * 32, 1, 1);
+            cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+            cfg.dynamicSmemBytes = sm;
+            cfg.attrs = at;
+            cfg.numAttrs = 1;
+            int ncl = 0;
+            if (cudaOccupancyMaxActiveClusters(&ncl, solve_kernel_dist<float, float>, &cfg) != cudaSuccess || ncl < 1) {
+                cudaGetLastError();
+                ncl = 0;
+            }
+            if (ncl >= 1) {
+                std::stable_sort(reg.begin(), reg.end(), [&](int a, int c) { return cost[a] > cost[c]; });
+                b->smem = sm;
+                b->dist = dl;
+                b->reg = reg;
+                b->ndist = (int)dl.size();
+                b->nreg = (int)reg.size();
+                ncl = std::min(ncl, (int)dl.size());
+                b->dist_grid = DIST_R * ncl;
+                b->reg_grid = std::max(0, std::min((int)reg.size(), nsm - b->dist_grid));
+                std::vector<int> regp(reg);
+                if (regp.empty()) regp.push_back(0);  // never read (nreg == 0)
+                if (upload(b->allocs, dl.data(), dl.size(), (const int**)&b->d_dist) ||
+                    upload(b->allocs, regp.data(), regp.size(), (const int**)&b->d_reg) ||
+                    dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
+                    return bail(LUNA_ERR_CUDA);
+            }
+        }
+    }
+    if (b->ndist == 0 && prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
         // Raman clusters for the instances whose Raman buffer alone overflows one CTA
         const int maxs = max_smem_optin();
         std::vector<int> big, reg;
@@ -1054,10 +1186,36 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
     // instances restart from y0: restore the per-instance pointers and counters
     CK(cudaMemcpyAsync(b->d_insts, b->h.data(), sizeof(LunaInst) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
-    if (b->cl_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
+    if (b->cl_grid > 0 || b->dist_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
     if (b->precision == LUNA_PREC_FP64) {
         solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem, nullptr);
+    } else if (b->dist_grid > 0) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = DIST_R;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(b->dist_grid, 1, 1);
+        cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+        cfg.dynamicSmemBytes = b->smem;
+        cfg.stream = b->stream;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int* c = b->d_cl_counters;
+        if (b->reg_grid > 0) {
+            CK(cudaEventRecord(b->evf, b->stream));
+            CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
+        }
+        CK(cudaLaunchKernelEx(&cfg, solve_kernel_dist<float, float>, b->d_insts, (const int*)b->d_dist, b->ndist, c,
+                              (const int*)b->d_reg, b->nreg, c + 1, tw.f, b->smem));
+        if (b->reg_grid > 0) {
+            solve_kernel<float, float><<<b->reg_grid, LUNA_BLOCK, b->smem, b->stream2>>>(
+                b->d_insts, b->nreg, c + 1, tw.f, b->smem, (const int*)b->d_reg);
+            CK(cudaEventRecord(b->evj, b->stream2));
+            CK(cudaStreamWaitEvent(b->stream, b->evj, 0));
+        }
     } else if (b->cl_grid > 0) {
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];
@@ -1128,7 +1286,12 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
 
 int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_instances, int* clusters) {
     if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_info: null batch");
-    if (kernels_per_run) *kernels_per_run = (b->cl_grid > 0) ? 1 + (b->reg_grid > 0) : 1;
+    if (kernels_per_run) *kernels_per_run = (b->cl_grid > 0 || b->dist_grid > 0) ? 1 + (b->reg_grid > 0) : 1;
+    if (b->dist_grid > 0) {
+        if (cluster_instances) *cluster_instances = b->ndist;
+        if (clusters) *clusters = b->dist_grid / DIST_R;
+        return LUNA_OK;
+    }
     if (cluster_instances) *cluster_instances = (b->cl_grid > 0) ? b->nbig : 0;
     if (clusters) *clusters = b->cl_grid / (CL_HELPERS + 1);
     return LUNA_OK;
@@ -1136,8 +1299,15 @@ int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_insta
 
 int luna_b200_batch_set_priority(luna_batch* b, const double* priority) {
     if (!b || !priority) return fail(LUNA_ERR_BAD_ARG, "batch_set_priority: null argument");
-    if (b->cl_grid == 0) return LUNA_OK;  // single list in index order
     auto by = [&](int a, int c) { return priority[a] > priority[c]; };
+    if (b->dist_grid > 0) {
+        std::stable_sort(b->dist.begin(), b->dist.end(), by);
+        std::stable_sort(b->reg.begin(), b->reg.end(), by);
+        CK(cudaMemcpy(b->d_dist, b->dist.data(), sizeof(int) * b->dist.size(), cudaMemcpyHostToDevice));
+        if (!b->reg.empty()) CK(cudaMemcpy(b->d_reg, b->reg.data(), sizeof(int) * b->reg.size(), cudaMemcpyHostToDevice));
+        return LUNA_OK;
+    }
+    if (b->cl_grid == 0) return LUNA_OK;  // single list in index order
     std::stable_sort(b->big.begin(), b->big.end(), by);
     std::stable_sort(b->reg.begin(), b->reg.end(), by);
     CK(cudaMemcpy(b->d_big, b->big.data(), sizeof(int) * b->big.size(), cudaMemcpyHostToDevice));

@@ -929,20 +929,21 @@ __device__ __forceinline__ cpx<double> inv_fac(cpx<Rl> f) {
 }
 
 // Dense output (RK45.jl:249-268) into row `out`; after an accepted step ks[1] holds k7,
-// so the k1 and k7 coefficients both apply to that buffer.
+// so the k1 and k7 coefficients both apply to that buffer. Bins r0, r0 + rs, r0 + 2 rs, ...
+// (all bins by default; one residue class per CTA of a distributed instance).
 template <typename Rl, typename Kt>
 __device__ void interpolate_row(int Nw, const double2* linop, const Ctl& c, double ti, void* const* k,
-                                const double2* py, const double2* pyn, double2* out) {
+                                const double2* py, const double2* pyn, double2* out, int r0 = 0, int rs = 1) {
     const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
     const cpx<double>* yn = reinterpret_cast<const cpx<double>*>(pyn);
     const cpx<double>* L = reinterpret_cast<const cpx<double>*>(linop);
     cpx<double>* o = reinterpret_cast<cpx<double>*>(out);
     if (ti == c.t) {
-        for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) o[i] = y[i];
+        for (int i = r0 + rs * threadIdx.x; i < Nw; i += rs * LUNA_BLOCK) o[i] = y[i];
         return;
     }
     if (ti == c.tn) {
-        for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) o[i] = yn[i];
+        for (int i = r0 + rs * threadIdx.x; i < Nw; i += rs * LUNA_BLOCK) o[i] = yn[i];
         return;
     }
     const double s = (ti - c.t) / c.dt;
@@ -956,7 +957,7 @@ __device__ void interpolate_row(int Nw, const double2* linop, const Ctl& c, doub
         b[j] = acc;
     }
     const double d = ti - c.t;
-    for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) {
+    for (int i = r0 + rs * threadIdx.x; i < Nw; i += rs * LUNA_BLOCK) {
         cpx<double> yi = mk<double>(0, 0);
         cpx<double> k1 = KT<Kt>::ld(k[0], i);
         yi = yi + scale(b[0], k1);
@@ -1281,7 +1282,8 @@ __device__ __noinline__ void step_stats(const LunaInst& I, Ws<Rl>& w, const doub
 // Weak error norm, PI step control, step limits and step bookkeeping after the stage
 // evaluations (RK45.jl:167-192, 343-354, 374-406); one thread. sy, syn and se are the
 // sums of |y|^2, |yn|^2 and |yerr|^2; flags are the status bits raised by the RHS.
-__device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, double syn, double se, int flags) {
+__device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, double syn, double se, int flags,
+                                             bool writer = true) {
     const double errwt = fmax(fmax(sqrt(sy), sqrt(syn)), I.atol);
     const double err = sqrt(se) / I.rtol / errwt;
     c.err = err;
@@ -1312,7 +1314,7 @@ __device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, dou
     if (ok) c.tn = c.t + c.dt;
     c.steps += 1;
     const long long si = c.steps - 1;
-    if (I.steplog && si < I.steplog_cap) {
+    if (writer && I.steplog && si < I.steplog_cap) {
         I.steplog[4 * si + 0] = c.t;
         I.steplog[4 * si + 1] = c.dt;
         I.steplog[4 * si + 2] = err;
@@ -1320,10 +1322,10 @@ __device__ __forceinline__ void control_step(LunaInst& I, Ctl& c, double sy, dou
     }
     if (ok) {
         c.repeated = 0;
-        I.accepted += 1;
+        if (writer) I.accepted += 1;
     } else {
         c.repeated += 1;
-        I.rejected += 1;
+        if (writer) I.rejected += 1;
         if (c.repeated > I.repeat_limit) {
             c.status = ST_REPEAT_LIMIT;
             c.done = 1;

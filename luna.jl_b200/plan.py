@@ -149,10 +149,12 @@ class Plan:
 
 
 def make_opts(saveN, zsave, rtol=1e-6, atol=1e-10, safety=0.9, max_dt=math.inf, min_dt=0.0,
-              repeat_limit=10, max_steps=200000, steplog_cap=0, replay=None, flags=0, stats_cap=0):
+              repeat_limit=10, max_steps=200000, steplog_cap=0, replay=None, flags=0, stats_cap=0,
+              dist_min_no=0):
     o = _lib.SolveOpts()
     o.flags = flags
     o.stats_cap = stats_cap
+    o.dist_min_no = dist_min_no
     if replay is not None:
         o.replay = _lib.dptr(replay)
         o.nreplay = len(replay) // 2

@@ -70,7 +70,7 @@ int main(void) {
     P(luna_solve_opts, replay); P(luna_solve_opts, nreplay); P(luna_solve_opts, flags);
     P(luna_radial_desc, Mf); P(luna_radial_desc, outfac);
     P(luna_grid_desc, omega); P(luna_grid_desc, escale); P(luna_solve_opts, stats_cap);
-    P(luna_solve_stats, nstats);
+    P(luna_solve_stats, nstats); P(luna_solve_opts, dist_min_no);
     P(luna_solve_stats, z); P(luna_solve_stats, dz);
     printf("luna_gradient_desc %zu\n", sizeof(luna_gradient_desc));
     P(luna_gradient_desc, Z); P(luna_gradient_desc, P2); P(luna_gradient_desc, dens_b);
@@ -106,6 +106,7 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_grid_desc.omega"]) == _lib.GridDesc.omega.offset
     assert int(out["luna_grid_desc.escale"]) == _lib.GridDesc.escale.offset
     assert int(out["luna_solve_opts.stats_cap"]) == _lib.SolveOpts.stats_cap.offset
+    assert int(out["luna_solve_opts.dist_min_no"]) == _lib.SolveOpts.dist_min_no.offset
     assert int(out["luna_solve_stats.nstats"]) == _lib.SolveStats.nstats.offset
     for f in ("Mf", "outfac"):
         assert int(out[f"luna_radial_desc.{f}"]) == getattr(_lib.RadialDesc, f).offset

@@ -555,9 +555,10 @@ struct luna_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf = nullptr, evj = nullptr;
     int reg_grid = 0;
     // distributed instances (clusters of DIST_R CTAs per instance)
-    int ndist = 0, dist_grid = 0;
+    int ndist = 0, dist_grid = 0, ncl_max = 0, nsm = 0;
     int* d_dist = nullptr;
-    std::vector<int> dist;
+    std::vector<int> dist, elig;
+    std::vector<char> big_raman;
 };
 
 namespace {
@@ -584,6 +585,34 @@ int upload(std::vector<void*>& allocs, const T* src, size_t n, const T** dst) {
 void free_all(std::vector<void*>& allocs) {
     for (void* p : allocs) cudaFree(p);
     allocs.clear();
+}
+
+// Which instances of a batch run distributed, from per-instance work estimates: the eligible
+// ones whose estimate is at least the mean load of an SM (total / SMs), the long poles of the
+// batch, and every eligible instance whose Raman buffers overflow one CTA; at most half of
+// the SMs start as clusters while single-CTA instances remain. Both lists in priority order.
+int dist_partition(luna_batch* b, const double* pr) {
+    const int n = b->n;
+    double W = 0;
+    for (int i = 0; i < n; ++i) W += pr[i];
+    const double thr = W / std::max(1, b->nsm);
+    std::vector<char> isd(n, 0);
+    for (int i : b->elig) isd[i] = (pr[i] >= thr) || b->big_raman[i];
+    b->dist.clear();
+    b->reg.clear();
+    for (int i = 0; i < n; ++i) (isd[i] ? b->dist : b->reg).push_back(i);
+    auto by = [&](int a, int c) { return pr[a] > pr[c]; };
+    std::stable_sort(b->dist.begin(), b->dist.end(), by);
+    std::stable_sort(b->reg.begin(), b->reg.end(), by);
+    b->ndist = (int)b->dist.size();
+    b->nreg = (int)b->reg.size();
+    int ncl = std::min(b->ncl_max, b->ndist);
+    if (b->nreg > 0) ncl = std::min(ncl, std::max(1, b->ncl_max / 2));
+    b->dist_grid = (b->ndist > 0) ? DIST_R * ncl : 0;
+    b->reg_grid = std::max(0, std::min(b->nreg, b->nsm - b->dist_grid));
+    if (b->ndist > 0) CK(cudaMemcpy(b->d_dist, b->dist.data(), sizeof(int) * b->ndist, cudaMemcpyHostToDevice));
+    if (b->nreg > 0) CK(cudaMemcpy(b->d_reg, b->reg.data(), sizeof(int) * b->nreg, cudaMemcpyHostToDevice));
+    return LUNA_OK;
 }
 
 }  // namespace
@@ -1054,21 +1083,20 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
                 ncl = 0;
             }
             if (ncl >= 1) {
-                std::stable_sort(reg.begin(), reg.end(), [&](int a, int c) { return cost[a] > cost[c]; });
                 b->smem = sm;
-                b->dist = dl;
-                b->reg = reg;
-                b->ndist = (int)dl.size();
-                b->nreg = (int)reg.size();
-                ncl = std::min(ncl, (int)dl.size());
-                b->dist_grid = DIST_R * ncl;
-                b->reg_grid = std::max(0, std::min((int)reg.size(), nsm - b->dist_grid));
-                std::vector<int> regp(reg);
-                if (regp.empty()) regp.push_back(0);  // never read (nreg == 0)
-                if (upload(b->allocs, dl.data(), dl.size(), (const int**)&b->d_dist) ||
-                    upload(b->allocs, regp.data(), regp.size(), (const int**)&b->d_reg) ||
+                b->elig = dl;
+                b->ncl_max = ncl;
+                b->nsm = nsm;
+                b->big_raman.assign(n, 0);
+                for (int i : dl) {
+                    const LunaInst& I = b->h[i];
+                    b->big_raman[i] = has_raman(I) && smem_wanted<float>(I) > (size_t)maxs;
+                }
+                if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_reg, sizeof(int) * n) ||
                     dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
                     return bail(LUNA_ERR_CUDA);
+                std::vector<double> pr(cost);
+                if (int rc = dist_partition(b, pr.data())) return bail(rc);
             }
         }
     }
@@ -1300,13 +1328,7 @@ int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_insta
 int luna_b200_batch_set_priority(luna_batch* b, const double* priority) {
     if (!b || !priority) return fail(LUNA_ERR_BAD_ARG, "batch_set_priority: null argument");
     auto by = [&](int a, int c) { return priority[a] > priority[c]; };
-    if (b->dist_grid > 0) {
-        std::stable_sort(b->dist.begin(), b->dist.end(), by);
-        std::stable_sort(b->reg.begin(), b->reg.end(), by);
-        CK(cudaMemcpy(b->d_dist, b->dist.data(), sizeof(int) * b->dist.size(), cudaMemcpyHostToDevice));
-        if (!b->reg.empty()) CK(cudaMemcpy(b->d_reg, b->reg.data(), sizeof(int) * b->reg.size(), cudaMemcpyHostToDevice));
-        return LUNA_OK;
-    }
+    if (!b->elig.empty()) return dist_partition(b, priority);
     if (b->cl_grid == 0) return LUNA_OK;  // single list in index order
     std::stable_sort(b->big.begin(), b->big.end(), by);
     std::stable_sort(b->reg.begin(), b->reg.end(), by);

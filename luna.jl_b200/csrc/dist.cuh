@@ -107,10 +107,19 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
     const int R = DIST_R, p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mbc = Mc / R;
     const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<DIST_R>();
-    for (int j = tid; p + R * j <= Mc; j += T) {
-        const int n = p + R * j;
-        const cpx<double> X = (n < Nw) ? load(n) : mk<double>(0, 0);
-        d.stg[Swz<Rl>::f(j)] = cvt<Rl>(X);
+    // DUNR own bins per thread and round: their loads are independent and issued together
+    for (int j0 = tid; p + R * j0 <= Mc; j0 += DUNR * T) {
+        cpx<double> X[DUNR];
+#pragma unroll
+        for (int u = 0; u < DUNR; ++u) {
+            const int n = p + R * (j0 + u * T);
+            X[u] = (n < Nw) ? load(n) : mk<double>(0, 0);
+        }
+#pragma unroll
+        for (int u = 0; u < DUNR; ++u) {
+            const int j = j0 + u * T;
+            if (p + R * j <= Mc) d.stg[Swz<Rl>::f(j)] = cvt<Rl>(X[u]);
+        }
     }
     dsync();
     const int po = (R - p) % R;
@@ -718,11 +727,21 @@ __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c
             const double zs = __dadd_rn(t0, __dmul_rn(c_nodes[s], dt));
             const double dd = __dsub_rn(zs, t0);
             if (s != 5) {
-                for (int t = tid; own(t) < Nw; t += T) {
-                    const int i = own(t);
-                    const cpx<Rl> f = expLd<Rl>(L[i], dd);
-                    d.ef[Swz<Rl>::f(t)] = f;
-                    if (s == 4) e1[i] = cvt<double>(f);
+                for (int t0 = tid; own(t0) < Nw; t0 += DUNR * T) {
+                    cpx<double> Lv[DUNR];
+#pragma unroll
+                    for (int u = 0; u < DUNR; ++u) {
+                        const int i = own(t0 + u * T);
+                        Lv[u] = (i < Nw) ? ldg(L + i) : mk<double>(0, 0);
+                    }
+#pragma unroll
+                    for (int u = 0; u < DUNR; ++u) {
+                        const int t = t0 + u * T, i = own(t);
+                        if (i >= Nw) continue;
+                        const cpx<Rl> f = expLd<Rl>(Lv[u], dd);
+                        d.ef[Swz<Rl>::f(t)] = f;
+                        if (s == 4) e1[i] = cvt<double>(f);
+                    }
                 }
             }
             __syncthreads();

@@ -40,7 +40,7 @@ from luna_b200 import _lib, scan  # noqa: E402
 from luna_b200 import plan as P  # noqa: E402
 
 METRIC = "capillary UPPE sims/hour/GPU, mixed+batched vs plain FP64 at ≤1e-3 spec. err"
-WORKLOAD = "scan256: 256 mode-averaged capillary instances (He/Ne/Ar/H2, PPT/ADK plasma, Raman for H2), mixed precision, persistent launches (single-CTA solver + 4-CTA response clusters)"
+WORKLOAD = "scan256: 256 mode-averaged capillary instances (He/Ne/Ar/H2, PPT/ADK plasma, Raman for H2), mixed precision, persistent launches (long instances distributed over 4-CTA clusters + single-CTA solver)"
 SAVEN = 201
 STEPS_FILE = os.path.join(ROOT, "oracle", "scan256_nrhs.json")
 

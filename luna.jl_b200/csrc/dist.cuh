@@ -309,8 +309,7 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
       }
     }
     __syncthreads();
-    sub_fft_any<Rl, false>(d.rb0, Mb, d.tw);
-    sub_fft_any<Rl, false>(d.rb1, Mb, d.tw);
+    sub_fft2<Rl, false, 8>(d.rb0, d.rb1, Mb, d.tw);
     // pairs (f, Mr - f) with f = 2R k + p; Zk/Zm are entries of the complex transform
     const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(rr.H);
     auto pair = [&](int f, cpx<Rl>* bk, int ik, cpx<Rl>* bm, int im) {
@@ -348,8 +347,7 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
         for (int k = tid; k < Mb; k += T) pair(2 * R * k + c, d.rb0, k, d.rb1, Mb - 1 - k);
     }
     __syncthreads();
-    sub_fft_any<Rl, true>(d.rb0, Mb, d.tw);
-    sub_fft_any<Rl, true>(d.rb1, Mb, d.tw);
+    sub_fft2<Rl, true, 8>(d.rb0, d.rb1, Mb, d.tw);
     for (int n1 = tid; n1 < Mb; n1 += T) {
         const int pos = Swz<Rl>::f(n1);
         if (pa) d.rb0[pos] = d.rb0[pos] * tw_pow<Rl, true>(d.tw, (unsigned)(pa * n1), lgMr);

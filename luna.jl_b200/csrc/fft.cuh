@@ -181,6 +181,70 @@ __device__ __forceinline__ void sub_fft(cpx<R>* buf, int Mb, const TwTab<R>& tw)
     }
 }
 
+// The same transform of two buffers at once: one pass processes both, so the two
+// transforms share their barriers and twiddles (E/RAD butterflies per buffer and thread).
+template <typename R, bool INV, int E, int RAD>
+__device__ __forceinline__ void pass_inplace2(cpx<R>* ba, cpx<R>* bb, int Mb, int L, int nact, const TwTab<R>& tw) {
+    const int t = threadIdx.x;
+    constexpr int NB = E / RAD;
+    cpx<R> va[E], vb[E];
+    const int stride = Mb / RAD;
+    if (t < nact) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + b * nact;
+#pragma unroll
+            for (int i = 0; i < RAD; ++i) {
+                const int a = Swz<R>::f(j + bitrev<RAD>(i) * stride);
+                va[b * RAD + i] = ba[a];
+                vb[b * RAD + i] = bb[a];
+            }
+        }
+    }
+    __syncthreads();
+    if (t < nact) {
+        const int shift = TW_LOG_MMAX - ilog2i((unsigned)(L * RAD));
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const int j = t + b * nact;
+            const int k = j & (L - 1);
+            if (L > 1) {
+                const cpx<R> w = twiddle<R, INV>(tw, (unsigned)k << shift);
+                apply_twiddles<R, RAD>(&va[b * RAD], w);
+                apply_twiddles<R, RAD>(&vb[b * RAD], w);
+            }
+            dft_br<R, INV, RAD>(&va[b * RAD]);
+            dft_br<R, INV, RAD>(&vb[b * RAD]);
+            const int base = (j - k) * RAD + k;
+#pragma unroll
+            for (int r = 0; r < RAD; ++r) {
+                const int a = Swz<R>::f(base + r * L);
+                ba[a] = va[b * RAD + r];
+                bb[a] = vb[b * RAD + r];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R, bool INV, int E>
+__device__ __forceinline__ void sub_fft2(cpx<R>* ba, cpx<R>* bb, int Mb, const TwTab<R>& tw) {
+    constexpr int LR = ilog2c<E>();
+    const int nact = Mb / E;
+    const int rem = ilog2i((unsigned)Mb) % LR;
+    int L = 1;
+    if (rem != 0) {
+        const int r0 = 1 << rem;
+        if constexpr (E > 2) { if (r0 == 2) pass_inplace2<R, INV, E, 2>(ba, bb, Mb, 1, nact, tw); }
+        if constexpr (E > 4) { if (r0 == 4) pass_inplace2<R, INV, E, 4>(ba, bb, Mb, 1, nact, tw); }
+        L = r0;
+    }
+    while (L < Mb) {
+        pass_inplace2<R, INV, E, E>(ba, bb, Mb, L, nact, tw);
+        L *= E;
+    }
+}
+
 // Radix-P pass joining the sub-transforms, in place (each thread owns the P elements
 // k + q*Mb). DIT (forward): X[k + q*Mb] = sum_p W_P^{pq} * (W_M^{pk} * A_p[k]).
 // DIF (inverse):           b_p[k] = W_M^{-pk} * sum_q W_P^{-pq} * x[k + q*Mb].

@@ -25,8 +25,11 @@
 
 namespace luna {
 
-#define DIST_R 4
-#define DUNR 4  // elements per thread whose remote loads are issued together
+#ifndef DIST_R
+#define DIST_R 8
+#endif
+#define DUNR (16 / DIST_R)  // elements per thread whose remote loads are issued together
+#define DUNR_RAMAN (8 / DIST_R > 0 ? 8 / DIST_R : 1)
 
 namespace dcg = cooperative_groups;
 
@@ -377,10 +380,11 @@ struct RamanOut {
     // P for the pairs n1 = tid + k T of this CTA's block into out[Swz(n1)] (remote loads of
     // two pairs in flight together)
     __device__ void block(cpx<Rl>* out, int Mb) const {
-        for (int n0 = threadIdx.x; n0 < Mb; n0 += 2 * LUNA_BLOCK) {
-            cpx<Rl> v0[2][DIST_R], v1[2][DIST_R];
+        constexpr int U = DUNR_RAMAN;
+        for (int n0 = threadIdx.x; n0 < Mb; n0 += U * LUNA_BLOCK) {
+            cpx<Rl> v0[U][DIST_R], v1[U][DIST_R];
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int pos = Swz<Rl>::f(min(n0 + u * LUNA_BLOCK, Mb - 1));
 #pragma unroll
                 for (int c = 0; c < DIST_R; ++c) {
@@ -389,7 +393,7 @@ struct RamanOut {
                 }
             }
 #pragma unroll
-            for (int u = 0; u < 2; ++u) {
+            for (int u = 0; u < U; ++u) {
                 const int n1 = n0 + u * LUNA_BLOCK;
                 if (n1 >= Mb) continue;
                 cpx<Rl> acc = v0[u][0] + v1[u][0] * w1[0];

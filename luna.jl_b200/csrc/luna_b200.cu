@@ -589,8 +589,9 @@ void free_all(std::vector<void*>& allocs) {
 
 // Which instances of a batch run distributed, from per-instance work estimates: the eligible
 // ones whose estimate is at least the mean load of an SM (total / SMs), the long poles of the
-// batch, and every eligible instance whose Raman buffers overflow one CTA; at most half of
-// the SMs start as clusters while single-CTA instances remain. Both lists in priority order.
+// batch, and every eligible instance whose Raman buffers overflow one CTA. Every SM that can
+// hold a cluster starts as one (longest instances first); the single-CTA instances fill the
+// SMs left over and the clusters once their list is empty. Both lists in priority order.
 int dist_partition(luna_batch* b, const double* pr) {
     const int n = b->n;
     double W = 0;
@@ -606,8 +607,7 @@ int dist_partition(luna_batch* b, const double* pr) {
     std::stable_sort(b->reg.begin(), b->reg.end(), by);
     b->ndist = (int)b->dist.size();
     b->nreg = (int)b->reg.size();
-    int ncl = std::min(b->ncl_max, b->ndist);
-    if (b->nreg > 0) ncl = std::min(ncl, std::max(1, b->ncl_max / 2));
+    const int ncl = std::min(b->ncl_max, b->ndist);
     b->dist_grid = (b->ndist > 0) ? DIST_R * ncl : 0;
     b->reg_grid = std::max(0, std::min(b->nreg, b->nsm - b->dist_grid));
     if (b->ndist > 0) CK(cudaMemcpy(b->d_dist, b->dist.data(), sizeof(int) * b->ndist, cudaMemcpyHostToDevice));

@@ -1,7 +1,7 @@
 """Distributed integration of one instance on a cluster of CTAs (mixed precision).
 
 The cluster solver splits the frequency bins, the time samples, the transforms, the plasma
-integrals and the Raman convolution of one instance over four CTAs; it must give the fields
+integrals and the Raman convolution of one instance over eight CTAs; it must give the fields
 of the single-CTA solver (the same accepted steps, agreement at FP32 rounding) and stay
 within the mixed-precision bar (1e-3 relative spectral L2) of the FP64 oracle.
 """
@@ -24,13 +24,13 @@ def _rel(a, b):
 
 
 def _case(gas, trange, plasma=None, energy=100e-6, flength=0.2):
-    # λlims (150 nm, 4 µm): trange 0.5 ps gives No = 8192, 1 ps No = 16384
+    # λlims (150 nm, 4 µm): trange 0.5 ps gives No = 8192, 1 ps 16384, 2 ps 32768
     return prop_capillary_args(125e-6, flength, gas, 1.0, λ0=800e-9, τfwhm=10e-15,
                                energy=energy, λlims=(150e-9, 4e-6), trange=trange,
                                plasma=plasma, saveN=11)
 
 
-def _batch(probs, flags=0, dist_min_no=8192, priority=None):
+def _batch(probs, flags=0, dist_min_no=16384, priority=None):
     from luna_b200 import plan as P
     plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
     b = P.Batch(plans, 11, np.linspace(0.0, 1.0, 11), flags=flags, dist_min_no=dist_min_no)
@@ -45,11 +45,11 @@ def _batch(probs, flags=0, dist_min_no=8192, priority=None):
     return b.results(), info
 
 
-@pytest.mark.parametrize("gas,trange,plasma", [("He", 0.5e-12, False), ("Ar", 0.5e-12, None),
-                                               ("H2", 0.5e-12, None), ("H2", 1e-12, None)])
-def test_distributed_matches_single_cta(gas, trange, plasma):
-    """Kerr only, Kerr + PPT plasma, Kerr + ADK plasma + Raman (No = 8192 and 16384)."""
-    p = _case(gas, trange, plasma)
+@pytest.mark.parametrize("gas,trange,plasma,flength", [("He", 1e-12, False, 0.2), ("Ar", 1e-12, None, 0.2),
+                                                       ("H2", 1e-12, None, 0.2), ("H2", 2e-12, None, 0.05)])
+def test_distributed_matches_single_cta(gas, trange, plasma, flength):
+    """Kerr only, Kerr + PPT plasma, Kerr + ADK plasma + Raman (No = 16384 and 32768)."""
+    p = _case(gas, trange, plasma, flength=flength)
     (rd,), info = _batch([p])
     assert info[1] == 1  # the instance ran on a cluster
     (rs,), info0 = _batch([p], flags=_lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS)
@@ -62,7 +62,7 @@ def test_distributed_matches_single_cta(gas, trange, plasma):
 
 
 def test_distributed_within_mixed_bar_of_oracle():
-    p = _case("Ar", 0.5e-12)
+    p = _case("Ar", 1e-12, flength=0.1)
     ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
     (rd,), info = _batch([p])
     assert info[1] == 1 and rd.status == 0
@@ -73,9 +73,9 @@ def test_distributed_within_mixed_bar_of_oracle():
 def test_mixed_batch_of_distributed_and_single_instances():
     """A batch where some instances run on clusters and the rest on single CTAs: every
     instance gives its own single-CTA result."""
-    probs = [_case("He", 0.25e-12), _case("Ar", 0.5e-12), _case("He", 0.5e-12, plasma=False),
-             _case("Ar", 0.25e-12)]
-    # the two No = 8192 instances are eligible; a high priority marks the long one
+    probs = [_case("He", 0.25e-12), _case("Ar", 1e-12, flength=0.1), _case("He", 1e-12, plasma=False),
+             _case("Ar", 0.5e-12)]
+    # the two No = 16384 instances are eligible; a high priority marks the long one
     res, info = _batch(probs, priority=[1.0, 10.0, 5.0, 1.0])
     assert info[1] >= 1
     ref, _ = _batch(probs, flags=_lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS)

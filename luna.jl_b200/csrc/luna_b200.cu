@@ -588,17 +588,18 @@ void free_all(std::vector<void*>& allocs) {
 }
 
 // Which instances of a batch run distributed, from per-instance work estimates: the eligible
-// ones whose estimate is at least the mean load of an SM (total / SMs), the long poles of the
-// batch, and every eligible instance whose Raman buffers overflow one CTA. Every SM that can
-// hold a cluster starts as one (longest instances first); the single-CTA instances fill the
-// SMs left over and the clusters once their list is empty. Both lists in priority order.
+// ones whose estimate is at least the mean load of an SM (total / SMs), i.e. the long poles
+// of the batch (a cluster costs more SM time than one CTA; shorter Raman instances whose
+// buffers overflow one CTA run single with them in global memory). Every SM that can hold a
+// cluster starts as one (longest instances first); the single-CTA instances fill the SMs
+// left over and the clusters once their list is empty. Both lists in priority order.
 int dist_partition(luna_batch* b, const double* pr) {
     const int n = b->n;
     double W = 0;
     for (int i = 0; i < n; ++i) W += pr[i];
     const double thr = W / std::max(1, b->nsm);
     std::vector<char> isd(n, 0);
-    for (int i : b->elig) isd[i] = (pr[i] >= thr) || b->big_raman[i];
+    for (int i : b->elig) isd[i] = pr[i] >= thr;
     b->dist.clear();
     b->reg.clear();
     for (int i = 0; i < n; ++i) (isd[i] ? b->dist : b->reg).push_back(i);
@@ -1100,7 +1101,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
             }
         }
     }
-    if (b->ndist == 0 && prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
+    if (b->elig.empty() && prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
         // Raman clusters for the instances whose Raman buffer alone overflows one CTA
         const int maxs = max_smem_optin();
         std::vector<int> big, reg;

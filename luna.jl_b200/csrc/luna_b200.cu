@@ -558,7 +558,6 @@ struct luna_batch {
     int ndist = 0, dist_grid = 0, ncl_max = 0, nsm = 0;
     int* d_dist = nullptr;
     std::vector<int> dist, elig;
-    std::vector<char> big_raman;
 };
 
 namespace {
@@ -1088,11 +1087,6 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
                 b->elig = dl;
                 b->ncl_max = ncl;
                 b->nsm = nsm;
-                b->big_raman.assign(n, 0);
-                for (int i : dl) {
-                    const LunaInst& I = b->h[i];
-                    b->big_raman[i] = has_raman(I) && smem_wanted<float>(I) > (size_t)maxs;
-                }
                 if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_reg, sizeof(int) * n) ||
                     dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
                     return bail(LUNA_ERR_CUDA);

@@ -3,9 +3,9 @@
 
 Workload: the seeded 256-instance mode-averaged capillary scan (energy 50-400 uJ, 0.5-5 bar,
 He/Ne/Ar/H2, core radius 75-150 um, 8-30 fs, 1-3 m, uneven grids No = 8192..32768),
-integrated to completion in mixed precision by persistent launches: a single-CTA solver,
-and 4-CTA response clusters for the instances whose Raman buffer overflows one CTA's
-shared memory, running concurrently. One bench step = one full scan. Metric: simulations
+integrated to completion in mixed precision by persistent launches: the long instances
+distributed over 8-CTA clusters (one instance per cluster) and a single-CTA solver for the
+rest, running concurrently. One bench step = one full scan. Metric: simulations
 per hour per GPU (completed instances / step time).
 
   value   device time of the solver launches, inputs already resident in HBM (CUDA events)
@@ -40,7 +40,7 @@ from luna_b200 import _lib, scan  # noqa: E402
 from luna_b200 import plan as P  # noqa: E402
 
 METRIC = "capillary UPPE sims/hour/GPU, mixed+batched vs plain FP64 at ≤1e-3 spec. err"
-WORKLOAD = "scan256: 256 mode-averaged capillary instances (He/Ne/Ar/H2, PPT/ADK plasma, Raman for H2), mixed precision, persistent launches (long instances distributed over 4-CTA clusters + single-CTA solver)"
+WORKLOAD = "scan256: 256 mode-averaged capillary instances (He/Ne/Ar/H2, PPT/ADK plasma, Raman for H2), mixed precision, persistent launches (long instances distributed over 8-CTA clusters + single-CTA solver)"
 SAVEN = 201
 STEPS_FILE = os.path.join(ROOT, "oracle", "scan256_nrhs.json")
 
@@ -515,7 +515,7 @@ def main():
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e * 1e3},
                 "gpu_launches": args.steps * kinfo[0],
                 "scheduling": {"kernels_per_step": kinfo[0], "cluster_instances": kinfo[1],
-                               "clusters_of_4_ctas": kinfo[2]},
+                               "clusters": kinfo[2]},
                 "rk_steps_per_scan": steps_all, "rhs_evals_per_s": nrhs_all / (ms / 1e3),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic,

@@ -286,6 +286,52 @@ int luna_b200_radial_solve(luna_radial_plan* plan, const double* linop, double* 
                            double dz0, double zmax, const luna_solve_opts* opts, double* saves,
                            double* steplog, luna_solve_stats* stats);
 
+/* ---------------------------------------------------------------- modal transform
+ * TransModal with full=false (NonlinearRHS.jl:148-302, built by Luna.setup for modes,
+ * Luna.jl:173-199) on a field-resolved grid: nmodes capillary modes sharing the polar
+ * limits (0, a), npol polarisation components (Modes.ToSpace, Modes.jl:411-442), the
+ * radial integral of the projected polarisation by the p-adaptive Clenshaw-Curtis rule of
+ * Cubature.pcubature_v (NonlinearRHS.jl:294-298) with the L2 error norm. Level l of the rule
+ * has 2^(l+1)+1 points on [0, a]; the end points contribute nothing, the other points are
+ * numbered in evaluation order ("slots": slot 0 the centre, then the 2^l points each level
+ * l >= 1 adds), nslots = 2^nlevels - 1. Level l is accepted when the L2 norm of its
+ * difference from level l-1 (level -1: the midpoint rule) is <= atol or <= rtol times its
+ * own L2 norm, or when it is the last level (the evaluation limit mfcn). Fields are
+ * column-major Nw x nmodes complex arrays (Julia's Matrix{ComplexF64}). */
+#define LUNA_MODAL_MAX_MODES 16
+#define LUNA_MODAL_MAX_LEVELS 9
+typedef struct {
+    int nmodes;            /* modes (columns of Eω), 1..LUNA_MODAL_MAX_MODES               */
+    int npol;              /* 1 (components :x or :y) or 2 (:xy; Kerr response only)      */
+    int nlevels;           /* cubature levels 0..nlevels-1, 1..LUNA_MODAL_MAX_LEVELS        */
+    const double* ems;     /* [nslots*nmodes*npol] Exy(mode, (r_s, 0))[component] at slot s */
+    const double* wts;     /* [nlevels*nslots] weight of slot s in level l's rule, 2πr_s and
+                              the half-width a/2 included (0 for slots beyond level l)     */
+    double wlow;           /* weight of slot 0 in the midpoint rule (level 0's comparison) */
+    double rtol, atol;     /* pcubature reltol and abstol                                  */
+    const double* outfac;  /* [2*Nw*nmodes] crop scale x ωwin x norm! per mode column     */
+} luna_modal_desc;
+
+typedef struct luna_modal_plan luna_modal_plan;
+
+/* Replaces the TransModal constructor (NonlinearRHS.jl:203-216). The grid descriptor is
+ * that of one point (kind 0; its outfac is ignored, in_scale = pad scale / No); responses
+ * as for luna_b200_plan_create (no Raman; with npol = 2 only Kerr). */
+int luna_b200_modal_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
+                                const luna_modal_desc* modal, int precision, luna_modal_plan** out);
+void luna_b200_modal_plan_destroy(luna_modal_plan* plan);
+/* (t::TransModal)(nl, Eω, z) — NonlinearRHS.jl:284-302. Host arrays of Nw*nmodes complex;
+ * nevals (may be NULL) receives the integrand evaluations the cubature took. */
+int luna_b200_modal_rhs(luna_modal_plan* plan, double* nl, const double* Ew, double z, int* nevals);
+int luna_b200_modal_rhs_device(luna_modal_plan* plan, double* nl_dev, const double* Ew_dev, double z,
+                               void* stream);
+/* RK45.solve_precon driven by Luna.run (Luna.jl:358-391) for a modal problem: linop and
+ * y_inout are Nw*nmodes complex (LinearOps.make_const_linop(grid, modes, λ0),
+ * LinearOps.jl:401-415), saves [saveN*2*Nw*nmodes] doubles, steplog as for luna_b200_solve. */
+int luna_b200_modal_solve(luna_modal_plan* plan, const double* linop, double* y_inout, double z0,
+                          double dz0, double zmax, const luna_solve_opts* opts, double* saves,
+                          double* steplog, luna_solve_stats* stats);
+
 /* Allocation-free variant of luna_b200_rhs_device. It has no counterpart in the reference:
  * it serves host programs that must not allocate device memory while they run (for
  * example a solver inside an allocator-managed runtime, or a process whose device memory

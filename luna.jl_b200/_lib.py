@@ -60,6 +60,11 @@ class RadialDesc(ctypes.Structure):
     _fields_ = [("Nr", c_int), ("Mi", PD), ("Mf", PD), ("outfac", PD)]
 
 
+class ModalDesc(ctypes.Structure):
+    _fields_ = [("nmodes", c_int), ("npol", c_int), ("nlevels", c_int), ("ems", PD), ("wts", PD),
+                ("wlow", c_double), ("rtol", c_double), ("atol", c_double), ("outfac", PD)]
+
+
 GRAD_MAXPTS = 16
 
 
@@ -98,7 +103,8 @@ EXPORTS = [
     "luna_b200_radial_rhs_device", "luna_b200_radial_solve", "luna_b200_qdht_device",
     "luna_b200_batch_timeline", "luna_b200_batch_set_priority",
     "luna_b200_batch_info", "luna_b200_batch_stats", "luna_b200_plan_set_gradient",
-    "luna_b200_plan_linop",
+    "luna_b200_plan_linop", "luna_b200_modal_plan_create", "luna_b200_modal_plan_destroy",
+    "luna_b200_modal_rhs", "luna_b200_modal_rhs_device", "luna_b200_modal_solve",
 ]
 
 _lib = None
@@ -148,6 +154,14 @@ def load():
     lib.luna_b200_radial_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
     lib.luna_b200_radial_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
                                            POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
+    lib.luna_b200_modal_plan_create.argtypes = [POINTER(GridDesc), POINTER(RespDesc), c_int,
+                                                POINTER(ModalDesc), c_int, POINTER(c_void_p)]
+    lib.luna_b200_modal_plan_destroy.argtypes = [c_void_p]
+    lib.luna_b200_modal_plan_destroy.restype = None
+    lib.luna_b200_modal_rhs.argtypes = [c_void_p, PD, PD, c_double, POINTER(c_int)]
+    lib.luna_b200_modal_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
+    lib.luna_b200_modal_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
+                                          POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
     lib.luna_b200_batch_info.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]
     lib.luna_b200_batch_set_priority.argtypes = [c_void_p, PD]
     lib.luna_b200_batch_timeline.argtypes = [c_void_p, PD, POINTER(c_int)]

@@ -15,7 +15,7 @@
 
 #include "../../include/luna_b200.h"
 #include "dist.cuh"
-#include "radial.cuh"
+#include "modal.cuh"
 #include "tc_gemm.cuh"
 
 using namespace luna;
@@ -1432,9 +1432,10 @@ int rad_column_setup(luna_radial_plan* p) {
         p->gstride = align_up(gscr_bytes<Rl>(I), 256);
         if (dalloc(p->allocs, &p->gscr, p->gstride * p->Nr)) return LUNA_ERR_CUDA;
     }
-    CK(cudaFuncSetAttribute(rad_column_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
-    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
-    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem));
+    // the device maximum, so that plans of different sizes never lower each other's limit
+    CK(cudaFuncSetAttribute(rad_column_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
     return LUNA_OK;
 }
 
@@ -1621,7 +1622,7 @@ int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, doub
 
 namespace {
 
-// Device buffers of one radial solve.
+// Device buffers of one column solve (radial or modal transform).
 struct RadSolve {
     std::vector<void*> allocs;
     double2 *L = nullptr, *y = nullptr, *yn = nullptr, *e1 = nullptr, *saves = nullptr;
@@ -1637,9 +1638,12 @@ struct RadSolve {
     }
 };
 
-template <typename Rl, typename Kt>
-int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double z0, double dz0, double zmax,
-              const luna_solve_opts* o, double* saves, double* steplog, luna_solve_stats* stats) {
+// RK45.solve_precon with Luna.run's stepfun on an Nw x Nr column state (RK45.jl:19-89,
+// Luna.jl:358-391). xform(tw, st, flags, stream) evaluates the transform of the stage
+// input in p->A into p->B (before the output factor); `who` names the caller in errors.
+template <typename Rl, typename Kt, typename PlanT, typename XF>
+int col_solve(PlanT* p, XF&& xform, const char* who, const double* linop, double* y_inout, double z0, double dz0,
+              double zmax, const luna_solve_opts* o, double* saves, double* steplog, luna_solve_stats* stats) {
     TwDev tw;
     int rc = get_tw(tw);
     if (rc) return rc;
@@ -1699,7 +1703,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
     rad_init_kernel<<<1, 32, 0, s>>>(S.st, S.opt, S.y, S.yn, S.d_k);
     // k1 = f(y0)
     rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, nullptr, (cpx<Rl>*)p->A);
-    rad_transform<Rl>(p, t, S.st, flags_dev, s);
+    xform(t, S.st, flags_dev, s);
     rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, (const cpx<Rl>*)p->B, nullptr);
     CK(cudaGetLastError());
     // steps are enqueued in chunks; the loop state on the device says when to stop
@@ -1711,7 +1715,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
             rad_begin_kernel<<<1, 32, 0, s>>>(S.st, S.opt);
             for (int sg = 0; sg < 6; ++sg) {
                 rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, nullptr, (cpx<Rl>*)p->A);
-                rad_transform<Rl>(p, t, S.st, flags_dev, s);
+                xform(t, S.st, flags_dev, s);
                 rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, (const cpx<Rl>*)p->B, nullptr);
             }
             rad_combine_kernel<Kt><<<nblk, 256, 0, s>>>(a, S.partial);
@@ -1723,7 +1727,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
         CK(cudaMemcpyAsync(S.h_fin, fin_dev, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         if (*S.h_fin) break;
-        if (enq > cap + 1) return fail(LUNA_ERR_CUDA, "radial_solve: loop did not end after max_steps");
+        if (enq > cap + 1) return fail(LUNA_ERR_CUDA, std::string(who) + ": loop did not end after max_steps");
         chunk = std::min(chunk * 2, 64);
     }
     // results
@@ -1747,7 +1751,7 @@ int rad_solve(luna_radial_plan* p, const double* linop, double* y_inout, double 
     if (r.status == ST_FIELD_ABOVE_EMAX) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
     if (r.status == ST_REPEAT_LIMIT) return fail(LUNA_REPEAT_LIMIT, "Reached limit for step repetition");
     if (r.status == ST_STEP_BUDGET) return fail(LUNA_STEP_BUDGET, "Step budget exhausted before zmax");
-    if (r.status == ST_WAIT_TIMEOUT) return fail(LUNA_WAIT_TIMEOUT, "radial_solve: a tensor-core wait timed out");
+    if (r.status == ST_WAIT_TIMEOUT) return fail(LUNA_WAIT_TIMEOUT, std::string(who) + ": a tensor-core wait timed out");
     return LUNA_OK;
 }
 
@@ -1761,8 +1765,249 @@ int luna_b200_radial_solve(luna_radial_plan* p, const double* linop, double* y_i
     if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "radial_solve: null argument");
     if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "radial_solve: save points missing");
     if (p->precision == LUNA_PREC_FP64)
-        return rad_solve<double, double>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
-    return rad_solve<float, float>(p, linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+        return col_solve<double, double>(
+            p, [p](const TwTab<double>& t, RadState* st, int* fl, cudaStream_t s) { return rad_transform<double>(p, t, st, fl, s); },
+            "radial_solve", linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+    return col_solve<float, float>(
+        p, [p](const TwTab<float>& t, RadState* st, int* fl, cudaStream_t s) { return rad_transform<float>(p, t, st, fl, s); },
+        "radial_solve", linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+}
+
+// ===================================================================== modal transform
+}  // extern "C"
+
+struct luna_modal_plan {
+    int precision = 0;
+    int Nw = 0, Nr = 0;           // Nr: modes (columns of the state)
+    int npol = 1, nlevels = 1, nslots = 1, P = 1, nchunk = 1;
+    double wlow = 0, rtol = 0, atol = 0, kerr = 0;
+    luna_plan* col = nullptr;     // grid and responses of one point
+    LunaInst* d_col = nullptr;
+    std::vector<void*> allocs;
+    const double2* outfac = nullptr;  // [Nr*Nw] crop * ωwin * norm!
+    const double* ems = nullptr;      // [nslots*Nr*npol]
+    const double* wts = nullptr;      // [nlevels*nslots]
+    char* gscr = nullptr;
+    size_t gstride = 0;
+    int smem = 0;
+    void* A = nullptr;   // [Nw*Nr] stage input
+    void* B = nullptr;   // [Nw*Nr] integrated transform of the last level
+    void* Et = nullptr;  // [Nr*No/2] field samples per mode
+    void* G = nullptr;   // [nslots*Nr*No/2] projected polarisation per node
+    ModalState* ms = nullptr;
+    int* d_flags = nullptr;
+    double2* d_Ew = nullptr;
+    double2* d_nl = nullptr;
+    cudaStream_t stream = nullptr;
+};
+
+namespace {
+
+ModalArgs modal_args(const luna_modal_plan* p, const RadState* st) {
+    ModalArgs a;
+    a.nmodes = p->Nr;
+    a.npol = p->npol;
+    a.nslots = p->nslots;
+    a.lmax = p->nlevels - 1;
+    a.P = p->P;
+    a.ems = p->ems;
+    a.wts = p->wts;
+    a.wlow = p->wlow;
+    a.rtol = p->rtol;
+    a.atol = p->atol;
+    a.kerr = p->kerr;
+    a.outfac = p->outfac;
+    a.Et = p->Et;
+    a.G = p->G;
+    a.ms = p->ms;
+    a.st = st;
+    return a;
+}
+
+// Transform of the stage input in A into B: fields per mode, then for each cubature level
+// its new nodes and its integral; levels after convergence return at once.
+template <typename Rl>
+int modal_xform(luna_modal_plan* p, const TwTab<Rl>& tw, RadState* st, int* flags, cudaStream_t s) {
+    const ModalArgs a = modal_args(p, st);
+    modal_time_kernel<Rl><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(p->d_col, (const cpx<Rl>*)p->A, a, tw, p->smem, p->gscr,
+                                                             p->gstride);
+    for (int l = 0; l < p->nlevels; ++l) {
+        const int s0 = (l == 0) ? 0 : (1 << l) - 1;
+        const int nn = (l == 0) ? 1 : (1 << l);
+        if (p->npol == 1)
+            modal_node_kernel<Rl><<<nn, LUNA_BLOCK, p->smem, s>>>(p->d_col, a, s0, tw, p->smem, p->gscr, p->gstride, flags);
+        else
+            modal_kerr2_kernel<Rl><<<dim3(nn, std::max(1, p->nchunk / nn)), 256, 0, s>>>(p->d_col, a, s0);
+        modal_level_kernel<Rl><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(p->d_col, a, l, (cpx<Rl>*)p->B, tw, p->smem, p->gscr,
+                                                                  p->gstride);
+    }
+    return LUNA_OK;
+}
+
+template <typename Rl>
+int modal_setup(luna_modal_plan* p) {
+    const LunaInst& I = p->col->proto;
+    const int maxs = max_smem_optin();
+    const size_t want = smem_wanted<Rl>(I);
+    p->smem = (int)std::min<size_t>(want, (size_t)maxs);
+    const int M = I.No / 2;
+    if (want > (size_t)maxs) {
+        p->gstride = align_up(gscr_bytes<Rl>(I), 256);
+        const int ncta = std::max(p->Nr, 1 << (p->nlevels - 1));
+        if (dalloc(p->allocs, &p->gscr, p->gstride * ncta)) return LUNA_ERR_CUDA;
+    }
+    // split factor of the time buffers: the block transform's when the buffer is in shared
+    // memory (the same test as plan_ws), natural order otherwise
+    const bool main_smem = LUNA_SMALL_BYTES + align_up((size_t)M * sizeof(cpx<Rl>), 256) <= (size_t)p->smem;
+    p->P = main_smem ? fft_nsplit<Rl>(M) : 1;
+    p->nchunk = std::max(1, std::min(M / 256, 4 * 148));
+    if (dalloc(p->allocs, &p->Et, sizeof(cpx<Rl>) * (size_t)p->Nr * M) ||
+        dalloc(p->allocs, &p->G, sizeof(cpx<Rl>) * (size_t)p->nslots * p->Nr * M))
+        return LUNA_ERR_CUDA;
+    CK(cudaFuncSetAttribute(modal_time_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(modal_node_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(modal_level_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    CK(cudaFuncSetAttribute(rad_post_kernel<Rl, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
+    return LUNA_OK;
+}
+
+template <typename Rl>
+int modal_rhs(luna_modal_plan* p, const double2* Ew, double2* nl, cudaStream_t s) {
+    TwDev tw;
+    int rc = get_tw(tw);
+    if (rc) return rc;
+    const TwTab<Rl>& t = *reinterpret_cast<const TwTab<Rl>*>(std::is_same<Rl, double>::value ? (const void*)&tw.d : (const void*)&tw.f);
+    RadArgs a{p->Nw, p->Nr, nullptr, p->outfac, nullptr, nullptr};
+    const size_t n = (size_t)p->Nw * p->Nr;
+    CK(cudaMemsetAsync(p->d_flags, 0, sizeof(int), s));
+    rad_stage_kernel<Rl, double><<<rad_grid(n), 256, 0, s>>>(a, -1, Ew, (cpx<Rl>*)p->A);
+    modal_xform<Rl>(p, t, nullptr, p->d_flags, s);
+    rad_store_kernel<Rl, double><<<rad_grid(n), 256, 0, s>>>(a, -1, (const cpx<Rl>*)p->B, nl);
+    CK(cudaGetLastError());
+    return LUNA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, int nresp,
+                                const luna_modal_desc* md, int precision, luna_modal_plan** out) {
+    if (!g || !md || !out || !md->ems || !md->wts || !md->outfac || (nresp > 0 && !resps))
+        return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: null argument");
+    if (g->kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: only field-resolved (RealGrid) modal transforms");
+    if (md->nmodes < 1 || md->nmodes > LUNA_MODAL_MAX_MODES)
+        return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: nmodes must be in 1..LUNA_MODAL_MAX_MODES");
+    if (md->npol != 1 && md->npol != 2) return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: npol must be 1 or 2");
+    if (md->nlevels < 1 || md->nlevels > LUNA_MODAL_MAX_LEVELS)
+        return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: nlevels must be in 1..LUNA_MODAL_MAX_LEVELS");
+    if (!(md->rtol >= 0) || !(md->atol >= 0)) return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: negative tolerance");
+    if (precision != LUNA_PREC_FP64 && precision != LUNA_PREC_MIXED)
+        return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: unknown precision");
+    double kerr = 0;
+    for (int i = 0; i < nresp; ++i) {
+        if (resps[i].kind == LUNA_RESP_RAMAN)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: Raman response not available for the modal transform");
+        if (md->npol == 2 && resps[i].kind != LUNA_RESP_KERR_FIELD)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support the Kerr response only");
+        if (resps[i].kind == LUNA_RESP_KERR_FIELD) kerr += resps[i].coef;
+    }
+    // the point plan: grid and responses; its output factor is unused (the modal one is
+    // applied after the cubature)
+    std::vector<double> ones(2 * (size_t)g->Nw, 0.0);
+    for (int k = 0; k < g->Nw; ++k) ones[2 * k] = 1.0;
+    luna_grid_desc gc = *g;
+    gc.outfac = ones.data();
+    luna_plan* col = nullptr;
+    int rc = luna_b200_plan_create(&gc, resps, nresp, precision, &col);
+    if (rc) return rc;
+    luna_modal_plan* p = new luna_modal_plan();
+    p->precision = precision;
+    p->Nw = g->Nw;
+    p->Nr = md->nmodes;
+    p->npol = md->npol;
+    p->nlevels = md->nlevels;
+    p->nslots = (2 << (md->nlevels - 1)) - 1;
+    p->wlow = md->wlow;
+    p->rtol = md->rtol;
+    p->atol = md->atol;
+    p->kerr = kerr;
+    p->col = col;
+    auto bail = [&](int code) {
+        free_all(p->allocs);
+        luna_b200_plan_destroy(p->col);
+        delete p;
+        return code;
+    };
+    const size_t n = (size_t)p->Nw * p->Nr;
+    const double* tmp = nullptr;
+    if (upload(p->allocs, md->outfac, 2 * n, &tmp) ||
+        upload(p->allocs, md->ems, (size_t)p->nslots * p->Nr * p->npol, &p->ems) ||
+        upload(p->allocs, md->wts, (size_t)p->nlevels * p->nslots, &p->wts))
+        return bail(LUNA_ERR_CUDA);
+    p->outfac = (const double2*)tmp;
+    const size_t cb = sizeof(double2);
+    if (dalloc(p->allocs, &p->A, cb * n) || dalloc(p->allocs, &p->B, cb * n) || dalloc(p->allocs, &p->d_flags, sizeof(int)) ||
+        dalloc(p->allocs, &p->ms, sizeof(ModalState)) || dalloc(p->allocs, &p->d_col, sizeof(LunaInst)))
+        return bail(LUNA_ERR_CUDA);
+    if (cudaMemset(p->ms, 0, sizeof(ModalState)) != cudaSuccess ||
+        cudaMemcpy(p->d_col, &col->proto, sizeof(LunaInst), cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(fail(LUNA_ERR_CUDA, "modal_plan_create: initialising the device state failed"));
+    rc = (precision == LUNA_PREC_FP64) ? modal_setup<double>(p) : modal_setup<float>(p);
+    if (rc) return bail(rc);
+    *out = p;
+    return LUNA_OK;
+}
+
+void luna_b200_modal_plan_destroy(luna_modal_plan* p) {
+    if (!p) return;
+    if (p->stream) cudaStreamDestroy(p->stream);
+    free_all(p->allocs);
+    luna_b200_plan_destroy(p->col);
+    delete p;
+}
+
+int luna_b200_modal_rhs_device(luna_modal_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
+    (void)z;  // constant density
+    if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "modal_rhs_device: null argument");
+    if (p->precision == LUNA_PREC_FP64) return modal_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+    return modal_rhs<float>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+}
+
+int luna_b200_modal_rhs(luna_modal_plan* p, double* nl, const double* Ew, double z, int* nevals) {
+    (void)z;
+    if (!p || !nl || !Ew) return fail(LUNA_ERR_BAD_ARG, "modal_rhs: null argument");
+    const size_t bytes = sizeof(double2) * p->Nw * p->Nr;
+    if (!p->d_Ew) {
+        if (dalloc(p->allocs, &p->d_Ew, bytes) || dalloc(p->allocs, &p->d_nl, bytes)) return LUNA_ERR_CUDA;
+        CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
+    }
+    CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
+    int rc = (p->precision == LUNA_PREC_FP64) ? modal_rhs<double>(p, p->d_Ew, p->d_nl, p->stream)
+                                              : modal_rhs<float>(p, p->d_Ew, p->d_nl, p->stream);
+    if (rc) return rc;
+    int fl = 0, nev = 0;
+    CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(&fl, p->d_flags, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaMemcpyAsync(&nev, &p->ms->nevals, sizeof(int), cudaMemcpyDeviceToHost, p->stream));
+    CK(cudaStreamSynchronize(p->stream));
+    if (nevals) *nevals = nev;
+    if (fl & (1 << ST_FIELD_ABOVE_EMAX)) return fail(LUNA_FIELD_ABOVE_EMAX, "Field strength exceeds maximum for PPT ionisation rate.");
+    return LUNA_OK;
+}
+
+int luna_b200_modal_solve(luna_modal_plan* p, const double* linop, double* y_inout, double z0, double dz0, double zmax,
+                          const luna_solve_opts* opts, double* saves, double* steplog, luna_solve_stats* stats) {
+    if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "modal_solve: null argument");
+    if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "modal_solve: save points missing");
+    if (p->precision == LUNA_PREC_FP64)
+        return col_solve<double, double>(
+            p, [p](const TwTab<double>& t, RadState* st, int* fl, cudaStream_t s) { return modal_xform<double>(p, t, st, fl, s); },
+            "modal_solve", linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
+    return col_solve<float, float>(
+        p, [p](const TwTab<float>& t, RadState* st, int* fl, cudaStream_t s) { return modal_xform<float>(p, t, st, fl, s); },
+        "modal_solve", linop, y_inout, z0, dz0, zmax, opts, saves, steplog, stats);
 }
 
 // ---------------------------------------------------------------- allocation-free RHS

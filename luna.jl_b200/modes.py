@@ -5,7 +5,8 @@
 * ``MarcatiliMode``: hollow-capillary HE/TE/TM modes with the complex effective index of
   Marcatili & Schmeltzer (Capillary.jl:29-186), effective area (Capillary.jl:284-300)
   and the group delay beta1 by a central finite difference (the reference uses
-  FiniteDifferences.jl, Maths.jl:18-32).
+  FiniteDifferences.jl, Maths.jl:18-32); the transverse field, its normalisation and
+  integration limits (Capillary.jl:267-287, Modes.jl:73) for the modal transform.
 """
 import math
 
@@ -84,8 +85,8 @@ def _unm(n, m, kind):
 class MarcatiliMode:
     """Hollow capillary mode filled with ``gas`` at pressure ``P`` (Capillary.jl:95-109)."""
 
-    def __init__(self, a, gas, P, n=1, m=1, kind="HE", T=pd.roomtemp, model="full", loss=True):
-        self.a, self.n, self.m, self.kind = a, n, m, kind
+    def __init__(self, a, gas, P, n=1, m=1, kind="HE", ϕ=0.0, T=pd.roomtemp, model="full", loss=True):
+        self.a, self.n, self.m, self.kind, self.ϕ = a, n, m, kind, ϕ
         self.model, self.loss = model, loss
         self.unm = _unm(n, m, kind)
         self.coren = pd.ref_index_fun(gas, P, T) if gas is not None else (lambda lam: 1.0 + 0j)
@@ -137,3 +138,30 @@ class MarcatiliMode:
 
     def Aeff(self, z=0.0):
         return self.a ** 2 * self.aeff_intg
+
+    def dimlimits(self, z=0.0):
+        """(:polar, (0, 0), (a, 2π)) (Capillary.jl:267)."""
+        return ("polar", (0.0, 0.0), (self.a, 2 * math.pi))
+
+    def field(self, r, θ=0.0):
+        """Unnormalised (Ex, Ey) at polar (r, θ) (Capillary.jl:270-282)."""
+        x = r * self.unm / self.a
+        if self.kind == "HE":
+            J = special.jv(self.n - 1, x)
+            s, c = math.sin(self.n * (θ + self.ϕ)), math.cos(self.n * (θ + self.ϕ))
+            return (J * (math.cos(θ) * s - math.sin(θ) * c), J * (math.sin(θ) * s + math.cos(θ) * c))
+        J = special.jv(1, x)
+        if self.kind == "TE":
+            return (-J * math.sin(θ), J * math.cos(θ))
+        return (J * math.cos(θ), J * math.sin(θ))
+
+    def N(self, z=0.0):
+        """Mode normalisation π/2 a² J_{n or 2}(unm)² sqrt(ε0/μ0) (Capillary.jl:284-287)."""
+        np1 = self.n if self.kind == "HE" else 2
+        return math.pi / 2 * self.a ** 2 * special.jv(np1, self.unm) ** 2 * math.sqrt(pd.eps_0 / pd.mu_0)
+
+    def Exy(self, r, θ=0.0):
+        """Normalised field field(m, xs)/sqrt(N(m)) (Modes.jl:73)."""
+        s = 1.0 / math.sqrt(self.N())
+        ex, ey = self.field(r, θ)
+        return (ex * s, ey * s)

@@ -231,8 +231,111 @@ def trans_radial(t, Ew, z):
     return nl * t.output_factor()
 
 
+def kerr_vector(out, E, rho, g3):
+    """KerrVector! (Nonlinear.jl:12-21): E is (n, 2)."""
+    fac = rho * EPS0 * g3
+    s = E[:, 0] ** 2 + E[:, 1] ** 2
+    out[:, 0] += fac * s * E[:, 0]
+    out[:, 1] += fac * s * E[:, 1]
+
+
+def et_to_pt_modal(Er, resp, rho):
+    """Et_to_Pt! on the (n, npol) real-space field of one point: scalar responses for one
+    component (Nonlinear.jl:24-34, 164-177 with size(Et, 2) == 1), vector Kerr for two."""
+    if Er.shape[1] == 1:
+        return et_to_pt(Er[:, 0], resp, rho)[:, None]
+    Pr = np.zeros_like(Er)
+    for r in resp:
+        if r.kind != "kerr_field":
+            raise NotImplementedError(r.kind)
+        kerr_vector(Pr, Er, rho, r.γ3)
+    return Pr
+
+
+def clenshaw_curtis_moments(n):
+    """Weights of the (n+1)-point Clenshaw-Curtis rule on [-1, 1] (nodes cos(jπ/n)) from its
+    definition: the rule integrates the Chebyshev polynomials T_0..T_n exactly,
+    sum_j w_j cos(kjπ/n) = ∫ T_k = (1 + (-1)^k)/(1 - k²) (0 for k = 1)."""
+    j = np.arange(n + 1)
+    A = np.cos(np.outer(j, j) * math.pi / n)  # A[k, j] = T_k(x_j)
+    k = j.astype(np.float64)
+    with np.errstate(divide="ignore"):
+        mom = np.where(k % 2 == 0, 2.0 / (1.0 - k * k), 0.0)
+    return np.cos(j * math.pi / n), np.linalg.solve(A, mom)
+
+
+def pcubature(f, lo, hi, rtol, atol, maxevals):
+    """One-dimensional ``Cubature.pcubature_v(fdim, f, (lo,), (hi,); reltol, abstol, maxevals,
+    error_norm=Cubature.L2)`` as called at NonlinearRHS.jl:294-298. Cubature.jl (compat 1.5.1,
+    Project.toml:62; not vendored, so the exact version is unpinned) wraps S. G. Johnson's cubature library; its p-adaptive routine,
+    as published, doubles the degree of nested Clenshaw-Curtis rules until the error estimate
+    (the difference from the previous rule) meets the tolerance. Restated here: level m uses
+    the 2^(m+1)+1-point rule, level -1 the midpoint rule; the error of level m is
+    ||I_m - I_{m-1}||_2 over the fdim components; converged when it is <= abstol or
+    <= reltol ||I_m||_2; the next level is only evaluated while its points fit in
+    maxevals. Integrand values are cached per point. Returns (I_m, error, evaluations)."""
+    c, h = (lo + hi) / 2, (hi - lo) / 2
+    cache = {}
+    DEPTH = 1 << 12
+
+    def F(j, n):  # node cos(jπ/n), keyed on the finest grid
+        key = j * (DEPTH // n)
+        if key not in cache:
+            cache[key] = f(c + h * math.cos(j * math.pi / n))
+        return cache[key]
+
+    Ilow = h * 2.0 * F(1, 2)
+    m = 0
+    while True:
+        n = 2 << m
+        _, w = clenshaw_curtis_moments(n)
+        I = h * sum(w[j] * F(j, n) for j in range(n + 1))
+        err = float(np.linalg.norm(I - Ilow))
+        if err <= atol or err <= rtol * float(np.linalg.norm(I)):
+            break
+        if (2 << (m + 1)) + 1 > maxevals or (2 << (m + 1)) > DEPTH:
+            break
+        Ilow = I
+        m += 1
+    return I, err, len(cache)
+
+
+def trans_modal(t, Ew, z):
+    """(t::TransModal)(nl, Eω, z) with full=false (NonlinearRHS.jl:234-302) for a
+    field-resolved grid: Ew is (Nω, nmodes). Per point r: to_space! (Modes.jl:458-495) at
+    (r, 0), to_time!, Et_to_Pt!, towin, to_freq!, ωwin, norm!, projection onto the modes
+    (Prω Emsᵀ) and the weight 2πr; points on or outside (0, a) give zero."""
+    g, ts = t.grid, t.ts
+    Nw = Ew.shape[0]
+    Nwo = len(g.ωo)
+    lo, hi = 0.0, t.a
+    of = g.ωwin * t.norm
+
+    def point(r):
+        if r <= lo or r >= hi:
+            return np.zeros_like(Ew)
+        Ems = ts.ems(r)                                  # (nmodes, npol)
+        Erω = Ew @ Ems                                   # (Nω, npol)
+        Erωo = np.zeros((Nwo, Erω.shape[1]), dtype=np.complex128)
+        Erωo[:Nw] = ((Nwo - 1) / (Nw - 1)) * Erω
+        Er = np.fft.irfft(Erωo, g.No, axis=0)
+        Pr = et_to_pt_modal(Er, t.resp, t.density) * g.towin[:, None]
+        Prω = ((Nw - 1) / (Nwo - 1)) * np.fft.rfft(Pr, axis=0)[:Nw]
+        Prω = Prω * of[:, None]
+        return 2 * math.pi * r * (Prω @ Ems.T)           # (Nω, nmodes)
+
+    val, err, nev = pcubature(point, lo, hi, t.rtol, t.atol, t.mfcn)
+    t.oracle_nevals = nev
+    return val
+
+
 def rhs(t, Ew, z):
-    return trans_radial(t, Ew, z) if getattr(t, "kind", "") == "radial" else trans_mode_avg(t, Ew, z)
+    kind = getattr(t, "kind", "")
+    if kind == "radial":
+        return trans_radial(t, Ew, z)
+    if kind == "modal":
+        return trans_modal(t, Ew, z)
+    return trans_mode_avg(t, Ew, z)
 
 
 # ------------------------------------------------------------------- RK45 (dopri)

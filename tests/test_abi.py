@@ -78,6 +78,9 @@ int main(void) {
     P(luna_gradient_desc, fd_xc); P(luna_gradient_desc, fd_vn); P(luna_gradient_desc, fd_h12);
     P(luna_gradient_desc, nta); P(luna_gradient_desc, ZA); P(luna_gradient_desc, eps0c2);
     P(luna_gradient_desc, vn);
+    printf("luna_modal_desc %zu\n", sizeof(luna_modal_desc));
+    P(luna_modal_desc, ems); P(luna_modal_desc, wts); P(luna_modal_desc, wlow);
+    P(luna_modal_desc, rtol); P(luna_modal_desc, atol); P(luna_modal_desc, outfac);
     return 0;
 }
 """
@@ -116,3 +119,6 @@ def test_struct_layout_matches_ctypes(tmp_path):
     for f in ("Z", "P2", "dens_b", "loss", "gam", "ofs", "fd_xc", "fd_vn", "fd_h12", "nta", "ZA",
               "eps0c2", "vn"):
         assert int(out[f"luna_gradient_desc.{f}"]) == getattr(_lib.GradientDesc, f).offset
+    assert int(out["luna_modal_desc"]) == ctypes.sizeof(_lib.ModalDesc)
+    for f in ("ems", "wts", "wlow", "rtol", "atol", "outfac"):
+        assert int(out[f"luna_modal_desc.{f}"]) == getattr(_lib.ModalDesc, f).offset

@@ -1,0 +1,161 @@
+"""Modal transform (TransModal, full=false): host set-up, the cubature rule and the oracle.
+
+The reference's own check of this path (test/test_multimode.jl:3-43, "Radial") propagates
+one HE11 mode with Kerr only both mode-averaged and modally and asks the spectra to agree to
+0.003; it is repeated here with the oracle (shorter fibre) and, on the GPU, in
+test_gpu_modal.py at full length.
+"""
+import math
+
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import numpy as np
+import pytest
+from scipy import integrate, special
+
+from luna_b200 import fields, modal, modes
+from luna_b200 import physdata as pd
+from luna_b200.grid import RealGrid
+from luna_b200.linops import make_const_linop
+from luna_b200.nonlinear import Kerr_field
+from luna_b200.nonlinearrhs import TransModeAvg, norm_mode_average
+from oracle import uppe
+
+A, GAS, PRES, TAU, LAM0 = 13e-6, "Ar", 5.0, 30e-15, 800e-9
+
+
+def test_clenshaw_curtis_host_rule_matches_oracle_rule():
+    """The product's closed-form weights and the oracle's moment-matching weights agree, and
+    the rule integrates polynomials up to its degree exactly."""
+    for n in (2, 4, 8, 16, 64, 256, 512):
+        x, w = modal.clenshaw_curtis(n)
+        xo, wo = uppe.clenshaw_curtis_moments(n)
+        np.testing.assert_allclose(x, xo, rtol=0, atol=1e-15)
+        np.testing.assert_allclose(w, wo, rtol=0, atol=2e-15)
+        for k in range(0, n + 1, 2):
+            assert abs(np.dot(w, x ** k) - 2.0 / (k + 1)) < 1e-13
+
+
+def test_cubature_tables_nested_levels():
+    """Slot weights of each level are that level's Clenshaw-Curtis weights on (0, a) times
+    2πr; level sums converge to ∫ 2πr dr = πa²."""
+    nl = modal.cubature_levels(512)
+    assert nl == 8  # 3, 5, ..., 257 points; 513 would exceed mfcn = 512
+    assert modal.cubature_levels(2) == 1 and modal.cubature_levels(5) == 2
+    r, wts, wlow = modal.cubature_tables(A, nl)
+    assert len(r) == 2 ** nl - 1 and wts.shape == (nl, len(r))
+    assert r[0] == pytest.approx(A / 2) and wlow == pytest.approx(A * 2 * math.pi * A / 2)
+    for l in range(nl):
+        x, w = modal.clenshaw_curtis(2 << l)
+        rl = A / 2 * (1 + x[1:-1])
+        used = wts[l] != 0
+        assert used.sum() == len(rl)
+        np.testing.assert_allclose(np.sort(r[used]), np.sort(rl), rtol=0, atol=1e-14 * A)
+        f = lambda rr: np.cos(rr / A) * np.exp(-rr / A)
+        ref = A / 2 * np.dot(w[1:-1], 2 * math.pi * rl * f(rl))
+        assert np.dot(wts[l], f(r)) == pytest.approx(ref, rel=1e-13)
+    assert wts[-1].sum() == pytest.approx(math.pi * A ** 2, rel=1e-4)
+
+
+@pytest.mark.parametrize("n,m,kind,phi", [(1, 1, "HE", 0.0), (1, 2, "HE", 0.0), (2, 1, "HE", -math.pi / 4),
+                                       (0, 1, "TE", 0.0), (0, 1, "TM", 0.0)])
+def test_mode_fields_carry_unit_power(n, m, kind, phi):
+    """Exy = field/sqrt(N) (Modes.jl:73) carries unit power: 1/2 sqrt(ε0/μ0) ∫|Exy|² dA = 1
+    (the normalisation Modes.N computes by cubature, Modes.jl:55-66)."""
+    md = modes.MarcatiliMode(A, GAS, PRES, n=n, m=m, kind=kind, ϕ=phi, loss=False)
+    th = np.linspace(0, 2 * math.pi, 64, endpoint=False)
+
+    def ring(r):
+        return np.mean([sum(c * c for c in md.Exy(r, t)) for t in th]) * 2 * math.pi * r
+
+    v, _ = integrate.quad(ring, 0, A, epsrel=1e-11, limit=200)
+    assert 0.5 * math.sqrt(pd.eps_0 / pd.mu_0) * v == pytest.approx(1.0, rel=1e-9)
+
+
+def test_mode_field_components():
+    """Capillary.jl:270-282 at θ = 0: HE11 is y-polarised, TM01 x, TE01 y."""
+    he = modes.MarcatiliMode(A, GAS, PRES, loss=False)
+    tm = modes.MarcatiliMode(A, GAS, PRES, n=0, m=1, kind="TM", loss=False)
+    te = modes.MarcatiliMode(A, GAS, PRES, n=0, m=1, kind="TE", loss=False)
+    r = 0.3 * A
+    assert he.field(r)[0] == 0 and he.field(r)[1] == pytest.approx(special.jv(0, r * he.unm / A))
+    assert tm.field(r)[1] == 0 and tm.field(r)[0] == pytest.approx(special.jv(1, r * tm.unm / A))
+    assert te.field(r)[0] == 0 and te.field(r)[1] == pytest.approx(special.jv(1, r * te.unm / A))
+    ts = modal.ToSpace((he, tm), components="xy")
+    e = ts.ems(r)
+    assert e.shape == (2, 2) and e[0, 0] == 0 and e[1, 1] == 0
+    assert modal.ToSpace((he,), components="y").ems(r).shape == (1, 1)
+    with pytest.raises(ValueError):
+        modal.ToSpace((he,), components="z")
+
+
+def test_oracle_pcubature_levels_and_limit():
+    """The restated p-adaptive rule: a smooth vector integrand converges to the quadrature
+    value within the tolerance, the error estimate is the difference of successive levels,
+    and the evaluation limit stops the doubling."""
+    f = lambda r: np.array([r * special.jv(0, 2.405 * r) ** 4, math.sin(3 * r)])
+    ref = np.array([integrate.quad(lambda r: f(r)[i], 0, 1, epsrel=1e-13)[0] for i in range(2)])
+    val, err, nev = uppe.pcubature(f, 0.0, 1.0, 1e-6, 0.0, 512)
+    assert np.linalg.norm(val - ref) <= 1e-6 * np.linalg.norm(ref)
+    assert err <= 1e-6 * np.linalg.norm(val) and nev in (9, 17, 33)
+    v2, e2, n2 = uppe.pcubature(f, 0.0, 1.0, 1e-14, 0.0, 20)
+    assert n2 == 17  # 33 points would exceed the limit of 20
+    v3, e3, n3 = uppe.pcubature(f, 0.0, 1.0, 0.9, 0.0, 512)
+    assert n3 == 3  # a loose tolerance accepts level 0 (end points are evaluated too)
+
+
+def _radial_case(flength):
+    grid = RealGrid(flength, 800e-9, (160e-9, 3000e-9), 1e-12)
+    m = modes.MarcatiliMode(A, GAS, PRES, loss=False)
+    dens = pd.density(GAS, PRES)
+    resp = (Kerr_field(pd.gamma3_gas(GAS)),)
+    inp = fields.GaussField(LAM0, TAU, energy=1e-6)
+    return grid, m, dens, resp, inp
+
+
+def test_doinput_mm_forms_agree():
+    """test_multimode.jl:151-176 ("FieldInputs"): a field, a tuple of fields and a tuple of
+    (mode, fields) entries put the same spectrum into mode 1."""
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    ms = (modes.MarcatiliMode(A, GAS, PRES, n=1, m=1, loss=False),
+          modes.MarcatiliMode(A, GAS, PRES, n=1, m=2, loss=False))
+    e1, _ = modal.setup_modal(grid, dens, resp, inp, ms, "y")
+    e2, _ = modal.setup_modal(grid, dens, resp, (inp,), ms, "y")
+    e3, _ = modal.setup_modal(grid, dens, resp, ({"mode": 1, "fields": (inp,)},), ms, "y")
+    assert np.array_equal(e1, e2) and np.array_equal(e1, e3)
+    assert np.all(e1[:, 1] == 0) and np.any(e1[:, 0] != 0)
+
+
+def test_modal_linop_matches_single_mode_on_sidx():
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    L1, _, β1 = make_const_linop(grid, m, LAM0)
+    Lm = modal.make_const_linop_modes(grid, (m,), LAM0)
+    s = grid.sidx
+    assert np.array_equal(Lm[s, 0], L1[s])
+    # outside sidx the multimode operator keeps β = 1 (LinearOps.jl:401-415)
+    np.testing.assert_allclose(Lm[~s, 0], 1j * (-1 + grid.ω[~s] * β1))
+
+
+def test_transmodal_rejects_full_and_envelope():
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    ts = modal.ToSpace((m,), components="y")
+    with pytest.raises(NotImplementedError):
+        modal.TransModal(grid, ts, resp, dens, modal.norm_modal(grid), full=True)
+
+
+def test_oracle_modal_single_mode_matches_mode_average():
+    """test_multimode.jl:3-43 ("Radial") with the oracle on 1 cm: one HE11 mode with Kerr,
+    mode-averaged and modal (radial integral), spectra within 0.003."""
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    linop, βconst, _ = make_const_linop(grid, m, LAM0)
+    t0 = TransModeAvg(grid, resp, dens, norm_mode_average(grid, βconst), m.Aeff())
+    ms = (modes.MarcatiliMode(A, GAS, PRES, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
+    Eωm, tm = modal.setup_modal(grid, dens, resp, inp, ms, "y")
+    Lm = modal.make_const_linop_modes(grid, ms, LAM0)
+    r0 = uppe.run(t0, grid, linop, inp(grid), saveN=11)
+    rm = uppe.run(tm, grid, Lm, Eωm, saveN=11)
+    Iω = np.abs(r0.Eω) ** 2
+    Iωr = np.abs(rm.Eω[:, :, 0]) ** 2
+    assert np.linalg.norm(Iω - Iωr) / np.linalg.norm(Iω) < 0.003

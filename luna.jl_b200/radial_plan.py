@@ -13,8 +13,10 @@ from .plan import SolveResult, _STATUS_MSG, make_opts, resp_descs
 
 
 def _colmajor(a):
-    """(Nw, Nr) complex -> C-contiguous (Nr, Nw), i.e. the column-major layout."""
-    return np.ascontiguousarray(np.asarray(a, dtype=np.complex128).T)
+    """(Nw, Nr) complex -> a new C-contiguous (Nr, Nw) array, i.e. the column-major layout.
+    Always a copy: a solve writes its final state into it, and for one column the
+    transpose of a contiguous array is itself contiguous (a view of the caller's array)."""
+    return np.array(np.asarray(a, dtype=np.complex128).T, order="C", copy=True)
 
 
 class RadialPlan:

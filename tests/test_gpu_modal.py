@@ -1,9 +1,11 @@
 """Modal transform (TransModal, full=false) on the GPU against the FP64 oracle.
 
 Cases follow test/test_multimode.jl: argon in a 13 µm capillary with HE11 alone (Kerr,
-"Radial"), TM01 + HE21 on both polarisation components (Kerr, the LP11 set of "Full, LP11
-vs TM01" with the radial integral), and HE11 + HE12 in a 50 µm capillary with Kerr + PPT
-plasma at 20 µJ (the plasma term is comparable to Kerr and the cubature needs 129 points).
+"Radial"), TM01 + HE21 on both polarisation components (Kerr; ϕ = 0 puts HE21 on y and TM01
+on x along θ = 0, where the radial integral samples the cross-section, so the vector Kerr
+term couples them; with the LP11 phase ϕ = -π/4 of "Full, LP11 vs TM01" and equal energies
+the two cancel there), and HE11 + HE12 in a 50 µm capillary with Kerr + PPT plasma at
+20 µJ (the plasma term is comparable to Kerr and the cubature needs 129 points).
 """
 import math
 
@@ -37,12 +39,13 @@ def _case(name, flength=1e-2):
         a, gas, pres, trange, energy = 13e-6, "Ar", 5.0, 1e-12, 1e-6
         ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
         comps, inputs, plasma = "y", fields.GaussField(LAM0, 30e-15, energy=energy), False
-    elif name == "lp11":
+    elif name == "vector":
         a, gas, pres, trange, energy = 13e-6, "Ar", 5.0, 0.4e-12, 1e-6
         ms = (modes.MarcatiliMode(a, gas, pres, n=0, m=1, kind="TM", ϕ=0.0, loss=False),
-              modes.MarcatiliMode(a, gas, pres, n=2, m=1, kind="HE", ϕ=-math.pi / 4, loss=False))
-        f = fields.GaussField(LAM0, 30e-15, energy=energy / 2)
-        comps, inputs, plasma = "xy", ({"mode": 1, "fields": (f,)}, {"mode": 2, "fields": (f,)}), False
+              modes.MarcatiliMode(a, gas, pres, n=2, m=1, kind="HE", ϕ=0.0, loss=False))
+        f1 = fields.GaussField(LAM0, 30e-15, energy=energy / 2)
+        f2 = fields.GaussField(LAM0, 30e-15, energy=energy / 5)
+        comps, inputs, plasma = "xy", ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)}), False
     else:  # two HE modes with Kerr + PPT plasma
         a, gas, pres, trange, energy = 50e-6, "Ar", 1.0, 0.4e-12, 20e-6
         ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, loss=False),
@@ -59,7 +62,7 @@ def _case(name, flength=1e-2):
     return grid, Eω, t, modal.make_const_linop_modes(grid, ms, LAM0)
 
 
-@pytest.mark.parametrize("name", ["he11", "lp11", "plasma"])
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma"])
 def test_modal_rhs_fp64_matches_oracle(name):
     """(t::TransModal)(nl, Eω, z) through the C ABI vs the oracle (NonlinearRHS.jl:284-302):
     the same number of cubature points and the integral within 1e-11. The device sums the
@@ -89,7 +92,7 @@ def test_modal_rhs_fp64_matches_oracle(name):
     assert np.array_equal(dev, nl)
 
 
-@pytest.mark.parametrize("name", ["he11", "lp11", "plasma"])
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma"])
 def test_modal_rhs_mixed_close_to_oracle(name):
     grid, Eω, t, _ = _case(name)
     plan = modal_plan.ModalPlan.from_transform(t, _lib.PREC_MIXED)
@@ -99,7 +102,7 @@ def test_modal_rhs_mixed_close_to_oracle(name):
     assert _rel(nl, ref) < 1e-3, _rel(nl, ref)
 
 
-@pytest.mark.parametrize("name,flength", [("he11", 5e-3), ("lp11", 2e-3), ("plasma", 1e-3)])
+@pytest.mark.parametrize("name,flength", [("he11", 5e-3), ("vector", 2e-3), ("plasma", 1e-3)])
 def test_modal_solve_replay_matches_oracle(name, flength):
     """Following the oracle's step sequence (replay), every saved field within 1e-10."""
     grid, Eω, t, L = _case(name, flength)
@@ -139,7 +142,7 @@ def test_modal_matches_mode_average_on_gpu():
 
 
 def test_modal_plan_rejects_unsupported_responses():
-    grid, Eω, t, _ = _case("lp11")
+    grid, Eω, t, _ = _case("vector")
     rate = ionisation.ionrate_PPTaccel("Ar", LAM0, N=2 ** 10)
     pl = PlasmaCumtrapz(grid.to, grid.to, rate, pd.ionisation_potential("Ar"))
     t2 = modal.TransModal(grid, t.ts, (t.resp[0], pl), t.density, t.norm)

@@ -13,7 +13,7 @@ import numpy as np
 from . import fields, ionisation, modes, physdata as pd, raman
 from .grid import EnvGrid, RealGrid
 from .linops import make_const_linop
-from .nonlinear import (Kerr_env, Kerr_field, PlasmaCumtrapz, RamanPolarEnv,
+from .nonlinear import (Kerr_env, Kerr_field, Kerr_field_nothg, PlasmaCumtrapz, RamanPolarEnv,
                         RamanPolarField, ionrate_fun_ADK)
 from .nonlinearrhs import TransModeAvg, norm_mode_average, norm_mode_average_gnlse
 
@@ -98,9 +98,10 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         density = pd.density(gas, pressure)
     resp = []
     if kerr:
-        if not thg:
-            raise NotImplementedError("Kerr_field_nothg is not supported on the device")
-        resp.append(Kerr_field(pd.gamma3_gas(gas)))
+        # Interface.jl:534-541: without THG the Kerr term uses the analytic signal (the
+        # oracle evaluates it; the device plan rejects it)
+        resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
+                    Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
     if plasma:
         ionpot = pd.ionisation_potential(gas)
         if gas in ("H2", "D2", "N2O", "CH4", "SF6"):
@@ -112,7 +113,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
         rr = _raman.raman_response(grid.to, gas)
-        resp.append(RamanPolarField(grid.to, rr))
+        resp.append(RamanPolarField(grid.to, rr, thg=thg))
     if grad is not None:
         # z-dependent linear operator and normalisation (LinearOps.make_linop,
         # LinearOps.jl:337-360; norm_mode_average with βfun!(β, z))

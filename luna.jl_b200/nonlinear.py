@@ -5,11 +5,17 @@ description of the response that the device evaluates inside the fused right-han
 
 * ``Kerr_field(γ3)``       -> ``out += rho*eps0*γ3*E^3``           (Nonlinear.jl:8-34)
 * ``Kerr_env(γ3)``         -> ``out += 3/4*rho*eps0*γ3*|E|^2*E``   (Nonlinear.jl:47-73)
+* ``Kerr_field_nothg(γ3, n)`` -> ``out += 3/4*rho*eps0*γ3*|hilbert(E)|^2*E`` (Nonlinear.jl:36-45)
+* ``Kerr_env_thg(γ3, ω0, t)`` -> ``out += rho*eps0*γ3/4*(3|E|^2 + exp(2iω0t) E^2)*E``
+  (Nonlinear.jl:75-84)
 * ``PlasmaCumtrapz(t, E, ratefunc, ionpot; preionfrac)``           (Nonlinear.jl:88-177)
 * ``RamanPolarField(t, r; thg)`` / ``RamanPolarEnv(t, r)``          (Nonlinear.jl:183-333)
 
 Responses accumulate into the polarisation in the order they are given, as
-``Et_to_Pt!`` does (NonlinearRHS.jl:121-126).
+``Et_to_Pt!`` does (NonlinearRHS.jl:121-126). The device evaluates Kerr_field, Kerr_env,
+PlasmaCumtrapz and the THG forms of the Raman responses; the no-THG Kerr and Raman forms
+and the THG envelope Kerr are described here and restated by the oracle, and the device
+plan rejects them (``plan.resp_descs``).
 """
 from . import physdata as pd
 from .ionisation import PPTSpline, adk_params
@@ -27,6 +33,30 @@ class Kerr_env:
 
     def __init__(self, γ3):
         self.γ3 = float(γ3)
+
+
+class Kerr_field_nothg:
+    """Kerr response of a real field without third-harmonic generation: the intensity of
+    the analytic signal (``Maths.plan_hilbert``) times the field."""
+
+    kind = "kerr_field_nothg"
+
+    def __init__(self, γ3, n):
+        self.γ3 = float(γ3)
+        self.n = int(n)
+
+
+class Kerr_env_thg:
+    """Kerr response of an envelope with its third harmonic (Genty et al., Opt. Express 15,
+    5382 (2007), Eq. 4) on the time grid ``t`` at the reference frequency ω0."""
+
+    kind = "kerr_env_thg"
+
+    def __init__(self, γ3, ω0, t):
+        import numpy as np
+        self.γ3 = float(γ3)
+        self.ω0 = float(ω0)
+        self.C = np.exp(2j * self.ω0 * np.asarray(t, dtype=np.float64))
 
 
 class ADKRate:
@@ -64,8 +94,6 @@ class RamanPolarField:
     kind = "raman_field"
 
     def __init__(self, t, r, thg=True):
-        if not thg:
-            raise NotImplementedError("RamanPolarField(thg=false) is not supported on the device")
         self.r = r
         self.thg = thg
         self.dt = float(t[1] - t[0])

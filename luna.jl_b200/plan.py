@@ -53,6 +53,10 @@ def resp_descs(resp, rho, keep):
                 keep += [x, y, D]
                 d.spl_x, d.spl_y, d.spl_D = _lib.dptr(x), _lib.dptr(y), _lib.dptr(D)
                 d.spl_n = len(x)
+        elif r.kind in ("kerr_field_nothg", "kerr_env_thg") or \
+                (r.kind == "raman_field" and not r.thg):
+            raise NotImplementedError(f"{type(r).__name__}{'' if r.kind != 'raman_field' else '(thg=false)'} "
+                                      "is not available on the device")
         elif r.kind in ("raman_field", "raman_env"):
             d.kind = _lib.RESP_RAMAN
             d.coef = rho

@@ -101,19 +101,40 @@ def plasma(out, E, rho, p):
     out += rho * P
 
 
+def hilbert(x):
+    """Maths.hilbert (Maths.jl:560-569): analytic signal of a real array of even length n:
+    FFT, bins 1..n/2-1 doubled, bins n/2..n-1 zeroed, inverse FFT."""
+    xf = np.fft.fft(x)
+    n1 = len(x) // 2
+    xf[1:n1] *= 2
+    xf[n1:] = 0
+    return np.fft.ifft(xf)
+
+
+def kerr_field_nothg(out, E, rho, g3):
+    """Kerr_field_nothg (Nonlinear.jl:36-45): 3/4 ρ ε0 γ3 |hilbert(E)|² E."""
+    out += rho * 3 / 4 * EPS0 * g3 * np.abs(hilbert(E)) ** 2 * E
+
+
+def kerr_env_thg(out, E, rho, r):
+    """Kerr_env_thg (Nonlinear.jl:75-84): ρ ε0 γ3/4 (3|E|² + exp(2iω0t) E²) E."""
+    out += rho * EPS0 * r.γ3 / 4 * (3 * np.abs(E) ** 2 + r.C * E ** 2) * E
+
+
 def raman_h(resp, rho):
     """CombinedRamanResponse(ht, rho) (Raman.jl:256-262)."""
     return resp.r.h(rho)
 
 
 def raman_field(out, E, rho, resp):
-    """RamanPolarField with thg=true (Nonlinear.jl:282-333) on a 2x zero-padded grid."""
+    """RamanPolarField (Nonlinear.jl:282-333) on a 2x zero-padded grid; E² is
+    1/2 |hilbert(E)|² without third-harmonic generation (sqr!, Nonlinear.jl:267-274)."""
     n = len(E)
     h = np.zeros(2 * n)
     h[:n] = raman_h(resp, rho)
     hw = np.fft.rfft(h)
     E2 = np.zeros(2 * n)
-    E2[:n] = E ** 2
+    E2[:n] = E ** 2 if getattr(resp, "thg", True) else 0.5 * np.abs(hilbert(E)) ** 2
     Pw = hw * np.fft.rfft(E2) * resp.dt
     P = np.fft.irfft(Pw, 2 * n)
     out += rho * E * P[:n]
@@ -140,6 +161,10 @@ def et_to_pt(Et, resp, rho):
             kerr_field(Pt, Et, rho, r.γ3)
         elif r.kind == "kerr_env":
             kerr_env(Pt, Et, rho, r.γ3)
+        elif r.kind == "kerr_field_nothg":
+            kerr_field_nothg(Pt, Et, rho, r.γ3)
+        elif r.kind == "kerr_env_thg":
+            kerr_env_thg(Pt, Et, rho, r)
         elif r.kind == "plasma":
             plasma(Pt, Et, rho, r)
         elif r.kind == "raman_field":

@@ -113,6 +113,59 @@ def test_kerr_field_vs_envelope_low_frequencies():
     a = np.abs(np.fft.rfft(outf))[1799:2400]
     b = np.abs(np.fft.rfft(oute.real))[1799:2400]
     assert isapprox(b, a, 1e-15)
+    # test_kerr.jl:13-16, 27: the no-THG form agrees with the full one there too
+    outn = np.zeros_like(E)
+    uppe.kerr_field_nothg(outn, E, 1.0, 1.0 / pd.eps_0)
+    c = np.abs(np.fft.rfft(outn))[1799:2400]
+    assert isapprox(c, a, 1e-15)
+
+
+def test_kerr_env_thg_is_the_envelope_of_the_field_kerr_term():
+    """Kerr_env_thg (Nonlinear.jl:75-84): for E = Re(A exp(iω0 t)), E³ has the envelope
+    (3|A|²A + exp(2iω0t) A³)/4, so Re(P exp(iω0 t)) reproduces the field-resolved Kerr
+    term exactly (Genty et al., Opt. Express 15, 5382 (2007), Eq. 4)."""
+    from luna_b200.nonlinear import Kerr_env_thg
+    n = 4096
+    t = (np.arange(n) - n / 2) * 2e-16
+    ω0 = 2 * np.pi * pd.c / 800e-9
+    rng = np.random.default_rng(7)
+    A = np.exp(-0.5 * (t / 12e-15) ** 2) * (1 + 0.3 * rng.standard_normal(n)) * np.exp(1j * 0.2 * rng.standard_normal(n))
+    E = (A * np.exp(1j * ω0 * t)).real
+    outf = np.zeros_like(E)
+    uppe.kerr_field(outf, E, 1.0, 1.0 / pd.eps_0)
+    r = Kerr_env_thg(1.0 / pd.eps_0, ω0, t)
+    oute = np.zeros_like(A)
+    uppe.kerr_env_thg(oute, A, 1.0, r)
+    back = (oute * np.exp(1j * ω0 * t)).real
+    assert np.max(np.abs(back - outf)) <= 1e-13 * np.max(np.abs(outf))
+
+
+def test_raman_field_nothg_squares_the_analytic_signal():
+    """sqr! without THG (Nonlinear.jl:267-274) uses 1/2 |hilbert(E)|²: E² minus its
+    second-harmonic part 1/2 Re(hilbert(E)²)."""
+    n = 2048
+    t = (np.arange(n) - n / 2) * 2e-16
+    E = np.exp(-0.5 * (t / 10e-15) ** 2) * np.cos(2 * np.pi * pd.c / 800e-9 * t)
+    A = uppe.hilbert(E)
+    np.testing.assert_allclose(A.real, E, atol=1e-15)
+    np.testing.assert_allclose(0.5 * np.abs(A) ** 2, E ** 2 - 0.5 * (A ** 2).real, atol=1e-15)
+
+
+def test_no_thg_responses_are_described_but_not_on_the_device():
+    """prop_capillary(thg=false) (Interface.jl:534-555) builds Kerr_field_nothg and
+    RamanPolarField(thg=false); the oracle evaluates them, the device plan refuses them."""
+    from luna_b200.interface import prop_capillary_args
+    from luna_b200.plan import resp_descs
+    p = prop_capillary_args(125e-6, 0.1, "H2", 1.0, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
+                            λlims=(150e-9, 4e-6), trange=0.25e-12, thg=False, saveN=5)
+    kinds = [(r.kind, getattr(r, "thg", None)) for r in p.transform.resp]
+    assert ("kerr_field_nothg", None) in kinds and ("raman_field", False) in kinds
+    nl = uppe.trans_mode_avg(p.transform, p.Eω, 0.0)
+    assert np.all(np.isfinite(nl)) and np.linalg.norm(nl) > 0
+    for r in p.transform.resp:
+        if r.kind in ("kerr_field_nothg", "raman_field"):
+            with pytest.raises(NotImplementedError):
+                resp_descs([r], 1.0, [])
 
 
 # ---------------------------------------------------------------- test_raman.jl:9-70

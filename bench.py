@@ -382,6 +382,135 @@ def run_radial(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- modal
+MODAL_METRIC = "modal UPPE RHS evaluations/s (TransModal, radial integral, FP64)"
+MODAL_WORKLOAD = ("modal: HE11 of a 13 µm capillary, Ar 5 bar, Nt=8192/No=16384 over 1 ps (160 nm - 3 µm), "
+                  "800 nm, 30 fs, 1 µJ, 5 cm, Kerr; p-adaptive Clenshaw-Curtis radial integral, "
+                  "reltol 1e-3, 512 evaluations at most")
+
+
+def modal_problem():
+    from luna_b200 import fields, modal, modes
+    from luna_b200.grid import RealGrid
+    from luna_b200.nonlinear import Kerr_field
+    import luna_b200.physdata as pd
+    grid = RealGrid(5e-2, 800e-9, (160e-9, 3000e-9), 1e-12)
+    ms = (modes.MarcatiliMode(13e-6, "Ar", 5.0, n=1, m=1, kind="HE", loss=False),)
+    Eω, t = modal.setup_modal(grid, pd.density("Ar", 5.0), (Kerr_field(pd.gamma3_gas("Ar")),),
+                              fields.GaussField(800e-9, 30e-15, energy=1e-6), ms, "y")
+    return grid, Eω, t, modal.make_const_linop_modes(grid, ms, 800e-9)
+
+
+def modal_cpu_rate(t, Eω, seconds=10.0):
+    """Oracle RHS evaluations per second on one core (bounded sample)."""
+    from oracle import uppe
+    n, t0 = 0, time.perf_counter()
+    while n < 2 or time.perf_counter() - t0 < seconds:
+        uppe.trans_modal(t, Eω, 0.0)
+        n += 1
+    return n / (time.perf_counter() - t0), n
+
+
+def run_modal(args, world, rank, local):
+    """Per-RHS throughput of the modal transform (one bench step = one evaluation of
+    (t::TransModal)(nl, Eω, z) on the Nw x nmodes field), replicas only across GPUs."""
+    grid, Eω, t, L = modal_problem()
+    if args.impl == "reference":
+        if rank == 0:
+            rate, n = modal_cpu_rate(t, Eω)
+            print(json.dumps({"impl": "reference", "metric": MODAL_METRIC, "value": rate, "unit": "RHS/s",
+                              "n_gpus": world, "steps": n, "warmup": 0, "ms_per_step": 1e3 / rate,
+                              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                              "dtype": "f64", "data": "synthetic", "config": {"workload": MODAL_WORKLOAD},
+                              "cpu_baseline": {"value": rate, "unit": "RHS/s", "cores": 1, "kind": "port",
+                                               "sample": f"{n} oracle evaluations (numpy FP64)"},
+                              "e2e": {"value": rate, "unit": "RHS/s", "h2d_bytes_per_step": 0,
+                                      "d2h_bytes_per_step": 0}}), flush=True)
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from luna_b200 import modal_plan as MP
+    lib = _lib.load()
+    plan = t.plan()
+    Nw, nm = Eω.shape
+    Ec = np.ascontiguousarray(Eω.T)
+    dE = torch.from_numpy(Ec.view(np.float64).copy()).cuda()
+    dN = torch.zeros_like(dE)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > L2
+    s = torch.cuda.current_stream()
+    vp = lambda x: _lib.ctypes.c_void_p(x.data_ptr())
+    sp = _lib.ctypes.c_void_p(s.cuda_stream)
+    rhs = lambda: _lib.check(lib.luna_b200_modal_rhs_device(plan.handle, vp(dN), vp(dE), 0.0, sp))
+    for _ in range(args.warmup):
+        rhs()
+    clk = Clocks(local)
+    ts = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        rhs()
+        e1.record(s)
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    clocks = clk.stop()
+    ms = statistics.mean(ts)
+    # end to end through the host-buffer entry point (pinned host memory); it also reports
+    # the number of cubature points the evaluation took
+    Eh = torch.empty(Ec.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    Nh = torch.empty(Ec.shape, dtype=torch.complex128, pin_memory=True).numpy()
+    Eh[:] = Ec
+    nev = _lib.ctypes.c_int(0)
+    call = lambda: _lib.check(lib.luna_b200_modal_rhs(plan.handle, _lib.dptr(Nh.view(np.float64)),
+                                                      _lib.dptr(Eh.view(np.float64)), 0.0,
+                                                      _lib.ctypes.byref(nev)))
+    for _ in range(args.warmup):
+        call()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    # one full propagation (Luna.run with 201 saves)
+    t0 = time.perf_counter()
+    r = MP.run(Eω, grid, L, t, saveN=201)
+    solve_s = time.perf_counter() - t0
+    # algorithmic bytes of one evaluation, per mode, in FP64 complex elements of 16 B: stage
+    # and store kernels read and write Nw twice; the field kernel reads Nw and writes M = No/2
+    # sample pairs; each interior node reads the M pairs and writes M; level l (up to the
+    # last one taken, lv) reads the 2^(l+1)-1 node arrays (level 0 once more for its
+    # midpoint comparison) and writes Nw
+    M = grid.No // 2
+    lv = int(round(np.log2(nev.value - 1))) - 1  # the last level has 2^(lv+1) + 1 points
+    nodes = (2 << lv) - 1
+    level_reads = 1 + sum((2 << l) - 1 for l in range(lv + 1))
+    byts = 16 * nm * (4 * Nw + (Nw + M) + 2 * M * nodes + M * level_reads + Nw * (lv + 1))
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            hpk, pk_kind = float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        hpk, pk_kind = 6650.0, "fallback"
+    ach = byts / (ms / 1e3) / 1e9
+    line = {"metric": MODAL_METRIC, "value": 1e3 / ms, "unit": "RHS/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": MODAL_WORKLOAD, "Nw": Nw, "nmodes": nm, "No": grid.No,
+                       "cubature_points": nev.value, "l2": "256 MB buffer written between timed evaluations"},
+            "e2e": {"value": 1.0 / e2e_s, "unit": "RHS/s", "h2d_bytes_per_step": Eh.nbytes,
+                    "d2h_bytes_per_step": Nh.nbytes},
+            "gpu_launches": (3 + 2 * MP.cubature_levels(t.mfcn)) * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "modal RHS (time, node, level kernels)", "achieved": ach,
+                         "peak": hpk, "unit": "GB/s", "frac": ach / hpk, "traffic": None, "peak_kind": pk_kind,
+                         "note": "algorithmic bytes of the whole evaluation over its duration; launch-bound"},
+            "solve": {"s": solve_s, "rk_steps": int(r.steps), "status": int(r.status)},
+            "clocks": clocks}
+    if not args.no_cpu_baseline:
+        rate, n = modal_cpu_rate(t, Eω)
+        line["cpu_baseline"] = {"value": rate, "unit": "RHS/s", "cores": 1, "kind": "port",
+                                "sample": f"{n} oracle evaluations of the same field (numpy FP64, one core)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -400,12 +529,15 @@ def main():
                     help="oversampled length from which an instance runs distributed (0: library default)")
     ap.add_argument("--no-clusters", action="store_true",
                     help="integrate every instance on one CTA (profiling aid)")
-    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial"],
-                    help="scan256: the batched capillary scan (headline); radial: TransRadial RHS")
+    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial", "modal"],
+                    help="scan256: the batched capillary scan (headline); radial: TransRadial RHS; "
+                         "modal: TransModal RHS")
     args = ap.parse_args()
     world, rank, local = dist_info()
     if args.workload == "radial":
         return run_radial(args, world, rank, local)
+    if args.workload == "modal":
+        return run_modal(args, world, rank, local)
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist

@@ -106,6 +106,42 @@ def test_oracle_pcubature_levels_and_limit():
     assert n3 == 3  # a loose tolerance accepts level 0 (end points are evaluated too)
 
 
+def _device_rule(f, a, rtol, atol, mfcn):
+    """The device's cubature on the host: the tables the plan uploads, level l summed over
+    its slots, compared with level l-1 (the midpoint rule for level 0), accepted as
+    modal_level_kernel accepts it."""
+    nl = modal.cubature_levels(mfcn)
+    r, wts, wlow = modal.cubature_tables(a, nl)
+    g = np.array([f(ri) / (2 * math.pi * ri) for ri in r])  # the tables carry 2πr
+    prev = wlow * g[0]
+    for l in range(nl):
+        cur = np.tensordot(wts[l], g, axes=1)
+        err = np.linalg.norm(cur - prev)
+        if err <= atol or err <= rtol * np.linalg.norm(cur) or l == nl - 1:
+            return cur, (2 << l) + 1
+        prev = cur
+
+
+@pytest.mark.parametrize("rtol,mfcn", [(1e-3, 512), (1e-6, 512), (1e-12, 512), (1e-9, 40)])
+def test_device_rule_reproduces_oracle_pcubature(rtol, mfcn):
+    """The slot tables and the level decisions of the device give the oracle's value and
+    number of evaluations for an integrand that vanishes at the end points like the modal
+    one (a J0² core profile times 2πr, vector-valued)."""
+    a = A
+    u = 2.405
+
+    def f(r):
+        if r <= 0 or r >= a:
+            return np.zeros(3)
+        j = special.jv(0, u * r / a)
+        return 2 * math.pi * r * np.array([j ** 2, j ** 4 * math.cos(7 * r / a), j ** 3 * r / a])
+
+    val, err, nev = uppe.pcubature(f, 0.0, a, rtol, 0.0, mfcn)
+    dval, dnev = _device_rule(f, a, rtol, 0.0, mfcn)
+    assert dnev == nev
+    np.testing.assert_allclose(dval, val, rtol=1e-13, atol=1e-13 * np.abs(val).max())
+
+
 def _radial_case(flength):
     grid = RealGrid(flength, 800e-9, (160e-9, 3000e-9), 1e-12)
     m = modes.MarcatiliMode(A, GAS, PRES, loss=False)

@@ -264,16 +264,35 @@ def kerr_vector(out, E, rho, g3):
     out[:, 1] += fac * s * E[:, 1]
 
 
+def plasma_vector(out, E, rho, p):
+    """PlasmaVector! (Nonlinear.jl:144-162): the rate and ionisation fraction from |E| of
+    the (n, 2) field, the phase, current and polarisation per component."""
+    Em = np.hypot(E[:, 0], E[:, 1])
+    r = rate(p.ratefunc, Em)
+    frac = cumtrapz(r, p.δt)
+    frac = p.preionfrac + 1 - np.exp(-frac)
+    for c in range(2):
+        phase = frac * E_RATIO * E[:, c]
+        J = cumtrapz(phase, p.δt)
+        nz = np.abs(Em) > 0
+        J[nz] += p.ionpot * r[nz] * (1 - frac[nz]) / Em[nz] ** 2 * E[nz, c]
+        out[:, c] += rho * cumtrapz(J, p.δt)
+
+
 def et_to_pt_modal(Er, resp, rho):
     """Et_to_Pt! on the (n, npol) real-space field of one point: scalar responses for one
-    component (Nonlinear.jl:24-34, 164-177 with size(Et, 2) == 1), vector Kerr for two."""
+    component (Nonlinear.jl:24-34, 164-177 with size(Et, 2) == 1), vector Kerr and vector
+    plasma for two."""
     if Er.shape[1] == 1:
         return et_to_pt(Er[:, 0], resp, rho)[:, None]
     Pr = np.zeros_like(Er)
     for r in resp:
-        if r.kind != "kerr_field":
+        if r.kind == "kerr_field":
+            kerr_vector(Pr, Er, rho, r.γ3)
+        elif r.kind == "plasma":
+            plasma_vector(Pr, Er, rho, r)
+        else:
             raise NotImplementedError(r.kind)
-        kerr_vector(Pr, Er, rho, r.γ3)
     return Pr
 
 

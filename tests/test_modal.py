@@ -195,3 +195,28 @@ def test_oracle_modal_single_mode_matches_mode_average():
     Iω = np.abs(r0.Eω) ** 2
     Iωr = np.abs(rm.Eω[:, :, 0]) ** 2
     assert np.linalg.norm(Iω - Iωr) / np.linalg.norm(Iω) < 0.003
+
+
+def test_oracle_vector_plasma_reduces_to_scalar_and_rotates():
+    """PlasmaVector! (Nonlinear.jl:144-162): a field on one component gives the scalar
+    response on it and nothing on the other; rotating the field vector rotates the
+    polarisation (the rate depends on |E| only)."""
+    from luna_b200 import ionisation
+    from luna_b200.nonlinear import PlasmaCumtrapz
+    n = 4096
+    t = (np.arange(n) - n / 2) * 5e-17
+    rate = ionisation.ionrate_PPTaccel("Ar", LAM0, N=2 ** 12)
+    pl = PlasmaCumtrapz(t, t, rate, pd.ionisation_potential("Ar"))
+    E = 2.5e10 * np.exp(-0.5 * (t / 8e-15) ** 2) * np.cos(2 * math.pi * pd.c / LAM0 * t)
+    Pv = np.zeros((n, 2))
+    uppe.plasma_vector(Pv, np.column_stack([E, np.zeros(n)]), 1e25, pl)
+    Ps = np.zeros(n)
+    uppe.plasma(Ps, E, 1e25, pl)
+    assert np.max(np.abs(Ps)) > 0
+    np.testing.assert_allclose(Pv[:, 0], Ps, rtol=0, atol=1e-12 * np.max(np.abs(Ps)))
+    assert np.all(Pv[:, 1] == 0)
+    φ = 0.7
+    Pr = np.zeros((n, 2))
+    uppe.plasma_vector(Pr, np.column_stack([E * math.cos(φ), E * math.sin(φ)]), 1e25, pl)
+    np.testing.assert_allclose(Pr[:, 0], Ps * math.cos(φ), rtol=0, atol=1e-9 * np.max(np.abs(Ps)))
+    np.testing.assert_allclose(Pr[:, 1], Ps * math.sin(φ), rtol=0, atol=1e-9 * np.max(np.abs(Ps)))

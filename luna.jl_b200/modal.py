@@ -14,8 +14,9 @@ on time samples and one forward transform per mode and cubature level gives the 
 see ``modal_plan``. The cubature rule is fixed here on the host: the nested Clenshaw-Curtis
 levels of the p-adaptive rule, their nodes on (0, a) and weights.
 
-Not available: ``full=true`` (the 2-D h-adaptive ``hcubature_v``), envelope grids, Raman
-responses and the vector plasma response (two polarisation components with ionisation).
+Not available on the device: ``full=true`` (the 2-D h-adaptive ``hcubature_v``; the
+transform describes it and the oracle evaluates it), envelope grids, Raman responses and the
+vector plasma response (two polarisation components with ionisation).
 """
 import math
 
@@ -141,9 +142,6 @@ class TransModal:
     kind = "modal"
 
     def __init__(self, grid, ts, resp, density, norm, rtol=1e-3, atol=0.0, mfcn=512, full=False):
-        if full:
-            raise NotImplementedError("the full 2-D modal integral (hcubature) is not available; "
-                                      "use full=False")
         if grid.kind != "real":
             raise NotImplementedError("the modal transform is available for field-resolved grids")
         dl = [m.dimlimits() for m in ts.ms]
@@ -154,7 +152,7 @@ class TransModal:
         self.density = float(density)
         self.norm = np.asarray(norm, dtype=np.complex128)
         self.rtol, self.atol, self.mfcn = float(rtol), float(atol), int(mfcn)
-        self.full = False
+        self.full = bool(full)  # full=true: described (the oracle evaluates it), not on the device
         self.a = dl[0][2][0]
         self._plan = None
 
@@ -170,6 +168,9 @@ class TransModal:
         return ems, wts, wlow
 
     def plan(self):
+        if self.full:
+            raise NotImplementedError("the full 2-D modal integral (hcubature) is not available on "
+                                      "the device; use full=False")
         if self._plan is None:
             from .modal_plan import ModalPlan
             self._plan = ModalPlan.from_transform(self)

@@ -44,6 +44,9 @@ class ModalPlan:
     @classmethod
     def from_transform(cls, t, precision=_lib.PREC_FP64):
         """Descriptors of a ``TransModal`` (NonlinearRHS.jl:203-216, 284-302)."""
+        if t.full:
+            raise NotImplementedError("the full 2-D modal integral (hcubature) is not available on "
+                                      "the device; use full=False")
         g, ts = t.grid, t.ts
         keep = []
         Nw, No, N = len(g.ω), g.No, g.N

@@ -344,21 +344,101 @@ def pcubature(f, lo, hi, rtol, atol, maxevals):
     return I, err, len(cache)
 
 
+# Genz-Malik degree-7 rule with its embedded degree-5 rule in two dimensions (A. C. Genz and
+# A. A. Malik, J. Comput. Appl. Math. 6, 295 (1980)); weights for a region of volume V sum
+# to one: I = V * sum(w f).
+_GM_L2, _GM_L3, _GM_L4, _GM_L5 = math.sqrt(9 / 70), math.sqrt(9 / 10), math.sqrt(9 / 10), math.sqrt(9 / 19)
+_GM_W7 = ((12824 - 9120 * 2 + 400 * 4) / 19683, 980 / 6561, (1820 - 400 * 2) / 19683, 200 / 19683,
+          6859 / 19683 / 4)
+_GM_W5 = ((729 - 950 * 2 + 50 * 4) / 729, 245 / 486, (265 - 100 * 2) / 1458, 25 / 729)
+
+
+def _gm_region(f, c, h):
+    """Integral, error vector and split dimension of the box c ± h (2-D Genz-Malik)."""
+    f0 = f(c[0], c[1])
+    s2, s3, d2, d3 = [], [], [], []
+    for i in range(2):
+        e = [0.0, 0.0]
+        e[i] = 1.0
+        a2 = [f(c[0] + s * _GM_L2 * h[0] * e[0], c[1] + s * _GM_L2 * h[1] * e[1]) for s in (1, -1)]
+        a3 = [f(c[0] + s * _GM_L3 * h[0] * e[0], c[1] + s * _GM_L3 * h[1] * e[1]) for s in (1, -1)]
+        s2.append(a2[0] + a2[1])
+        s3.append(a3[0] + a3[1])
+        # fourth difference along dimension i: the split criterion
+        d = (a2[0] + a2[1] - 2 * f0) - (_GM_L2 / _GM_L3) ** 2 * (a3[0] + a3[1] - 2 * f0)
+        d2.append(float(np.linalg.norm(d)))
+    s4 = sum(f(c[0] + sx * _GM_L4 * h[0], c[1] + sy * _GM_L4 * h[1]) for sx in (1, -1) for sy in (1, -1))
+    s5 = sum(f(c[0] + sx * _GM_L5 * h[0], c[1] + sy * _GM_L5 * h[1]) for sx in (1, -1) for sy in (1, -1))
+    V = 4 * h[0] * h[1]
+    S2, S3 = s2[0] + s2[1], s3[0] + s3[1]
+    I7 = V * (_GM_W7[0] * f0 + _GM_W7[1] * S2 + _GM_W7[2] * S3 + _GM_W7[3] * s4 + _GM_W7[4] * s5)
+    I5 = V * (_GM_W5[0] * f0 + _GM_W5[1] * S2 + _GM_W5[2] * S3 + _GM_W5[3] * s4)
+    split = 0 if d2[0] >= d2[1] else 1
+    return I7, np.abs(I7 - I5), split
+
+
+def hcubature2(f, lo, hi, rtol, atol, maxevals):
+    """Two-dimensional ``Cubature.hcubature_v(fdim, f, lo, hi; reltol, abstol, maxevals,
+    error_norm=Cubature.L2)`` as called at NonlinearRHS.jl:287-293 (full=true). Restated from
+    the published h-adaptive algorithm of the cubature library (Cubature.jl compat 1.5.1,
+    not vendored, unpinned): the regions form a heap on their error norm; while the summed
+    error vector's L2 norm exceeds max(abstol, reltol ||I||) and evaluations remain, the
+    regions with the largest errors are taken until the rest would meet the tolerance, each
+    is bisected along the dimension of largest fourth difference and both halves are
+    evaluated with the 17-point rule. Returns (I, error vector, evaluations)."""
+    import heapq
+    c = [(lo[0] + hi[0]) / 2, (lo[1] + hi[1]) / 2]
+    h = [(hi[0] - lo[0]) / 2, (hi[1] - lo[1]) / 2]
+    I, E, sp = _gm_region(f, c, h)
+    heap = [(-float(np.linalg.norm(E)), 0, c, h, I, E, sp)]
+    nev, uid = 17, 1
+    tot_I, tot_E = I.copy(), E.copy()
+
+    def ok(err, val):
+        n = float(np.linalg.norm(err))
+        return n <= atol or n <= rtol * float(np.linalg.norm(val))
+
+    while not ok(tot_E, tot_I) and (not maxevals or nev < maxevals):
+        take, rest_E = [], tot_E.copy()
+        while heap:
+            item = heapq.heappop(heap)
+            take.append(item)
+            rest_E = rest_E - item[5]
+            if ok(rest_E, tot_I):
+                break
+        for _, _, rc, rh, rI, rE, rsp in take:
+            hh = list(rh)
+            hh[rsp] /= 2
+            for s in (-1, 1):
+                cc = list(rc)
+                cc[rsp] += s * hh[rsp]
+                I2, E2, sp2 = _gm_region(f, cc, hh)
+                nev += 17
+                heapq.heappush(heap, (-float(np.linalg.norm(E2)), uid, cc, hh, I2, E2, sp2))
+                uid += 1
+        # totals summed afresh over the regions (in creation order), not updated in place
+        regs = sorted(heap, key=lambda q: q[1])
+        tot_I = sum(q[4] for q in regs)
+        tot_E = sum(q[5] for q in regs)
+    return tot_I, tot_E, nev
+
+
 def trans_modal(t, Ew, z):
-    """(t::TransModal)(nl, Eω, z) with full=false (NonlinearRHS.jl:234-302) for a
-    field-resolved grid: Ew is (Nω, nmodes). Per point r: to_space! (Modes.jl:458-495) at
-    (r, 0), to_time!, Et_to_Pt!, towin, to_freq!, ωwin, norm!, projection onto the modes
-    (Prω Emsᵀ) and the weight 2πr; points on or outside (0, a) give zero."""
+    """(t::TransModal)(nl, Eω, z) (NonlinearRHS.jl:234-302) for a field-resolved grid: Ew is
+    (Nω, nmodes). Per point: to_space! (Modes.jl:458-495), to_time!, Et_to_Pt!, towin,
+    to_freq!, ωwin, norm!, projection onto the modes (Prω Emsᵀ) and the weight (2πr at
+    θ = 0 for full=false, r over (r, θ) for full=true); points on or outside (0, a) give
+    zero."""
     g, ts = t.grid, t.ts
     Nw = Ew.shape[0]
     Nwo = len(g.ωo)
     lo, hi = 0.0, t.a
     of = g.ωwin * t.norm
 
-    def point(r):
+    def point(r, θ=0.0):
         if r <= lo or r >= hi:
             return np.zeros_like(Ew)
-        Ems = ts.ems(r)                                  # (nmodes, npol)
+        Ems = ts.ems(r, θ)                               # (nmodes, npol)
         Erω = Ew @ Ems                                   # (Nω, npol)
         Erωo = np.zeros((Nwo, Erω.shape[1]), dtype=np.complex128)
         Erωo[:Nw] = ((Nwo - 1) / (Nw - 1)) * Erω
@@ -368,7 +448,14 @@ def trans_modal(t, Ew, z):
         Prω = Prω * of[:, None]
         return 2 * math.pi * r * (Prω @ Ems.T)           # (Nω, nmodes)
 
-    val, err, nev = pcubature(point, lo, hi, t.rtol, t.atol, t.mfcn)
+    if getattr(t, "full", False):
+        def point2(r, θ):
+            if r <= lo or r >= hi:
+                return np.zeros_like(Ew)
+            return point(r, θ) / (2 * math.pi)    # weight r (polar), not 2πr
+        val, err, nev = hcubature2(point2, (lo, 0.0), (hi, 2 * math.pi), t.rtol, t.atol, t.mfcn)
+    else:
+        val, err, nev = pcubature(point, lo, hi, t.rtol, t.atol, t.mfcn)
     t.oracle_nevals = nev
     return val
 

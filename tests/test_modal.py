@@ -174,11 +174,68 @@ def test_modal_linop_matches_single_mode_on_sidx():
     np.testing.assert_allclose(Lm[~s, 0], 1j * (-1 + grid.ω[~s] * β1))
 
 
-def test_transmodal_rejects_full_and_envelope():
+def test_transmodal_full_is_described_but_not_on_the_device():
     grid, m, dens, resp, inp = _radial_case(1e-2)
     ts = modal.ToSpace((m,), components="y")
+    t = modal.TransModal(grid, ts, resp, dens, modal.norm_modal(grid), full=True)
+    assert t.full
     with pytest.raises(NotImplementedError):
-        modal.TransModal(grid, ts, resp, dens, modal.norm_modal(grid), full=True)
+        t.plan()
+
+
+def test_oracle_hcubature2_integrates_and_adapts():
+    """The restated 2-D h-adaptive rule: the 17-point Genz-Malik rule is exact for degree 7,
+    and a peaked integrand is refined to the tolerance."""
+    f = lambda x, y: np.array([x ** 3 * y ** 4 + x * y + 1.0])
+    v, e, n = uppe.hcubature2(f, (0.0, 0.0), (1.0, 2.0), 1.0, 0.0, 1000)
+    assert n == 17 and v[0] == pytest.approx(2 ** 5 / 20 + 1.0 + 2.0, rel=1e-14)
+    assert e[0] > 0  # the degree-5 comparison is not exact for degree 7
+    g = lambda x, y: np.array([math.exp(-50 * ((x - 0.3) ** 2 + (y - 0.6) ** 2)),
+                               math.cos(3 * x) * math.sin(2 * y)])
+    ref = [integrate.dblquad(lambda y, x: g(x, y)[i], 0, 1, 0, 1, epsabs=0, epsrel=1e-12)[0] for i in range(2)]
+    v, e, n = uppe.hcubature2(g, (0.0, 0.0), (1.0, 1.0), 1e-8, 0.0, 100000)
+    assert np.linalg.norm(v - ref) <= 1e-7 * np.linalg.norm(ref) and n > 17
+    v2, e2, n2 = uppe.hcubature2(g, (0.0, 0.0), (1.0, 1.0), 1e-14, 0.0, 200)
+    assert n2 <= 200 + 2 * 17 * 12  # stops once the evaluations exceed the limit
+
+
+def _lp11_he11(full, name):
+    """test_multimode.jl:178-213 ("Nonlinear coupling"): TM01 + HE21(ϕ = -π/4) (vertical LP11)
+    and HE11 in a 125 µm capillary with Ar at 0.167 bar, 10 fs, 150 µJ, energy in LP11 only."""
+    a, gas, pres, λ0 = 125e-6, "Ar", 0.167, 800e-9
+    ms = (modes.MarcatiliMode(a, gas, pres, n=0, m=1, kind="TM", ϕ=0.0),
+          modes.MarcatiliMode(a, gas, pres, n=2, m=1, kind="HE", ϕ=-math.pi / 4),
+          modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=0.0))
+    grid = RealGrid(3.0, λ0, (160e-9, 3000e-9), 0.4e-12)
+    f = fields.GaussField(λ0, 10e-15, energy=150e-6 / 2)
+    Eω, t = modal.setup_modal(grid, pd.density(gas, pres), (Kerr_field(pd.gamma3_gas(gas)),),
+                              ({"mode": 1, "fields": (f,)}, {"mode": 2, "fields": (f,)}), ms, name,
+                              full=full)
+    return Eω, t
+
+
+def test_oracle_full_lp11_does_not_couple_to_he11():
+    """test_multimode.jl:178-213 with full=true: the nonlinear polarisation of LP11 has no
+    HE11 component (sin³θ integrates to zero over θ): norm(|nl3|²) / norm(|nl12|²) < 1e-32,
+    the reference's bound (the oracle gives 4.8e-33 with 527 evaluations)."""
+    Eω, t = _lp11_he11(True, "xy")
+    nl = uppe.trans_modal(t, Eω, 0.0)
+    Inl12 = np.sum(np.abs(nl[:, :2]) ** 2, axis=1)
+    Inl3 = np.abs(nl[:, 2]) ** 2
+    assert np.linalg.norm(Inl12) > 0
+    assert np.linalg.norm(Inl3) / np.linalg.norm(Inl12) < 1e-32
+
+
+def test_oracle_full_matches_radial_for_he11():
+    """For HE11 alone the integrand does not depend on θ, so the full 2-D integral and the
+    radial one agree to the cubature tolerance (test_multimode.jl "Full" vs "Radial")."""
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    ms = (modes.MarcatiliMode(A, GAS, PRES, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
+    Eω, tr = modal.setup_modal(grid, dens, resp, inp, ms, "y")
+    _, tf = modal.setup_modal(grid, dens, resp, inp, ms, "y", full=True)
+    nr = uppe.trans_modal(tr, Eω, 0.0)
+    nf = uppe.trans_modal(tf, Eω, 0.0)
+    assert np.linalg.norm(nf - nr) / np.linalg.norm(nr) < 1e-4  # 2.1e-6 (17 vs 51 points)
 
 
 def test_oracle_modal_single_mode_matches_mode_average():

@@ -3,8 +3,10 @@
 ``prop_gnlse_args`` (Interface.jl:921-979) and ``prop_capillary_args``
 (Interface.jl:360-401) build the grid, linear operator, responses, transform and
 initial field exactly as the reference does, for the configurations this package
-supports: single-mode mode-averaged propagation with a constant fill. ``prop_gnlse``
-and ``prop_capillary`` then integrate on the GPU (``Luna.run``, Luna.jl:358-391).
+supports: mode-averaged propagation (constant fill, pressure gradients, tapers) and, with
+``modes`` a number or a tuple of modes, multimode propagation with the modal transform
+(constant fill). ``prop_gnlse`` and ``prop_capillary`` then integrate on the GPU
+(``Luna.run``, Luna.jl:358-391).
 """
 import math
 
@@ -62,14 +64,70 @@ def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=No
 _raman = raman
 
 
+def parse_mode(mode):
+    """``parse_mode`` (Interface.jl:464-476): "HE11" -> {kind: "HE", n: 1, m: 1}."""
+    if isinstance(mode, dict):
+        return mode
+    ms = str(mode).lstrip(":")
+    if len(ms) > 4:
+        raise ValueError(f"Ambiguous mode designation {mode}. Pass modes as dicts to disambiguate, "
+                         "e.g. {'kind': 'HE', 'n': 1, 'm': 12}.")
+    return {"kind": ms[:2], "n": int(ms[2]), "m": int(ms[3])}
+
+
+def needpol_modes(modes_):
+    """``needpol_modes`` (Interface.jl:439-446): two components unless only HE1m modes."""
+    if isinstance(modes_, (str, int, dict)):
+        return False
+    return any(parse_mode(m)["kind"] != "HE" or parse_mode(m)["n"] > 1 for m in modes_)
+
+
+def makemode_s(modes_, radius, gas, pressure, T, model, loss, pol):
+    """``makemode_s`` / ``makemodes_pol`` (Interface.jl:478-513) for a constant fill: a mode
+    name gives one mode; a number n gives HE11..HE1n; a tuple gives each of its modes; with
+    two components every HE1m mode comes twice (ϕ = 0 and π/2)."""
+    def one(md):
+        md = parse_mode(md)
+        kw = dict(n=md["n"], m=md["m"], kind=md["kind"], T=T, model=model, loss=loss)
+        if pol:
+            if md["kind"] == "HE" and md["n"] == 1:
+                return [modes.MarcatiliMode(radius, gas, pressure, ϕ=0.0, **kw),
+                        modes.MarcatiliMode(radius, gas, pressure, ϕ=math.pi / 2, **kw)]
+            return [modes.MarcatiliMode(radius, gas, pressure, ϕ=0.0, **kw)]
+        return modes.MarcatiliMode(radius, gas, pressure, **kw)
+
+    if isinstance(modes_, int):
+        modes_ = tuple({"kind": "HE", "n": 1, "m": m} for m in range(1, modes_ + 1))
+    if isinstance(modes_, (tuple, list)):
+        out = []
+        for md in modes_:
+            r = one(md)
+            out += r if isinstance(r, list) else [r]
+        return out
+    return one(modes_)
+
+
+def needfull(ms):
+    """``needfull`` (Interface.jl:801-803): the 2-D integral unless every mode is HE1m."""
+    return not all(m.kind == "HE" and m.n == 1 for m in ms)
+
+
 def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, τfwhm=None,
                         energy=None, power=None, pulseshape="gauss", shotnoise=False,
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
-                        raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16):
-    """Mode-averaged HE11 capillary set-up (Interface.jl:360-401). ``pressure`` is a number,
-    a (p0, p1) gradient over the fibre or (Z, P) nodes (Capillary.gradient,
-    Capillary.jl:306-337); ``radius`` is a number or (Z, A) nodes of a piecewise-linear taper
-    (a z-dependent radius, Interface.jl:249-250)."""
+                        raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
+                        modes="HE11", radial_integral_rtol=1e-3):
+    """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
+    over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
+    a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
+    Interface.jl:249-250). ``modes`` (Interface.jl:478-513, 805-820): a mode name (e.g.
+    "HE11", the default) gives mode-averaged propagation in that mode; a number n
+    (HE11..HE1n) or a tuple of names gives multimode propagation with ``modal.TransModal``,
+    linearly polarised input in the first mode, the radial integral when every mode is HE1m
+    (the device runs it) and the full 2-D integral otherwise (described, evaluated by the
+    oracle only); constant fill only."""
+    modes_ = modes
+    from . import modes
     if shotnoise:
         raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
     if envelope:
@@ -77,11 +135,18 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     plasma = (not envelope) if plasma is None else plasma
     thg = (not envelope) if thg is None else thg
     grid = RealGrid(flength, λ0, λlims, trange, δt)
+    if not isinstance(modes_, str) or parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
+        if isinstance(modes_, (int, tuple, list)):
+            return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
+                                         energy, power, pulseshape, thg, kerr, plasma, raman, loss,
+                                         model, saveN, ppt_N, radial_integral_rtol)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
         # pressure gradient (p0, p1) or (Z, P) (Interface.jl:495-504, 524-531) and/or a
         # z-dependent radius (Interface.jl:249-250), given here as nodes (Z, A)
+        if parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
+            raise NotImplementedError("pressure gradients and tapers are supported for HE11 only")
         from .gradient import Gradient, MarcatiliGradientMode, Taper
         if not isinstance(pressure, (tuple, list)):
             grad = Gradient(gas, flength, pressure, pressure)
@@ -94,7 +159,9 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         mode = MarcatiliGradientMode(radius, grad, model=model, loss=loss)
         density = grad.density(0.0)
     else:
-        mode = modes.MarcatiliMode(radius, gas, pressure, model=model, loss=loss)
+        md = parse_mode(modes_)
+        mode = modes.MarcatiliMode(radius, gas, pressure, n=md["n"], m=md["m"], kind=md["kind"],
+                                   model=model, loss=loss)
         density = pd.density(gas, pressure)
     resp = []
     if kerr:
@@ -133,3 +200,39 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
     Eω = fld(grid)
     return Problem(Eω, grid, linop, transform, saveN)
+
+
+def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
+                          pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol):
+    """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
+    linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
+    (``makeinputs``, Interface.jl:721-733)."""
+    from . import modal
+    if isinstance(pressure, (tuple, list)) or isinstance(radius, (tuple, list)):
+        raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
+    pol = needpol_modes(modes_)
+    ms = makemode_s(modes_, radius, gas, pressure, pd.roomtemp, model, loss, pol)
+    thg = True if thg is None else thg
+    plasma = True if plasma is None else plasma
+    resp = []
+    if kerr:
+        resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
+                    Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
+    if plasma:
+        ionpot = pd.ionisation_potential(gas)
+        if gas in ("H2", "D2", "N2O", "CH4", "SF6"):
+            rate = ionrate_fun_ADK(gas)
+        else:
+            rate = ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
+        resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, ionpot))
+    if raman is None:
+        raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
+    if raman:
+        resp.append(RamanPolarField(grid.to, _raman.raman_response(grid.to, gas), thg=thg))
+    if pulseshape == "gauss":
+        fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
+    else:
+        fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
+    Eω, t = modal.setup_modal(grid, pd.density(gas, pressure), resp, fld, ms, "xy" if pol else "y",
+                              full=needfull(ms), rtol=rtol)
+    return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0), t, saveN)

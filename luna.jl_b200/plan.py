@@ -333,8 +333,13 @@ def solve_precon(transform, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, ato
 
 
 def run(problem, precision=_lib.PREC_FP64, **kw):
-    """Luna.run (Luna.jl:358-391) on the GPU for a ``Problem`` from the interface module."""
+    """Luna.run (Luna.jl:358-391) on the GPU for a ``Problem`` from the interface module
+    (a multimode problem goes to the modal solver)."""
     g = problem.grid
+    if getattr(problem.transform, "kind", "") == "modal":
+        from . import modal_plan
+        return modal_plan.run(problem.Eω, g, problem.linop, problem.transform, saveN=problem.saveN,
+                              precision=precision, **kw)
     kw.setdefault("max_dt", g.zmax / 2)
     return solve_precon(problem.transform, problem.linop, problem.Eω, 0.0, 1e-4, g.zmax,
                         saveN=problem.saveN, precision=precision, **kw)

@@ -277,3 +277,32 @@ def test_oracle_vector_plasma_reduces_to_scalar_and_rotates():
     uppe.plasma_vector(Pr, np.column_stack([E * math.cos(φ), E * math.sin(φ)]), 1e25, pl)
     np.testing.assert_allclose(Pr[:, 0], Ps * math.cos(φ), rtol=0, atol=1e-9 * np.max(np.abs(Ps)))
     np.testing.assert_allclose(Pr[:, 1], Ps * math.sin(φ), rtol=0, atol=1e-9 * np.max(np.abs(Ps)))
+
+
+def test_prop_capillary_modes_keyword():
+    """prop_capillary(...; modes) (Interface.jl:360-401, 478-513, 805-820): a number gives
+    HE11..HE1n on one component with the radial integral and the input pulse in HE11 (the
+    mode-averaged input field); a tuple with other kinds needs both components (HE1m twice,
+    ϕ = 0 and π/2) and the full 2-D integral; another mode name stays mode-averaged."""
+    from luna_b200.interface import parse_mode, prop_capillary_args
+    kw = dict(λ0=800e-9, τfwhm=10e-15, energy=50e-6, λlims=(150e-9, 4e-6), trange=0.25e-12, saveN=5)
+    p1 = prop_capillary_args(125e-6, 0.1, "Ar", 1.0, **kw)
+    p3 = prop_capillary_args(125e-6, 0.1, "Ar", 1.0, modes=3, **kw)
+    t = p3.transform
+    assert t.kind == "modal" and not t.full and t.ts.npol == 1 and p3.Eω.shape[1] == 3
+    assert [(m.kind, m.n, m.m) for m in t.ts.ms] == [("HE", 1, 1), ("HE", 1, 2), ("HE", 1, 3)]
+    assert np.array_equal(p3.Eω[:, 0], p1.Eω) and not np.any(p3.Eω[:, 1:])
+    assert [r.kind for r in t.resp] == ["kerr_field", "plasma"]
+    nl = uppe.rhs(t, p3.Eω, 0.0)
+    assert np.all(np.isfinite(nl)) and np.all(np.linalg.norm(nl, axis=0) > 0)
+    px = prop_capillary_args(125e-6, 0.1, "Ar", 1.0, modes=("HE11", "TE01"), **kw)
+    tx = px.transform
+    assert tx.full and tx.ts.npol == 2
+    assert [(m.kind, m.n, m.m, m.ϕ) for m in tx.ts.ms] == [("HE", 1, 1, 0.0), ("HE", 1, 1, math.pi / 2),
+                                                          ("TE", 0, 1, 0.0)]
+    ph = prop_capillary_args(125e-6, 0.1, "Ar", 1.0, modes="HE12", **kw)
+    assert getattr(ph.transform, "kind", "modeavg") != "modal"
+    assert ph.transform.aeff == pytest.approx(modes.MarcatiliMode(125e-6, "Ar", 1.0, n=1, m=2).Aeff())
+    assert parse_mode("TM01") == {"kind": "TM", "n": 0, "m": 1}
+    with pytest.raises(ValueError):
+        parse_mode("HE112")

@@ -340,3 +340,25 @@ def test_oracle_vector_plasma_reference_property():
     rtol = math.sqrt(np.finfo(float).eps)
     assert np.linalg.norm(Is - Iv) <= rtol * np.linalg.norm(Is)
     assert np.linalg.norm(Is - I45) <= rtol * np.linalg.norm(Is)
+
+
+def test_oracle_linear_polarisation_at_45_degrees_reference_property():
+    """test_polarisation_field.jl:4-62 ("Linear") with the radial integral on 1 cm: HE11 on
+    one component and the same energy split over HE11 at ϕ = 0 and π/2 (two components,
+    vector Kerr) give the same total spectrum, within the reference's 1.07e-12."""
+    a, gas, pres, τ, λ0, energy = 13e-6, "Ar", 5.0, 30e-15, 800e-9, 1e-6
+    grid = RealGrid(1e-2, λ0, (160e-9, 3000e-9), 1e-12)
+    dens = pd.density(gas, pres)
+    resp = (Kerr_field(pd.gamma3_gas(gas)),)
+    m1 = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
+    E1, t1 = modal.setup_modal(grid, dens, resp, fields.GaussField(λ0, τ, energy=energy), m1, "y")
+    r1 = uppe.run(t1, grid, modal.make_const_linop_modes(grid, m1, λ0), E1, saveN=2)
+    m2 = m1 + (modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=math.pi / 2, loss=False),)
+    h = fields.GaussField(λ0, τ, energy=energy / 2)
+    E2, t2 = modal.setup_modal(grid, dens, resp, ({"mode": 1, "fields": (h,)}, {"mode": 2, "fields": (h,)}),
+                               m2, "xy")
+    r2 = uppe.run(t2, grid, modal.make_const_linop_modes(grid, m2, λ0), E2, saveN=2)
+    I1 = np.abs(r1.Eω[-1][:, 0]) ** 2
+    I2 = np.sum(np.abs(r2.Eω[-1]) ** 2, axis=1)
+    assert r1.steps == r2.steps
+    assert np.linalg.norm(I1 - I2) / np.linalg.norm(I1) < 1.07e-12

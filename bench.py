@@ -11,9 +11,10 @@ per hour per GPU (completed instances / step time).
   value   device time of the solver launches, inputs already resident in HBM (CUDA events)
   e2e     the same step through the C ABI with host buffers: H2D of every instance's
           linear operator and input field, the launch, D2H of all 201 saved spectra
-  cpu_baseline / --impl reference: the FP64 numpy restatement of the reference algorithm
-          timed per RK step on a bounded sample of the scan, extrapolated with the
-          reference step counts of every instance
+  cpu_baseline / --impl reference: the FP64 C++ restatement of the reference algorithm
+          (oracle/uppe_cpu.cpp, checked against the numpy one) timed per RK step on a
+          bounded sample of the scan, extrapolated with the reference RHS counts of every
+          instance
 
 Multi-GPU (torchrun): each rank integrates a cost-balanced shard of a 256*N-instance scan
 (weak scaling, no collective on the data path; the timing uses a max over ranks).
@@ -136,13 +137,30 @@ def build(world, rank, n_per_rank):
 
 # ----------------------------------------------------------------------------- CPU side
 def _oracle_sample(args):
-    """Time `nsteps` oracle RK steps of one scan instance (FP64 numpy, one core)."""
+    """Time RK steps of one scan instance on one core with the FP64 C++ restatement of the
+    reference algorithm (oracle/uppe_cpu.cpp, the same steps as the numpy restatement),
+    or the numpy restatement when the C++ library is not there. Returns (instance, RHS
+    evaluations, seconds, RK steps, which restatement)."""
     idx, budget = args
     import luna_b200_loader as L
     L.load()
     from luna_b200 import scan as S
     from oracle import uppe
     p = S.build_problem(S.draw_instances()[idx])
+    try:
+        from oracle import cpu
+        cp = cpu.CpuPlan(p.transform)
+    except Exception:
+        cp = None
+    if cp is not None:
+        zmax = p.grid.zmax
+        t0 = time.perf_counter()
+        _, _, st = cp.solve(p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=2, max_steps=5)
+        per_step = (time.perf_counter() - t0) / max(st.steps, 1)
+        nsteps = int(min(max(5, budget / per_step), 10 ** 6))
+        t0 = time.perf_counter()
+        _, _, st = cp.solve(p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=2, max_steps=nsteps)
+        return idx, st.nrhs, time.perf_counter() - t0, st.steps, "C++"
     f = lambda y, z: uppe.trans_mode_avg(p.transform, y, z)
     st = uppe.PreconStepper(f, p.linop, p.Eω, 0.0, 1e-4, max_dt=p.grid.zmax / 2)
     nrhs0 = st.nrhs
@@ -155,7 +173,7 @@ def _oracle_sample(args):
     except ValueError:
         pass
     dt = time.perf_counter() - t0
-    return idx, st.nrhs - nrhs0, dt, done
+    return idx, st.nrhs - nrhs0, dt, done, "numpy"
 
 
 def cpu_estimate(sample_seconds=20.0, workers=1):
@@ -177,6 +195,11 @@ def cpu_estimate(sample_seconds=20.0, workers=1):
     # about sample_seconds of CPU work in total: RK steps per class until the class's
     # share of the time is used (at least 3)
     jobs = [(i, sample_seconds / len(reps)) for i in reps]
+    try:  # compile the C++ restatement once, before any worker loads it
+        from oracle import cpu
+        cpu.build()
+    except Exception:
+        pass
     t0 = time.perf_counter()
     if workers > 1:
         import multiprocessing as mp
@@ -186,12 +209,13 @@ def cpu_estimate(sample_seconds=20.0, workers=1):
         res = [_oracle_sample(j) for j in jobs]
     wall = time.perf_counter() - t0
     per_rhs = {}
-    for i, nr, dt, done in res:
+    for i, nr, dt, done, _ in res:
         per_rhs[cls[i]] = dt / max(nr, 1)
     total = sum(per_rhs[cls[i]] * nrhs[i] for i in range(len(nrhs)))
     ok = int(np.sum(status == 0))
     sims_per_hour_core = 3600.0 * ok / total
     return sims_per_hour_core, {"classes": len(classes), "rk_steps_each": [r[3] for r in res],
+                                "impl": "FP64 C++" if all(r[4] == "C++" for r in res) else "FP64 numpy",
                                 "sample_wall_s": round(wall, 1),
                                 "per_rhs_ms": {f"No={k[0]}{'+Raman' if k[1] else ''}": round(v * 1e3, 2)
                                                for k, v in per_rhs.items()}}
@@ -251,7 +275,8 @@ def run_reference(args, world, rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "instances": 256, "saveN": SAVEN},
             "cpu_baseline": {"value": value, "unit": "sims/hour", "cores": cores, "kind": "port",
-                             "sample": f"FP64 numpy oracle, {info['rk_steps_each']} RK steps per grid class "
+                             "sample": f"{info['impl']} restatement of the reference algorithm, "
+                                       f"{info['rk_steps_each']} RK steps per grid class "
                                        f"({info['classes']} classes) in parallel on {cores} cores, "
                                        "scaled by each instance's reference RHS count"},
             "e2e": {"value": value, "unit": "sims/hour", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -673,7 +698,7 @@ def main():
             try:
                 v1, info = cpu_estimate(workers=1)
                 line["cpu_baseline"] = {"value": v1, "unit": "sims/hour", "cores": 1, "kind": "port",
-                                        "sample": f"FP64 numpy oracle, {info['rk_steps_each']} RK steps of one instance per grid class ({info['classes']} classes, {info['sample_wall_s']} s), scaled by each instance's reference RHS count",
+                                        "sample": f"{info['impl']} restatement of the reference algorithm, {info['rk_steps_each']} RK steps of one instance per grid class ({info['classes']} classes, {info['sample_wall_s']} s), scaled by each instance's reference RHS count",
                                         "per_rhs_ms": info["per_rhs_ms"]}
             except Exception as e:  # report, do not hide
                 line["cpu_baseline"] = {"value": None, "error": str(e)[:200]}

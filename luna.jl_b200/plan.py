@@ -104,40 +104,11 @@ class Plan:
 
     @classmethod
     def from_transform(cls, t, precision=_lib.PREC_FP64):
-        g = t.grid
-        keep = []
-        Nw = len(g.ω)
-        N, No = g.N, g.No
-        if g.kind == "real":
-            Nwo = len(g.ωo)
-            pad = (Nwo - 1) / (Nw - 1)
-            crop = (Nw - 1) / (Nwo - 1)
-            kind = 0
-        else:
-            pad = No / Nw
-            crop = Nw / No
-            kind = 1
-        zdep = getattr(t, "kind", "") == "modeavg_z"
-        # a pressure gradient scales the output by ρ(z) pre/β(z) on the device
-        outfac = _c128(np.full(Nw, crop, dtype=np.complex128) if zdep else crop * t.output_factor())
-        wwin, towin, twin = _f64(g.ωwin), _f64(g.towin), _f64(g.twin)
-        keep += [outfac, wwin, towin, twin]
-        gd = _lib.GridDesc()
-        gd.kind, gd.N, gd.Nw, gd.No = kind, N, Nw, No
-        gd.outfac = _lib.dptr(outfac.view(np.float64))
-        gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
-        gd.in_scale = pad / No / (nlscale * math.sqrt(t.aeff))
-        # per-step statistics (Stats.default): grid axes, Aeff and the field scale
-        om, tt = _f64(g.ω), _f64(g.t)
-        keep += [om, tt]
-        gd.omega, gd.t = _lib.dptr(om), _lib.dptr(tt)
-        gd.aeff = t.aeff
-        gd.escale = 1.0 / math.sqrt(pd.eps_0 * pd.c * t.aeff / 2)
-        rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep)
+        gd, rds, keep, Nw, zdep, crop, pad = transform_descs(t)
         plan = cls(gd, rds, keep, precision, Nw)
         if zdep:
             from .gradient import gradient_desc
-            gdesc = gradient_desc(t, crop, pad / No, plan._keep)
+            gdesc = gradient_desc(t, crop, pad / t.grid.No, plan._keep)
             plan._gdesc = gdesc
             _lib.check(_lib.load().luna_b200_plan_set_gradient(plan.handle, _lib.ctypes.byref(gdesc)))
         return plan
@@ -150,6 +121,43 @@ class Plan:
         _lib.check(_lib.load().luna_b200_rhs(self._h, _lib.dptr(nl.view(np.float64)),
                                              _lib.dptr(Ew.view(np.float64)), float(z)))
         return nl
+
+
+def transform_descs(t):
+    """C-ABI descriptors of a mode-averaged transform (NonlinearRHS.jl:344-399): the grid
+    descriptor, the response descriptors and the arrays they point to, plus (Nw, whether a
+    pressure gradient makes the transform z-dependent, crop and pad scales)."""
+    g = t.grid
+    keep = []
+    Nw = len(g.ω)
+    N, No = g.N, g.No
+    if g.kind == "real":
+        Nwo = len(g.ωo)
+        pad = (Nwo - 1) / (Nw - 1)
+        crop = (Nw - 1) / (Nwo - 1)
+        kind = 0
+    else:
+        pad = No / Nw
+        crop = Nw / No
+        kind = 1
+    zdep = getattr(t, "kind", "") == "modeavg_z"
+    # a pressure gradient scales the output by ρ(z) pre/β(z) on the device
+    outfac = _c128(np.full(Nw, crop, dtype=np.complex128) if zdep else crop * t.output_factor())
+    wwin, towin, twin = _f64(g.ωwin), _f64(g.towin), _f64(g.twin)
+    keep += [outfac, wwin, towin, twin]
+    gd = _lib.GridDesc()
+    gd.kind, gd.N, gd.Nw, gd.No = kind, N, Nw, No
+    gd.outfac = _lib.dptr(outfac.view(np.float64))
+    gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
+    gd.in_scale = pad / No / (nlscale * math.sqrt(t.aeff))
+    # per-step statistics (Stats.default): grid axes, Aeff and the field scale
+    om, tt = _f64(g.ω), _f64(g.t)
+    keep += [om, tt]
+    gd.omega, gd.t = _lib.dptr(om), _lib.dptr(tt)
+    gd.aeff = t.aeff
+    gd.escale = 1.0 / math.sqrt(pd.eps_0 * pd.c * t.aeff / 2)
+    rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep)
+    return gd, rds, keep, Nw, zdep, crop, pad
 
 
 def make_opts(saveN, zsave, rtol=1e-6, atol=1e-10, safety=0.9, max_dt=math.inf, min_dt=0.0,

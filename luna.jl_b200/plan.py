@@ -321,14 +321,17 @@ _STATUS_MSG = {
 def solve_precon(transform, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, atol=1e-10,
                  safety=0.9, max_dt=math.inf, min_dt=0.0, repeat_limit=10, max_steps=200000,
                  steplog_cap=0, precision=_lib.PREC_FP64, raise_on_status=True, replay=None,
-                 stats_cap=0):
+                 stats_cap=0, zsave=None):
     """RK45.solve_precon (RK45.jl:19-25) with Luna.run's window filter and saves, on the GPU.
 
-    ``replay`` (optional, flat (dz, accepted) pairs) makes the integrator follow a given
-    step sequence instead of its controller's choices; it is a verification aid.
+    Saves are taken at ``saveN`` points on [z0, zmax], or at the points ``zsave`` (a
+    resumed propagation keeps the save grid of the whole fibre). ``replay`` (optional,
+    flat (dz, accepted) pairs) makes the integrator follow a given step sequence instead of
+    its controller's choices; it is a verification aid.
     """
     plan = transform.plan() if precision == _lib.PREC_FP64 else Plan.from_transform(transform, precision)
-    zs = np.linspace(z0, zmax, saveN)
+    zs = np.linspace(z0, zmax, saveN) if zsave is None else np.asarray(zsave, dtype=np.float64)
+    saveN = len(zs)
     b = Batch([plan], saveN, zs, rtol=rtol, atol=atol, safety=safety, max_dt=max_dt,
               min_dt=min_dt, repeat_limit=repeat_limit, max_steps=max_steps,
               steplog_cap=steplog_cap, replay=replay, stats_cap=stats_cap)

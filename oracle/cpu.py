@@ -89,17 +89,19 @@ class CpuPlan:
         return nl
 
     def solve(self, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, atol=1e-10, safety=0.9,
-              max_dt=None, min_dt=0.0, repeat_limit=10, max_steps=0):
-        """Luna.run with RK45.solve_precon; returns (saves[nsaved, Nw], y, stats)."""
+              max_dt=None, min_dt=0.0, repeat_limit=10, max_steps=0, zsave=None):
+        """Luna.run with RK45.solve_precon; saves at saveN points on [z0, zmax] or at
+        ``zsave``; returns (saves[nsaved, Nw], y, stats)."""
         from luna_b200 import _lib as L
         from luna_b200.plan import make_opts
-        zs = np.linspace(z0, zmax, saveN)
+        zs = np.linspace(z0, zmax, saveN) if zsave is None else np.asarray(zsave, dtype=np.float64)
+        saveN = len(zs)
         o = make_opts(saveN, zs, rtol=rtol, atol=atol, safety=safety,
                       max_dt=(zmax / 2 if max_dt is None else max_dt), min_dt=min_dt,
                       repeat_limit=repeat_limit, max_steps=max_steps)
         Lc = np.ascontiguousarray(linop, dtype=np.complex128)
         y = np.array(Eω, dtype=np.complex128, copy=True)
-        saves = np.zeros((saveN, self.Nw), dtype=np.complex128)
+        saves = np.zeros((max(saveN, 1), self.Nw), dtype=np.complex128)
         st = L.SolveStats()
         load().uo_solve(self._h, L.dptr(Lc.view(np.float64)), L.dptr(y.view(np.float64)), float(z0),
                         float(dz0), float(zmax), ctypes.byref(o), L.dptr(saves.view(np.float64)),

@@ -54,8 +54,8 @@ def load():
 
 
 class CpuPlan:
-    """A mode-averaged transform on the host in C++ (field-resolved grids; Kerr, PPT/ADK
-    plasma, Raman with THG)."""
+    """A mode-averaged transform on the host in C++: field-resolved grids (Kerr, PPT/ADK
+    plasma, Raman with THG) and envelope grids (Kerr_env, RamanPolarEnv)."""
 
     def __init__(self, transform):
         from luna_b200 import _lib as L

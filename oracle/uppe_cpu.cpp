@@ -7,8 +7,10 @@
 // PlasmaCumtrapz with the PPT spline or ADK rate (Nonlinear.jl:88-177, Ionisation.jl:43-59,
 // 257-270, Maths.jl:299-328, 764-848), RamanPolarField with THG (Nonlinear.jl:282-333),
 // the PreconStepper (RK45.jl:128-310, 343-406, dopri.jl:2-28) and Luna.run's stepfun and
-// GridCondition saves (Luna.jl:358-391, Output.jl:490-502). It reads the same descriptors
-// as the device library (include/luna_b200.h): field-resolved grids only.
+// GridCondition saves (Luna.jl:358-391, Output.jl:490-502), on field-resolved grids and on
+// envelope grids (Kerr_env, Nonlinear.jl:47-73; RamanPolarEnv, Nonlinear.jl:276-333; the
+// two-sided padding of copy_scale_both!, NonlinearRHS.jl:56-114). It reads the same
+// descriptors as the device library (include/luna_b200.h).
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -121,15 +123,18 @@ struct Resp {
 };
 
 struct Plan {
+    int kind = 0;  // 0: field-resolved, 1: envelope
     int N = 0, Nw = 0, No = 0;
     double in_scale = 0;
     std::vector<cd> outfac;
     std::vector<double> wwin, towin, twin;
     std::vector<Resp> resp;
     Rfft ro, rc, rr;
+    Fft co, cc, cr;  // envelope grids: complex transforms of No, N and 2 No points
     bool raman = false;
     // scratch
     std::vector<cd> X, Xr;
+    std::vector<cd> Ec, Pc, Rc;  // envelope fields
     std::vector<double> E, P, rate, frac, tmp, J, E2, pr;
     std::string err;
 };
@@ -234,6 +239,44 @@ int rhs(Plan* p, const cd* Ew, cd* nl) {
     return LUNA_OK;
 }
 
+// (t::TransModeAvg)(nl, Eω, z) on an envelope grid: the Nw bins go to both ends of the No
+// bins (copy_scale_both!), complex transforms, the envelope responses
+int rhs_env(Plan* p, const cd* Ew, cd* nl) {
+    const int No = p->No, Nw = p->Nw, h = Nw / 2;
+    std::fill(p->Ec.begin(), p->Ec.end(), cd(0, 0));
+    for (int k = 0; k < h; ++k) p->Ec[k] = Ew[k];
+    for (int j = 0; j < h; ++j) p->Ec[No - h + j] = Ew[Nw - h + j];
+    p->co.run(p->Ec.data(), true);
+    for (int t = 0; t < No; ++t) p->Ec[t] *= p->in_scale;
+    std::fill(p->Pc.begin(), p->Pc.end(), cd(0, 0));
+    for (const Resp& r : p->resp) {
+        if (r.kind == LUNA_RESP_KERR_ENV) {
+            for (int t = 0; t < No; ++t) {
+                const cd e = p->Ec[t];
+                p->Pc[t] += 3.0 / 4 * r.coef * std::norm(e) * e;
+            }
+        } else if (r.kind == LUNA_RESP_RAMAN) {
+            std::fill(p->Rc.begin(), p->Rc.end(), cd(0, 0));
+            for (int t = 0; t < No; ++t) p->Rc[t] = cd(0.5 * std::norm(p->Ec[t]), 0.0);
+            p->cr.run(p->Rc.data(), false);
+            for (int k = 0; k < 2 * No; ++k) p->Rc[k] = r.H[k] * p->Rc[k] * r.hdt;
+            p->cr.run(p->Rc.data(), true);
+            const double s = 1.0 / (2.0 * (double)No);
+            for (int t = 0; t < No; ++t) p->Pc[t] += r.coef * p->Ec[t] * (p->Rc[t] * s);
+        } else {
+            return fail(p, LUNA_ERR_UNSUPPORTED, "response not available on envelope grids");
+        }
+    }
+    for (int t = 0; t < No; ++t) p->Pc[t] *= p->towin[t];
+    p->co.run(p->Pc.data(), false);
+    if (Nw % 2) nl[h] = cd(0, 0);  // grids have even Nw; an odd middle bin has no source
+    for (int k = 0; k < h; ++k) nl[k] = p->Pc[k] * p->outfac[k];
+    for (int j = 0; j < h; ++j) nl[Nw - h + j] = p->Pc[No - h + j] * p->outfac[Nw - h + j];
+    return LUNA_OK;
+}
+
+int rhs_any(Plan* p, const cd* Ew, cd* nl) { return p->kind == 0 ? rhs(p, Ew, nl) : rhs_env(p, Ew, nl); }
+
 // ------------------------------------------------------------------ RK45 (dopri)
 const double Bt[6][6] = {{1.0 / 5},
                          {3.0 / 40, 9.0 / 40},
@@ -267,7 +310,7 @@ struct Stepper {
     void fbar(const std::vector<cd>& ybar, double t1, double t2, std::vector<cd>& res) {
         tmp = ybar;
         prop(tmp, t2 - t1);
-        const int rc = rhs(p, tmp.data(), res.data());
+        const int rc = rhs_any(p, tmp.data(), res.data());
         if (rc && status == LUNA_OK) status = rc;
         ++nrhs;
         prop(res, t1 - t2);
@@ -368,8 +411,9 @@ extern "C" {
 
 int uo_plan_create(const luna_grid_desc* g, const luna_resp_desc* rs, int nresp, void** out) {
     if (!g || !out || (nresp > 0 && !rs)) return LUNA_ERR_BAD_ARG;
-    if (g->kind != 0) return LUNA_ERR_UNSUPPORTED;
+    if (g->kind != 0 && g->kind != 1) return LUNA_ERR_UNSUPPORTED;
     Plan* p = new Plan();
+    p->kind = g->kind;
     p->N = g->N;
     p->Nw = g->Nw;
     p->No = g->No;
@@ -379,8 +423,14 @@ int uo_plan_create(const luna_grid_desc* g, const luna_resp_desc* rs, int nresp,
     p->wwin.assign(g->wwin, g->wwin + g->Nw);
     p->towin.assign(g->towin, g->towin + g->No);
     p->twin.assign(g->twin, g->twin + g->N);
-    p->ro.init(g->No);
-    p->rc.init(g->N);
+    const bool env = g->kind == 1;
+    if (env) {
+        p->co.init(g->No);
+        p->cc.init(g->N);
+    } else {
+        p->ro.init(g->No);
+        p->rc.init(g->N);
+    }
     const int No = g->No;
     for (int i = 0; i < nresp; ++i) {
         const luna_resp_desc& d = rs[i];
@@ -406,7 +456,8 @@ int uo_plan_create(const luna_grid_desc* g, const luna_resp_desc* rs, int nresp,
             // h(t) = sum_i hpre_i(t) exp(-t/tau2_i) w(t) on the first half of 2 No points
             // (CombinedRamanResponse, Raman.jl:249-262), then its real spectrum
             if (!p->raman) {
-                p->rr.init(2 * No);
+                if (env) p->cr.init(2 * No);
+                else p->rr.init(2 * No);
                 p->raman = true;
             }
             std::vector<double> h(2 * No, 0.0);
@@ -415,10 +466,16 @@ int uo_plan_create(const luna_grid_desc* g, const luna_resp_desc* rs, int nresp,
                 for (int c = 0; c < d.ncomp; ++c) acc += d.hpre[(size_t)c * No + t] * std::exp(-d.htt[t] / d.tau2[c]);
                 h[t] = acc * d.hwin[t];
             }
-            r.H.resize(No + 1);
-            p->rr.forward(h.data(), r.H.data());
+            if (env) {  // complex spectrum of the 2 No-point response (RamanPolarEnv)
+                r.H.assign(2 * No, cd(0, 0));
+                for (int t = 0; t < 2 * No; ++t) r.H[t] = cd(h[t], 0.0);
+                p->cr.run(r.H.data(), false);
+            } else {
+                r.H.resize(No + 1);
+                p->rr.forward(h.data(), r.H.data());
+            }
             r.hdt = d.hdt;
-        } else if (d.kind != LUNA_RESP_KERR_FIELD) {
+        } else if (d.kind != (env ? LUNA_RESP_KERR_ENV : LUNA_RESP_KERR_FIELD)) {
             delete p;
             return LUNA_ERR_UNSUPPORTED;
         }
@@ -434,6 +491,11 @@ int uo_plan_create(const luna_grid_desc* g, const luna_resp_desc* rs, int nresp,
     p->J.resize(No);
     p->E2.resize(2 * No);
     p->pr.resize(2 * No);
+    if (env) {
+        p->Ec.resize(No);
+        p->Pc.resize(No);
+        p->Rc.resize(2 * No);
+    }
     *out = p;
     return LUNA_OK;
 }
@@ -442,7 +504,7 @@ void uo_plan_destroy(void* h) { delete static_cast<Plan*>(h); }
 
 int uo_rhs(void* h, double* nl, const double* Ew) {
     Plan* p = static_cast<Plan*>(h);
-    return rhs(p, reinterpret_cast<const cd*>(Ew), reinterpret_cast<cd*>(nl));
+    return rhs_any(p, reinterpret_cast<const cd*>(Ew), reinterpret_cast<cd*>(nl));
 }
 
 // Luna.run with RK45.solve_precon (a MemoryOutput on saveN GridCondition points): y_inout
@@ -471,7 +533,7 @@ int uo_solve(void* h, const double* linop, double* y_inout, double z0, double dz
     long long steps = 0, rejected = 0;
     int status = s.status;
     std::vector<double> Et(p->N);
-    std::vector<cd> Y(p->N / 2 + 1);
+    std::vector<cd> Y(p->N / 2 + 1), Yc(p->kind == 1 ? p->N : 0);
     cd* sv = reinterpret_cast<cd*>(saves);
     while (status == LUNA_OK && s.tn <= zmax) {
         const bool ok = s.step();
@@ -482,12 +544,20 @@ int uo_solve(void* h, const double* linop, double* y_inout, double z0, double dz
         }
         if (ok) {
             // stepfun (Luna.jl:366-372): ωwin, back to time, twin, forward
-            for (int k = 0; k < n; ++k) Y[k] = s.yn[k] * p->wwin[k];
-            for (int k = n; k <= p->N / 2; ++k) Y[k] = cd(0, 0);
-            p->rc.inverse(Y.data(), Et.data());
-            for (int t = 0; t < p->N; ++t) Et[t] = Et[t] / (double)p->N * p->twin[t];
-            p->rc.forward(Et.data(), Y.data());
-            for (int k = 0; k < n; ++k) s.yn[k] = Y[k];
+            if (p->kind == 0) {
+                for (int k = 0; k < n; ++k) Y[k] = s.yn[k] * p->wwin[k];
+                for (int k = n; k <= p->N / 2; ++k) Y[k] = cd(0, 0);
+                p->rc.inverse(Y.data(), Et.data());
+                for (int t = 0; t < p->N; ++t) Et[t] = Et[t] / (double)p->N * p->twin[t];
+                p->rc.forward(Et.data(), Y.data());
+                for (int k = 0; k < n; ++k) s.yn[k] = Y[k];
+            } else {
+                for (int k = 0; k < n; ++k) Yc[k] = s.yn[k] * p->wwin[k];
+                p->cc.run(Yc.data(), true);
+                for (int t = 0; t < p->N; ++t) Yc[t] = Yc[t] / (double)p->N * p->twin[t];
+                p->cc.run(Yc.data(), false);
+                for (int k = 0; k < n; ++k) s.yn[k] = Yc[k];
+            }
             while (saved < o->saveN && o->zsave[saved] <= s.tn) {
                 if (sv) s.interpolate(o->zsave[saved], sv + (size_t)saved * n);
                 ++saved;

@@ -55,11 +55,33 @@ def test_cpu_restatement_step_budget_and_field_limit():
         cp.rhs(strong.Eω * 1e3)  # far above the PPT table: the reference errors
 
 
-def test_cpu_restatement_rejects_envelope_grids():
+def test_cpu_restatement_envelope_rhs_matches_numpy():
+    """GNLSE on an envelope grid: Kerr_env + RamanPolarEnv (Nonlinear.jl:47-73, 276-333)."""
     p = prop_gnlse_args(0.11, 0.15, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9,
                         λlims=(500e-9, 2400e-9), trange=12.5e-12, τfwhm=50e-15, power=10e3, saveN=5)
-    with pytest.raises(NotImplementedError):
-        cpu.CpuPlan(p.transform)
+    cp = cpu.CpuPlan(p.transform)
+    rng = np.random.default_rng(4)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    assert _rel(cp.rhs(Ew), uppe.trans_mode_avg(p.transform, Ew, 0.0)) < 1e-12
+
+
+def test_cpu_restatement_soliton_shift_golden_values():
+    """test_gnlse.jl:33-56: the soliton self-frequency shift's peak frequency and time
+    (golden values of the reference, rtol 1e-14) from the C++ restatement as well."""
+    γ, β2, fr, τ0 = 0.1, -1e-26, 0.18, 10e-15
+    P0 = abs(β2) / ((1 - fr) * γ * τ0 ** 2)
+    flength = np.pi / 2 * τ0 ** 2 / abs(β2) * 90
+    p = prop_gnlse_args(γ, flength, [0.0, 0.0, β2], λ0=835e-9, τfwhm=1.763 * τ0, power=P0,
+                        pulseshape="sech", λlims=[450e-9, 8000e-9], trange=13e-12, raman=True,
+                        shock=False, fr=fr)
+    sv, _, st = cpu.CpuPlan(p.transform).solve(p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=201)
+    assert st.status == 0 and st.nsaved == 201
+    Ew = sv[-1]
+    wpk = p.grid.ω[np.argmax(np.abs(Ew) ** 2)]
+    assert abs(wpk / 1.3975031072069625e15 - 1) <= 1e-14
+    Et = np.fft.ifft(Ew) * np.exp(1j * p.grid.ω0 * p.grid.t)
+    tpk = p.grid.t[np.argmax(np.abs(Et) ** 2)]
+    assert abs(tpk / 6.079566076444579e-12 - 1) <= 1e-14
 
 
 def test_scan_reference_rhs_counts_reproduced_by_the_cpu_restatement():

@@ -225,6 +225,9 @@ __device__ __forceinline__ double ppt_rate<double>(const LunaResp& r, double aE,
     if (aE <= xmin) i1 = 2;
     else if (aE >= xmax) i1 = n;
     else i1 = (int)ceil((aE - xmin) / (xmax - xmin) * (double)(n - 1)) + 1;
+    // already in [2, n] for every field inside the table; a NaN field (which passes both
+    // range tests) would otherwise index before the table
+    i1 = max(2, min(n, i1));
     const int i = i1 - 1;
     const double xi = __ldg(r.sx + i), xm = __ldg(r.sx + i - 1);
     const double yi = __ldg(r.sy + i), ym = __ldg(r.sy + i - 1);

@@ -161,7 +161,7 @@ bool ppt_rate(const Resp& r, double E, double* out) {
     const int n = (int)r.sx.size();
     const double xmin = r.sx[0], xmax = r.sx[n - 1];
     if (aE > xmax) return false;
-    if (aE < xmin) {
+    if (!(aE >= xmin)) {  // below the table, or NaN (the numpy restatement masks both)
         *out = 0.0;
         return true;
     }
@@ -169,6 +169,7 @@ bool ppt_rate(const Resp& r, double E, double* out) {
     if (aE <= xmin) i1 = 2;
     else if (aE >= xmax) i1 = n;
     else i1 = (int)std::ceil((aE - xmin) / (xmax - xmin) * (double)(n - 1)) + 1;
+    i1 = std::max(2, std::min(n, i1));
     const int i = i1 - 1;
     const double xi = r.sx[i], xm = r.sx[i - 1], yi = r.sy[i], ym = r.sy[i - 1];
     double v;

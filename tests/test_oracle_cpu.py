@@ -98,3 +98,16 @@ def test_scan_reference_rhs_counts_reproduced_by_the_cpu_restatement():
         p = scan.build_problem(inst[i], saveN=201)
         _, _, st = cpu.CpuPlan(p.transform).solve(p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=201)
         assert st.nrhs == ref["nrhs"][i] and st.status == ref["status"][i], i
+
+
+def test_nan_in_the_field_ends_in_the_repeat_limit():
+    """A NaN in y0 makes every error estimate non-finite: dz halves (RK45.jl:389-391) and
+    after repeat_limit rejections the run stops with the reference's error (RK45.jl:72-76),
+    in both restatements after the same 11 steps."""
+    p = _case("Ar", None)
+    y0 = p.Eω.copy()
+    y0[len(y0) // 3] = np.nan
+    _, _, st = cpu.CpuPlan(p.transform).solve(p.linop, y0, 0.0, 1e-4, p.grid.zmax, saveN=5)
+    assert st.status == 2 and st.steps == 11 and st.accepted == 0  # LUNA_REPEAT_LIMIT
+    with pytest.raises(RuntimeError, match="repetition"):
+        uppe.run(p.transform, p.grid, p.linop, y0, saveN=5)

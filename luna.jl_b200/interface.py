@@ -116,7 +116,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         energy=None, power=None, pulseshape="gauss", shotnoise=False,
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
-                        modes="HE11", radial_integral_rtol=1e-3):
+                        modes="HE11", radial_integral_rtol=1e-3, temperature=pd.roomtemp,
+                        rotation=True, vibration=True):
     """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
     over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
     a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
@@ -125,7 +126,9 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     (HE11..HE1n) or a tuple of names gives multimode propagation with ``modal.TransModal``,
     linearly polarised input in the first mode, the radial integral when every mode is HE1m
     (the device runs it) and the full 2-D integral otherwise (described, evaluated by the
-    oracle only); constant fill only."""
+    oracle only); constant fill only. ``temperature`` sets the gas density, the core index
+    and the Raman response's thermal populations; ``rotation``/``vibration`` select the Raman
+    components (Interface.jl:360-374, 519-531, 534-560)."""
     modes_ = modes
     from . import modes
     if shotnoise:
@@ -139,7 +142,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         if isinstance(modes_, (int, tuple, list)):
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
-                                         model, saveN, ppt_N, radial_integral_rtol)
+                                         model, saveN, ppt_N, radial_integral_rtol, temperature,
+                                         rotation, vibration)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
@@ -149,11 +153,11 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
             raise NotImplementedError("pressure gradients and tapers are supported for HE11 only")
         from .gradient import Gradient, MarcatiliGradientMode, Taper
         if not isinstance(pressure, (tuple, list)):
-            grad = Gradient(gas, flength, pressure, pressure)
+            grad = Gradient(gas, flength, pressure, pressure, T=temperature)
         elif len(pressure) == 2 and all(np.ndim(x) == 0 for x in pressure):
-            grad = Gradient(gas, flength, *pressure)      # (p0, p1)
+            grad = Gradient(gas, flength, *pressure, T=temperature)      # (p0, p1)
         else:
-            grad = Gradient(gas, *pressure)               # (Z, P)
+            grad = Gradient(gas, *pressure, T=temperature)               # (Z, P)
         if isinstance(radius, (tuple, list)):
             radius = Taper(*radius)
         mode = MarcatiliGradientMode(radius, grad, model=model, loss=loss)
@@ -161,8 +165,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     else:
         md = parse_mode(modes_)
         mode = modes.MarcatiliMode(radius, gas, pressure, n=md["n"], m=md["m"], kind=md["kind"],
-                                   model=model, loss=loss)
-        density = pd.density(gas, pressure)
+                                   T=temperature, model=model, loss=loss)
+        density = pd.density(gas, pressure, temperature)
     resp = []
     if kerr:
         # Interface.jl:534-541: without THG the Kerr term uses the analytic signal (the
@@ -179,7 +183,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     if raman is None:
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
-        rr = _raman.raman_response(grid.to, gas)
+        rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
         resp.append(RamanPolarField(grid.to, rr, thg=thg))
     if grad is not None:
         # z-dependent linear operator and normalisation (LinearOps.make_linop,
@@ -203,7 +207,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
 
 
 def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
-                          pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol):
+                          pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol,
+                          temperature, rotation, vibration):
     """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
     linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
     (``makeinputs``, Interface.jl:721-733)."""
@@ -211,7 +216,7 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     if isinstance(pressure, (tuple, list)) or isinstance(radius, (tuple, list)):
         raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
     pol = needpol_modes(modes_)
-    ms = makemode_s(modes_, radius, gas, pressure, pd.roomtemp, model, loss, pol)
+    ms = makemode_s(modes_, radius, gas, pressure, temperature, model, loss, pol)
     thg = True if thg is None else thg
     plasma = True if plasma is None else plasma
     resp = []
@@ -228,11 +233,13 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     if raman is None:
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
-        resp.append(RamanPolarField(grid.to, _raman.raman_response(grid.to, gas), thg=thg))
+        resp.append(RamanPolarField(grid.to, _raman.raman_response(grid.to, gas, rotation=rotation,
+                                                                   vibration=vibration, temp=temperature),
+                                    thg=thg))
     if pulseshape == "gauss":
         fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
     else:
         fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
-    Eω, t = modal.setup_modal(grid, pd.density(gas, pressure), resp, fld, ms, "xy" if pol else "y",
+    Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
     return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0), t, saveN)

@@ -111,3 +111,27 @@ def test_nan_in_the_field_ends_in_the_repeat_limit():
     assert st.status == 2 and st.steps == 11 and st.accepted == 0  # LUNA_REPEAT_LIMIT
     with pytest.raises(RuntimeError, match="repetition"):
         uppe.run(p.transform, p.grid, p.linop, y0, saveN=5)
+
+
+@pytest.mark.parametrize("gas,extra", [("He", {}), ("H2", {"kerr": False, "plasma": False})])
+def test_temperature_changes_results(gas, extra):
+    """test_interface.jl ("Temperature"): the same temperature gives identical spectra, a
+    different one changes them (density and core index; for H2 with Kerr and plasma off,
+    the Raman response's thermal populations), run on the C++ restatement."""
+    kw = dict(λ0=800e-9, τfwhm=10e-15, energy=1e-12, trange=400e-15, λlims=(200e-9, 4e-6),
+              saveN=5, **extra)
+
+    def final(T):
+        p = prop_capillary_args(100e-6, 0.1, gas, 1.0, temperature=T, **kw)
+        sv, _, st = cpu.CpuPlan(p.transform).solve(p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=5)
+        assert st.status == 0
+        return sv[-1], p
+
+    a, p300 = final(300.0)
+    b, _ = final(300.0)
+    c, p400 = final(400.0)
+    assert np.array_equal(a, b) and not np.array_equal(a, c)
+    if gas == "H2":
+        r300, r400 = p300.transform.resp[0], p400.transform.resp[0]
+        assert r300.kind == "raman_field"
+        assert not np.array_equal(r300.r.h(p300.transform.density), r400.r.h(p400.transform.density))

@@ -243,3 +243,19 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
     return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0), t, saveN)
+
+
+def prop_capillary(*args, precision=None, **kwargs):
+    """``prop_capillary`` (Interface.jl:345-349): ``prop_capillary_args`` then ``Luna.run`` on
+    the GPU (``plan.run``; a multimode set-up goes to the modal solver). Returns the solve
+    result: the saved spectra ``Eω`` at ``z``, the final state and the step counts."""
+    from . import _lib, plan
+    p = prop_capillary_args(*args, **kwargs)
+    return plan.run(p, precision=_lib.PREC_FP64 if precision is None else precision)
+
+
+def prop_gnlse(*args, precision=None, **kwargs):
+    """``prop_gnlse`` (Interface.jl:921-979): ``prop_gnlse_args`` then ``Luna.run`` on the GPU."""
+    from . import _lib, plan
+    p = prop_gnlse_args(*args, **kwargs)
+    return plan.run(p, precision=_lib.PREC_FP64 if precision is None else precision)

@@ -255,7 +255,7 @@ def prop_capillary(*args, precision=None, **kwargs):
 
 
 def prop_gnlse(*args, precision=None, **kwargs):
-    """``prop_gnlse`` (Interface.jl:921-979): ``prop_gnlse_args`` then ``Luna.run`` on the GPU."""
+    """``prop_gnlse`` (Interface.jl:906-910): ``prop_gnlse_args`` then ``Luna.run`` on the GPU."""
     from . import _lib, plan
     p = prop_gnlse_args(*args, **kwargs)
     return plan.run(p, precision=_lib.PREC_FP64 if precision is None else precision)

@@ -362,3 +362,23 @@ def test_oracle_linear_polarisation_at_45_degrees_reference_property():
     I2 = np.sum(np.abs(r2.Eω[-1]) ** 2, axis=1)
     assert r1.steps == r2.steps
     assert np.linalg.norm(I1 - I2) / np.linalg.norm(I1) < 1.07e-12
+
+
+def test_multimode_setup_helpers():
+    """doinput_mm! adds several fields into one mode (Luna.jl:154-162); makemode_s takes
+    dict designations and splits HE1m into two polarisations when both components are
+    needed; needpol_modes / needfull follow Interface.jl:439-446, 801-803."""
+    from luna_b200.interface import makemode_s, needfull, needpol_modes
+    grid, m, dens, resp, inp = _radial_case(1e-2)
+    ms = (modes.MarcatiliMode(A, GAS, PRES, loss=False), modes.MarcatiliMode(A, GAS, PRES, m=2, loss=False))
+    one = modal.doinput_mm(grid, inp, 2)
+    two = modal.doinput_mm(grid, ({"mode": 2, "fields": (inp, inp)},), 2)
+    np.testing.assert_allclose(two[:, 1], 2 * one[:, 0], rtol=1e-15)
+    assert not np.any(two[:, 0])
+    assert not needpol_modes(3) and not needpol_modes("HE11")
+    assert not needpol_modes(("HE11", "HE12")) and needpol_modes(("HE11", "HE21"))
+    assert needpol_modes(({"kind": "TM", "n": 0, "m": 1},))
+    got = makemode_s(({"kind": "HE", "n": 1, "m": 12}, "TE01"), A, GAS, PRES, pd.roomtemp, "full", False, True)
+    assert [(g.kind, g.n, g.m, g.ϕ) for g in got] == [("HE", 1, 12, 0.0), ("HE", 1, 12, math.pi / 2),
+                                                     ("TE", 0, 1, 0.0)]
+    assert needfull(got) and not needfull(makemode_s(2, A, GAS, PRES, pd.roomtemp, "full", False, False))

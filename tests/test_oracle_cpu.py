@@ -76,12 +76,16 @@ def test_cpu_restatement_soliton_shift_golden_values():
                         shock=False, fr=fr)
     sv, _, st = cpu.CpuPlan(p.transform).solve(p.linop, p.Eω, 0.0, 1e-4, p.grid.zmax, saveN=201)
     assert st.status == 0 and st.nsaved == 201
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "reference_golden.json")) as f:
+        ss = json.load(f)["soliton_shift"]
     Ew = sv[-1]
     wpk = p.grid.ω[np.argmax(np.abs(Ew) ** 2)]
-    assert abs(wpk / 1.3975031072069625e15 - 1) <= 1e-14
+    assert abs(wpk / ss["omega_peak"] - 1) <= ss["rtol"]
     Et = np.fft.ifft(Ew) * np.exp(1j * p.grid.ω0 * p.grid.t)
     tpk = p.grid.t[np.argmax(np.abs(Et) ** 2)]
-    assert abs(tpk / 6.079566076444579e-12 - 1) <= 1e-14
+    assert abs(tpk / ss["t_peak"] - 1) <= ss["rtol"]
 
 
 def test_scan_reference_rhs_counts_reproduced_by_the_cpu_restatement():

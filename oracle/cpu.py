@@ -46,7 +46,7 @@ def load():
     lib.uo_plan_destroy.restype = None
     lib.uo_rhs.argtypes = [ctypes.c_void_p, L.PD, L.PD]
     lib.uo_solve.argtypes = [ctypes.c_void_p, L.PD, L.PD, ctypes.c_double, ctypes.c_double,
-                             ctypes.c_double, P(L.SolveOpts), L.PD, P(L.SolveStats)]
+                             ctypes.c_double, P(L.SolveOpts), L.PD, L.PD, P(L.SolveStats)]
     lib.uo_last_error.argtypes = [ctypes.c_void_p]
     lib.uo_last_error.restype = ctypes.c_char_p
     _lib = lib
@@ -89,21 +89,30 @@ class CpuPlan:
         return nl
 
     def solve(self, linop, Eω, z0, dz0, zmax, saveN=201, rtol=1e-6, atol=1e-10, safety=0.9,
-              max_dt=None, min_dt=0.0, repeat_limit=10, max_steps=0, zsave=None):
+              max_dt=None, min_dt=0.0, repeat_limit=10, max_steps=0, zsave=None, steplog_cap=0,
+              replay=None):
         """Luna.run with RK45.solve_precon; saves at saveN points on [z0, zmax] or at
-        ``zsave``; returns (saves[nsaved, Nw], y, stats)."""
+        ``zsave``; returns (saves[nsaved, Nw], y, stats), or with ``steplog_cap`` > 0
+        (saves, y, stats, steplog[steps, 4]) with rows (z, dz, err, accepted) as the device
+        solver logs them. ``replay`` (flat (dz, accepted) pairs) makes the integrator follow
+        a recorded step sequence."""
         from luna_b200 import _lib as L
         from luna_b200.plan import make_opts
         zs = np.linspace(z0, zmax, saveN) if zsave is None else np.asarray(zsave, dtype=np.float64)
         saveN = len(zs)
+        rp = None if replay is None else np.ascontiguousarray(replay, dtype=np.float64)
         o = make_opts(saveN, zs, rtol=rtol, atol=atol, safety=safety,
                       max_dt=(zmax / 2 if max_dt is None else max_dt), min_dt=min_dt,
-                      repeat_limit=repeat_limit, max_steps=max_steps)
+                      repeat_limit=repeat_limit, max_steps=max_steps, steplog_cap=steplog_cap,
+                      replay=rp)
         Lc = np.ascontiguousarray(linop, dtype=np.complex128)
         y = np.array(Eω, dtype=np.complex128, copy=True)
         saves = np.zeros((max(saveN, 1), self.Nw), dtype=np.complex128)
+        log = np.zeros((max(steplog_cap, 1), 4))
         st = L.SolveStats()
         load().uo_solve(self._h, L.dptr(Lc.view(np.float64)), L.dptr(y.view(np.float64)), float(z0),
                         float(dz0), float(zmax), ctypes.byref(o), L.dptr(saves.view(np.float64)),
-                        ctypes.byref(st))
+                        L.dptr(log) if steplog_cap else L.dptr(None), ctypes.byref(st))
+        if steplog_cap:
+            return saves[: st.nsaved], y, st, log[: min(st.steps, steplog_cap)]
         return saves[: st.nsaved], y, st

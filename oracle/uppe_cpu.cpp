@@ -348,6 +348,10 @@ struct Stepper {
             ok = true;
         }
     }
+    // replay (verification aid, as in the device solver): the accept decision and the next
+    // step size come from a recorded sequence instead of the controller
+    const double* replay = nullptr;
+    long long nreplay = 0, nstep = 0;
     bool step() {
         evaluate();
         std::vector<cd> nn = y;
@@ -373,6 +377,11 @@ struct Stepper {
         err = std::sqrt(se) / rtol / errwt;
         ok = err <= 1;
         stepcontrol();
+        if (replay && nstep < nreplay) {
+            ok = replay[2 * nstep + 1] != 0.0;
+            if (nstep + 1 < nreplay) dtn = replay[2 * (nstep + 1)];
+        }
+        ++nstep;
         if (ok) {
             tn = t + dt;
             ks[0] = ks[6];
@@ -509,9 +518,11 @@ int uo_rhs(void* h, double* nl, const double* Ew) {
 }
 
 // Luna.run with RK45.solve_precon (a MemoryOutput on saveN GridCondition points): y_inout
-// holds Eω on entry and the final state on return; saves [saveN][Nw] complex.
+// holds Eω on entry and the final state on return; saves [saveN][Nw] complex; steplog
+// (optional) [4*o->steplog_cap] rows (z, dz, err, accepted) of the first steps, the rows of
+// the device solver's step log.
 int uo_solve(void* h, const double* linop, double* y_inout, double z0, double dz0, double zmax,
-             const luna_solve_opts* o, double* saves, luna_solve_stats* stats) {
+             const luna_solve_opts* o, double* saves, double* steplog, luna_solve_stats* stats) {
     Plan* p = static_cast<Plan*>(h);
     const int n = p->Nw;
     Stepper s;
@@ -529,6 +540,8 @@ int uo_solve(void* h, const double* linop, double* y_inout, double z0, double dz
     s.safety = o->safety;
     s.max_dt = o->max_dt;
     s.min_dt = o->min_dt;
+    s.replay = o->replay;
+    s.nreplay = o->replay ? o->nreplay : 0;
     s.fbar(s.y, s.t, s.t, s.ks[0]);
     int saved = 0, repeated = 0;
     long long steps = 0, rejected = 0;
@@ -537,7 +550,15 @@ int uo_solve(void* h, const double* linop, double* y_inout, double z0, double dz
     std::vector<cd> Y(p->N / 2 + 1), Yc(p->kind == 1 ? p->N : 0);
     cd* sv = reinterpret_cast<cd*>(saves);
     while (status == LUNA_OK && s.tn <= zmax) {
+        const double zstep = s.tn, dzstep = s.dtn;  // the step about to be taken (evaluate())
         const bool ok = s.step();
+        if (steplog && steps < o->steplog_cap) {
+            double* row = steplog + 4 * steps;
+            row[0] = zstep;
+            row[1] = dzstep;
+            row[2] = s.err;
+            row[3] = ok ? 1.0 : 0.0;
+        }
         ++steps;
         if (s.status != LUNA_OK) {
             status = s.status;

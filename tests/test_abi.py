@@ -122,3 +122,55 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_modal_desc"]) == ctypes.sizeof(_lib.ModalDesc)
     for f in ("ems", "wts", "wlow", "rtol", "atol", "outfac"):
         assert int(out[f"luna_modal_desc.{f}"]) == getattr(_lib.ModalDesc, f).offset
+
+
+# ------------------------------------------------------------------ the Julia binding
+_JL_TYPES = {"Cint": ctypes.c_int, "Float64": ctypes.c_double, "Clonglong": ctypes.c_longlong}
+
+
+def _julia_blocks():
+    import re
+    text = (HEADER.parent.parent / "INTEGRATION.md").read_text()
+    return "\n".join(re.findall(r"```julia\n(.*?)```", text, flags=re.S))
+
+
+def _julia_structs():
+    """Immutable `struct Name ... end` blocks of the Julia shim: {name: [(field, type)]}."""
+    import re
+    out = {}
+    for m in re.finditer(r"^struct (\w+)\s*\n(.*?)^end", _julia_blocks(), flags=re.S | re.M):
+        body = re.sub(r"#.*", "", m.group(2))
+        out[m.group(1)] = re.findall(r"(\w+)::(\w+(?:\{[^}]*\})?)", body)
+    return out
+
+
+def _ctype_matches(jl, ct):
+    import re
+    if jl.startswith("Ptr{"):
+        return ct is _lib.PD or ct is ctypes.c_void_p or issubclass(ct, ctypes._Pointer)
+    m = re.fullmatch(r"NTuple\{(\d+),\s*(\w+)\}", jl)
+    if m:
+        return issubclass(ct, ctypes.Array) and ct._length_ == int(m.group(1)) \
+            and ct._type_ is _JL_TYPES[m.group(2)]
+    return ct is _JL_TYPES[jl]
+
+
+@pytest.mark.parametrize("name", ["GridDesc", "RespDesc", "RadialDesc", "ModalDesc", "GradientDesc",
+                                  "SolveOpts", "SolveStats"])
+def test_julia_binding_structs_match_the_header(name):
+    """INTEGRATION.md's Julia structs mirror the C structs field for field (names, order and
+    types); the ctypes structures they are compared with are checked against the C
+    compiler's layout above."""
+    jl = _julia_structs()[name]
+    ct = getattr(_lib, name)._fields_
+    assert [f for f, _ in jl] == [f for f, _ in ct], name
+    for (f, jt), (_, ctt) in zip(jl, ct):
+        assert _ctype_matches(jt, ctt), (name, f, jt, ctt)
+
+
+def test_julia_binding_solveopts_call_passes_every_field():
+    import re
+    calls = re.findall(r"SolveOpts\(([^()]*(?:\([^()]*\)[^()]*)*)\)", _julia_blocks())
+    assert calls
+    for c in calls:
+        assert len([a for a in c.split(",") if a.strip()]) == len(_lib.SolveOpts._fields_), c

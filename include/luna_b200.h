@@ -21,6 +21,10 @@
  *     on one plan must be serialised; different plans may be used from different threads.
  *   - There is no CPU fallback: without a usable CUDA device every call fails with
  *     LUNA_ERR_CUDA.
+ *   - The library keeps per-device state for the life of the process (twiddle tables, the
+ *     device address of the allocation-free entry point's buffer). Destroying a device's
+ *     primary context (cudaDeviceReset) invalidates it together with every plan and batch
+ *     on that device: do not call the library on that device again in the same process.
  */
 #ifndef LUNA_B200_H
 #define LUNA_B200_H

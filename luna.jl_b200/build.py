@@ -6,7 +6,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 SRC = os.path.join(HERE, "csrc", "luna_b200.cu")
 OUT = os.path.join(HERE, "libluna_b200.so")
-DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc"))]
+DEPS = [os.path.join(HERE, "csrc", f) for f in os.listdir(os.path.join(HERE, "csrc")) if f != "peaks.cu"]
 DEPS.append(os.path.join(HERE, "..", "include", "luna_b200.h"))
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
@@ -20,10 +20,17 @@ def up_to_date():
     return all(os.path.getmtime(d) <= t for d in DEPS)
 
 
+# FMA-throughput microbenchmark (the compute ceilings of the benchmark's roofline)
+PEAKS_SRC = os.path.join(HERE, "csrc", "peaks.cu")
+PEAKS_OUT = os.path.join(HERE, "libluna_peaks.so")
+
+
 def build(force=False, verbose=False):
+    nvcc = os.environ.get("NVCC", "nvcc")
+    if force or not os.path.exists(PEAKS_OUT) or os.path.getmtime(PEAKS_SRC) > os.path.getmtime(PEAKS_OUT):
+        subprocess.run([nvcc] + NVCC_FLAGS + ["-o", PEAKS_OUT, PEAKS_SRC], check=True)
     if not force and up_to_date():
         return OUT
-    nvcc = os.environ.get("NVCC", "nvcc")
     cmd = [nvcc] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose else []) + ["-o", OUT, SRC]
     subprocess.run(cmd, check=True)
     return OUT

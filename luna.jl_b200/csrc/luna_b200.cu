@@ -2052,6 +2052,10 @@ int find_tw(TwDev& out) {
 }
 }  // namespace
 
+// The kernel's status word is documented as the public codes
+static_assert(ST_OK == LUNA_OK && ST_FIELD_ABOVE_EMAX == LUNA_FIELD_ABOVE_EMAX,
+              "rhs_kernel_noalloc writes ST_* values where the header promises LUNA_* codes");
+
 // The instance description travels as a kernel parameter, so the call needs no device copy.
 template <typename Rl>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)

@@ -109,3 +109,24 @@ def test_multi_rank_scan_split_gloo():
     m = np.array(masks)
     assert np.all(m.sum(axis=0) == 1)  # every instance on exactly one rank
     assert m[0].sum() > 0 and m[1].sum() > 0
+
+
+def test_accuracy_energy_weights_follow_energyfuncs():
+    """energy_ω of Fields.energyfuncs (Fields.jl:510-532) as a weight vector: the input
+    pulse carries its prescribed energy, and the weights reproduce SimpsonEven."""
+    from luna_b200 import accuracy, fields
+    from luna_b200.interface import prop_capillary_args
+    p = prop_capillary_args(125e-6, 0.01, "He", 1.0, λ0=800e-9, τfwhm=10e-15, energy=120e-6,
+                            λlims=(150e-9, 4e-6), trange=0.25e-12)
+    w = accuracy.Weights(p.grid.ω, "real")
+    assert abs(w.energy @ np.abs(p.Eω) ** 2 / 120e-6 - 1) < 1e-12
+    y = np.random.default_rng(0).random(len(p.grid.ω))
+    ref = 2 * np.pi / p.grid.ω[-1] ** 2 * fields.simpson_even(p.grid.ω, y)
+    assert abs(w.energy @ y / ref - 1) < 1e-13
+    # the drift of a scaled field: (1 + s)^2 - 1 in both energy and photon number
+    c = accuracy.compare(np.stack([p.Eω * 1.001]), np.stack([p.Eω]), p.grid.ω)
+    assert abs(c["energy"][0] - (1.001 ** 2 - 1)) < 1e-12
+    assert abs(c["photons"][0] - (1.001 ** 2 - 1)) < 1e-12
+    assert abs(c["spectral"][0] - (1.001 ** 2 - 1)) < 1e-12
+    s = accuracy.summary([c, None, accuracy.compare(np.stack([p.Eω]), np.stack([p.Eω]), p.grid.ω)])
+    assert s["instances"] == 2 and s["worst_instance"] == 0 and s["above_1e-3"] == [0]

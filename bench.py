@@ -55,6 +55,9 @@ IMPL = ("mixed precision (FP32 transforms/responses/stage derivatives, FP64 stat
         "norms/plasma sums), persistent launches: long instances distributed over 8-CTA clusters, "
         "the rest on single CTAs")
 SAVEN = 201
+# relative tolerance of the mixed-precision integrations (the plain FP64 path keeps the
+# reference's 1e-6)
+MIXED_RTOL = 1e-6
 STEPS_FILE = os.path.join(ROOT, "oracle", "scan256_nrhs.json")
 
 
@@ -621,6 +624,136 @@ def run_modal(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------------------- surrogate
+SG_METRIC = "surrogate scan queries/s (capillary family, 4-member MLP ensemble) at held-out log-spectrum error"
+SG_WORKLOAD = ("surrogate: (energy 50-400 uJ, 0.5-5 bar, He/Ne/Ar/H2, radius 75-150 um, 8-30 fs, z 0-3 m) -> "
+               "log10 spectrum on 512 log-spaced bins 150 nm - 4 um + 256-sample envelope; 6x512 SiLU MLP, "
+               "Fourier-feature input, 4 members, BF16 tensor-core training and inference, 10^6 queries per pass")
+
+
+def run_surrogate(args, world, rank, local):
+    """Data from the batched mixed-precision solver (args.sg_runs runs of 3 m, 201 saves),
+    training of the ensemble, error on held-out runs against the solver and against the
+    method without the network (the nearest training point), and the throughput of 10^6
+    queries against the plain FP64 solver's time per query."""
+    import torch
+    from luna_b200 import surrogate as S
+    torch.cuda.set_device(local)
+    log = (lambda m: print(m, file=sys.stderr, flush=True)) if rank == 0 else None
+    params = S.draw(args.sg_runs, seed=7 + rank)
+    t0 = time.perf_counter()
+    xr, T, runs, status, dev_s = S.generate(params, rtol=args.mixed_rtol, chunk=512, log=log)
+    gen_wall = time.perf_counter() - t0
+    ok_runs = sorted(set(runs.tolist()))
+    nheld = max(1, len(ok_runs) // 10)
+    held = set(ok_runs[-nheld:])
+    tr = np.array([r not in held for r in runs])
+    std = S.Standardise(xr[tr])
+    x = torch.tensor(std(xr), dtype=torch.float32, device="cuda")
+    trm = torch.from_numpy(tr).cuda()
+    xt, Tt = x[trm].contiguous(), T[trm].contiguous()
+    model = S.Ensemble(members=4, seed=11, batch=4096)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = S.train(model, xt, Tt, epochs=args.sg_epochs, log=log)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    steps = args.sg_epochs * (xt.shape[0] // model.batch)
+    # held-out error (every save of the held-out runs) and the method without the network
+    xq, Tq = x[~trm].contiguous(), T[~trm].contiguous()
+    mean, spread = S.predict(model, xq)
+    e = S.spectral_error(mean, Tq)
+    e_env = ((mean[:, S.NSPEC:] - Tq[:, S.NSPEC:]) ** 2).mean(dim=1).sqrt()
+    e_nn = S.spectral_error(S.nearest_neighbour(xt, Tt, xq), Tq)
+    flag = spread > args.sg_spread
+    # 1 % audit of the held-out points against the solver's values
+    g = torch.Generator(device="cuda").manual_seed(3)
+    audit = torch.randperm(xq.shape[0], device="cuda", generator=g)[: max(1, xq.shape[0] // 100)]
+    # 10^6 queries: parameter draws x random z (standardised like the training inputs)
+    nq = 1_000_064
+    rng = np.random.default_rng(17)
+    qp = S.draw(nq // 64, seed=23)
+    zq = rng.uniform(0.0, 3.0, nq)
+    pick = np.repeat(np.arange(len(qp)), 64)
+    xq_raw = S.raw_features([qp[i]["energy"] for i in pick], [qp[i]["pressure"] for i in pick],
+                            [qp[i]["radius"] for i in pick], [qp[i]["τfwhm"] for i in pick], zq,
+                            [qp[i]["gas"] for i in pick])
+    xh = torch.tensor(std(xq_raw), dtype=torch.float32).pin_memory()
+    xd = xh.cuda()
+    for _ in range(args.warmup):
+        S.predict(model, xd, chunk=nq)
+    st = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tms = []
+    for _ in range(args.steps):
+        e0.record(st)
+        mq, sq = S.predict(model, xd, chunk=nq)
+        e1.record(st)
+        e1.synchronize()
+        tms.append(e0.elapsed_time(e1))
+    ms = statistics.median(tms)
+    # end to end: host inputs in, host means and spreads out
+    mh = torch.empty(nq, S.NOUT, pin_memory=True)
+    sh = torch.empty(nq, pin_memory=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    m2, s2 = S.predict(model, xh.cuda(non_blocking=True), chunk=nq)
+    mh.copy_(m2)
+    sh.copy_(s2)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    qflag = float((sq > args.sg_spread).float().mean())
+    # the plain FP64 solver's time per query point: single-instance solves of held-out
+    # parameter sets (one luna_b200_solve per run), over the 201 points a run saves
+    t_plain = []
+    for i in sorted(held)[:3]:
+        pr = S.problem(params[i])
+        plan = P.Plan.from_transform(pr.transform, _lib.PREC_FP64)
+        b = P.Batch([plan], 201, np.linspace(0.0, 3.0, 201), max_dt=1.5)
+        b.upload([pr.linop], [pr.Eω], [0.0], [1e-4], [3.0])
+        t_plain.append(b.run() / 1e3)
+        del b, plan
+    plain_q_s = statistics.mean(t_plain) / 201
+    batched_q_s = dev_s / max(1, len(ok_runs)) / 201
+    flops = 4 * 2.0 * sum(k * n for k, n in zip(S.WIDTHS[:-1], S.WIDTHS[1:])) * nq
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            tpk, pk_kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        tpk, pk_kind = 1590.0, "fallback"
+    ach = flops / (ms / 1e3) / 1e12
+    value = nq / (ms / 1e3)
+    if rank == 0:
+        line = {"metric": SG_METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "bf16 (FP32 accumulate)", "data": "synthetic (batched-solver runs)",
+                "config": {"workload": SG_WORKLOAD, "runs": args.sg_runs, "completed_runs": len(ok_runs),
+                           "held_out_runs": nheld, "samples_train": int(xt.shape[0]), "epochs": args.sg_epochs,
+                           "adam_steps": steps, "queries_per_step": nq,
+                           "l2": "activations of 10^6 queries (GBs) exceed the 126 MB L2"},
+                "e2e": {"value": nq / e2e_s, "unit": "queries/s", "h2d_bytes_per_step": int(xh.numel() * 4),
+                        "d2h_bytes_per_step": int(mh.numel() * 4 + sh.numel() * 4)},
+                "gpu_launches": (1 + 6 + 1) * args.steps,
+                "roofline": {"bound": "tensor", "kernel": "sg_gemm (forward, 4 members)", "achieved": ach, "peak": tpk,
+                             "unit": "TFLOP/s", "frac": ach / tpk, "traffic": None, "peak_kind": pk_kind},
+                "accuracy": {"heldout_points": int(xq.shape[0]),
+                             "log_spectrum_rms_decades": {"mean": float(e.mean()), "median": float(e.median()),
+                                                          "p90": float(torch.quantile(e, 0.9))},
+                             "envelope_rms": float(e_env.mean()),
+                             "nearest_training_point": {"mean": float(e_nn.mean()), "median": float(e_nn.median())},
+                             "audit_1pct": {"points": int(audit.numel()), "mean": float(e[audit].mean())},
+                             "bar": 5e-2, "met_mean": bool(float(e.mean()) <= 5e-2),
+                             "spread_limit_decades": args.sg_spread,
+                             "flagged_heldout": float(flag.float().mean()),
+                             "error_unflagged": float(e[~flag].mean()) if bool((~flag).any()) else None},
+                "speed": {"plain_fp64_s_per_query": plain_q_s, "batched_mixed_s_per_query": batched_q_s,
+                          "surrogate_s_per_query": ms / 1e3 / nq, "vs_plain": plain_q_s / (ms / 1e3 / nq),
+                          "vs_batched": batched_q_s / (ms / 1e3 / nq), "flagged_queries": qflag},
+                "training": {"s": train_s, "final_loss": hist[-1], "data_gen_s_device": dev_s,
+                             "data_gen_s_wall": gen_wall}}
+        print(json.dumps(line), flush=True)
+
+
 # ----------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -642,15 +775,27 @@ def main():
     ap.add_argument("--accuracy", choices=["auto", "on", "off"], default="auto",
                     help="FP64 pass over the same scan after the timed region and the error of "
                          "every mixed save against it (auto: on at one GPU)")
-    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial", "modal"],
+    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial", "modal", "surrogate"],
                     help="scan256: the batched capillary scan (headline); radial: TransRadial RHS; "
-                         "modal: TransModal RHS")
+                         "modal: TransModal RHS; surrogate: the learned surrogate's queries")
+    ap.add_argument("--mixed-rtol", type=float, default=MIXED_RTOL,
+                    help="relative tolerance of the mixed-precision integrations")
+    ap.add_argument("--sg-runs", type=int, default=2560, help="surrogate: solver runs of training data")
+    ap.add_argument("--sg-epochs", type=int, default=60, help="surrogate: training epochs")
+    ap.add_argument("--sg-spread", type=float, default=0.1,
+                    help="surrogate: ensemble spread (decades) above which a query goes to the solver")
     args = ap.parse_args()
     world, rank, local = dist_info()
     if args.workload == "radial":
         return run_radial(args, world, rank, local)
     if args.workload == "modal":
         return run_modal(args, world, rank, local)
+    if args.workload == "surrogate":
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no surrogate (it always integrates)"}))
+            return
+        return run_surrogate(args, world, rank, local)
     if args.impl == "reference":
         if world > 1:
             import torch.distributed as dist
@@ -674,7 +819,7 @@ def main():
     n = len(probs)
     plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
     # each instance saves on its own GridCondition range(0, zmax, 201) with max_dz = zmax/2
-    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps,
+    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps, rtol=args.mixed_rtol,
                     flags=(_lib.SOLVE_NO_CLUSTERS if args.no_clusters else 0) |
                     (_lib.SOLVE_NO_DIST if args.no_dist else 0),
                     dist_min_no=args.dist_min_no)
@@ -814,7 +959,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64", "data": "synthetic (seeded scan draw, no noise)",
-                "config": scan_config(), "implementation": IMPL,
+                "config": scan_config(), "implementation": IMPL, "mixed_rtol": args.mixed_rtol,
                 "instances_this_rank": n, "failed_instances": failed,
                 "e2e": {"value": e2e_value, "unit": "sims/hour", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e * 1e3},

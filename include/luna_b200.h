@@ -50,6 +50,14 @@ extern "C" {
 #define LUNA_RESP_PLASMA_PPT 3  /* PlasmaCumtrapz with ionrate_fun!_PPTcached  Nonlinear.jl:107 */
 #define LUNA_RESP_PLASMA_ADK 4  /* PlasmaCumtrapz with ionrate_fun!_ADK         Nonlinear.jl:107 */
 #define LUNA_RESP_RAMAN 5       /* RamanPolarField(thg=true) / RamanPolarEnv Nonlinear.jl:223-264 */
+#define LUNA_RESP_KERR_FIELD_NOTHG 6 /* Nonlinear.Kerr_field_nothg(γ3, n): 3/4 ρ ε0 γ3 |hilbert(E)|^2 E
+                                        Nonlinear.jl:36-45 (RealGrid)                     */
+#define LUNA_RESP_RAMAN_NOTHG 7 /* RamanPolarField(t, r; thg=false): the convolution of
+                                   1/2 |hilbert(E)|^2 (sqr!, Nonlinear.jl:267-275); fields as
+                                   LUNA_RESP_RAMAN (RealGrid)                              */
+#define LUNA_RESP_KERR_ENV_THG 8 /* Nonlinear.Kerr_env_thg(γ3, ω0, t): ρ ε0 γ3/4 (3|E|^2 +
+                                    exp(2iω0t) E^2) E, Nonlinear.jl:75-84 (EnvGrid); coef and
+                                    cthg                                                   */
 
 /* precision modes */
 #define LUNA_PREC_FP64 0  /* plain: every operation in FP64 */
@@ -95,6 +103,8 @@ typedef struct {
     const double* hwin;     /* [No] Planck-taper window of the response                  */
     const double* htt;      /* [No] response time axis (0..No-1)*dt                      */
     double hdt;             /* response grid spacing (scales the convolution)            */
+    /* Kerr_env_thg */
+    const double* cthg;     /* [2*No] exp(2iω0 t) on the oversampled grid.to (complex)   */
 } luna_resp_desc;
 
 typedef struct {
@@ -250,6 +260,11 @@ int luna_b200_batch_set_priority(luna_batch* b, const double* priority);
  * start and end of its integration in seconds from the earliest start ([2*n] doubles) and
  * the SM that integrated it ([n] ints, may be NULL). */
 int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm);
+/* Step sequence of instance i for the next runs (a verification aid, no counterpart in the
+ * reference; the per-instance form of luna_solve_opts.replay): [2*nreplay] doubles, the
+ * (dz, accepted) of each step as luna_b200_batch_steplog records them (columns 1 and 3);
+ * nreplay = 0 removes it. Takes effect at the next luna_b200_batch_upload. */
+int luna_b200_batch_set_replay(luna_batch* b, int i, const double* replay, long long nreplay);
 void luna_b200_batch_destroy(luna_batch* b);
 
 /* ---------------------------------------------------------------- radial transform

@@ -31,6 +31,9 @@ RESP_KERR_ENV = 2
 RESP_PLASMA_PPT = 3
 RESP_PLASMA_ADK = 4
 RESP_RAMAN = 5
+RESP_KERR_FIELD_NOTHG = 6
+RESP_RAMAN_NOTHG = 7
+RESP_KERR_ENV_THG = 8
 
 PREC_FP64 = 0
 PREC_MIXED = 1
@@ -53,7 +56,7 @@ class RespDesc(ctypes.Structure):
                 ("adk_pre", c_double), ("adk_a", c_double), ("adk_b", c_double),
                 ("adk_pw", c_double), ("adk_thr", c_double),
                 ("ncomp", c_int), ("hpre", PD), ("tau2", PD), ("hwin", PD), ("htt", PD),
-                ("hdt", c_double)]
+                ("hdt", c_double), ("cthg", PD)]
 
 
 class RadialDesc(ctypes.Structure):
@@ -105,6 +108,7 @@ EXPORTS = [
     "luna_b200_batch_info", "luna_b200_batch_stats", "luna_b200_plan_set_gradient",
     "luna_b200_plan_linop", "luna_b200_modal_plan_create", "luna_b200_modal_plan_destroy",
     "luna_b200_modal_rhs", "luna_b200_modal_rhs_device", "luna_b200_modal_solve",
+    "luna_b200_batch_set_replay",
 ]
 
 _lib = None
@@ -164,6 +168,7 @@ def load():
                                           POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
     lib.luna_b200_batch_info.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]
     lib.luna_b200_batch_set_priority.argtypes = [c_void_p, PD]
+    lib.luna_b200_batch_set_replay.argtypes = [c_void_p, c_int, PD, c_longlong]
     lib.luna_b200_batch_timeline.argtypes = [c_void_p, PD, POINTER(c_int)]
     lib.luna_b200_qdht_device.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p]
     lib.luna_b200_last_error.restype = ctypes.c_char_p

@@ -44,6 +44,12 @@ typedef struct {
     const double* htt;     // [No] response time axis
     double hdt;            // response grid spacing
     int ncomp;
+    // no-THG forms (Kerr_field_nothg, RamanPolarField(thg=false)): the squared field is
+    // |hilbert(E)|^2 = E^2 + H^2, H the Hilbert transform of E (kind stays KERR_FIELD /
+    // RAMAN)
+    int hilb;
+    // Kerr_env_thg (kind KERR_ENV): [No] exp(2i w0 t) on the oversampled grid, or null
+    const double2* cthg;
 } LunaResp;
 
 // Pressure-gradient fill and/or taper (z-dependent density, radius, normalisation and

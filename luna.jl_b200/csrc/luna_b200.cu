@@ -503,6 +503,7 @@ size_t smem_wanted(const LunaInst& I) {
     const size_t c = sizeof(cpx<Rl>);
     size_t s = LUNA_SMALL_BYTES;
     s += align_up((size_t)main_len(I) * c, 256);
+    if (needs_hilbert(I)) s += align_up((size_t)(I.No / 2) * c, 256);
     s += align_up((size_t)I.Nw * c, 256);
     if (has_raman(I)) s += align_up((size_t)I.No * c, 256);
     return s;
@@ -641,7 +642,8 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
         const int Mmain = (g->kind == 0) ? g->No / 2 : g->No;
         const int lim = (precision == LUNA_PREC_FP64) ? FftMmax<double>::v : FftMmax<float>::v;
         bool raman = false;
-        for (int i = 0; i < nresp; ++i) raman = raman || resps[i].kind == LUNA_RESP_RAMAN;
+        for (int i = 0; i < nresp; ++i)
+            raman = raman || resps[i].kind == LUNA_RESP_RAMAN || resps[i].kind == LUNA_RESP_RAMAN_NOTHG;
         if (Mmain > lim || (raman && g->No > lim) || g->No > FftMmax<double>::v * 2)
             return fail(LUNA_ERR_UNSUPPORTED, "plan_create: grid too large for one CTA");
         if (g->No < 2 * LUNA_BLOCK)
@@ -694,9 +696,22 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
         r.kind = d.kind;
         r.coef = d.coef;
         switch (d.kind) {
+            case LUNA_RESP_KERR_FIELD_NOTHG:
+                r.kind = LUNA_RESP_KERR_FIELD;
+                r.hilb = 1;
+                // fall through
             case LUNA_RESP_KERR_FIELD:
                 if (g->kind != 0) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Kerr_field needs a RealGrid"); }
                 break;
+            case LUNA_RESP_KERR_ENV_THG:
+                if (!d.cthg) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Kerr_env_thg needs its exp(2iω0t) table"); }
+                if (g->kind == 1) {
+                    const double* c;
+                    UP(d.cthg, 2 * (size_t)g->No, &c);
+                    r.cthg = reinterpret_cast<const double2*>(c);
+                }
+                r.kind = LUNA_RESP_KERR_ENV;
+                // fall through
             case LUNA_RESP_KERR_ENV:
                 if (g->kind != 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Kerr_env needs an EnvGrid"); }
                 break;
@@ -735,7 +750,13 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
                 }
                 break;
             }
+            case LUNA_RESP_RAMAN_NOTHG:
             case LUNA_RESP_RAMAN: {
+                if (d.kind == LUNA_RESP_RAMAN_NOTHG) {
+                    if (g->kind != 0) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "RamanPolarField(thg=false) needs a RealGrid"); }
+                    r.kind = LUNA_RESP_RAMAN;
+                    r.hilb = 1;
+                }
                 p->has_raman = true;
                 if (++nraman > 1) { free_all(p->allocs); delete p; return fail(LUNA_ERR_UNSUPPORTED, "at most one Raman response"); }
                 if (d.ncomp < 1 || !d.hpre || !d.tau2 || !d.hwin || !d.htt) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Raman response tables missing"); }
@@ -1048,7 +1069,8 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         for (int i = 0; i < n; ++i) {
             const LunaInst& I = b->h[i];
             const int M = I.No / 2, Mc = I.N / 2;
-            const bool ok = I.kind == 0 && !I.grad && opts->stats_cap <= 0 && I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
+            const bool ok = I.kind == 0 && !I.grad && !needs_hilbert(I) && opts->stats_cap <= 0 &&
+                            I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
                             M % DIST_R == 0 && M / DIST_R >= 2 * LUNA_BLOCK &&
                             M / DIST_R <= FftEmax<float>::v * LUNA_BLOCK && Mc % DIST_R == 0 &&
                             Mc / DIST_R >= 64 && Mc <= M && I.Nw <= Mc + 1 &&
@@ -1105,7 +1127,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
             const size_t half = align_up((size_t)(I.No / 2) * sizeof(float2), 256);
             const size_t efac = align_up((size_t)I.Nw * sizeof(float2), 256);
             const bool fits1 = smem_wanted<float>(I) <= (size_t)maxs;
-            const bool ok_cl = I.kind == 0 && has_raman(I) && !fits1 &&
+            const bool ok_cl = I.kind == 0 && has_raman(I) && !fits1 && !needs_hilbert(I) &&
                                LUNA_SMALL_BYTES + half + efac <= (size_t)std::min<int>(maxs, b->smem);
             if (ok_cl) big.push_back(i);
             else reg.push_back(i);
@@ -1359,6 +1381,22 @@ int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog) {
     return LUNA_OK;
 }
 
+int luna_b200_batch_set_replay(luna_batch* b, int i, const double* replay, long long nreplay) {
+    if (!b || i < 0 || i >= b->n || nreplay < 0 || (nreplay > 0 && !replay))
+        return fail(LUNA_ERR_BAD_ARG, "batch_set_replay: bad argument");
+    LunaInst& I = b->h[i];
+    if (nreplay == 0) {
+        I.replay = nullptr;
+        I.nreplay = 0;
+        return LUNA_OK;
+    }
+    const double* rp = nullptr;
+    if (upload(b->allocs, replay, 2 * (size_t)nreplay, &rp)) return LUNA_ERR_CUDA;
+    I.replay = rp;
+    I.nreplay = nreplay;
+    return LUNA_OK;
+}
+
 void luna_b200_batch_destroy(luna_batch* b) {
     if (!b) return;
     if (b->ev0) cudaEventDestroy(b->ev0);
@@ -1515,9 +1553,12 @@ int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* 
         return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: unknown precision");
     if (precision == LUNA_PREC_MIXED && rd->Nr % 64 != 0)
         return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: the mixed-precision QDHT needs Nr to be a multiple of 64");
-    for (int i = 0; i < nresp; ++i)
-        if (resps[i].kind == LUNA_RESP_RAMAN)
+    for (int i = 0; i < nresp; ++i) {
+        if (resps[i].kind == LUNA_RESP_RAMAN || resps[i].kind == LUNA_RESP_RAMAN_NOTHG)
             return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Raman response not available for the radial transform");
+        if (resps[i].kind == LUNA_RESP_KERR_FIELD_NOTHG)
+            return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Kerr_field_nothg not available for the radial transform");
+    }
     // the column plan: grid and responses; its output factor is unused (the radial one
     // is applied after the QDHT)
     std::vector<double> ones(2 * (size_t)g->Nw, 0.0);
@@ -1907,8 +1948,10 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
         return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: unknown precision");
     double kerr = 0;
     for (int i = 0; i < nresp; ++i) {
-        if (resps[i].kind == LUNA_RESP_RAMAN)
+        if (resps[i].kind == LUNA_RESP_RAMAN || resps[i].kind == LUNA_RESP_RAMAN_NOTHG)
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: Raman response not available for the modal transform");
+        if (resps[i].kind == LUNA_RESP_KERR_FIELD_NOTHG)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: Kerr_field_nothg not available for the modal transform");
         if (md->npol == 2 && resps[i].kind != LUNA_RESP_KERR_FIELD)
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support the Kerr response only");
         if (resps[i].kind == LUNA_RESP_KERR_FIELD) kerr += resps[i].coef;

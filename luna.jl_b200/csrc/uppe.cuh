@@ -27,6 +27,8 @@ struct Ws {
     cpx<Rl>* efac;      // exp(L*dz) of the current stage, Nw entries
     cpx<Rl>* ram;       // Raman convolution buffer (No complex)
     cpx<Rl>* ram_alt;
+    cpx<Rl>* hil;       // Hilbert transform H of the field (no-THG responses), No/2 pairs
+    cpx<Rl>* hil_alt;   // its out-of-place partner (global memory only)
     double* red;        // 3 * LUNA_WARPS reduction scratch
     double* tot;        // 3 * LUNA_WARPS scan totals
     double* edge;       // 4 edge values carried between scan chunks
@@ -85,6 +87,13 @@ __host__ __device__ inline bool has_raman(const LunaInst& I) {
     return false;
 }
 
+// an instance with a no-THG response needs the Hilbert transform of its field
+__host__ __device__ inline bool needs_hilbert(const LunaInst& I) {
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].hilb) return true;
+    return false;
+}
+
 __host__ __device__ inline bool has_plasma(const LunaInst& I) {
     for (int i = 0; i < I.nresp; ++i)
         if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) return true;
@@ -97,6 +106,7 @@ __host__ __device__ inline size_t gscr_bytes(const LunaInst& I) {
     size_t c = sizeof(cpx<Rl>);
     size_t b = 0;
     b += 2 * align_up((size_t)main_len(I) * c, 256);
+    if (needs_hilbert(I)) b += 2 * align_up((size_t)(I.No / 2) * c, 256);
     b += align_up((size_t)I.Nw * c, 256);
     if (has_raman(I)) b += 2 * align_up((size_t)I.No * c, 256);
     return b;
@@ -129,6 +139,18 @@ __device__ void plan_ws(const LunaInst& I, char* smem, int smem_bytes, Ws<Rl>& w
         w.main_alt = reinterpret_cast<cpx<Rl>*>(g + goff + mb);
     }
     goff += 2 * mb;
+    w.hil = w.hil_alt = nullptr;
+    if (needs_hilbert(I)) {
+        const size_t hb = align_up((size_t)(I.No / 2) * c, 256);
+        if (off + hb <= (size_t)smem_bytes) {
+            w.hil = reinterpret_cast<cpx<Rl>*>(smem + off);
+            off += hb;
+        } else {
+            w.hil = reinterpret_cast<cpx<Rl>*>(g + goff);
+            w.hil_alt = reinterpret_cast<cpx<Rl>*>(g + goff + hb);
+        }
+        goff += 2 * hb;
+    }
     size_t eb = align_up((size_t)I.Nw * c, 256);
     if (off + eb <= (size_t)smem_bytes) {
         w.efac = reinterpret_cast<cpx<Rl>*>(smem + off);
@@ -509,11 +531,19 @@ __device__ void plasma_only(const LunaInst& I, Ws<Rl>& w, const cpx<Rl>* xr, cpx
 // to_time! (NonlinearRHS.jl:16-23): C2R pre-twiddle of the zero-padded spectrum and the
 // inverse transform. Returns the buffer holding slot m = samples (2m, 2m+1) in split
 // order with factor *P (unscaled: multiply by the pad scale / No).
+//
+// With hx != null the same pass also transforms the spectrum -i X[k] (k >= 1; DC and
+// Nyquist zero) into w.hil: the Hilbert transform H of the field, so that the analytic
+// signal of Maths.hilbert (Maths.jl:560-569) is E + iH (the padded spectrum is zero at
+// the Nyquist bin, so its real part is E itself). *hx receives the buffer holding H in
+// split order with factor *Ph, scaled like E.
 template <typename Rl, typename LoadF>
-__device__ __forceinline__ cpx<Rl>* c2r_to_time(Ws<Rl>& w, int M, int Nw, LoadF&& load, int* P) {
+__device__ __forceinline__ cpx<Rl>* c2r_to_time(Ws<Rl>& w, int M, int Nw, LoadF&& load, int* P,
+                                                cpx<Rl>** hx = nullptr, int* Ph = nullptr) {
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
     cpx<Rl>* buf = w.main;
+    cpx<Rl>* hb = hx ? w.hil : nullptr;
     // Z[k] = (X[k] + conj X[M-k]) + i W^-k (X[k] - conj X[M-k])
     for (int k = tid; k <= M / 2; k += T) {
         const int km = M - k;
@@ -532,17 +562,37 @@ __device__ __forceinline__ cpx<Rl>* c2r_to_time(Ws<Rl>& w, int M, int Nw, LoadF&
             cpx<double> Zm = (Xm + conj(Xk)) + mul_mi<double, true>(Wmi * (Xm - conj(Xk)));
             buf[Swz<Rl>::f(km)] = cvt<Rl>(Zm);
         }
+        if (hb) {
+            // -i X (DC and Nyquist bins dropped, as the analytic signal does)
+            const cpx<double> Hk = (k == 0) ? mk<double>(0, 0) : mk<double>(Xk.y, -Xk.x);
+            const cpx<double> Hm = (k == 0) ? mk<double>(0, 0) : mk<double>(Xm.y, -Xm.x);
+            hb[Swz<Rl>::f(k)] = cvt<Rl>((Hk + conj(Hm)) + mul_mi<double, true>(Wi * (Hk - conj(Hm))));
+            if (k != 0 && km != k) {
+                cpx<double> Wmi = scale(-1.0, conj(Wi));
+                hb[Swz<Rl>::f(km)] = cvt<Rl>((Hm + conj(Hk)) + mul_mi<double, true>(Wmi * (Hm - conj(Hk))));
+            }
+        }
     }
     __syncthreads();
     cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, M, w.tw);
     *P = buf_split<Rl>(w.main_alt, M);
+    if (hb) {
+        *hx = block_fft<Rl, true>(hb, w.hil_alt, M, w.tw);
+        *Ph = buf_split<Rl>(w.hil_alt, M);
+    }
     return x;
 }
 
 // Et_to_Pt! (NonlinearRHS.jl:121-126) and the time window, in place on the samples held
-// by x (split factor P); sc converts the stored samples to the field in V/m.
-template <typename Rl>
-__device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int M, int P, double sc) {
+// by x (split factor P); sc converts the stored samples to the field in V/m. hx (split
+// factor Ph) holds the Hilbert transform of the field for the no-THG responses, whose
+// squared field is |hilbert(E)|^2 = E^2 + H^2 (Kerr_field_nothg: 3/4 coef (E^2 + H^2) E,
+// Nonlinear.jl:36-45; RamanPolarField(thg=false): 1/2 (E^2 + H^2), Nonlinear.jl:267-275).
+// HIL selects the no-THG variant at compile time, so that the THG forms (the common case)
+// compile to the same code as without it.
+template <typename Rl, bool HIL>
+__device__ __forceinline__ void pointwise_real_t(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int M, int P, double sc,
+                                                 const cpx<Rl>* hx, int Ph) {
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
     int ip = -1, ir = -1;
@@ -552,7 +602,7 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
     }
     const int Pr_split = (ir >= 0) ? buf_split<Rl>(w.ram_alt, I.No) : 1;
     cpx<Rl>* Pr = nullptr;
-    if (w.cl) {
+    if (!HIL && w.cl) {
         // response cluster: Raman halves on ranks 1-2 (P_raman[m] = even[m] + odd[m] in
         // the split order of their No/2-point transforms), plasma polarisation on rank 3
         // (same positions as x); the responses are added here in tuple order
@@ -602,13 +652,22 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
         return;
     }
     if (ir >= 0) {
-        // E^2 on the first half of the 2*No grid (thg=true form of sqr!), split order
+        // E^2 (thg=true form of sqr!) or 1/2 (E^2 + H^2) (thg=false) on the first half of
+        // the 2*No grid, split order
+        const bool hq = HIL && I.resp[ir].hilb;
         for (int m = tid; m < I.No; m += T) {
             cpx<Rl> v = mk<Rl>(0, 0);
             if (m < M) {
                 cpx<Rl> e = x[Swz<Rl>::f(split_pos(m, M, P))];
                 Rl e0 = e.x * (Rl)sc, e1 = e.y * (Rl)sc;
                 v = mk<Rl>(e0 * e0, e1 * e1);
+                if constexpr (HIL) {
+                    if (hq) {
+                        const cpx<Rl> h = hx[Swz<Rl>::f(split_pos(m, M, Ph))];
+                        const Rl h0 = h.x * (Rl)sc, h1 = h.y * (Rl)sc;
+                        v = mk<Rl>((Rl)0.5 * (e0 * e0 + h0 * h0), (Rl)0.5 * (e1 * e1 + h1 * h1));
+                    }
+                }
             }
             w.ram[Swz<Rl>::f(split_pos(m, I.No, Pr_split))] = v;
         }
@@ -621,18 +680,26 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
             const int m0 = c0 + 2 * tid;
             const bool act[2] = {m0 < M, m0 + 1 < M};
             int pos[2];
-            double E[4];
+            double E[4], H2[4] = {0, 0, 0, 0};
 #pragma unroll
             for (int q = 0; q < 2; ++q) {
                 pos[q] = Swz<Rl>::f(split_pos(act[q] ? m0 + q : 0, M, P));
                 const cpx<Rl> e = act[q] ? x[pos[q]] : mk<Rl>(0, 0);
                 E[2 * q] = (double)e.x * sc;
                 E[2 * q + 1] = (double)e.y * sc;
+                if constexpr (HIL) {
+                    const cpx<Rl> h = act[q] ? hx[Swz<Rl>::f(split_pos(m0 + q, M, Ph))] : mk<Rl>(0, 0);
+                    H2[2 * q] = (double)h.x * sc * ((double)h.x * sc);
+                    H2[2 * q + 1] = (double)h.y * sc * ((double)h.y * sc);
+                }
             }
             double Pq[4] = {0, 0, 0, 0};
             for (int i = 0; i < I.nresp; ++i) {
                 const LunaResp& r = I.resp[i];
-                if (r.kind == LUNA_RESP_KERR_FIELD) {
+                if (HIL && r.kind == LUNA_RESP_KERR_FIELD && r.hilb) {
+#pragma unroll
+                    for (int s = 0; s < 4; ++s) Pq[s] += 0.75 * r.coef * (E[s] * E[s] + H2[s]) * E[s];
+                } else if (r.kind == LUNA_RESP_KERR_FIELD) {
 #pragma unroll
                     for (int s = 0; s < 4; ++s) Pq[s] += r.coef * (E[s] * E[s] * E[s]);
                 } else if (i == ir) {
@@ -664,10 +731,19 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
         const int pos = Swz<Rl>::f(split_pos(m, M, P));
         cpx<Rl> e = act ? x[pos] : mk<Rl>(0, 0);
         const double E0 = (double)e.x * sc, E1 = (double)e.y * sc;
+        double Hq0 = 0, Hq1 = 0;
+        if constexpr (HIL) {
+            const cpx<Rl> h = act ? hx[Swz<Rl>::f(split_pos(m, M, Ph))] : mk<Rl>(0, 0);
+            Hq0 = (double)h.x * sc * ((double)h.x * sc);
+            Hq1 = (double)h.y * sc * ((double)h.y * sc);
+        }
         double P0 = 0, P1 = 0;
         for (int i = 0; i < I.nresp; ++i) {
             const LunaResp& r = I.resp[i];
-            if (r.kind == LUNA_RESP_KERR_FIELD) {
+            if (HIL && r.kind == LUNA_RESP_KERR_FIELD && r.hilb) {
+                P0 += 0.75 * r.coef * (E0 * E0 + Hq0) * E0;
+                P1 += 0.75 * r.coef * (E1 * E1 + Hq1) * E1;
+            } else if (r.kind == LUNA_RESP_KERR_FIELD) {
                 P0 += r.coef * (E0 * E0 * E0);
                 P1 += r.coef * (E1 * E1 * E1);
             } else if (i == ir) {
@@ -682,6 +758,18 @@ __device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx
         }
     }
     __syncthreads();
+}
+
+template <typename Rl>
+__device__ __forceinline__ void pointwise_real(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int M, int P, double sc) {
+    pointwise_real_t<Rl, false>(I, w, x, M, P, sc, nullptr, 1);
+}
+
+// the no-THG variant, out of line: it adds the Hilbert samples to every path
+template <typename Rl>
+__device__ __noinline__ void pointwise_real_hilb(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int M, int P, double sc,
+                                                 const cpx<Rl>* hx, int Ph) {
+    pointwise_real_t<Rl, true>(I, w, x, M, P, sc, hx, Ph);
 }
 
 // to_freq! (NonlinearRHS.jl:39-45): forward transform of x (split factor of the buffer),
@@ -711,11 +799,13 @@ __device__ __forceinline__ void r2c_to_freq(Ws<Rl>& w, cpx<Rl>* x, int M, int Nw
 template <typename Rl, typename LoadF, typename StoreF>
 __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
     const int M = I.No / 2;
-    int P;
-    cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P);
+    int P, Ph = 1;
+    cpx<Rl>* hx = nullptr;
+    cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, load, &P, w.hil ? &hx : nullptr, &Ph);
     // field scale 1/(nlscale sqrt(Aeff)) x pad/No; a taper's is in outz[Nw] at this node
     const double sc = I.grad ? I.outz[I.Nw].x : I.in_scale;
-    pointwise_real<Rl>(I, w, x, M, P, sc);
+    if (hx) pointwise_real_hilb<Rl>(I, w, x, M, P, sc, hx, Ph);
+    else pointwise_real<Rl>(I, w, x, M, P, sc);
     const cpx<double>* of = reinterpret_cast<const cpx<double>*>(I.outfac);
     // with a pressure gradient the factor of the current z is in outz, written by this
     // kernel (plain loads, not the read-only path)
@@ -765,7 +855,11 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
         cpx<double> Pt = mk<double>(0, 0);
         for (int i = 0; i < I.nresp; ++i) {
             const LunaResp& r = I.resp[i];
-            if (r.kind == LUNA_RESP_KERR_ENV) {
+            if (r.kind == LUNA_RESP_KERR_ENV && r.cthg) {
+                // Kerr_env_thg (Nonlinear.jl:75-84): coef/4 (3|E|^2 + exp(2i w0 t) E^2) E
+                const cpx<double> C = ldg(reinterpret_cast<const cpx<double>*>(r.cthg) + n);
+                Pt = Pt + scale(0.25 * r.coef, scale(3.0 * abs2(E), E) + C * (E * E) * E);
+            } else if (r.kind == LUNA_RESP_KERR_ENV) {
                 Pt = Pt + scale(0.75 * r.coef * abs2(E), E);
             } else if (i == ir) {
                 cpx<Rl> p = Pr[Swz<Rl>::f(split_pos(n >> 1, No, Pr_split))];

@@ -169,8 +169,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         density = pd.density(gas, pressure, temperature)
     resp = []
     if kerr:
-        # Interface.jl:534-541: without THG the Kerr term uses the analytic signal (the
-        # oracle evaluates it; the device plan rejects it)
+        # Interface.jl:534-541: without THG the Kerr term uses the analytic signal
         resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
                     Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
     if plasma:

@@ -12,10 +12,10 @@ description of the response that the device evaluates inside the fused right-han
 * ``RamanPolarField(t, r; thg)`` / ``RamanPolarEnv(t, r)``          (Nonlinear.jl:183-333)
 
 Responses accumulate into the polarisation in the order they are given, as
-``Et_to_Pt!`` does (NonlinearRHS.jl:121-126). The device evaluates Kerr_field, Kerr_env,
-PlasmaCumtrapz and the THG forms of the Raman responses; the no-THG Kerr and Raman forms
-and the THG envelope Kerr are described here and restated by the oracle, and the device
-plan rejects them (``plan.resp_descs``).
+``Et_to_Pt!`` does (NonlinearRHS.jl:121-126). The device evaluates all of them in the
+mode-averaged transform; the no-THG forms take the Hilbert transform H of the field from one
+more inverse transform (|hilbert(E)|^2 = E^2 + H^2) and run on the single-CTA solvers.
+The radial and modal transforms take Kerr_field and PlasmaCumtrapz.
 """
 from . import physdata as pd
 from .ionisation import PPTSpline, adk_params

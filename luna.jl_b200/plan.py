@@ -30,9 +30,18 @@ def resp_descs(resp, rho, keep):
         if r.kind == "kerr_field":
             d.kind = _lib.RESP_KERR_FIELD
             d.coef = rho * pd.eps_0 * r.γ3
+        elif r.kind == "kerr_field_nothg":
+            d.kind = _lib.RESP_KERR_FIELD_NOTHG
+            d.coef = rho * pd.eps_0 * r.γ3
         elif r.kind == "kerr_env":
             d.kind = _lib.RESP_KERR_ENV
             d.coef = rho * pd.eps_0 * r.γ3
+        elif r.kind == "kerr_env_thg":
+            d.kind = _lib.RESP_KERR_ENV_THG
+            d.coef = rho * pd.eps_0 * r.γ3
+            C = np.ascontiguousarray(r.C, dtype=np.complex128)
+            keep.append(C)
+            d.cthg = _lib.dptr(C.view(np.float64))
         elif r.kind == "plasma":
             d.coef = rho
             d.ionpot = r.ionpot
@@ -53,12 +62,8 @@ def resp_descs(resp, rho, keep):
                 keep += [x, y, D]
                 d.spl_x, d.spl_y, d.spl_D = _lib.dptr(x), _lib.dptr(y), _lib.dptr(D)
                 d.spl_n = len(x)
-        elif r.kind in ("kerr_field_nothg", "kerr_env_thg") or \
-                (r.kind == "raman_field" and not r.thg):
-            raise NotImplementedError(f"{type(r).__name__}{'' if r.kind != 'raman_field' else '(thg=false)'} "
-                                      "is not available on the device")
         elif r.kind in ("raman_field", "raman_env"):
-            d.kind = _lib.RESP_RAMAN
+            d.kind = _lib.RESP_RAMAN if (r.kind == "raman_env" or r.thg) else _lib.RESP_RAMAN_NOTHG
             d.coef = rho
             resp = r.r
             hpre = _f64(np.stack(resp.hpres))
@@ -278,6 +283,15 @@ class Batch:
         """Start instances with a larger priority first (an estimate of their work)."""
         self._prio = _f64(priority)
         _lib.check(_lib.load().luna_b200_batch_set_priority(self._h, _lib.dptr(self._prio)))
+
+    def set_replay(self, i, replay):
+        """Make instance i follow a recorded step sequence (flat (dz, accepted) pairs, e.g.
+        columns 1 and 3 of its step log) from the next upload on; None removes it."""
+        if replay is None:
+            _lib.check(_lib.load().luna_b200_batch_set_replay(self._h, i, _lib.dptr(None), 0))
+            return
+        r = _f64(replay)
+        _lib.check(_lib.load().luna_b200_batch_set_replay(self._h, i, _lib.dptr(r), len(r) // 2))
 
     def timeline(self):
         """(begin, end) seconds of every instance's integration in the last run, and the SM

@@ -1,5 +1,6 @@
-"""The C-ABI library loads, exports every entry point declared in include/luna_b200.h, and
-its descriptor structs have the layout the ctypes bindings assume. No compute calls."""
+"""The C-ABI libraries load and export every entry point declared in include/luna_b200.h and
+include/luna_surrogate.h, and the descriptor structs have the layout the ctypes (and the
+documented Julia) bindings assume. No compute calls."""
 import luna_b200_loader  # registers the luna.jl_b200 package
 
 luna_b200_loader.load()
@@ -40,6 +41,22 @@ def test_every_declared_symbol_is_exported():
     assert set(names) == set(_lib.EXPORTS)
 
 
+def test_surrogate_library_exports_its_header():
+    """libluna_surrogate.so (the learned surrogate's kernels) exports every function that
+    include/luna_surrogate.h declares, and the ctypes binding loads them all."""
+    from luna_b200 import surrogate
+    hdr = (ROOT / "include" / "luna_surrogate.h").read_text()
+    names = sorted(set(re.findall(r"\b(luna_sg_\w+)\s*\(", hdr)))
+    assert len(names) == 7
+    out = subprocess.run(["nm", "-D", "--defined-only", surrogate.LIB_PATH], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(l.split()[-1] for l in out.splitlines() if l.strip())
+    assert not [n for n in names if n not in exported]
+    lib = surrogate.load()
+    for n in names:
+        assert getattr(lib, n).argtypes is not None, n
+
+
 def test_plan_create_without_device_fails_loudly():
     # On a machine without a GPU the library must refuse, not compute on the host.
     try:
@@ -66,7 +83,7 @@ int main(void) {
            sizeof(luna_grid_desc), sizeof(luna_resp_desc), sizeof(luna_solve_opts), sizeof(luna_solve_stats));
     printf("luna_radial_desc %zu\n", sizeof(luna_radial_desc));
     P(luna_grid_desc, in_scale); P(luna_resp_desc, spl_n); P(luna_resp_desc, adk_thr);
-    P(luna_resp_desc, hdt); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
+    P(luna_resp_desc, hdt); P(luna_resp_desc, cthg); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
     P(luna_solve_opts, replay); P(luna_solve_opts, nreplay); P(luna_solve_opts, flags);
     P(luna_radial_desc, Mf); P(luna_radial_desc, outfac);
     P(luna_grid_desc, omega); P(luna_grid_desc, escale); P(luna_solve_opts, stats_cap);
@@ -101,6 +118,7 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_resp_desc.spl_n"]) == _lib.RespDesc.spl_n.offset
     assert int(out["luna_resp_desc.adk_thr"]) == _lib.RespDesc.adk_thr.offset
     assert int(out["luna_resp_desc.hdt"]) == _lib.RespDesc.hdt.offset
+    assert int(out["luna_resp_desc.cthg"]) == _lib.RespDesc.cthg.offset
     assert int(out["luna_solve_opts.zsave"]) == _lib.SolveOpts.zsave.offset
     assert int(out["luna_solve_opts.steplog_cap"]) == _lib.SolveOpts.steplog_cap.offset
     assert int(out["luna_radial_desc"]) == ctypes.sizeof(_lib.RadialDesc)

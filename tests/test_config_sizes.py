@@ -1,0 +1,138 @@
+"""Parity at the stated sizes of the single-instance workloads, on their full propagation
+lengths, against the FP64 oracle run on the same inputs at test time:
+
+  * GNLSE (prop_gnlse form): Nt = 2^13 envelope grid over 12.5 ps at 835 nm, β2 = -11.83e-27
+    s^2/m, β3 = 8.1e-41 s^3/m, γ = 0.11 /W/m, fused-silica Raman (fR 0.18), sech^2 50 fs /
+    10 kW, 15 cm, 201 saves (the set-up of test_gnlse.jl with these βs); C++ restatement.
+  * The README capillary call (README.md:51): 125 µm He capillary at 1 bar, 3 m, 800 nm,
+    10 fs, 120 µJ, λ 150 nm - 4 µm over 1 ps (Nt 8192, No 16384), Kerr + PPT plasma, 201
+    saves, no shot noise; C++ restatement.
+  * Radial free-space propagation (TransRadial): Nr = 256 over 3 mm, No = 4096 over 0.5 ps,
+    Ar at 1 bar, w0 = 1 mm, 800 nm, 30 fs, 0.5 mJ, f = 1 m focusing, 2 m, Kerr + PPT
+    plasma; numpy restatement.
+
+Bars: plain FP64 takes the oracle's accepted-step sequence (step sizes to the rounding of
+the error estimate: 1e-6 relative with plasma, 1e-9 without) and matches every saved field
+to 1e-10 relative L2; mixed precision stays within 1e-3 relative spectral L2 of |Eω|^2 at
+every save.
+"""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import numpy as np
+import pytest
+
+from luna_b200 import _lib
+from luna_b200 import plan as P
+from luna_b200.interface import prop_capillary_args, prop_gnlse_args
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def _spec(a, b):
+    return _rel(np.abs(a) ** 2, np.abs(b) ** 2)
+
+
+def gnlse_cfg():
+    return prop_gnlse_args(0.11, 0.15, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9, τfwhm=50e-15,
+                           power=10e3, pulseshape="sech", λlims=(500e-9, 2400e-9), trange=12.5e-12,
+                           raman=True)
+
+
+def readme_cfg():
+    return prop_capillary_args(125e-6, 3.0, "He", 1.0, λ0=800e-9, τfwhm=10e-15, energy=120e-6,
+                               λlims=(150e-9, 4e-6), trange=1e-12)
+
+
+_CACHE = {}
+
+
+def _pair(name):
+    """(problem, oracle saves, oracle stats, oracle step log, device FP64 result)."""
+    if name not in _CACHE:
+        from oracle import cpu
+        p = {"gnlse": gnlse_cfg, "readme": readme_cfg}[name]()
+        zmax = p.grid.zmax
+        saves, _, st, log = cpu.CpuPlan(p.transform).solve(p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=201,
+                                                           max_dt=zmax / 2, steplog_cap=400000)
+        r = P.solve_precon(p.transform, p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=201, max_dt=zmax / 2,
+                           steplog_cap=400000)
+        _CACHE[name] = (p, saves, st, log, r)
+    return _CACHE[name]
+
+
+@pytest.mark.parametrize("name", ["gnlse", "readme"])
+def test_full_length_fp64_same_steps_and_fields(name):
+    p, saves, st, log, r = _pair(name)
+    assert p.grid.N == 8192 and (name == "gnlse" or p.grid.No == 16384)
+    assert st.status == 0 and r.status == 0
+    assert r.steps == st.steps and r.rejected == st.rejected, (r.steps, st.steps)
+    plasma = any(x.kind == "plasma" for x in p.transform.resp)
+    np.testing.assert_allclose(r.steplog[:, 1], log[:, 1], rtol=1e-6 if plasma else 1e-9, atol=0)
+    assert r.nsaved == st.nsaved == 201
+    errs = [_rel(a, b) for a, b in zip(r.Eω, saves)]
+    assert max(errs) <= 1e-10, (max(errs), int(np.argmax(errs)))
+
+
+@pytest.mark.parametrize("name", ["gnlse", "readme"])
+def test_full_length_mixed_spectral_error(name):
+    p, saves, st, _, _ = _pair(name)
+    zmax = p.grid.zmax
+    m = P.solve_precon(p.transform, p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=201, max_dt=zmax / 2,
+                       precision=_lib.PREC_MIXED)
+    assert m.status == 0 and m.nsaved == 201
+    errs = [_spec(a, b) for a, b in zip(m.Eω, saves)]
+    assert max(errs) <= 1e-3, (max(errs), int(np.argmax(errs)))
+
+
+# ------------------------------------------------------------------ radial, Nr = 256
+_RAD = {}
+
+
+def _radial():
+    if not _RAD:
+        from luna_b200.radial import prop_radial_args
+        from oracle import uppe
+        p = prop_radial_args("Ar", 1.0, R=3e-3, N=256, flength=2.0, λ0=800e-9, λlims=(400e-9, 2000e-9),
+                             trange=0.5e-12, τfwhm=30e-15, energy=0.5e-3, w0=1e-3, focal_length=1.0,
+                             plasma="PPT")
+        assert p.Eω.shape == (1025, 256) and p.grid.No == 4096
+        _RAD["p"] = p
+        _RAD["o"] = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=201)
+    return _RAD["p"], _RAD["o"]
+
+
+def test_radial_nr256_rhs_matches_oracle():
+    from luna_b200 import radial_plan
+    from oracle import uppe
+    p, _ = _radial()
+    rng = np.random.default_rng(11)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    ref = uppe.trans_radial(p.transform, Ew, 0.0)
+    nl = np.zeros_like(Ew)
+    p.transform(nl, Ew, 0.0)
+    assert _rel(nl, ref) < 1e-11, _rel(nl, ref)
+    plan = radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    nm = np.zeros_like(Ew)
+    plan.rhs(nm, Ew, 0.0)
+    assert _rel(nm, ref) < 2e-4, _rel(nm, ref)
+
+
+def test_radial_nr256_full_length_fp64_and_mixed():
+    from luna_b200 import radial_plan
+    p, o = _radial()
+    r = radial_plan.run(p, steplog_cap=1000)
+    assert r.status == 0 and r.steps == o.steps and r.nsaved == 201
+    acc = r.steplog[r.steplog[:, 3] == 1]
+    np.testing.assert_allclose(acc[:, 1], np.array(o.accepted)[:, 1], rtol=1e-6)
+    errs = [_rel(a, b) for a, b in zip(r.Eω, o.Eω)]
+    assert max(errs) <= 1e-10, max(errs)
+    m = radial_plan.run(p, precision=_lib.PREC_MIXED)
+    assert m.status == 0 and m.nsaved == 201
+    errs = [_spec(a, b) for a, b in zip(m.Eω, o.Eω)]
+    assert max(errs) <= 1e-3, max(errs)

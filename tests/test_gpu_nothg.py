@@ -1,0 +1,118 @@
+"""The responses without third-harmonic generation on the device, against the FP64 oracle:
+
+  * Kerr_field_nothg (Nonlinear.jl:36-45): 3/4 ρ ε0 γ3 |hilbert(E)|^2 E;
+  * RamanPolarField(thg=false) (sqr!, Nonlinear.jl:267-275): the Raman convolution of
+    1/2 |hilbert(E)|^2;
+  * Kerr_env_thg (Nonlinear.jl:75-84) on an envelope grid: ρ ε0 γ3/4 (3|E|^2 + exp(2iω0t) E^2) E.
+
+prop_capillary(thg=false) selects the first two (Interface.jl:534-556). The device takes the
+Hilbert transform H of the field from one more inverse transform of the padded spectrum
+times -i (|hilbert(E)|^2 = E^2 + H^2, the Nyquist bin of the padded spectrum being zero).
+Bars as for the other RHS parity tests: FP64 1e-11 (plasma and Raman present), mixed 1e-5;
+solves take the oracle's steps with every save within 1e-10 (FP64) or 1e-3 spectral
+(mixed).
+"""
+import luna_b200_loader  # registers the luna.jl_b200 package
+
+luna_b200_loader.load()
+
+import numpy as np
+import pytest
+
+from luna_b200 import _lib
+from luna_b200 import plan as P
+from luna_b200.interface import prop_capillary_args, prop_gnlse_args
+from oracle import uppe
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def capillary_nothg(gas="He", zmax=0.02, trange=0.25e-12):
+    kw = dict(energy=100e-6, radius=100e-6, pressure=2.0, τ=15e-15) if gas == "H2" else \
+        dict(energy=120e-6, radius=125e-6, pressure=1.0, τ=10e-15)
+    return prop_capillary_args(kw["radius"], zmax, gas, kw["pressure"], λ0=800e-9, τfwhm=kw["τ"],
+                               energy=kw["energy"], λlims=(150e-9, 4e-6), trange=trange, thg=False)
+
+
+def envelope_thg():
+    """A GNLSE set-up whose Kerr term is Kerr_env_thg on the oversampled envelope grid."""
+    from luna_b200.nonlinear import Kerr_env_thg
+    from luna_b200.nonlinearrhs import TransModeAvg
+    p = prop_gnlse_args(0.11, 0.01, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9, τfwhm=50e-15,
+                        power=10e3, pulseshape="sech", λlims=(500e-9, 2400e-9), trange=12.5e-12,
+                        raman=False)
+    t = p.transform
+    kerr = t.resp[0]
+    assert kerr.kind == "kerr_env"
+    r = Kerr_env_thg(kerr.γ3, p.grid.ω0, p.grid.to)
+    p.transform = TransModeAvg(t.grid, (r,), t.density, t.norm, t.aeff)
+    return p
+
+
+CASES = {"He_kerr_nothg_ppt": lambda: capillary_nothg("He"),
+         "H2_kerr_nothg_adk_raman_nothg": lambda: capillary_nothg("H2"),
+         "He_1ps": lambda: capillary_nothg("He", trange=1e-12),
+         "env_kerr_thg": envelope_thg}
+
+
+def test_case_responses_are_the_no_thg_forms():
+    kinds = [r.kind for r in CASES["H2_kerr_nothg_adk_raman_nothg"]().transform.resp]
+    assert kinds[0] == "kerr_field_nothg" and kinds[-1] == "raman_field"
+    assert not CASES["H2_kerr_nothg_adk_raman_nothg"]().transform.resp[-1].thg
+    assert CASES["env_kerr_thg"]().transform.resp[0].kind == "kerr_env_thg"
+
+
+@pytest.mark.parametrize("name", list(CASES))
+@pytest.mark.parametrize("prec", [_lib.PREC_FP64, _lib.PREC_MIXED], ids=["fp64", "mixed"])
+def test_rhs_no_thg_forms_match_oracle(name, prec):
+    prob = CASES[name]()
+    rng = np.random.default_rng(2)
+    Ew = prob.Eω * np.exp(1j * 0.3 * rng.standard_normal(len(prob.Eω)))
+    ref = uppe.trans_mode_avg(prob.transform, Ew, 0.0)
+    pl = P.Plan.from_transform(prob.transform, prec)
+    nl = pl.rhs(np.zeros_like(Ew), Ew, 0.0)
+    tol = (1e-11 if name != "env_kerr_thg" else 1e-12) if prec == _lib.PREC_FP64 else 1e-5
+    assert _rel(nl, ref) <= tol, _rel(nl, ref)
+
+
+@pytest.mark.parametrize("name", ["He_kerr_nothg_ppt", "H2_kerr_nothg_adk_raman_nothg", "env_kerr_thg"])
+def test_solve_no_thg_forms_match_oracle(name):
+    prob = CASES[name]()
+    zmax = prob.grid.zmax
+    dz0 = 1e-3 if name != "env_kerr_thg" else 1e-4
+    ores = uppe.run(prob.transform, prob.grid, prob.linop, prob.Eω, init_dz=dz0, saveN=11)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    g = P.solve_precon(prob.transform, prob.linop, prob.Eω, 0.0, dz0, zmax, saveN=11,
+                       max_dt=zmax / 2, replay=replay)
+    assert g.status == 0 and g.steps == ores.steps and g.nsaved == 11
+    errs = [_rel(a, o) for a, o in zip(g.Eω, ores.Eω)]
+    assert max(errs) <= 1e-10, max(errs)
+    m = P.solve_precon(prob.transform, prob.linop, prob.Eω, 0.0, dz0, zmax, saveN=11,
+                       max_dt=zmax / 2, precision=_lib.PREC_MIXED)
+    assert m.status == 0
+    errs = [_rel(np.abs(a) ** 2, np.abs(o) ** 2) for a, o in zip(m.Eω, ores.Eω)]
+    assert max(errs) <= 1e-3, max(errs)
+
+
+def test_no_thg_instances_stay_on_single_ctas_in_a_mixed_batch():
+    """A no-THG instance on the 16384-point grid is not distributed (the cluster solvers
+    evaluate the THG forms only); it runs on a single CTA beside a distributed one."""
+    probs = [capillary_nothg("He", zmax=0.01, trange=1e-12),
+             prop_capillary_args(125e-6, 0.01, "Ar", 1.0, λ0=800e-9, τfwhm=10e-15, energy=100e-6,
+                                 λlims=(150e-9, 4e-6), trange=1e-12, saveN=5)]
+    plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
+    b = P.Batch(plans, 5, np.linspace(0.0, 1.0, 5))
+    b.upload([p.linop for p in probs], [p.Eω for p in probs], [0.0, 0.0], [1e-4, 1e-4],
+             [p.grid.zmax for p in probs], [np.linspace(0.0, p.grid.zmax, 5) for p in probs],
+             [p.grid.zmax / 2 for p in probs])
+    assert b.info()[1] == 1
+    b.run()
+    r = b.results()[0]
+    o = uppe.run(probs[0].transform, probs[0].grid, probs[0].linop, probs[0].Eω, saveN=5)
+    assert r.status == 0
+    errs = [_rel(np.abs(a) ** 2, np.abs(x) ** 2) for a, x in zip(r.Eω, o.Eω)]
+    assert max(errs) <= 1e-3, max(errs)

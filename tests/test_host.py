@@ -130,3 +130,33 @@ def test_accuracy_energy_weights_follow_energyfuncs():
     assert abs(c["spectral"][0] - (1.001 ** 2 - 1)) < 1e-12
     s = accuracy.summary([c, None, accuracy.compare(np.stack([p.Eω]), np.stack([p.Eω]), p.grid.ω)])
     assert s["instances"] == 2 and s["worst_instance"] == 0 and s["above_1e-3"] == [0]
+
+
+def test_surrogate_cpu_gradients_match_finite_differences():
+    """The CPU restatement that checks the device's training gradients is itself exact:
+    in FP64 (no BF16 rounding) its gradients match central differences of its loss."""
+    from luna_b200 import surrogate as S
+    rng = np.random.default_rng(4)
+    widths = (6, 5, 4, 3)
+    W = [rng.standard_normal((n, k)) * 0.5 for k, n in zip(widths[:-1], widths[1:])]
+    b = [rng.standard_normal(n) * 0.1 for n in widths[1:]]
+    X = rng.standard_normal((7, widths[0]))
+    T = rng.standard_normal((7, widths[-1]))
+    loss, gW, gb = S.reference_gradients(X, W, b, T, rounding=False)
+    h = 1e-6
+    for l in range(len(W)):
+        for (i, j) in ((0, 0), (W[l].shape[0] - 1, W[l].shape[1] - 1)):
+            Wp = [w.copy() for w in W]
+            Wm = [w.copy() for w in W]
+            Wp[l][i, j] += h
+            Wm[l][i, j] -= h
+            fd = (S.reference_gradients(X, Wp, b, T, rounding=False)[0] -
+                  S.reference_gradients(X, Wm, b, T, rounding=False)[0]) / (2 * h)
+            assert abs(fd - gW[l][i, j]) <= 1e-7 * max(1.0, abs(fd)), (l, i, j)
+        bp = [v.copy() for v in b]
+        bm = [v.copy() for v in b]
+        bp[l][0] += h
+        bm[l][0] -= h
+        fd = (S.reference_gradients(X, W, bp, T, rounding=False)[0] -
+              S.reference_gradients(X, W, bm, T, rounding=False)[0]) / (2 * h)
+        assert abs(fd - gb[l][0]) <= 1e-7 * max(1.0, abs(fd)), l

@@ -152,9 +152,11 @@ def test_raman_field_nothg_squares_the_analytic_signal():
     np.testing.assert_allclose(0.5 * np.abs(A) ** 2, E ** 2 - 0.5 * (A ** 2).real, atol=1e-15)
 
 
-def test_no_thg_responses_are_described_but_not_on_the_device():
+def test_no_thg_responses_map_to_their_device_kinds():
     """prop_capillary(thg=false) (Interface.jl:534-555) builds Kerr_field_nothg and
-    RamanPolarField(thg=false); the oracle evaluates them, the device plan refuses them."""
+    RamanPolarField(thg=false); the oracle evaluates them and the descriptors carry the
+    no-THG kinds of the C ABI (the device evaluates them, tests/test_gpu_nothg.py)."""
+    from luna_b200 import _lib
     from luna_b200.interface import prop_capillary_args
     from luna_b200.plan import resp_descs
     p = prop_capillary_args(125e-6, 0.1, "H2", 1.0, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
@@ -163,10 +165,8 @@ def test_no_thg_responses_are_described_but_not_on_the_device():
     assert ("kerr_field_nothg", None) in kinds and ("raman_field", False) in kinds
     nl = uppe.trans_mode_avg(p.transform, p.Eω, 0.0)
     assert np.all(np.isfinite(nl)) and np.linalg.norm(nl) > 0
-    for r in p.transform.resp:
-        if r.kind in ("kerr_field_nothg", "raman_field"):
-            with pytest.raises(NotImplementedError):
-                resp_descs([r], 1.0, [])
+    ds = resp_descs(p.transform.resp, 1.0, [])
+    assert [d.kind for d in ds] == [_lib.RESP_KERR_FIELD_NOTHG, _lib.RESP_PLASMA_ADK, _lib.RESP_RAMAN_NOTHG]
 
 
 # ---------------------------------------------------------------- test_raman.jl:9-70

@@ -51,9 +51,11 @@ from luna_b200 import plan as P  # noqa: E402
 METRIC = "capillary UPPE sims/hour/GPU, mixed+batched vs plain FP64 at ≤1e-3 spec. err"
 WORKLOAD = ("scan256: 256 mode-averaged capillary instances (seed 20261203; He/Ne/Ar/H2, PPT/ADK "
             "plasma, Raman for H2; No 8192-32768), each integrated to its fibre length with 201 saves")
-IMPL = ("mixed precision (FP32 transforms/responses/stage derivatives, FP64 state/phase/controller/"
-        "norms/plasma sums), persistent launches: long instances distributed over 8-CTA clusters, "
-        "the rest on single CTAs")
+IMPL = {"fp64": ("FP64 batched: persistent launches, long instances distributed over 8-CTA clusters "
+                 "(FP64 sub-transforms and responses), the rest on single CTAs"),
+        "mixed": ("mixed precision (FP32 transforms/responses/stage derivatives, FP64 state/phase/controller/"
+                  "norms/plasma sums), persistent launches: long instances distributed over 8-CTA clusters, "
+                  "the rest on single CTAs")}
 SAVEN = 201
 # relative tolerance of the mixed-precision integrations (the plain FP64 path keeps the
 # reference's 1e-6)
@@ -300,31 +302,42 @@ def cpu_estimate(sample_seconds=20.0, workers=1, pool=None):
         "per_rhs_ms": {f"No={k[0]}{'+Raman' if k[1] else ''}": round(v * 1e3, 3) for k, v in per_rhs.items()}}
 
 
-def plain_fp64_measured(inst, probs, dur, status64, k=16):
-    """The plain FP64 drop-in, measured: one luna_b200_solve-style single-instance FP64
-    solve after another (device time of each, CUDA events) for a stratified subset of the
-    completed instances (k quantiles of their integration times in the FP64 batch).
-    Returns the subset's own sims/hour, the scan estimate (the batch's per-instance times
-    scaled by the subset's measured/batch ratio) and the per-instance record."""
+def plain_fp64_measured(inst, probs, dur, status64, k=8):
+    """The plain FP64 drop-in, measured: one single-instance FP64 solve after another (a
+    batch of one, as luna_b200_solve runs it: on an 8-CTA cluster for the long grids, No >=
+    16384, on one CTA otherwise), device time with CUDA events, for a stratified subset of
+    the completed instances: in each of the two strata (cluster, single CTA) k quantiles of
+    their integration times in the single-CTA FP64 batch. Returns the subset's own
+    sims/hour, the scan estimate (per stratum, the batch's per-instance times scaled by the
+    subset's measured/batch ratio) and the per-instance record."""
     done = [i for i in range(len(probs)) if status64[i] == 0]
-    order = sorted(done, key=lambda i: dur[i])
-    pick = sorted({order[min(len(order) - 1, int((j + 0.5) * len(order) / k))] for j in range(k)})
-    rows, t_sub, d_sub = [], 0.0, 0.0
-    for i in pick:
-        p = probs[i]
-        plan = P.Plan.from_transform(p.transform, _lib.PREC_FP64)
-        b = P.Batch([plan], SAVEN, np.linspace(0.0, p.grid.zmax, SAVEN), max_dt=p.grid.zmax / 2)
-        b.upload([p.linop], [p.Eω], [0.0], [1e-4], [p.grid.zmax])
-        ms = b.run()
-        st = b.download()[2][0]
-        rows.append({"instance": i, "gas": inst[i]["gas"], "No": p.grid.No, "steps": int(st.steps),
-                     "s": round(ms / 1e3, 3), "status": int(st.status)})
-        t_sub += ms / 1e3
-        d_sub += dur[i]
-        del b, plan
-    ok = len(done)
-    scan_s = float(np.sum([dur[i] for i in done])) * (t_sub / max(d_sub, 1e-30))
-    return 3600.0 * len(pick) / t_sub, 3600.0 * ok / scan_s, rows
+    strata = {True: [], False: []}
+    for i in done:
+        strata[probs[i].grid.No >= 16384].append(i)
+    rows, t_all, n_all, scan_s = [], 0.0, 0, 0.0
+    for big, members in strata.items():
+        if not members:
+            continue
+        order = sorted(members, key=lambda i: dur[i])
+        pick = sorted({order[min(len(order) - 1, int((j + 0.5) * len(order) / k))] for j in range(k)})
+        t_sub, d_sub = 0.0, 0.0
+        for i in pick:
+            p = probs[i]
+            plan = P.Plan.from_transform(p.transform, _lib.PREC_FP64)
+            b = P.Batch([plan], SAVEN, np.linspace(0.0, p.grid.zmax, SAVEN), max_dt=p.grid.zmax / 2)
+            b.upload([p.linop], [p.Eω], [0.0], [1e-4], [p.grid.zmax])
+            clusters = b.info()[1]
+            ms = b.run()
+            st = b.download()[2][0]
+            rows.append({"instance": i, "gas": inst[i]["gas"], "No": p.grid.No, "steps": int(st.steps),
+                         "s": round(ms / 1e3, 3), "status": int(st.status), "cluster": bool(clusters)})
+            t_sub += ms / 1e3
+            d_sub += dur[i]
+            del b, plan
+        t_all += t_sub
+        n_all += len(pick)
+        scan_s += float(np.sum([dur[i] for i in members])) * (t_sub / max(d_sub, 1e-30))
+    return 3600.0 * n_all / t_all, 3600.0 * len(done) / scan_s, rows
 
 
 def run_reference(args, world, rank):
@@ -780,6 +793,9 @@ def main():
                          "modal: TransModal RHS; surrogate: the learned surrogate's queries")
     ap.add_argument("--mixed-rtol", type=float, default=MIXED_RTOL,
                     help="relative tolerance of the mixed-precision integrations")
+    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
+                    help="precision of the timed batched scan (the other one is run once and "
+                         "reported beside it when the accuracy pass is on)")
     ap.add_argument("--sg-runs", type=int, default=2560, help="surrogate: solver runs of training data")
     ap.add_argument("--sg-epochs", type=int, default=60, help="surrogate: training epochs")
     ap.add_argument("--sg-spread", type=float, default=0.1,
@@ -817,9 +833,11 @@ def main():
     t_setup = time.perf_counter()
     inst, probs = build(world, rank, args.instances)
     n = len(probs)
-    plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
+    prec = _lib.PREC_FP64 if args.precision == "fp64" else _lib.PREC_MIXED
+    rtol = 1e-6 if prec == _lib.PREC_FP64 else args.mixed_rtol
+    plans = [P.Plan.from_transform(p.transform, prec) for p in probs]
     # each instance saves on its own GridCondition range(0, zmax, 201) with max_dz = zmax/2
-    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps, rtol=args.mixed_rtol,
+    batch = P.Batch(plans, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps, rtol=rtol,
                     flags=(_lib.SOLVE_NO_CLUSTERS if args.no_clusters else 0) |
                     (_lib.SOLVE_NO_DIST if args.no_dist else 0),
                     dist_min_no=args.dist_min_no)
@@ -888,14 +906,14 @@ def main():
     e2e_value = total_ok / e2e * 3600.0
     steps_all = sum(s.steps for s in stats)
     nrhs_all = sum(s.nrhs for s in stats)
-    alg_bytes = sum(s.steps * step_bytes(len(p.Eω), True) for s, p in zip(stats, probs))
+    alg_bytes = sum(s.steps * step_bytes(len(p.Eω), prec == _lib.PREC_MIXED) for s, p in zip(stats, probs))
     raman_of = [any(r.kind == "raman_field" for r in p.transform.resp) for p in probs]
     alg_flops = sum(s.steps * step_flops(p.grid.No, p.grid.N, rm) for s, p, rm in zip(stats, probs, raman_of))
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (ms / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "solve_kernel_scan_traffic.json")
-    if os.path.exists(tf):
+    if os.path.exists(tf) and prec == _lib.PREC_MIXED:  # captured on the mixed-precision solver
         with open(tf) as f:
             tj = json.load(f)
         traffic = tj.get("dram_bytes_per_rk_step", 0) * steps_all
@@ -908,48 +926,70 @@ def main():
     except Exception as e:
         timeline = {"error": str(e)[:200]}
     del batch
-    # ------------------------------------------------ accuracy: the same scan in plain FP64
-    acc, fp64b, plain = None, None, None
+    del plans
+    # ------------------------------------------------ accuracy against the plain FP64 path
+    acc, fp64b, plain, other = None, None, None, None
     if args.accuracy == "on" or (args.accuracy == "auto" and world == 1):
         from luna_b200 import accuracy as A
         t_acc = time.perf_counter()
-        plans64 = [P.Plan.from_transform(p.transform, _lib.PREC_FP64) for p in probs]
-        b64 = P.Batch(plans64, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps)
-        b64.upload(Lh, Yh, z0, dz0, zmax, zsaves, max_dts)
-        b64.set_priority(prios)
-        ms64 = b64.run()
-        S64 = [np.zeros((SAVEN, len(p.Eω)), dtype=np.complex128) for p in probs]
-        _, _, st64 = b64.download(S64, None)
-        be64, _ = b64.timeline()
-        dur64 = be64[:, 1] - be64[:, 0]
-        del b64
-        per = []
-        for i, p in enumerate(probs):
-            if stats[i].status != 0 or st64[i].status != 0:
-                per.append(None)
-                continue
-            k = min(stats[i].nsaved, st64[i].nsaved)
-            per.append(A.compare(Sh[i][:k], S64[i][:k], p.grid.ω))
-        ok64 = sum(1 for s in st64 if s.status == 0)
-        acc = A.summary(per)
-        acc.update({"reference": "the same scan in plain FP64 on this GPU (the path checked against "
-                                 "the FP64 oracle), every save of every completed instance",
+
+        def scan_once(pr, flags=0, rt=1e-6):
+            pl = [P.Plan.from_transform(p.transform, pr) for p in probs]
+            bb = P.Batch(pl, SAVEN, np.linspace(0.0, 1.0, SAVEN), max_steps=args.max_rk_steps, rtol=rt, flags=flags)
+            bb.upload(Lh, Yh, z0, dz0, zmax, zsaves, max_dts)
+            bb.set_priority(prios)
+            ms_ = bb.run()
+            S_ = [np.zeros((SAVEN, len(p.Eω)), dtype=np.complex128) for p in probs]
+            _, _, st_ = bb.download(S_, None)
+            be_, _ = bb.timeline()
+            return ms_, S_, st_, be_[:, 1] - be_[:, 0]
+
+        def compare(S_, st_, Sref, stref):
+            per = []
+            for i, p in enumerate(probs):
+                if st_[i].status != 0 or stref[i].status != 0:
+                    per.append(None)
+                    continue
+                k = min(st_[i].nsaved, stref[i].nsaved)
+                per.append(A.compare(S_[i][:k], Sref[i][:k], p.grid.ω))
+            out = A.summary(per)
+            out["status_agree"] = int(sum(1 for x, y in zip(st_, stref) if x.status == y.status))
+            return out
+
+        # the plain path's arithmetic: every instance on one CTA with the FP64 solver of
+        # luna_b200_solve (no clusters)
+        ms64, S64, st64, dur64 = scan_once(_lib.PREC_FP64, flags=_lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS)
+        ok64 = sum(1 for x in st64 if x.status == 0)
+        acc = compare(Sh, stats, S64, st64)
+        acc.update({"reference": "the same scan integrated by the plain FP64 path's solver (one CTA per "
+                                 "instance, the arithmetic of luna_b200_solve), every save of every completed instance",
                     "bar": 1e-3, "met": bool(acc.get("spectral_max", 1.0) <= 1e-3),
-                    "status_agree": int(sum(1 for a, c in zip(stats, st64) if a.status == c.status)),
-                    "steps_mixed": int(sum(s.steps for s in stats)),
-                    "steps_fp64": int(sum(s.steps for s in st64))})
-        fp64b = {"value": 3600.0 * ok64 / (ms64 / 1e3), "unit": "sims/hour", "ms": ms64,
-                 "completed": ok64, "long_pole_s": float(np.max(dur64)),
-                 "method": "the whole scan in plain FP64 as one batch (single-CTA persistent solver), device time"}
-        del S64
+                    "steps_timed": int(sum(x.steps for x in stats)),
+                    "steps_reference": int(sum(x.steps for x in st64))})
+        if prec == _lib.PREC_FP64:
+            acc["note"] = ("both are FP64 with different summation orders: an instance above the bar is one whose "
+                           "FP64 result is not determined beyond rounding (it diverges at this level under any "
+                           "rounding-level change, e.g. a 1-ulp change of its first step)")
+        fp64b = {"value": 3600.0 * ok64 / (ms64 / 1e3), "unit": "sims/hour", "ms": ms64, "completed": ok64,
+                 "long_pole_s": float(np.max(dur64)),
+                 "method": "the whole scan in plain FP64 as one batch on single CTAs, device time"}
+        # the other precision, once
+        oprec = _lib.PREC_MIXED if prec == _lib.PREC_FP64 else _lib.PREC_FP64
+        mso, So, sto, _ = scan_once(oprec, rt=args.mixed_rtol if oprec == _lib.PREC_MIXED else 1e-6)
+        oko = sum(1 for x in sto if x.status == 0)
+        other = {"precision": "mixed" if oprec == _lib.PREC_MIXED else "fp64",
+                 "value": 3600.0 * oko / (mso / 1e3), "unit": "sims/hour", "ms": mso,
+                 "accuracy": compare(So, sto, S64, st64)}
+        del So, S64
         if not args.no_cpu_baseline and args.instances == 256:
             try:
-                v_sub, v_scan, rows = plain_fp64_measured(inst, probs, dur64, [s.status for s in st64])
+                v_sub, v_scan, rows = plain_fp64_measured(inst, probs, dur64, [x.status for x in st64])
                 plain = {"value": v_scan, "unit": "sims/hour", "subset_value": v_sub,
                          "method": ("plain FP64 drop-in measured: one single-instance FP64 solve after another "
-                                    f"(device time) for {len(rows)} instances stratified by their FP64 batch time; "
-                                    "value = the scan's sims/hour with the batch's per-instance times scaled by "
-                                    "the subset's measured/batch ratio, subset_value = the subset's own"),
+                                    f"(device time; 8-CTA clusters for No >= 16384) for {len(rows)} instances, "
+                                    "8 quantiles of the single-CTA FP64 batch time in each of the two strata; value = "
+                                    "the scan's sims/hour with each stratum's per-instance batch times scaled by its "
+                                    "subset's measured/batch ratio, subset_value = the subset's own"),
                          "subset": rows, "speedup_of_value": value / v_scan}
             except Exception as e:  # report, do not hide
                 plain = {"value": None, "error": str(e)[:200]}
@@ -958,8 +998,10 @@ def main():
         line = {"metric": METRIC, "value": value, "unit": "sims/hour", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32+f64", "data": "synthetic (seeded scan draw, no noise)",
-                "config": scan_config(), "implementation": IMPL, "mixed_rtol": args.mixed_rtol,
+                "dtype": "f64" if prec == _lib.PREC_FP64 else "f32+f64",
+                "data": "synthetic (seeded scan draw, no noise)",
+                "config": scan_config(), "implementation": IMPL[args.precision],
+                "rtol": rtol,
                 "instances_this_rank": n, "failed_instances": failed,
                 "e2e": {"value": e2e_value, "unit": "sims/hour", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e * 1e3},
@@ -976,17 +1018,20 @@ def main():
             line["roofline_compute"] = {"error": fpk_err}
         else:
             ach_tf = alg_flops / (ms / 1e3) / 1e12
+            pk = fpk["fp64"] if prec == _lib.PREC_FP64 else fpk["fp32"]
             line["roofline_compute"] = {
-                "bound": "fp32", "achieved": ach_tf, "peak": fpk["fp32"], "unit": "TFLOP/s",
-                "frac": ach_tf / fpk["fp32"], "peak_fp64": fpk["fp64"], "peak_kind": "measured (FMA microkernel, this run)",
+                "bound": "fp64" if prec == _lib.PREC_FP64 else "fp32", "achieved": ach_tf, "peak": pk,
+                "unit": "TFLOP/s", "frac": ach_tf / pk, "peak_fp32": fpk["fp32"], "peak_fp64": fpk["fp64"],
+                "peak_kind": "measured (FMA microkernel, this run)",
                 "flops_per_scan": alg_flops,
                 "note": "algorithmic flops of every RK step (transforms 2.5 N log2 N, pointwise responses, stage combines) over the step time"}
             if traffic:
                 line["roofline"]["traffic_over_algorithmic"] = traffic / alg_bytes
         if acc is not None:
             line["accuracy"] = acc
-            line["fp64_batched"] = fp64b
-            line["fp64_batched"]["speedup_of_value"] = value / fp64b["value"]
+            line["fp64_single_cta_batched"] = fp64b
+            line["fp64_single_cta_batched"]["speedup_of_value"] = value / fp64b["value"]
+            line["other_precision"] = other
         if plain is not None:
             line["plain_fp64"] = plain
         if not args.no_cpu_baseline and world == 1:

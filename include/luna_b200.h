@@ -120,9 +120,9 @@ typedef struct {
     long long nreplay;
     int flags;                                 /* LUNA_SOLVE_* bits, 0 for the defaults     */
     long long stats_cap;                       /* rows of per-step statistics; 0: off       */
-    int dist_min_no;                           /* batches (mixed precision): instances with at
-                                                  least this many oversampled samples run on a
-                                                  cluster of CTAs each; 0: 16384            */
+    int dist_min_no;                           /* batches: instances with at least this many
+                                                  oversampled samples run on a cluster of CTAs
+                                                  each (in the batch's precision); 0: 16384  */
 } luna_solve_opts;
 
 /* Per-step statistics (Stats.default, Stats.jl:495-532, for a mode-averaged field-resolved

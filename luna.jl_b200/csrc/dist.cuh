@@ -467,7 +467,7 @@ struct RateF {
 // of the CTAs before it) and the integrands' first samples exchanged through the cluster.
 // Mixed precision: rates, ionisation fractions (1 - exp(-x) as -expm1(-x)) and the
 // ionisation-loss current are FP32 per sample (kept in shared memory at [s*T + tid]
-// between the passes), the running integrals FP64.
+// between the passes), the running integrals FP64. FP64: every quantity FP64.
 template <typename Rl, int NS>
 __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, double sc, int ip, int ir, double kc,
                                          double rc) {
@@ -478,8 +478,11 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     const double dt = r.dt, er = r.eratio, preion = r.preion, coef = r.coef;
     const float ipf = (float)r.ionpot;
     const int pr0 = tid * (NS / 2);
-    float* rrb = reinterpret_cast<float*>(d.stg);  // rates (the staged spectrum is dead)
-    float* frb = reinterpret_cast<float*>(d.fb);   // ionisation fractions
+    // per-sample rates and ionisation fractions in the solver's precision: FP32 in mixed
+    // precision, FP64 (the arithmetic of the single-CTA FP64 plasma scan) otherwise
+    constexpr bool F64 = sizeof(Rl) == 8;
+    Rl* rrb = reinterpret_cast<Rl*>(d.stg);  // rates (the staged spectrum is dead)
+    Rl* frb = reinterpret_cast<Rl*>(d.fb);   // ionisation fractions
     Rl ev[NS];  // stored field samples; E = ev * sc
 #pragma unroll
     for (int h = 0; h < NS / 2; ++h) {
@@ -490,8 +493,18 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     auto E = [&](int s) -> double { return (double)ev[s] * sc; };
     // pass A: rates; exclusive scan of the thread sums and the block total
     double racc = 0;
-    float r0 = 0;
-    {
+    Rl r0 = 0;
+    if constexpr (F64) {
+        const bool ppt = r.kind == LUNA_RESP_PLASMA_PPT;
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const double aE = fabs(E(s));
+            const double rv = ppt ? ppt_rate<double>(r, aE, d.flag) : adk_rate<double>(r, aE);
+            rrb[s * T + tid] = rv;
+            racc += rv;
+            if (s == 0) r0 = rv;
+        }
+    } else {
         RateF rf;
         rf.init(r);
 #pragma unroll
@@ -526,8 +539,14 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
         for (int s = 0; s < NS; ++s) {
             const double rr = rrb[s * T + tid];
             S += rr;
-            const float fx = (float)(dt * (S - 0.5 * (y0r + rr)));
-            const float fr = (float)(preion - (double)expm1f(-fx));
+            Rl fr;
+            if constexpr (F64) {
+                const double f = dt * (S - 0.5 * (y0r + rr));
+                fr = preion + 1.0 - ((f == 0.0) ? 1.0 : exp(-f));
+            } else {
+                const float fx = (float)(dt * (S - 0.5 * (y0r + rr)));
+                fr = (float)(preion - (double)expm1f(-fx));
+            }
             frb[s * T + tid] = fr;
             const double ph = (double)fr * er * E(s);
             ph_acc += ph;
@@ -545,12 +564,18 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     const double y0p = drem(d.xs, 0)[3];
     // the current density of sample s, advancing the running phase integral Tv
     auto current = [&](int s, double& Tv) -> double {
-        const float rr = rrb[s * T + tid], fr = frb[s * T + tid];
+        const Rl rr = rrb[s * T + tid], fr = frb[s * T + tid];
         const double ph = (double)fr * er * E(s);
         Tv += ph;
-        const float Ef = (float)E(s);
-        const float ion = (Ef != 0.0f) ? ipf * rr * (1.0f - fr) / Ef : 0.0f;
-        return dt * (Tv - 0.5 * (y0p + ph)) + (double)ion;
+        double ion;
+        if constexpr (F64) {
+            const double Es = E(s);
+            ion = (fabs(Es) > 0) ? r.ionpot * rr * (1.0 - fr) / Es : 0.0;
+        } else {
+            const float Ef = (float)E(s);
+            ion = (double)((Ef != 0.0f) ? ipf * rr * (1.0f - fr) / Ef : 0.0f);
+        }
+        return dt * (Tv - 0.5 * (y0p + ph)) + ion;
     };
     double J_acc = 0, J_first = 0;
     {

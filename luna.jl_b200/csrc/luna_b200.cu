@@ -616,6 +616,96 @@ int dist_partition(luna_batch* b, const double* pr) {
     return LUNA_OK;
 }
 
+// Distributed instances of a batch: the long ones (No >= dist_min_no, default 16384) that
+// the cluster solver supports, each on DIST_R CTAs, in the batch's precision (FP32 or FP64
+// sub-transforms and responses). Sets b->elig and the partition when at least one cluster
+// fits on the device; a batch without eligible instances is left unchanged.
+template <typename Rl>
+int dist_setup(luna_batch* b, const luna_solve_opts* opts, int nsm) {
+    const int n = b->n;
+    const int maxs = max_smem_optin();
+    const size_t cs = sizeof(cpx<Rl>);
+    std::vector<int> dl;
+    std::vector<double> cost(n);
+    size_t dsm = 0;
+    for (int i = 0; i < n; ++i) {
+        const LunaInst& I = b->h[i];
+        const int M = I.No / 2, Mc = I.N / 2;
+        const bool ok = I.kind == 0 && !I.grad && !needs_hilbert(I) && opts->stats_cap <= 0 &&
+                        I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
+                        M % DIST_R == 0 && M / DIST_R >= 2 * LUNA_BLOCK &&
+                        M / DIST_R <= FftEmax<Rl>::v * LUNA_BLOCK && Mc % DIST_R == 0 &&
+                        Mc / DIST_R >= 64 && Mc <= M && I.Nw <= Mc + 1 &&
+                        dist_smem_bytes(I.No, cs) <= (size_t)maxs;
+        if (ok) {
+            dl.push_back(i);
+            dsm = std::max(dsm, dist_smem_bytes(I.No, cs));
+        }
+        cost[i] = (double)I.No * std::log2((double)I.No) * (has_raman(I) ? 2.0 : 1.0);
+    }
+    if (dl.empty()) return LUNA_OK;
+    const int sm = (int)std::max<size_t>((size_t)b->smem, dsm);
+    if (cudaFuncSetAttribute(solve_kernel_dist<Rl, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
+        cudaFuncSetAttribute(solve_kernel<Rl, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
+        return fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size (distributed solver)");
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = DIST_R;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(DIST_R * 32, 1, 1);
+    cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+    cfg.dynamicSmemBytes = sm;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int ncl = 0;
+    if (cudaOccupancyMaxActiveClusters(&ncl, solve_kernel_dist<Rl, Rl>, &cfg) != cudaSuccess || ncl < 1) {
+        cudaGetLastError();
+        return LUNA_OK;
+    }
+    b->smem = sm;
+    b->elig = dl;
+    b->ncl_max = ncl;
+    b->nsm = nsm;
+    if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_reg, sizeof(int) * n) ||
+        dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
+        return LUNA_ERR_CUDA;
+    return dist_partition(b, cost.data());
+}
+
+// The distributed solver on its clusters and the single-CTA solver on the SMs left over
+// (second stream), both in the batch's precision.
+template <typename Rl>
+int dist_launch(luna_batch* b, const TwTab<Rl>& tw) {
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = DIST_R;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(b->dist_grid, 1, 1);
+    cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+    cfg.dynamicSmemBytes = b->smem;
+    cfg.stream = b->stream;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int* c = b->d_cl_counters;
+    if (b->reg_grid > 0) {
+        CK(cudaEventRecord(b->evf, b->stream));
+        CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
+    }
+    CK(cudaLaunchKernelEx(&cfg, solve_kernel_dist<Rl, Rl>, b->d_insts, (const int*)b->d_dist, b->ndist, c,
+                          (const int*)b->d_reg, b->nreg, c + 1, tw, b->smem));
+    if (b->reg_grid > 0) {
+        solve_kernel<Rl, Rl><<<b->reg_grid, LUNA_BLOCK, b->smem, b->stream2>>>(b->d_insts, b->nreg, c + 1, tw, b->smem,
+                                                                              (const int*)b->d_reg);
+        CK(cudaEventRecord(b->evj, b->stream2));
+        CK(cudaStreamWaitEvent(b->stream, b->evj, 0));
+    }
+    return LUNA_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1059,63 +1149,9 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
     }
     if (occ < 1) return bail(fail(LUNA_ERR_CUDA, "batch_create: solver kernel does not fit on an SM"));
     b->grid = std::min(n, nsm * occ);
-    if (prec == LUNA_PREC_MIXED && !(opts->flags & (LUNA_SOLVE_NO_CLUSTERS | LUNA_SOLVE_NO_DIST))) {
-        // distributed instances: the long ones (No >= LUNA_DIST_MIN_NO) that the cluster
-        // solver supports, each on DIST_R CTAs
-        const int maxs = max_smem_optin();
-        std::vector<int> dl, reg;
-        std::vector<double> cost(n);
-        size_t dsm = 0;
-        for (int i = 0; i < n; ++i) {
-            const LunaInst& I = b->h[i];
-            const int M = I.No / 2, Mc = I.N / 2;
-            const bool ok = I.kind == 0 && !I.grad && !needs_hilbert(I) && opts->stats_cap <= 0 &&
-                            I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
-                            M % DIST_R == 0 && M / DIST_R >= 2 * LUNA_BLOCK &&
-                            M / DIST_R <= FftEmax<float>::v * LUNA_BLOCK && Mc % DIST_R == 0 &&
-                            Mc / DIST_R >= 64 && Mc <= M && I.Nw <= Mc + 1 &&
-                            dist_smem_bytes(I.No, sizeof(float2)) <= (size_t)maxs;
-            if (ok) {
-                dl.push_back(i);
-                dsm = std::max(dsm, dist_smem_bytes(I.No, sizeof(float2)));
-            } else {
-                reg.push_back(i);
-            }
-            cost[i] = (double)I.No * std::log2((double)I.No) * (has_raman(I) ? 2.0 : 1.0);
-        }
-        if (!dl.empty()) {
-            const int sm = (int)std::max<size_t>((size_t)b->smem, dsm);
-            if (cudaFuncSetAttribute(solve_kernel_dist<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
-                cudaFuncSetAttribute(solve_kernel<float, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
-                return bail(fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size (distributed solver)"));
-            cudaLaunchConfig_t cfg = {};
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeClusterDimension;
-            at[0].val.clusterDim.x = DIST_R;
-            at[0].val.clusterDim.y = 1;
-            at[0].val.clusterDim.z = 1;
-            cfg.gridDim = dim3(DIST_R * 32, 1, 1);
-            cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
-            cfg.dynamicSmemBytes = sm;
-            cfg.attrs = at;
-            cfg.numAttrs = 1;
-            int ncl = 0;
-            if (cudaOccupancyMaxActiveClusters(&ncl, solve_kernel_dist<float, float>, &cfg) != cudaSuccess || ncl < 1) {
-                cudaGetLastError();
-                ncl = 0;
-            }
-            if (ncl >= 1) {
-                b->smem = sm;
-                b->elig = dl;
-                b->ncl_max = ncl;
-                b->nsm = nsm;
-                if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_reg, sizeof(int) * n) ||
-                    dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
-                    return bail(LUNA_ERR_CUDA);
-                std::vector<double> pr(cost);
-                if (int rc = dist_partition(b, pr.data())) return bail(rc);
-            }
-        }
+    if (!(opts->flags & (LUNA_SOLVE_NO_CLUSTERS | LUNA_SOLVE_NO_DIST))) {
+        const int rc = (prec == LUNA_PREC_FP64) ? dist_setup<double>(b, opts, nsm) : dist_setup<float>(b, opts, nsm);
+        if (rc) return bail(rc);
     }
     if (b->elig.empty() && prec == LUNA_PREC_MIXED && !(opts->flags & LUNA_SOLVE_NO_CLUSTERS)) {
         // Raman clusters for the instances whose Raman buffer alone overflows one CTA
@@ -1233,34 +1269,11 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
     CK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
     if (b->cl_grid > 0 || b->dist_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
-    if (b->precision == LUNA_PREC_FP64) {
+    if (b->dist_grid > 0) {
+        rc = (b->precision == LUNA_PREC_FP64) ? dist_launch<double>(b, tw.d) : dist_launch<float>(b, tw.f);
+        if (rc) return rc;
+    } else if (b->precision == LUNA_PREC_FP64) {
         solve_kernel<double, double><<<b->grid, LUNA_BLOCK, b->smem, b->stream>>>(b->d_insts, b->n, b->d_counter, tw.d, b->smem, nullptr);
-    } else if (b->dist_grid > 0) {
-        cudaLaunchConfig_t cfg = {};
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = DIST_R;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.gridDim = dim3(b->dist_grid, 1, 1);
-        cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
-        cfg.dynamicSmemBytes = b->smem;
-        cfg.stream = b->stream;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        int* c = b->d_cl_counters;
-        if (b->reg_grid > 0) {
-            CK(cudaEventRecord(b->evf, b->stream));
-            CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
-        }
-        CK(cudaLaunchKernelEx(&cfg, solve_kernel_dist<float, float>, b->d_insts, (const int*)b->d_dist, b->ndist, c,
-                              (const int*)b->d_reg, b->nreg, c + 1, tw.f, b->smem));
-        if (b->reg_grid > 0) {
-            solve_kernel<float, float><<<b->reg_grid, LUNA_BLOCK, b->smem, b->stream2>>>(
-                b->d_insts, b->nreg, c + 1, tw.f, b->smem, (const int*)b->d_reg);
-            CK(cudaEventRecord(b->evj, b->stream2));
-            CK(cudaStreamWaitEvent(b->stream, b->evj, 0));
-        }
     } else if (b->cl_grid > 0) {
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute at[1];

@@ -334,7 +334,8 @@ def generate(params, precision=1, rtol=1e-6, flength=3.0, saveN=201, chunk=256, 
                                    [q["τfwhm"]] * saveN, zs, [q["gas"]] * saveN))
             runs.append(np.full(saveN, c0 + i))
         del b, plans
-        log(f"data: {min(c0 + chunk, len(probs))}/{len(probs)} runs, {dev_s:.1f} s of device time")
+        if log:
+            log(f"data: {min(c0 + chunk, len(probs))}/{len(probs)} runs, {dev_s:.1f} s of device time")
     return np.concatenate(xs), torch.cat(ts), np.concatenate(runs), status, dev_s
 
 

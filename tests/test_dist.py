@@ -30,9 +30,9 @@ def _case(gas, trange, plasma=None, energy=100e-6, flength=0.2):
                                plasma=plasma, saveN=11)
 
 
-def _batch(probs, flags=0, dist_min_no=16384, priority=None, steplog_cap=0, replay=None):
+def _batch(probs, flags=0, dist_min_no=16384, priority=None, steplog_cap=0, replay=None, prec=_lib.PREC_MIXED):
     from luna_b200 import plan as P
-    plans = [P.Plan.from_transform(p.transform, _lib.PREC_MIXED) for p in probs]
+    plans = [P.Plan.from_transform(p.transform, prec) for p in probs]
     b = P.Batch(plans, 11, np.linspace(0.0, 1.0, 11), flags=flags, dist_min_no=dist_min_no,
                 steplog_cap=steplog_cap, replay=replay)
     b.upload([p.linop for p in probs], [p.Eω for p in probs], [0.0] * len(probs),
@@ -93,3 +93,30 @@ def test_mixed_batch_of_distributed_and_single_instances():
         assert r.status == 0 and s.status == 0
         assert abs(r.steps - s.steps) <= 2
         assert _rel(r.Eω[-1], s.Eω[-1]) < 2e-3
+
+
+# ------------------------------------------------------------------ FP64 clusters
+@pytest.mark.parametrize("gas,trange,flength", [("Ar", 1e-12, 0.1), ("H2", 2e-12, 0.03)])
+def test_fp64_distributed_matches_oracle_on_its_step_sequence(gas, trange, flength):
+    """The distributed solver in FP64 (PPT plasma on 16384 points; ADK plasma and Raman on
+    32768 points) follows the oracle's step sequence with every save within 1e-10, as the
+    single-CTA FP64 solver does."""
+    p = _case(gas, trange, flength=flength)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    (rd,), info = _batch([p], prec=_lib.PREC_FP64, replay=replay)
+    assert info[1] == 1 and rd.status == 0 and rd.steps == ores.steps
+    for a, b in zip(rd.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+
+
+def test_fp64_distributed_free_running_matches_single_cta():
+    """Free-running, the FP64 distributed and single-CTA solvers take the same steps and
+    agree to the rounding of their different summation orders."""
+    p = _case("Ar", 1e-12, flength=0.2)
+    (rd,), info = _batch([p], prec=_lib.PREC_FP64)
+    (rs,), info0 = _batch([p], prec=_lib.PREC_FP64, flags=_lib.SOLVE_NO_DIST)
+    assert info[1] == 1 and info0[1] == 0
+    assert rd.status == rs.status == 0 and rd.steps == rs.steps
+    for a, b in zip(rd.Eω, rs.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)

@@ -668,7 +668,7 @@ def run_surrogate(args, world, rank, local):
     model = S.Ensemble(members=4, seed=11, batch=4096)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    hist = S.train(model, xt, Tt, epochs=args.sg_epochs, log=log)
+    hist = S.train(model, xt, Tt, epochs=args.sg_epochs, lr=(args.sg_lr, 1e-5), log=log)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     steps = args.sg_epochs * (xt.shape[0] // model.batch)
@@ -676,6 +676,9 @@ def run_surrogate(args, world, rank, local):
     xq, Tq = x[~trm].contiguous(), T[~trm].contiguous()
     mean, spread = S.predict(model, xq)
     e = S.spectral_error(mean, Tq)
+    # the same over the bins within 3 decades of the run's input peak (the informative part)
+    inf = Tq[:, :S.NSPEC] > -3.0
+    e3 = (((mean[:, :S.NSPEC] - Tq[:, :S.NSPEC]) ** 2 * inf).sum(dim=1) / inf.sum(dim=1).clamp(min=1)).sqrt()
     e_env = ((mean[:, S.NSPEC:] - Tq[:, S.NSPEC:]) ** 2).mean(dim=1).sqrt()
     e_nn = S.spectral_error(S.nearest_neighbour(xt, Tt, xq), Tq)
     flag = spread > args.sg_spread
@@ -752,6 +755,7 @@ def run_surrogate(args, world, rank, local):
                 "accuracy": {"heldout_points": int(xq.shape[0]),
                              "log_spectrum_rms_decades": {"mean": float(e.mean()), "median": float(e.median()),
                                                           "p90": float(torch.quantile(e, 0.9))},
+                             "log_spectrum_rms_top3_decades": {"mean": float(e3.mean()), "median": float(e3.median())},
                              "envelope_rms": float(e_env.mean()),
                              "nearest_training_point": {"mean": float(e_nn.mean()), "median": float(e_nn.median())},
                              "audit_1pct": {"points": int(audit.numel()), "mean": float(e[audit].mean())},
@@ -793,11 +797,14 @@ def main():
                          "modal: TransModal RHS; surrogate: the learned surrogate's queries")
     ap.add_argument("--mixed-rtol", type=float, default=MIXED_RTOL,
                     help="relative tolerance of the mixed-precision integrations")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="shapes from the fixed work-estimate rule instead of the measured autotuner")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="precision of the timed batched scan (the other one is run once and "
                          "reported beside it when the accuracy pass is on)")
     ap.add_argument("--sg-runs", type=int, default=2560, help="surrogate: solver runs of training data")
-    ap.add_argument("--sg-epochs", type=int, default=60, help="surrogate: training epochs")
+    ap.add_argument("--sg-epochs", type=int, default=400, help="surrogate: training epochs")
+    ap.add_argument("--sg-lr", type=float, default=2e-3, help="surrogate: peak learning rate")
     ap.add_argument("--sg-spread", type=float, default=0.1,
                     help="surrogate: ensemble spread (decades) above which a query goes to the solver")
     args = ap.parse_args()
@@ -877,7 +884,19 @@ def main():
         fpk, fpk_err = None, str(e)[:200]
     prios = [scan.schedule_priority(p, q) for p, q in zip(inst, probs)]
     batch.upload(Lh, Yh, z0, dz0, zmax, zsaves, max_dts)
-    batch.set_priority(prios)
+    tune = None
+    if not args.no_autotune and not (args.no_dist or args.no_clusters):
+        # shapes and processing order from measured ms per RK step of each grid class
+        from luna_b200 import autotune
+        table, tune_s = autotune.measure(probs, prec)
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        shapes, tprios, _ = autotune.schedule(inst, probs, table, nsm)
+        batch.set_shapes(shapes)
+        batch.set_priority(tprios)
+        tune = {"ms_per_rk_step": table, "tune_s": round(tune_s, 1), "cluster_shapes": int((shapes == 2).sum()),
+                "rule": "cluster when faster for the class and the predicted single-CTA time is above the mean SM load"}
+    else:
+        batch.set_priority(prios)
     kinfo = batch.info()
     for _ in range(args.warmup):
         batch.run()
@@ -1007,7 +1026,7 @@ def main():
                         "d2h_bytes_per_step": d2h, "ms_per_step": e2e * 1e3},
                 "gpu_launches": args.steps * kinfo[0],
                 "scheduling": {"kernels_per_step": kinfo[0], "cluster_instances": kinfo[1],
-                               "clusters": kinfo[2]},
+                               "clusters": kinfo[2], "autotune": tune},
                 "rk_steps_per_scan": steps_all, "rhs_evals_per_s": nrhs_all / (ms / 1e3),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                              "frac": achieved / hbm, "traffic": traffic,

@@ -260,6 +260,12 @@ int luna_b200_batch_set_priority(luna_batch* b, const double* priority);
  * start and end of its integration in seconds from the earliest start ([2*n] doubles) and
  * the SM that integrated it ([n] ints, may be NULL). */
 int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm);
+/* Shape of every instance for the next luna_b200_batch_set_priority (no counterpart in the
+ * reference; an autotuner's decision): [n] ints, 0 = decided from the work estimates (an
+ * eligible instance whose estimate is at least the mean load of an SM runs on a cluster),
+ * 1 = one CTA, 2 = a cluster of CTAs when the instance is eligible (one CTA otherwise);
+ * NULL restores 0 for all. */
+int luna_b200_batch_set_shapes(luna_batch* b, const int* shape);
 /* Step sequence of instance i for the next runs (a verification aid, no counterpart in the
  * reference; the per-instance form of luna_solve_opts.replay): [2*nreplay] doubles, the
  * (dz, accepted) of each step as luna_b200_batch_steplog records them (columns 1 and 3);

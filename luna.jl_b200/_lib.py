@@ -108,7 +108,7 @@ EXPORTS = [
     "luna_b200_batch_info", "luna_b200_batch_stats", "luna_b200_plan_set_gradient",
     "luna_b200_plan_linop", "luna_b200_modal_plan_create", "luna_b200_modal_plan_destroy",
     "luna_b200_modal_rhs", "luna_b200_modal_rhs_device", "luna_b200_modal_solve",
-    "luna_b200_batch_set_replay",
+    "luna_b200_batch_set_replay", "luna_b200_batch_set_shapes",
 ]
 
 _lib = None
@@ -169,6 +169,7 @@ def load():
     lib.luna_b200_batch_info.argtypes = [c_void_p, POINTER(c_int), POINTER(c_int), POINTER(c_int)]
     lib.luna_b200_batch_set_priority.argtypes = [c_void_p, PD]
     lib.luna_b200_batch_set_replay.argtypes = [c_void_p, c_int, PD, c_longlong]
+    lib.luna_b200_batch_set_shapes.argtypes = [c_void_p, POINTER(c_int)]
     lib.luna_b200_batch_timeline.argtypes = [c_void_p, PD, POINTER(c_int)]
     lib.luna_b200_qdht_device.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p]
     lib.luna_b200_last_error.restype = ctypes.c_char_p

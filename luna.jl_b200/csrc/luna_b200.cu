@@ -559,6 +559,7 @@ struct luna_batch {
     int ndist = 0, dist_grid = 0, ncl_max = 0, nsm = 0;
     int* d_dist = nullptr;
     std::vector<int> dist, elig;
+    std::vector<int> shape;  // per instance: 0 the work-estimate rule, 1 one CTA, 2 a cluster
 };
 
 namespace {
@@ -599,7 +600,10 @@ int dist_partition(luna_batch* b, const double* pr) {
     for (int i = 0; i < n; ++i) W += pr[i];
     const double thr = W / std::max(1, b->nsm);
     std::vector<char> isd(n, 0);
-    for (int i : b->elig) isd[i] = pr[i] >= thr;
+    for (int i : b->elig) {
+        const int sh = b->shape.empty() ? 0 : b->shape[i];
+        isd[i] = sh == 2 || (sh == 0 && pr[i] >= thr);
+    }
     b->dist.clear();
     b->reg.clear();
     for (int i = 0; i < n; ++i) (isd[i] ? b->dist : b->reg).push_back(i);
@@ -1391,6 +1395,18 @@ int luna_b200_batch_stats(luna_batch* b, int i, double* stats) {
 int luna_b200_batch_steplog(luna_batch* b, int i, double* steplog) {
     if (!b || i < 0 || i >= b->n || !steplog || !b->steplogs[i]) return fail(LUNA_ERR_BAD_ARG, "batch_steplog: bad argument");
     CK(cudaMemcpy(steplog, b->steplogs[i], sizeof(double) * 4 * b->opts.steplog_cap, cudaMemcpyDeviceToHost));
+    return LUNA_OK;
+}
+
+int luna_b200_batch_set_shapes(luna_batch* b, const int* shape) {
+    if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_set_shapes: null batch");
+    if (!shape) {
+        b->shape.clear();
+    } else {
+        for (int i = 0; i < b->n; ++i)
+            if (shape[i] < 0 || shape[i] > 2) return fail(LUNA_ERR_BAD_ARG, "batch_set_shapes: shape must be 0, 1 or 2");
+        b->shape.assign(shape, shape + b->n);
+    }
     return LUNA_OK;
 }
 

@@ -284,6 +284,15 @@ class Batch:
         self._prio = _f64(priority)
         _lib.check(_lib.load().luna_b200_batch_set_priority(self._h, _lib.dptr(self._prio)))
 
+    def set_shapes(self, shapes):
+        """Per-instance shape for the next set_priority: 0 decided by the work estimates,
+        1 one CTA, 2 a cluster (when eligible); None restores 0 for all."""
+        if shapes is None:
+            _lib.check(_lib.load().luna_b200_batch_set_shapes(self._h, None))
+            return
+        arr = (_lib.c_int * len(self.plans))(*[int(x) for x in shapes])
+        _lib.check(_lib.load().luna_b200_batch_set_shapes(self._h, arr))
+
     def set_replay(self, i, replay):
         """Make instance i follow a recorded step sequence (flat (dz, accepted) pairs, e.g.
         columns 1 and 3 of its step log) from the next upload on; None removes it."""

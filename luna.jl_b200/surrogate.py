@@ -224,6 +224,12 @@ class Ensemble:
                                     self.lr, 0.9, 0.999, 1e-8, self.step_no, None, st), "adam")
         return bf["loss"]
 
+    def fold_output_scaling(self, mu, sd):
+        """Make the last layer predict sd * y + mu (FP32 master weights and BF16 copy)."""
+        self.W[-1] *= sd[None, :, None]
+        self.b[-1].mul_(sd[None, :]).add_(mu[None, :])
+        self.Wb[-1] = self.W[-1].to(self.torch.bfloat16)
+
     def predict(self, x):
         """Ensemble mean [B, 768] and spread [B] (largest member standard deviation over the
         spectral outputs, in decades) for standardised inputs x [B, 8]."""
@@ -348,11 +354,19 @@ class Standardise:
         return (x - self.mu) / self.sd
 
 
-def train(model, x, T, epochs=40, lr=(1e-3, 1e-5), seed=0, log=print):
+def train(model, x, T, epochs=40, lr=(1e-3, 1e-5), seed=0, log=print, standardise=True):
     """Adam over shuffled batches of the training set (x: standardised FP32 tensor [n, 8],
-    T: FP32 tensor [n, 768]) with a cosine learning-rate decay; returns the loss history."""
+    T: FP32 tensor [n, 768]) with a cosine learning-rate decay; returns the loss history.
+    With ``standardise`` every output is fitted in units of its spread over the training set
+    and the scaling is folded into the last layer afterwards (the trained network then
+    predicts the targets' own units)."""
     import torch
     n = x.shape[0]
+    mu = sd = None
+    if standardise:
+        mu = T.mean(dim=0)
+        sd = T.std(dim=0).clamp(min=1e-3)
+        T = ((T - mu) / sd).contiguous()
     B = model.batch
     steps = epochs * (n // B)
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -369,6 +383,8 @@ def train(model, x, T, epochs=40, lr=(1e-3, 1e-5), seed=0, log=print):
         if log and (ep % max(1, epochs // 8) == 0 or ep == epochs - 1):
             log(f"epoch {ep + 1}/{epochs}: loss per member {np.round(hist[-1], 5).tolist()}")
     model.check_timeout()
+    if standardise:
+        model.fold_output_scaling(mu, sd)
     return hist
 
 

@@ -68,17 +68,26 @@ def _pair(name):
 
 @pytest.mark.parametrize("name", ["gnlse", "readme"])
 def test_full_length_fp64_same_steps_and_fields(name):
+    """Free-running: the oracle's accepted-step sequence. Without plasma the fields match to
+    1e-10; with plasma the error estimates carry the ~1e-12 rounding of the cumulative
+    integrals, one step size of the 367 over 3 m moves by 4.3e-6 and the fields by 1.4e-8
+    (measured on a B200), so there the 1e-10 check is made on the oracle's step sequence."""
     p, saves, st, log, r = _pair(name)
     assert p.grid.N == 8192 and (name == "gnlse" or p.grid.No == 16384)
     assert st.status == 0 and r.status == 0
     assert r.steps == st.steps and r.rejected == st.rejected, (r.steps, st.steps)
-    # with plasma the error estimates carry the ~1e-12 rounding of the cumulative
-    # integrals; over the 367 steps of 3 m one step size moves by 4.3e-6 (measured on a B200)
     plasma = any(x.kind == "plasma" for x in p.transform.resp)
     np.testing.assert_allclose(r.steplog[:, 1], log[:, 1], rtol=1e-5 if plasma else 1e-9, atol=0)
     assert r.nsaved == st.nsaved == 201
     errs = [_rel(a, b) for a, b in zip(r.Eω, saves)]
-    assert max(errs) <= 1e-10, (max(errs), int(np.argmax(errs)))
+    assert max(errs) <= (1e-7 if plasma else 1e-10), (max(errs), int(np.argmax(errs)))
+    if plasma:
+        zmax = p.grid.zmax
+        replay = np.stack([log[:, 1], log[:, 3]], axis=1).ravel()
+        rr = P.solve_precon(p.transform, p.linop, p.Eω, 0.0, 1e-4, zmax, saveN=201, max_dt=zmax / 2,
+                            replay=replay)
+        errs = [_rel(a, b) for a, b in zip(rr.Eω, saves)]
+        assert rr.steps == st.steps and max(errs) <= 1e-10, (max(errs), int(np.argmax(errs)))
 
 
 # Mixed precision at full length: the FP32 transforms' error accumulates with the number of

@@ -771,6 +771,48 @@ def run_surrogate(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_surrogate_forward(args, world, rank, local):
+    """The surrogate's inference kernels alone (a randomly initialised ensemble of the
+    trained architecture; no data generation or training): one forward of the 4 members and
+    the ensemble statistics on args.sg_queries queries per step."""
+    import torch
+    from luna_b200 import surrogate as S
+    torch.cuda.set_device(local)
+    model = S.Ensemble(members=4, seed=11, batch=4096)
+    nq = args.sg_queries
+    x = torch.randn(nq, S.NFEAT, device="cuda")
+    for _ in range(args.warmup):
+        S.predict(model, x, chunk=nq)
+    st = torch.cuda.current_stream()
+    tms = []
+    for _ in range(args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        S.predict(model, x, chunk=nq)
+        e1.record(st)
+        e1.synchronize()
+        tms.append(e0.elapsed_time(e1))
+    model.check_timeout()
+    ms = statistics.median(tms)
+    flops = 4 * 2.0 * sum(k * n for k, n in zip(S.WIDTHS[:-1], S.WIDTHS[1:])) * nq
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            tpk, pk_kind = float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        tpk, pk_kind = 1590.0, "fallback"
+    ach = flops / (ms / 1e3) / 1e12
+    if rank == 0:
+        print(json.dumps({"metric": "surrogate forward queries/s (4 members, random weights)", "value": nq / (ms / 1e3),
+                          "unit": "queries/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                          "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                          "dtype": "bf16 (FP32 accumulate)", "data": "synthetic",
+                          "config": {"workload": "surrogate_forward: " + SG_WORKLOAD, "queries": nq},
+                          "gpu_launches": 8 * args.steps,
+                          "roofline": {"bound": "tensor", "kernel": "sg_gemm (forward, 4 members)", "achieved": ach,
+                                       "peak": tpk, "unit": "TFLOP/s", "frac": ach / tpk, "traffic": None,
+                                       "peak_kind": pk_kind}}), flush=True)
+
+
 # ----------------------------------------------------------------------------- GPU side
 def main():
     ap = argparse.ArgumentParser()
@@ -792,7 +834,9 @@ def main():
     ap.add_argument("--accuracy", choices=["auto", "on", "off"], default="auto",
                     help="FP64 pass over the same scan after the timed region and the error of "
                          "every mixed save against it (auto: on at one GPU)")
-    ap.add_argument("--workload", default="scan256", choices=["scan256", "radial", "modal", "surrogate"],
+    ap.add_argument("--sg-queries", type=int, default=1_000_064, help="surrogate_forward: queries per step")
+    ap.add_argument("--workload", default="scan256",
+                    choices=["scan256", "radial", "modal", "surrogate", "surrogate_forward"],
                     help="scan256: the batched capillary scan (headline); radial: TransRadial RHS; "
                          "modal: TransModal RHS; surrogate: the learned surrogate's queries")
     ap.add_argument("--mixed-rtol", type=float, default=MIXED_RTOL,
@@ -813,6 +857,8 @@ def main():
         return run_radial(args, world, rank, local)
     if args.workload == "modal":
         return run_modal(args, world, rank, local)
+    if args.workload == "surrogate_forward":
+        return run_surrogate_forward(args, world, rank, local)
     if args.workload == "surrogate":
         if args.impl == "reference":
             if rank == 0:

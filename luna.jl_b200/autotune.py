@@ -60,7 +60,7 @@ def _step_ms(prob, precision, flags, steps):
     return (t[1] - t[0]) / (steps[1] - steps[0]), on_cluster
 
 
-def measure(probs, precision, steps=(20, 80), refresh=False, log=None):
+def measure(probs, precision, steps=(20, 80), refresh=False, log=None, tries=8):
     """{class: {"single": ms/step, "cluster": ms/step or None}} for the classes of probs,
     from the cache where present."""
     path = _cache_path()
@@ -71,18 +71,26 @@ def measure(probs, precision, steps=(20, 80), refresh=False, log=None):
         cache = {}
     key = f"{_device_key()}|prec={precision}"
     table = cache.get(key, {}) if not refresh else {}
-    reps = {}
+    members = {}
     for p in probs:
-        reps.setdefault(grid_class(p), p)
+        members.setdefault(grid_class(p), []).append(p)
     t0 = time.perf_counter()
-    for c, p in reps.items():
-        if c in table:
+    for c, ps in members.items():
+        if c in table and table[c].get("single"):
             continue
-        single, _ = _step_ms(p, precision, _lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS, steps)
-        cl, on = _step_ms(p, precision, 0, steps)
-        table[c] = {"single": single, "cluster": cl if on else None}
+        # the first member of the class that runs the whole step budget (an instance that
+        # stops early, e.g. at the PPT table limit, gives no timing)
+        row = {"single": None, "cluster": None}
+        for p in ps[:tries]:
+            single, _ = _step_ms(p, precision, _lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS, steps)
+            if single is None:
+                continue
+            cl, on = _step_ms(p, precision, 0, steps)
+            row = {"single": single, "cluster": cl if on else None}
+            break
+        table[c] = row
         if log:
-            log(f"autotune {c}: single {single} ms/step, cluster {table[c]['cluster']} ms/step")
+            log(f"autotune {c}: single {row['single']} ms/step, cluster {row['cluster']} ms/step")
     cache[key] = table
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
@@ -100,12 +108,21 @@ def schedule(params, probs, table, nsm):
     w = np.array([scan.nonlinear_phase(p) ** 0.6 for p in params])
     single = np.zeros(n)
     cluster = np.full(n, np.inf)
+    # a class without a timing (every tried member stopped early) falls back to the
+    # transform-cost model of scan.schedule_priority, scaled like the measured classes
+    measured = [(int(c.split("=")[1].split("+")[0]), r["single"]) for c, r in table.items() if r.get("single")]
+    ref = np.mean([s / (No * np.log2(No)) for No, s in measured]) if measured else 1.0
     for i, p in enumerate(probs):
         row = table.get(grid_class(p), {})
-        s = row.get("single") or 1.0
+        s = row.get("single")
+        if not s:
+            No = p.grid.No
+            s = ref * No * np.log2(No) * (2.0 if "Raman" in grid_class(p) else 1.0)
         single[i] = w[i] * s
         if row.get("cluster"):
             cluster[i] = w[i] * row["cluster"]
+        elif not row.get("single") and p.grid.No >= 16384:
+            cluster[i] = single[i] / 2.0  # untimed long grid: assume the typical cluster gain
     mean_load = single.sum() / max(1, nsm)
     shapes = np.where((cluster < single) & (single >= mean_load), 2, 1)
     pred = np.where(shapes == 2, cluster, single)

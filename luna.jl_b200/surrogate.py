@@ -160,29 +160,33 @@ class Ensemble:
         self.err = torch.zeros(1, dtype=torch.int32, device=device)
         self._bufs = {}
 
-    def _buf(self, B):
-        if B not in self._bufs:
+    def _buf(self, B, train=True):
+        """Buffers for a batch of B: activations and outputs, and for training also the
+        pre-activations and gradients."""
+        if (B, train) not in self._bufs:
             t = self.torch
             bf = t.bfloat16
             m = self.members
-            self._bufs[B] = {
-                "x": t.empty(B, NFEAT, device=self.dev), "feat": t.empty(B, NIN, dtype=bf, device=self.dev),
-                "A": [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:-1]],
-                "Z": [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:-1]],
-                "dZ": [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:]],
-                "Y": t.empty(m, B, NOUT, device=self.dev),
-                "loss": t.zeros(m, dtype=t.float64, device=self.dev)}
-        return self._bufs[B]
+            d = {"feat": t.empty(B, NIN, dtype=bf, device=self.dev),
+                 "A": [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:-1]],
+                 "Y": t.empty(m, B, NOUT, device=self.dev),
+                 "loss": t.zeros(m, dtype=t.float64, device=self.dev)}
+            if train:
+                d["Z"] = [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:-1]]
+                d["dZ"] = [t.empty(m, B, n, dtype=bf, device=self.dev) for n in WIDTHS[1:]]
+            self._bufs[(B, train)] = d
+        return self._bufs[(B, train)]
 
     @staticmethod
     def _p(x):
         return ctypes.c_void_p(x.data_ptr()) if x is not None else None
 
-    def forward(self, x, B=None):
-        """Outputs [members, B, 768] FP32 for standardised inputs x [B, 8] (FP32 tensor)."""
+    def forward(self, x, B=None, keep=True):
+        """Outputs [members, B, 768] FP32 for standardised inputs x [B, 8] (FP32 tensor);
+        ``keep`` stores the pre-activations a backward pass needs."""
         lib, p = load(), self._p
         B = x.shape[0] if B is None else B
-        bf = self._buf(B)
+        bf = self._buf(B, keep)
         st = ctypes.c_void_p(self.torch.cuda.current_stream().cuda_stream)
         _check(lib.luna_sg_features(p(x), B, p(self.fourier), NFOURIER, p(bf["feat"]), NIN, st), "features")
         X, sX = bf["feat"], 0
@@ -191,7 +195,8 @@ class Ensemble:
             K, N = WIDTHS[l], WIDTHS[l + 1]
             last = l == nl - 1
             _check(lib.luna_sg_linear_fwd(p(X), sX, p(self.Wb[l]), p(self.b[l]), B, K, N, 0 if last else 1,
-                                          None if last else p(bf["A"][l]), None if last else p(bf["Z"][l]),
+                                          None if last else p(bf["A"][l]),
+                                          None if (last or not keep) else p(bf["Z"][l]),
                                           p(bf["Y"]) if last else None, self.members, p(self.err), st), "fwd")
             if not last:
                 X, sX = bf["A"][l], B * N
@@ -235,7 +240,7 @@ class Ensemble:
         spectral outputs, in decades) for standardised inputs x [B, 8]."""
         lib, p, t = load(), self._p, self.torch
         B = x.shape[0]
-        Y = self.forward(x, B)
+        Y = self.forward(x, B, keep=False)
         mean = t.empty(B, NOUT, device=self.dev)
         spread = t.empty(B, device=self.dev)
         _check(lib.luna_sg_ensemble(p(Y), self.members, B, NOUT, NSPEC, p(mean), p(spread),

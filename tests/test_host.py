@@ -160,3 +160,38 @@ def test_surrogate_cpu_gradients_match_finite_differences():
         fd = (S.reference_gradients(X, W, bp, T, rounding=False)[0] -
               S.reference_gradients(X, W, bm, T, rounding=False)[0]) / (2 * h)
         assert abs(fd - gb[l][0]) <= 1e-7 * max(1.0, abs(fd)), l
+
+
+def test_autotune_schedule_rule():
+    """Clusters go to the instances whose predicted single-CTA time is above the mean SM
+    load and whose grid class runs faster on a cluster; the priority is the predicted time
+    on the chosen shape (longest first)."""
+    from luna_b200 import autotune
+
+    class G:
+        def __init__(self, No):
+            self.No = No
+
+    class T:
+        def __init__(self, raman):
+            self.resp = [type("R", (), {"kind": "raman_field" if raman else "kerr_field"})()]
+
+    class Pr:
+        def __init__(self, No, raman=False):
+            self.grid, self.transform = G(No), T(raman)
+
+    inst = scan.draw_instances(6)
+    probs = [Pr(32768, True), Pr(32768), Pr(16384), Pr(8192), Pr(16384), Pr(8192)]
+    table = {"No=32768+Raman": {"single": 3.0, "cluster": 1.5}, "No=32768": {"single": 1.6, "cluster": 0.7},
+             "No=16384": {"single": 0.8, "cluster": 0.9}, "No=8192": {"single": 0.4, "cluster": None}}
+    shapes, prio, pred = autotune.schedule(inst, probs, table, nsm=2)
+    w = np.array([scan.nonlinear_phase(p) ** 0.6 for p in inst])
+    single = w * np.array([3.0, 1.6, 0.8, 0.4, 0.8, 0.4])
+    mean_load = single.sum() / 2
+    for i in range(6):
+        cl = {0: 1.5, 1: 0.7}.get(i)
+        want = 2 if (cl is not None and single[i] >= mean_load) else 1
+        assert shapes[i] == want, i
+        assert prio[i] == pytest.approx(w[i] * cl if want == 2 else single[i])
+    assert all(s == 1 for s in shapes[2:])  # the 16384 class is slower on a cluster here
+    assert autotune.grid_class(probs[0]) == "No=32768+Raman"

@@ -87,21 +87,33 @@ def raw_features(energy, pressure, radius, tau, z, gas):
 
 
 class Targets:
-    """Spectral and envelope targets of the saved fields of one frequency grid: a linear
-    interpolation matrix from |Eω|^2 ω^2/(2πc) onto the 512 log-spaced λ bins, and the
-    analytic field's power interpolated onto 256 times (torch on the GPU)."""
+    """Spectral and envelope targets of the saved fields of one frequency grid: a matrix
+    averaging |Eω|^2 ω^2/(2πc) over each of the 512 log-spaced λ bins, and the analytic
+    field's power interpolated onto 256 times (torch on the GPU)."""
 
     def __init__(self, grid, device="cuda"):
         import torch
         self.torch = torch
         ω = np.asarray(grid.ω)
-        lam = np.geomspace(LAMBDA[0], LAMBDA[1], NSPEC)
+        # 512 log-spaced wavelength bins; each target is the mean of the λ-Jacobian-weighted
+        # intensity over the grid frequencies inside its bin (linear interpolation at the
+        # bin centre where a bin holds no grid frequency), i.e. the spectrum downsampled
+        # rather than sampled, so fringes finer than a bin do not alias
+        edges = np.geomspace(LAMBDA[0], LAMBDA[1], NSPEC + 1)
+        lam = np.sqrt(edges[:-1] * edges[1:])
         wq = 2 * np.pi * pd.c / lam
         j = np.clip(np.searchsorted(ω, wq) - 1, 0, len(ω) - 2)
         f = (wq - ω[j]) / (ω[j + 1] - ω[j])
         M = np.zeros((NSPEC, len(ω)))
-        M[np.arange(NSPEC), j] = (1 - f)
-        M[np.arange(NSPEC), j + 1] = f
+        whi = 2 * np.pi * pd.c / edges[:-1]
+        wlo = 2 * np.pi * pd.c / edges[1:]
+        for b in range(NSPEC):
+            inside = np.nonzero((ω >= wlo[b]) & (ω < whi[b]))[0]
+            if len(inside):
+                M[b, inside] = 1.0 / len(inside)
+            else:
+                M[b, j[b]] = 1 - f[b]
+                M[b, j[b] + 1] = f[b]
         jac = ω ** 2 / (2 * np.pi * pd.c)
         self.M = torch.tensor(M * jac[None, :], dtype=torch.float64, device=device)
         self.N = grid.N

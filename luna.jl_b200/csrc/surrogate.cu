@@ -8,8 +8,9 @@
 //     k contiguous), backward data dX = dZ W (B = W read with n contiguous) and backward
 //     weights dW = dZ^T X (both read with the batch index contiguous). The CTA's threads
 //     stage 128 x 64 tiles of A and B into shared memory in the K-major core-matrix layout
-//     (transposing where the source is stored the other way), one thread issues the MMAs,
-//     and a two-stage ring overlaps the staging of chunk c+1 with the MMAs of chunk c.
+//     (asynchronous 16-byte copies where k is contiguous, through registers where the source
+//     is stored the other way), one thread issues the MMAs, and a three-stage ring keeps two
+//     chunks in flight while the MMAs of a third run.
 //     Fused epilogues: bias + SiLU with the pre-activation kept (forward), the SiLU
 //     derivative of the layer input (backward data), plain FP32 (backward weights).
 //     blockIdx.z runs over ensemble members (strided operands).
@@ -35,7 +36,8 @@ namespace {
 constexpr int SG_BM = 128, SG_BN = 128, SG_KC = 64, SG_THREADS = 256;
 constexpr int SG_TILE_BYTES = SG_BM * SG_KC * 2;      // one 128 x 64 BF16 tile
 constexpr int SG_STAGE_BYTES = 2 * SG_TILE_BYTES;     // A and B
-constexpr int SG_SMEM = 2 * SG_STAGE_BYTES + 1024;    // two stages + alignment slack
+constexpr int SG_STAGES = 3;                          // ring depth: two chunks in flight
+constexpr int SG_SMEM = SG_STAGES * SG_STAGE_BYTES + 1024;  // stages + alignment slack
 
 enum { EPI_F32 = 0, EPI_FWD = 1, EPI_BWD_DATA = 2 };
 
@@ -100,6 +102,30 @@ __device__ __forceinline__ void sg_stage(const bf16* __restrict__ src, long long
     }
 }
 
+// Asynchronous form of sg_stage for an operand stored with k contiguous: one 16-byte
+// cp.async per core-matrix row (no register round trip); other layouts are staged through
+// registers (sg_stage<true>).
+template <bool T>
+__device__ __forceinline__ void sg_load(const bf16* __restrict__ src, long long ld, int r0, int k0, unsigned char* dst,
+                                        int tid) {
+    if constexpr (T) {
+        sg_stage<true>(src, ld, r0, k0, dst, tid);
+    } else {
+#pragma unroll
+        for (int q = 0; q < (SG_BM * 8) / SG_THREADS; ++q) {
+            const int u = tid + SG_THREADS * q;
+            const int row = u >> 3, kch = u & 7;
+            const bf16* g = src + (size_t)(r0 + row) * ld + k0 + kch * 8;
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(dst + tc_off(row, kch))), "l"(g)
+                         : "memory");
+        }
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 __device__ __forceinline__ uint4 pack8(const float* v) {
     uint4 o;
     o.x = pack_bf16(v[0], v[1]);
@@ -120,9 +146,9 @@ __device__ __forceinline__ void unpack8(uint4 u, float* v) {
 
 // Grid (M/128, N/128, members), 256 threads.
 template <bool AT, bool BT>
-__global__ void __launch_bounds__(SG_THREADS, 1) sg_gemm(const SgArgs a, int* err) {
+__global__ void __launch_bounds__(SG_THREADS, 2) sg_gemm(const SgArgs a, int* err) {
     extern __shared__ __align__(1024) unsigned char sg_smem_raw[];
-    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(8) uint64_t mbar[SG_STAGES];
     __shared__ uint32_t tmem_base_sh;
     unsigned char* sm = (unsigned char*)(((uintptr_t)sg_smem_raw + 1023) & ~(uintptr_t)1023);
     const int tid = threadIdx.x, warp = tid >> 5;
@@ -138,8 +164,8 @@ __global__ void __launch_bounds__(SG_THREADS, 1) sg_gemm(const SgArgs a, int* er
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[1])));
+#pragma unroll
+        for (int q = 0; q < SG_STAGES; ++q) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[q])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     tc_fence_before();
@@ -147,37 +173,52 @@ __global__ void __launch_bounds__(SG_THREADS, 1) sg_gemm(const SgArgs a, int* er
     tc_fence_after();
     const uint32_t tmem = tmem_base_sh;
 
+    // chunk c of K lives in stage c % SG_STAGES; the MMAs of chunk c commit to that stage's
+    // mbarrier (phase c / SG_STAGES), which frees the stage for chunk c + SG_STAGES
     const int nk = a.K / SG_KC;
+    auto stA = [&](int c) { return sm + (c % SG_STAGES) * SG_STAGE_BYTES; };
     bool ok = true;
     int issued = 0;
-    for (int kc = 0; kc < nk; ++kc) {
-        const int s = kc & 1;
-        unsigned char* sA = sm + s * SG_STAGE_BYTES;
-        unsigned char* sB = sA + SG_TILE_BYTES;
-        if (kc >= 2) {  // the stage's previous MMAs must have finished reading it
-            const bool w = mbar_wait(smem_u32(&mbar[s]), ((kc - 2) >> 1) & 1);
-            ok = __syncthreads_and(w) != 0;
-            if (!ok) break;
+#pragma unroll
+    for (int c = 0; c < SG_STAGES - 1; ++c) {
+        if (c < nk) {
+            sg_load<AT>(A, a.lda, m0, c * SG_KC, stA(c), tid);
+            sg_load<BT>(B, a.ldb, n0, c * SG_KC, stA(c) + SG_TILE_BYTES, tid);
         }
-        sg_stage<AT>(A, a.lda, m0, kc * SG_KC, sA, tid);
-        sg_stage<BT>(B, a.ldb, n0, kc * SG_KC, sB, tid);
+        cp_async_commit();
+    }
+    for (int kc = 0; kc < nk; ++kc) {
+        const int nxt = kc + SG_STAGES - 1;
+        if (nxt < nk) {
+            if (nxt >= SG_STAGES) {  // the stage's previous chunk (kc - 1) must be consumed
+                const bool w = mbar_wait(smem_u32(&mbar[nxt % SG_STAGES]), ((nxt - SG_STAGES) / SG_STAGES) & 1);
+                ok = __syncthreads_and(w) != 0;
+                if (!ok) break;
+            }
+            sg_load<AT>(A, a.lda, m0, nxt * SG_KC, stA(nxt), tid);
+            sg_load<BT>(B, a.ldb, n0, nxt * SG_KC, stA(nxt) + SG_TILE_BYTES, tid);
+        }
+        cp_async_commit();
+        cp_async_wait<SG_STAGES - 1>();  // this thread's copies of chunk kc have landed
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t aa = smem_u32(sA), bb = smem_u32(sB);
+            const uint32_t aa = smem_u32(stA(kc)), bb = aa + SG_TILE_BYTES;
 #pragma unroll
             for (int kk = 0; kk < SG_KC / 16; ++kk) {
                 const uint32_t off = kk * 256;  // two 16-byte k-chunks per K=16 step
                 tc_mma(tmem, tc_desc(aa + off, 128, 1024), tc_desc(bb + off, 128, 1024), idesc,
                        (kc > 0 || kk > 0) ? 1u : 0u);
             }
-            tc_commit(smem_u32(&mbar[s]));
+            tc_commit(smem_u32(&mbar[kc % SG_STAGES]));
         }
         issued = kc + 1;
     }
+    cp_async_wait<0>();  // no copy in flight past this point
     if (issued > 0) {
-        const bool w = mbar_wait(smem_u32(&mbar[(issued - 1) & 1]), ((issued - 1) >> 1) & 1);
+        const int c = issued - 1;
+        const bool w = mbar_wait(smem_u32(&mbar[c % SG_STAGES]), (c / SG_STAGES) & 1);
         ok = (__syncthreads_and(w) != 0) && ok && issued == nk;
     }
     if (!ok && tid == 0 && err) atomicOr(err, 1);

@@ -76,3 +76,31 @@ def test_check_cache_ignores_missing_or_earlier_caches(tmp_path):
     other = O.CheckpointOutput(tmp_path / "none.npz", p.grid.zmax, 21)
     with pytest.raises(ValueError):
         other.check_cache(p.Eω, 0.0, 1e-4)
+
+
+@pytest.mark.gpu
+def test_device_resumable_run_matches_cpu_and_resumes_exactly(tmp_path):
+    """output.run with the device integrator (its default solver): the segmented run agrees
+    with the same segmented run on the C++ restatement, and an interrupted device run
+    resumed from its cache repeats the uninterrupted device run exactly."""
+    p = _problem()
+    solve, _ = _solver(p)
+    cpu_out = O.run(p, O.CheckpointOutput(tmp_path / "c.npz", p.grid.zmax, 11), segments=4, solver=solve)
+    dev = O.run(p, O.CheckpointOutput(tmp_path / "d.npz", p.grid.zmax, 11), segments=4)
+    assert len(dev.Eω) == 11
+    for a, b in zip(dev.data["Eω"], cpu_out.data["Eω"]):
+        # the same FP64 algorithm; the segments' step sequences follow rounding at this level
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
+    path = tmp_path / "e.npz"
+    seen = []
+
+    def stop_after_two(z):
+        seen.append(z)
+        if len(seen) == 2:
+            raise KeyboardInterrupt
+
+    with pytest.raises(KeyboardInterrupt):
+        O.run(p, O.CheckpointOutput(path, p.grid.zmax, 11), segments=4, on_segment=stop_after_two)
+    out = O.run(p, O.CheckpointOutput(path, p.grid.zmax, 11), segments=4)
+    for a, b in zip(out.data["Eω"], dev.data["Eω"]):
+        np.testing.assert_array_equal(a, b)

@@ -262,9 +262,10 @@ int luna_b200_batch_set_priority(luna_batch* b, const double* priority);
 int luna_b200_batch_timeline(luna_batch* b, double* begin_end_s, int* sm);
 /* Shape of every instance for the next luna_b200_batch_set_priority (no counterpart in the
  * reference; an autotuner's decision): [n] ints, 0 = decided from the work estimates (an
- * eligible instance whose estimate is at least the mean load of an SM runs on a cluster),
- * 1 = one CTA, 2 = a cluster of CTAs when the instance is eligible (one CTA otherwise);
- * NULL restores 0 for all. */
+ * eligible instance whose estimate is at least the mean load of an SM runs on a cluster of
+ * 8 CTAs, at least four times that on a cluster of 16 where the grid allows one),
+ * 1 = one CTA, 2 = a cluster of 8 CTAs, 3 = a cluster of 16 CTAs, each when the instance is
+ * eligible (the next smaller shape otherwise); NULL restores 0 for all. */
 int luna_b200_batch_set_shapes(luna_batch* b, const int* shape);
 /* Step sequence of instance i for the next runs (a verification aid, no counterpart in the
  * reference; the per-instance form of luna_solve_opts.replay): [2*nreplay] doubles, the

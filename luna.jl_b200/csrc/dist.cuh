@@ -1,5 +1,6 @@
 // Distributed solver: one mode-averaged instance integrated by a thread-block cluster of
-// DIST_R CTAs, for the long instances of a batch (field-resolved grid, mixed precision).
+// R CTAs (DIST_R, or DIST_R_BIG for the longest instances), for the long instances of a
+// batch (field-resolved grid, FP64 or mixed precision).
 //
 // The RK45 loop, stage combinations, error norm and controller are those of
 // solve_instance; what is split is every per-bin and per-sample loop and every transform:
@@ -25,11 +26,16 @@
 
 namespace luna {
 
-#ifndef DIST_R
+// cluster sizes: DIST_R CTAs per distributed instance, DIST_R_BIG for the longest ones
+// (non-portable clusters); the device code is templated on the size R
 #define DIST_R 8
-#endif
-#define DUNR (16 / DIST_R)  // elements per thread whose remote loads are issued together
-#define DUNR_RAMAN (8 / DIST_R > 0 ? 8 / DIST_R : 1)
+#define DIST_R_BIG 16
+// elements per thread whose remote loads are issued together
+template <int R>
+struct DUnr {
+    static constexpr int v = 16 / R > 0 ? 16 / R : 1;
+    static constexpr int raman = 8 / R > 0 ? 8 / R : 1;
+};
 
 namespace dcg = cooperative_groups;
 
@@ -49,12 +55,12 @@ struct DWs {
     int rank;
 };
 
-__host__ __device__ inline size_t dist_smem_bytes(int No, size_t csize) {
-    const size_t Mb = (size_t)(No / 2) / DIST_R;
+__host__ __device__ inline size_t dist_smem_bytes(int No, size_t csize, int R = DIST_R) {
+    const size_t Mb = (size_t)(No / 2) / R;
     return LUNA_SMALL_BYTES + 2 * align_up((Mb + 16) * csize, 256) + 4 * align_up(Mb * csize, 256);
 }
 
-template <typename Rl>
+template <typename Rl, int R>
 __device__ void plan_dws(const LunaInst& I, char* smem, DWs<Rl>& d, const TwTab<Rl>& tw, int rank) {
     d.red = reinterpret_cast<double*>(smem);
     d.tot = d.red + 3 * LUNA_WARPS;
@@ -63,7 +69,7 @@ __device__ void plan_dws(const LunaInst& I, char* smem, DWs<Rl>& d, const TwTab<
     d.tw = tw;
     d.rank = rank;
     const size_t c = sizeof(cpx<Rl>);
-    const size_t Mb = (size_t)(I.No / 2) / DIST_R;
+    const size_t Mb = (size_t)(I.No / 2) / R;
     const size_t bs = align_up((Mb + 16) * c, 256), bm = align_up(Mb * c, 256);
     size_t off = LUNA_SMALL_BYTES;
     d.stg = reinterpret_cast<cpx<Rl>*>(smem + off);
@@ -105,21 +111,21 @@ __device__ __forceinline__ cpx<Rl> tw_pow(const TwTab<Rl>& tw, unsigned a, int l
 // n = Mc): C2R pre-twiddle Z[n] = (X[n] + conj X[Mc-n]) + i W^-n (X[n] - conj X[Mc-n]) and
 // an Mc-point inverse transform. On return tb holds this CTA's block of sample pairs
 // m = rank Mbc + n1 (unscaled). load is called once for each own bin.
-template <typename Rl, typename LoadF>
+template <typename Rl, int R, typename LoadF>
 __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) {
-    const int R = DIST_R, p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mbc = Mc / R;
-    const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<DIST_R>();
-    // DUNR own bins per thread and round: their loads are independent and issued together
-    for (int j0 = tid; p + R * j0 <= Mc; j0 += DUNR * T) {
-        cpx<double> X[DUNR];
+    const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<R>();
+    // DUnr<R>::v own bins per thread and round: their loads are independent and issued together
+    for (int j0 = tid; p + R * j0 <= Mc; j0 += DUnr<R>::v * T) {
+        cpx<double> X[DUnr<R>::v];
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int n = p + R * (j0 + u * T);
             X[u] = (n < Nw) ? load(n) : mk<double>(0, 0);
         }
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int j = j0 + u * T;
             if (p + R * j <= Mc) d.stg[Swz<Rl>::f(j)] = cvt<Rl>(X[u]);
         }
@@ -127,17 +133,17 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
     dsync();
     const int po = (R - p) % R;
     const cpx<Rl>* so = drem(d.stg, po);
-    // remote loads of DUNR elements are issued before any is used (latency of the cluster)
-    for (int k0 = tid; k0 < Mbc; k0 += DUNR * T) {
-        cpx<Rl> xm[DUNR];
+    // remote loads of DUnr<R>::v elements are issued before any is used (latency of the cluster)
+    for (int k0 = tid; k0 < Mbc; k0 += DUnr<R>::v * T) {
+        cpx<Rl> xm[DUnr<R>::v];
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int k = k0 + u * T;
             const int nm = Mc - (R * k + p);  // the partner bin, owned by CTA po
             xm[u] = (k < Mbc) ? so[Swz<Rl>::f((nm - po) / R)] : mk<Rl>(0, 0);
         }
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int k = k0 + u * T;
             if (k >= Mbc) continue;
             const int n = R * k + p;
@@ -162,27 +168,27 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
     }
     dsync();
     // join: x[n1 + Mbc q] = sum_r W_R^{-r q} B_r[n1], q = this CTA
-    const cpx<Rl>* fr[DIST_R];
-    cpx<Rl> wq[DIST_R];
+    const cpx<Rl>* fr[R];
+    cpx<Rl> wq[R];
 #pragma unroll
-    for (int r = 0; r < DIST_R; ++r) {
+    for (int r = 0; r < R; ++r) {
         fr[r] = drem(d.fb, r);
         wq[r] = tw_pow<Rl, true>(d.tw, (unsigned)(r * p), lgR);
     }
-    for (int n0 = tid; n0 < Mbc; n0 += DUNR * T) {
-        cpx<Rl> v[DUNR][DIST_R];
+    for (int n0 = tid; n0 < Mbc; n0 += DUnr<R>::v * T) {
+        cpx<Rl> v[DUnr<R>::v][R];
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int pos = Swz<Rl>::f(min(n0 + u * T, Mbc - 1));
 #pragma unroll
-            for (int r = 0; r < DIST_R; ++r) v[u][r] = fr[r][pos];
+            for (int r = 0; r < R; ++r) v[u][r] = fr[r][pos];
         }
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             if (n0 + u * T >= Mbc) continue;
             cpx<Rl> acc = v[u][0];
 #pragma unroll
-            for (int r = 1; r < DIST_R; ++r) acc = acc + v[u][r] * wq[r];
+            for (int r = 1; r < R; ++r) acc = acc + v[u][r] * wq[r];
             d.tb[Swz<Rl>::f(n0 + u * T)] = acc;
         }
     }
@@ -194,34 +200,34 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
 // X[k] = 1/2 (Z[k] + conj Z[Mc-k]) - i/2 W^k (Z[k] - conj Z[Mc-k]) and store(k, X) for the
 // own bins k < Nw. Opens with a cluster barrier (every block complete, every remote read of
 // the previous phase done).
-template <typename Rl, typename StoreF>
+template <typename Rl, int R, typename StoreF>
 __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store) {
-    const int R = DIST_R, p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mbc = Mc / R;
-    const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<DIST_R>();
+    const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<R>();
     dsync();
-    const cpx<Rl>* tr[DIST_R];
-    cpx<Rl> wq[DIST_R];
+    const cpx<Rl>* tr[R];
+    cpx<Rl> wq[R];
 #pragma unroll
-    for (int q = 0; q < DIST_R; ++q) {
+    for (int q = 0; q < R; ++q) {
         tr[q] = drem(d.tb, q);
         wq[q] = tw_pow<Rl, false>(d.tw, (unsigned)(p * q), lgR);
     }
-    for (int n0 = tid; n0 < Mbc; n0 += DUNR * T) {
-        cpx<Rl> v[DUNR][DIST_R];
+    for (int n0 = tid; n0 < Mbc; n0 += DUnr<R>::v * T) {
+        cpx<Rl> v[DUnr<R>::v][R];
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int pos = Swz<Rl>::f(min(n0 + u * T, Mbc - 1));
 #pragma unroll
-            for (int q = 0; q < DIST_R; ++q) v[u][q] = tr[q][pos];
+            for (int q = 0; q < R; ++q) v[u][q] = tr[q][pos];
         }
 #pragma unroll
-        for (int u = 0; u < DUNR; ++u) {
+        for (int u = 0; u < DUnr<R>::v; ++u) {
             const int n1 = n0 + u * T;
             if (n1 >= Mbc) continue;
             cpx<Rl> acc = v[u][0];
 #pragma unroll
-            for (int q = 1; q < DIST_R; ++q) acc = acc + v[u][q] * wq[q];
+            for (int q = 1; q < R; ++q) acc = acc + v[u][q] * wq[q];
             if (p) acc = acc * tw_pow<Rl, false>(d.tw, (unsigned)(p * n1), lgM);
             d.fb[Swz<Rl>::f(n1)] = acc;
         }
@@ -231,15 +237,15 @@ __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store
     dsync();
     const int po = (R - p) % R;
     const cpx<Rl>* fo = drem(d.fb, po);
-    for (int j0 = tid; p + R * j0 < Nw; j0 += DUNR * T) {
-      cpx<Rl> zm[DUNR];
+    for (int j0 = tid; p + R * j0 < Nw; j0 += DUnr<R>::v * T) {
+      cpx<Rl> zm[DUnr<R>::v];
 #pragma unroll
-      for (int u = 0; u < DUNR; ++u) {
+      for (int u = 0; u < DUnr<R>::v; ++u) {
           const int k = p + R * (j0 + u * T);
           zm[u] = (k < Nw) ? fo[Swz<Rl>::f(((Mc - k) & (Mc - 1)) / R)] : mk<Rl>(0, 0);
       }
 #pragma unroll
-      for (int u = 0; u < DUNR; ++u) {
+      for (int u = 0; u < DUnr<R>::v; ++u) {
         const int k = p + R * (j0 + u * T);
         if (k >= Nw) continue;
         const int kk = k & (Mc - 1);
@@ -264,44 +270,44 @@ __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store
 // inverse split (as raman_conv), then the inverse sub-transforms; rb0/rb1 end holding
 // B_p[n1] = W_2M^{-p n1} IFFT_Mb(Y_p)[n1] for this CTA's pair of sub-transforms. Needs
 // every CTA's field block (call after a cluster barrier).
-template <typename Rl>
+template <typename Rl, int R>
 __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int M, double sc) {
-    const int R = DIST_R, c = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int c = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mb = M / R, Mr = 2 * M;
-    const int lgMr = ilog2i((unsigned)Mr), lg2R = ilog2c<DIST_R>() + 1;
+    const int lgMr = ilog2i((unsigned)Mr), lg2R = ilog2c<R>() + 1;
     const int pa = (c == 0) ? 0 : c, pb = (c == 0) ? R : 2 * R - c;
-    const cpx<Rl>* tr[DIST_R];
-    cpx<Rl> wa[DIST_R], wb[DIST_R];
+    const cpx<Rl>* tr[R];
+    cpx<Rl> wa[R], wb[R];
 #pragma unroll
-    for (int q = 0; q < DIST_R; ++q) {
+    for (int q = 0; q < R; ++q) {
         tr[q] = drem(d.tb, q);
         wa[q] = tw_pow<Rl, false>(d.tw, (unsigned)(pa * q), lg2R);
         wb[q] = tw_pow<Rl, false>(d.tw, (unsigned)(pb * q), lg2R);
     }
     const Rl s = (Rl)sc;
-    for (int n0 = tid; n0 < Mb; n0 += DUNR * T) {
-      cpx<Rl> ev[DUNR][DIST_R];
+    for (int n0 = tid; n0 < Mb; n0 += DUnr<R>::v * T) {
+      cpx<Rl> ev[DUnr<R>::v][R];
 #pragma unroll
-      for (int u = 0; u < DUNR; ++u) {
+      for (int u = 0; u < DUnr<R>::v; ++u) {
           const int pos = Swz<Rl>::f(min(n0 + u * T, Mb - 1));
 #pragma unroll
-          for (int q = 0; q < DIST_R; ++q) ev[u][q] = tr[q][pos];
+          for (int q = 0; q < R; ++q) ev[u][q] = tr[q][pos];
       }
 #pragma unroll
-      for (int u = 0; u < DUNR; ++u) {
+      for (int u = 0; u < DUnr<R>::v; ++u) {
         const int n1 = n0 + u * T;
         if (n1 >= Mb) continue;
         const int pos = Swz<Rl>::f(n1);
-        cpx<Rl> z[DIST_R];
+        cpx<Rl> z[R];
 #pragma unroll
-        for (int q = 0; q < DIST_R; ++q) {
+        for (int q = 0; q < R; ++q) {
             const cpx<Rl> e = ev[u][q];
             const Rl e0 = e.x * s, e1 = e.y * s;
             z[q] = mk<Rl>(e0 * e0, e1 * e1);
         }
         cpx<Rl> a = z[0], b = z[0];
 #pragma unroll
-        for (int q = 1; q < DIST_R; ++q) {
+        for (int q = 1; q < R; ++q) {
             a = a + z[q] * wa[q];
             b = b + z[q] * wb[q];
         }
@@ -361,15 +367,15 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
 
 // Raman polarisation pair of this CTA's block at n1 from every CTA's B_p (after a barrier
 // that follows dist_raman_fwd in every CTA): P[n1 + Mb q] = sum_p W_2R^{-p q} B_p[n1].
-template <typename Rl>
+template <typename Rl, int R>
 struct RamanOut {
-    const cpx<Rl>* b0[DIST_R];
-    const cpx<Rl>* b1[DIST_R];
-    cpx<Rl> w0[DIST_R], w1[DIST_R];
+    const cpx<Rl>* b0[R];
+    const cpx<Rl>* b1[R];
+    cpx<Rl> w0[R], w1[R];
     __device__ void init(DWs<Rl>& d) {
-        const int R = DIST_R, q = d.rank, lg2R = ilog2c<DIST_R>() + 1;
+        const int q = d.rank, lg2R = ilog2c<R>() + 1;
 #pragma unroll
-        for (int c = 0; c < DIST_R; ++c) {
+        for (int c = 0; c < R; ++c) {
             b0[c] = drem(d.rb0, c);
             b1[c] = drem(d.rb1, c);
             const int pa = (c == 0) ? 0 : c, pb = (c == 0) ? R : 2 * R - c;
@@ -380,14 +386,14 @@ struct RamanOut {
     // P for the pairs n1 = tid + k T of this CTA's block into out[Swz(n1)] (remote loads of
     // two pairs in flight together)
     __device__ void block(cpx<Rl>* out, int Mb) const {
-        constexpr int U = DUNR_RAMAN;
+        constexpr int U = DUnr<R>::raman;
         for (int n0 = threadIdx.x; n0 < Mb; n0 += U * LUNA_BLOCK) {
-            cpx<Rl> v0[U][DIST_R], v1[U][DIST_R];
+            cpx<Rl> v0[U][R], v1[U][R];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int pos = Swz<Rl>::f(min(n0 + u * LUNA_BLOCK, Mb - 1));
 #pragma unroll
-                for (int c = 0; c < DIST_R; ++c) {
+                for (int c = 0; c < R; ++c) {
                     v0[u][c] = b0[c][pos];
                     v1[u][c] = b1[c][pos];
                 }
@@ -398,21 +404,21 @@ struct RamanOut {
                 if (n1 >= Mb) continue;
                 cpx<Rl> acc = v0[u][0] + v1[u][0] * w1[0];
 #pragma unroll
-                for (int c = 1; c < DIST_R; ++c) acc = acc + v0[u][c] * w0[c] + v1[u][c] * w1[c];
+                for (int c = 1; c < R; ++c) acc = acc + v0[u][c] * w0[c] + v1[u][c] * w1[c];
                 out[Swz<Rl>::f(n1)] = acc;
             }
         }
     }
     __device__ __forceinline__ cpx<Rl> at(int pos) const {
-        cpx<Rl> v0[DIST_R], v1[DIST_R];
+        cpx<Rl> v0[R], v1[R];
 #pragma unroll
-        for (int c = 0; c < DIST_R; ++c) {
+        for (int c = 0; c < R; ++c) {
             v0[c] = b0[c][pos];
             v1[c] = b1[c][pos];
         }
         cpx<Rl> acc = v0[0] + v1[0] * w1[0];
 #pragma unroll
-        for (int c = 1; c < DIST_R; ++c) acc = acc + v0[c] * w0[c] + v1[c] * w1[c];
+        for (int c = 1; c < R; ++c) acc = acc + v0[c] * w0[c] + v1[c] * w1[c];
         return acc;
     }
 };
@@ -468,10 +474,10 @@ struct RateF {
 // Mixed precision: rates, ionisation fractions (1 - exp(-x) as -expm1(-x)) and the
 // ionisation-loss current are FP32 per sample (kept in shared memory at [s*T + tid]
 // between the passes), the running integrals FP64. FP64: every quantity FP64.
-template <typename Rl, int NS>
+template <typename Rl, int NS, int R>
 __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, double sc, int ip, int ir, double kc,
                                          double rc) {
-    const int R = DIST_R, q = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int q = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mb = M / R;
     const int mbase = q * Mb;
     const LunaResp& r = I.resp[ip];
@@ -524,7 +530,7 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     dsync();  // totals published; Raman sub-transforms ready; field blocks no longer read
     if (ir >= 0) {
         // the Raman polarisation of this block into tb (the field now lives in ev)
-        RamanOut<Rl> ro;
+        RamanOut<Rl, R> ro;
         ro.init(d);
         ro.block(d.tb, Mb);
     }
@@ -626,9 +632,9 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
 // Et_to_Pt! and the time window on this CTA's block (PlasmaScalar!, Nonlinear.jl:121-133,
 // as running trapezoids written as prefix sums; the carries into the block are the block
 // totals of the CTAs before it, exchanged through the cluster).
-template <typename Rl>
+template <typename Rl, int R>
 __device__ __noinline__ void dist_pointwise(const LunaInst& I, DWs<Rl>& d, int M, double sc) {
-    const int R = DIST_R, q = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int q = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Mb = M / R;
     const int mbase = q * Mb;
     int ip = -1, ir = -1;
@@ -653,10 +659,10 @@ __device__ __noinline__ void dist_pointwise(const LunaInst& I, DWs<Rl>& d, int M
         return;
     }
     dsync();  // every field block complete; every read of the sub-transforms done
-    if (ir >= 0) dist_raman_fwd<Rl>(I.resp[ir], d, M, sc);
+    if (ir >= 0) dist_raman_fwd<Rl, R>(I.resp[ir], d, M, sc);
     if (ip < 0) {
         dsync();  // every CTA's Raman sub-transforms ready; every read of the field blocks done
-        RamanOut<Rl> ro;
+        RamanOut<Rl, R> ro;
         ro.init(d);
         ro.block(d.fb, Mb);  // the sub-transform buffer is free after the barrier above
         __syncthreads();
@@ -674,17 +680,17 @@ __device__ __noinline__ void dist_pointwise(const LunaInst& I, DWs<Rl>& d, int M
         return;
     }
     switch (2 * Mb / T) {  // samples per thread
-        case 4: dist_plasma<Rl, 4>(I, d, M, sc, ip, ir, kc, rc); break;
-        case 8: dist_plasma<Rl, 8>(I, d, M, sc, ip, ir, kc, rc); break;
-        default: dist_plasma<Rl, 16>(I, d, M, sc, ip, ir, kc, rc); break;
+        case 4: dist_plasma<Rl, 4, R>(I, d, M, sc, ip, ir, kc, rc); break;
+        case 8: dist_plasma<Rl, 8, R>(I, d, M, sc, ip, ir, kc, rc); break;
+        default: dist_plasma<Rl, 16, R>(I, d, M, sc, ip, ir, kc, rc); break;
     }
 }
 
 // ------------------------------------------------------------------ the integrator
 // solve_instance for a distributed instance; every CTA of the cluster runs it.
-template <typename Rl, typename Kt>
+template <typename Rl, typename Kt, int R>
 __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c) {
-    const int R = DIST_R, p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
+    const int p = d.rank, T = LUNA_BLOCK, tid = threadIdx.x;
     const int Nw = I.Nw, M = I.No / 2, Mcoarse = I.N / 2;
     const bool writer = (p == 0);
     const cpx<double>* L = reinterpret_cast<const cpx<double>*>(I.linop);
@@ -721,9 +727,9 @@ __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c
     __syncthreads();
     const double sc = I.in_scale;
     auto rhs_d = [&](auto&& load, auto&& store) {
-        dist_c2r<Rl>(d, M, Nw, load);
-        dist_pointwise<Rl>(I, d, M, sc);
-        dist_r2c<Rl>(d, M, Nw, [&](int kb, cpx<double> X) { store(kb, X * ldg(of + kb)); });
+        dist_c2r<Rl, R>(d, M, Nw, load);
+        dist_pointwise<Rl, R>(I, d, M, sc);
+        dist_r2c<Rl, R>(d, M, Nw, [&](int kb, cpx<double> X) { store(kb, X * ldg(of + kb)); });
     };
     {
         const cpx<double>* y = reinterpret_cast<const cpx<double>*>(py);
@@ -754,15 +760,15 @@ __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c
             const double zs = __dadd_rn(t0, __dmul_rn(c_nodes[s], dt));
             const double dd = __dsub_rn(zs, t0);
             if (s != 5) {
-                for (int t0 = tid; own(t0) < Nw; t0 += DUNR * T) {
-                    cpx<double> Lv[DUNR];
+                for (int t0 = tid; own(t0) < Nw; t0 += DUnr<R>::v * T) {
+                    cpx<double> Lv[DUnr<R>::v];
 #pragma unroll
-                    for (int u = 0; u < DUNR; ++u) {
+                    for (int u = 0; u < DUnr<R>::v; ++u) {
                         const int i = own(t0 + u * T);
                         Lv[u] = (i < Nw) ? ldg(L + i) : mk<double>(0, 0);
                     }
 #pragma unroll
-                    for (int u = 0; u < DUNR; ++u) {
+                    for (int u = 0; u < DUnr<R>::v; ++u) {
                         const int t = t0 + u * T, i = own(t);
                         if (i >= Nw) continue;
                         const cpx<Rl> f = expLd<Rl>(Lv[u], dd);
@@ -858,7 +864,7 @@ __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c
             {
                 cpx<double>* Yo = reinterpret_cast<cpx<double>*>(pyn);
                 const double inv = 1.0 / (double)I.N;
-                dist_c2r<Rl>(d, Mcoarse, Nw, [&](int i) -> cpx<double> {
+                dist_c2r<Rl, R>(d, Mcoarse, Nw, [&](int i) -> cpx<double> {
                     return scale(__ldg(I.wwin + i), Yo[i] * e1[i]);
                 });
                 const int Mbc = Mcoarse / R;
@@ -871,7 +877,7 @@ __device__ __noinline__ void solve_instance_dist(LunaInst& I, DWs<Rl>& d, Ctl& c
                     d.tb[pos] = mk<Rl>((Rl)a, (Rl)b);
                 }
                 __syncthreads();
-                dist_r2c<Rl>(d, Mcoarse, Nw, [&](int i, cpx<double> X) { Yo[i] = X; });
+                dist_r2c<Rl, R>(d, Mcoarse, Nw, [&](int i, cpx<double> X) { Yo[i] = X; });
             }
             while (saved < I.saveN && I.zsave[saved] <= c.tn) {
                 interpolate_row<Rl, Kt>(Nw, I.linop, c, I.zsave[saved], k, py, pyn,

@@ -291,11 +291,11 @@ solve_kernel_cl(LunaInst* insts, const int* big, int nbig, int* big_counter, con
     }
 }
 
-// Persistent solver on clusters of DIST_R CTAs. Phase 1: each cluster integrates the
+// Persistent solver on clusters of R CTAs. Phase 1: each cluster integrates the
 // instances of `dl` (the long ones, in priority order) together, every CTA holding one
 // residue class of the frequency bins and one block of the time samples. Phase 2: once
 // `dl` is empty, every CTA integrates instances of `reg` on its own.
-template <typename Rl, typename Kt>
+template <typename Rl, typename Kt, int R>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
 solve_kernel_dist(LunaInst* insts, const int* dl, int nd, int* d_counter, const int* reg, int nreg,
                   int* reg_counter, TwTab<Rl> tw, int smem_bytes) {
@@ -321,8 +321,8 @@ solve_kernel_dist(LunaInst* insts, const int* dl, int nd, int* d_counter, const 
             I.sm = (int)sm;
         }
         DWs<Rl> d;
-        plan_dws<Rl>(I, smem, d, tw, rank);
-        solve_instance_dist<Rl, Kt>(I, d, ctl);
+        plan_dws<Rl, R>(I, smem, d, tw, rank);
+        solve_instance_dist<Rl, Kt, R>(I, d, ctl);
         if (rank == 0 && threadIdx.x == 0) {
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -555,11 +555,18 @@ struct luna_batch {
     cudaStream_t stream2 = nullptr;  // single-CTA solver beside the cluster solver
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, evf = nullptr, evj = nullptr;
     int reg_grid = 0;
-    // distributed instances (clusters of DIST_R CTAs per instance)
+    // distributed instances (clusters of DIST_R CTAs per instance, DIST_R_BIG for the
+    // longest ones, each on its own stream)
     int ndist = 0, dist_grid = 0, ncl_max = 0, nsm = 0;
     int* d_dist = nullptr;
     std::vector<int> dist, elig;
-    std::vector<int> shape;  // per instance: 0 the work-estimate rule, 1 one CTA, 2 a cluster
+    int ndist16 = 0, dist16_grid = 0, ncl16_max = 0;
+    int* d_dist16 = nullptr;
+    std::vector<int> dist16, elig16;
+    cudaStream_t stream3 = nullptr;
+    cudaEvent_t evj3 = nullptr;
+    std::vector<int> shape;  // per instance: 0 the work-estimate rule, 1 one CTA, 2 a cluster,
+                             // 3 a cluster of DIST_R_BIG
 };
 
 namespace {
@@ -599,23 +606,36 @@ int dist_partition(luna_batch* b, const double* pr) {
     double W = 0;
     for (int i = 0; i < n; ++i) W += pr[i];
     const double thr = W / std::max(1, b->nsm);
-    std::vector<char> isd(n, 0);
+    // 0: one CTA, 1: a cluster of DIST_R, 2: a cluster of DIST_R_BIG. The big clusters take
+    // the eligible instances whose estimate is at least four times the mean SM load (those
+    // that would set the makespan even on a cluster of DIST_R)
+    std::vector<char> isd(n, 0), big(n, 0);
+    for (int i = 0; i < n; ++i) big[i] = 0;
+    for (int i : b->elig16) big[i] = 1;
     for (int i : b->elig) {
         const int sh = b->shape.empty() ? 0 : b->shape[i];
-        isd[i] = sh == 2 || (sh == 0 && pr[i] >= thr);
+        isd[i] = sh == 2 || sh == 3 || (sh == 0 && pr[i] >= thr);
+        if (isd[i] && big[i] && b->ncl16_max > 0 && (sh == 3 || (sh == 0 && pr[i] >= 4.0 * thr))) isd[i] = 2;
     }
     b->dist.clear();
+    b->dist16.clear();
     b->reg.clear();
-    for (int i = 0; i < n; ++i) (isd[i] ? b->dist : b->reg).push_back(i);
+    for (int i = 0; i < n; ++i) (isd[i] == 2 ? b->dist16 : isd[i] ? b->dist : b->reg).push_back(i);
     auto by = [&](int a, int c) { return pr[a] > pr[c]; };
     std::stable_sort(b->dist.begin(), b->dist.end(), by);
+    std::stable_sort(b->dist16.begin(), b->dist16.end(), by);
     std::stable_sort(b->reg.begin(), b->reg.end(), by);
     b->ndist = (int)b->dist.size();
+    b->ndist16 = (int)b->dist16.size();
     b->nreg = (int)b->reg.size();
-    const int ncl = std::min(b->ncl_max, b->ndist);
+    const int n16 = std::min(b->ncl16_max, b->ndist16);
+    // a big cluster takes the room of DIST_R_BIG / DIST_R small ones
+    const int ncl = std::min(std::max(1, b->ncl_max - n16 * (DIST_R_BIG / DIST_R)), b->ndist);
+    b->dist16_grid = DIST_R_BIG * n16;
     b->dist_grid = (b->ndist > 0) ? DIST_R * ncl : 0;
-    b->reg_grid = std::max(0, std::min(b->nreg, b->nsm - b->dist_grid));
+    b->reg_grid = std::max(0, std::min(b->nreg, b->nsm - b->dist_grid - b->dist16_grid));
     if (b->ndist > 0) CK(cudaMemcpy(b->d_dist, b->dist.data(), sizeof(int) * b->ndist, cudaMemcpyHostToDevice));
+    if (b->ndist16 > 0) CK(cudaMemcpy(b->d_dist16, b->dist16.data(), sizeof(int) * b->ndist16, cudaMemcpyHostToDevice));
     if (b->nreg > 0) CK(cudaMemcpy(b->d_reg, b->reg.data(), sizeof(int) * b->nreg, cudaMemcpyHostToDevice));
     return LUNA_OK;
 }
@@ -629,78 +649,107 @@ int dist_setup(luna_batch* b, const luna_solve_opts* opts, int nsm) {
     const int n = b->n;
     const int maxs = max_smem_optin();
     const size_t cs = sizeof(cpx<Rl>);
-    std::vector<int> dl;
+    std::vector<int> dl, dl16;
     std::vector<double> cost(n);
     size_t dsm = 0;
+    const int dmin = opts->dist_min_no > 0 ? opts->dist_min_no : 16384;
+    auto fits = [&](const LunaInst& I, int R) {
+        const int M = I.No / 2, Mc = I.N / 2;
+        return M % R == 0 && M / R >= 2 * LUNA_BLOCK && M / R <= FftEmax<Rl>::v * LUNA_BLOCK && Mc % R == 0 &&
+               Mc / R >= 64 && Mc <= M && I.Nw <= Mc + 1 && dist_smem_bytes(I.No, cs, R) <= (size_t)maxs;
+    };
     for (int i = 0; i < n; ++i) {
         const LunaInst& I = b->h[i];
-        const int M = I.No / 2, Mc = I.N / 2;
-        const bool ok = I.kind == 0 && !I.grad && !needs_hilbert(I) && opts->stats_cap <= 0 &&
-                        I.No >= (opts->dist_min_no > 0 ? opts->dist_min_no : 16384) &&
-                        M % DIST_R == 0 && M / DIST_R >= 2 * LUNA_BLOCK &&
-                        M / DIST_R <= FftEmax<Rl>::v * LUNA_BLOCK && Mc % DIST_R == 0 &&
-                        Mc / DIST_R >= 64 && Mc <= M && I.Nw <= Mc + 1 &&
-                        dist_smem_bytes(I.No, cs) <= (size_t)maxs;
+        const bool ok = I.kind == 0 && !I.grad && !needs_hilbert(I) && opts->stats_cap <= 0 && I.No >= dmin &&
+                        fits(I, DIST_R);
         if (ok) {
             dl.push_back(i);
             dsm = std::max(dsm, dist_smem_bytes(I.No, cs));
+            if (fits(I, DIST_R_BIG)) dl16.push_back(i);
         }
         cost[i] = (double)I.No * std::log2((double)I.No) * (has_raman(I) ? 2.0 : 1.0);
     }
     if (dl.empty()) return LUNA_OK;
     const int sm = (int)std::max<size_t>((size_t)b->smem, dsm);
-    if (cudaFuncSetAttribute(solve_kernel_dist<Rl, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
+    if (cudaFuncSetAttribute(solve_kernel_dist<Rl, Rl, DIST_R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess ||
         cudaFuncSetAttribute(solve_kernel<Rl, Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) != cudaSuccess)
         return fail(LUNA_ERR_CUDA, "batch_create: cannot set shared memory size (distributed solver)");
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = DIST_R;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(DIST_R * 32, 1, 1);
-    cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
-    cfg.dynamicSmemBytes = sm;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int ncl = 0;
-    if (cudaOccupancyMaxActiveClusters(&ncl, solve_kernel_dist<Rl, Rl>, &cfg) != cudaSuccess || ncl < 1) {
-        cudaGetLastError();
-        return LUNA_OK;
-    }
+    auto max_clusters = [&](auto kern, int R) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = R;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(R * 32, 1, 1);
+        cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+        cfg.dynamicSmemBytes = sm;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, kern, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            ncl = 0;
+        }
+        return ncl;
+    };
+    const int ncl = max_clusters(solve_kernel_dist<Rl, Rl, DIST_R>, DIST_R);
+    if (ncl < 1) return LUNA_OK;
+    int ncl16 = 0;
+    if (!dl16.empty() &&
+        cudaFuncSetAttribute(solve_kernel_dist<Rl, Rl, DIST_R_BIG>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm) == cudaSuccess &&
+        cudaFuncSetAttribute(solve_kernel_dist<Rl, Rl, DIST_R_BIG>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess)
+        ncl16 = max_clusters(solve_kernel_dist<Rl, Rl, DIST_R_BIG>, DIST_R_BIG);
+    cudaGetLastError();
     b->smem = sm;
     b->elig = dl;
+    b->elig16 = ncl16 > 0 ? dl16 : std::vector<int>();
     b->ncl_max = ncl;
+    b->ncl16_max = ncl16;
     b->nsm = nsm;
-    if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_reg, sizeof(int) * n) ||
-        dalloc(b->allocs, &b->d_cl_counters, 3 * sizeof(int)))
+    if (dalloc(b->allocs, &b->d_dist, sizeof(int) * n) || dalloc(b->allocs, &b->d_dist16, sizeof(int) * n) ||
+        dalloc(b->allocs, &b->d_reg, sizeof(int) * n) || dalloc(b->allocs, &b->d_cl_counters, 4 * sizeof(int)))
         return LUNA_ERR_CUDA;
     return dist_partition(b, cost.data());
 }
 
-// The distributed solver on its clusters and the single-CTA solver on the SMs left over
-// (second stream), both in the batch's precision.
+// The distributed solvers on their clusters (DIST_R_BIG on a third stream, DIST_R) and the
+// single-CTA solver on the SMs left over (second stream), all in the batch's precision;
+// every kernel takes single-CTA instances once its own list is empty.
 template <typename Rl>
 int dist_launch(luna_batch* b, const TwTab<Rl>& tw) {
-    cudaLaunchConfig_t cfg = {};
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeClusterDimension;
-    at[0].val.clusterDim.x = DIST_R;
-    at[0].val.clusterDim.y = 1;
-    at[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(b->dist_grid, 1, 1);
-    cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
-    cfg.dynamicSmemBytes = b->smem;
-    cfg.stream = b->stream;
-    cfg.attrs = at;
-    cfg.numAttrs = 1;
-    int* c = b->d_cl_counters;
-    if (b->reg_grid > 0) {
-        CK(cudaEventRecord(b->evf, b->stream));
-        CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
+    int* c = b->d_cl_counters;  // [0] clusters, [1] single CTAs, [2] error flag, [3] big clusters
+    auto cfg_for = [&](int R, int grid, cudaStream_t st, cudaLaunchAttribute* at) {
+        cudaLaunchConfig_t cfg = {};
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = R;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(grid, 1, 1);
+        cfg.blockDim = dim3(LUNA_BLOCK, 1, 1);
+        cfg.dynamicSmemBytes = b->smem;
+        cfg.stream = st;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        return cfg;
+    };
+    CK(cudaEventRecord(b->evf, b->stream));
+    if (b->reg_grid > 0) CK(cudaStreamWaitEvent(b->stream2, b->evf, 0));
+    if (b->dist16_grid > 0) {
+        CK(cudaStreamWaitEvent(b->stream3, b->evf, 0));
+        cudaLaunchAttribute at16[1];
+        cudaLaunchConfig_t cfg16 = cfg_for(DIST_R_BIG, b->dist16_grid, b->stream3, at16);
+        CK(cudaLaunchKernelEx(&cfg16, solve_kernel_dist<Rl, Rl, DIST_R_BIG>, b->d_insts, (const int*)b->d_dist16,
+                              b->ndist16, c + 3, (const int*)b->d_reg, b->nreg, c + 1, tw, b->smem));
+        CK(cudaEventRecord(b->evj3, b->stream3));
     }
-    CK(cudaLaunchKernelEx(&cfg, solve_kernel_dist<Rl, Rl>, b->d_insts, (const int*)b->d_dist, b->ndist, c,
-                          (const int*)b->d_reg, b->nreg, c + 1, tw, b->smem));
+    if (b->dist_grid > 0) {
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = cfg_for(DIST_R, b->dist_grid, b->stream, at);
+        CK(cudaLaunchKernelEx(&cfg, solve_kernel_dist<Rl, Rl, DIST_R>, b->d_insts, (const int*)b->d_dist, b->ndist, c,
+                              (const int*)b->d_reg, b->nreg, c + 1, tw, b->smem));
+    }
+    if (b->dist16_grid > 0) CK(cudaStreamWaitEvent(b->stream, b->evj3, 0));
     if (b->reg_grid > 0) {
         solve_kernel<Rl, Rl><<<b->reg_grid, LUNA_BLOCK, b->smem, b->stream2>>>(b->d_insts, b->nreg, c + 1, tw, b->smem,
                                                                               (const int*)b->d_reg);
@@ -1214,9 +1263,11 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
     }
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream3, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess ||
         cudaEventCreateWithFlags(&b->evf, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&b->evj, cudaEventDisableTiming) != cudaSuccess)
+        cudaEventCreateWithFlags(&b->evj, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&b->evj3, cudaEventDisableTiming) != cudaSuccess)
         return bail(fail(LUNA_ERR_CUDA, "batch_create: stream/event creation failed"));
     *out = b;
     return LUNA_OK;
@@ -1271,9 +1322,10 @@ int luna_b200_batch_run(luna_batch* b, float* device_ms) {
     // instances restart from y0: restore the per-instance pointers and counters
     CK(cudaMemcpyAsync(b->d_insts, b->h.data(), sizeof(LunaInst) * b->n, cudaMemcpyHostToDevice, b->stream));
     CK(cudaMemsetAsync(b->d_counter, 0, sizeof(int), b->stream));
-    if (b->cl_grid > 0 || b->dist_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
+    if (b->cl_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 3 * sizeof(int), b->stream));
+    if (b->dist_grid > 0 || b->dist16_grid > 0) CK(cudaMemsetAsync(b->d_cl_counters, 0, 4 * sizeof(int), b->stream));
     CK(cudaEventRecord(b->ev0, b->stream));
-    if (b->dist_grid > 0) {
+    if (b->dist_grid > 0 || b->dist16_grid > 0) {
         rc = (b->precision == LUNA_PREC_FP64) ? dist_launch<double>(b, tw.d) : dist_launch<float>(b, tw.f);
         if (rc) return rc;
     } else if (b->precision == LUNA_PREC_FP64) {
@@ -1348,10 +1400,13 @@ int luna_b200_batch_download(luna_batch* b, double* const* saves, double* const*
 
 int luna_b200_batch_info(luna_batch* b, int* kernels_per_run, int* cluster_instances, int* clusters) {
     if (!b) return fail(LUNA_ERR_BAD_ARG, "batch_info: null batch");
-    if (kernels_per_run) *kernels_per_run = (b->cl_grid > 0 || b->dist_grid > 0) ? 1 + (b->reg_grid > 0) : 1;
-    if (b->dist_grid > 0) {
-        if (cluster_instances) *cluster_instances = b->ndist;
-        if (clusters) *clusters = b->dist_grid / DIST_R;
+    if (kernels_per_run)
+        *kernels_per_run = (b->cl_grid > 0 || b->dist_grid > 0 || b->dist16_grid > 0)
+                               ? (b->dist_grid > 0) + (b->dist16_grid > 0) + (b->cl_grid > 0) + (b->reg_grid > 0)
+                               : 1;
+    if (b->dist_grid > 0 || b->dist16_grid > 0) {
+        if (cluster_instances) *cluster_instances = b->ndist + b->ndist16;
+        if (clusters) *clusters = b->dist_grid / DIST_R + b->dist16_grid / DIST_R_BIG;
         return LUNA_OK;
     }
     if (cluster_instances) *cluster_instances = (b->cl_grid > 0) ? b->nbig : 0;
@@ -1404,7 +1459,7 @@ int luna_b200_batch_set_shapes(luna_batch* b, const int* shape) {
         b->shape.clear();
     } else {
         for (int i = 0; i < b->n; ++i)
-            if (shape[i] < 0 || shape[i] > 2) return fail(LUNA_ERR_BAD_ARG, "batch_set_shapes: shape must be 0, 1 or 2");
+            if (shape[i] < 0 || shape[i] > 3) return fail(LUNA_ERR_BAD_ARG, "batch_set_shapes: shape must be 0..3");
         b->shape.assign(shape, shape + b->n);
     }
     return LUNA_OK;
@@ -1432,6 +1487,8 @@ void luna_b200_batch_destroy(luna_batch* b) {
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->evf) cudaEventDestroy(b->evf);
     if (b->evj) cudaEventDestroy(b->evj);
+    if (b->evj3) cudaEventDestroy(b->evj3);
+    if (b->stream3) cudaStreamDestroy(b->stream3);
     if (b->stream) cudaStreamDestroy(b->stream);
     if (b->stream2) cudaStreamDestroy(b->stream2);
     free_all(b->allocs);

@@ -30,7 +30,8 @@ def _case(gas, trange, plasma=None, energy=100e-6, flength=0.2):
                                plasma=plasma, saveN=11)
 
 
-def _batch(probs, flags=0, dist_min_no=16384, priority=None, steplog_cap=0, replay=None, prec=_lib.PREC_MIXED):
+def _batch(probs, flags=0, dist_min_no=16384, priority=None, steplog_cap=0, replay=None, prec=_lib.PREC_MIXED,
+           shapes=None):
     from luna_b200 import plan as P
     plans = [P.Plan.from_transform(p.transform, prec) for p in probs]
     b = P.Batch(plans, 11, np.linspace(0.0, 1.0, 11), flags=flags, dist_min_no=dist_min_no,
@@ -39,6 +40,10 @@ def _batch(probs, flags=0, dist_min_no=16384, priority=None, steplog_cap=0, repl
              [1e-4] * len(probs), [p.grid.zmax for p in probs],
              [np.linspace(0.0, p.grid.zmax, 11) for p in probs],
              [p.grid.zmax / 2 for p in probs])
+    if shapes is not None:
+        b.set_shapes(shapes)
+        if priority is None:
+            b.set_priority([1.0] * len(probs))
     if priority is not None:
         b.set_priority(priority)
     info = b.info()
@@ -120,3 +125,25 @@ def test_fp64_distributed_free_running_matches_single_cta():
     assert rd.status == rs.status == 0 and rd.steps == rs.steps
     for a, b in zip(rd.Eω, rs.Eω):
         assert _rel(a, b) < 1e-10, _rel(a, b)
+
+
+# ------------------------------------------------------------------ 16-CTA clusters
+def test_sixteen_cta_cluster_fp64_matches_oracle_and_mixed_matches_single_cta():
+    """The longest instances run on non-portable clusters of 16 CTAs (each holding 1024
+    sample pairs of the 32768-point grid): FP64 on the oracle's step sequence within 1e-10
+    at every save, mixed precision on the single-CTA solver's step sequence within FP32
+    rounding (2e-4), as for clusters of 8."""
+    p = _case("H2", 2e-12, flength=0.03)
+    assert p.grid.No == 32768
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    (r16,), info = _batch([p], prec=_lib.PREC_FP64, replay=replay, shapes=[3])
+    assert info[1] == 1 and r16.status == 0 and r16.steps == ores.steps
+    for a, b in zip(r16.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+    (rl,), _ = _batch([p], flags=_lib.SOLVE_NO_DIST | _lib.SOLVE_NO_CLUSTERS, steplog_cap=100000)
+    rep = np.stack([rl.steplog[:, 1], rl.steplog[:, 3]], axis=1).ravel()
+    (rm,), info = _batch([p], replay=rep, shapes=[3])
+    assert info[1] == 1 and rm.steps == rl.steps
+    for a, b in zip(rm.Eω, rl.Eω):
+        assert _rel(a, b) < 2e-4, _rel(a, b)

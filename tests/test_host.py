@@ -182,8 +182,9 @@ def test_autotune_schedule_rule():
 
     inst = scan.draw_instances(6)
     probs = [Pr(32768, True), Pr(32768), Pr(16384), Pr(8192), Pr(16384), Pr(8192)]
-    table = {"No=32768+Raman": {"single": 3.0, "cluster": 1.5}, "No=32768": {"single": 1.6, "cluster": 0.7},
-             "No=16384": {"single": 0.8, "cluster": 0.9}, "No=8192": {"single": 0.4, "cluster": None}}
+    table = {"No=32768+Raman": {"single": 3.0, "cluster": 1.5, "cluster16": None},
+             "No=32768": {"single": 1.6, "cluster": 0.7}, "No=16384": {"single": 0.8, "cluster": 0.9},
+             "No=8192": {"single": 0.4, "cluster": None}}
     shapes, prio, pred = autotune.schedule(inst, probs, table, nsm=2)
     w = np.array([scan.nonlinear_phase(p) ** 0.6 for p in inst])
     single = w * np.array([3.0, 1.6, 0.8, 0.4, 0.8, 0.4])
@@ -195,3 +196,24 @@ def test_autotune_schedule_rule():
         assert prio[i] == pytest.approx(w[i] * cl if want == 2 else single[i])
     assert all(s == 1 for s in shapes[2:])  # the 16384 class is slower on a cluster here
     assert autotune.grid_class(probs[0]) == "No=32768+Raman"
+
+
+def test_autotune_schedule_picks_sixteen_ctas_for_the_longest():
+    """An instance whose 8-CTA time is at least twice the mean SM load goes to 16 CTAs when
+    they are faster for its class."""
+    from luna_b200 import autotune
+
+    class Pr:
+        def __init__(self, No):
+            self.grid = type("G", (), {"No": No})()
+            self.transform = type("T", (), {"resp": []})()
+
+    inst = scan.draw_instances(40)
+    probs = [Pr(32768)] + [Pr(8192)] * 39
+    w = np.array([scan.nonlinear_phase(p) ** 0.6 for p in inst])
+    # make instance 0 dominate: its class is slow on one CTA and fast on clusters
+    table = {"No=32768": {"single": 1000.0 / w[0], "cluster": 300.0 / w[0], "cluster16": 200.0 / w[0]},
+             "No=8192": {"single": 0.01, "cluster": None}}
+    shapes, prio, _ = autotune.schedule(inst, probs, table, nsm=148)
+    assert shapes[0] == 3 and prio[0] == pytest.approx(200.0)
+    assert all(s == 1 for s in shapes[1:])

@@ -175,13 +175,9 @@ def step_bytes(Nw, mixed):
 def build(world, rank, n_per_rank):
     inst = scan.draw_instances(n_per_rank * world)
     if world > 1:
-        # cost-balanced shard of the whole draw (no collective on the data path)
-        from luna_b200.grid import RealGrid
-        costs = []
-        for p in inst:
-            g = RealGrid(p["flength"], 800e-9, (p["λmin"], p["λmax"]), p["trange"])
-            costs.append(g.No * math.log2(g.No) * p["flength"] * (3 if p["gas"] == "H2" else 1))
-        idx = scan.shard(costs, rank, world)
+        # cost-balanced shard of the whole draw by the scheduler's step model (no
+        # collective on the data path; every rank computes the same costs)
+        idx = scan.shard([scan.shard_cost(p) for p in inst], rank, world)
         inst = [inst[i] for i in idx]
     probs = [scan.build_problem(p, saveN=SAVEN) for p in inst]
     return inst, probs
@@ -977,8 +973,10 @@ def main():
     hbm, peak_kind = peaks()
     achieved = alg_bytes / (ms / 1e3) / 1e9
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "solve_kernel_scan_traffic.json")
-    if os.path.exists(tf) and prec == _lib.PREC_MIXED:  # captured on the mixed-precision solver
+    # DRAM bytes per RK step from an ncu capture of the same solver (profiles/)
+    tf = os.path.join(ROOT, "profiles", "solve_kernel_scan_traffic.json" if prec == _lib.PREC_MIXED
+                      else "solve_kernel_dist_fp64_traffic.json")
+    if os.path.exists(tf):
         with open(tf) as f:
             tj = json.load(f)
         traffic = tj.get("dram_bytes_per_rk_step", 0) * steps_all

@@ -11,6 +11,7 @@ import numpy as np
 from .interface import prop_capillary_args
 
 GASES = ("He", "Ne", "Ar", "H2")
+RAMAN_GASES = ("N2", "H2", "D2", "N2O", "CH4", "SF6")
 RADII = (75e-6, 100e-6, 125e-6, 150e-6)
 
 
@@ -54,11 +55,24 @@ def nonlinear_phase(p):
             / p["radius"] ** 2)
 
 
+def _work(No, raman, p):
+    return No * math.log2(No) * (2.0 if raman else 1.0) * nonlinear_phase(p) ** 0.6
+
+
 def schedule_priority(p, prob):
     """Estimated work of an instance: per-step transform cost times nonlinear phase^0.6."""
-    No = prob.grid.No
     raman = any(r.kind in ("raman_field", "raman_env") for r in prob.transform.resp)
-    return No * math.log2(No) * (2.0 if raman else 1.0) * nonlinear_phase(p) ** 0.6
+    return _work(prob.grid.No, raman, p)
+
+
+def shard_cost(p, λ0=800e-9):
+    """``schedule_priority`` of an instance from its arguments alone (the grid, without the
+    mode and response set-up), so that every rank of a multi-GPU scan computes the same
+    costs for the whole draw cheaply and deterministically. Raman is on for the molecular
+    gases, as in ``prop_capillary``'s default (Interface.jl:538-556)."""
+    from .grid import RealGrid
+    g = RealGrid(p["flength"], λ0, (p["λmin"], p["λmax"]), p["trange"])
+    return _work(g.No, p["gas"] in RAMAN_GASES, p)
 
 
 def partition(costs, nparts):

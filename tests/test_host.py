@@ -82,6 +82,8 @@ def _rank_main(rank, world, port, costs, q):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
+    if costs is None:  # each rank prices the whole draw itself, as bench.py's ranks do
+        costs = [scan.shard_cost(p) for p in scan.draw_instances(64)]
     mine = scan.shard(costs, rank, world)
     t = torch.zeros(len(costs), dtype=torch.int64)
     t[mine] = 1
@@ -92,10 +94,16 @@ def _rank_main(rank, world, port, costs, q):
     dist.destroy_process_group()
 
 
-def test_multi_rank_scan_split_gloo():
+def test_shard_cost_is_the_schedule_priority():
+    for p in scan.draw_instances(12):
+        prob = scan.build_problem(p, saveN=2)
+        assert scan.shard_cost(p) == pytest.approx(scan.schedule_priority(p, prob), rel=1e-12)
+
+
+@pytest.mark.parametrize("costs", [np.random.default_rng(5).uniform(1, 10, 64).tolist(), None])
+def test_multi_rank_scan_split_gloo(costs):
     torch = pytest.importorskip("torch")
     import torch.multiprocessing as mp
-    costs = np.random.default_rng(5).uniform(1, 10, 64).tolist()
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()

@@ -105,6 +105,16 @@ typedef struct {
     double hdt;             /* response grid spacing (scales the convolution)            */
     /* Kerr_env_thg */
     const double* cthg;     /* [2*No] exp(2iω0 t) on the oversampled grid.to (complex)   */
+    /* Raman with a pressure gradient: the density dependence of each component's
+     * dephasing time, [4*ncomp] rows (model, A, B, C), or NULL when no component depends on
+     * the density. model 0: tau2[c] at every density; model 1 (RamanRespRotationalNonRigid
+     * with Bρ, Raman.jl:229-238): τ2(ρ) = 1/(π (A/(ρ/amg) + B ρ/amg)) for ρ > 0, ∞ at ρ = 0;
+     * model 2 (RamanRespVibrational with Bρ, Raman.jl:142-157): τ2(ρ) = 1/(π (C + A/(ρ/amg)
+     * + B ρ/amg)). Used only once a gradient is attached: the response spectrum is then
+     * rebuilt at ρ(z) of every stage node, as the reference rebuilds h(t; ρ) at every call
+     * (Nonlinear.jl:306-307). */
+    const double* tau2_rho;
+    double amg;             /* the amagat density [m^-3] of the τ2(ρ) laws                */
 } luna_resp_desc;
 
 typedef struct {
@@ -181,8 +191,10 @@ int luna_b200_rhs_device(luna_plan* plan, double* nl_dev, const double* Ew_dev, 
  *   Aeff(z) = a(z)^2 aeff_intg (Capillary.jl:295),
  * each in IEEE-rounded real operations in the order written (no fused multiply-adds).
  * The linop argument of the solve entry points is ignored for such a plan (may be NULL).
- * Field-resolved grids only; plans with a Raman response are rejected (its dephasing
- * times depend on the density). */
+ * Field-resolved grids only. A Raman response whose dephasing times depend on the density
+ * (luna_resp_desc.tau2_rho) has its spectrum rebuilt at ρ(z) before every evaluation (one
+ * extra transform of the 2*No response grid); its rebuild buffer is per plan for the RHS
+ * entry points and per instance in a batch. */
 #define LUNA_GRAD_MAXPTS 16
 typedef struct {
     int npts;                    /* pressure nodes, 2..LUNA_GRAD_MAXPTS                     */
@@ -275,7 +287,7 @@ int luna_b200_batch_set_replay(luna_batch* b, int i, const double* replay, long 
 void luna_b200_batch_destroy(luna_batch* b);
 
 /* ---------------------------------------------------------------- radial transform
- * TransRadial (NonlinearRHS.jl:406-474) on a field-resolved grid with an order-0 QDHT of
+ * TransRadial (NonlinearRHS.jl:406-474) on a field-resolved or envelope grid with an order-0 QDHT of
  * Nr points (Hankel.jl QDHT(R, N, dim=2), as built by Luna.setup for radial symmetry,
  * Luna.jl:239-279). Fields are column-major Nw x Nr complex arrays (Julia's
  * Matrix{ComplexF64}): element (ω, k) at k*Nw + ω. */
@@ -289,8 +301,9 @@ typedef struct {
 typedef struct luna_radial_plan luna_radial_plan;
 
 /* Replaces the TransRadial constructor (NonlinearRHS.jl:430-458). The grid descriptor is
- * that of one radial column (kind 0; its outfac is ignored, in_scale = pad scale / No);
- * responses as for luna_b200_plan_create (Raman is not available here). */
+ * that of one radial column (kind 0 or 1; its outfac is ignored, in_scale = pad scale / No);
+ * responses as for luna_b200_plan_create, applied column by column as Et_to_Pt! does with
+ * its CartesianIndices (NonlinearRHS.jl:137-141). */
 int luna_b200_radial_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
                                  const luna_radial_desc* radial, int precision, luna_radial_plan** out);
 void luna_b200_radial_plan_destroy(luna_radial_plan* plan);

@@ -56,7 +56,7 @@ class RespDesc(ctypes.Structure):
                 ("adk_pre", c_double), ("adk_a", c_double), ("adk_b", c_double),
                 ("adk_pw", c_double), ("adk_thr", c_double),
                 ("ncomp", c_int), ("hpre", PD), ("tau2", PD), ("hwin", PD), ("htt", PD),
-                ("hdt", c_double), ("cthg", PD)]
+                ("hdt", c_double), ("cthg", PD), ("tau2_rho", PD), ("amg", c_double)]
 
 
 class RadialDesc(ctypes.Structure):

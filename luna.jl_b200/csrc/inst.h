@@ -50,7 +50,14 @@ typedef struct {
     int hilb;
     // Kerr_env_thg (kind KERR_ENV): [No] exp(2i w0 t) on the oversampled grid, or null
     const double2* cthg;
+    // Raman with a pressure gradient: [4 * ncomp] (model, A, B, C) of tau2(rho) per
+    // component, or null; amg the amagat density; hscale = 1/max|hpre| (the normalisation of
+    // the spectrum); hz = 1 when H is rebuilt at rho(z) in place (read with plain loads)
+    const double* t2rho;
+    double amg, hscale;
+    int hz;
 } LunaResp;
+#define LUNA_RAMAN_MAXC 4  // components of a density-dependent Raman response
 
 // Pressure-gradient fill and/or taper (z-dependent density, radius, normalisation and
 // linear operator); the fields mirror luna_gradient_desc of the public header.
@@ -93,6 +100,7 @@ typedef struct {
     const LunaGrad* grad;
     double2* linz;  // [Nw]
     double2* outz;  // [Nw + 1]
+    int ramz;       // 1 + index of a Raman response rebuilt at rho(z) (its H is writable), 0: none
     // ---- integrator (RK45.solve_precon) ----
     const double2* y0;   // [Nw] initial field (kept, so a batch can be re-run)
     double2* y;

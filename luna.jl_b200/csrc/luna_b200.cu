@@ -393,14 +393,8 @@ raman_h_kernel(LunaResp r, int No, double hscale, cpx<double>* buf, cpx<Rl>* H, 
     for (int m = tid; m < No; m += LUNA_BLOCK) {
         double a = 0, b = 0;
         if (m < No / 2) {
-            for (int j = 0; j < 2; ++j) {
-                const int n = 2 * m + j;
-                double h = 0;
-                for (int c = 0; c < r.ncomp; ++c) h += r.hpre[(size_t)c * No + n] * exp(-r.htt[n] / r.tau2[c]);
-                h *= r.hwin[n] * hscale;
-                if (j == 0) a = h;
-                else b = h;
-            }
+            a = raman_sample(r, No, 2 * m, r.tau2, hscale);
+            b = raman_sample(r, No, 2 * m + 1, r.tau2, hscale);
         }
         buf[Swz<double>::f(split_pos(m, No, P))] = mk<double>(a, b);
     }
@@ -516,6 +510,7 @@ struct luna_plan {
     LunaInst proto{};
     std::vector<void*> allocs;
     bool has_raman = false;
+    void* d_hbuf = nullptr;      // FP64 work buffer of the Raman spectrum build ([No] complex)
     LunaGrad* d_grad = nullptr;  // pressure gradient (device copy), or null
     // single-call RHS resources
     bool inst_stale = false;     // d_inst predates a change of proto
@@ -913,11 +908,27 @@ int luna_b200_plan_create(const luna_grid_desc* g, const luna_resp_desc* resps, 
                 UP(d.tau2, d.ncomp, &r.tau2);
                 UP(d.hwin, g->No, &r.hwin);
                 UP(d.htt, g->No, &r.htt);
+                r.hscale = 1.0 / hmax;
+                if (d.tau2_rho) {
+                    // density laws of the dephasing times (used once a gradient is attached)
+                    bool dep = false;
+                    for (int c = 0; c < d.ncomp; ++c) {
+                        const double m = d.tau2_rho[4 * c];
+                        if (m != 0.0 && m != 1.0 && m != 2.0) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Raman tau2_rho: unknown model"); }
+                        dep = dep || m != 0.0;
+                    }
+                    if (dep) {
+                        if (d.ncomp > LUNA_RAMAN_MAXC || !(d.amg > 0)) { free_all(p->allocs); delete p; return fail(LUNA_ERR_BAD_ARG, "Raman tau2_rho: at most 4 components and amg > 0"); }
+                        UP(d.tau2_rho, 4 * (size_t)d.ncomp, &r.t2rho);
+                        r.amg = d.amg;
+                    }
+                }
                 // spectrum of the response, computed once on the device in FP64
                 cpx<double>* b1 = nullptr;
                 if (dalloc(p->allocs, &b1, sizeof(cpx<double>) * g->No)) {
                     free_all(p->allocs); delete p; return LUNA_ERR_CUDA;
                 }
+                p->d_hbuf = b1;
                 if (precision == LUNA_PREC_FP64) {
                     cpx<double>* H = nullptr;
                     if (dalloc(p->allocs, &H, sizeof(cpx<double>) * (g->No + 1))) { free_all(p->allocs); delete p; return LUNA_ERR_CUDA; }
@@ -991,12 +1002,24 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
     if (!g) {
         p->proto.grad = nullptr;
         p->inst_stale = true;
+        if (p->proto.ramz) {
+            // back to the spectrum at the dephasing times given at plan creation
+            LunaResp& r = p->proto.resp[p->proto.ramz - 1];
+            r.hz = 0;
+            p->proto.ramz = 0;
+            TwDev tw;
+            int rc = get_tw(tw);
+            if (rc) return rc;
+            if (p->precision == LUNA_PREC_FP64)
+                raman_h_kernel<double><<<1, LUNA_BLOCK>>>(r, p->proto.No, r.hscale, (cpx<double>*)p->d_hbuf, (cpx<double>*)const_cast<void*>(r.H), tw.d);
+            else
+                raman_h_kernel<float><<<1, LUNA_BLOCK>>>(r, p->proto.No, r.hscale, (cpx<double>*)p->d_hbuf, (cpx<float>*)const_cast<void*>(r.H), tw.d);
+            CK(cudaGetLastError());
+            CK(cudaDeviceSynchronize());
+        }
         return LUNA_OK;
     }
     if (p->proto.kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "plan_set_gradient: field-resolved grids only");
-    if (p->has_raman)
-        return fail(LUNA_ERR_UNSUPPORTED, "plan_set_gradient: Raman responses depend on the density through "
-                                          "their dephasing times; not available with a pressure gradient");
     if (g->npts < 2 || g->npts > LUNA_GRAD_MAXPTS) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: npts out of range");
     if (g->two_point && g->npts != 2) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: a two-point fill has npts == 2");
     for (int i = 0; i + 1 < g->npts; ++i)
@@ -1050,6 +1073,15 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
     h.ofs = (const double2*)t;
     const LunaGrad* d = nullptr;
     if (upload(p->allocs, &h, 1, &d)) return LUNA_ERR_CUDA;
+    // a Raman response with density-dependent dephasing: its spectrum (the plan's own
+    // buffer for the RHS entry points; batches give every instance one) is rebuilt at ρ(z)
+    for (int i = 0; i < p->proto.nresp; ++i) {
+        LunaResp& r = p->proto.resp[i];
+        if (r.kind == LUNA_RESP_RAMAN && r.t2rho) {
+            r.hz = 1;
+            p->proto.ramz = i + 1;
+        }
+    }
     p->d_grad = const_cast<LunaGrad*>(d);
     p->proto.grad = p->d_grad;
     p->inst_stale = true;
@@ -1137,6 +1169,8 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         for (int j = 0; j < 7; ++j) ok[j] = carve(Nw * kel);
         const size_t oe1 = carve(Nw * sizeof(double2));
         const size_t olz = carve(I.grad ? Nw * sizeof(double2) : 0), ooz = carve(I.grad ? (Nw + 1) * sizeof(double2) : 0);
+        // Raman spectrum at ρ(z), rebuilt by the solver in this instance's own buffer
+        const size_t ohz = carve((I.grad && I.ramz) ? ((size_t)I.No + 1) * kel : 0);
         const size_t og = carve(gsb);
         const size_t osv = carve((size_t)opts->saveN * Nw * sizeof(double2));
         const size_t olog = carve((size_t)(opts->steplog_cap > 0 ? opts->steplog_cap : 0) * 4 * sizeof(double));
@@ -1154,6 +1188,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
         if (I.grad) {
             I.linz = (double2*)(slab + olz);
             I.outz = (double2*)(slab + ooz);
+            if (I.ramz) I.resp[I.ramz - 1].H = slab + ohz;
         }
         I.gscr = slab + og;
         I.saves = (double2*)(slab + osv);
@@ -1216,7 +1251,7 @@ int luna_b200_batch_create(luna_plan* const* plans, int n, const luna_solve_opts
             const size_t half = align_up((size_t)(I.No / 2) * sizeof(float2), 256);
             const size_t efac = align_up((size_t)I.Nw * sizeof(float2), 256);
             const bool fits1 = smem_wanted<float>(I) <= (size_t)maxs;
-            const bool ok_cl = I.kind == 0 && has_raman(I) && !fits1 && !needs_hilbert(I) &&
+            const bool ok_cl = I.kind == 0 && has_raman(I) && !fits1 && !needs_hilbert(I) && !I.grad &&
                                LUNA_SMALL_BYTES + half + efac <= (size_t)std::min<int>(maxs, b->smem);
             if (ok_cl) big.push_back(i);
             else reg.push_back(i);
@@ -1633,18 +1668,11 @@ int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* 
                                  const luna_radial_desc* rd, int precision, luna_radial_plan** out) {
     if (!g || !rd || !out || !rd->Mi || !rd->Mf || !rd->outfac)
         return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: null argument");
-    if (g->kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: only field-resolved (RealGrid) radial transforms");
     if (rd->Nr < 1 || rd->Nr > 4096) return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: Nr must be in 1..4096");
     if (precision != LUNA_PREC_FP64 && precision != LUNA_PREC_MIXED)
         return fail(LUNA_ERR_BAD_ARG, "radial_plan_create: unknown precision");
     if (precision == LUNA_PREC_MIXED && rd->Nr % 64 != 0)
         return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: the mixed-precision QDHT needs Nr to be a multiple of 64");
-    for (int i = 0; i < nresp; ++i) {
-        if (resps[i].kind == LUNA_RESP_RAMAN || resps[i].kind == LUNA_RESP_RAMAN_NOTHG)
-            return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Raman response not available for the radial transform");
-        if (resps[i].kind == LUNA_RESP_KERR_FIELD_NOTHG)
-            return fail(LUNA_ERR_UNSUPPORTED, "radial_plan_create: Kerr_field_nothg not available for the radial transform");
-    }
     // the column plan: grid and responses; its output factor is unused (the radial one
     // is applied after the QDHT)
     std::vector<double> ones(2 * (size_t)g->Nw, 0.0);

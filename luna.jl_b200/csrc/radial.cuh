@@ -179,8 +179,12 @@ __global__ void __launch_bounds__(256) rad_gemm_f64(const double* __restrict__ A
 
 // ------------------------------------------------------------------ per-column responses
 // One CTA per radial column n: Pw[:, n] = crop-free rfft(towin * P(irfft(pad Er[:, n])))
-// (to_time!, Et_to_Pt!, towin, to_freq! of TransRadial on one column; the pad scale and
-// 1/No are in I.in_scale, the crop scale in the output factor).
+// (to_time!, Et_to_Pt!, towin, to_freq! of TransRadial on one column, which the reference
+// applies column by column, NonlinearRHS.jl:137-141; the pad scale and 1/No are in
+// I.in_scale, the crop scale in the output factor). The column is the mode-averaged
+// transform of a plan whose output factor is one: field-resolved grids with every response
+// form (Raman and the analytic-signal forms included) and envelope grids (fft/ifft with
+// copy_scale_both! padding).
 template <typename Rl>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
 rad_column_kernel(const LunaInst* inst, const cpx<Rl>* Er, cpx<Rl>* Pw, TwTab<Rl> tw, int smem_bytes,
@@ -193,13 +197,9 @@ rad_column_kernel(const LunaInst* inst, const cpx<Rl>* Er, cpx<Rl>* Pw, TwTab<Rl
     plan_ws<Rl>(I, smem, smem_bytes, w, tw, gscr ? gscr + (size_t)c * gstride : nullptr);
     if (threadIdx.x == 0) *w.flag = 0;
     __syncthreads();
-    const int M = I.No / 2;
     const cpx<Rl>* E = Er + (size_t)c * I.Nw;
     cpx<Rl>* o = Pw + (size_t)c * I.Nw;
-    int P;
-    cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, [&](int k) { return cvt<double>(E[k]); }, &P);
-    pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
-    r2c_to_freq<Rl>(w, x, M, I.Nw, [&](int k, cpx<double> X) { o[k] = cvt<Rl>(X); });
+    rhs<Rl>(I, w, [&](int k) { return cvt<double>(E[k]); }, [&](int k, cpx<double> X) { o[k] = cvt<Rl>(X); });
     if (threadIdx.x == 0 && *w.flag) atomicOr(flags, *w.flag);
 }
 

@@ -342,8 +342,11 @@ __device__ __forceinline__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>
             cpx<double> a2 = Zm + conj(Zk), b2 = Zm - conj(Zk);
             Xm = scale(0.5, a2) + scale(0.5, mul_mi<double, false>(Wm * b2));
         }
-        cpx<double> Yk = Xk * cvt<double>(ldg(H + k));
-        cpx<double> Ym = Xm * cvt<double>(ldg(H + (M - k)));
+        // a spectrum rebuilt at rho(z) by this kernel is read with plain loads
+        const cpx<double> Hk = r.hz ? cvt<double>(H[k]) : cvt<double>(ldg(H + k));
+        const cpx<double> Hm = r.hz ? cvt<double>(H[M - k]) : cvt<double>(ldg(H + (M - k)));
+        cpx<double> Yk = Xk * Hk;
+        cpx<double> Ym = Xm * Hm;
         // inverse split: Z'[k] = (Y[k] + conj Y[M-k]) + i W^-k (Y[k] - conj Y[M-k])
         cpx<double> Wi = conj(Wk);
         cpx<double> Zk2 = (Yk + conj(Ym)) + mul_mi<double, true>(Wi * (Yk - conj(Ym)));
@@ -357,6 +360,69 @@ __device__ __forceinline__ cpx<Rl>* raman_conv(const LunaResp& r, int No, Ws<Rl>
     __syncthreads();
     cpx<Rl>* other = w.ram_alt ? ((Z == w.ram) ? w.ram_alt : w.ram) : nullptr;
     return block_fft<Rl, true>(Z, other, No, w.tw);
+}
+
+// Dephasing time of Raman component c at density rho (Raman.jl:142-157, 229-238): the laws
+// of luna_resp_desc.tau2_rho in the reference's order of operations, each rounded.
+__device__ __forceinline__ double raman_tau2(const LunaResp& r, int c, double rho) {
+    const double* q = r.t2rho + 4 * c;
+    const int model = (int)q[0];
+    if (model == 0) return r.tau2[c];
+    if (model == 1 && !(rho > 0)) return INFINITY;
+    const double s = __dadd_rn(__dadd_rn(model == 2 ? q[3] : 0.0, __ddiv_rn(q[1], __ddiv_rn(rho, r.amg))),
+                               __ddiv_rn(__dmul_rn(q[2], rho), r.amg));
+    return __ddiv_rn(1.0, __dmul_rn(3.141592653589793, s));  // π as a double
+}
+
+// hscale * h(t_n; tau2) of a Raman response (CombinedRamanResponse(ht, rho), Raman.jl:256-262):
+// w(t_n) * sum_c hpre_c(t_n) exp(-t_n / tau2_c). The damping at t = 0 is 1 for every tau2,
+// including tau2 = 0 (a vibrational law at rho = 0, where the reference forms 0/0; its
+// undamped response is 0 there, and the polarisation is scaled by rho = 0).
+__device__ __forceinline__ double raman_sample(const LunaResp& r, int No, int n, const double* tau2, double hscale) {
+    const double tt = r.htt[n];
+    double h = 0;
+    for (int c = 0; c < r.ncomp; ++c) h += r.hpre[(size_t)c * No + n] * (tt == 0.0 ? 1.0 : exp(-tt / tau2[c]));
+    return h * (r.hwin[n] * hscale);
+}
+
+// Raman response spectrum at density rho for a plan with a pressure gradient whose
+// dephasing times depend on the density; the reference rebuilds h(t; rho) and transforms it
+// at every call (Nonlinear.jl:306-307). Samples as raman_h_kernel, transformed in the compute
+// precision in the Raman buffers (free between evaluations) into the writable r.H.
+template <typename Rl>
+__device__ __noinline__ void raman_h_at(const LunaInst& I, Ws<Rl>& w, double rho) {
+    const LunaResp& r = I.resp[I.ramz - 1];
+    const int No = I.No, tid = threadIdx.x;
+    double t2[LUNA_RAMAN_MAXC];
+#pragma unroll
+    for (int c = 0; c < LUNA_RAMAN_MAXC; ++c) t2[c] = (c < r.ncomp) ? raman_tau2(r, c, rho) : 1.0;
+    const int P = buf_split<Rl>(w.ram_alt, No);
+    __syncthreads();
+    for (int m = tid; m < No; m += LUNA_BLOCK) {
+        double a = 0, b = 0;
+        if (m < No / 2) {
+            a = raman_sample(r, No, 2 * m, t2, r.hscale);
+            b = raman_sample(r, No, 2 * m + 1, t2, r.hscale);
+        }
+        w.ram[Swz<Rl>::f(split_pos(m, No, P))] = mk<Rl>((Rl)a, (Rl)b);
+    }
+    __syncthreads();
+    const cpx<Rl>* Z = block_fft<Rl, false>(w.ram, w.ram_alt, No, w.tw);
+    cpx<Rl>* H = reinterpret_cast<cpx<Rl>*>(const_cast<void*>(r.H));
+    const int M = No;
+    for (int k = tid; k <= M; k += LUNA_BLOCK) {
+        const cpx<double> Zk = cvt<double>(Z[Swz<Rl>::f(k & (M - 1))]);
+        const cpx<double> Zm = cvt<double>(Z[Swz<Rl>::f((M - k) & (M - 1))]);
+        cpx<double> X;
+        if (k == 0) X = mk<double>(Zk.x + Zk.y, 0.0);
+        else if (k == M) X = mk<double>(Zk.x - Zk.y, 0.0);
+        else {
+            const cpx<double> Wk = half_twiddle<Rl, false>(w.tw, k, M);
+            X = scale(0.5, Zk + conj(Zm)) + scale(0.5, mul_mi<double, false>(Wk * (Zk - conj(Zm))));
+        }
+        H[k] = cvt<Rl>(X);
+    }
+    __syncthreads();
 }
 
 // ------------------------------------------------------------------ Raman clusters
@@ -1261,9 +1327,12 @@ __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double 
     __syncthreads();
 }
 
+// ... and, with wantH, the Raman spectrum at rho(z) of a density-dependent response (before
+// a right-hand-side evaluation at z; grad_fill_to leaves rho in w.red[0])
 template <typename Rl>
-__device__ __forceinline__ void grad_fill(const LunaInst& I, Ws<Rl>& w, double z, bool wantL) {
+__device__ __forceinline__ void grad_fill(const LunaInst& I, Ws<Rl>& w, double z, bool wantL, bool wantH = true) {
     grad_fill_to(I, w.red, z, wantL, I.linz, I.outz);
+    if (wantH && I.ramz) raman_h_at<Rl>(I, w, w.red[0]);
 }
 
 // Stats.default for a mode-averaged field-resolved transform (Stats.jl:495-532) on the
@@ -1590,7 +1659,7 @@ __device__ void solve_instance(LunaInst& I, Ws<Rl>& w, Ctl& c) {
             // GridCondition saves (Output.jl:65-82, 490-502)
             while (saved < I.saveN && I.zsave[saved] <= c.tn) {
                 // make_prop! evaluates a z-dependent linop at the save point itself
-                if (I.grad) grad_fill<Rl>(I, w, I.zsave[saved], true);
+                if (I.grad) grad_fill<Rl>(I, w, I.zsave[saved], true, false);
                 interpolate_row<Rl, Kt>(Nw, I.grad ? I.linz : I.linop, c, I.zsave[saved], k, py, pyn,
                                         I.saves + (size_t)saved * Nw);
                 ++saved;

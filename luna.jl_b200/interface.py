@@ -188,8 +188,6 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         # z-dependent linear operator and normalisation (LinearOps.make_linop,
         # LinearOps.jl:337-360; norm_mode_average with βfun!(β, z))
         from .gradient import TransModeAvgZ, make_linop
-        if raman:
-            raise NotImplementedError("Raman responses with a pressure gradient are not supported")
         linop, _ = make_linop(grid, mode, λ0)
         transform = TransModeAvgZ(grid, resp, grad, mode, λ0)
     else:

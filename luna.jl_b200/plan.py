@@ -21,9 +21,11 @@ def _c128(a):
     return np.ascontiguousarray(a, dtype=np.complex128)
 
 
-def resp_descs(resp, rho, keep):
+def resp_descs(resp, rho, keep, rho_tau2=None):
     """C-ABI descriptors of the responses (Et_to_Pt! order) at density ``rho``; arrays the
-    descriptors point to are appended to ``keep``."""
+    descriptors point to are appended to ``keep``. ``rho_tau2`` (default ``rho``) is the
+    density of the Raman dephasing times at plan creation (a pressure gradient's plan has
+    coefficients for rho = 1 and rebuilds the Raman spectrum at rho(z))."""
     rds = []
     for r in resp:
         d = _lib.RespDesc()
@@ -67,7 +69,13 @@ def resp_descs(resp, rho, keep):
             d.coef = rho
             resp = r.r
             hpre = _f64(np.stack(resp.hpres))
-            tau2 = _f64(resp.tau2s(rho))
+            tau2 = _f64(resp.tau2s(rho if rho_tau2 is None else rho_tau2))
+            rows = resp.tau2_rows()
+            if rows is not None:
+                rows = _f64(rows.ravel())
+                keep.append(rows)
+                d.tau2_rho = _lib.dptr(rows)
+                d.amg = pd.amg
             hwin, htt = _f64(resp.w), _f64(resp.tt)
             keep += [hpre, tau2, hwin, htt]
             d.ncomp = len(resp.hpres)
@@ -161,7 +169,8 @@ def transform_descs(t):
     gd.omega, gd.t = _lib.dptr(om), _lib.dptr(tt)
     gd.aeff = t.aeff
     gd.escale = 1.0 / math.sqrt(pd.eps_0 * pd.c * t.aeff / 2)
-    rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep)
+    rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep,
+                     rho_tau2=t.densityfun(0.0) if zdep else None)
     return gd, rds, keep, Nw, zdep, crop, pad
 
 

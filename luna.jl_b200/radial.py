@@ -1,15 +1,18 @@
 """Radially symmetric free-space propagation (host setup), mirroring Luna.jl.
 
-* ``make_const_linop_radial`` — LinearOps.make_const_linop(grid::RealGrid, q::QDHT, nfun)
-  (LinearOps.jl:130-144, 185-197): L(ω, k) = -i(sqrt(k(ω)^2 - k_r^2) - β1 ω), evanescent
-  components damped by min(sqrt|.|, 200).
+* ``make_const_linop_radial`` — LinearOps.make_const_linop(grid, q::QDHT, nfun)
+  (LinearOps.jl:130-166, 185-197, 213-226): L(ω, k) = -i(sqrt(k(ω)^2 - k_r^2) - β1 ω),
+  evanescent components damped by min(sqrt|.|, 200); on an envelope grid without THG the
+  reference propagation constant β(ω0) is taken out (+iβ(ω0)).
 * ``const_norm_radial`` — NonlinearRHS.const_norm_radial / norm_radial
   (NonlinearRHS.jl:482-524): sqrt(k^2 - k_r^2)/(μ0 ω), 1 where that is not real or ω = 0.
 * ``TransRadial`` — the transform description (NonlinearRHS.jl:406-474) that the device
   plan is built from.
 * ``GaussGaussField`` — Fields.SpatioTemporalField with a Gaussian profile in time and
   radius, energy normalisation by ``energyfuncs(grid, q)`` and free-space propagation by
-  ``propz`` (Fields.jl:343-411, 536-549); ``focal_length`` adds a thin-lens phase.
+  ``propz`` (Fields.jl:343-411, 536-560); ``focal_length`` adds a thin-lens phase. On an
+  envelope grid the field is sqrt(I) exp(i(ϕ + Δω t)) and the time transform a complex FFT
+  (make_Etr for EnvGrid, Fields.jl:374-378).
 """
 import math
 
@@ -17,11 +20,12 @@ import numpy as np
 
 from . import physdata as pd
 from .fields import analytic, simpson_even
-from .grid import RealGrid
+from .grid import EnvGrid, RealGrid
 from .hankel import QDHT
 from .maths import gauss
-from .nonlinear import Kerr_field, PlasmaCumtrapz, ionrate_fun_ADK
-from . import ionisation
+from .nonlinear import (Kerr_env, Kerr_env_thg, Kerr_field, Kerr_field_nothg, PlasmaCumtrapz,
+                        RamanPolarEnv, RamanPolarField, ionrate_fun_ADK)
+from . import ionisation, raman as _raman
 
 
 def _n_on_sidx(grid, nfun):
@@ -39,7 +43,7 @@ def _beta1(nfun, λ0):
     return (-f(w0 + 2 * h) + 8 * f(w0 + h) - 8 * f(w0 - h) + f(w0 - 2 * h)) / (12 * h)
 
 
-def make_const_linop_radial(grid, q, nfun):
+def make_const_linop_radial(grid, q, nfun, thg=False):
     n = _n_on_sidx(grid, nfun)
     β1 = _beta1(nfun, grid.referenceλ)
     k2 = (n * grid.ω / pd.c) ** 2
@@ -49,6 +53,10 @@ def make_const_linop_radial(grid, q, nfun):
     L = np.where(βsq < 0,
                  -1j * (-β1 * w) - np.minimum(np.sqrt(np.abs(βsq)), 200.0),
                  -1j * (np.sqrt(np.maximum(βsq, 0.0)) - β1 * w))
+    if grid.kind == "env" and not thg:
+        # out -= -im*βref, βref = ω0/c n(λ0) (LinearOps.jl:146-156, 213-226)
+        βref = grid.ω0 / pd.c * float(np.real(nfun(np.array([2 * math.pi * pd.c / grid.ω0]))[0]))
+        L = L - (-1j * βref)
     return np.ascontiguousarray(L.astype(np.complex128)), β1
 
 
@@ -93,8 +101,9 @@ class TransRadial:
 
 
 def energy_t_radial(grid, q, Etr):
-    """energyfuncs(grid::RealGrid, q)[1] (Fields.jl:536-541): Etr is (Nt, Nr)."""
-    Eta = np.apply_along_axis(analytic, 0, Etr)
+    """energyfuncs(grid, q)[1] (Fields.jl:536-554): Etr is (Nt, Nr); the analytic signal
+    of a real field, the envelope itself on an envelope grid."""
+    Eta = np.apply_along_axis(analytic, 0, Etr) if grid.kind == "real" else Etr
     tint = np.array([simpson_even(grid.t, np.abs(Eta[:, i]) ** 2) for i in range(Etr.shape[1])])
     return 2 * math.pi * pd.c * pd.eps_0 / 2 * q.integrateR(tint)
 
@@ -103,9 +112,12 @@ def GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=0.0, focal_length=No
     t = grid.t
     ω0 = pd.wlfreq(λ0)
     shape = gauss(t, τfwhm)[:, None] * np.exp(-0.5 * (q.r / (w0 / 2)) ** 2)[None, :]
-    Etr = np.sqrt(shape) * np.cos(ω0 * t + ϕ)[:, None]
+    if grid.kind == "real":
+        Etr = np.sqrt(shape) * np.cos(ω0 * t + ϕ)[:, None]
+    else:
+        Etr = np.sqrt(shape) * np.exp(1j * (ϕ + (ω0 - grid.ω0) * t))[:, None]
     Etr = Etr * math.sqrt(energy) / math.sqrt(energy_t_radial(grid, q, Etr))
-    Eωr = np.fft.rfft(Etr, axis=0)
+    Eωr = np.fft.rfft(Etr, axis=0) if grid.kind == "real" else np.fft.fft(Etr, axis=0)
     if focal_length is not None:
         # thin lens: exp(-i ω r^2 / (2 c f)) applied in (ω, r)
         Eωr = Eωr * np.exp(-1j * grid.ω[:, None] * (q.r ** 2)[None, :] / (2 * pd.c * focal_length))
@@ -125,20 +137,33 @@ class RadialProblem:
 
 def prop_radial_args(gas, pressure, *, R, N, flength, λ0, λlims, trange, τfwhm, energy, w0,
                      propz=0.0, focal_length=None, plasma="PPT", kerr=True, saveN=201,
-                     ppt_N=2 ** 16):
-    """Low-level radial set-up as in test/test_radial.jl and the freespace/radial example."""
-    grid = RealGrid(flength, λ0, λlims, trange)
+                     ppt_N=2 ** 16, envelope=False, thg=None, raman=False):
+    """Low-level radial set-up as in test/test_radial.jl and the freespace/radial and
+    radial_env examples. ``envelope`` builds an EnvGrid (Kerr_env, or Kerr_env_thg with
+    ``thg``; no plasma); ``thg=False`` on a field-resolved grid selects Kerr_field_nothg;
+    ``raman`` adds the gas's molecular Raman response (RamanPolarField / RamanPolarEnv,
+    applied per radial column)."""
+    if thg is None:
+        thg = not envelope
+    grid = EnvGrid(flength, λ0, λlims, trange, thg=thg) if envelope else RealGrid(flength, λ0, λlims, trange)
     q = QDHT(R, N)
     nfun = pd.ref_index_fun(gas, pressure)
     dens0 = pd.density(gas, pressure)
     resp = []
+    γ3 = pd.gamma3_gas(gas)
     if kerr:
-        resp.append(Kerr_field(pd.gamma3_gas(gas)))
-    if plasma:
+        if envelope:
+            resp.append(Kerr_env_thg(γ3, grid.ω0, grid.to) if thg else Kerr_env(γ3))
+        else:
+            resp.append(Kerr_field(γ3) if thg else Kerr_field_nothg(γ3, len(grid.to)))
+    if plasma and not envelope:
         ionpot = pd.ionisation_potential(gas)
         rate = ionrate_fun_ADK(gas) if plasma == "ADK" else ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
         resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, ionpot))
-    linop, _ = make_const_linop_radial(grid, q, nfun)
+    if raman:
+        rr = _raman.raman_response(grid.to, gas)
+        resp.append(RamanPolarEnv(grid.to, rr) if envelope else RamanPolarField(grid.to, rr, thg=thg))
+    linop, _ = make_const_linop_radial(grid, q, nfun, thg=thg)
     norm = const_norm_radial(grid, q, nfun)
     transform = TransRadial(grid, q, resp, dens0, norm)
     Eω = GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=propz, focal_length=focal_length)

@@ -38,7 +38,32 @@ class SDO:
 def RamanRespNormedSingleDampedOscillator(K, Omega, tau2):
     """SDO normalised to unit integral then scaled by K (Raman.jl:53-59)."""
     K = K * (Omega ** 2 + 1 / tau2 ** 2) / Omega
-    return SDO(K, Omega, lambda rho: tau2)
+    return SDO(K, Omega, Dephasing(0, tau2=tau2))
+
+
+class Dephasing:
+    """Dephasing time tau2(rho) of a Raman component, in the three forms of Raman.jl and with
+    the (model, A, B, C) row the C ABI takes (luna_resp_desc.tau2_rho):
+
+    * model 0, constant: ``rho -> tau2`` (Raman.jl:53-59, 145-149, 223-227);
+    * model 1, rotational with Brho (Raman.jl:229-235): 1/(pi (A/(rho/amg) + B rho/amg))
+      for rho > 0, inf at rho = 0;
+    * model 2, vibrational with Brho (Raman.jl:150-155): 1/(pi (C + A/(rho/amg) + B rho/amg)).
+    """
+
+    def __init__(self, model, tau2=math.nan, A=0.0, B=0.0, C=0.0):
+        self.model, self.tau2, self.A, self.B, self.C = model, tau2, A, B, C
+
+    def row(self):
+        return [float(self.model), self.A, self.B, self.C]
+
+    def __call__(self, rho):
+        if self.model == 0:
+            return self.tau2
+        if self.model == 1:
+            return (1 / (math.pi * (self.A / (rho / pd.amg) + self.B * rho / pd.amg))
+                    if rho > 0 else math.inf)
+        return 1 / (math.pi * (self.C + self.A / (rho / pd.amg) + self.B * rho / pd.amg))
 
 
 def RamanRespVibrational(Omega_v, dadQ, mu, tau2=None, Brho=None, Arho=None, C=0.0):
@@ -47,9 +72,9 @@ def RamanRespVibrational(Omega_v, dadQ, mu, tau2=None, Brho=None, Arho=None, C=0
     if Brho is None:
         if tau2 is None:
             raise ValueError("one of tau2 or Brho must be specified")
-        f = lambda rho: tau2
+        f = Dephasing(0, tau2=tau2)
     else:
-        f = lambda rho: 1 / (math.pi * (C + Arho / (rho / pd.amg) + Brho * rho / pd.amg))
+        f = Dephasing(2, A=Arho, B=Brho, C=C)
     return SDO(K, Omega_v, f)
 
 
@@ -75,10 +100,9 @@ class RotationalNonRigid:
         if Brho is None:
             if tau2 is None:
                 raise ValueError("one of tau2 or Brho must be specified")
-            self.tau2fun = lambda rho: tau2
+            self.tau2fun = Dephasing(0, tau2=tau2)
         else:
-            self.tau2fun = lambda rho: (1 / (math.pi * (Arho / (rho / pd.amg) + Brho * rho / pd.amg))
-                                        if rho > 0 else math.inf)
+            self.tau2fun = Dephasing(1, A=Arho, B=Brho)
         self.Rs = [SDO(K * (Js[i] + 1) * (Js[i] + 2) / (2 * Js[i] + 3)
                        * (rhoJ[i + 2] / (2 * Js[i] + 5) - rhoJ[i] / (2 * Js[i] + 1)),
                        Om[i], self.tau2fun) for i in range(len(Js))]
@@ -107,6 +131,12 @@ class CombinedRamanResponse:
 
     def tau2s(self, rho):
         return [R.hrdamp(rho) for R in self.Rs]
+
+    def tau2_rows(self):
+        """[ncomp, 4] (model, A, B, C) rows of the components' dephasing laws, or None when
+        none depends on the density (luna_resp_desc.tau2_rho)."""
+        rows = [R.tau2fun.row() for R in self.Rs]
+        return np.array(rows, dtype=np.float64) if any(r[0] != 0 for r in rows) else None
 
     def h(self, rho):
         """h(t; rho) on tt (Raman.jl:256-262): sum of damped components times window."""

@@ -36,8 +36,7 @@ def load():
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(LIB):
-        build()
+    build()  # compiles only when the source or the descriptor header is newer
     from luna_b200 import _lib as L
     lib = ctypes.CDLL(LIB)
     P = ctypes.POINTER

@@ -237,22 +237,19 @@ def trans_mode_avg(t, Ew, z):
 
 
 def trans_radial(t, Ew, z):
-    """(t::TransRadial)(nl, Eω, z) (NonlinearRHS.jl:466-474) for a field-resolved grid:
-    Ew is (Nω, Nr) in (ω, k) space."""
+    """(t::TransRadial)(nl, Eω, z) (NonlinearRHS.jl:466-474) for a field-resolved or an
+    envelope grid: Ew is (Nω, Nr) in (ω, k) space; the responses act on each radial column
+    (Et_to_Pt! with CartesianIndices, NonlinearRHS.jl:137-141)."""
     g, q = t.grid, t.q
-    Nw = Ew.shape[0]
-    Nwo = len(g.ωo)
-    Ewo = np.zeros((Nwo, Ew.shape[1]), dtype=np.complex128)
-    Ewo[:Nw] = ((Nwo - 1) / (Nw - 1)) * Ew
-    Et = np.fft.irfft(Ewo, g.No, axis=0)          # to_time! along dim 1
+    Nw, Nr = Ew.shape
+    Et = np.stack([to_time(g, Ew[:, i]) for i in range(Nr)], axis=1)  # to_time! along dim 1
     Er = q.inverse(Et, axis=1)                     # ldiv!(Eto, QDHT, Eto): k -> r
     Pr = np.zeros_like(Er)
-    for i in range(Er.shape[1]):                   # Et_to_Pt! per radial column
+    for i in range(Nr):                            # Et_to_Pt! per radial column
         Pr[:, i] = et_to_pt(Er[:, i], t.resp, t.density)
     Pr = Pr * g.towin[:, None]
     Pk = q.forward(Pr, axis=1)                     # mul!(Pto, QDHT, Pto): r -> k
-    Pwo = np.fft.rfft(Pk, axis=0)
-    nl = ((Nw - 1) / (Nwo - 1)) * Pwo[:Nw]          # to_freq!
+    nl = np.stack([to_freq(g, Pk[:, i], Nw) for i in range(Nr)], axis=1)  # to_freq!
     return nl * t.output_factor()
 
 

@@ -83,7 +83,8 @@ int main(void) {
            sizeof(luna_grid_desc), sizeof(luna_resp_desc), sizeof(luna_solve_opts), sizeof(luna_solve_stats));
     printf("luna_radial_desc %zu\n", sizeof(luna_radial_desc));
     P(luna_grid_desc, in_scale); P(luna_resp_desc, spl_n); P(luna_resp_desc, adk_thr);
-    P(luna_resp_desc, hdt); P(luna_resp_desc, cthg); P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
+    P(luna_resp_desc, hdt); P(luna_resp_desc, cthg); P(luna_resp_desc, tau2_rho); P(luna_resp_desc, amg);
+    P(luna_solve_opts, zsave); P(luna_solve_opts, steplog_cap);
     P(luna_solve_opts, replay); P(luna_solve_opts, nreplay); P(luna_solve_opts, flags);
     P(luna_radial_desc, Mf); P(luna_radial_desc, outfac);
     P(luna_grid_desc, omega); P(luna_grid_desc, escale); P(luna_solve_opts, stats_cap);
@@ -119,6 +120,8 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_resp_desc.adk_thr"]) == _lib.RespDesc.adk_thr.offset
     assert int(out["luna_resp_desc.hdt"]) == _lib.RespDesc.hdt.offset
     assert int(out["luna_resp_desc.cthg"]) == _lib.RespDesc.cthg.offset
+    assert int(out["luna_resp_desc.tau2_rho"]) == _lib.RespDesc.tau2_rho.offset
+    assert int(out["luna_resp_desc.amg"]) == _lib.RespDesc.amg.offset
     assert int(out["luna_solve_opts.zsave"]) == _lib.SolveOpts.zsave.offset
     assert int(out["luna_solve_opts.steplog_cap"]) == _lib.SolveOpts.steplog_cap.offset
     assert int(out["luna_radial_desc"]) == ctypes.sizeof(_lib.RadialDesc)

@@ -2,7 +2,8 @@
 
 Cases follow test/test_radial.jl: argon, a focused Gaussian beam, Kerr plus PPT or ADK
 plasma, at energies where the plasma term is a visible part of the response (20 µJ: ~0.3%
-with PPT; 50 µJ: ~6% with ADK, ~97% with PPT).
+with PPT; 50 µJ: ~6% with ADK, ~97% with PPT); and the other response forms per radial
+column (Raman, the analytic-signal Kerr term) and envelope grids (freespace/radial_env.jl).
 """
 import luna_b200_loader  # registers the luna.jl_b200 package
 
@@ -111,18 +112,82 @@ def test_radial_focus_matches_paraxial_gaussian_beam_on_gpu():
     assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < 1.5e-4
 
 
-def test_radial_plan_rejects_raman_and_envelope():
-    from luna_b200 import raman
-    from luna_b200.nonlinear import RamanPolarField
-    from luna_b200.radial import TransRadial
-    p = _problem(20e-6, "PPT")
-    t = p.transform
-    rr = raman.raman_response(t.grid.to, "N2")
-    bad = TransRadial(t.grid, t.q, list(t.resp) + [RamanPolarField(t.grid.to, rr)],
-                      t.density, t.normfun)
-    with pytest.raises(_lib.LunaError) as e:
-        radial_plan.RadialPlan.from_transform(bad)
-    assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED
+# ------------------------------------------------------------------ every response form, envelopes
+# TransRadial applies Et_to_Pt! column by column (NonlinearRHS.jl:137-141), so every
+# response of the mode-averaged transform is available per radial column: Raman
+# (RamanPolarField with and without THG), Kerr_field_nothg, and on an envelope grid
+# (freespace/radial_env.jl) Kerr_env, Kerr_env_thg and RamanPolarEnv.
+_FORMS = {
+    "H2-raman": dict(gas="H2", pressure=1.0, plasma="ADK", raman=True, energy=30e-6),
+    "H2-raman-nothg": dict(gas="H2", pressure=1.0, plasma=False, raman=True, thg=False, energy=30e-6),
+    "Ar-kerr-nothg": dict(gas="Ar", pressure=1.2, plasma="PPT", thg=False, energy=30e-6),
+    "Ar-env": dict(gas="Ar", pressure=1.2, envelope=True, energy=30e-6),
+    "Ar-env-thg": dict(gas="Ar", pressure=1.2, envelope=True, thg=True, energy=30e-6),
+    "N2-env-raman": dict(gas="N2", pressure=2.0, envelope=True, raman=True, energy=30e-6),
+}
+
+
+def _form(name, flength=0.01, N=64, saveN=5):
+    """The envelope cases take 0.8 ps so that the oversampled grid has the 1024 samples the
+    device's block transforms need at least (0.2 ps gives 256 on an envelope grid)."""
+    c = dict(_FORMS[name])
+    trange = 0.8e-12 if c.get("envelope") else 0.2e-12
+    return prop_radial_args(c.pop("gas"), c.pop("pressure"), R=1e-3, N=N, flength=flength, λ0=800e-9,
+                            λlims=(400e-9, 2000e-9), trange=trange, τfwhm=20e-15, w0=40e-6,
+                            saveN=saveN, **c)
+
+
+@pytest.mark.parametrize("name", list(_FORMS))
+def test_radial_rhs_every_form_matches_oracle(name):
+    p = _form(name)
+    rng = np.random.default_rng(13)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    nl = np.zeros_like(Ew)
+    p.transform(nl, Ew, 0.0)
+    ref = uppe.trans_radial(p.transform, Ew, 0.0)
+    assert _rel(nl, ref) < 1e-11, _rel(nl, ref)
+    plan = radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    nm = np.zeros_like(Ew)
+    plan.rhs(nm, Ew, 0.0)
+    assert _rel(nm, ref) < 2e-4, _rel(nm, ref)
+
+
+@pytest.mark.parametrize("name", ["H2-raman", "Ar-env", "N2-env-raman"])
+def test_radial_solve_every_form_replay_matches_oracle(name):
+    """On the oracle's step sequence every saved field within 1e-10 (FP64); the mixed
+    precision solve within 1e-3 spectral at every save."""
+    p = _form(name, flength=0.02)
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    r = radial_plan.run(p, replay=replay)
+    assert r.status == 0 and r.nsaved == 5 and r.steps == ores.steps
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+    m = radial_plan.run(p, precision=_lib.PREC_MIXED)
+    assert m.status == 0 and m.nsaved == 5
+    for a, b in zip(m.Eω, ores.Eω):
+        assert _rel(np.abs(a) ** 2, np.abs(b) ** 2) < 1e-3
+
+
+def test_radial_env_focus_matches_paraxial_gaussian_beam_on_gpu():
+    """freespace/radial_env.jl on the device: a 2 nJ envelope through a focus at 0.3 m over
+    0.6 m; the fluence profile at ω0 matches the paraxial Gaussian-beam width (as the
+    field-resolved test_radial.jl case). 0.8 ps for the device's 1024-sample minimum."""
+    w0, L = 40e-6, 0.6
+    p = prop_radial_args("Ar", 1.2, R=4e-3, N=128, flength=L, λ0=800e-9, λlims=(400e-9, 2000e-9),
+                         trange=0.8e-12, τfwhm=20e-15, energy=2e-9, w0=w0, propz=-0.3,
+                         envelope=True, plasma=False)
+    r = radial_plan.run(p)
+    assert r.status == 0
+    g, q = p.grid, p.q
+    Er = q.inverse(r.Eω[-1], axis=1)
+    i0 = np.argmin(np.abs(g.ω - 2 * np.pi * pd.c / 800e-9))
+    lam0 = 2 * np.pi * pd.c / g.ω[i0]
+    w1 = w0 * np.sqrt(1 + (L / 2 * lam0 / (np.pi * w0 ** 2)) ** 2)
+    Ia = np.exp(-0.5 * (q.r / (w1 / 2)) ** 2) * (w0 / w1) ** 2
+    Ir = np.abs(Er[i0]) ** 2
+    Ir, Ia = Ir / Ir.max(), Ia / Ia.max()
+    assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < 1.5e-4
 
 
 # ------------------------------------------------------------------ mixed precision

@@ -109,10 +109,45 @@ def test_equal_pressure_gradient_propagation_matches_constant():
             assert _rel(a[s], b[s]) < 1e-12
 
 
-def test_gradient_rejects_raman():
-    with pytest.raises(NotImplementedError):
-        prop_capillary_args(125e-6, 1.0, "H2", (2.0, 0.2), λ0=800e-9, τfwhm=10e-15,
-                            energy=50e-6, λlims=(400e-9, 2000e-9), trange=0.5e-12)
+def test_raman_dephasing_laws_and_rows():
+    """The dephasing laws of the molecular Raman models (Raman.jl:142-157, 229-238) and the
+    (model, A, B, C) rows the C ABI takes: H2 has density-dependent rotational and vibrational
+    linewidths, N2 a density-dependent rotational and a constant vibrational one."""
+    from luna_b200 import raman
+    from luna_b200.grid import RealGrid
+    g = RealGrid(0.3, 800e-9, (150e-9, 4e-6), 0.25e-12)
+    h2 = raman.raman_response(g.to, "H2")
+    rows = h2.tau2_rows()
+    assert rows.shape == (2, 4) and list(rows[:, 0]) == [1.0, 2.0]
+    rp = pd.raman_parameters("H2")
+    for rho in (0.3 * pd.amg, pd.amg, 4.5 * pd.amg):
+        r = rho / pd.amg
+        assert h2.tau2s(rho)[0] == 1 / (math.pi * (rp["Arho_r"] / r + rp["Brho_r"] * rho / pd.amg))
+        assert h2.tau2s(rho)[1] == 1 / (math.pi * (rp.get("Cv", 0.0) + rp["Arho_v"] / r + rp["Brho_v"] * rho / pd.amg))
+    assert h2.Rs[0].hrdamp(0.0) == math.inf
+    n2 = raman.raman_response(g.to, "N2")
+    rows = n2.tau2_rows()
+    assert list(rows[:, 0]) == [1.0, 0.0]
+    assert n2.tau2s(pd.amg)[1] == n2.tau2s(3 * pd.amg)[1]
+    # the glass response of the GNLSE form does not depend on the density
+    sio2 = raman.RamanRespNormedSingleDampedOscillator(1.0, 1e13, 32e-15)
+    assert raman.CombinedRamanResponse(g.to, [sio2]).tau2_rows() is None
+
+
+def test_gradient_with_raman_rebuilds_the_response_at_the_local_density():
+    """prop_capillary with a pressure gradient in a Raman-active gas (Interface.jl:538-556):
+    the transform's Raman response is h(t; ρ(z)) (Nonlinear.jl:306-307), so its spectrum at
+    z equals the constant-fill one at the local pressure."""
+    p = prop_capillary_args(125e-6, 0.3, "H2", (3.0, 0.5), λ0=800e-9, τfwhm=10e-15, energy=50e-6,
+                            λlims=(150e-9, 4e-6), trange=0.25e-12)
+    t = p.transform
+    rr = [r for r in t.resp if r.kind == "raman_field"][0].r
+    for z in (0.0, 0.13, 0.3):
+        pz = t.grad.p(z)
+        c = prop_capillary_args(125e-6, 0.3, "H2", pz, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
+                                λlims=(150e-9, 4e-6), trange=0.25e-12)
+        rc = [r for r in c.transform.resp if r.kind == "raman_field"][0].r
+        assert _rel(rr.h(t.densityfun(z)), rc.h(c.transform.density)) < 1e-12, z
 
 
 def _taper_case(radius, pressure=5.0, flength=5e-2):
@@ -172,6 +207,13 @@ _CASES = {
     "Ne-taper-3node": dict(radius=([0, 0.05, 0.15], [120e-6, 80e-6, 80e-6]), flength=0.15,
                            gas="Ne", pressure=2.0, λ0=800e-9, τfwhm=10e-15, energy=200e-6,
                            λlims=(150e-9, 4e-6), trange=0.25e-12),
+    # Raman-active fills: H2 (rotational and vibrational linewidths depend on the density,
+    # ADK plasma) and N2 (density-dependent rotational, constant vibrational linewidth)
+    "H2-falling": dict(radius=125e-6, flength=0.3, gas="H2", pressure=(3.0, 0.5), λ0=800e-9,
+                       τfwhm=10e-15, energy=60e-6, λlims=(150e-9, 4e-6), trange=0.25e-12),
+    "N2-rising": dict(radius=100e-6, flength=0.2, gas="N2", pressure=(0.3, 2.0), λ0=800e-9,
+                      τfwhm=20e-15, energy=40e-6, λlims=(200e-9, 4e-6), trange=0.5e-12,
+                      plasma=False),
 }
 
 
@@ -206,7 +248,8 @@ def test_device_linop_is_bit_identical_to_host(name):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "He-taper-gradient"])
+@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "He-taper-gradient", "H2-falling",
+                                  "N2-rising"])
 def test_gradient_rhs_matches_oracle(name):
     """(t::TransModeAvg)(nl, Eω, z) with densityfun(z) and βfun!(β, z) through the C ABI."""
     p = _case(name)
@@ -317,9 +360,9 @@ def test_gradient_step_stats_use_local_density(name):
 
 @pytest.mark.gpu
 def test_gradient_rejections():
-    """A Raman plan takes no gradient (its dephasing times depend on the density); the
-    allocation-free entry point rejects gradient plans; a plan without a gradient has no
-    device linop(z)."""
+    """A Raman plan whose gradient is removed again integrates as before it was attached (the
+    spectrum rebuilt at ρ(z) goes back to the one at plan creation); the allocation-free
+    entry point rejects gradient plans; a plan without a gradient has no device linop(z)."""
     from luna_b200 import _lib
     from luna_b200.gradient import gradient_desc
     from luna_b200.plan import Plan
@@ -333,7 +376,12 @@ def test_gradient_rejections():
     h2 = prop_capillary_args(125e-6, 0.3, "H2", 1.0, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
                              λlims=(150e-9, 4e-6), trange=0.25e-12)
     rplan = Plan.from_transform(h2.transform)
-    assert lib.luna_b200_plan_set_gradient(rplan.handle, _lib.ctypes.byref(d)) == _lib.LUNA_ERR_UNSUPPORTED
+    Ew = h2.Eω * np.exp(1j * 0.1 * np.random.default_rng(2).standard_normal(h2.Eω.shape))
+    nl0 = rplan.rhs(np.zeros_like(Ew), Ew, 0.0)
+    assert lib.luna_b200_plan_set_gradient(rplan.handle, _lib.ctypes.byref(d)) == 0
+    rplan.rhs(np.zeros_like(Ew), Ew, 0.13)
+    assert lib.luna_b200_plan_set_gradient(rplan.handle, None) == 0
+    assert np.array_equal(rplan.rhs(np.zeros_like(Ew), Ew, 0.0), nl0)
     L = np.zeros(len(h2.grid.ω), dtype=np.complex128)
     assert lib.luna_b200_plan_linop(rplan.handle, 0.0, _lib.dptr(L.view(np.float64)),
                                     _lib.dptr(None)) == _lib.LUNA_ERR_BAD_ARG

@@ -296,6 +296,32 @@ def test_radial_focus_matches_paraxial_gaussian_beam():
     assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < GOLDEN["radial_focus_bound"]
 
 
+def test_radial_env_focus_matches_paraxial_gaussian_beam():
+    """freespace/radial_env.jl's check on the envelope form of the oracle: a 2 nJ envelope
+    (EnvGrid, Kerr_env, linop with β(ω0) taken out) through a focus at 0.3 m over 0.6 m;
+    the fluence profile at ω0 matches the paraxial width to the same bound."""
+    from luna_b200.radial import prop_radial_args
+    w0, L = 40e-6, 0.6
+    p = prop_radial_args("Ar", 1.2, R=4e-3, N=128, flength=L, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=2e-9, w0=w0, propz=-0.3, envelope=True)
+    assert p.grid.kind == "env" and [r.kind for r in p.transform.resp] == ["kerr_env"]
+    res = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=3)
+    g, q = p.grid, p.q
+    Er = q.inverse(res.Eω[-1], axis=1)
+    i0 = np.argmin(np.abs(g.ω - 2 * np.pi * pd.c / 800e-9))
+    lam0 = 2 * np.pi * pd.c / g.ω[i0]
+    w1 = w0 * np.sqrt(1 + (L / 2 * lam0 / (np.pi * w0 ** 2)) ** 2)
+    Ia = np.exp(-0.5 * (q.r / (w1 / 2)) ** 2) * (w0 / w1) ** 2
+    Ir = np.abs(Er[i0]) ** 2
+    Ir, Ia = Ir / Ir.max(), Ia / Ia.max()
+    assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < GOLDEN["radial_focus_bound"]
+    # the input carries the requested energy (energyfuncs(grid::EnvGrid, q), Fields.jl:550-560)
+    from luna_b200.radial import energy_t_radial
+    Et = np.fft.ifft(q.inverse(p.Eω, axis=1), axis=0)
+    assert abs(energy_t_radial(g, q, Et) / 2e-9 - 1) < 1e-12
+
+
 def test_qdht_roundtrip_and_gaussian_pair():
     from luna_b200.hankel import QDHT
     q = QDHT(4e-3, 128)

@@ -191,7 +191,7 @@ int luna_b200_rhs_device(luna_plan* plan, double* nl_dev, const double* Ew_dev, 
  *   Aeff(z) = a(z)^2 aeff_intg (Capillary.jl:295),
  * each in IEEE-rounded real operations in the order written (no fused multiply-adds).
  * The linop argument of the solve entry points is ignored for such a plan (may be NULL).
- * Field-resolved grids only. A Raman response whose dephasing times depend on the density
+ * Field-resolved and envelope grids (for the latter see env_ref). A Raman response whose dephasing times depend on the density
  * (luna_resp_desc.tau2_rho) has its spectrum rebuilt at ρ(z) before every evaluation (one
  * extra transform of the 2*No response grid); its rebuild buffer is per plan for the RHS
  * entry points and per instance in a batch. */
@@ -216,7 +216,7 @@ typedef struct {
     const double* gam;           /* [Nw] γ(ω): Sellmeier susceptibility per unit density    */
     const double* vn;            /* [2*Nw] cladding term get_vn(εcl(ω)) (Capillary.jl:88-93) */
     const double* wc;            /* [Nw] ω/c on sidx, 0 elsewhere                           */
-    const double* om;            /* [Nw] ω                                                  */
+    const double* om;            /* [Nw] ω (ω - ω0 on an envelope grid)                     */
     const double* imcap;         /* [Nw] 3000 c/ω: conj_clamp's bound on Im neff            */
     const double* ofs;           /* [2*Nw] crop scale x pre*ωwin on sidx (times
                                     sqrt(Aeff(z))/β(z) on the device), crop scale else;
@@ -225,6 +225,13 @@ typedef struct {
     double fd_gam[4];            /* γ(x)                                                    */
     double fd_vn[8];             /* vn(x), complex                                          */
     double fd_h12;               /* 12 h                                                    */
+    /* envelope grids (kind 1; om above holds ω - ω0): make_linop for EnvGrid
+     * (LinearOps.jl:363-388) adds + i β(ω0; z) without THG, β(ω0; z) = ω0/c Re neff(ω0; z)
+     * (the 1e-3 rule with more than one radius node) */
+    int env_ref;                 /* 1: take out β(ω0; z) (thg = false), 0: thg = true        */
+    double ref_xc;               /* ω0/c                                                    */
+    double ref_gam;              /* γ(ω0)                                                   */
+    double ref_vn[2];            /* vn(ω0), complex                                         */
 } luna_gradient_desc;
 /* Attach (or, with grad == NULL, remove) a pressure gradient and/or taper. Replaces building
  * the transform with densityfun/aeff/βfun! and the linop with make_linop (Luna.jl:115-151). */

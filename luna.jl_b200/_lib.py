@@ -80,7 +80,8 @@ class GradientDesc(ctypes.Structure):
                 ("in_base", c_double), ("eps0c2", c_double),
                 ("gam", PD), ("vn", PD), ("wc", PD), ("om", PD),
                 ("imcap", PD), ("ofs", PD), ("fd_xc", c_double * 4), ("fd_gam", c_double * 4),
-                ("fd_vn", c_double * 8), ("fd_h12", c_double)]
+                ("fd_vn", c_double * 8), ("fd_h12", c_double), ("env_ref", c_int),
+                ("ref_xc", c_double), ("ref_gam", c_double), ("ref_vn", c_double * 2)]
 
 
 class SolveOpts(ctypes.Structure):

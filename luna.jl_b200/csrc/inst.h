@@ -76,6 +76,10 @@ typedef struct {
     double fd_xc[4], fd_gam[4];
     double2 fd_vn[4];
     double fd_h12;
+    // envelope grid without THG: + i β(ω0; z), β from neff at ω0 (ω0/c, γ(ω0), vn(ω0))
+    int bref;
+    double ref_xc, ref_gam;
+    double2 ref_vn;
 } LunaGrad;
 
 typedef struct {

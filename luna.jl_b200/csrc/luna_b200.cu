@@ -376,7 +376,7 @@ rhs_kernel(LunaInst* inst, const double2* Ew, double2* nl, TwTab<Rl> tw, int sme
 // linop!(out, z) of a pressure-gradient plan and the output factor at z, on one CTA.
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
 grad_linop_kernel(LunaInst I, double z, double2* L, double2* of) {
-    __shared__ double bc[4];
+    __shared__ double bc[5];
     grad_fill_to(I, bc, z, true, L, of);
 }
 
@@ -1019,7 +1019,8 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
         }
         return LUNA_OK;
     }
-    if (p->proto.kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "plan_set_gradient: field-resolved grids only");
+    if (p->proto.kind == 1 && g->env_ref != 0 && g->env_ref != 1)
+        return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: env_ref must be 0 or 1");
     if (g->npts < 2 || g->npts > LUNA_GRAD_MAXPTS) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: npts out of range");
     if (g->two_point && g->npts != 2) return fail(LUNA_ERR_BAD_ARG, "plan_set_gradient: a two-point fill has npts == 2");
     for (int i = 0; i + 1 < g->npts; ++i)
@@ -1064,6 +1065,11 @@ int luna_b200_plan_set_gradient(luna_plan* p, const luna_gradient_desc* g) {
         h.fd_vn[j] = make_double2(g->fd_vn[2 * j], g->fd_vn[2 * j + 1]);
     }
     h.fd_h12 = g->fd_h12;
+    // envelope grids without THG: the reference propagation constant β(ω0; z) is taken out
+    h.bref = (p->proto.kind == 1) ? g->env_ref : 0;
+    h.ref_xc = g->ref_xc;
+    h.ref_gam = g->ref_gam;
+    h.ref_vn = make_double2(g->ref_vn[0], g->ref_vn[1]);
     const double* t;
     if (upload(p->allocs, g->gam, Nw, &h.gam) || upload(p->allocs, g->vn, 2 * Nw, &t)) return LUNA_ERR_CUDA;
     h.vn = (const double2*)t;

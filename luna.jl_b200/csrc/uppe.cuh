@@ -896,7 +896,8 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
     __syncthreads();
     cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, No, w.tw);  // E(t), split order
     const int P = buf_split<Rl>(w.main_alt, No);
-    const double sc = I.in_scale;
+    // field scale; a taper's at this node is in outz[Nw]
+    const double sc = I.grad ? I.outz[I.Nw].x : I.in_scale;
     int ir = -1;
     for (int i = 0; i < I.nresp; ++i)
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
@@ -940,7 +941,9 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
     for (int k = tid; k < N; k += T) {
         const int src = (k < h) ? k : (No - N + k);
         cpx<double> X = cvt<double>(Z[Swz<Rl>::f(src)]);
-        store(k, X * ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k));
+        // with a pressure gradient the factor at the current z (outz, plain loads)
+        store(k, X * (I.grad ? reinterpret_cast<const cpx<double>*>(I.outz)[k]
+                             : ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k)));
     }
     __syncthreads();
 }
@@ -1284,7 +1287,8 @@ __device__ __forceinline__ double grad_beta1(const LunaGrad* g, double rho, doub
 // The gradient/taper at z for the whole CTA: L(ω; z) into Lout (when wantL), the output
 // factor ρ(z) sqrt(Aeff(z)) ofs/β(z) (ρ(z) ofs off sidx) into oout[0..Nw-1] and
 // (field scale, Aeff) into oout[Nw]. One thread evaluates the scalars and passes them
-// through bc (4 doubles of shared memory).
+// through bc (5 doubles of shared memory). On an envelope grid `om` holds ω - ω0 and,
+// without THG, L gains + i β(ω0; z) (make_linop for EnvGrid, LinearOps.jl:363-388).
 __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double z, bool wantL, double2* Lout,
                                           double2* oout) {
     const LunaGrad* g = I.grad;
@@ -1297,10 +1301,17 @@ __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double 
         bc[1] = a;
         bc[2] = wantL ? grad_beta1(g, rho, a) : 0.0;
         bc[3] = ae;
+        double br = 0.0;
+        if (wantL && g->bref) {
+            // Modes.β(mode, ω0; z) = ω0/c Re neff(ω0; z), with the low-index rule of a taper
+            const double re = grad_neff(g->ref_gam, g->ref_xc, g->ref_vn, g->unm, a, rho, g->loss).x;
+            br = __dmul_rn(g->ref_xc, (g->nta > 1 && re < 1e-3) ? 1e-3 : re);
+        }
+        bc[4] = br;
         oout[I.Nw] = make_double2(g->in_base / sqrt(ae), ae);
     }
     __syncthreads();
-    const double rho = bc[0], a = bc[1], b1 = bc[2], sae = sqrt(bc[3]);
+    const double rho = bc[0], a = bc[1], b1 = bc[2], sae = sqrt(bc[3]), br = bc[4];
     const bool tapered = g->nta > 1;
     cpx<double>* Lz = reinterpret_cast<cpx<double>*>(Lout);
     cpx<double>* oz = reinterpret_cast<cpx<double>*>(oout);
@@ -1317,7 +1328,7 @@ __device__ __noinline__ void grad_fill_to(const LunaInst& I, double* bc, double 
             const double re = fmax(n.x, 1e-3);                       // conj_clamp
             const double im = fmin(fmax(n.y, 0.0), __ldg(g->imcap + i));
             const double X = __dsub_rn(__dmul_rn(wc, re), __dmul_rn(__ldg(g->om + i), b1));
-            Lz[i] = mk<double>(-__dmul_rn(wc, im), -X);
+            Lz[i] = mk<double>(-__dmul_rn(wc, im), g->bref ? __dadd_rn(-X, br) : -X);
         }
         // β(z) = ω/c Re neff, with the low-index rule of neff(m, ω; z) for a taper
         const double nb = (tapered && n.x < 1e-3) ? 1e-3 : n.x;

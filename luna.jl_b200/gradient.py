@@ -180,20 +180,39 @@ def conj_clamp(n, ω):
     return np.clip(np.real(n), 1e-3, None) - 1j * np.clip(np.imag(n), 0, 3000 * pd.c / ω)
 
 
-def make_linop(grid, mode, λ0):
-    """(linop(z), βfun(z)) for a field-resolved grid (LinearOps.jl:330-360):
-    L = -i(ω/c conj_clamp(neff) - ω β1(z)) on sidx, written out in real arithmetic
-    (Re L = -ω/c Im nc, Im L = -(ω/c Re nc - ω β1)), as the device evaluates it."""
+def _om(grid):
+    """The frequency factor of the group-delay term: ω, or ω - ω0 on an envelope grid."""
+    return grid.ω - grid.ω0 if grid.kind == "env" else grid.ω
+
+
+def make_linop(grid, mode, λ0, thg=False):
+    """(linop(z), βfun(z)) (LinearOps.jl:330-388): on a field-resolved grid
+    L = -i(ω/c conj_clamp(neff) - ω β1(z)), on an envelope grid
+    L = -i(ω/c conj_clamp(neff) - (ω - ω0) β1(z)) + i β(ω0; z) (the last term without THG),
+    on sidx, written out in real arithmetic (Re L = -ω/c Im nc,
+    Im L = -(ω/c Re nc - ω' β1) [+ β(ω0; z)]), as the device evaluates it."""
     ω0 = pd.wlfreq(λ0)
     s = grid.sidx
     ω = grid.ω[s]
+    om = _om(grid)[s]
     wc = ω / pd.c
     cap = 3000 * pd.c / ω
     gam = mode.grad.gamma(ω)
     vn = mode.vn(ω)
+    env_ref = grid.kind == "env" and not thg
 
     def parts(z):
         return mode.neff_parts(gam, wc, vn, mode.grad.density(z), mode.radius(z))
+
+    def βref(z):
+        """Modes.β(mode, ω0; z) = ω0/c Re neff(ω0; z), the 1e-3 rule for a taper."""
+        x = np.array([ω0])
+        re, _ = mode.neff_parts(mode.grad.gamma(x), x / pd.c, mode.vn(x), mode.grad.density(z),
+                                mode.radius(z))
+        re = float(re[0])
+        if mode.tapered and re < 1e-3:
+            re = 1e-3
+        return ω0 / pd.c * re
 
     def linop(z):
         out = np.zeros(len(grid.ω), dtype=np.complex128)
@@ -202,7 +221,9 @@ def make_linop(grid, mode, λ0):
         re = np.maximum(re, 1e-3)                   # conj_clamp (LinearOps.jl:254)
         im = np.minimum(np.maximum(im, 0.0), cap)
         out.real[s] = -(wc * im)
-        out.imag[s] = -(wc * re - ω * β1)
+        out.imag[s] = -(wc * re - om * β1)
+        if env_ref:                                 # out -= -im*βref (LinearOps.jl:380-382)
+            out.imag[s] = out.imag[s] + βref(z)
         return out
 
     def βfun(z):
@@ -222,12 +243,12 @@ class TransModeAvgZ(TransModeAvg):
 
     kind = "modeavg_z"
 
-    def __init__(self, grid, resp, grad, mode, λ0, shock=True):
-        self.grad, self.mode, self.λ0 = grad, mode, λ0
+    def __init__(self, grid, resp, grad, mode, λ0, shock=True, thg=False):
+        self.grad, self.mode, self.λ0, self.thg = grad, mode, λ0, thg
         ω = grid.ω
         shockterm = ω ** 2 if shock else ω * pd.wlfreq(grid.referenceλ)
         self.pre = -1j * shockterm / 4 / nlscale / pd.c
-        _, self.βfun = make_linop(grid, mode, λ0)
+        _, self.βfun = make_linop(grid, mode, λ0, thg=thg)
         super().__init__(grid, resp, grad.density(0.0), None, mode.Aeff_z(0.0))
 
     def densityfun(self, z):
@@ -271,7 +292,7 @@ def gradient_desc(t, crop, pad_No, keep):
     cap[s] = 3000 * pd.c / ω[s]
     ofs = np.full(len(ω), crop, dtype=np.complex128)
     ofs[s] = crop * (t.pre[s] * grid.ωwin[s])
-    om = np.ascontiguousarray(ω, dtype=np.float64)
+    om = np.ascontiguousarray(_om(grid), dtype=np.float64)
     arrs = [np.ascontiguousarray(a) for a in (gam, vn, wc, om, cap, ofs)]
     keep += arrs
     d = _lib.GradientDesc()
@@ -291,4 +312,12 @@ def gradient_desc(t, crop, pad_No, keep):
         d.fd_xc[j], d.fd_gam[j] = xc[j], fg[j]
         d.fd_vn[2 * j], d.fd_vn[2 * j + 1] = fv[j].real, fv[j].imag
     d.fd_h12 = h12
+    if grid.kind == "env":
+        ω0 = pd.wlfreq(t.λ0)
+        x = np.array([ω0])
+        d.env_ref = int(not getattr(t, "thg", False))
+        d.ref_xc = ω0 / pd.c
+        d.ref_gam = float(grad.gamma(x)[0])
+        v = complex(mode.vn(x)[0])
+        d.ref_vn[0], d.ref_vn[1] = v.real, v.imag
     return d

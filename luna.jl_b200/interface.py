@@ -15,7 +15,7 @@ import numpy as np
 from . import fields, ionisation, modes, physdata as pd, raman
 from .grid import EnvGrid, RealGrid
 from .linops import make_const_linop
-from .nonlinear import (Kerr_env, Kerr_field, Kerr_field_nothg, PlasmaCumtrapz, RamanPolarEnv,
+from .nonlinear import (Kerr_env, Kerr_env_thg, Kerr_field, Kerr_field_nothg, PlasmaCumtrapz, RamanPolarEnv,
                         RamanPolarField, ionrate_fun_ADK)
 from .nonlinearrhs import TransModeAvg, norm_mode_average, norm_mode_average_gnlse
 
@@ -133,13 +133,17 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     from . import modes
     if shotnoise:
         raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
-    if envelope:
-        raise NotImplementedError("envelope capillary propagation is not supported")
     plasma = (not envelope) if plasma is None else plasma
     thg = (not envelope) if thg is None else thg
-    grid = RealGrid(flength, λ0, λlims, trange, δt)
+    if envelope and plasma:  # makeresponse for EnvGrid (Interface.jl:593-594)
+        raise ValueError("Plasma response for envelope fields has not been implemented yet.")
+    # makegrid (Interface.jl:453-461)
+    grid = EnvGrid(flength, λ0, λlims, trange, δt=δt, thg=thg) if envelope else \
+        RealGrid(flength, λ0, λlims, trange, δt)
     if not isinstance(modes_, str) or parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
         if isinstance(modes_, (int, tuple, list)):
+            if envelope:
+                raise NotImplementedError("multimode envelope propagation is not supported")
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
@@ -168,7 +172,11 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                                    T=temperature, model=model, loss=loss)
         density = pd.density(gas, pressure, temperature)
     resp = []
-    if kerr:
+    if kerr and envelope:
+        # makeresponse for EnvGrid (Interface.jl:593-605)
+        resp.append(Kerr_env_thg(pd.gamma3_gas(gas), pd.wlfreq(grid.referenceλ), grid.to) if thg else
+                    Kerr_env(pd.gamma3_gas(gas)))
+    elif kerr:
         # Interface.jl:534-541: without THG the Kerr term uses the analytic signal
         resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
                     Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
@@ -183,16 +191,16 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
         rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
-        resp.append(RamanPolarField(grid.to, rr, thg=thg))
+        resp.append(RamanPolarEnv(grid.to, rr) if envelope else RamanPolarField(grid.to, rr, thg=thg))
     if grad is not None:
         # z-dependent linear operator and normalisation (LinearOps.make_linop,
-        # LinearOps.jl:337-360; norm_mode_average with βfun!(β, z))
+        # LinearOps.jl:337-388; norm_mode_average with βfun!(β, z))
         from .gradient import TransModeAvgZ, make_linop
-        linop, _ = make_linop(grid, mode, λ0)
-        transform = TransModeAvgZ(grid, resp, grad, mode, λ0)
+        linop, _ = make_linop(grid, mode, λ0, thg=thg)
+        transform = TransModeAvgZ(grid, resp, grad, mode, λ0, thg=thg)
     else:
         aeff = mode.Aeff()
-        linop, βconst, β1 = make_const_linop(grid, mode, λ0)
+        linop, βconst, β1 = make_const_linop(grid, mode, λ0, thg=thg)
         norm = norm_mode_average(grid, βconst)
         transform = TransModeAvg(grid, resp, density, norm, aeff)
     if pulseshape == "gauss":

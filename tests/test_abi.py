@@ -95,7 +95,8 @@ int main(void) {
     P(luna_gradient_desc, loss); P(luna_gradient_desc, gam); P(luna_gradient_desc, ofs);
     P(luna_gradient_desc, fd_xc); P(luna_gradient_desc, fd_vn); P(luna_gradient_desc, fd_h12);
     P(luna_gradient_desc, nta); P(luna_gradient_desc, ZA); P(luna_gradient_desc, eps0c2);
-    P(luna_gradient_desc, vn);
+    P(luna_gradient_desc, vn); P(luna_gradient_desc, env_ref); P(luna_gradient_desc, ref_xc);
+    P(luna_gradient_desc, ref_gam); P(luna_gradient_desc, ref_vn);
     printf("luna_modal_desc %zu\n", sizeof(luna_modal_desc));
     P(luna_modal_desc, ems); P(luna_modal_desc, wts); P(luna_modal_desc, wlow);
     P(luna_modal_desc, rtol); P(luna_modal_desc, atol); P(luna_modal_desc, outfac);
@@ -138,7 +139,7 @@ def test_struct_layout_matches_ctypes(tmp_path):
     assert int(out["luna_solve_stats.dz"]) == _lib.SolveStats.dz.offset
     assert int(out["luna_gradient_desc"]) == ctypes.sizeof(_lib.GradientDesc)
     for f in ("Z", "P2", "dens_b", "loss", "gam", "ofs", "fd_xc", "fd_vn", "fd_h12", "nta", "ZA",
-              "eps0c2", "vn"):
+              "eps0c2", "vn", "env_ref", "ref_xc", "ref_gam", "ref_vn"):
         assert int(out[f"luna_gradient_desc.{f}"]) == getattr(_lib.GradientDesc, f).offset
     assert int(out["luna_modal_desc"]) == ctypes.sizeof(_lib.ModalDesc)
     for f in ("ems", "wts", "wlow", "rtol", "atol", "outfac"):

@@ -37,9 +37,9 @@ def gnlse(raman=True, zmax=0.15):
 
 
 def capillary(gas="He", plasma=None, zmax=0.3, trange=0.25e-12, energy=120e-6, radius=125e-6,
-              pressure=1.0, τ=10e-15):
+              pressure=1.0, τ=10e-15, **kw):
     return prop_capillary_args(radius, zmax, gas, pressure, λ0=800e-9, τfwhm=τ, energy=energy,
-                               λlims=(150e-9, 4e-6), trange=trange, plasma=plasma)
+                               λlims=(150e-9, 4e-6), trange=trange, plasma=plasma, **kw)
 
 
 CASES = {
@@ -49,6 +49,11 @@ CASES = {
     "real_kerr_ppt": lambda: capillary(),
     "real_kerr_adk_raman_H2": lambda: capillary("H2", energy=100e-6, radius=100e-6, pressure=2.0, τ=15e-15),
     "real_kerr_ppt_1ps": lambda: capillary(trange=1e-12),
+    # prop_capillary(envelope=true): Kerr_env, Kerr_env_thg on the THG grid, RamanPolarEnv
+    "env_capillary_Ar": lambda: capillary("Ar", trange=0.5e-12, envelope=True),
+    "env_capillary_He_thg": lambda: capillary(trange=0.5e-12, envelope=True, thg=True),
+    "env_capillary_H2_raman": lambda: capillary("H2", energy=100e-6, radius=100e-6, pressure=2.0,
+                                                τ=15e-15, trange=0.5e-12, envelope=True),
 }
 
 
@@ -121,6 +126,7 @@ SOLVE_CASES = {
     "gnlse_1.5cm": (lambda: gnlse(), 0.015, 1e-4),
     "capillary_He_ppt_5cm": (lambda: capillary(), 0.05, 1e-3),
     "capillary_H2_adk_raman_3cm": (CASES["real_kerr_adk_raman_H2"], 0.03, 1e-3),
+    "env_capillary_H2_raman_3cm": (CASES["env_capillary_H2_raman"], 0.03, 1e-3),
 }
 
 

@@ -89,6 +89,51 @@ def test_gradient_linop_tracks_local_pressure():
         assert _rel(p.linop(z), linc) < 1e-12, (z, _rel(p.linop(z), linc))
 
 
+@pytest.mark.parametrize("thg", [False, True])
+def test_envelope_equal_pressure_linop_matches_constant(thg):
+    """make_linop for an EnvGrid (LinearOps.jl:363-388) at equal pressures is the constant
+    envelope operator make_const_linop(grid::EnvGrid, mode, λ0; thg) (LinearOps.jl:266-300):
+    -i(β - β1 (ω - ω0) - β(ω0)) without THG, -i(β - β1 (ω - ω0)) with it."""
+    p = prop_capillary_args(125e-6, 0.5, "Ar", 1.0, λ0=800e-9, τfwhm=10e-15, energy=50e-6,
+                            λlims=(200e-9, 2000e-9), trange=0.5e-12, envelope=True, thg=thg)
+    c = p.grid
+    assert c.kind == "env" and [r.kind for r in p.transform.resp] == (["kerr_env_thg"] if thg else ["kerr_env"])
+    g = Gradient("Ar", 0.5, 1.0, 1.0)
+    m = MarcatiliGradientMode(125e-6, g)
+    lin, _ = make_linop(c, m, 800e-9, thg=thg)
+    for z in (0.0, 0.2, 0.5):
+        assert _rel(lin(z), p.linop) < 1e-13, (z, _rel(lin(z), p.linop))
+
+
+def test_envelope_capillary_set_up_follows_the_interface():
+    """prop_capillary(envelope=true) (Interface.jl:360-401, 453-461, 593-605): an EnvGrid
+    without THG by default, Kerr_env, RamanPolarEnv for the molecular gases, and no plasma
+    response for envelopes."""
+    kw = dict(λ0=800e-9, τfwhm=10e-15, energy=50e-6, λlims=(200e-9, 2000e-9), trange=0.5e-12)
+    p = prop_capillary_args(125e-6, 0.5, "H2", (2.0, 0.5), envelope=True, **kw)
+    assert p.grid.kind == "env" and [r.kind for r in p.transform.resp] == ["kerr_env", "raman_env"]
+    with pytest.raises(ValueError):
+        prop_capillary_args(125e-6, 0.5, "Ar", 1.0, envelope=True, plasma=True, **kw)
+    # the envelope and field-resolved set-ups carry the same pulse energy
+    pe = prop_capillary_args(125e-6, 0.5, "Ar", 1.0, envelope=True, **kw)
+    from luna_b200.fields import energy_t
+    Et = np.fft.ifft(pe.Eω)
+    assert abs(energy_t(pe.grid, Et) / 50e-6 - 1) < 1e-6
+
+
+def test_envelope_equal_pressure_gradient_propagation_matches_constant():
+    """test_gradient.jl's equal-pressure check on an envelope grid (oracle, FP64)."""
+    kw = dict(λ0=800e-9, τfwhm=30e-15, energy=1e-6, λlims=(160e-9, 3000e-9), trange=1e-12,
+              envelope=True, loss=False, saveN=11)
+    c = prop_capillary_args(13e-6, 2e-2, "Ar", 5.0, **kw)
+    rc = uppe.run(c.transform, c.grid, c.linop, c.Eω, saveN=11)
+    p = prop_capillary_args(13e-6, 2e-2, "Ar", (5.0, 5.0), **kw)
+    r = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=11)
+    assert r.steps == rc.steps
+    for a, b in zip(r.Eω, rc.Eω):
+        assert _rel(a, b) < 1e-12
+
+
 def _field_case(pressure):
     return prop_capillary_args(13e-6, 5e-2, "Ar", pressure, λ0=800e-9, τfwhm=30e-15,
                                energy=1e-6, λlims=(160e-9, 3000e-9), trange=0.5e-12,
@@ -214,6 +259,14 @@ _CASES = {
     "N2-rising": dict(radius=100e-6, flength=0.2, gas="N2", pressure=(0.3, 2.0), λ0=800e-9,
                       τfwhm=20e-15, energy=40e-6, λlims=(200e-9, 4e-6), trange=0.5e-12,
                       plasma=False),
+    # envelope grids: gradients/gradient_modeAvg_env.jl (Ar 7.5 bar to vacuum over 15 cm in a
+    # 13 µm core, Kerr_env, no loss), and H2 with its Raman response (RamanPolarEnv)
+    "Ar-env-falling": dict(radius=13e-6, flength=0.15, gas="Ar", pressure=(7.5, 0.0), λ0=800e-9,
+                           τfwhm=30e-15, energy=1e-6, λlims=(160e-9, 3000e-9), trange=1e-12,
+                           envelope=True, loss=False),
+    "H2-env-raman": dict(radius=125e-6, flength=0.3, gas="H2", pressure=(3.0, 0.5), λ0=800e-9,
+                         τfwhm=10e-15, energy=60e-6, λlims=(150e-9, 4e-6), trange=0.5e-12,
+                         envelope=True),
 }
 
 
@@ -249,7 +302,7 @@ def test_device_linop_is_bit_identical_to_host(name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "He-taper-gradient", "H2-falling",
-                                  "N2-rising"])
+                                  "N2-rising", "Ar-env-falling", "H2-env-raman"])
 def test_gradient_rhs_matches_oracle(name):
     """(t::TransModeAvg)(nl, Eω, z) with densityfun(z) and βfun!(β, z) through the C ABI."""
     p = _case(name)

@@ -362,7 +362,10 @@ typedef struct luna_modal_plan luna_modal_plan;
 
 /* Replaces the TransModal constructor (NonlinearRHS.jl:203-216). The grid descriptor is
  * that of one point (kind 0; its outfac is ignored, in_scale = pad scale / No); responses
- * as for luna_b200_plan_create (no Raman; with npol = 2 only Kerr). */
+ * as for luna_b200_plan_create without the no-THG forms: with npol = 1 Kerr, plasma and
+ * Raman (scalar RamanPolar on the modal field, Nonlinear.jl:284-290); with npol = 2 Kerr
+ * (KerrVector!) and plasma (PlasmaVector!, Nonlinear.jl:144-162; vector Raman is not
+ * implemented in the reference either). */
 int luna_b200_modal_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
                                 const luna_modal_desc* modal, int precision, luna_modal_plan** out);
 void luna_b200_modal_plan_destroy(luna_modal_plan* plan);

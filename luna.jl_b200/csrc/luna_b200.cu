@@ -1955,6 +1955,8 @@ struct luna_modal_plan {
     void* B = nullptr;   // [Nw*Nr] integrated transform of the last level
     void* Et = nullptr;  // [Nr*No/2] field samples per mode
     void* G = nullptr;   // [nslots*Nr*No/2] projected polarisation per node
+    double* vscr = nullptr;  // two components with plasma: [6*No] doubles per node CTA
+    bool vplasma = false;
     ModalState* ms = nullptr;
     int* d_flags = nullptr;
     double2* d_Ew = nullptr;
@@ -1997,6 +1999,8 @@ int modal_xform(luna_modal_plan* p, const TwTab<Rl>& tw, RadState* st, int* flag
         const int nn = (l == 0) ? 1 : (1 << l);
         if (p->npol == 1)
             modal_node_kernel<Rl><<<nn, LUNA_BLOCK, p->smem, s>>>(p->d_col, a, s0, tw, p->smem, p->gscr, p->gstride, flags);
+        else if (p->vplasma)
+            modal_vec_kernel<Rl><<<nn, LUNA_BLOCK, 0, s>>>(p->d_col, a, s0, p->vscr, flags);
         else
             modal_kerr2_kernel<Rl><<<dim3(nn, std::max(1, p->nchunk / nn)), 256, 0, s>>>(p->d_col, a, s0);
         modal_level_kernel<Rl><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(p->d_col, a, l, (cpx<Rl>*)p->B, tw, p->smem, p->gscr,
@@ -2024,6 +2028,9 @@ int modal_setup(luna_modal_plan* p) {
     p->nchunk = std::max(1, std::min(M / 256, 4 * 148));
     if (dalloc(p->allocs, &p->Et, sizeof(cpx<Rl>) * (size_t)p->Nr * M) ||
         dalloc(p->allocs, &p->G, sizeof(cpx<Rl>) * (size_t)p->nslots * p->Nr * M))
+        return LUNA_ERR_CUDA;
+    // the largest level has 2^(nlevels - 1) new nodes, one CTA each
+    if (p->vplasma && dalloc(p->allocs, &p->vscr, sizeof(double) * 6 * (size_t)I.No * ((size_t)1 << (p->nlevels - 1))))
         return LUNA_ERR_CUDA;
     CK(cudaFuncSetAttribute(modal_time_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
     CK(cudaFuncSetAttribute(modal_node_kernel<Rl>, cudaFuncAttributeMaxDynamicSharedMemorySize, maxs));
@@ -2067,14 +2074,22 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
     if (precision != LUNA_PREC_FP64 && precision != LUNA_PREC_MIXED)
         return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: unknown precision");
     double kerr = 0;
+    bool vplasma = false;
     for (int i = 0; i < nresp; ++i) {
-        if (resps[i].kind == LUNA_RESP_RAMAN || resps[i].kind == LUNA_RESP_RAMAN_NOTHG)
-            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: Raman response not available for the modal transform");
-        if (resps[i].kind == LUNA_RESP_KERR_FIELD_NOTHG)
-            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: Kerr_field_nothg not available for the modal transform");
-        if (md->npol == 2 && resps[i].kind != LUNA_RESP_KERR_FIELD)
-            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support the Kerr response only");
-        if (resps[i].kind == LUNA_RESP_KERR_FIELD) kerr += resps[i].coef;
+        const int k = resps[i].kind;
+        // RamanPolar on a modal field: the scalar case only (Nonlinear.jl:284-293, "vector
+        // Raman not yet implemented"); the analytic-signal forms are not available here
+        if (k == LUNA_RESP_RAMAN_NOTHG || k == LUNA_RESP_KERR_FIELD_NOTHG)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: the no-THG response forms are not available for the modal transform");
+        if (md->npol == 2 && k == LUNA_RESP_RAMAN)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: vector Raman is not implemented (as in the reference)");
+        if (md->npol == 2 && k != LUNA_RESP_KERR_FIELD && k != LUNA_RESP_PLASMA_PPT && k != LUNA_RESP_PLASMA_ADK)
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support Kerr and plasma");
+        if (md->npol == 2 && (k == LUNA_RESP_PLASMA_PPT || k == LUNA_RESP_PLASMA_ADK)) {
+            if (vplasma) return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: at most one plasma response");
+            vplasma = true;
+        }
+        if (k == LUNA_RESP_KERR_FIELD) kerr += resps[i].coef;
     }
     // the point plan: grid and responses; its output factor is unused (the modal one is
     // applied after the cubature)
@@ -2096,6 +2111,7 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
     p->rtol = md->rtol;
     p->atol = md->atol;
     p->kerr = kerr;
+    p->vplasma = vplasma;
     p->col = col;
     auto bail = [&](int code) {
         free_all(p->allocs);

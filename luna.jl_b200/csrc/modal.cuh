@@ -162,6 +162,153 @@ __global__ void __launch_bounds__(256) modal_kerr2_kernel(const LunaInst* inst, 
     }
 }
 
+// Exclusive prefix of v over the CTA's threads (thread order) and the total; sh holds
+// LUNA_WARPS doubles.
+__device__ __forceinline__ double cta_exscan(double v, double* sh, double& total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    double x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        double t = (lane < LUNA_WARPS) ? sh[lane] : 0.0;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, t, o);
+            if (lane >= o) t += y;
+        }
+        if (lane < LUNA_WARPS) sh[lane] = t;
+    }
+    __syncthreads();
+    const double base = wid ? sh[wid - 1] : 0.0;
+    total = sh[LUNA_WARPS - 1];
+    __syncthreads();
+    return base + x - v;
+}
+
+// Maths.cumtrapz! (Maths.jl:323-328) of v[0..n) on one CTA, written as the prefix sum
+// out[j] = dt (S_j - (v_0 + v_j)/2), S_j = v_0 + ... + v_j, each thread a contiguous run.
+__device__ __forceinline__ void cta_cumtrapz(const double* v, double* out, int n, double dt, double* sh) {
+    const int C = (n + LUNA_BLOCK - 1) / LUNA_BLOCK;
+    const int b = threadIdx.x * C, e = min(n, b + C);
+    const double v0 = v[0];  // read before the scan's barriers: out may alias v
+    double s = 0;
+    for (int j = b; j < e; ++j) s += v[j];
+    double tot;
+    double pre = cta_exscan(s, sh, tot);
+    for (int j = b; j < e; ++j) {
+        pre += v[j];
+        out[j] = dt * (pre - 0.5 * (v0 + v[j]));
+    }
+    __syncthreads();
+}
+
+// Two polarisation components with the plasma response (PlasmaVector!, Nonlinear.jl:144-162)
+// and vector Kerr (KerrVector!, Nonlinear.jl:12-21): one CTA per new node. The node's field
+// (Ex, Ey) in natural time order, the rate of |E| = hypot(Ex, Ey) and the ionisation fraction,
+// the phase integrands and currents of both components, their cumulative integrals, then
+// the polarisation times the time window projected on each mode's field at the node.
+// Scratch: 6 No doubles per CTA in global memory (vs).
+template <typename Rl>
+__global__ void __launch_bounds__(LUNA_BLOCK, 1)
+modal_vec_kernel(const LunaInst* inst, ModalArgs a, int slot0, double* vscr, int* flags) {
+    __shared__ double sh[LUNA_WARPS];
+    __shared__ int flag;
+    if (modal_skip(a)) return;
+    const LunaInst& I = *inst;
+    const int slot = slot0 + blockIdx.x;
+    const int M = I.No / 2, No = I.No, nm = a.nmodes, P = a.P, Lb = M / P;
+    const int tid = threadIdx.x;
+    if (tid == 0) flag = 0;
+    int ip = -1;
+    for (int i = 0; i < I.nresp; ++i)
+        if (I.resp[i].kind == LUNA_RESP_PLASMA_PPT || I.resp[i].kind == LUNA_RESP_PLASMA_ADK) ip = i;
+    const LunaResp& r = I.resp[ip];
+    const double* e = a.ems + (size_t)slot * nm * 2;
+    const cpx<Rl>* Et = reinterpret_cast<const cpx<Rl>*>(a.Et);
+    cpx<Rl>* G = reinterpret_cast<cpx<Rl>*>(a.G) + (size_t)slot * nm * M;
+    double* ex = vscr + (size_t)blockIdx.x * 6 * No;
+    double* ey = ex + No;
+    double* rt = ey + No;   // rate, then Px
+    double* fr = rt + No;   // cumulative rate, the fraction, then Py
+    double* jx = fr + No;   // phase integrand and current, x
+    double* jy = jx + No;   // phase integrand and current, y
+    const double sc = I.in_scale, kc = a.kerr, dt = r.dt;
+    __syncthreads();
+    // the node's field in natural order (buffer slot i holds the sample pair n)
+    for (int i = tid; i < M; i += LUNA_BLOCK) {
+        const int sp = Swz<Rl>::f(i);
+        const int n = (sp % Lb) * P + sp / Lb;
+        double x0 = 0, y0 = 0, x1 = 0, y1 = 0;
+        for (int m = 0; m < nm; ++m) {
+            const cpx<Rl> v = Et[(size_t)m * M + i];
+            const double fx = e[2 * m], fy = e[2 * m + 1];
+            x0 += fx * (double)v.x;
+            y0 += fy * (double)v.x;
+            x1 += fx * (double)v.y;
+            y1 += fy * (double)v.y;
+        }
+        ex[2 * n] = x0 * sc;
+        ey[2 * n] = y0 * sc;
+        ex[2 * n + 1] = x1 * sc;
+        ey[2 * n + 1] = y1 * sc;
+    }
+    __syncthreads();
+    for (int j = tid; j < No; j += LUNA_BLOCK) {
+        const double Em = hypot(ex[j], ey[j]);
+        rt[j] = (r.kind == LUNA_RESP_PLASMA_PPT) ? ppt_rate<double>(r, Em, &flag) : adk_rate<double>(r, Em);
+    }
+    __syncthreads();
+    cta_cumtrapz(rt, fr, No, dt, sh);
+    for (int j = tid; j < No; j += LUNA_BLOCK) {
+        const double f = r.preion + 1.0 - exp(-fr[j]);
+        fr[j] = f;
+        jx[j] = f * r.eratio * ex[j];
+        jy[j] = f * r.eratio * ey[j];
+    }
+    __syncthreads();
+    // J = cumtrapz(phase) + ionpot rate (1 - fraction)/|E|^2 E per component, in place
+    cta_cumtrapz(jx, jx, No, dt, sh);
+    cta_cumtrapz(jy, jy, No, dt, sh);
+    for (int j = tid; j < No; j += LUNA_BLOCK) {
+        const double Em = hypot(ex[j], ey[j]);
+        const double f = fr[j];
+        if (fabs(Em) > 0) {
+            const double pre = r.ionpot * rt[j] * (1.0 - f) / (Em * Em);
+            jx[j] += pre * ex[j];
+            jy[j] += pre * ey[j];
+        }
+    }
+    __syncthreads();
+    cta_cumtrapz(jx, rt, No, dt, sh);  // Px (the rates are no longer needed)
+    cta_cumtrapz(jy, fr, No, dt, sh);  // Py
+    const double coef = r.coef;
+    for (int i = tid; i < M; i += LUNA_BLOCK) {
+        const int sp = Swz<Rl>::f(i);
+        const int n = (sp % Lb) * P + sp / Lb;
+        double pxy[2][2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = 2 * n + h;
+            const double Ex = ex[j], Ey = ey[j];
+            const double fk = kc * (Ex * Ex + Ey * Ey);
+            const double tw = __ldg(I.towin + j);
+            pxy[h][0] = (fk * Ex + coef * rt[j]) * tw;
+            pxy[h][1] = (fk * Ey + coef * fr[j]) * tw;
+        }
+        for (int m = 0; m < nm; ++m) {
+            const double fx = e[2 * m], fy = e[2 * m + 1];
+            G[(size_t)m * M + i] = mk<Rl>((Rl)(fx * pxy[0][0] + fy * pxy[0][1]), (Rl)(fx * pxy[1][0] + fy * pxy[1][1]));
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && flag && flags) atomicOr(flags, flag);
+}
+
 // Level l of the rule for mode c: X_l = rfft(sum_s W[l][s] g_s,c) into B (level 0 first
 // puts the midpoint rule there), the two L2 sums against the previous level, and the
 // convergence decision by the last CTA to finish (Cubature's L2 error norm).

@@ -4,8 +4,10 @@ Cases follow test/test_multimode.jl: argon in a 13 µm capillary with HE11 alone
 "Radial"), TM01 + HE21 on both polarisation components (Kerr; ϕ = 0 puts HE21 on y and TM01
 on x along θ = 0, where the radial integral samples the cross-section, so the vector Kerr
 term couples them; with the LP11 phase ϕ = -π/4 of "Full, LP11 vs TM01" and equal energies
-the two cancel there), and HE11 + HE12 in a 50 µm capillary with Kerr + PPT plasma at
-20 µJ (the plasma term is comparable to Kerr and the cubature needs 129 points).
+the two cancel there), HE11 + HE12 in a 50 µm capillary with Kerr + PPT plasma at
+20 µJ (the plasma term is comparable to Kerr and the cubature needs 129 points), TM01 + HE21
+with the vector plasma response (PlasmaVector!) at 3 µJ (23 % of the response), and HE11 + HE12 in H2 with the
+scalar Raman response.
 """
 import math
 
@@ -16,11 +18,11 @@ luna_b200_loader.load()
 import numpy as np
 import pytest
 
-from luna_b200 import _lib, fields, ionisation, modal, modal_plan, modes
+from luna_b200 import _lib, fields, ionisation, modal, modal_plan, modes, raman
 from luna_b200 import physdata as pd
 from luna_b200.grid import RealGrid
 from luna_b200.linops import make_const_linop
-from luna_b200.nonlinear import Kerr_field, PlasmaCumtrapz
+from luna_b200.nonlinear import Kerr_field, Kerr_field_nothg, PlasmaCumtrapz, RamanPolarField
 from luna_b200.nonlinearrhs import TransModeAvg, norm_mode_average
 from luna_b200.plan import solve_precon
 from oracle import uppe
@@ -46,6 +48,18 @@ def _case(name, flength=1e-2):
         f1 = fields.GaussField(LAM0, 30e-15, energy=energy / 2)
         f2 = fields.GaussField(LAM0, 30e-15, energy=energy / 5)
         comps, inputs, plasma = "xy", ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)}), False
+    elif name == "vector_plasma":  # TM01 + HE21 with vector Kerr and PlasmaVector!
+        a, gas, pres, trange, energy = 13e-6, "Ar", 5.0, 0.4e-12, 3e-6
+        ms = (modes.MarcatiliMode(a, gas, pres, n=0, m=1, kind="TM", ϕ=0.0, loss=False),
+              modes.MarcatiliMode(a, gas, pres, n=2, m=1, kind="HE", ϕ=0.0, loss=False))
+        f1 = fields.GaussField(LAM0, 10e-15, energy=energy / 2)
+        f2 = fields.GaussField(LAM0, 10e-15, energy=energy / 5)
+        comps, inputs, plasma = "xy", ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)}), True
+    elif name == "raman":  # HE11 + HE12 in H2 with Kerr and the scalar Raman response
+        a, gas, pres, trange, energy = 50e-6, "H2", 2.0, 0.4e-12, 20e-6
+        ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, loss=False),
+              modes.MarcatiliMode(a, gas, pres, n=1, m=2, loss=False))
+        comps, inputs, plasma = "y", fields.GaussField(LAM0, 10e-15, energy=energy), False
     else:  # two HE modes with Kerr + PPT plasma
         a, gas, pres, trange, energy = 50e-6, "Ar", 1.0, 0.4e-12, 20e-6
         ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, loss=False),
@@ -56,13 +70,15 @@ def _case(name, flength=1e-2):
     if plasma:
         rate = ionisation.ionrate_PPTaccel(gas, LAM0, N=2 ** 12)
         resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, pd.ionisation_potential(gas)))
+    if name == "raman":
+        resp.append(RamanPolarField(grid.to, raman.raman_response(grid.to, gas)))
     Eω, t = modal.setup_modal(grid, pd.density(gas, pres), resp, inputs, ms, comps)
-    if name == "plasma":
+    if name in ("plasma", "raman"):
         Eω[:, 1] = 0.3 * Eω[:, 0]  # some energy in HE12 as well
     return grid, Eω, t, modal.make_const_linop_modes(grid, ms, LAM0)
 
 
-@pytest.mark.parametrize("name", ["he11", "vector", "plasma"])
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"])
 def test_modal_rhs_fp64_matches_oracle(name):
     """(t::TransModal)(nl, Eω, z) through the C ABI vs the oracle (NonlinearRHS.jl:284-302):
     the same number of cubature points and the integral within 1e-11. The device sums the
@@ -75,7 +91,7 @@ def test_modal_rhs_fp64_matches_oracle(name):
     t(nl, Ew, 0.0)
     ref = uppe.trans_modal(t, Ew, 0.0)
     assert t.plan().nevals == t.oracle_nevals
-    tol = 1e-11 if name == "plasma" else 1e-12
+    tol = 1e-11 if name in ("plasma", "vector_plasma", "raman") else 1e-12
     assert _rel(nl, ref) < tol, _rel(nl, ref)
     # the device-pointer entry point gives the same numbers
     torch = pytest.importorskip("torch")
@@ -92,7 +108,7 @@ def test_modal_rhs_fp64_matches_oracle(name):
     assert np.array_equal(dev, nl)
 
 
-@pytest.mark.parametrize("name", ["he11", "vector", "plasma"])
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"])
 def test_modal_rhs_mixed_close_to_oracle(name):
     grid, Eω, t, _ = _case(name)
     plan = modal_plan.ModalPlan.from_transform(t, _lib.PREC_MIXED)
@@ -102,7 +118,8 @@ def test_modal_rhs_mixed_close_to_oracle(name):
     assert _rel(nl, ref) < 1e-3, _rel(nl, ref)
 
 
-@pytest.mark.parametrize("name,flength", [("he11", 5e-3), ("vector", 2e-3), ("plasma", 1e-3)])
+@pytest.mark.parametrize("name,flength", [("he11", 5e-3), ("vector", 2e-3), ("plasma", 1e-3),
+                                          ("vector_plasma", 1e-3), ("raman", 1e-3)])
 def test_modal_solve_replay_matches_oracle(name, flength):
     """Following the oracle's step sequence (replay), every saved field within 1e-10."""
     grid, Eω, t, L = _case(name, flength)
@@ -142,10 +159,12 @@ def test_modal_matches_mode_average_on_gpu():
 
 
 def test_modal_plan_rejects_unsupported_responses():
+    """Vector Raman (an error in the reference too, Nonlinear.jl:288-292) and the no-THG
+    response forms are refused."""
     grid, Eω, t, _ = _case("vector")
-    rate = ionisation.ionrate_PPTaccel("Ar", LAM0, N=2 ** 10)
-    pl = PlasmaCumtrapz(grid.to, grid.to, rate, pd.ionisation_potential("Ar"))
-    t2 = modal.TransModal(grid, t.ts, (t.resp[0], pl), t.density, t.norm)
-    with pytest.raises(_lib.LunaError) as e:
-        t2.plan()
-    assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED
+    rr = RamanPolarField(grid.to, raman.raman_response(grid.to, "N2"))
+    for extra in (rr, Kerr_field_nothg(pd.gamma3_gas("Ar"), len(grid.to))):
+        t2 = modal.TransModal(grid, t.ts, (t.resp[0], extra), t.density, t.norm)
+        with pytest.raises(_lib.LunaError) as e:
+            t2.plan()
+        assert e.value.code == _lib.LUNA_ERR_UNSUPPORTED

@@ -314,6 +314,26 @@ typedef struct luna_radial_plan luna_radial_plan;
 int luna_b200_radial_plan_create(const luna_grid_desc* grid, const luna_resp_desc* resps, int nresp,
                                  const luna_radial_desc* radial, int precision, luna_radial_plan** out);
 void luna_b200_radial_plan_destroy(luna_radial_plan* plan);
+/* Attach (or, with grad == NULL, remove) a gas fill gradient: make_linop(grid, q, nfun)
+ * (LinearOps.jl:174-226) and norm_radial (NonlinearRHS.jl:494-524) with
+ * nfun(ω; z) = sqrt(1 + γ(ω) ρ(z)) and the densityfun(z) of TransRadial, ρ(z) the fill law
+ * of luna_gradient_desc (npts, two_point, Z, P, P2, dens_a, dens_b). Fields used: gam [Nw]
+ * γ(ω) on sidx, wc [Nw] ω/c on sidx (0 elsewhere), om [Nw] ω, ofs [2*Nw] crop scale x
+ * ωwin (-iω)/2, fd_xc/fd_gam/fd_h12 for β1(z) (the 4-point central difference of
+ * x/c n(x; z) at ω0, h = 1e-4 ω0), and on an envelope grid env_ref/ref_xc/ref_gam
+ * (+ i β(ω0; z) without THG); kr2 [Nr] the QDHT's k_r^2, mu0w [Nw] μ0 ω. Then, at every
+ * stage node, step end and save point:
+ *   k2 = ((n ω/c))^2 on sidx (as n x (ω/c)), βsq = k2 - k_r^2,
+ *   L = -i (sqrt(βsq) - β1 ω), or -i (-β1 ω) - min(sqrt|βsq|, 200) for βsq < 0,
+ *   output factor = ρ(z) ofs / normfun, normfun = sqrt(βsq)/(μ0 ω) (1 where ω = 0 or βsq <= 0),
+ * in IEEE-rounded operations in this order; the responses' coefficients are for ρ = 1 and
+ * the linop argument of luna_b200_radial_solve is ignored (may be NULL). A Raman response
+ * whose dephasing depends on the density is refused here. */
+int luna_b200_radial_set_gradient(luna_radial_plan* plan, const luna_gradient_desc* grad, const double* kr2,
+                                  const double* mu0w);
+/* linop!(out, z) and the output factor of a radial plan with a gas fill gradient, evaluated
+ * on the device as the solver does: host arrays of Nw*Nr complex (outfac may be NULL). */
+int luna_b200_radial_linop(luna_radial_plan* plan, double z, double* linop, double* outfac);
 /* (t::TransRadial)(nl, Eω, z) — NonlinearRHS.jl:466-474. Host arrays of Nw*Nr complex. */
 int luna_b200_radial_rhs(luna_radial_plan* plan, double* nl, const double* Ew, double z);
 int luna_b200_radial_rhs_device(luna_radial_plan* plan, double* nl_dev, const double* Ew_dev, double z,

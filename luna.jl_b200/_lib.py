@@ -109,7 +109,8 @@ EXPORTS = [
     "luna_b200_batch_info", "luna_b200_batch_stats", "luna_b200_plan_set_gradient",
     "luna_b200_plan_linop", "luna_b200_modal_plan_create", "luna_b200_modal_plan_destroy",
     "luna_b200_modal_rhs", "luna_b200_modal_rhs_device", "luna_b200_modal_solve",
-    "luna_b200_batch_set_replay", "luna_b200_batch_set_shapes",
+    "luna_b200_batch_set_replay", "luna_b200_batch_set_shapes", "luna_b200_radial_set_gradient",
+    "luna_b200_radial_linop",
 ]
 
 _lib = None
@@ -159,6 +160,8 @@ def load():
     lib.luna_b200_radial_rhs_device.argtypes = [c_void_p, c_void_p, c_void_p, c_double, c_void_p]
     lib.luna_b200_radial_solve.argtypes = [c_void_p, PD, PD, c_double, c_double, c_double,
                                            POINTER(SolveOpts), PD, PD, POINTER(SolveStats)]
+    lib.luna_b200_radial_set_gradient.argtypes = [c_void_p, POINTER(GradientDesc), PD, PD]
+    lib.luna_b200_radial_linop.argtypes = [c_void_p, c_double, PD, PD]
     lib.luna_b200_modal_plan_create.argtypes = [POINTER(GridDesc), POINTER(RespDesc), c_int,
                                                 POINTER(ModalDesc), c_int, POINTER(c_void_p)]
     lib.luna_b200_modal_plan_destroy.argtypes = [c_void_p]

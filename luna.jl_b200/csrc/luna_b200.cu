@@ -1583,6 +1583,10 @@ struct luna_radial_plan {
     double2* d_Ew = nullptr;
     double2* d_nl = nullptr;
     cudaStream_t stream = nullptr;
+    // gas fill gradient (luna_b200_radial_set_gradient): the fill law and tables, and the
+    // output factor at the current node
+    RadGrad grad{nullptr, nullptr, nullptr};
+    double2* ofz = nullptr;
 };
 
 namespace {
@@ -1651,13 +1655,18 @@ int rad_transform(luna_radial_plan* p, const TwTab<Rl>& tw, RadState* st, int* f
 }
 
 template <typename Rl>
-int rad_rhs(luna_radial_plan* p, const double2* Ew, double2* nl, cudaStream_t s) {
+int rad_rhs(luna_radial_plan* p, const double2* Ew, double2* nl, cudaStream_t s, double z) {
     TwDev tw;
     int rc = get_tw(tw);
     if (rc) return rc;
     const TwTab<Rl>& t = *reinterpret_cast<const TwTab<Rl>*>(std::is_same<Rl, double>::value ? (const void*)&tw.d : (const void*)&tw.f);
     RadArgs a{p->Nw, p->Nr, nullptr, p->outfac, nullptr, nullptr};
     const size_t n = (size_t)p->Nw * p->Nr;
+    if (p->grad.g) {
+        // densityfun(z) and normfun(z) of a gas fill gradient
+        rad_gradfill_kernel<<<rad_grid(n), 256, 0, s>>>(a, p->grad, -2, z, nullptr, p->ofz);
+        a.outfac = p->ofz;
+    }
     CK(cudaMemsetAsync(p->d_flags, 0, sizeof(int), s));
     rad_stage_kernel<Rl, double><<<rad_grid(n), 256, 0, s>>>(a, -1, Ew, (cpx<Rl>*)p->A);
     rad_transform<Rl>(p, t, nullptr, p->d_flags, s);
@@ -1747,8 +1756,82 @@ void luna_b200_radial_plan_destroy(luna_radial_plan* p) {
 int luna_b200_radial_rhs_device(luna_radial_plan* p, double* nl_dev, const double* Ew_dev, double z, void* stream) {
     (void)z;  // constant density and normalisation
     if (!p || !nl_dev || !Ew_dev) return fail(LUNA_ERR_BAD_ARG, "radial_rhs_device: null argument");
-    if (p->precision == LUNA_PREC_FP64) return rad_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
-    return rad_rhs<float>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream);
+    if (p->precision == LUNA_PREC_FP64) return rad_rhs<double>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream, z);
+    return rad_rhs<float>(p, (const double2*)Ew_dev, (double2*)nl_dev, (cudaStream_t)stream, z);
+}
+
+int luna_b200_radial_set_gradient(luna_radial_plan* p, const luna_gradient_desc* g, const double* kr2,
+                                  const double* mu0w) {
+    if (!p) return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: null plan");
+    if (!g) {
+        p->grad = RadGrad{nullptr, nullptr, nullptr};
+        return LUNA_OK;
+    }
+    const LunaInst& C = p->col->proto;
+    for (int i = 0; i < C.nresp; ++i)
+        if (C.resp[i].kind == LUNA_RESP_RAMAN && C.resp[i].t2rho)
+            return fail(LUNA_ERR_UNSUPPORTED, "radial_set_gradient: a Raman response whose dephasing depends on the "
+                                              "density is not available for the radial transform with a gradient");
+    if (g->npts < 2 || g->npts > LUNA_GRAD_MAXPTS) return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: npts out of range");
+    if (g->two_point && (g->npts != 2 || g->Z[0] != 0.0))
+        return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: a two-point fill has npts == 2 and starts at z = 0");
+    for (int i = 0; i + 1 < g->npts; ++i)
+        if (!(g->Z[i + 1] > g->Z[i])) return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: Z must increase");
+    for (int i = 0; i < g->npts; ++i)
+        if (!(g->P[i] >= 0) || g->P2[i] != g->P[i] * g->P[i])
+            return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: pressures must be >= 0 with P2 = P*P");
+    if (!g->gam || !g->wc || !g->om || !g->ofs || !kr2 || !mu0w || !(g->fd_h12 > 0))
+        return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: null table");
+    if (C.kind == 1 && g->env_ref != 0 && g->env_ref != 1)
+        return fail(LUNA_ERR_BAD_ARG, "radial_set_gradient: env_ref must be 0 or 1");
+    const size_t Nw = (size_t)p->Nw, Nr = (size_t)p->Nr;
+    LunaGrad h;
+    memset(&h, 0, sizeof(h));
+    h.npts = g->npts;
+    h.two_point = g->two_point;
+    for (int i = 0; i < g->npts; ++i) {
+        h.Z[i] = g->Z[i];
+        h.P[i] = g->P[i];
+        h.P2[i] = g->P2[i];
+    }
+    h.dens_a = g->dens_a;
+    h.dens_b = g->dens_b;
+    for (int j = 0; j < 4; ++j) {
+        h.fd_xc[j] = g->fd_xc[j];
+        h.fd_gam[j] = g->fd_gam[j];
+    }
+    h.fd_h12 = g->fd_h12;
+    h.bref = (C.kind == 1) ? g->env_ref : 0;
+    h.ref_xc = g->ref_xc;
+    h.ref_gam = g->ref_gam;
+    const double* t = nullptr;
+    if (upload(p->allocs, g->gam, Nw, &h.gam) || upload(p->allocs, g->wc, Nw, &h.wc) ||
+        upload(p->allocs, g->om, Nw, &h.om) || upload(p->allocs, g->ofs, 2 * Nw, &t))
+        return LUNA_ERR_CUDA;
+    h.ofs = (const double2*)t;
+    const LunaGrad* d = nullptr;
+    const double *dk = nullptr, *dm = nullptr;
+    if (upload(p->allocs, &h, 1, &d) || upload(p->allocs, kr2, Nr, &dk) || upload(p->allocs, mu0w, Nw, &dm))
+        return LUNA_ERR_CUDA;
+    if (!p->ofz && dalloc(p->allocs, &p->ofz, sizeof(double2) * Nw * Nr)) return LUNA_ERR_CUDA;
+    p->grad = RadGrad{d, dk, dm};
+    return LUNA_OK;
+}
+
+int luna_b200_radial_linop(luna_radial_plan* p, double z, double* linop, double* outfac) {
+    if (!p || !linop) return fail(LUNA_ERR_BAD_ARG, "radial_linop: null argument");
+    if (!p->grad.g) return fail(LUNA_ERR_BAD_ARG, "radial_linop: the plan has no gas fill gradient");
+    const size_t n = (size_t)p->Nw * p->Nr, bytes = sizeof(double2) * n;
+    double2* dL = nullptr;
+    CK(cudaMalloc(&dL, 2 * bytes));
+    RadArgs a{p->Nw, p->Nr, nullptr, nullptr, nullptr, nullptr};
+    rad_gradfill_kernel<<<rad_grid(n), 256>>>(a, p->grad, -2, z, dL, dL + n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(linop, dL, bytes, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && outfac) e = cudaMemcpy(outfac, dL + n, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(dL);
+    if (e != cudaSuccess) return fail(LUNA_ERR_CUDA, std::string("radial_linop: ") + cudaGetErrorString(e));
+    return LUNA_OK;
 }
 
 int luna_b200_qdht_device(luna_radial_plan* p, void* Y_dev, const void* X_dev, int forward, void* stream) {
@@ -1767,8 +1850,8 @@ int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, doub
         CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     }
     CK(cudaMemcpyAsync(p->d_Ew, Ew, bytes, cudaMemcpyHostToDevice, p->stream));
-    int rc = (p->precision == LUNA_PREC_FP64) ? rad_rhs<double>(p, p->d_Ew, p->d_nl, p->stream)
-                                              : rad_rhs<float>(p, p->d_Ew, p->d_nl, p->stream);
+    int rc = (p->precision == LUNA_PREC_FP64) ? rad_rhs<double>(p, p->d_Ew, p->d_nl, p->stream, z)
+                                              : rad_rhs<float>(p, p->d_Ew, p->d_nl, p->stream, z);
     if (rc) return rc;
     int fl = 0;
     CK(cudaMemcpyAsync(nl, p->d_nl, bytes, cudaMemcpyDeviceToHost, p->stream));
@@ -1783,10 +1866,14 @@ int luna_b200_radial_rhs(luna_radial_plan* p, double* nl, const double* Ew, doub
 
 namespace {
 
+// A gas fill gradient of the column transform (radial plans; none for modal plans).
+inline RadGrad plan_grad(const luna_radial_plan* p) { return p->grad; }
+inline RadGrad plan_grad(const luna_modal_plan*) { return RadGrad{nullptr, nullptr, nullptr}; }
+
 // Device buffers of one column solve (radial or modal transform).
 struct RadSolve {
     std::vector<void*> allocs;
-    double2 *L = nullptr, *y = nullptr, *yn = nullptr, *e1 = nullptr, *saves = nullptr;
+    double2 *L = nullptr, *y = nullptr, *yn = nullptr, *e1 = nullptr, *saves = nullptr, *ofz = nullptr;
     void* k[7] = {};
     void** d_k = nullptr;
     double *zsave = nullptr, *steplog = nullptr, *replay = nullptr, *partial = nullptr;
@@ -1811,7 +1898,10 @@ int col_solve(PlanT* p, XF&& xform, const char* who, const double* linop, double
     const TwTab<Rl>& t = *reinterpret_cast<const TwTab<Rl>*>(std::is_same<Rl, double>::value ? (const void*)&tw.d : (const void*)&tw.f);
     const size_t n = (size_t)p->Nw * p->Nr;
     const size_t cb = sizeof(double2);
+    const RadGrad G = plan_grad(p);
+    if (!linop && !G.g) return fail(LUNA_ERR_BAD_ARG, std::string(who) + ": null linop");
     RadSolve S;
+    if (G.g && dalloc(S.allocs, &S.ofz, cb * n)) return LUNA_ERR_CUDA;
     if (dalloc(S.allocs, &S.L, cb * n) || dalloc(S.allocs, &S.y, cb * n) || dalloc(S.allocs, &S.yn, cb * n) ||
         dalloc(S.allocs, &S.e1, cb * n) || dalloc(S.allocs, &S.st, sizeof(RadState)) ||
         dalloc(S.allocs, &S.opt, sizeof(LunaInst)) || dalloc(S.allocs, &S.d_k, sizeof(void*) * 7))
@@ -1851,18 +1941,20 @@ int col_solve(PlanT* p, XF&& xform, const char* who, const double* linop, double
     I.replay = S.replay;
     I.nreplay = S.replay ? o->nreplay : 0;
     CK(cudaMemcpy(S.opt, &I, sizeof(LunaInst), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(S.L, linop, cb * n, cudaMemcpyHostToDevice));
+    // with a gas fill gradient L(z) is evaluated on the device and linop is ignored
+    if (!G.g) CK(cudaMemcpy(S.L, linop, cb * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S.y, y_inout, cb * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S.yn, y_inout, cb * n, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(S.d_k, S.k, sizeof(void*) * 7, cudaMemcpyHostToDevice));
     if (!p->stream) CK(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     cudaStream_t s = p->stream;
-    RadArgs a{p->Nw, p->Nr, S.L, p->outfac, S.e1, S.st};
+    RadArgs a{p->Nw, p->Nr, S.L, G.g ? S.ofz : p->outfac, S.e1, S.st};
     const int eg = rad_grid(n);
     int* flags_dev = (int*)((char*)S.st + offsetof(RadState, flags));
     const int* fin_dev = (const int*)((char*)S.st + offsetof(RadState, finished));
     rad_init_kernel<<<1, 32, 0, s>>>(S.st, S.opt, S.y, S.yn, S.d_k);
     // k1 = f(y0)
+    if (G.g) rad_gradfill_kernel<<<eg, 256, 0, s>>>(a, G, -1, 0.0, S.L, S.ofz);
     rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, nullptr, (cpx<Rl>*)p->A);
     xform(t, S.st, flags_dev, s);
     rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, -1, (const cpx<Rl>*)p->B, nullptr);
@@ -1875,13 +1967,15 @@ int col_solve(PlanT* p, XF&& xform, const char* who, const double* linop, double
         for (int q = 0; q < chunk; ++q) {
             rad_begin_kernel<<<1, 32, 0, s>>>(S.st, S.opt);
             for (int sg = 0; sg < 6; ++sg) {
+                // L(z) and the output factor at this stage's node (make_prop!, RK45.jl:284-297)
+                if (G.g) rad_gradfill_kernel<<<eg, 256, 0, s>>>(a, G, sg, 0.0, S.L, S.ofz);
                 rad_stage_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, nullptr, (cpx<Rl>*)p->A);
                 xform(t, S.st, flags_dev, s);
                 rad_store_kernel<Rl, Kt><<<eg, 256, 0, s>>>(a, sg, (const cpx<Rl>*)p->B, nullptr);
             }
             rad_combine_kernel<Kt><<<nblk, 256, 0, s>>>(a, S.partial);
             rad_control_kernel<<<1, 256, 0, s>>>(S.st, S.opt, S.partial, nblk);
-            rad_post_kernel<Rl, Kt><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(a, p->d_col, S.opt, t, p->smem, p->gscr, p->gstride);
+            rad_post_kernel<Rl, Kt><<<p->Nr, LUNA_BLOCK, p->smem, s>>>(a, p->d_col, S.opt, t, p->smem, p->gscr, p->gstride, G);
         }
         CK(cudaGetLastError());
         enq += chunk;
@@ -1923,7 +2017,7 @@ extern "C" {
 int luna_b200_radial_solve(luna_radial_plan* p, const double* linop, double* y_inout, double z0, double dz0,
                            double zmax, const luna_solve_opts* opts, double* saves, double* steplog,
                            luna_solve_stats* stats) {
-    if (!p || !linop || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "radial_solve: null argument");
+    if (!p || (!linop && !p->grad.g) || !y_inout || !opts) return fail(LUNA_ERR_BAD_ARG, "radial_solve: null argument");
     if (opts->saveN < 0 || (opts->saveN > 0 && !opts->zsave)) return fail(LUNA_ERR_BAD_ARG, "radial_solve: save points missing");
     if (p->precision == LUNA_PREC_FP64)
         return col_solve<double, double>(

@@ -37,11 +37,96 @@ struct RadState {
 
 struct RadArgs {
     int Nw, Nr;
-    const double2* L;       // [Nw*Nr] linear operator
-    const double2* outfac;  // [Nw*Nr] crop * ωwin * (-iω) / (2 normfun)
+    const double2* L;       // [Nw*Nr] linear operator (of the current node with a gas fill gradient)
+    const double2* outfac;  // [Nw*Nr] crop * ωwin * (-iω) / (2 normfun) (x ρ(z) with a gradient)
     double2* e1;            // [Nw*Nr] exp(L dt) of the last stage with node 1
     RadState* st;
 };
+
+// ------------------------------------------------------------------ gas fill gradient
+// make_linop(grid, q, nfun) for radial symmetry (LinearOps.jl:174-226) and norm_radial
+// (NonlinearRHS.jl:494-524) with nfun(ω; z) = sqrt(1 + γ(ω) ρ(z)), ρ(z) the density law of a
+// luna_gradient_desc (Capillary.gradient, Capillary.jl:306-337):
+//   k2(ω) = (n ω/c)^2 on sidx (0 elsewhere), βsq = k2 - k_r^2,
+//   L = -i (sqrt(βsq) - β1(z) ω), or -i (-β1 ω) - min(sqrt|βsq|, 200) when βsq < 0,
+//   + i β(ω0; z) on an envelope grid without THG, β1(z) the 4-point central difference of
+//   x/c n(x; z) at ω0 (h = 1e-4 ω0); normfun = sqrt(βsq)/(μ0 ω) for ω != 0 and βsq > 0, else 1;
+// each in IEEE-rounded operations in the order of the host restatement. The responses'
+// coefficients are given for ρ = 1; ρ(z) scales the output factor.
+struct RadGrad {
+    const LunaGrad* g;  // fill law, γ and ω/c on sidx (wc = 0 elsewhere), ω (om), ofs, fd tables
+    const double* kr2;  // [Nr] k_r^2 of the QDHT
+    const double* mw;   // [Nw] μ0 ω
+};
+
+// (ρ(z), β1(z), β(ω0; z)) into out[3]
+__device__ __forceinline__ void rad_grad_scalars(const LunaGrad* g, double z, double* out) {
+    const double rho = grad_density(g, z);
+    double f[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) f[j] = __dmul_rn(g->fd_xc[j], __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(g->fd_gam[j], rho))));
+    const double num = __dadd_rn(__dsub_rn(__dadd_rn(-f[0], __dmul_rn(8.0, f[1])), __dmul_rn(8.0, f[2])), f[3]);
+    out[0] = rho;
+    out[1] = __ddiv_rn(num, g->fd_h12);
+    out[2] = g->bref ? __dmul_rn(g->ref_xc, __dsqrt_rn(__dadd_rn(1.0, __dmul_rn(g->ref_gam, rho)))) : 0.0;
+}
+
+// L and the output factor of element (ω index i, k index c)
+__device__ __forceinline__ void rad_grad_elem(const RadGrad& G, int i, int c, const double* sc, cpx<double>& L,
+                                              cpx<double>& of) {
+    const LunaGrad* g = G.g;
+    const double rho = sc[0], b1 = sc[1];
+    const double wc = __ldg(g->wc + i), w = __ldg(g->om + i);
+    double k2 = 0.0;
+    if (wc != 0.0) {
+        const double nk = __dmul_rn(__dsqrt_rn(__dadd_rn(1.0, __dmul_rn(__ldg(g->gam + i), rho))), wc);
+        k2 = __dmul_rn(nk, nk);
+    }
+    const double bsq = __dsub_rn(k2, __ldg(G.kr2 + c));
+    const double bw = __dmul_rn(b1, w);
+    double re, im;
+    if (bsq < 0) {
+        re = -fmin(__dsqrt_rn(-bsq), 200.0);
+        im = bw;
+    } else {
+        re = 0.0;
+        im = -__dsub_rn(__dsqrt_rn(bsq), bw);
+    }
+    if (g->bref) im = __dadd_rn(im, sc[2]);
+    L = mk<double>(re, im);
+    const double2 o = __ldg(g->ofs + i);
+    double ox = __dmul_rn(rho, o.x), oy = __dmul_rn(rho, o.y);
+    if (w != 0.0 && bsq > 0) {
+        const double nr = __ddiv_rn(__dsqrt_rn(bsq), __ldg(G.mw + i));
+        ox = __ddiv_rn(ox, nr);
+        oy = __ddiv_rn(oy, nr);
+    }
+    of = mk<double>(ox, oy);
+}
+
+// L(z) and the output factor at z over the whole Nw x Nr array, z the node of stage s of
+// the current step (s >= 0), the current z of the loop (s == -1) or zfix (s == -2).
+__global__ void __launch_bounds__(256) rad_gradfill_kernel(RadArgs a, RadGrad G, int s, double zfix, double2* Lz,
+                                                           double2* ofz) {
+    const RadState* st = a.st;
+    if (s != -2 && st->finished) return;
+    __shared__ double sc[3];
+    if (threadIdx.x == 0) {
+        double z = zfix;
+        if (s >= 0) z = __dadd_rn(st->c.t, __dmul_rn(c_nodes[s], st->c.dt));
+        else if (s == -1) z = st->c.t;
+        rad_grad_scalars(G.g, z, sc);
+    }
+    __syncthreads();
+    const size_t n = (size_t)a.Nw * a.Nr;
+    for (size_t e = (size_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (size_t)gridDim.x * blockDim.x) {
+        const int c = (int)(e / a.Nw), i = (int)(e - (size_t)c * a.Nw);
+        cpx<double> L, of;
+        rad_grad_elem(G, i, c, sc, L, of);
+        if (Lz) reinterpret_cast<cpx<double>*>(Lz)[e] = L;
+        reinterpret_cast<cpx<double>*>(ofz)[e] = of;
+    }
+}
 
 // ------------------------------------------------------------------ elementwise stages
 // Stage input A = exp(L d) (y + dt sum_j B[s][j] k_j) (the load of the fused mode-averaged
@@ -58,7 +143,7 @@ __global__ void __launch_bounds__(256) rad_stage_kernel(RadArgs a, int s, const 
         return;
     }
     const double t0 = st->c.t, dt = st->c.dt;
-    const double d = (t0 + c_nodes[s] * dt) - t0;
+    const double d = __dsub_rn(__dadd_rn(t0, __dmul_rn(c_nodes[s], dt)), t0);  // node - t, as rounded
     const bool propk1 = (s == 0) && (st->dprop != 0.0);
     const cpx<double>* y = reinterpret_cast<const cpx<double>*>(st->y);
     const cpx<double>* L = reinterpret_cast<const cpx<double>*>(a.L);
@@ -100,7 +185,7 @@ __global__ void __launch_bounds__(256) rad_store_kernel(RadArgs a, int s, const 
         return;
     }
     const double t0 = st->c.t, dt = st->c.dt;
-    const double d = (t0 + c_nodes[s] * dt) - t0;
+    const double d = __dsub_rn(__dadd_rn(t0, __dmul_rn(c_nodes[s], dt)), t0);
     const cpx<double>* L = reinterpret_cast<const cpx<double>*>(a.L);
     void* kout = st->c.k[s + 1];
     for (size_t i = i0; i < n; i += di) {
@@ -361,7 +446,7 @@ __global__ void __launch_bounds__(256) rad_control_kernel(RadState* st, LunaInst
 template <typename Rl, typename Kt>
 __global__ void __launch_bounds__(LUNA_BLOCK, 1)
 rad_post_kernel(RadArgs a, const LunaInst* inst, const LunaInst* opt, TwTab<Rl> tw, int smem_bytes, char* gscr,
-                size_t gstride) {
+                size_t gstride, RadGrad G) {
     extern __shared__ __align__(256) char smem[];
     const RadState* st = a.st;
     if (st->finished) return;
@@ -380,9 +465,25 @@ rad_post_kernel(RadArgs a, const LunaInst* inst, const LunaInst* opt, TwTab<Rl> 
     void* kc[7];
 #pragma unroll
     for (int j = 0; j < 7; ++j) kc[j] = (char*)st->c.k[j] + off * sizeof(cpx<Kt>);
-    for (int si = st->save_lo; si < st->save_hi; ++si)
+    for (int si = st->save_lo; si < st->save_hi; ++si) {
+        if (G.g) {
+            // L of this column at the save point (a gas fill gradient: prop! to z_i with
+            // linop!(z_i), RK45.jl:284-297); the node buffer is free until the next step
+            __shared__ double sc[3];
+            __syncthreads();
+            if (threadIdx.x == 0) rad_grad_scalars(G.g, opt->zsave[si], sc);
+            __syncthreads();
+            cpx<double>* Lc = reinterpret_cast<cpx<double>*>(const_cast<double2*>(a.L)) + off;
+            for (int i = threadIdx.x; i < Nw; i += LUNA_BLOCK) {
+                cpx<double> L, of;
+                rad_grad_elem(G, i, c, sc, L, of);
+                Lc[i] = L;
+            }
+            __syncthreads();
+        }
         interpolate_row<Rl, Kt>(Nw, a.L + off, st->c, opt->zsave[si], kc, y, yn,
                                 opt->saves + (size_t)si * Nw * a.Nr + off);
+    }
 }
 
 }  // namespace luna

@@ -129,6 +129,86 @@ def GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=0.0, focal_length=No
     return np.ascontiguousarray(Eωk)
 
 
+# ------------------------------------------------------------------ gas fill gradient
+def _sidx_mask(grid):
+    m = np.zeros(len(grid.ω), dtype=bool)
+    m[grid.sidx] = True
+    return m
+
+
+class RadialFill:
+    """The z-dependent parts of radial propagation through a gas fill gradient: nfun(ω; z) =
+    sqrt(1 + γ(ω) ρ(z)) with ρ(z) of ``gradient.Gradient``; make_linop(grid, q, nfun)
+    (LinearOps.jl:174-226), norm_radial (NonlinearRHS.jl:494-524) and β1(z) as the 4-point
+    central difference of x/c n(x; z) at ω0 (h = 1e-4 ω0), written out in IEEE-rounded
+    operations in the order the device evaluates them (k2 as (n x ω/c)^2)."""
+
+    def __init__(self, grid, q, grad, λ0, thg=False):
+        self.grid, self.q, self.grad, self.λ0 = grid, q, grad, λ0
+        s = _sidx_mask(grid)
+        self.s = s
+        ω = np.asarray(grid.ω, dtype=np.float64)
+        self.om = ω
+        self.wc = np.where(s, ω / pd.c, 0.0)
+        self.gam = np.zeros(len(ω))
+        self.gam[s] = grad.gamma(ω[s])
+        self.kr2 = np.asarray(q.k, dtype=np.float64) ** 2
+        self.mw = pd.mu_0 * ω
+        ω0 = pd.wlfreq(λ0)
+        h = ω0 * 1e-4
+        x = np.array([ω0 + 2 * h, ω0 + h, ω0 - h, ω0 - 2 * h])
+        self.fd_xc, self.fd_gam, self.fd_h12 = x / pd.c, grad.gamma(x), 12 * h
+        self.env_ref = grid.kind == "env" and not thg
+        self.ref_xc = ω0 / pd.c
+        self.ref_gam = float(grad.gamma(np.array([ω0]))[0])
+
+    def scalars(self, z):
+        rho = self.grad.density(z)
+        f = self.fd_xc * np.sqrt(1.0 + self.fd_gam * rho)
+        b1 = (-f[0] + 8 * f[1] - 8 * f[2] + f[3]) / self.fd_h12
+        br = self.ref_xc * math.sqrt(1.0 + self.ref_gam * rho) if self.env_ref else 0.0
+        return rho, b1, br
+
+    def _bsq(self, rho):
+        nk = np.sqrt(1.0 + self.gam * rho) * self.wc
+        k2 = np.where(self.s, nk * nk, 0.0)
+        return k2[:, None] - self.kr2[None, :]
+
+    def linop(self, z):
+        rho, b1, br = self.scalars(z)
+        bsq = self._bsq(rho)
+        bw = (b1 * self.om)[:, None] * np.ones((1, len(self.kr2)))
+        neg = bsq < 0
+        re = np.where(neg, -np.minimum(np.sqrt(np.where(neg, -bsq, 0.0)), 200.0), 0.0)
+        im = np.where(neg, bw, -(np.sqrt(np.where(neg, 0.0, bsq)) - bw))
+        if self.env_ref:
+            im = im + br
+        return np.ascontiguousarray(re + 1j * im)
+
+    def normfun(self, z):
+        bsq = self._bsq(self.grad.density(z))
+        ok = (self.om[:, None] != 0) & (bsq > 0)
+        mw = np.where(self.om != 0, self.mw, 1.0)[:, None]
+        return np.where(ok, np.sqrt(np.where(ok, bsq, 1.0)) / mw, 1.0)
+
+
+class TransRadialZ(TransRadial):
+    """TransRadial with densityfun(z) and normfun(z) of a gas fill gradient."""
+
+    kind = "radial_z"
+
+    def __init__(self, grid, q, resp, fill):
+        self.fill = fill
+        super().__init__(grid, q, resp, fill.grad.density(0.0), fill.normfun(0.0))
+
+    def densityfun(self, z):
+        return self.fill.grad.density(z)
+
+    def output_factor_z(self, z):
+        g = self.grid
+        return (g.ωwin * (-1j * g.ω))[:, None] / (2 * self.fill.normfun(z))
+
+
 class RadialProblem:
     def __init__(self, Eω, grid, linop, transform, q, saveN=201):
         self.Eω, self.grid, self.linop, self.transform, self.q = Eω, grid, linop, transform, q
@@ -142,11 +222,21 @@ def prop_radial_args(gas, pressure, *, R, N, flength, λ0, λlims, trange, τfwh
     radial_env examples. ``envelope`` builds an EnvGrid (Kerr_env, or Kerr_env_thg with
     ``thg``; no plasma); ``thg=False`` on a field-resolved grid selects Kerr_field_nothg;
     ``raman`` adds the gas's molecular Raman response (RamanPolarField / RamanPolarEnv,
-    applied per radial column)."""
+    applied per radial column). ``pressure`` as a (p0, p1) pair or (Z, P) nodes gives a gas
+    fill gradient (Capillary.gradient's law, Capillary.jl:306-337): make_linop(grid, q,
+    nfun) with nfun(ω; z) = sqrt(1 + γ(ω) ρ(z)), densityfun(z) and norm_radial at z."""
     if thg is None:
         thg = not envelope
     grid = EnvGrid(flength, λ0, λlims, trange, thg=thg) if envelope else RealGrid(flength, λ0, λlims, trange)
     q = QDHT(R, N)
+    grad = None
+    if isinstance(pressure, (tuple, list)):
+        from .gradient import Gradient
+        if len(pressure) == 2 and all(np.ndim(x) == 0 for x in pressure):
+            grad = Gradient(gas, flength, *pressure)
+        else:
+            grad = Gradient(gas, *pressure)
+        pressure = grad.p0
     nfun = pd.ref_index_fun(gas, pressure)
     dens0 = pd.density(gas, pressure)
     resp = []
@@ -163,8 +253,13 @@ def prop_radial_args(gas, pressure, *, R, N, flength, λ0, λlims, trange, τfwh
     if raman:
         rr = _raman.raman_response(grid.to, gas)
         resp.append(RamanPolarEnv(grid.to, rr) if envelope else RamanPolarField(grid.to, rr, thg=thg))
-    linop, _ = make_const_linop_radial(grid, q, nfun, thg=thg)
-    norm = const_norm_radial(grid, q, nfun)
-    transform = TransRadial(grid, q, resp, dens0, norm)
+    if grad is not None:
+        fill = RadialFill(grid, q, grad, λ0, thg=thg)
+        linop = fill.linop
+        transform = TransRadialZ(grid, q, resp, fill)
+    else:
+        linop, _ = make_const_linop_radial(grid, q, nfun, thg=thg)
+        norm = const_norm_radial(grid, q, nfun)
+        transform = TransRadial(grid, q, resp, dens0, norm)
     Eω = GaussGaussField(grid, q, λ0, τfwhm, energy, w0, propz=propz, focal_length=focal_length)
     return RadialProblem(Eω, grid, linop, transform, q, saveN)

@@ -69,7 +69,10 @@ class RadialPlan:
         gd.outfac = _lib.dptr(None)
         gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
         gd.in_scale = pad / No
-        rds = resp_descs(t.resp, t.density, keep)
+        zdep = getattr(t, "kind", "") == "radial_z"
+        # a gas fill gradient scales the output by ρ(z) on the device: coefficients for ρ = 1
+        rds = resp_descs(t.resp, 1.0 if zdep else t.density, keep,
+                         rho_tau2=t.densityfun(0.0) if zdep else None)
         Mi = np.ascontiguousarray(q.Mi, dtype=np.float64)
         Mf = np.ascontiguousarray(q.Mf, dtype=np.float64)
         of = _colmajor(crop * t.output_factor())
@@ -78,7 +81,22 @@ class RadialPlan:
         rd.Nr = q.N
         rd.Mi, rd.Mf = _lib.dptr(Mi), _lib.dptr(Mf)
         rd.outfac = _lib.dptr(of.view(np.float64))
-        return cls(gd, rds, rd, keep, precision, Nw, q.N)
+        plan = cls(gd, rds, rd, keep, precision, Nw, q.N)
+        if zdep:
+            gdesc, kr2, mw = radial_gradient_desc(t, crop, plan._keep)
+            plan._gdesc = gdesc
+            _lib.check(_lib.load().luna_b200_radial_set_gradient(plan.handle, _lib.ctypes.byref(gdesc),
+                                                                 _lib.dptr(kr2), _lib.dptr(mw)))
+        return plan
+
+    def linop(self, z):
+        """The device's linop!(out, z) and output factor of a plan with a gas fill gradient,
+        (Nw, Nr) complex each."""
+        L = np.zeros((self.Nr, self.Nw), dtype=np.complex128)
+        of = np.zeros_like(L)
+        _lib.check(_lib.load().luna_b200_radial_linop(self._h, float(z), _lib.dptr(L.view(np.float64)),
+                                                      _lib.dptr(of.view(np.float64))))
+        return L.T, of.T
 
     def rhs(self, nl, Eω, z=0.0):
         """nl[:, :] = T(Eω) on the GPU; (Nw, Nr) complex128 host arrays."""
@@ -91,19 +109,21 @@ class RadialPlan:
 
     def solve(self, linop, Eω, z0, dz0, zmax, saveN=201, steplog_cap=0, replay=None,
               raise_on_status=True, **opt):
+        if callable(linop):  # a gas fill gradient: L(z) is evaluated on the device
+            linop = None
         """RK45.solve_precon with Luna.run's stepfun and saves (RK45.jl:19-25,
         Luna.jl:358-391); saves come back as (nsaved, Nw, Nr)."""
         zs = np.linspace(z0, zmax, saveN)
         if replay is not None:
             replay = np.ascontiguousarray(replay, dtype=np.float64).ravel()
         o = make_opts(saveN, zs, steplog_cap=steplog_cap, replay=replay, **opt)
-        L = _colmajor(linop)
+        L = _colmajor(linop) if linop is not None else None
         y = _colmajor(Eω)
         saves = np.zeros((saveN, self.Nr, self.Nw), dtype=np.complex128)
         log = np.zeros((max(steplog_cap, 1), 4))
         st = _lib.SolveStats()
         rc = _lib.load().luna_b200_radial_solve(
-            self._h, _lib.dptr(L.view(np.float64)), _lib.dptr(y.view(np.float64)), float(z0),
+            self._h, _lib.dptr(L.view(np.float64) if L is not None else None), _lib.dptr(y.view(np.float64)), float(z0),
             float(dz0), float(zmax), _lib.ctypes.byref(o), _lib.dptr(saves.view(np.float64)),
             _lib.dptr(log) if steplog_cap else _lib.dptr(None), _lib.ctypes.byref(st))
         if rc not in (_lib.LUNA_OK, _lib.LUNA_FIELD_ABOVE_EMAX, _lib.LUNA_REPEAT_LIMIT,
@@ -115,6 +135,33 @@ class RadialPlan:
         sv = np.ascontiguousarray(saves[:n].transpose(0, 2, 1))
         steplog = log[: min(st.steps, steplog_cap)] if steplog_cap else None
         return SolveResult(zs[:n], sv, np.ascontiguousarray(y.T), st, steplog)
+
+
+def radial_gradient_desc(t, crop, keep):
+    """luna_gradient_desc, kr2 and μ0 ω of a TransRadialZ for luna_b200_radial_set_gradient;
+    the arrays are appended to ``keep``."""
+    f, g = t.fill, t.grid
+    grad = f.grad
+    if len(grad.Z) > _lib.GRAD_MAXPTS:
+        raise ValueError(f"at most {_lib.GRAD_MAXPTS} pressure nodes")
+    ofs = np.ascontiguousarray(crop * (g.ωwin * (-1j * g.ω)) / 2, dtype=np.complex128)
+    arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (f.gam, f.wc, f.om, f.kr2, f.mw)]
+    keep += arrs + [ofs]
+    gam, wc, om, kr2, mw = arrs
+    d = _lib.GradientDesc()
+    d.npts, d.two_point = len(grad.Z), int(grad.two_point)
+    for i in range(len(grad.Z)):
+        d.Z[i], d.P[i], d.P2[i] = grad.Z[i], grad.P[i], grad.P2[i]
+    d.dens_a, d.dens_b = grad.dens_a, grad.dens_b
+    d.nta = 1
+    d.gam, d.wc, d.om = _lib.dptr(gam), _lib.dptr(wc), _lib.dptr(om)
+    d.ofs = _lib.dptr(ofs.view(np.float64))
+    for j in range(4):
+        d.fd_xc[j], d.fd_gam[j] = f.fd_xc[j], f.fd_gam[j]
+    d.fd_h12 = f.fd_h12
+    d.env_ref = int(f.env_ref)
+    d.ref_xc, d.ref_gam = f.ref_xc, f.ref_gam
+    return d, kr2, mw
 
 
 def run(problem, precision=_lib.PREC_FP64, **kw):

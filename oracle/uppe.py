@@ -242,15 +242,17 @@ def trans_radial(t, Ew, z):
     (Et_to_Pt! with CartesianIndices, NonlinearRHS.jl:137-141)."""
     g, q = t.grid, t.q
     Nw, Nr = Ew.shape
+    zdep = getattr(t, "kind", "") == "radial_z"   # densityfun(z), normfun(z) of a gas fill gradient
+    rho = t.densityfun(z) if zdep else t.density
     Et = np.stack([to_time(g, Ew[:, i]) for i in range(Nr)], axis=1)  # to_time! along dim 1
     Er = q.inverse(Et, axis=1)                     # ldiv!(Eto, QDHT, Eto): k -> r
     Pr = np.zeros_like(Er)
     for i in range(Nr):                            # Et_to_Pt! per radial column
-        Pr[:, i] = et_to_pt(Er[:, i], t.resp, t.density)
+        Pr[:, i] = et_to_pt(Er[:, i], t.resp, rho)
     Pr = Pr * g.towin[:, None]
     Pk = q.forward(Pr, axis=1)                     # mul!(Pto, QDHT, Pto): r -> k
     nl = np.stack([to_freq(g, Pk[:, i], Nw) for i in range(Nr)], axis=1)  # to_freq!
-    return nl * t.output_factor()
+    return nl * (t.output_factor_z(z) if zdep else t.output_factor())
 
 
 def kerr_vector(out, E, rho, g3):
@@ -459,7 +461,7 @@ def trans_modal(t, Ew, z):
 
 def rhs(t, Ew, z):
     kind = getattr(t, "kind", "")
-    if kind == "radial":
+    if kind in ("radial", "radial_z"):
         return trans_radial(t, Ew, z)
     if kind == "modal":
         return trans_modal(t, Ew, z)

@@ -190,6 +190,57 @@ def test_radial_env_focus_matches_paraxial_gaussian_beam_on_gpu():
     assert np.max(np.abs(Ir - Ia)) / np.linalg.norm(Ir) < 1.5e-4
 
 
+# ------------------------------------------------------------------ gas fill gradient
+# make_linop(grid, q, nfun) with nfun(ω; z) from a pressure gradient (LinearOps.jl:174-226),
+# densityfun(z) and norm_radial(z) (NonlinearRHS.jl:494-524), evaluated on the device at every
+# stage node, step end and save point.
+def _fill(name, flength=0.02, saveN=5):
+    c = dict(R=1e-3, N=64, flength=flength, λ0=800e-9, λlims=(400e-9, 2000e-9), τfwhm=20e-15,
+             w0=40e-6, saveN=saveN)
+    if name == "Ar-falling":
+        return prop_radial_args("Ar", (2.0, 0.3), trange=0.2e-12, energy=30e-6, plasma="PPT", **c)
+    if name == "Ne-multipoint":
+        return prop_radial_args("Ne", ([0, 0.005, 0.015, 0.02], [0.5, 3.0, 3.0, 1.0]), trange=0.2e-12,
+                                energy=40e-6, plasma="PPT", **c)
+    return prop_radial_args("Ar", (2.0, 0.3), trange=0.8e-12, energy=30e-6, plasma=False, envelope=True, **c)
+
+
+@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "Ar-env-falling"])
+def test_radial_fill_linop_is_bit_identical_to_host(name):
+    p = _fill(name)
+    plan = p.transform.plan()
+    f = p.transform.fill
+    crop = ((len(p.grid.ω) - 1) / (len(p.grid.ωo) - 1)) if p.grid.kind == "real" else len(p.grid.ω) / p.grid.No
+    for z in (-0.01, 0.0, 0.004, 0.005, 0.0123, 0.02, 0.03):
+        L, of = plan.linop(z)
+        ref = f.linop(z)
+        assert np.array_equal(L, ref), (z, _rel(L, ref))
+        oref = crop * p.transform.densityfun(z) * p.transform.output_factor_z(z)
+        assert _rel(of, oref) < 1e-14, (z, _rel(of, oref))
+
+
+@pytest.mark.parametrize("name", ["Ar-falling", "Ne-multipoint", "Ar-env-falling"])
+def test_radial_fill_rhs_and_replay_match_oracle(name):
+    p = _fill(name)
+    rng = np.random.default_rng(17)
+    Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))
+    for z in (0.0, 0.0071, 0.02):
+        nl = np.zeros_like(Ew)
+        p.transform(nl, Ew, z)
+        ref = uppe.trans_radial(p.transform, Ew, z)
+        assert _rel(nl, ref) < 1e-11, (z, _rel(nl, ref))
+    ores = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    replay = np.array(ores.steps_all, dtype=np.float64).ravel()
+    r = radial_plan.run(p, replay=replay)
+    assert r.status == 0 and r.nsaved == 5 and r.steps == ores.steps
+    for a, b in zip(r.Eω, ores.Eω):
+        assert _rel(a, b) < 1e-10, _rel(a, b)
+    m = radial_plan.run(p, precision=_lib.PREC_MIXED)
+    assert m.status == 0 and m.nsaved == 5
+    for a, b in zip(m.Eω, ores.Eω):
+        assert _rel(np.abs(a) ** 2, np.abs(b) ** 2) < 1e-3
+
+
 # ------------------------------------------------------------------ mixed precision
 # FP32 transforms and responses, QDHT as 3xBF16 tensor-core products (tcgen05) with FP32
 # accumulation; FP64 state, phase, controller and plasma prefix sums.

@@ -322,6 +322,41 @@ def test_radial_env_focus_matches_paraxial_gaussian_beam():
     assert abs(energy_t_radial(g, q, Et) / 2e-9 - 1) < 1e-12
 
 
+@pytest.mark.parametrize("envelope,thg", [(False, None), (True, False), (True, True)])
+def test_radial_fill_gradient_at_equal_pressures_is_the_constant_fill(envelope, thg):
+    """test_linops.jl "radial, field/env": make_linop(grid, q, nfun) with a z-independent
+    fill equals make_const_linop(grid, q, nfun) at every z; here the fill is a gradient
+    between equal pressures (LinearOps.jl:130-226), and norm_radial equals
+    const_norm_radial."""
+    from luna_b200.radial import prop_radial_args
+    kw = dict(R=1e-3, N=64, flength=0.02, λ0=800e-9, λlims=(400e-9, 2000e-9), τfwhm=20e-15,
+              energy=30e-6, w0=40e-6, plasma=False, envelope=envelope, thg=thg,
+              trange=0.8e-12 if envelope else 0.2e-12)
+    c = prop_radial_args("Ar", 1.2, **kw)
+    p = prop_radial_args("Ar", (1.2, 1.2), **kw)
+    assert p.transform.kind == "radial_z"
+    for z in (0.0, 0.013, 0.02, 0.05):
+        L = p.linop(z)
+        assert np.max(np.abs(L - c.linop)) <= 1e-14 * np.max(np.abs(c.linop)), z
+        assert np.max(np.abs(p.transform.fill.normfun(z) / c.transform.normfun - 1)) < 1e-14
+        assert p.transform.densityfun(z) == pytest.approx(c.transform.density, rel=1e-15)
+
+
+def test_radial_fill_gradient_propagation_at_equal_pressures():
+    """The oracle's radial solve through an equal-pressure gradient takes the constant
+    fill's steps; the saved fields agree to the rounding of β1 (a finite difference)."""
+    from luna_b200.radial import prop_radial_args
+    kw = dict(R=1e-3, N=64, flength=0.02, λ0=800e-9, λlims=(400e-9, 2000e-9), trange=0.2e-12,
+              τfwhm=20e-15, energy=30e-6, w0=40e-6, plasma="PPT", saveN=5)
+    c = prop_radial_args("Ar", 1.2, **kw)
+    p = prop_radial_args("Ar", (1.2, 1.2), **kw)
+    rc = uppe.run(c.transform, c.grid, c.linop, c.Eω, saveN=5)
+    rp = uppe.run(p.transform, p.grid, p.linop, p.Eω, saveN=5)
+    assert rp.steps == rc.steps
+    for a, b in zip(rp.Eω, rc.Eω):
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-9
+
+
 def test_qdht_roundtrip_and_gaussian_pair():
     from luna_b200.hankel import QDHT
     q = QDHT(4e-3, 128)

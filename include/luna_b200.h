@@ -381,8 +381,9 @@ typedef struct {
 typedef struct luna_modal_plan luna_modal_plan;
 
 /* Replaces the TransModal constructor (NonlinearRHS.jl:203-216). The grid descriptor is
- * that of one point (kind 0; its outfac is ignored, in_scale = pad scale / No); responses
- * as for luna_b200_plan_create without the no-THG forms: with npol = 1 Kerr, plasma and
+ * that of one point (kind 0 or 1; its outfac is ignored, in_scale = pad scale / No); responses
+ * as for luna_b200_plan_create without the no-THG forms (and without plasma on an envelope
+ * grid, as in the reference): with npol = 1 Kerr, plasma and
  * Raman (scalar RamanPolar on the modal field, Nonlinear.jl:284-290); with npol = 2 Kerr
  * (KerrVector!) and plasma (PlasmaVector!, Nonlinear.jl:144-162; vector Raman is not
  * implemented in the reference either). */

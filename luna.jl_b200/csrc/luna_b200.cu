@@ -2035,6 +2035,7 @@ struct luna_modal_plan {
     int precision = 0;
     int Nw = 0, Nr = 0;           // Nr: modes (columns of the state)
     int npol = 1, nlevels = 1, nslots = 1, P = 1, nchunk = 1;
+    int Mt = 0;  // complex samples of a time buffer: No/2 (real grid) or No (envelope)
     double wlow = 0, rtol = 0, atol = 0, kerr = 0;
     luna_plan* col = nullptr;     // grid and responses of one point
     LunaInst* d_col = nullptr;
@@ -2067,6 +2068,7 @@ ModalArgs modal_args(const luna_modal_plan* p, const RadState* st) {
     a.nslots = p->nslots;
     a.lmax = p->nlevels - 1;
     a.P = p->P;
+    a.Mt = p->Mt;
     a.ems = p->ems;
     a.wts = p->wts;
     a.wlow = p->wlow;
@@ -2109,7 +2111,9 @@ int modal_setup(luna_modal_plan* p) {
     const int maxs = max_smem_optin();
     const size_t want = smem_wanted<Rl>(I);
     p->smem = (int)std::min<size_t>(want, (size_t)maxs);
-    const int M = I.No / 2;
+    // time buffer: No/2 sample pairs (real grid) or No complex samples (envelope)
+    const int M = (I.kind == 1) ? I.No : I.No / 2;
+    p->Mt = M;
     if (want > (size_t)maxs) {
         p->gstride = align_up(gscr_bytes<Rl>(I), 256);
         const int ncta = std::max(p->Nr, 1 << (p->nlevels - 1));
@@ -2158,7 +2162,6 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
                                 const luna_modal_desc* md, int precision, luna_modal_plan** out) {
     if (!g || !md || !out || !md->ems || !md->wts || !md->outfac || (nresp > 0 && !resps))
         return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: null argument");
-    if (g->kind != 0) return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: only field-resolved (RealGrid) modal transforms");
     if (md->nmodes < 1 || md->nmodes > LUNA_MODAL_MAX_MODES)
         return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: nmodes must be in 1..LUNA_MODAL_MAX_MODES");
     if (md->npol != 1 && md->npol != 2) return fail(LUNA_ERR_BAD_ARG, "modal_plan_create: npol must be 1 or 2");
@@ -2179,6 +2182,8 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: vector Raman is not implemented (as in the reference)");
         if (md->npol == 2 && k != LUNA_RESP_KERR_FIELD && k != LUNA_RESP_PLASMA_PPT && k != LUNA_RESP_PLASMA_ADK)
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support Kerr and plasma");
+        if (g->kind == 1 && (k == LUNA_RESP_PLASMA_PPT || k == LUNA_RESP_PLASMA_ADK))
+            return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: no plasma response for envelope fields (as in the reference)");
         if (md->npol == 2 && (k == LUNA_RESP_PLASMA_PPT || k == LUNA_RESP_PLASMA_ADK)) {
             if (vplasma) return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: at most one plasma response");
             vplasma = true;

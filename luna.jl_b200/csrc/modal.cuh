@@ -41,6 +41,7 @@ struct ModalState {
 
 struct ModalArgs {
     int nmodes, npol, nslots, lmax, P;
+    int Mt;                 // complex samples of a time buffer: No/2 pairs (real grid), No (envelope)
     const double* ems;      // [nslots][nmodes][npol] normalised mode fields at the nodes
     const double* wts;      // [lmax + 1][nslots] node weights of each level's rule
     double wlow;            // weight of node 0 in the midpoint rule (level 0's comparison)
@@ -72,12 +73,14 @@ modal_time_kernel(const LunaInst* inst, const cpx<Rl>* A, ModalArgs a, TwTab<Rl>
     }
     Ws<Rl> w;
     plan_ws<Rl>(I, smem, smem_bytes, w, tw, gscr ? gscr + (size_t)c * gstride : nullptr);
-    const int M = I.No / 2;
+    const int M = I.No / 2, Mt = a.Mt;
     const cpx<Rl>* E = A + (size_t)c * I.Nw;
     int P;
-    cpx<Rl>* x = c2r_to_time<Rl>(w, M, I.Nw, [&](int k) { return cvt<double>(E[k]); }, &P);
-    cpx<Rl>* out = reinterpret_cast<cpx<Rl>*>(a.Et) + (size_t)c * M;
-    for (int i = threadIdx.x; i < M; i += LUNA_BLOCK) out[i] = x[i];
+    auto ld = [&](int k) { return cvt<double>(E[k]); };
+    // envelope grids: to_time! with copy_scale_both! (NonlinearRHS.jl:16-32), No complex samples
+    cpx<Rl>* x = (I.kind == 1) ? env_to_time<Rl>(I, w, ld, &P) : c2r_to_time<Rl>(w, M, I.Nw, ld, &P);
+    cpx<Rl>* out = reinterpret_cast<cpx<Rl>*>(a.Et) + (size_t)c * Mt;
+    for (int i = threadIdx.x; i < Mt; i += LUNA_BLOCK) out[i] = x[i];
 }
 
 // One polarisation component: one CTA per new node. The point's field is built in the
@@ -95,7 +98,7 @@ modal_node_kernel(const LunaInst* inst, ModalArgs a, int slot0, TwTab<Rl> tw, in
     Ws<Rl> w;
     plan_ws<Rl>(I, smem, smem_bytes, w, tw, gscr ? gscr + (size_t)blockIdx.x * gstride : nullptr);
     if (threadIdx.x == 0) *w.flag = 0;
-    const int M = I.No / 2, nm = a.nmodes;
+    const int M = a.Mt, nm = a.nmodes;
     const int P = buf_split<Rl>(w.main_alt, M);
     const double* e = a.ems + (size_t)slot * nm;
     const cpx<Rl>* Et = reinterpret_cast<const cpx<Rl>*>(a.Et);
@@ -110,7 +113,8 @@ modal_node_kernel(const LunaInst* inst, ModalArgs a, int slot0, TwTab<Rl> tw, in
         x[i] = mk<Rl>((Rl)sx, (Rl)sy);
     }
     __syncthreads();
-    pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
+    if (I.kind == 1) pointwise_env<Rl>(I, w, x, P, I.in_scale);  // Kerr_env(_thg), RamanPolarEnv
+    else pointwise_real<Rl>(I, w, x, M, P, I.in_scale);
     cpx<Rl>* G = reinterpret_cast<cpx<Rl>*>(a.G) + (size_t)slot * nm * M;
     for (int m = 0; m < nm; ++m) {
         const double em = e[m];
@@ -130,11 +134,32 @@ __global__ void __launch_bounds__(256) modal_kerr2_kernel(const LunaInst* inst, 
     if (modal_skip(a)) return;
     const LunaInst& I = *inst;
     const int slot = slot0 + blockIdx.x;
-    const int M = I.No / 2, nm = a.nmodes, P = a.P, Lb = M / P;
+    const int M = a.Mt, nm = a.nmodes, P = a.P, Lb = M / P;
     const double* e = a.ems + (size_t)slot * nm * 2;
     const cpx<Rl>* Et = reinterpret_cast<const cpx<Rl>*>(a.Et);
     cpx<Rl>* G = reinterpret_cast<cpx<Rl>*>(a.G) + (size_t)slot * nm * M;
     const double sc = I.in_scale, kc = a.kerr;
+    if (I.kind == 1) {
+        // KerrVectorEnv! (Nonlinear.jl:52-63): slot i holds the complex sample n
+        for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < M; i += gridDim.y * blockDim.x) {
+            const int sp = Swz<Rl>::f(i);
+            const int n = (sp % Lb) * P + sp / Lb;
+            cpx<double> ex = mk<double>(0, 0), ey = mk<double>(0, 0);
+            for (int m = 0; m < nm; ++m) {
+                const cpx<double> v = cvt<double>(Et[(size_t)m * M + i]);
+                ex = ex + scale(e[2 * m], v);
+                ey = ey + scale(e[2 * m + 1], v);
+            }
+            ex = scale(sc, ex);
+            ey = scale(sc, ey);
+            const double ax = abs2(ex), ay = abs2(ey), f = 0.75 * kc, tw = __ldg(I.towin + n);
+            const cpx<double> px = scale(f, scale(ax + 2.0 / 3 * ay, ex) + scale(1.0 / 3, conj(ex) * (ey * ey)));
+            const cpx<double> py = scale(f, scale(ay + 2.0 / 3 * ax, ey) + scale(1.0 / 3, conj(ey) * (ex * ex)));
+            for (int m = 0; m < nm; ++m)
+                G[(size_t)m * M + i] = cvt<Rl>(scale(tw, scale(e[2 * m], px) + scale(e[2 * m + 1], py)));
+        }
+        return;
+    }
     for (int i = blockIdx.y * blockDim.x + threadIdx.x; i < M; i += gridDim.y * blockDim.x) {
         const int sp = Swz<Rl>::f(i);            // the swizzle is its own inverse
         const int n = (sp % Lb) * P + sp / Lb;   // inverse of split_pos
@@ -322,7 +347,7 @@ modal_level_kernel(const LunaInst* inst, ModalArgs a, int l, cpx<Rl>* B, TwTab<R
     const int c = blockIdx.x;
     Ws<Rl> w;
     plan_ws<Rl>(I, smem, smem_bytes, w, tw, gscr ? gscr + (size_t)c * gstride : nullptr);
-    const int M = I.No / 2, Nw = I.Nw, nm = a.nmodes;
+    const int M = a.Mt, Nw = I.Nw, nm = a.nmodes;
     const int ns = (2 << l) - 1;  // interior nodes of level l
     const double* wl = a.wts + (size_t)l * a.nslots;
     const cpx<Rl>* G = reinterpret_cast<const cpx<Rl>*>(a.G);
@@ -349,14 +374,16 @@ modal_level_kernel(const LunaInst* inst, ModalArgs a, int l, cpx<Rl>* B, TwTab<R
         }
         __syncthreads();
         const bool cmp = pass == 1;
-        r2c_to_freq<Rl>(w, x, M, Nw, [&](int k, cpx<double> X) {
+        auto st = [&](int k, cpx<double> X) {
             if (cmp) {
                 const cpx<double> o = ldg(of + k);
                 se += abs2((X - cvt<double>(Bc[k])) * o);
                 sv += abs2(X * o);
             }
             Bc[k] = cvt<Rl>(X);
-        });
+        };
+        if (I.kind == 1) env_to_freq<Rl>(I, w, x, st);
+        else r2c_to_freq<Rl>(w, x, M, Nw, st);
     }
     double unused = 0;
     block_sum3(se, sv, unused, w.red);

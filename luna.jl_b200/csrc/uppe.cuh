@@ -880,24 +880,14 @@ __device__ __forceinline__ void rhs_real(const LunaInst& I, Ws<Rl>& w, LoadF&& l
     r2c_to_freq<Rl>(w, x, M, I.Nw, [&](int k, cpx<double> X) { store(k, X * (zdep ? oz[k] : ldg(of + k))); });
 }
 
-// envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
-template <typename Rl, typename LoadF, typename StoreF>
-__device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
-    const int No = I.No, N = I.N, h = I.N / 2;
+// Et_to_Pt! and the time window for an envelope on the CTA's time buffer x (No complex
+// samples in split order P, field = sc * x): Kerr_env, Kerr_env_thg and RamanPolarEnv
+// (Nonlinear.jl:47-84, 296-333), in place.
+template <typename Rl>
+__device__ __noinline__ void pointwise_env(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, int P, double sc) {
+    const int No = I.No;
     const int T = LUNA_BLOCK;
     const int tid = threadIdx.x;
-    cpx<Rl>* buf = w.main;
-    for (int j = tid; j < No; j += T) {
-        cpx<double> X = mk<double>(0, 0);
-        if (j < h) X = load(j);
-        else if (j >= No - h) X = load(j - No + N);
-        buf[Swz<Rl>::f(j)] = cvt<Rl>(X);
-    }
-    __syncthreads();
-    cpx<Rl>* x = block_fft<Rl, true>(buf, w.main_alt, No, w.tw);  // E(t), split order
-    const int P = buf_split<Rl>(w.main_alt, No);
-    // field scale; a taper's at this node is in outz[Nw]
-    const double sc = I.grad ? I.outz[I.Nw].x : I.in_scale;
     int ir = -1;
     for (int i = 0; i < I.nresp; ++i)
         if (I.resp[i].kind == LUNA_RESP_RAMAN) ir = i;
@@ -937,15 +927,52 @@ __device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& lo
         x[pos] = cvt<Rl>(scale(__ldg(I.towin + n), Pt));
     }
     __syncthreads();
-    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, No, w.tw);
-    for (int k = tid; k < N; k += T) {
-        const int src = (k < h) ? k : (No - N + k);
-        cpx<double> X = cvt<double>(Z[Swz<Rl>::f(src)]);
-        // with a pressure gradient the factor at the current z (outz, plain loads)
-        store(k, X * (I.grad ? reinterpret_cast<const cpx<double>*>(I.outz)[k]
-                             : ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k)));
+}
+
+// envelope grid: to_time! of an Nw-bin spectrum with copy_scale_both! padding (the pad
+// scale is in the field scale), as No complex time samples in split order; returns the
+// buffer that holds them and their split factor in *P
+template <typename Rl, typename LoadF>
+__device__ __forceinline__ cpx<Rl>* env_to_time(const LunaInst& I, Ws<Rl>& w, LoadF&& load, int* P) {
+    const int No = I.No, N = I.N, h = I.N / 2;
+    cpx<Rl>* buf = w.main;
+    for (int j = threadIdx.x; j < No; j += LUNA_BLOCK) {
+        cpx<double> X = mk<double>(0, 0);
+        if (j < h) X = load(j);
+        else if (j >= No - h) X = load(j - No + N);
+        buf[Swz<Rl>::f(j)] = cvt<Rl>(X);
     }
     __syncthreads();
+    *P = buf_split<Rl>(w.main_alt, No);
+    return block_fft<Rl, true>(buf, w.main_alt, No, w.tw);  // E(t), split order
+}
+
+// envelope grid: to_freq! of the time buffer x (split order) into store(k, X), k < N
+template <typename Rl, typename StoreF>
+__device__ __forceinline__ void env_to_freq(const LunaInst& I, Ws<Rl>& w, cpx<Rl>* x, StoreF&& store) {
+    const int No = I.No, N = I.N, h = I.N / 2;
+    cpx<Rl>* buf = w.main;
+    cpx<Rl>* Z = block_fft<Rl, false>(x, w.main_alt ? ((x == buf) ? w.main_alt : buf) : nullptr, No, w.tw);
+    for (int k = threadIdx.x; k < N; k += LUNA_BLOCK) {
+        const int src = (k < h) ? k : (No - N + k);
+        store(k, cvt<double>(Z[Swz<Rl>::f(src)]));
+    }
+    __syncthreads();
+}
+
+// envelope grid (EnvGrid): complex transforms with copy_scale_both! padding
+template <typename Rl, typename LoadF, typename StoreF>
+__device__ __forceinline__ void rhs_env(const LunaInst& I, Ws<Rl>& w, LoadF&& load, StoreF&& store) {
+    int P;
+    cpx<Rl>* x = env_to_time<Rl>(I, w, load, &P);
+    // field scale; a taper's at this node is in outz[Nw]
+    const double sc = I.grad ? I.outz[I.Nw].x : I.in_scale;
+    pointwise_env<Rl>(I, w, x, P, sc);
+    // with a pressure gradient the factor at the current z (outz, plain loads)
+    env_to_freq<Rl>(I, w, x, [&](int k, cpx<double> X) {
+        store(k, X * (I.grad ? reinterpret_cast<const cpx<double>*>(I.outz)[k]
+                             : ldg(reinterpret_cast<const cpx<double>*>(I.outfac) + k)));
+    });
 }
 
 template <typename Rl, typename LoadF, typename StoreF>

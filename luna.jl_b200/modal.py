@@ -14,9 +14,10 @@ on time samples and one forward transform per mode and cubature level gives the 
 see ``modal_plan``. The cubature rule is fixed here on the host: the nested Clenshaw-Curtis
 levels of the p-adaptive rule, their nodes on (0, a) and weights.
 
-Not available on the device: ``full=true`` (the 2-D h-adaptive ``hcubature_v``; the
-transform describes it and the oracle evaluates it), envelope grids, Raman responses and the
-vector plasma response (two polarisation components with ionisation).
+On the device: Kerr, plasma and Raman for one polarisation component, Kerr and the vector
+plasma response for two. Not available on the device: ``full=true`` (the 2-D h-adaptive
+``hcubature_v``; the transform describes it and the oracle evaluates it), envelope grids,
+vector Raman (not implemented in the reference either) and the no-THG response forms.
 """
 import math
 
@@ -63,23 +64,32 @@ def norm_modal(grid, shock=True):
     return np.full(len(grid.ω), -1j * ω0 / 4)
 
 
-def make_const_linop_modes(grid, modes, λ0, ref_mode=1):
-    """``make_const_linop(grid::RealGrid, modes, λ0; ref_mode=1)`` (LinearOps.jl:401-415):
-    one column per mode, ``i(-β + ω β1) - α/2`` with β = 1 outside sidx and the frame
-    velocity of mode ``ref_mode`` (1-based) at λ0. Unlike the single-mode operator, bins
-    outside sidx are not zeroed."""
-    if grid.kind != "real":
-        raise NotImplementedError("the modal transform is available for field-resolved grids")
-    β1 = modes[ref_mode - 1].dispersion(1, pd.wlfreq(λ0))
+def make_const_linop_modes(grid, modes, λ0, ref_mode=1, thg=False):
+    """``make_const_linop(grid, modes, λ0; ref_mode=1)`` (LinearOps.jl:401-435): one column
+    per mode with β = 1 outside sidx and the frame velocity of mode ``ref_mode`` (1-based) at
+    λ0; ``i(-β + ω β1) - α/2`` on a field-resolved grid (α on sidx), and on an envelope grid
+    ``-i(β - (ω - ω0) β1 - βref) - α/2`` with βref = β(ω0) of the reference mode (0 with THG)
+    and α over every bin. Unlike the single-mode operator, bins outside sidx are not
+    zeroed."""
+    ω0 = pd.wlfreq(λ0)
+    β1 = modes[ref_mode - 1].dispersion(1, ω0)
     s = grid.sidx
+    env = grid.kind == "env"
+    βref = 0.0 if (not env or thg) else float(modes[ref_mode - 1].β(np.array([ω0]))[0])
     L = np.zeros((len(grid.ω), len(modes)), dtype=np.complex128)
     for i, m in enumerate(modes):
         β = np.ones(len(grid.ω))
         β[s] = m.β(grid.ω[s])
         α = np.zeros(len(grid.ω))
-        α[s] = m.α(grid.ω[s])
+        if env:
+            α = np.asarray(m.α(grid.ω), dtype=np.float64).copy()
+        else:
+            α[s] = m.α(grid.ω[s])
         α = np.clip(α, 0.0, 3000.0)
-        L[:, i] = 1j * (-β + grid.ω * β1) - α / 2
+        if env:
+            L[:, i] = -1j * (β - (grid.ω - grid.ω0) * β1 - βref) - α / 2
+        else:
+            L[:, i] = 1j * (-β + grid.ω * β1) - α / 2
     return L
 
 
@@ -142,8 +152,6 @@ class TransModal:
     kind = "modal"
 
     def __init__(self, grid, ts, resp, density, norm, rtol=1e-3, atol=0.0, mfcn=512, full=False):
-        if grid.kind != "real":
-            raise NotImplementedError("the modal transform is available for field-resolved grids")
         dl = [m.dimlimits() for m in ts.ms]
         if any(d[0] != "polar" for d in dl) or len({d[2][0] for d in dl}) != 1:
             raise NotImplementedError("modes must share polar limits (0, a)")
@@ -196,8 +204,9 @@ def doinput_mm(grid, inputs, nmodes):
 
 def setup_modal(grid, density, responses, inputs, modes, components, full=False, norm=None,
                 rtol=1e-3, atol=0.0, mfcn=512):
-    """``Luna.setup(grid::RealGrid, densityfun, responses, inputs, modes, components; full,
-    norm!, rtol, atol, mfcn)`` (Luna.jl:173-199) with a constant density: (Eω, transform)."""
+    """``Luna.setup(grid, densityfun, responses, inputs, modes, components; full, norm!,
+    rtol, atol, mfcn)`` (Luna.jl:173-227, field-resolved and envelope grids) with a constant
+    density: (Eω, transform)."""
     ts = ToSpace(modes, components=components)
     norm = norm_modal(grid) if norm is None else norm
     t = TransModal(grid, ts, responses, density, norm, rtol=rtol, atol=atol, mfcn=mfcn, full=full)

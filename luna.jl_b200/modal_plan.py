@@ -50,15 +50,19 @@ class ModalPlan:
         g, ts = t.grid, t.ts
         keep = []
         Nw, No, N = len(g.ω), g.No, g.N
-        Nwo = len(g.ωo)
-        pad = (Nwo - 1) / (Nw - 1)
-        crop = (Nw - 1) / (Nwo - 1)
+        if g.kind == "real":
+            Nwo = len(g.ωo)
+            pad = (Nwo - 1) / (Nw - 1)
+            crop = (Nw - 1) / (Nwo - 1)
+        else:  # copy_scale_both! (NonlinearRHS.jl:16-53)
+            pad = No / Nw
+            crop = Nw / No
         wwin = np.ascontiguousarray(g.ωwin, dtype=np.float64)
         towin = np.ascontiguousarray(g.towin, dtype=np.float64)
         twin = np.ascontiguousarray(g.twin, dtype=np.float64)
         keep += [wwin, towin, twin]
         gd = _lib.GridDesc()
-        gd.kind, gd.N, gd.Nw, gd.No = 0, N, Nw, No
+        gd.kind, gd.N, gd.Nw, gd.No = (0 if g.kind == "real" else 1), N, Nw, No
         gd.outfac = _lib.dptr(None)
         gd.wwin, gd.towin, gd.twin = _lib.dptr(wwin), _lib.dptr(towin), _lib.dptr(twin)
         gd.in_scale = pad / No

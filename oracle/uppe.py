@@ -288,11 +288,22 @@ def et_to_pt_modal(Er, resp, rho):
     for r in resp:
         if r.kind == "kerr_field":
             kerr_vector(Pr, Er, rho, r.γ3)
+        elif r.kind == "kerr_env":
+            kerr_vector_env(Pr, Er, rho, r.γ3)
         elif r.kind == "plasma":
             plasma_vector(Pr, Er, rho, r)
         else:
             raise NotImplementedError(r.kind)
     return Pr
+
+
+def kerr_vector_env(out, E, rho, g3):
+    """KerrVectorEnv! (Nonlinear.jl:52-63): E is the (n, 2) complex envelope."""
+    fac = rho * EPS0 * g3
+    Ex, Ey = E[:, 0], E[:, 1]
+    Ex2, Ey2 = np.abs(Ex) ** 2, np.abs(Ey) ** 2
+    out[:, 0] += 3 / 4 * fac * ((Ex2 + 2 / 3 * Ey2) * Ex + 1 / 3 * np.conj(Ex) * Ey ** 2)
+    out[:, 1] += 3 / 4 * fac * ((Ey2 + 2 / 3 * Ex2) * Ey + 1 / 3 * np.conj(Ey) * Ex ** 2)
 
 
 def clenshaw_curtis_moments(n):
@@ -423,14 +434,13 @@ def hcubature2(f, lo, hi, rtol, atol, maxevals):
 
 
 def trans_modal(t, Ew, z):
-    """(t::TransModal)(nl, Eω, z) (NonlinearRHS.jl:234-302) for a field-resolved grid: Ew is
+    """(t::TransModal)(nl, Eω, z) (NonlinearRHS.jl:234-302) for a field-resolved or envelope grid: Ew is
     (Nω, nmodes). Per point: to_space! (Modes.jl:458-495), to_time!, Et_to_Pt!, towin,
     to_freq!, ωwin, norm!, projection onto the modes (Prω Emsᵀ) and the weight (2πr at
     θ = 0 for full=false, r over (r, θ) for full=true); points on or outside (0, a) give
     zero."""
     g, ts = t.grid, t.ts
     Nw = Ew.shape[0]
-    Nwo = len(g.ωo)
     lo, hi = 0.0, t.a
     of = g.ωwin * t.norm
 
@@ -439,11 +449,10 @@ def trans_modal(t, Ew, z):
             return np.zeros_like(Ew)
         Ems = ts.ems(r, θ)                               # (nmodes, npol)
         Erω = Ew @ Ems                                   # (Nω, npol)
-        Erωo = np.zeros((Nwo, Erω.shape[1]), dtype=np.complex128)
-        Erωo[:Nw] = ((Nwo - 1) / (Nw - 1)) * Erω
-        Er = np.fft.irfft(Erωo, g.No, axis=0)
+        # to_time! / to_freq! per component (real: irfft/rfft; envelope: copy_scale_both!)
+        Er = np.stack([to_time(g, Erω[:, k]) for k in range(Erω.shape[1])], axis=1)
         Pr = et_to_pt_modal(Er, t.resp, t.density) * g.towin[:, None]
-        Prω = ((Nw - 1) / (Nwo - 1)) * np.fft.rfft(Pr, axis=0)[:Nw]
+        Prω = np.stack([to_freq(g, Pr[:, k], Nw) for k in range(Pr.shape[1])], axis=1)
         Prω = Prω * of[:, None]
         return 2 * math.pi * r * (Prω @ Ems.T)           # (Nω, nmodes)
 

@@ -20,9 +20,10 @@ import pytest
 
 from luna_b200 import _lib, fields, ionisation, modal, modal_plan, modes, raman
 from luna_b200 import physdata as pd
-from luna_b200.grid import RealGrid
+from luna_b200.grid import EnvGrid, RealGrid
 from luna_b200.linops import make_const_linop
-from luna_b200.nonlinear import Kerr_field, Kerr_field_nothg, PlasmaCumtrapz, RamanPolarField
+from luna_b200.nonlinear import (Kerr_env, Kerr_env_thg, Kerr_field, Kerr_field_nothg, PlasmaCumtrapz,
+                                 RamanPolarEnv, RamanPolarField)
 from luna_b200.nonlinearrhs import TransModeAvg, norm_mode_average
 from luna_b200.plan import solve_precon
 from oracle import uppe
@@ -37,6 +38,8 @@ def _rel(a, b):
 
 
 def _case(name, flength=1e-2):
+    if name.startswith("env_"):
+        return _env_case(name, flength)
     if name == "he11":
         a, gas, pres, trange, energy = 13e-6, "Ar", 5.0, 1e-12, 1e-6
         ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
@@ -78,7 +81,42 @@ def _case(name, flength=1e-2):
     return grid, Eω, t, modal.make_const_linop_modes(grid, ms, LAM0)
 
 
-@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"])
+def _env_case(name, flength):
+    """Envelope grids (basic_modal_env.jl): HE11 with Kerr_env; TM01 + HE21 on both
+    components with KerrVectorEnv!; HE11 + HE12 in H2 with Kerr_env and RamanPolarEnv; HE11
+    with Kerr_env_thg on a THG grid."""
+    thg = name == "env_thg"
+    grid = EnvGrid(flength, LAM0, (160e-9, 3000e-9), 1e-12, thg=thg)
+    if name == "env_vector":
+        a, gas, pres, energy = 13e-6, "Ar", 5.0, 1e-6
+        ms = (modes.MarcatiliMode(a, gas, pres, n=0, m=1, kind="TM", ϕ=0.0, loss=False),
+              modes.MarcatiliMode(a, gas, pres, n=2, m=1, kind="HE", ϕ=0.0, loss=False))
+        f1 = fields.GaussField(LAM0, 30e-15, energy=energy / 2)
+        f2 = fields.GaussField(LAM0, 30e-15, energy=energy / 5)
+        comps, inputs = "xy", ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)})
+    elif name == "env_raman":
+        a, gas, pres, energy = 50e-6, "H2", 2.0, 20e-6
+        ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, loss=False),
+              modes.MarcatiliMode(a, gas, pres, n=1, m=2, loss=False))
+        comps, inputs = "y", fields.GaussField(LAM0, 10e-15, energy=energy)
+    else:
+        a, gas, pres, energy = 13e-6, "Ar", 5.0, 1e-6
+        ms = (modes.MarcatiliMode(a, gas, pres, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
+        comps, inputs = "y", fields.GaussField(LAM0, 30e-15, energy=energy)
+    g3 = pd.gamma3_gas(gas)
+    resp = [Kerr_env_thg(g3, grid.ω0, grid.to) if thg else Kerr_env(g3)]
+    if name == "env_raman":
+        resp.append(RamanPolarEnv(grid.to, raman.raman_response(grid.to, gas)))
+    Eω, t = modal.setup_modal(grid, pd.density(gas, pres), resp, inputs, ms, comps)
+    if name == "env_raman":
+        Eω[:, 1] = 0.3 * Eω[:, 0]
+    return grid, Eω, t, modal.make_const_linop_modes(grid, ms, LAM0, thg=thg)
+
+
+_ENV = ["env_he11", "env_vector", "env_raman", "env_thg"]
+
+
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"] + _ENV)
 def test_modal_rhs_fp64_matches_oracle(name):
     """(t::TransModal)(nl, Eω, z) through the C ABI vs the oracle (NonlinearRHS.jl:284-302):
     the same number of cubature points and the integral within 1e-11. The device sums the
@@ -91,7 +129,7 @@ def test_modal_rhs_fp64_matches_oracle(name):
     t(nl, Ew, 0.0)
     ref = uppe.trans_modal(t, Ew, 0.0)
     assert t.plan().nevals == t.oracle_nevals
-    tol = 1e-11 if name in ("plasma", "vector_plasma", "raman") else 1e-12
+    tol = 1e-11 if name in ("plasma", "vector_plasma", "raman", "env_raman") else 1e-12
     assert _rel(nl, ref) < tol, _rel(nl, ref)
     # the device-pointer entry point gives the same numbers
     torch = pytest.importorskip("torch")
@@ -108,7 +146,7 @@ def test_modal_rhs_fp64_matches_oracle(name):
     assert np.array_equal(dev, nl)
 
 
-@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"])
+@pytest.mark.parametrize("name", ["he11", "vector", "plasma", "vector_plasma", "raman"] + _ENV)
 def test_modal_rhs_mixed_close_to_oracle(name):
     grid, Eω, t, _ = _case(name)
     plan = modal_plan.ModalPlan.from_transform(t, _lib.PREC_MIXED)
@@ -119,7 +157,8 @@ def test_modal_rhs_mixed_close_to_oracle(name):
 
 
 @pytest.mark.parametrize("name,flength", [("he11", 5e-3), ("vector", 2e-3), ("plasma", 1e-3),
-                                          ("vector_plasma", 1e-3), ("raman", 1e-3)])
+                                          ("vector_plasma", 1e-3), ("raman", 1e-3), ("env_he11", 5e-3),
+                                          ("env_vector", 2e-3), ("env_raman", 1e-3)])
 def test_modal_solve_replay_matches_oracle(name, flength):
     """Following the oracle's step sequence (replay), every saved field within 1e-10."""
     grid, Eω, t, L = _case(name, flength)

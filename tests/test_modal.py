@@ -17,9 +17,9 @@ from scipy import integrate, special
 
 from luna_b200 import fields, modal, modes
 from luna_b200 import physdata as pd
-from luna_b200.grid import RealGrid
+from luna_b200.grid import EnvGrid, RealGrid
 from luna_b200.linops import make_const_linop
-from luna_b200.nonlinear import Kerr_field
+from luna_b200.nonlinear import Kerr_env, Kerr_field
 from luna_b200.nonlinearrhs import TransModeAvg, norm_mode_average
 from oracle import uppe
 
@@ -242,6 +242,38 @@ def test_oracle_modal_single_mode_matches_mode_average():
     """test_multimode.jl:3-43 ("Radial") with the oracle on 1 cm: one HE11 mode with Kerr,
     mode-averaged and modal (radial integral), spectra within 0.003."""
     grid, m, dens, resp, inp = _radial_case(1e-2)
+    linop, βconst, _ = make_const_linop(grid, m, LAM0)
+    t0 = TransModeAvg(grid, resp, dens, norm_mode_average(grid, βconst), m.Aeff())
+    ms = (modes.MarcatiliMode(A, GAS, PRES, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)
+    Eωm, tm = modal.setup_modal(grid, dens, resp, inp, ms, "y")
+    Lm = modal.make_const_linop_modes(grid, ms, LAM0)
+    r0 = uppe.run(t0, grid, linop, inp(grid), saveN=11)
+    rm = uppe.run(tm, grid, Lm, Eωm, saveN=11)
+    Iω = np.abs(r0.Eω) ** 2
+    Iωr = np.abs(rm.Eω[:, :, 0]) ** 2
+    assert np.linalg.norm(Iω - Iωr) / np.linalg.norm(Iω) < 0.003
+
+
+@pytest.mark.parametrize("thg", [False, True])
+def test_envelope_modal_linop_matches_single_mode_on_sidx(thg):
+    """make_const_linop(grid::EnvGrid, modes, λ0; thg) (LinearOps.jl:417-435) for one mode is
+    the mode-averaged envelope operator on sidx (LinearOps.jl:266-300)."""
+    grid = EnvGrid(1e-2, 800e-9, (160e-9, 3000e-9), 1e-12, thg=thg)
+    m = modes.MarcatiliMode(A, GAS, PRES, loss=False)
+    L1, _, _ = make_const_linop(grid, m, LAM0, thg=thg)
+    Lm = modal.make_const_linop_modes(grid, (m,), LAM0, thg=thg)
+    s = grid.sidx
+    np.testing.assert_allclose(Lm[s, 0], L1[s], rtol=1e-14, atol=0)
+
+
+def test_oracle_envelope_modal_single_mode_matches_mode_average():
+    """The "Radial" comparison of test_multimode.jl on an envelope grid with the oracle: HE11
+    with Kerr_env, mode-averaged and modal (radial integral) spectra within 0.003."""
+    grid = EnvGrid(1e-2, 800e-9, (160e-9, 3000e-9), 1e-12)
+    m = modes.MarcatiliMode(A, GAS, PRES, loss=False)
+    dens = pd.density(GAS, PRES)
+    resp = (Kerr_env(pd.gamma3_gas(GAS)),)
+    inp = fields.GaussField(LAM0, TAU, energy=1e-6)
     linop, βconst, _ = make_const_linop(grid, m, LAM0)
     t0 = TransModeAvg(grid, resp, dens, norm_mode_average(grid, βconst), m.Aeff())
     ms = (modes.MarcatiliMode(A, GAS, PRES, n=1, m=1, kind="HE", ϕ=0.0, loss=False),)

@@ -142,8 +142,6 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         RealGrid(flength, λ0, λlims, trange, δt)
     if not isinstance(modes_, str) or parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
         if isinstance(modes_, (int, tuple, list)):
-            if envelope:
-                raise NotImplementedError("multimode envelope propagation is not supported")
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
@@ -222,10 +220,14 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
         raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
     pol = needpol_modes(modes_)
     ms = makemode_s(modes_, radius, gas, pressure, temperature, model, loss, pol)
-    thg = True if thg is None else thg
-    plasma = True if plasma is None else plasma
+    env = grid.kind == "env"
+    thg = (not env) if thg is None else thg
+    plasma = (not env) if plasma is None else plasma
     resp = []
-    if kerr:
+    if kerr and env:  # makeresponse for EnvGrid (Interface.jl:592-605)
+        resp.append(Kerr_env_thg(pd.gamma3_gas(gas), pd.wlfreq(grid.referenceλ), grid.to) if thg else
+                    Kerr_env(pd.gamma3_gas(gas)))
+    elif kerr:
         resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
                     Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
     if plasma:
@@ -238,16 +240,15 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     if raman is None:
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
-        resp.append(RamanPolarField(grid.to, _raman.raman_response(grid.to, gas, rotation=rotation,
-                                                                   vibration=vibration, temp=temperature),
-                                    thg=thg))
+        rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
+        resp.append(RamanPolarEnv(grid.to, rr) if env else RamanPolarField(grid.to, rr, thg=thg))
     if pulseshape == "gauss":
         fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
     else:
         fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
     Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
-    return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0), t, saveN)
+    return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0, thg=thg), t, saveN)
 
 
 def prop_capillary(*args, precision=None, **kwargs):

@@ -286,6 +286,19 @@ def test_oracle_envelope_modal_single_mode_matches_mode_average():
     assert np.linalg.norm(Iω - Iωr) / np.linalg.norm(Iω) < 0.003
 
 
+def test_prop_capillary_multimode_envelope():
+    """prop_capillary(modes=2, envelope=true): an EnvGrid without THG, Kerr_env (and
+    RamanPolarEnv for a molecular gas), no plasma; the envelope multimode operator."""
+    from luna_b200.interface import prop_capillary_args
+    kw = dict(λ0=800e-9, τfwhm=30e-15, energy=1e-6, λlims=(160e-9, 3000e-9), trange=1e-12)
+    p = prop_capillary_args(13e-6, 1e-2, "Ar", 5.0, modes=2, envelope=True, **kw)
+    assert p.grid.kind == "env" and p.transform.kind == "modal"
+    assert [r.kind for r in p.transform.resp] == ["kerr_env"]
+    assert p.linop.shape == (len(p.grid.ω), 2)
+    h = prop_capillary_args(50e-6, 1e-2, "H2", 2.0, modes=2, envelope=True, **kw)
+    assert [r.kind for r in h.transform.resp] == ["kerr_env", "raman_env"]
+
+
 def test_oracle_vector_plasma_reduces_to_scalar_and_rotates():
     """PlasmaVector! (Nonlinear.jl:144-162): a field on one component gives the scalar
     response on it and nothing on the other; rotating the field vector rotates the

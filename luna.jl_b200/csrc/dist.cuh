@@ -167,6 +167,24 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
         }
     }
     dsync();
+    if constexpr (R == 8) {
+        // join, transposed: this CTA takes the n1 of its slice [p S, (p + 1) S), S = Mbc/R,
+        // gathers B_r[n1] from every CTA, forms x[n1 + Mbc q] = sum_r W_R^{-r q} B_r[n1] for
+        // every q with one in-register DFT and stores each into CTA q's block. Each CTA reads
+        // Mbc values instead of R Mbc; the stores are visible after the closing barrier.
+        const int S = Mbc / R, n1b = p * S;
+        for (int j = tid; j < S; j += T) {
+            const int pos = Swz<Rl>::f(n1b + j);
+            cpx<Rl> v[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = drem(d.fb, bitrev<R>(i))[pos];
+            dft_br<Rl, true, R>(v);
+#pragma unroll
+            for (int q = 0; q < R; ++q) drem(d.tb, q)[pos] = v[q];
+        }
+        dsync();
+        return;
+    }
     // join: x[n1 + Mbc q] = sum_r W_R^{-r q} B_r[n1], q = this CTA
     const cpx<Rl>* fr[R];
     cpx<Rl> wq[R];
@@ -206,6 +224,24 @@ __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store
     const int Mbc = Mc / R;
     const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<R>();
     dsync();
+    if constexpr (R == 8) {
+        // radix-R step, transposed: this CTA takes the n1 of its slice, gathers every CTA's
+        // block at n1, forms y_r = W_M^{r n1} sum_q W_R^{r q} x[n1 + Mbc q] for every r with
+        // one in-register DFT and stores each into CTA r's sub-transform buffer
+        const int S = Mbc / R, n1b = p * S;
+        for (int j = tid; j < S; j += T) {
+            const int n1 = n1b + j;
+            const int pos = Swz<Rl>::f(n1);
+            cpx<Rl> v[R];
+#pragma unroll
+            for (int i = 0; i < R; ++i) v[i] = drem(d.tb, bitrev<R>(i))[pos];
+            dft_br<Rl, false, R>(v);
+            drem(d.fb, 0)[pos] = v[0];
+#pragma unroll
+            for (int r = 1; r < R; ++r) drem(d.fb, r)[pos] = v[r] * tw_pow<Rl, false>(d.tw, (unsigned)(r * n1), lgM);
+        }
+        dsync();
+    } else {
     const cpx<Rl>* tr[R];
     cpx<Rl> wq[R];
 #pragma unroll
@@ -233,6 +269,7 @@ __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store
         }
     }
     __syncthreads();
+    }
     sub_fft_any<Rl, false>(d.fb, Mbc, d.tw);
     dsync();
     const int po = (R - p) % R;
@@ -276,6 +313,41 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
     const int Mb = M / R, Mr = 2 * M;
     const int lgMr = ilog2i((unsigned)Mr), lg2R = ilog2c<R>() + 1;
     const int pa = (c == 0) ? 0 : c, pb = (c == 0) ? R : 2 * R - c;
+    const Rl s = (Rl)sc;
+    if constexpr (R == 8) {
+        // the radix-2R step, transposed: this CTA takes the n1 of its slice, squares every
+        // CTA's field pair at n1, forms X_f = sum_q W_2R^{f q} z[n1 + Mb q] for all 2R
+        // sub-transforms f with one in-register DFT (z is zero for q >= R) and stores
+        // X_f W_2M^{f n1} into the buffer of the CTA that owns f (f = c and 2R - c of CTA c,
+        // 0 and R of CTA 0)
+        constexpr int R2 = 2 * R;
+        const int S = Mb / R, n1b = c * S;
+        for (int j = tid; j < S; j += T) {
+            const int n1 = n1b + j;
+            const int pos = Swz<Rl>::f(n1);
+            cpx<Rl> v[R2];
+#pragma unroll
+            for (int i = 0; i < R2; ++i) {
+                const int q = bitrev<R2>(i);
+                if (q < R) {
+                    const cpx<Rl> e = drem(d.tb, q)[pos];
+                    const Rl e0 = e.x * s, e1 = e.y * s;
+                    v[i] = mk<Rl>(e0 * e0, e1 * e1);
+                } else {
+                    v[i] = mk<Rl>(0, 0);
+                }
+            }
+            dft_br<Rl, false, R2>(v);
+            drem(d.rb0, 0)[pos] = v[0];
+            drem(d.rb1, 0)[pos] = v[R] * tw_pow<Rl, false>(d.tw, (unsigned)(R * n1), lgMr);
+#pragma unroll
+            for (int cc = 1; cc < R; ++cc) {
+                drem(d.rb0, cc)[pos] = v[cc] * tw_pow<Rl, false>(d.tw, (unsigned)(cc * n1), lgMr);
+                drem(d.rb1, cc)[pos] = v[R2 - cc] * tw_pow<Rl, false>(d.tw, (unsigned)((R2 - cc) * n1), lgMr);
+            }
+        }
+        dsync();
+    } else {
     const cpx<Rl>* tr[R];
     cpx<Rl> wa[R], wb[R];
 #pragma unroll
@@ -284,7 +356,6 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
         wa[q] = tw_pow<Rl, false>(d.tw, (unsigned)(pa * q), lg2R);
         wb[q] = tw_pow<Rl, false>(d.tw, (unsigned)(pb * q), lg2R);
     }
-    const Rl s = (Rl)sc;
     for (int n0 = tid; n0 < Mb; n0 += DUnr<R>::v * T) {
       cpx<Rl> ev[DUnr<R>::v][R];
 #pragma unroll
@@ -318,6 +389,7 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
       }
     }
     __syncthreads();
+    }
     sub_fft2<Rl, false, 8>(d.rb0, d.rb1, Mb, d.tw);
     // pairs (f, Mr - f) with f = 2R k + p; Zk/Zm are entries of the complex transform
     const cpx<Rl>* H = reinterpret_cast<const cpx<Rl>*>(rr.H);
@@ -422,6 +494,32 @@ struct RamanOut {
         return acc;
     }
 };
+
+// RamanOut::block transposed for clusters of 8: this CTA takes the n1 of its slice
+// [r S, (r + 1) S), S = Mb/R, gathers the 2R sub-transform values B_p[n1] (two per CTA),
+// forms P[n1 + Mb q] = sum_p W_2R^{-p q} B_p[n1] for every q with one in-register DFT and
+// stores each into CTA q's out. Each CTA reads 2 Mb values instead of 2 R Mb; the stores
+// are visible to CTA q after the next cluster barrier.
+template <typename Rl, int R>
+__device__ __forceinline__ void raman_out_scatter(DWs<Rl>& d, cpx<Rl>* out, int Mb) {
+    constexpr int R2 = 2 * R;
+    const int S = Mb / R, n1b = d.rank * S;
+    for (int j = threadIdx.x; j < S; j += LUNA_BLOCK) {
+        const int pos = Swz<Rl>::f(n1b + j);
+        cpx<Rl> x[R2];
+#pragma unroll
+        for (int c = 0; c < R; ++c) {
+            x[c] = drem(d.rb0, c)[pos];
+            x[c == 0 ? R : R2 - c] = drem(d.rb1, c)[pos];
+        }
+        cpx<Rl> v[R2];
+#pragma unroll
+        for (int i = 0; i < R2; ++i) v[i] = x[bitrev<R2>(i)];
+        dft_br<Rl, true, R2>(v);
+#pragma unroll
+        for (int q = 0; q < R; ++q) drem(out, q)[pos] = v[q];
+    }
+}
 
 // ------------------------------------------------------------------ plasma
 // The rate-function parameters in registers (ppt_rate<float> / adk_rate<float> with the
@@ -529,10 +627,15 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     }
     dsync();  // totals published; Raman sub-transforms ready; field blocks no longer read
     if (ir >= 0) {
-        // the Raman polarisation of this block into tb (the field now lives in ev)
-        RamanOut<Rl, R> ro;
-        ro.init(d);
-        ro.block(d.tb, Mb);
+        // the Raman polarisation of this block into tb (the field now lives in ev); with the
+        // transposed form other CTAs write it, visible after the next barriers below
+        if constexpr (R == 8) {
+            raman_out_scatter<Rl, R>(d, d.tb, Mb);
+        } else {
+            RamanOut<Rl, R> ro;
+            ro.init(d);
+            ro.block(d.tb, Mb);
+        }
     }
     double c1 = 0;
     for (int j = 0; j < q; ++j) c1 += drem(d.xs, j)[0];
@@ -662,10 +765,16 @@ __device__ __noinline__ void dist_pointwise(const LunaInst& I, DWs<Rl>& d, int M
     if (ir >= 0) dist_raman_fwd<Rl, R>(I.resp[ir], d, M, sc);
     if (ip < 0) {
         dsync();  // every CTA's Raman sub-transforms ready; every read of the field blocks done
-        RamanOut<Rl, R> ro;
-        ro.init(d);
-        ro.block(d.fb, Mb);  // the sub-transform buffer is free after the barrier above
-        __syncthreads();
+        // the sub-transform buffer is free after the barrier above
+        if constexpr (R == 8) {
+            raman_out_scatter<Rl, R>(d, d.fb, Mb);
+            dsync();  // every CTA's stores into this block
+        } else {
+            RamanOut<Rl, R> ro;
+            ro.init(d);
+            ro.block(d.fb, Mb);
+            __syncthreads();
+        }
         for (int n1 = tid; n1 < Mb; n1 += T) {
             const int pos = Swz<Rl>::f(n1);
             const cpx<Rl> e = d.tb[pos];

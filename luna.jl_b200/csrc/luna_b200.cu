@@ -2180,15 +2180,17 @@ int luna_b200_modal_plan_create(const luna_grid_desc* g, const luna_resp_desc* r
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: the no-THG response forms are not available for the modal transform");
         if (md->npol == 2 && k == LUNA_RESP_RAMAN)
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: vector Raman is not implemented (as in the reference)");
-        if (md->npol == 2 && k != LUNA_RESP_KERR_FIELD && k != LUNA_RESP_PLASMA_PPT && k != LUNA_RESP_PLASMA_ADK)
+        if (md->npol == 2 && k != LUNA_RESP_KERR_FIELD && k != LUNA_RESP_KERR_ENV && k != LUNA_RESP_PLASMA_PPT &&
+            k != LUNA_RESP_PLASMA_ADK)
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: two polarisation components support Kerr and plasma");
+        // (Kerr_env_thg is a scalar form: two components take Kerr_env, KerrVectorEnv!)
         if (g->kind == 1 && (k == LUNA_RESP_PLASMA_PPT || k == LUNA_RESP_PLASMA_ADK))
             return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: no plasma response for envelope fields (as in the reference)");
         if (md->npol == 2 && (k == LUNA_RESP_PLASMA_PPT || k == LUNA_RESP_PLASMA_ADK)) {
             if (vplasma) return fail(LUNA_ERR_UNSUPPORTED, "modal_plan_create: at most one plasma response");
             vplasma = true;
         }
-        if (k == LUNA_RESP_KERR_FIELD) kerr += resps[i].coef;
+        if (k == LUNA_RESP_KERR_FIELD || k == LUNA_RESP_KERR_ENV) kerr += resps[i].coef;
     }
     // the point plan: grid and responses; its output factor is unused (the modal one is
     // applied after the cubature)

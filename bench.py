@@ -839,6 +839,9 @@ def main():
                     help="relative tolerance of the mixed-precision integrations")
     ap.add_argument("--no-autotune", action="store_true",
                     help="shapes from the fixed work-estimate rule instead of the measured autotuner")
+    ap.add_argument("--cluster-shape", type=int, choices=[0, 2, 3], default=0,
+                    help="profiling aid with --no-autotune: every instance that may run distributed "
+                         "runs on a cluster of 8 (2) or 16 (3) CTAs; 0: the work-estimate rule")
     ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64",
                     help="precision of the timed batched scan (the other one is run once and "
                          "reported beside it when the accuracy pass is on)")
@@ -938,6 +941,8 @@ def main():
         tune = {"ms_per_rk_step": table, "tune_s": round(tune_s, 1), "cluster_shapes": int((shapes == 2).sum()),
                 "rule": "cluster when faster for the class and the predicted single-CTA time is above the mean SM load"}
     else:
+        if args.cluster_shape:
+            batch.set_shapes(np.full(len(probs), args.cluster_shape, dtype=int))
         batch.set_priority(prios)
     kinfo = batch.info()
     for _ in range(args.warmup):

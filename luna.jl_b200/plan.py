@@ -295,7 +295,8 @@ class Batch:
 
     def set_shapes(self, shapes):
         """Per-instance shape for the next set_priority: 0 decided by the work estimates,
-        1 one CTA, 2 a cluster (when eligible); None restores 0 for all."""
+        1 one CTA, 2 a cluster of 8, 3 a cluster of 16 (when eligible); None restores 0 for
+        all."""
         if shapes is None:
             _lib.check(_lib.load().luna_b200_batch_set_shapes(self._h, None))
             return

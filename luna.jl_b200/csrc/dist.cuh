@@ -183,8 +183,7 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
             for (int q = 0; q < R; ++q) drem(d.tb, q)[pos] = v[q];
         }
         dsync();
-        return;
-    }
+    } else {
     // join: x[n1 + Mbc q] = sum_r W_R^{-r q} B_r[n1], q = this CTA
     const cpx<Rl>* fr[R];
     cpx<Rl> wq[R];
@@ -211,6 +210,7 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
         }
     }
     __syncthreads();
+    }
 }
 
 // to_freq! of the sample pairs in tb (every CTA's block): radix-R step, Mbc-point forward

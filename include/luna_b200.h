@@ -343,7 +343,7 @@ int luna_b200_radial_rhs_device(luna_radial_plan* plan, double* nl_dev, const do
  * (ldiv!, k -> r) — Hankel.jl's QDHT as called at NonlinearRHS.jl:468, 471. X and Y hold
  * complex FP64 for LUNA_PREC_FP64 plans and complex FP32 for LUNA_PREC_MIXED plans (where
  * the product runs as 3xBF16 tensor-core MMAs with FP32 accumulation); they must not
- * overlap. Enqueued on `stream`. */
+ * overlap and must be 8-byte aligned (LUNA_ERR_BAD_ARG otherwise). Enqueued on `stream`. */
 int luna_b200_qdht_device(luna_radial_plan* plan, void* Y_dev, const void* X_dev, int forward, void* stream);
 /* RK45.solve_precon driven by Luna.run (Luna.jl:358-391) for a radial problem: linop and
  * y_inout are Nw*Nr complex (LinearOps.make_const_linop(grid, q, nfun), LinearOps.jl:130-144),

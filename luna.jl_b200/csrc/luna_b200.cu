@@ -1563,6 +1563,10 @@ int luna_b200_solve(luna_plan* p, const double* linop, double* y_inout, double z
 // ===================================================================== radial transform
 }  // extern "C"
 
+// Columns of one tensor-core QDHT tile: 32 gives 2 x ceil(2Nw/128) x Nr/64 CTAs (136 for
+// Nw = 1025, Nr = 256 on 148 SMs).
+#define RAD_TC_BN 32
+
 struct luna_radial_plan {
     int precision = 0;
     int Nw = 0, Nr = 0;
@@ -1571,8 +1575,9 @@ struct luna_radial_plan {
     std::vector<void*> allocs;
     const double* Mi = nullptr;      // [Nr*Nr] row-major QDHT k -> r
     const double* Mf = nullptr;      // [Nr*Nr] row-major QDHT r -> k
-    // mixed precision: BF16 hi/lo splits of the QDHT matrices for the tensor-core products
-    const __nv_bfloat16 *Mi_hi = nullptr, *Mi_lo = nullptr, *Mf_hi = nullptr, *Mf_lo = nullptr;
+    // mixed precision: BF16 hi/lo splits of the QDHT matrices, pre-tiled for the
+    // tensor-core products (tc_btile_index<RAD_TC_BN>)
+    const __nv_bfloat16 *Mi_t = nullptr, *Mf_t = nullptr;
     const double2* outfac = nullptr; // [Nw*Nr]
     char* gscr = nullptr;            // per-column scratch when a column does not fit in shared memory
     size_t gstride = 0;
@@ -1610,7 +1615,6 @@ int rad_column_setup(luna_radial_plan* p) {
 
 int rad_grid(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 8); }
 
-#define RAD_TC_BN 64
 
 uint16_t bf16_rne(float f) {
     uint32_t b;
@@ -1637,8 +1641,7 @@ int rad_qdht(luna_radial_plan* p, const void* X, bool fwd, void* Y, const RadSta
         dim3 g((rows + TC_BM - 1) / TC_BM, p->Nr / RAD_TC_BN);
         const int* fin = st ? (const int*)((const char*)st + offsetof(RadState, finished)) : nullptr;
         tc_gemm_3xbf16<RAD_TC_BN><<<g, TC_THREADS, tc_smem_bytes<RAD_TC_BN>(), s>>>(
-            (const float*)X, rows, rows, fwd ? p->Mf_hi : p->Mi_hi, fwd ? p->Mf_lo : p->Mi_lo, (float*)Y, p->Nr,
-            fin, flags);
+            (const float*)X, rows, rows, fwd ? p->Mf_t : p->Mi_t, (float*)Y, p->Nr, fin, flags);
     }
     return LUNA_OK;
 }
@@ -1715,19 +1718,24 @@ int luna_b200_radial_plan_create(const luna_grid_desc* g, const luna_resp_desc* 
         return bail(LUNA_ERR_CUDA);
     p->outfac = (const double2*)tmp;
     if (precision == LUNA_PREC_MIXED) {
-        std::vector<uint16_t> h(nn), l(nn);
+        // B[n, m] = M[n*Nr + m] (row-major Nr x Nr), split into hi and lo and laid out in
+        // the tiles the tensor-core kernel copies whole into shared memory
+        std::vector<uint16_t> t(2 * nn);
         const double* src[2] = {rd->Mi, rd->Mf};
-        const __nv_bfloat16** dh[2] = {&p->Mi_hi, &p->Mf_hi};
-        const __nv_bfloat16** dl[2] = {&p->Mi_lo, &p->Mf_lo};
+        const __nv_bfloat16** dt[2] = {&p->Mi_t, &p->Mf_t};
+        const size_t lo_off = (size_t)RAD_TC_BN * TC_KC;
         for (int w = 0; w < 2; ++w) {
-            for (size_t j = 0; j < nn; ++j) {
-                h[j] = bf16_rne((float)src[w][j]);
-                l[j] = bf16_rne((float)(src[w][j] - (double)bf16_val(h[j])));
-            }
-            const uint16_t *th = nullptr, *tl = nullptr;
-            if (upload(p->allocs, h.data(), nn, &th) || upload(p->allocs, l.data(), nn, &tl)) return bail(LUNA_ERR_CUDA);
-            *dh[w] = (const __nv_bfloat16*)th;
-            *dl[w] = (const __nv_bfloat16*)tl;
+            for (int n = 0; n < p->Nr; ++n)
+                for (int m = 0; m < p->Nr; ++m) {
+                    const double x = src[w][(size_t)n * p->Nr + m];
+                    const uint16_t h = bf16_rne((float)x);
+                    const size_t i = tc_btile_index<RAD_TC_BN>(n, m, p->Nr);
+                    t[i] = h;
+                    t[i + lo_off] = bf16_rne((float)(x - (double)bf16_val(h)));
+                }
+            const uint16_t* d = nullptr;
+            if (upload(p->allocs, t.data(), 2 * nn, &d)) return bail(LUNA_ERR_CUDA);
+            *dt[w] = (const __nv_bfloat16*)d;
         }
         if (cudaFuncSetAttribute(tc_gemm_3xbf16<RAD_TC_BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  tc_smem_bytes<RAD_TC_BN>()) != cudaSuccess)
@@ -1836,6 +1844,8 @@ int luna_b200_radial_linop(luna_radial_plan* p, double z, double* linop, double*
 
 int luna_b200_qdht_device(luna_radial_plan* p, void* Y_dev, const void* X_dev, int forward, void* stream) {
     if (!p || !Y_dev || !X_dev || X_dev == Y_dev) return fail(LUNA_ERR_BAD_ARG, "qdht_device: null or aliased argument");
+    if (((uintptr_t)X_dev | (uintptr_t)Y_dev) & 7)
+        return fail(LUNA_ERR_BAD_ARG, "qdht_device: X and Y must be 8-byte aligned");
     rad_qdht(p, X_dev, forward != 0, Y_dev, nullptr, p->d_flags, (cudaStream_t)stream);
     CK(cudaGetLastError());
     return LUNA_OK;

@@ -279,11 +279,13 @@ def test_radial_mixed_rejects_nr_not_multiple_of_64():
 
 @pytest.mark.parametrize("prec,tol", [(_lib.PREC_FP64, 1e-13), (_lib.PREC_MIXED, 3e-5)])
 @pytest.mark.parametrize("forward", [True, False])
-def test_qdht_device_matches_matrix_product(prec, tol, forward):
+@pytest.mark.parametrize("N", [128, 256])
+def test_qdht_device_matches_matrix_product(prec, tol, forward, N):
     """luna_b200_qdht_device: the plan's Hankel transform along the radial index (mul!/ldiv!
-    of Hankel.jl's QDHT), FP64 CUDA-core tiles or 3xBF16 tensor-core products."""
+    of Hankel.jl's QDHT), FP64 CUDA-core tiles or 3xBF16 tensor-core products (N = 128: two
+    64-deep K chunks, fewer than the kernel's prefetch ring; N = 256: four, more than it)."""
     torch = pytest.importorskip("torch")
-    p = prop_radial_args("Ar", 1.2, R=1e-3, N=128, flength=0.01, λ0=800e-9,
+    p = prop_radial_args("Ar", 1.2, R=1e-3, N=N, flength=0.01, λ0=800e-9,
                          λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
                          energy=1e-6, w0=40e-6, plasma=False)
     plan = radial_plan.RadialPlan.from_transform(p.transform, prec)
@@ -302,3 +304,19 @@ def test_qdht_device_matches_matrix_product(prec, tol, forward):
     torch.cuda.synchronize()
     Y = dY.cpu().numpy().view(ct).reshape(Xc.shape).T.astype(np.complex128)
     assert _rel(Y, ref) < tol, _rel(Y, ref)
+
+
+def test_qdht_device_rejects_unaligned_arrays():
+    """The entry point checks the alignment of X and Y on the host, before any launch."""
+    torch = pytest.importorskip("torch")
+    p = prop_radial_args("Ar", 1.2, R=1e-3, N=64, flength=0.01, λ0=800e-9,
+                         λlims=(400e-9, 2000e-9), trange=0.2e-12, τfwhm=20e-15,
+                         energy=1e-6, w0=40e-6, plasma=False)
+    plan = radial_plan.RadialPlan.from_transform(p.transform, _lib.PREC_MIXED)
+    n = 2 * p.Eω.size
+    dX = torch.zeros(n + 2, dtype=torch.float32, device="cuda")
+    dY = torch.zeros(n + 2, dtype=torch.float32, device="cuda")
+    s = _lib.ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    rc = _lib.load().luna_b200_qdht_device(plan.handle, _lib.ctypes.c_void_p(dY.data_ptr()),
+                                           _lib.ctypes.c_void_p(dX.data_ptr() + 4), 1, s)
+    assert rc == _lib.LUNA_ERR_BAD_ARG

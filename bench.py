@@ -300,10 +300,11 @@ def cpu_estimate(sample_seconds=20.0, workers=1, pool=None):
 
 def plain_fp64_measured(inst, probs, dur, status64, k=8):
     """The plain FP64 drop-in, measured: one single-instance FP64 solve after another (a
-    batch of one, as luna_b200_solve runs it: on an 8-CTA cluster for the long grids, No >=
-    16384, on one CTA otherwise), device time with CUDA events, for a stratified subset of
-    the completed instances: in each of the two strata (cluster, single CTA) k quantiles of
-    their integration times in the single-CTA FP64 batch. Returns the subset's own
+    batch of one, as luna_b200_solve runs it: on a cluster for the long grids, 16 CTAs for
+    No = 32768 and 8 for No = 16384, on one CTA otherwise), device time with CUDA events, for
+    a stratified subset of the completed instances: in each of the two strata (cluster,
+    single CTA) k quantiles of their integration times in the single-CTA FP64 batch.
+    Returns the subset's own
     sims/hour, the scan estimate (per stratum, the batch's per-instance times scaled by the
     subset's measured/batch ratio) and the per-instance record."""
     done = [i for i in range(len(probs)) if status64[i] == 0]
@@ -1054,7 +1055,7 @@ def main():
                 v_sub, v_scan, rows = plain_fp64_measured(inst, probs, dur64, [x.status for x in st64])
                 plain = {"value": v_scan, "unit": "sims/hour", "subset_value": v_sub,
                          "method": ("plain FP64 drop-in measured: one single-instance FP64 solve after another "
-                                    f"(device time; 8-CTA clusters for No >= 16384) for {len(rows)} instances, "
+                                    f"(device time; clusters of 16 CTAs for No = 32768, of 8 for No = 16384) for {len(rows)} instances, "
                                     "8 quantiles of the single-CTA FP64 batch time in each of the two strata; value = "
                                     "the scan's sims/hour with each stratum's per-instance batch times scaled by its "
                                     "subset's measured/batch ratio, subset_value = the subset's own"),

@@ -167,7 +167,7 @@ __device__ __noinline__ void dist_c2r(DWs<Rl>& d, int Mc, int Nw, LoadF&& load) 
         }
     }
     dsync();
-    if constexpr (R == 8) {
+    if constexpr (R == 8 || R == 16) {
         // join, transposed: this CTA takes the n1 of its slice [p S, (p + 1) S), S = Mbc/R,
         // gathers B_r[n1] from every CTA, forms x[n1 + Mbc q] = sum_r W_R^{-r q} B_r[n1] for
         // every q with one in-register DFT and stores each into CTA q's block. Each CTA reads
@@ -224,7 +224,7 @@ __device__ __noinline__ void dist_r2c(DWs<Rl>& d, int Mc, int Nw, StoreF&& store
     const int Mbc = Mc / R;
     const int lgM = ilog2i((unsigned)Mc), lgR = ilog2c<R>();
     dsync();
-    if constexpr (R == 8) {
+    if constexpr (R == 8 || R == 16) {
         // radix-R step, transposed: this CTA takes the n1 of its slice, gathers every CTA's
         // block at n1, forms y_r = W_M^{r n1} sum_q W_R^{r q} x[n1 + Mbc q] for every r with
         // one in-register DFT and stores each into CTA r's sub-transform buffer
@@ -344,6 +344,37 @@ __device__ __noinline__ void dist_raman_fwd(const LunaResp& rr, DWs<Rl>& d, int 
             for (int cc = 1; cc < R; ++cc) {
                 drem(d.rb0, cc)[pos] = v[cc] * tw_pow<Rl, false>(d.tw, (unsigned)(cc * n1), lgMr);
                 drem(d.rb1, cc)[pos] = v[R2 - cc] * tw_pow<Rl, false>(d.tw, (unsigned)((R2 - cc) * n1), lgMr);
+            }
+        }
+        dsync();
+    } else if constexpr (R == 16) {
+        // the same transposed step with the 2R-point DFT as two R-point ones (a 2R-point
+        // one does not fit in registers): z is zero for q >= R, so
+        // X_{2g+e} = sum_{q<R} W_R^{g q} (W_2R^{e q} z_q), e = 0, 1; each half gathers the
+        // squares again instead of holding them
+        const int S = Mb / R, n1b = c * S;
+        for (int j = tid; j < S; j += T) {
+            const int n1 = n1b + j;
+            const int pos = Swz<Rl>::f(n1);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                cpx<Rl> v[R];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int q = bitrev<R>(i);
+                    const cpx<Rl> ev = drem(d.tb, q)[pos];
+                    const Rl e0 = ev.x * s, e1 = ev.y * s;
+                    v[i] = mk<Rl>(e0 * e0, e1 * e1);
+                    if (e && q) v[i] = v[i] * tw_pow<Rl, false>(d.tw, (unsigned)q, lg2R);
+                }
+                dft_br<Rl, false, R>(v);
+#pragma unroll
+                for (int g = 0; g < R; ++g) {
+                    const int f = 2 * g + e;  // sub-transform f: rb0 of CTA f (f < R), rb1 of CTA 2R - f
+                    if (f == 0) drem(d.rb0, 0)[pos] = v[g];
+                    else if (f < R) drem(d.rb0, f)[pos] = v[g] * tw_pow<Rl, false>(d.tw, (unsigned)(f * n1), lgMr);
+                    else drem(d.rb1, f == R ? 0 : 2 * R - f)[pos] = v[g] * tw_pow<Rl, false>(d.tw, (unsigned)(f * n1), lgMr);
+                }
             }
         }
         dsync();
@@ -495,15 +526,39 @@ struct RamanOut {
     }
 };
 
-// RamanOut::block transposed for clusters of 8: this CTA takes the n1 of its slice
+// RamanOut::block transposed for clusters of 8 and 16: this CTA takes the n1 of its slice
 // [r S, (r + 1) S), S = Mb/R, gathers the 2R sub-transform values B_p[n1] (two per CTA),
 // forms P[n1 + Mb q] = sum_p W_2R^{-p q} B_p[n1] for every q with one in-register DFT and
 // stores each into CTA q's out. Each CTA reads 2 Mb values instead of 2 R Mb; the stores
 // are visible to CTA q after the next cluster barrier.
+// For R = 16 the 2R-point DFT runs as two R-point ones over p = g + R e:
+// P_{2h} = IDFT_R(B_g + B_{g+R})[h] and P_{2h+1} = IDFT_R((B_g - B_{g+R}) W_2R^{-g})[h],
+// h < R/2 (only q < R is wanted); each half gathers the 2R values again.
 template <typename Rl, int R>
 __device__ __forceinline__ void raman_out_scatter(DWs<Rl>& d, cpx<Rl>* out, int Mb) {
     constexpr int R2 = 2 * R;
     const int S = Mb / R, n1b = d.rank * S;
+    if constexpr (R == 16) {
+        constexpr int lg2R = ilog2c<R2>();
+        for (int j = threadIdx.x; j < S; j += LUNA_BLOCK) {
+            const int pos = Swz<Rl>::f(n1b + j);
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                cpx<Rl> v[R];
+#pragma unroll
+                for (int i = 0; i < R; ++i) {
+                    const int g = bitrev<R>(i);
+                    const cpx<Rl> a = drem(d.rb0, g)[pos];                   // B_g
+                    const cpx<Rl> b = drem(d.rb1, g == 0 ? 0 : R - g)[pos];  // B_{g+R}
+                    v[i] = e ? (g ? (a - b) * tw_pow<Rl, true>(d.tw, (unsigned)g, lg2R) : a - b) : a + b;
+                }
+                dft_br<Rl, true, R>(v);
+#pragma unroll
+                for (int h = 0; h < R / 2; ++h) drem(out, 2 * h + e)[pos] = v[h];
+            }
+        }
+        return;
+    }
     for (int j = threadIdx.x; j < S; j += LUNA_BLOCK) {
         const int pos = Swz<Rl>::f(n1b + j);
         cpx<Rl> x[R2];
@@ -629,7 +684,7 @@ __device__ __noinline__ void dist_plasma(const LunaInst& I, DWs<Rl>& d, int M, d
     if (ir >= 0) {
         // the Raman polarisation of this block into tb (the field now lives in ev); with the
         // transposed form other CTAs write it, visible after the next barriers below
-        if constexpr (R == 8) {
+        if constexpr (R == 8 || R == 16) {
             raman_out_scatter<Rl, R>(d, d.tb, Mb);
         } else {
             RamanOut<Rl, R> ro;
@@ -766,7 +821,7 @@ __device__ __noinline__ void dist_pointwise(const LunaInst& I, DWs<Rl>& d, int M
     if (ip < 0) {
         dsync();  // every CTA's Raman sub-transforms ready; every read of the field blocks done
         // the sub-transform buffer is free after the barrier above
-        if constexpr (R == 8) {
+        if constexpr (R == 8 || R == 16) {
             raman_out_scatter<Rl, R>(d, d.fb, Mb);
             dsync();  // every CTA's stores into this block
         } else {

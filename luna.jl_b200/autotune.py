@@ -1,11 +1,12 @@
-"""Autotuner of a batch's CTA-per-instance shapes (north-star form (2); the reference has no
-counterpart: its scans run one ``prop_capillary`` after another, Scans.jl:275-353).
+"""Autotuner of a batch's CTA-per-instance shapes (the reference has no counterpart: its
+scans run one ``prop_capillary`` after another, Scans.jl:275-353).
 
 For every grid class of a batch (oversampled length No and whether a Raman response is
 present) and the batch's precision it measures the device time of one RK step on one CTA,
-on an 8-CTA cluster and (for the 32768-point grids) on a 16-CTA cluster (a batch of one representative instance, the difference of two step
-budgets, CUDA events), once per device, and caches the table in a JSON file
-(``$LUNA_B200_TUNE_CACHE``, default ``~/.cache/luna_b200/tune.json``). An instance's
+on an 8-CTA cluster and (for the 32768-point grids) on a 16-CTA cluster (a batch of one
+representative instance, the difference of two step budgets, CUDA events), once per device,
+and caches the table in a JSON file (``$LUNA_B200_TUNE_CACHE``, default
+``~/.cache/luna_b200/tune.json``). An instance's
 predicted integration time on a shape is its class's time per step times its predicted
 step count, ``scan.nonlinear_phase(p) ** 0.6`` up to a constant (the step model of
 ``scan.schedule_priority``; the constant cancels in every decision below).

@@ -1,6 +1,6 @@
-// Learned surrogate of the capillary scan (north-star form (4); no counterpart in the
-// reference): an ensemble of multilayer perceptrons mapping the scan parameters and z to
-// the log spectrum and temporal envelope, trained and evaluated by the kernels of this file.
+// Learned surrogate of the capillary scan (no counterpart in the reference): an ensemble
+// of multilayer perceptrons mapping the scan parameters and z to the log spectrum and
+// temporal envelope, trained and evaluated by the kernels of this file.
 //
 //   * sg_gemm<AT, BT>: C[m, n] = sum_k A(m, k) B(n, k) on the 5th-generation tensor cores
 //     (tcgen05.mma kind::f16, BF16 operands, FP32 accumulator in tensor memory) for the

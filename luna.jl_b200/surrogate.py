@@ -1,5 +1,5 @@
-"""Learned surrogate of the capillary scan family (north-star form (4); the reference has no
-counterpart: it always integrates).
+"""Learned surrogate of the capillary scan family (the reference has no counterpart: it
+always integrates).
 
 An ensemble of multilayer perceptrons maps (energy, pressure, core radius, τfwhm, z, gas)
 to the log10 spectral intensity on 512 log-spaced wavelength bins (150 nm - 4 µm, the

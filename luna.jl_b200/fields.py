@@ -70,6 +70,32 @@ class PulseField:
         return to_freq_coarse(grid, Et)
 
 
+class ShotNoise:
+    """One photon per mode quantum noise (``Fields.ShotNoise``, Fields.jl:284-321): on every
+    frequency bin (envelope grids: the bins of the signal window, ``sidx``) the spectral
+    amplitude sqrt(ħω/δω), scaled to the grid's transform (sqrt(2π)/(2δt) for the real one,
+    sqrt(2π)/δt for the complex one), with a phase drawn uniformly from [0, 2π). ``rng`` is
+    a numpy ``Generator`` (default: a fresh one); the reference draws from Julia's global
+    RNG, so individual draws differ between the two while their distribution is the same."""
+
+    def __init__(self, rng=None):
+        self.rng = np.random.default_rng() if rng is None else rng
+
+    def __call__(self, grid):
+        ω = np.asarray(grid.ω)
+        δω = ω[1] - ω[0]
+        δt = grid.t[1] - grid.t[0]
+        if grid.kind == "real":
+            amp = np.sqrt(pd.hbar * ω / δω)
+            famp = math.sqrt(2 * math.pi) / (2 * δt) * amp
+        else:
+            amp = np.zeros_like(ω)
+            amp[grid.sidx] = np.sqrt(pd.hbar * ω[grid.sidx] / δω)
+            famp = math.sqrt(2 * math.pi) / δt * amp
+        φ = 2 * math.pi * self.rng.random(len(ω))
+        return famp * np.exp(1j * φ)
+
+
 def GaussField(λ0, τfwhm, energy=None, power=None, m=1):
     return PulseField(λ0, lambda t: gauss(t, τfwhm, power=2 * m), energy, power)
 

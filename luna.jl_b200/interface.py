@@ -31,10 +31,10 @@ class Problem:
 def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=None, τw=None,
                     power=None, energy=None, pulseshape="gauss", shotnoise=False,
                     shock=True, loss=0.0, raman=True, fr=0.18, ramanmodel="sdo",
-                    τ1=12.2e-15, τ2=32e-15, saveN=201):
-    """GNLSE set-up (Interface.jl:921-979)."""
-    if shotnoise:
-        raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
+                    τ1=12.2e-15, τ2=32e-15, saveN=201, rng=None):
+    """GNLSE set-up (Interface.jl:921-979). ``shotnoise=True`` adds one photon per mode
+    (``fields.ShotNoise(rng)``, as ``shotnoise_maybe`` does, Interface.jl:773-776, 967);
+    the default here is False, so that a set-up is reproducible unless noise is asked for."""
     grid = EnvGrid(flength, λ0, λlims, trange, δt=δt, thg=False)
     mode = modes.SimpleMode(pd.wlfreq(λ0), βs, loss=loss)
     aeff = 1.0
@@ -58,6 +58,8 @@ def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=No
     norm = norm_mode_average_gnlse(grid, shock=shock)
     transform = TransModeAvg(grid, resp, density, norm, aeff)
     Eω = fld(grid)
+    if shotnoise:
+        Eω = Eω + fields.ShotNoise(rng)(grid)
     return Problem(Eω, grid, linop, transform, saveN)
 
 
@@ -117,7 +119,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
                         modes="HE11", radial_integral_rtol=1e-3, temperature=pd.roomtemp,
-                        rotation=True, vibration=True):
+                        rotation=True, vibration=True, rng=None):
     """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
     over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
     a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
@@ -128,11 +130,12 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     (the device runs it) and the full 2-D integral otherwise (described, evaluated by the
     oracle only); constant fill only. ``temperature`` sets the gas density, the core index
     and the Raman response's thermal populations; ``rotation``/``vibration`` select the Raman
-    components (Interface.jl:360-374, 519-531, 534-560)."""
+    components (Interface.jl:360-374, 519-531, 534-560). ``shotnoise=True`` adds one photon
+    per mode to the input of every propagation mode (``fields.ShotNoise(rng)``, as
+    ``shotnoise_maybe`` does, Interface.jl:389, 773-781); the default here is False, so that
+    a set-up is reproducible unless noise is asked for."""
     modes_ = modes
     from . import modes
-    if shotnoise:
-        raise NotImplementedError("shot noise uses a global RNG; pass shotnoise=False")
     plasma = (not envelope) if plasma is None else plasma
     thg = (not envelope) if thg is None else thg
     if envelope and plasma:  # makeresponse for EnvGrid (Interface.jl:593-594)
@@ -145,7 +148,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
-                                         rotation, vibration)
+                                         rotation, vibration, shotnoise, rng)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
@@ -206,15 +209,18 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     else:
         fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
     Eω = fld(grid)
+    if shotnoise:
+        Eω = Eω + fields.ShotNoise(rng)(grid)
     return Problem(Eω, grid, linop, transform, saveN)
 
 
 def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
                           pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol,
-                          temperature, rotation, vibration):
+                          temperature, rotation, vibration, shotnoise=False, rng=None):
     """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
     linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
-    (``makeinputs``, Interface.jl:721-733)."""
+    (``makeinputs``, Interface.jl:721-733); with ``shotnoise`` one photon per mode in every
+    mode (``shotnoise_maybe``, Interface.jl:778-781)."""
     from . import modal
     if isinstance(pressure, (tuple, list)) or isinstance(radius, (tuple, list)):
         raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
@@ -248,6 +254,11 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
         fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
     Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
+    if shotnoise:
+        noise = fields.ShotNoise(rng)
+        Eω = np.array(Eω, dtype=np.complex128, copy=True)
+        for m in range(Eω.shape[1]):
+            Eω[:, m] += noise(grid)
     return Problem(Eω, grid, modal.make_const_linop_modes(grid, ms, λ0, thg=thg), t, saveN)
 
 

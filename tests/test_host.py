@@ -225,3 +225,60 @@ def test_autotune_schedule_picks_sixteen_ctas_for_the_longest():
     shapes, prio, _ = autotune.schedule(inst, probs, table, nsm=148)
     assert shapes[0] == 3 and prio[0] == pytest.approx(200.0)
     assert all(s == 1 for s in shapes[1:])
+
+
+def test_shotnoise_is_one_photon_per_mode():
+    """fields.ShotNoise (Fields.jl:304-321): amplitude sqrt(2π)/(2δt) sqrt(ħω/δω) on the
+    real grid and sqrt(2π)/δt sqrt(ħω/δω) inside the envelope grid's signal window (zero
+    outside), phases 2π times the generator's uniform draws; the energy weights of the
+    reference's energy functions then count one photon per frequency bin (exactly on the
+    envelope grid, within the SimpsonEven end weights on the real one)."""
+    from luna_b200 import accuracy, fields
+    from luna_b200 import physdata as pd
+    g = RealGrid(0.1, 800e-9, (150e-9, 4e-6), 0.25e-12)
+    n = fields.ShotNoise(np.random.default_rng(3))(g)
+    δω, δt = g.ω[1] - g.ω[0], g.t[1] - g.t[0]
+    amp = np.sqrt(2 * np.pi) / (2 * δt) * np.sqrt(pd.hbar * g.ω / δω)
+    assert np.allclose(np.abs(n), amp, rtol=1e-13, atol=0)
+    φ = 2 * np.pi * np.random.default_rng(3).random(len(g.ω))
+    assert np.allclose(n, amp * np.exp(1j * φ), rtol=1e-13, atol=0)
+    w = accuracy.Weights(g.ω, "real")
+    photons = w.photons @ np.abs(n) ** 2 / pd.hbar
+    assert abs(photons / np.count_nonzero(g.ω > 0) - 1) < 0.01
+    e = EnvGrid(0.1, 800e-9, (150e-9, 4e-6), 0.25e-12)
+    ne = fields.ShotNoise(np.random.default_rng(4))(e)
+    assert np.all(ne[~e.sidx] == 0)
+    δω, δt = e.ω[1] - e.ω[0], e.t[1] - e.t[0]
+    amp = np.sqrt(2 * np.pi) / δt * np.sqrt(pd.hbar * e.ω[e.sidx] / δω)
+    assert np.allclose(np.abs(ne[e.sidx]), amp, rtol=1e-13, atol=0)
+    we = accuracy.Weights(e.ω, "env")
+    photons = we.photons @ np.abs(ne) ** 2 / pd.hbar
+    assert abs(photons / np.count_nonzero(e.sidx) - 1) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["capillary", "gnlse", "multimode"])
+def test_setup_shotnoise_adds_the_noise_to_every_mode(kind):
+    """shotnoise=true (shotnoise_maybe, Interface.jl:773-781): the input spectrum of every
+    propagation mode gains one ShotNoise draw; the rest of the set-up is unchanged."""
+    from luna_b200 import fields
+    if kind == "capillary":
+        f = lambda **k: prop_capillary_args(125e-6, 0.01, "He", 1.0, λ0=800e-9, τfwhm=10e-15,
+                                            energy=120e-6, λlims=(150e-9, 4e-6), trange=0.25e-12, **k)
+    elif kind == "gnlse":
+        f = lambda **k: prop_gnlse_args(0.11, 0.15, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9,
+                                        τfwhm=50e-15, power=10e3, λlims=(450e-9, 8000e-9),
+                                        trange=4e-12, **k)
+    else:
+        f = lambda **k: prop_capillary_args(13e-6, 1e-2, "Ar", 5.0, modes=2, envelope=True, λ0=800e-9,
+                                            τfwhm=30e-15, energy=1e-6, λlims=(160e-9, 3000e-9),
+                                            trange=1e-12, **k)
+    p0 = f()
+    p1 = f(shotnoise=True, rng=np.random.default_rng(11))
+    noise = fields.ShotNoise(np.random.default_rng(11))
+    d = np.asarray(p1.Eω) - np.asarray(p0.Eω)
+    if d.ndim == 1:
+        assert np.allclose(d, noise(p0.grid), rtol=0, atol=1e-12 * np.abs(p0.Eω).max())
+    else:
+        for m in range(d.shape[1]):
+            assert np.allclose(d[:, m], noise(p0.grid), rtol=0, atol=1e-12 * np.abs(p0.Eω).max())
+    assert np.array_equal(p1.linop, p0.linop)

@@ -45,11 +45,18 @@ def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=No
     χ3 = 4 / 3 * (1 - fr) * n2 * (pd.eps_0 * pd.c)
     resp = [Kerr_env(χ3)]
     if raman:
-        if ramanmodel != "sdo":
-            raise NotImplementedError("only ramanmodel='sdo' is supported")
+        # Interface.jl:945-961: the single damped oscillator, or fused silica's
+        # intermediate-broadening model (ramanmodel "SiO2")
         χ3R = 2 * fr * n2 * (pd.eps_0 * pd.c)
-        rr = _raman.CombinedRamanResponse(
-            grid.to, [_raman.RamanRespNormedSingleDampedOscillator(χ3R * pd.eps_0, 1 / τ1, τ2)])
+        if ramanmodel == "SiO2":
+            rr = _raman.raman_response(grid.to, "SiO2", χ3R * pd.eps_0)
+        elif ramanmodel == "sdo":
+            if τ1 is None or τ2 is None:
+                raise ValueError("for :sdo ramanmodel you must specify τ1 and τ2")
+            rr = _raman.CombinedRamanResponse(
+                grid.to, [_raman.RamanRespNormedSingleDampedOscillator(χ3R * pd.eps_0, 1 / τ1, τ2)])
+        else:
+            raise ValueError("unrecognised value for ramanmodel")
         resp.append(RamanPolarEnv(grid.to, rr))
     if pulseshape == "gauss":
         fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)

@@ -178,8 +178,9 @@ def polarisability_difference(gas):
 
 
 def raman_parameters(gas):
-    """Molecular Raman parameters (PhysData.jl:968-1026) for the gases this package
-    supports. Values are literature data and are kept identical to reproduce the physics."""
+    """Raman parameters (PhysData.jl:968-1070) for the gases this package supports (and the
+    intermediate-broadening model of fused silica used by ``prop_gnlse(ramanmodel="SiO2")``).
+    Values are literature data and are kept identical to reproduce the physics."""
     if gas == "N2":
         return dict(kind="molecular", rotation="nonrigid", vibration="sdo", B=199.0, D=5.74e-4,
                     qJodd=1, qJeven=2, dalpha=6.7e-31, Brho_r=3.3e9, Arho_r=0.0,
@@ -190,4 +191,20 @@ def raman_parameters(gas):
                     qJodd=3, qJeven=1, dalpha=3e-31, Brho_r=114e6, Arho_r=6.15e6,
                     dadQ=1.3e-20, Omega_v=2 * math.pi * 124.5669e12,
                     mu=(m_u * 1.00784) ** 2 / (2 * m_u * 1.00784), Brho_v=52.2e6, Arho_v=309e6)
+    if gas == "D2":
+        return dict(kind="molecular", rotation="nonrigid", vibration="sdo", B=2930.0, D=2.1,
+                    qJodd=1, qJeven=2, dalpha=3e-31, Brho_r=4e-3 * 100.0 * c, Arho_r=0.0,
+                    dadQ=1.4e-20, Omega_v=2 * math.pi * 2987 * 100.0 * c,
+                    mu=(m_u * 2.014) ** 2 / (2 * m_u * 2.014), Brho_v=120e6, Arho_v=101e6)
+    if gas == "SiO2":
+        # Hollenbeck and Cantrell, J. Opt. Soc. Am. B 19, 2886 (2002): line centres, amplitudes,
+        # Gaussian and Lorentzian widths of the intermediate-broadening model
+        return dict(kind="intermediate",
+                    omega_i=[200 * math.pi * c * x for x in (56.25, 100.0, 231.25, 362.50, 463.00, 497.00, 611.50,
+                                                            691.67, 793.67, 835.50, 930.0, 1080.00, 1215.00)],
+                    A_i=[1.0, 11.40, 36.67, 67.67, 74.00, 4.50, 6.80, 4.60, 4.20, 4.50, 2.70, 3.10, 3.00],
+                    Gamma_i=[100 * math.pi * c * x for x in (52.10, 110.42, 175.00, 162.50, 135.33, 24.50, 41.50,
+                                                            155.0, 59.50, 64.30, 150.00, 91.00, 160.00)],
+                    gamma_i=[100 * math.pi * c * x for x in (17.37, 38.81, 58.33, 54.17, 45.11, 8.17, 13.83,
+                                                            51.67, 19.83, 21.43, 50.00, 30.33, 53.33)])
     raise ValueError(f"no Raman parameters for {gas}")

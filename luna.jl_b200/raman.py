@@ -8,7 +8,9 @@ A response is reduced to what the device needs to rebuild h(t; rho) on the Raman
 grid: for each component its undamped response ``hpre_i(t)`` sampled on
 ``tt = (0..N-1)*dt``, its density-dependent dephasing time ``tau2_i(rho)`` and the
 Planck-taper window ``w`` (Raman.jl:249-262). The device forms
-``h = w * sum_i hpre_i * exp(-tt/tau2_i)`` and transforms it.
+``h = w * sum_i hpre_i * exp(-tt/tau2_i)`` and transforms it. The intermediate-broadening
+model of fused silica (Raman.jl:66-113) fits the same form as one component with
+``tau2 = inf`` and ``w = 1``.
 """
 import math
 
@@ -169,5 +171,58 @@ def molecular_raman_response(t, rp, rotation=True, vibration=True, minJ=0, maxJ=
     return CombinedRamanResponse(t, Rs)
 
 
-def raman_response(t, gas, **kw):
-    return molecular_raman_response(t, pd.raman_parameters(gas), **kw)
+class RamanRespIntermediateBroadening:
+    """Intermediate-broadening model (Raman.jl:66-113, after Hollenbeck and Cantrell, J. Opt.
+    Soc. Am. B 19, 2886 (2002)): h(t) = s sum_i A_i exp(-γ_i t) exp(-Γ_i² t²/4) sin(ω_i t)
+    on tt = (0..N-1) dt, with s = scale / (integral of the unscaled sum over (0, 1 ns)).
+    The reference integrates with Cubature's hquadrature at its default tolerance (relative
+    sqrt(eps)); here adaptive Gauss-Kronrod quadrature runs to 1e-12 relative, so the two
+    scales agree to the reference's tolerance. No window and no density dependence: for the
+    device it is one component with tau2 = inf and w = 1 (``hpres``, ``tau2s``, ``w``)."""
+
+    def __init__(self, t, omega_i, A_i, Gamma_i, gamma_i, scale):
+        self.omega_i, self.A_i = np.asarray(omega_i, float), np.asarray(A_i, float)
+        self.Gamma_i, self.gamma_i = np.asarray(Gamma_i, float), np.asarray(gamma_i, float)
+        n = len(self.omega_i)
+        if not (len(self.A_i) == len(self.Gamma_i) == len(self.gamma_i) == n):
+            raise ValueError("all component vectors must have same length")
+        from scipy.integrate import quad
+        self.scale = 1.0
+        # the response lives in the first picoseconds: integrate there to 1e-12 relative,
+        # then the (vanishing) rest of (0, 1 ns) to an absolute bound below that
+        edges = [0.0, 2e-14, 1e-13, 3e-13, 1e-12, 3e-12]
+        head = sum(quad(self, a, b, limit=500, epsabs=0.0, epsrel=1e-12)[0] for a, b in zip(edges[:-1], edges[1:]))
+        tail = quad(self, edges[-1], 1e-9, limit=500, epsabs=1e-14 * abs(head), epsrel=0.0)[0]
+        self.scale = scale / (head + tail)
+        t = np.asarray(t, dtype=np.float64)
+        self.Rs = []
+        self.dt = t[1] - t[0]
+        self.tt = np.arange(len(t), dtype=np.float64) * self.dt
+        self.hpres = [np.asarray(self(self.tt), dtype=np.float64)]
+        self.w = np.ones_like(self.tt)
+
+    def __call__(self, t):
+        t = np.asarray(t, dtype=np.float64)
+        h = np.zeros_like(t)
+        for w, A, G, g in zip(self.omega_i, self.A_i, self.Gamma_i, self.gamma_i):
+            h = h + self.scale * A * np.exp(-g * t) * np.exp(-G ** 2 * t ** 2 / 4) * np.sin(w * t)
+        return h if h.ndim else float(h)
+
+    def tau2s(self, rho):
+        return [math.inf]
+
+    def tau2_rows(self):
+        return None
+
+    def h(self, rho):
+        """h(t) on tt (the response does not depend on the density)."""
+        return self.hpres[0].copy()
+
+
+def raman_response(t, material, scale=1.0, **kw):
+    """``Raman.raman_response`` (Raman.jl:316-328): the molecular model of a gas, or the
+    intermediate-broadening model of fused silica ("SiO2") scaled by ``scale``."""
+    rp = pd.raman_parameters(material)
+    if rp["kind"] == "intermediate":
+        return RamanRespIntermediateBroadening(t, rp["omega_i"], rp["A_i"], rp["Gamma_i"], rp["gamma_i"], scale)
+    return molecular_raman_response(t, rp, **kw)

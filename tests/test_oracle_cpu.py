@@ -21,9 +21,10 @@ def _case(gas, plasma, trange=0.5e-12, flength=0.05):
                                λlims=(150e-9, 4e-6), trange=trange, plasma=plasma, saveN=5)
 
 
-@pytest.mark.parametrize("gas,plasma", [("He", False), ("Ar", None), ("H2", None)])
+@pytest.mark.parametrize("gas,plasma", [("He", False), ("Ar", None), ("H2", None), ("D2", None)])
 def test_cpu_restatement_rhs_matches_numpy(gas, plasma):
-    """Kerr only; Kerr + PPT plasma; Kerr + ADK plasma + Raman (NonlinearRHS.jl:362-373)."""
+    """Kerr only; Kerr + PPT plasma; Kerr + ADK plasma + Raman, for H2 and D2
+    (NonlinearRHS.jl:362-373)."""
     p = _case(gas, plasma)
     cp = cpu.CpuPlan(p.transform)
     rng = np.random.default_rng(1)
@@ -55,10 +56,14 @@ def test_cpu_restatement_step_budget_and_field_limit():
         cp.rhs(strong.Eω * 1e3)  # far above the PPT table: the reference errors
 
 
-def test_cpu_restatement_envelope_rhs_matches_numpy():
-    """GNLSE on an envelope grid: Kerr_env + RamanPolarEnv (Nonlinear.jl:47-73, 276-333)."""
+@pytest.mark.parametrize("ramanmodel", ["sdo", "SiO2"])
+def test_cpu_restatement_envelope_rhs_matches_numpy(ramanmodel):
+    """GNLSE on an envelope grid: Kerr_env + RamanPolarEnv (Nonlinear.jl:47-73, 276-333), with
+    the single damped oscillator or fused silica's intermediate-broadening model
+    (Interface.jl:945-961)."""
     p = prop_gnlse_args(0.11, 0.15, [0.0, 0.0, -11.83e-27, 8.1e-41], λ0=835e-9,
-                        λlims=(500e-9, 2400e-9), trange=12.5e-12, τfwhm=50e-15, power=10e3, saveN=5)
+                        λlims=(500e-9, 2400e-9), trange=12.5e-12, τfwhm=50e-15, power=10e3, saveN=5,
+                        ramanmodel=ramanmodel)
     cp = cpu.CpuPlan(p.transform)
     rng = np.random.default_rng(4)
     Ew = p.Eω * np.exp(1j * 0.1 * rng.standard_normal(p.Eω.shape))

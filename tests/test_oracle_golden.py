@@ -212,6 +212,41 @@ def test_raman_h2_vibrational_and_rotational_peaks():
     assert abs(_raman_peak(grid, hr, rho, True) / (2 * np.pi * 17.45e12) - 1) < 1e-4
 
 
+def test_raman_d2_vibrational_and_rotational_peaks():
+    """D2 (PhysData.jl:1011-1026): the vibrational line at Ωv, and the rotational spectrum
+    peaking on one of the S(J) lines of the non-rigid rotor (B and D in 1/m, Raman.jl:199-200)."""
+    grid = EnvGrid(1.0, 800e-9, (200e-9, 2000e-9), 40e-12)
+    rho = pd.density("D2", 5.0)
+    hv = raman.raman_response(grid.to, "D2", rotation=False)
+    assert abs(_raman_peak(grid, hv, rho, True) / pd.raman_parameters("D2")["Omega_v"] - 1) < 1e-4
+    hr = raman.raman_response(grid.to, "D2", vibration=False)
+    wr = _raman_peak(grid, hr, rho, True)
+    B, D = 2930.0, 2.1
+    E = lambda J: B * J * (J + 1) - D * (J * (J + 1)) ** 2
+    lines = [2 * np.pi * pd.c * (E(J + 2) - E(J)) for J in range(6)]
+    assert min(abs(wr / w - 1) for w in lines) < 1e-3
+
+
+def test_raman_sio2_intermediate_broadening_response():
+    """Raman.jl:66-113 with the fused-silica lines (PhysData.jl:1060-1068): the samples follow
+    the formula, the response integrates to its scale over (0, 1 ns), and the device
+    descriptor carries it as one component with tau2 = inf and no window."""
+    from luna_b200.plan import resp_descs
+    from luna_b200.nonlinear import RamanPolarEnv
+    grid = EnvGrid(1.0, 835e-9, (500e-9, 2400e-9), 12.5e-12)
+    r = raman.raman_response(grid.to, "SiO2", 2.5)
+    rp = pd.raman_parameters("SiO2")
+    tt = r.tt
+    h = sum(r.scale * A * np.exp(-g * tt) * np.exp(-G ** 2 * tt ** 2 / 4) * np.sin(w * tt)
+            for w, A, G, g in zip(rp["omega_i"], rp["A_i"], rp["Gamma_i"], rp["gamma_i"]))
+    assert np.allclose(r.h(1.0), h, rtol=1e-13, atol=0)
+    x = np.linspace(0.0, 3e-12, 3_000_001)
+    assert abs(np.trapezoid(r(x), x) / 2.5 - 1) < 1e-6
+    ds = resp_descs([RamanPolarEnv(grid.to, r)], 1.0, [])
+    assert ds[0].ncomp == 1 and ds[0].tau2[0] == np.inf
+    assert np.all(np.ctypeslib.as_array(ds[0].hwin, shape=(len(tt),)) == 1.0)
+
+
 # ---------------------------------------------------------------- Maths.cumtrapz!
 def test_cumtrapz_is_the_sequential_recurrence():
     rng = np.random.default_rng(0)

@@ -49,11 +49,26 @@ def to_freq_coarse(grid, Et):
     return np.fft.rfft(Et) if grid.kind == "real" else np.fft.fft(Et)
 
 
+def prop_taylor(Eω, ω, ϕs, λ0):
+    """``prop_taylor`` (Fields.jl:618-636): Eω exp(-i sum_n ϕs[n] Δω^n / n!) with
+    Δω = ω - ω(λ0) (ϕs = CEP, group delay, GDD, TOD, ...)."""
+    Δω = np.asarray(ω) - pd.wlfreq(λ0)
+    ϕ = np.zeros(len(Δω))
+    for n, ϕi in enumerate(ϕs):
+        ϕ = ϕ + Δω ** n / math.factorial(n) * ϕi
+    return np.asarray(Eω) * np.exp(-1j * ϕ)
+
+
 class PulseField:
-    def __init__(self, λ0, Itshape, energy=None, power=None):
+    """``PulseField`` (Fields.jl:40-57, 112-145): the intensity shape on the grid's time axis
+    (field-resolved or envelope), the spectral phases ``ϕ`` applied in the frequency domain
+    (``prop_taylor``), then scaled to the energy or to the peak power after the phases."""
+
+    def __init__(self, λ0, Itshape, energy=None, power=None, ϕ=()):
         if (energy is None) == (power is None):
             raise ValueError("exactly one of energy or power must be given")
         self.λ0, self.Itshape, self.energy, self.power = λ0, Itshape, energy, power
+        self.ϕ = tuple(float(x) for x in np.atleast_1d(ϕ)) if ϕ is not None else ()
 
     def __call__(self, grid):
         t = grid.t
@@ -63,6 +78,9 @@ class PulseField:
         else:
             Δω = ω0 - grid.ω0
             Et = np.sqrt(self.Itshape(t)) * np.exp(1j * (Δω * t))
+        if len(self.ϕ) >= 1:
+            Eω = prop_taylor(to_freq_coarse(grid, Et), grid.ω, self.ϕ, self.λ0)
+            Et = np.fft.irfft(Eω, len(t)) if grid.kind == "real" else np.fft.ifft(Eω)
         if self.energy is not None:
             Et = Et * (math.sqrt(self.energy) / math.sqrt(energy_t(grid, Et)))
         else:
@@ -96,14 +114,18 @@ class ShotNoise:
         return famp * np.exp(1j * φ)
 
 
-def GaussField(λ0, τfwhm, energy=None, power=None, m=1):
-    return PulseField(λ0, lambda t: gauss(t, τfwhm, power=2 * m), energy, power)
+def GaussField(λ0, τfwhm, energy=None, power=None, m=1, ϕ=()):
+    return PulseField(λ0, lambda t: gauss(t, τfwhm, power=2 * m), energy, power, ϕ)
 
 
-def SechField(λ0, τfwhm=None, τw=None, energy=None, power=None):
+def SechField(λ0, τfwhm=None, τw=None, energy=None, power=None, ϕ=()):
+    if τfwhm is not None and τw is not None:
+        raise ValueError("only one of `τw` or `τfwhm` can be specified")
     if τw is None:
+        if τfwhm is None:
+            raise ValueError("one of `τw` or `τfwhm` must be specified")
         τw = τfwhm / (2 * math.log(1 + math.sqrt(2)))
     def shape(t):
         with np.errstate(over="ignore"):
             return 1 / np.cosh(t / τw) ** 2
-    return PulseField(λ0, shape, energy, power)
+    return PulseField(λ0, shape, energy, power, ϕ)

@@ -31,8 +31,9 @@ class Problem:
 def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=None, τw=None,
                     power=None, energy=None, pulseshape="gauss", shotnoise=False,
                     shock=True, loss=0.0, raman=True, fr=0.18, ramanmodel="sdo",
-                    τ1=12.2e-15, τ2=32e-15, saveN=201, rng=None):
-    """GNLSE set-up (Interface.jl:921-979). ``shotnoise=True`` adds one photon per mode
+                    τ1=12.2e-15, τ2=32e-15, saveN=201, rng=None, ϕ=()):
+    """GNLSE set-up (Interface.jl:921-979); ``ϕ`` are the input pulse's spectral phases
+    (CEP, group delay, GDD, ..., ``prop_taylor``). ``shotnoise=True`` adds one photon per mode
     (``fields.ShotNoise(rng)``, as ``shotnoise_maybe`` does, Interface.jl:773-776, 967);
     the default here is False, so that a set-up is reproducible unless noise is asked for."""
     grid = EnvGrid(flength, λ0, λlims, trange, δt=δt, thg=False)
@@ -58,10 +59,7 @@ def prop_gnlse_args(γ, flength, βs, *, λ0, λlims, trange, δt=1.0, τfwhm=No
         else:
             raise ValueError("unrecognised value for ramanmodel")
         resp.append(RamanPolarEnv(grid.to, rr))
-    if pulseshape == "gauss":
-        fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
-    else:
-        fld = fields.SechField(λ0, τfwhm=τfwhm, τw=τw, energy=energy, power=power)
+    fld = _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ)
     norm = norm_mode_average_gnlse(grid, shock=shock)
     transform = TransModeAvg(grid, resp, density, norm, aeff)
     Eω = fld(grid)
@@ -121,12 +119,37 @@ def needfull(ms):
     return not all(m.kind == "HE" and m.n == 1 for m in ms)
 
 
+def _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ):
+    """``makeinputs`` for a single pulse (Interface.jl:621-632): a Gaussian or sech² pulse
+    with spectral phases ϕ."""
+    if pulseshape == "gauss":
+        return fields.GaussField(λ0, τfwhm, energy=energy, power=power, ϕ=ϕ)
+    if pulseshape == "sech":
+        return fields.SechField(λ0, τfwhm=τfwhm, τw=τw, energy=energy, power=power, ϕ=ϕ)
+    raise ValueError("Valid pulse shapes are :gauss and :sech")
+
+
+def _plasma(grid, gas, model, λ0, ppt_N, preionfrac):
+    """``makeplasma!`` (Interface.jl:560-590): the ADK rate for molecular gases and the PPT
+    rate otherwise (``model`` True), or the rate ``model`` names ("ADK" / "PPT")."""
+    if model is True:
+        model = "ADK" if gas in ("H2", "D2", "N2O", "CH4", "SF6") else "PPT"
+    ionpot = pd.ionisation_potential(gas)
+    if model == "ADK":
+        rate = ionrate_fun_ADK(gas)
+    elif model == "PPT":
+        rate = ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
+    else:
+        raise ValueError(f"Unknown ionisation rate {model}.")
+    return PlasmaCumtrapz(grid.to, grid.to, rate, ionpot, preionfrac=preionfrac)
+
+
 def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, τfwhm=None,
                         energy=None, power=None, pulseshape="gauss", shotnoise=False,
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
                         modes="HE11", radial_integral_rtol=1e-3, temperature=pd.roomtemp,
-                        rotation=True, vibration=True, rng=None):
+                        rotation=True, vibration=True, rng=None, τw=None, ϕ=(), preionfrac=0.0):
     """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
     over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
     a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
@@ -137,7 +160,11 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     (the device runs it) and the full 2-D integral otherwise (described, evaluated by the
     oracle only); constant fill only. ``temperature`` sets the gas density, the core index
     and the Raman response's thermal populations; ``rotation``/``vibration`` select the Raman
-    components (Interface.jl:360-374, 519-531, 534-560). ``shotnoise=True`` adds one photon
+    components (Interface.jl:360-374, 519-531, 534-560). ``plasma`` True selects ADK for
+    molecular gases and PPT otherwise, "ADK" or "PPT" names the rate (makeplasma!,
+    Interface.jl:560-590), ``preionfrac`` is the pre-ionised fraction; ``ϕ`` are the input
+    pulse's spectral phases and ``τw`` the natural width of a sech² pulse (makeinputs,
+    Interface.jl:621-632). ``shotnoise=True`` adds one photon
     per mode to the input of every propagation mode (``fields.ShotNoise(rng)``, as
     ``shotnoise_maybe`` does, Interface.jl:389, 773-781); the default here is False, so that
     a set-up is reproducible unless noise is asked for."""
@@ -155,7 +182,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
-                                         rotation, vibration, shotnoise, rng)
+                                         rotation, vibration, shotnoise, rng, preionfrac=preionfrac,
+                                         ϕ=ϕ, τw=τw)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
@@ -189,12 +217,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
                     Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
     if plasma:
-        ionpot = pd.ionisation_potential(gas)
-        if gas in ("H2", "D2", "N2O", "CH4", "SF6"):
-            rate = ionrate_fun_ADK(gas)
-        else:
-            rate = ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
-        resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, ionpot))
+        resp.append(_plasma(grid, gas, plasma, λ0, ppt_N, preionfrac))
     if raman is None:
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
@@ -211,10 +234,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         linop, βconst, β1 = make_const_linop(grid, mode, λ0, thg=thg)
         norm = norm_mode_average(grid, βconst)
         transform = TransModeAvg(grid, resp, density, norm, aeff)
-    if pulseshape == "gauss":
-        fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
-    else:
-        fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
+    fld = _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ)
     Eω = fld(grid)
     if shotnoise:
         Eω = Eω + fields.ShotNoise(rng)(grid)
@@ -223,7 +243,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
 
 def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
                           pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol,
-                          temperature, rotation, vibration, shotnoise=False, rng=None):
+                          temperature, rotation, vibration, shotnoise=False, rng=None, preionfrac=0.0,
+                          ϕ=(), τw=None):
     """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
     linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
     (``makeinputs``, Interface.jl:721-733); with ``shotnoise`` one photon per mode in every
@@ -244,21 +265,13 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
         resp.append(Kerr_field(pd.gamma3_gas(gas)) if thg else
                     Kerr_field_nothg(pd.gamma3_gas(gas), len(grid.to)))
     if plasma:
-        ionpot = pd.ionisation_potential(gas)
-        if gas in ("H2", "D2", "N2O", "CH4", "SF6"):
-            rate = ionrate_fun_ADK(gas)
-        else:
-            rate = ionisation.ionrate_PPTaccel(gas, λ0, N=ppt_N)
-        resp.append(PlasmaCumtrapz(grid.to, grid.to, rate, ionpot))
+        resp.append(_plasma(grid, gas, plasma, λ0, ppt_N, preionfrac))
     if raman is None:
         raman = gas in ("N2", "H2", "D2", "N2O", "CH4", "SF6")
     if raman:
         rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
         resp.append(RamanPolarEnv(grid.to, rr) if env else RamanPolarField(grid.to, rr, thg=thg))
-    if pulseshape == "gauss":
-        fld = fields.GaussField(λ0, τfwhm, energy=energy, power=power)
-    else:
-        fld = fields.SechField(λ0, τfwhm=τfwhm, energy=energy, power=power)
+    fld = _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ)
     Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
     if shotnoise:

@@ -282,3 +282,45 @@ def test_setup_shotnoise_adds_the_noise_to_every_mode(kind):
         for m in range(d.shape[1]):
             assert np.allclose(d[:, m], noise(p0.grid), rtol=0, atol=1e-12 * np.abs(p0.Eω).max())
     assert np.array_equal(p1.linop, p0.linop)
+
+
+def test_input_spectral_phase_follows_prop_taylor():
+    """PulseField with ϕ (Fields.jl:131-145, prop_taylor Fields.jl:618-625): the spectrum of a
+    pulse with GDD and TOD is the unchirped spectrum times exp(-i(ϕ2 Δω²/2 + ϕ3 Δω³/6)) (the
+    energy is unchanged by a phase), and the Gaussian's duration grows as
+    sqrt(1 + (4 ln2 ϕ2 / τ²)²)."""
+    from luna_b200 import fields
+    from luna_b200 import physdata as pd
+    g = RealGrid(0.1, 800e-9, (150e-9, 4e-6), 1e-12)
+    τ, ϕ2, ϕ3 = 10e-15, 50e-30, 20e-45
+    E0 = fields.GaussField(800e-9, τ, energy=1e-6)(g)
+    E1 = fields.GaussField(800e-9, τ, energy=1e-6, ϕ=[0.0, 0.0, ϕ2, ϕ3])(g)
+    Δω = g.ω - pd.wlfreq(800e-9)
+    ref = E0 * np.exp(-1j * (ϕ2 * Δω ** 2 / 2 + ϕ3 * Δω ** 3 / 6))
+    big = np.abs(E0) > 1e-3 * np.abs(E0).max()
+    assert np.allclose(E1[big], ref[big], rtol=1e-6, atol=1e-9 * np.abs(E0).max())
+    E2 = fields.GaussField(800e-9, τ, energy=1e-6, ϕ=[0.0, 0.0, ϕ2])(g)
+    It = np.abs(fields.analytic(np.fft.irfft(E2, len(g.t)))) ** 2
+    above = g.t[It >= It.max() / 2]
+    width = above.max() - above.min()
+    assert abs(width / (τ * np.sqrt(1 + (4 * np.log(2) * ϕ2 / τ ** 2) ** 2)) - 1) < 0.02
+
+
+def test_capillary_plasma_model_preionisation_and_sech_width():
+    """makeplasma! (Interface.jl:560-590): plasma=true picks PPT for atoms and ADK for
+    molecules, "ADK"/"PPT" name the rate, preionfrac reaches PlasmaCumtrapz; makeinputs'
+    sech² pulse from its natural width τw equals the one from τfwhm = 2 ln(1+√2) τw."""
+    from luna_b200.nonlinear import ADKRate, PPTSpline
+    kw = dict(λ0=800e-9, energy=120e-6, λlims=(150e-9, 4e-6), trange=0.25e-12)
+    plasma_of = lambda p: [r for r in p.transform.resp if r.kind == "plasma"][0]
+    p = prop_capillary_args(125e-6, 0.01, "Ar", 1.0, τfwhm=10e-15, **kw)
+    assert isinstance(plasma_of(p).ratefunc, PPTSpline) and plasma_of(p).preionfrac == 0.0
+    p = prop_capillary_args(125e-6, 0.01, "Ar", 1.0, τfwhm=10e-15, plasma="ADK", preionfrac=0.1, **kw)
+    assert isinstance(plasma_of(p).ratefunc, ADKRate) and plasma_of(p).preionfrac == 0.1
+    with pytest.raises(ValueError):
+        prop_capillary_args(125e-6, 0.01, "Ar", 1.0, τfwhm=10e-15, plasma="SFA", **kw)
+    τw = 6e-15
+    a = prop_capillary_args(125e-6, 0.01, "He", 1.0, pulseshape="sech", τw=τw, **kw)
+    b = prop_capillary_args(125e-6, 0.01, "He", 1.0, pulseshape="sech",
+                            τfwhm=2 * np.log(1 + np.sqrt(2)) * τw, **kw)
+    assert np.allclose(a.Eω, b.Eω, rtol=1e-12, atol=1e-12 * np.abs(b.Eω).max())

@@ -89,6 +89,58 @@ def needpol_modes(modes_):
     return any(parse_mode(m)["kind"] != "HE" or parse_mode(m)["n"] > 1 for m in modes_)
 
 
+def needpol(polarisation):
+    """``needpol`` (Interface.jl:421-431): two field components unless linearly polarised."""
+    if isinstance(polarisation, str):
+        pol = polarisation.lstrip(":")
+        if pol == "linear":
+            return False
+        if pol in ("circular", "x", "y"):
+            return True
+        raise ValueError(f"Polarisation must be :linear, :circular, :x/:y, or an ellipticity, not {polarisation}")
+    return True
+
+
+def ellfac(polarisation):
+    """``ellfac`` (Interface.jl:744-749): the energy fractions (py, px) of the two components:
+    one half each for circular polarisation, (1 - ε²/(1+ε²), ε²/(1+ε²)) for an ellipticity ε."""
+    if isinstance(polarisation, str):
+        return 0.5, 0.5
+    ε = float(polarisation)
+    if not -1 <= ε <= 1:
+        raise ValueError("Ellipticity must be between -1 and 1.")
+    return 1 - ε ** 2 / (1 + ε ** 2), ε ** 2 / (1 + ε ** 2)
+
+
+def _addphase(ϕ, phase):
+    """``addphase`` (Interface.jl:706-718): ``phase`` added to the constant spectral phase."""
+    ϕ = [float(x) for x in np.atleast_1d(ϕ)] if ϕ is not None else []
+    if phase == 0:
+        return ϕ
+    if not ϕ:
+        return [phase]
+    ϕ[0] += phase
+    return ϕ
+
+
+def makeinputs_pol(pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation):
+    """``makeinputs`` for one pulse in the lowest mode (Interface.jl:621-632, 638-649, 721-733,
+    751-761): linear or x polarisation in mode 1, y in mode 2, circular or elliptical split
+    into (mode 1, fraction py) and (mode 2, fraction px, constant phase + π/2 sign(ε))."""
+    nm = lambda x, f: None if x is None else x * f
+    pol = polarisation.lstrip(":") if isinstance(polarisation, str) else polarisation
+    if pol in ("linear", "x"):
+        return ({"mode": 1, "fields": (_pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ),)},)
+    if pol == "y":
+        return ({"mode": 2, "fields": (_pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ),)},)
+    py, px = ellfac(pol)
+    ε = 1.0 if isinstance(pol, str) else float(pol)
+    f1 = _pulse(pulseshape, λ0, τfwhm, τw, nm(energy, py), nm(power, py), ϕ)
+    f2 = _pulse(pulseshape, λ0, τfwhm, τw, nm(energy, px), nm(power, px),
+                _addphase(ϕ, math.pi / 2 * float(np.sign(ε))))
+    return ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)})
+
+
 def makemode_s(modes_, radius, gas, pressure, T, model, loss, pol):
     """``makemode_s`` / ``makemodes_pol`` (Interface.jl:478-513) for a constant fill: a mode
     name gives one mode; a number n gives HE11..HE1n; a tuple gives each of its modes; with
@@ -149,7 +201,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         envelope=False, thg=None, δt=1.0, kerr=True, plasma=None,
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
                         modes="HE11", radial_integral_rtol=1e-3, temperature=pd.roomtemp,
-                        rotation=True, vibration=True, rng=None, τw=None, ϕ=(), preionfrac=0.0):
+                        rotation=True, vibration=True, rng=None, τw=None, ϕ=(), preionfrac=0.0,
+                        polarisation="linear"):
     """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
     over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
     a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
@@ -164,7 +217,11 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     molecular gases and PPT otherwise, "ADK" or "PPT" names the rate (makeplasma!,
     Interface.jl:560-590), ``preionfrac`` is the pre-ionised fraction; ``ϕ`` are the input
     pulse's spectral phases and ``τw`` the natural width of a sech² pulse (makeinputs,
-    Interface.jl:621-632). ``shotnoise=True`` adds one photon
+    Interface.jl:621-632). ``polarisation`` ("linear", "x", "y", "circular" or an
+    ellipticity -1 <= ε <= 1, Interface.jl:285-287) other than linear propagates two
+    polarisation components: every HE1m mode twice (ϕ = 0 and π/2) in the multimode
+    transform, as the reference's ``needpol`` does (Interface.jl:376, 421-431, 478-489).
+    ``shotnoise=True`` adds one photon
     per mode to the input of every propagation mode (``fields.ShotNoise(rng)``, as
     ``shotnoise_maybe`` does, Interface.jl:389, 773-781); the default here is False, so that
     a set-up is reproducible unless noise is asked for."""
@@ -177,13 +234,15 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     # makegrid (Interface.jl:453-461)
     grid = EnvGrid(flength, λ0, λlims, trange, δt=δt, thg=thg) if envelope else \
         RealGrid(flength, λ0, λlims, trange, δt)
+    if needpol(polarisation) and isinstance(modes_, str):
+        modes_ = (modes_,)  # makemodes_pol: the mode in both polarisations
     if not isinstance(modes_, str) or parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
         if isinstance(modes_, (int, tuple, list)):
             return _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm,
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
                                          rotation, vibration, shotnoise, rng, preionfrac=preionfrac,
-                                         ϕ=ϕ, τw=τw)
+                                         ϕ=ϕ, τw=τw, polarisation=polarisation)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
@@ -244,7 +303,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
 def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
                           pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol,
                           temperature, rotation, vibration, shotnoise=False, rng=None, preionfrac=0.0,
-                          ϕ=(), τw=None):
+                          ϕ=(), τw=None, polarisation="linear"):
     """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
     linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
     (``makeinputs``, Interface.jl:721-733); with ``shotnoise`` one photon per mode in every
@@ -252,7 +311,7 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     from . import modal
     if isinstance(pressure, (tuple, list)) or isinstance(radius, (tuple, list)):
         raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
-    pol = needpol_modes(modes_)
+    pol = needpol(polarisation) or needpol_modes(modes_)
     ms = makemode_s(modes_, radius, gas, pressure, temperature, model, loss, pol)
     env = grid.kind == "env"
     thg = (not env) if thg is None else thg
@@ -271,8 +330,8 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     if raman:
         rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
         resp.append(RamanPolarEnv(grid.to, rr) if env else RamanPolarField(grid.to, rr, thg=thg))
-    fld = _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ)
-    Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, fld, ms, "xy" if pol else "y",
+    inputs = makeinputs_pol(pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation)
+    Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, inputs, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
     if shotnoise:
         noise = fields.ShotNoise(rng)

@@ -427,3 +427,29 @@ def test_multimode_setup_helpers():
     assert [(g.kind, g.n, g.m, g.ϕ) for g in got] == [("HE", 1, 12, 0.0), ("HE", 1, 12, math.pi / 2),
                                                      ("TE", 0, 1, 0.0)]
     assert needfull(got) and not needfull(makemode_s(2, A, GAS, PRES, pd.roomtemp, "full", False, False))
+
+
+@pytest.mark.parametrize("pol", ["circular", 0.5, -0.5, "x", "y"])
+def test_prop_capillary_polarisation_inputs(pol):
+    """polarisation (Interface.jl:285-287, 421-431, 721-761): anything but linear propagates
+    HE11 in both polarisations (ϕ = 0, π/2) with the multimode transform; x and y go into one
+    component, circular splits the energy in halves and an ellipticity ε into
+    (1 - ε²/(1+ε²), ε²/(1+ε²)), the second component π/2 sign(ε) behind in phase."""
+    from luna_b200.interface import prop_capillary_args
+    kw = dict(λ0=800e-9, τfwhm=30e-15, energy=1e-6, λlims=(160e-9, 3000e-9), trange=0.5e-12)
+    p = prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, polarisation=pol, **kw)
+    lin = prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, modes=("HE11",), **kw)
+    assert p.transform.kind == "modal" and p.transform.ts.npol == 2 and p.Eω.shape[1] == 2
+    E0, E1, L = p.Eω[:, 0], p.Eω[:, 1], lin.Eω[:, 0]
+    tol = 1e-12 * np.abs(L).max()
+    if pol == "x":
+        assert np.allclose(E0, L, rtol=0, atol=tol) and not E1.any()
+    elif pol == "y":
+        assert np.allclose(E1, L, rtol=0, atol=tol) and not E0.any()
+    else:
+        ε = 1.0 if pol == "circular" else pol
+        py, px = 1 - ε ** 2 / (1 + ε ** 2), ε ** 2 / (1 + ε ** 2)
+        assert np.allclose(E0, np.sqrt(py) * L, rtol=0, atol=tol)
+        assert np.allclose(E1, np.sqrt(px) * L * np.exp(-1j * np.pi / 2 * np.sign(ε)), rtol=0, atol=tol)
+    with pytest.raises(ValueError):
+        prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, polarisation="diagonal", **kw)

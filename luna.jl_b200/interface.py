@@ -123,22 +123,38 @@ def _addphase(ϕ, phase):
     return ϕ
 
 
-def makeinputs_pol(pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation):
-    """``makeinputs`` for one pulse in the lowest mode (Interface.jl:621-632, 638-649, 721-733,
-    751-761): linear or x polarisation in mode 1, y in mode 2, circular or elliptical split
-    into (mode 1, fraction py) and (mode 2, fraction px, constant phase + π/2 sign(ε))."""
-    nm = lambda x, f: None if x is None else x * f
-    pol = polarisation.lstrip(":") if isinstance(polarisation, str) else polarisation
+def findmode(ms, pulse):
+    """``findmode`` (Interface.jl:638-656): the 1-based indices of the modes a pulse goes
+    into: the lowest mode (both of its polarisations unless linear), or every mode of the
+    named kind, n and m."""
+    if pulse.mode == "lowest":
+        return [1] if pulse.polarisation == "linear" else [1, 2]
+    md = parse_mode(pulse.mode)
+    return [i + 1 for i, m in enumerate(ms) if (m.kind, m.n, m.m) == (md["kind"], md["n"], md["m"])]
+
+
+def makeinputs(ms, pulse):
+    """``makeinputs`` for one pulse (Interface.jl:721-733, 751-761): linear or x polarisation
+    into its first mode, y into the second, circular or elliptical split into (first mode,
+    fraction py) and (second mode, fraction px, constant phase + π/2 sign(ε))."""
+    idcs = findmode(ms, pulse)
+    if not idcs:
+        raise ValueError(f"Mode {pulse.mode} not found in mode list")
+    pol = pulse.polarisation.lstrip(":") if isinstance(pulse.polarisation, str) else pulse.polarisation
+    f = pulse.field
     if pol in ("linear", "x"):
-        return ({"mode": 1, "fields": (_pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ),)},)
+        return ({"mode": idcs[0], "fields": (f,)},)
+    if len(idcs) != 2:
+        raise ValueError("Modes not set up for circular/elliptical polarisation")
     if pol == "y":
-        return ({"mode": 2, "fields": (_pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ),)},)
+        return ({"mode": idcs[1], "fields": (f,)},)
     py, px = ellfac(pol)
     ε = 1.0 if isinstance(pol, str) else float(pol)
-    f1 = _pulse(pulseshape, λ0, τfwhm, τw, nm(energy, py), nm(power, py), ϕ)
-    f2 = _pulse(pulseshape, λ0, τfwhm, τw, nm(energy, px), nm(power, px),
-                _addphase(ϕ, math.pi / 2 * float(np.sign(ε))))
-    return ({"mode": 1, "fields": (f1,)}, {"mode": 2, "fields": (f2,)})
+    nm = lambda x, k: None if x is None else x * k
+    f1 = fields.PulseField(f.λ0, f.Itshape, nm(f.energy, py), nm(f.power, py), f.ϕ)
+    f2 = fields.PulseField(f.λ0, f.Itshape, nm(f.energy, px), nm(f.power, px),
+                           _addphase(f.ϕ, math.pi / 2 * float(np.sign(ε))))
+    return ({"mode": idcs[0], "fields": (f1,)}, {"mode": idcs[1], "fields": (f2,)})
 
 
 def makemode_s(modes_, radius, gas, pressure, T, model, loss, pol):
@@ -169,6 +185,14 @@ def makemode_s(modes_, radius, gas, pressure, T, model, loss, pol):
 def needfull(ms):
     """``needfull`` (Interface.jl:801-803): the 2-D integral unless every mode is HE1m."""
     return not all(m.kind == "HE" and m.n == 1 for m in ms)
+
+
+def _pulses(pulses, pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation):
+    """The ``pulses`` list, or the one pulse the scalar arguments describe (Interface.jl:621-632)."""
+    from .pulses import Pulse
+    if pulses is not None:
+        return list(pulses)
+    return [Pulse(_pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ), "lowest", polarisation)]
 
 
 def _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ):
@@ -202,7 +226,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                         raman=None, loss=True, model="full", saveN=201, ppt_N=2 ** 16,
                         modes="HE11", radial_integral_rtol=1e-3, temperature=pd.roomtemp,
                         rotation=True, vibration=True, rng=None, τw=None, ϕ=(), preionfrac=0.0,
-                        polarisation="linear"):
+                        polarisation="linear", pulses=None):
     """Capillary set-up (Interface.jl:360-401). ``pressure`` is a number, a (p0, p1) gradient
     over the fibre or (Z, P) nodes (Capillary.gradient, Capillary.jl:306-337); ``radius`` is
     a number or (Z, A) nodes of a piecewise-linear taper (a z-dependent radius,
@@ -221,7 +245,9 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     ellipticity -1 <= ε <= 1, Interface.jl:285-287) other than linear propagates two
     polarisation components: every HE1m mode twice (ϕ = 0 and π/2) in the multimode
     transform, as the reference's ``needpol`` does (Interface.jl:376, 421-431, 478-489).
-    ``shotnoise=True`` adds one photon
+    ``pulses`` (a list of ``pulses.GaussPulse`` / ``SechPulse``, each with its mode and
+    polarisation) replaces the single pulse of the scalar arguments (Interface.jl:634-636,
+    735-739). ``shotnoise=True`` adds one photon
     per mode to the input of every propagation mode (``fields.ShotNoise(rng)``, as
     ``shotnoise_maybe`` does, Interface.jl:389, 773-781); the default here is False, so that
     a set-up is reproducible unless noise is asked for."""
@@ -234,7 +260,8 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
     # makegrid (Interface.jl:453-461)
     grid = EnvGrid(flength, λ0, λlims, trange, δt=δt, thg=thg) if envelope else \
         RealGrid(flength, λ0, λlims, trange, δt)
-    if needpol(polarisation) and isinstance(modes_, str):
+    pl = _pulses(pulses, pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation)
+    if any(needpol(q.polarisation) for q in pl) and isinstance(modes_, str):
         modes_ = (modes_,)  # makemodes_pol: the mode in both polarisations
     if not isinstance(modes_, str) or parse_mode(modes_) != {"kind": "HE", "n": 1, "m": 1}:
         if isinstance(modes_, (int, tuple, list)):
@@ -242,7 +269,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
                                          energy, power, pulseshape, thg, kerr, plasma, raman, loss,
                                          model, saveN, ppt_N, radial_integral_rtol, temperature,
                                          rotation, vibration, shotnoise, rng, preionfrac=preionfrac,
-                                         ϕ=ϕ, τw=τw, polarisation=polarisation)
+                                         ϕ=ϕ, τw=τw, polarisation=polarisation, pulses=pl)
     grad = None
     tapered = isinstance(radius, (tuple, list)) or type(radius).__name__ == "Taper"
     if isinstance(pressure, (tuple, list)) or tapered:
@@ -293,8 +320,14 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
         linop, βconst, β1 = make_const_linop(grid, mode, λ0, thg=thg)
         norm = norm_mode_average(grid, βconst)
         transform = TransModeAvg(grid, resp, density, norm, aeff)
-    fld = _pulse(pulseshape, λ0, τfwhm, τw, energy, power, ϕ)
-    Eω = fld(grid)
+    # doinput_sm (Luna.jl:94-113): every pulse goes into the one propagation mode
+    md = parse_mode(modes_)
+    for q in pl:
+        if q.mode != "lowest" and parse_mode(q.mode) != md:
+            raise ValueError("For mode-averaged propagation, all inputs must be in 1st mode.")
+    Eω = pl[0].field(grid)
+    for q in pl[1:]:
+        Eω = Eω + q.field(grid)
     if shotnoise:
         Eω = Eω + fields.ShotNoise(rng)(grid)
     return Problem(Eω, grid, linop, transform, saveN)
@@ -303,7 +336,7 @@ def prop_capillary_args(radius, flength, gas, pressure, *, λlims, trange, λ0, 
 def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τfwhm, energy, power,
                           pulseshape, thg, kerr, plasma, raman, loss, model, saveN, ppt_N, rtol,
                           temperature, rotation, vibration, shotnoise=False, rng=None, preionfrac=0.0,
-                          ϕ=(), τw=None, polarisation="linear"):
+                          ϕ=(), τw=None, polarisation="linear", pulses=None):
     """Multimode branch of ``prop_capillary_args``: ``setup(grid, modes, ...)`` with a constant
     linear operator (Interface.jl:805-812) and linearly polarised input in the first mode
     (``makeinputs``, Interface.jl:721-733); with ``shotnoise`` one photon per mode in every
@@ -311,7 +344,8 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     from . import modal
     if isinstance(pressure, (tuple, list)) or isinstance(radius, (tuple, list)):
         raise NotImplementedError("multimode propagation with a pressure gradient or a taper is not supported")
-    pol = needpol(polarisation) or needpol_modes(modes_)
+    pl = _pulses(pulses, pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation)
+    pol = any(needpol(q.polarisation) for q in pl) or needpol_modes(modes_)
     ms = makemode_s(modes_, radius, gas, pressure, temperature, model, loss, pol)
     env = grid.kind == "env"
     thg = (not env) if thg is None else thg
@@ -330,7 +364,7 @@ def _prop_capillary_modal(radius, flength, gas, pressure, grid, modes_, λ0, τf
     if raman:
         rr = _raman.raman_response(grid.to, gas, rotation=rotation, vibration=vibration, temp=temperature)
         resp.append(RamanPolarEnv(grid.to, rr) if env else RamanPolarField(grid.to, rr, thg=thg))
-    inputs = makeinputs_pol(pulseshape, λ0, τfwhm, τw, energy, power, ϕ, polarisation)
+    inputs = tuple(x for q in pl for x in makeinputs(ms, q))
     Eω, t = modal.setup_modal(grid, pd.density(gas, pressure, temperature), resp, inputs, ms, "xy" if pol else "y",
                               full=needfull(ms), rtol=rtol)
     if shotnoise:

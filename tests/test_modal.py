@@ -453,3 +453,28 @@ def test_prop_capillary_polarisation_inputs(pol):
         assert np.allclose(E1, np.sqrt(px) * L * np.exp(-1j * np.pi / 2 * np.sign(ε)), rtol=0, atol=tol)
     with pytest.raises(ValueError):
         prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, polarisation="diagonal", **kw)
+
+
+def test_prop_capillary_pulse_list():
+    """pulses (Interface.jl:634-636, 638-656, 735-739): a two-colour input adds both fields
+    in mode-averaged propagation; in a multimode set-up each pulse goes into its named mode;
+    a mode-averaged input in another mode, or a mode missing from the list, is an error."""
+    from luna_b200 import fields
+    from luna_b200.interface import prop_capillary_args
+    from luna_b200.pulses import GaussPulse
+    kw = dict(λ0=800e-9, λlims=(160e-9, 3000e-9), trange=0.5e-12)
+    two = [GaussPulse(λ0=800e-9, τfwhm=30e-15, energy=1e-6), GaussPulse(λ0=400e-9, τfwhm=40e-15, energy=0.2e-6)]
+    p = prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, pulses=two, **kw)
+    ref = fields.GaussField(800e-9, 30e-15, energy=1e-6)(p.grid) + fields.GaussField(400e-9, 40e-15, energy=0.2e-6)(p.grid)
+    assert getattr(p.transform, "kind", None) != "modal" and np.allclose(p.Eω, ref, rtol=1e-13, atol=0)
+    mm = [GaussPulse(λ0=800e-9, τfwhm=30e-15, energy=1e-6), GaussPulse(λ0=800e-9, τfwhm=30e-15, energy=0.3e-6, mode="HE12")]
+    q = prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, pulses=mm, modes=3, **kw)
+    one = fields.GaussField(800e-9, 30e-15, energy=1e-6)(q.grid)
+    assert np.allclose(q.Eω[:, 0], one, rtol=1e-13, atol=0)
+    assert np.allclose(q.Eω[:, 1], np.sqrt(0.3) * one, rtol=1e-12, atol=1e-12 * np.abs(one).max())
+    assert not q.Eω[:, 2].any()
+    with pytest.raises(ValueError):
+        prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, pulses=[mm[1]], **kw)
+    with pytest.raises(ValueError):
+        prop_capillary_args(50e-6, 1e-2, "Ar", 1.0, pulses=[GaussPulse(λ0=800e-9, τfwhm=30e-15, energy=1e-6,
+                                                                       mode="HE14")], modes=3, **kw)
